@@ -1,0 +1,1046 @@
+// ORACLE — TEST INFRASTRUCTURE ONLY. Nothing in the product links, loads or calls this file; only the
+// tests, the smoke check and bench.py's CPU-baseline leg do, as the checker and the timed CPU reference.
+//
+// A CPU restatement, in C++, of the Integrity engine's SPH giant-impact step (sean-reid/BotheadStudios,
+// project `integrity-engine`). The reference is Rust + WGSL run through wgpu; it cannot be compiled here
+// (no Rust toolchain) and its GPU path needs a graphics API that does not exist on these machines, so each
+// function below restates the reference's arithmetic from its source and cites the file:line it follows.
+//
+// Two precisions are restated on purpose:
+//   * f32 "GPU-parity" functions follow the WGSL kernels' operation order (shaders/sph_step.wgsl,
+//     shaders/bh_gravity.wgsl). They are compiled with -ffp-contract=off so a product kernel that uses the
+//     same single-rounding operations reproduces integer/quantised outputs (Morton codes, permutation,
+//     tree topology, neighbour sets) bit for bit and float outputs to the last few ulps.
+//   * f64 functions follow the CPU physics of record (crates/engine/src/hydrostatic.rs, eos.rs, bhtree.rs,
+//     neighbors.rs, atmosphere.rs) and the f64 verifier (tools/sph-verify/src/main.rs). HydroBody::step is
+//     also the timed CPU baseline (single thread = the reference; an OpenMP gather variant for all cores).
+//
+// Parity pinning: the reference ships no golden-vector files. This oracle is pinned against the reference's
+// own known-answer tests (exact EOS parameters, EOS invariants, Barnes-Hut theta bounds, the neighbour-grid
+// pair-set identity, bbox/Morton exactness and coincident-point codes, Karras tree structure, root COM,
+// and the sph-verify force and 50-step integration bounds); see tests/test_oracle_pins.py.
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <numeric>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+constexpr double kPi = 3.14159265358979323846;
+constexpr float kPiF = 3.14159265359f;  // sph_step.wgsl:20
+
+// ---------------------------------------------------------------------------------------------------
+// Tillotson EOS. f64 form: crates/engine/src/eos.rs:52-96. f32 form: shaders/sph_step.wgsl:78-100.
+// The f64 parameter block is [rho0, a, b, A, B, E0, E_iv, E_cv, alpha, beta].
+// The f32 block is the 48-byte SphEos layout (gpu_sph.rs:42; sph_step.wgsl:43):
+// [rho0, a, b, A, B, E0, E_iv, E_cv, alpha, beta, _p0, _p1].
+// ---------------------------------------------------------------------------------------------------
+double pressure64(const double* e, double rho, double u) {
+  // eos.rs:52-69 (pressure), :71-74 (p_compressed), :77-83 (p_expanded)
+  const double rho0 = e[0], a = e[1], b = e[2], A = e[3], B = e[4], e0 = e[5], eiv = e[6], ecv = e[7],
+               al = e[8], be = e[9];
+  rho = std::max(rho, 1.0e-9);
+  const double eta = rho / rho0;
+  const double mu = eta - 1.0;
+  const double omega_c = u / (e0 * eta * eta) + 1.0;
+  const double pc = (a + b / omega_c) * rho * u + A * mu + B * mu * mu;
+  if (eta >= 1.0 || u <= eiv) return pc;
+  const double omega_e = u / (e0 * eta * eta) + 1.0;
+  const double z = rho0 / rho - 1.0;
+  const double pe = a * rho * u + (b * rho * u / omega_e + A * mu * std::exp(-be * z)) * std::exp(-al * z * z);
+  if (u >= ecv) return pe;
+  return ((u - eiv) * pe + (ecv - u) * pc) / (ecv - eiv);
+}
+
+// eos.rs:88-96: central differences with dρ = 1e-4 ρ and du = 1e-4|u| + 1.
+double sound_speed_sq64(const double* e, double rho, double u) {
+  rho = std::max(rho, 1.0e-9);
+  const double dr = rho * 1.0e-4;
+  const double du = std::fabs(u) * 1.0e-4 + 1.0;
+  const double dpdr = (pressure64(e, rho + dr, u) - pressure64(e, rho - dr, u)) / (2.0 * dr);
+  const double dpdu = (pressure64(e, rho, u + du) - pressure64(e, rho, u - du)) / (2.0 * du);
+  const double p = pressure64(e, rho, u);
+  return std::max(dpdr + p / (rho * rho) * dpdu, 0.0);
+}
+
+// tools/sph-verify/src/main.rs:97-105: the f64 restatement that follows the WGSL 1e-3 steps.
+double sound_speed64_wgsl(const double* e, double rho, double u, double du_floor) {
+  const double r = std::max(rho, 1.0e-9);
+  const double dr = r * 1.0e-3;
+  const double dp = (pressure64(e, r + dr, u) - pressure64(e, r - dr, u)) / (2.0 * dr);
+  const double du = std::fabs(u) * 1.0e-3 + du_floor;
+  const double dpu = (pressure64(e, r, u + du) - pressure64(e, r, u - du)) / (2.0 * du);
+  const double pp = pressure64(e, r, u);
+  return std::sqrt(std::max(dp + pp / (r * r) * dpu, 0.0));
+}
+
+// sph_step.wgsl:78-89. rho_floor is 1e-9 in the reference's SI units.
+float pressure32(const float* e, float rho, float u, float rho_floor) {
+  const float r = std::max(rho, rho_floor);
+  const float eta = r / e[0];
+  const float mu = eta - 1.0f;
+  const float omega = u / (e[5] * eta * eta) + 1.0f;
+  const float p_c = (e[1] + e[2] / omega) * r * u + e[3] * mu + e[4] * mu * mu;
+  if (eta >= 1.0f || u <= e[6]) return p_c;
+  const float z = e[0] / r - 1.0f;
+  const float p_e = e[1] * r * u + (e[2] * r * u / omega + e[3] * mu * std::exp(-e[9] * z)) * std::exp(-e[8] * z * z);
+  if (u >= e[7]) return p_e;
+  return ((u - e[6]) * p_e + (e[7] - u) * p_c) / (e[7] - e[6]);
+}
+
+// sph_step.wgsl:90-100. du_floor is the "+ 1.0" (J/kg) of dfdu, rho_floor the 1e-9 of max(rho, 1e-9).
+float sound_speed32(const float* e, float rho, float u, float du_floor, float rho_floor) {
+  const float r = std::max(rho, rho_floor);
+  const float dr = r * 1.0e-3f;
+  const float dp = (pressure32(e, r + dr, u, rho_floor) - pressure32(e, r - dr, u, rho_floor)) / (2.0f * dr);
+  const float p = pressure32(e, r, u, rho_floor);
+  const float du = std::fabs(u) * 1.0e-3f + du_floor;
+  const float dfdu = (pressure32(e, r, u + du, rho_floor) - pressure32(e, r, u - du, rho_floor)) / (2.0f * du);
+  return std::sqrt(std::max(dp + p / (r * r) * dfdu, 0.0f));
+}
+
+// ---------------------------------------------------------------------------------------------------
+// SPH kernels. Cubic spline with support radius h: f64 atmosphere.rs:39-62, f32 sph_step.wgsl:64-77.
+// Wendland C2 (Wendland 1995; Dehnen & Aly 2012, MNRAS 425, Table 1) written from the formula with the
+// same support-radius-h convention: W = 21/(2π h³)(1-q)^4(1+4q), dW/dr = 21/(2π h³)·(-20 q (1-q)^3)/h.
+// ---------------------------------------------------------------------------------------------------
+double w_cubic64(double r, double h) {  // atmosphere.rs:39-49
+  const double q = r / h;
+  const double sigma = 8.0 / (kPi * h * h * h);
+  if (q < 0.5) return sigma * (6.0 * (q * q * q - q * q) + 1.0);
+  if (q < 1.0) return sigma * 2.0 * (1.0 - q) * (1.0 - q) * (1.0 - q);
+  return 0.0;
+}
+double dw_cubic64(double r, double h) {  // atmosphere.rs:52-62
+  const double q = r / h;
+  const double sigma = 8.0 / (kPi * h * h * h * h);
+  if (q < 0.5) return sigma * (18.0 * q * q - 12.0 * q);
+  if (q < 1.0) return sigma * -6.0 * (1.0 - q) * (1.0 - q);
+  return 0.0;
+}
+double w_cubic64_verify(double r, double h) {  // tools/sph-verify/src/main.rs:70-74
+  const double q = r / h;
+  const double sig = 8.0 / (kPi * h * h * h);
+  if (q < 0.5) return sig * (1.0 - 6.0 * q * q + 6.0 * q * q * q);
+  if (q < 1.0) { const double t = 1.0 - q; return sig * 2.0 * t * t * t; }
+  return 0.0;
+}
+double dw_cubic64_verify(double r, double h) {  // tools/sph-verify/src/main.rs:75-79
+  const double q = r / h;
+  const double sig = 8.0 / (kPi * h * h * h);
+  if (q < 0.5) return sig * (-12.0 * q + 18.0 * q * q) / h;
+  if (q < 1.0) { const double t = 1.0 - q; return sig * (-6.0 * t * t) / h; }
+  return 0.0;
+}
+double w_wendland64(double r, double h) {
+  const double q = r / h;
+  if (q >= 1.0) return 0.0;
+  const double t = 1.0 - q;
+  return 21.0 / (2.0 * kPi * h * h * h) * t * t * t * t * (1.0 + 4.0 * q);
+}
+double dw_wendland64(double r, double h) {
+  const double q = r / h;
+  if (q >= 1.0) return 0.0;
+  const double t = 1.0 - q;
+  return 21.0 / (2.0 * kPi * h * h * h) * (-20.0 * q * t * t * t) / h;
+}
+float w_cubic32(float r, float h) {  // sph_step.wgsl:64-70
+  const float q = r / h;
+  const float sig = 8.0f / (kPiF * h * h * h);
+  if (q < 0.5f) return sig * (1.0f - 6.0f * q * q + 6.0f * q * q * q);
+  if (q < 1.0f) { const float t = 1.0f - q; return sig * 2.0f * t * t * t; }
+  return 0.0f;
+}
+float dw_cubic32(float r, float h) {  // sph_step.wgsl:71-77
+  const float q = r / h;
+  const float sig = 8.0f / (kPiF * h * h * h);
+  if (q < 0.5f) return sig * (-12.0f * q + 18.0f * q * q) / h;
+  if (q < 1.0f) { const float t = 1.0f - q; return sig * (-6.0f * t * t) / h; }
+  return 0.0f;
+}
+float w_wendland32(float r, float h) {
+  const float q = r / h;
+  if (q >= 1.0f) return 0.0f;
+  const float t = 1.0f - q;
+  return 21.0f / (2.0f * kPiF * h * h * h) * t * t * t * t * (1.0f + 4.0f * q);
+}
+float dw_wendland32(float r, float h) {
+  const float q = r / h;
+  if (q >= 1.0f) return 0.0f;
+  const float t = 1.0f - q;
+  return 21.0f / (2.0f * kPiF * h * h * h) * (-20.0f * q * t * t * t) / h;
+}
+inline float kern_w32(int kind, float r, float h) { return kind == 1 ? w_wendland32(r, h) : w_cubic32(r, h); }
+inline float kern_dw32(int kind, float r, float h) { return kind == 1 ? dw_wendland32(r, h) : dw_cubic32(r, h); }
+
+// Pair distance exactly as the product computes it: single-rounded products and sums, left to right, then
+// an IEEE square root (the WGSL `length(pi.pos - pj.pos)` of sph_step.wgsl:141 with no contraction).
+inline float pair_r32(const float* pi, const float* pj) {
+  const float dx = pi[0] - pj[0], dy = pi[1] - pj[1], dz = pi[2] - pj[2];
+  return std::sqrt((dx * dx + dy * dy) + dz * dz);
+}
+
+// ---------------------------------------------------------------------------------------------------
+// Morton codes (bh_gravity.wgsl:49-108; CPU twin gpu_gravity.rs:336-357,495-502).
+// ---------------------------------------------------------------------------------------------------
+uint32_t expand_bits(uint32_t v) {  // bh_gravity.wgsl:82-89
+  v &= 0x000003ffu;
+  v = (v * 0x00010001u) & 0xff0000ffu;
+  v = (v * 0x00000101u) & 0x0f00f00fu;
+  v = (v * 0x00000011u) & 0xc30c30c3u;
+  v = (v * 0x00000005u) & 0x49249249u;
+  return v;
+}
+uint32_t morton32(const float* p, const float* lo, const float* hi) {  // bh_gravity.wgsl:91-98,105
+  uint32_t q[3];
+  for (int k = 0; k < 3; ++k) {
+    const float ext = std::max(hi[k] - lo[k], 1.0e-30f);
+    float u = (p[k] - lo[k]) / ext;
+    u = std::min(std::max(u, 0.0f), 1.0f);
+    float f = std::floor(u * 1024.0f);
+    f = std::min(std::max(f, 0.0f), 1023.0f);
+    q[k] = static_cast<uint32_t>(f);
+  }
+  return expand_bits(q[0]) * 4u + expand_bits(q[1]) * 2u + expand_bits(q[2]);
+}
+
+inline int clz32(uint32_t x) { return x == 0 ? 32 : __builtin_clz(x); }
+
+// Karras δ with the index tiebreak, bh_gravity.wgsl:114-120.
+inline int kdelta(const uint32_t* codes, int L, int i, int j) {
+  if (j < 0 || j >= L) return -1;
+  const uint32_t ci = codes[i], cj = codes[j];
+  if (ci == cj) return 32 + clz32(static_cast<uint32_t>(i) ^ static_cast<uint32_t>(j));
+  return clz32(ci ^ cj);
+}
+
+// One internal node of the Karras build, bh_gravity.wgsl:135-184. Returns (left, right).
+void karras_node(const uint32_t* codes, int L, int i, uint32_t* left, uint32_t* right) {
+  const int d = kdelta(codes, L, i, i + 1) > kdelta(codes, L, i, i - 1) ? 1 : -1;
+  const int dmin = kdelta(codes, L, i, i - d);
+  int lmax = 2;
+  while (kdelta(codes, L, i, i + lmax * d) > dmin) lmax *= 2;
+  int l = 0;
+  for (int t = lmax / 2; t >= 1; t /= 2)
+    if (kdelta(codes, L, i, i + (l + t) * d) > dmin) l += t;
+  const int j = i + l * d;
+  const int first = std::min(i, j), last = std::max(i, j);
+  int split = first;
+  const uint32_t fc = codes[first], lc = codes[last];
+  if (fc == lc) {
+    split = (first + last) >> 1;
+  } else {
+    const int cpfx = clz32(fc ^ lc);
+    int step = last - first;
+    for (;;) {
+      step = (step + 1) >> 1;
+      const int ns = split + step;
+      if (ns < last && clz32(fc ^ codes[ns]) > cpfx) split = ns;
+      if (step <= 1) break;
+    }
+  }
+  const bool ll = (split == first), rl = (split + 1 == last);
+  *left = ll ? static_cast<uint32_t>((L - 1) + split) : static_cast<uint32_t>(split);
+  *right = rl ? static_cast<uint32_t>((L - 1) + split + 1) : static_cast<uint32_t>(split + 1);
+}
+
+// ---------------------------------------------------------------------------------------------------
+// Uniform cell list used only to enumerate candidate pairs; the neighbour predicate is always exact.
+// ---------------------------------------------------------------------------------------------------
+struct CellList {
+  double cell = 1.0;
+  std::vector<int64_t> keys;     // sorted cell keys
+  std::vector<int> start, order;  // order[] = particle indices sorted by cell key (stable)
+  static int64_t pack(int64_t x, int64_t y, int64_t z) {
+    return ((x + (1 << 20)) << 42) | ((y + (1 << 20)) << 21) | (z + (1 << 20));
+  }
+  template <class GetPos>
+  void build(int n, double cell_size, GetPos pos) {
+    cell = std::max(cell_size, 1.0e-30);
+    std::vector<int64_t> k(n);
+    for (int i = 0; i < n; ++i) {
+      double p[3];
+      pos(i, p);
+      k[i] = pack((int64_t)std::floor(p[0] / cell), (int64_t)std::floor(p[1] / cell), (int64_t)std::floor(p[2] / cell));
+    }
+    order.resize(n);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return k[a] < k[b]; });
+    keys.clear();
+    start.clear();
+    for (int s = 0; s < n; ++s) {
+      if (s == 0 || k[order[s]] != k[order[s - 1]]) {
+        keys.push_back(k[order[s]]);
+        start.push_back(s);
+      }
+    }
+    start.push_back(n);
+  }
+  // Calls f(j) for every particle in the 27 cells around point p.
+  template <class F>
+  void around(const double* p, F f) const {
+    const int64_t cx = (int64_t)std::floor(p[0] / cell), cy = (int64_t)std::floor(p[1] / cell),
+                  cz = (int64_t)std::floor(p[2] / cell);
+    for (int dz = -1; dz <= 1; ++dz)
+      for (int dy = -1; dy <= 1; ++dy)
+        for (int dx = -1; dx <= 1; ++dx) {
+          const int64_t key = pack(cx + dx, cy + dy, cz + dz);
+          auto it = std::lower_bound(keys.begin(), keys.end(), key);
+          if (it == keys.end() || *it != key) continue;
+          const size_t c = it - keys.begin();
+          for (int s = start[c]; s < start[c + 1]; ++s) f(order[s]);
+        }
+  }
+};
+
+// ---------------------------------------------------------------------------------------------------
+// f64 Barnes-Hut octree, crates/engine/src/bhtree.rs:21-190 (BRUTE_BELOW 1024, MAX_DEPTH 28, MAC
+// (2·half)/dist < θ with dist = sqrt(|d|²+ε²)).
+// ---------------------------------------------------------------------------------------------------
+struct OctNode {
+  double center[3], half, com[3], mass;
+  int children[8];
+  int leaf_begin, leaf_end;  // into OctTree::leaf_idx; empty range = internal
+};
+struct OctTree {
+  std::vector<OctNode> nodes;
+  std::vector<int> leaf_idx;
+  double theta = 0.5, soft2 = 0.0, G = 6.674e-11;
+  int n = 0;
+  const double* pos = nullptr;
+  const double* mass = nullptr;
+
+  int build_node(std::vector<int>& idx, const double* c, double half, int depth) {
+    const int id = (int)nodes.size();
+    double m = 0.0, com[3] = {0, 0, 0};
+    for (int i : idx) {
+      m += mass[i];
+      for (int k = 0; k < 3; ++k) com[k] += pos[3 * i + k] * mass[i];
+    }
+    OctNode nd;
+    for (int k = 0; k < 3; ++k) {
+      nd.center[k] = c[k];
+      nd.com[k] = m > 0.0 ? com[k] / m : c[k];
+    }
+    nd.half = half;
+    nd.mass = m;
+    for (int o = 0; o < 8; ++o) nd.children[o] = -1;
+    nd.leaf_begin = nd.leaf_end = 0;
+    nodes.push_back(nd);
+    if (idx.size() <= 1 || depth >= 28) {
+      nodes[id].leaf_begin = (int)leaf_idx.size();
+      leaf_idx.insert(leaf_idx.end(), idx.begin(), idx.end());
+      nodes[id].leaf_end = (int)leaf_idx.size();
+      return id;
+    }
+    std::vector<int> oct[8];
+    for (int i : idx) {
+      const double* p = pos + 3 * i;
+      const int o = (p[0] >= c[0] ? 1 : 0) | (p[1] >= c[1] ? 2 : 0) | (p[2] >= c[2] ? 4 : 0);
+      oct[o].push_back(i);
+    }
+    idx.clear();
+    idx.shrink_to_fit();
+    const double ch = half * 0.5;
+    for (int o = 0; o < 8; ++o) {
+      if (oct[o].empty()) continue;
+      const double cc[3] = {c[0] + ((o & 1) ? ch : -ch), c[1] + ((o & 2) ? ch : -ch), c[2] + ((o & 4) ? ch : -ch)};
+      const int cid = build_node(oct[o], cc, ch, depth + 1);
+      nodes[id].children[o] = cid;
+    }
+    return id;
+  }
+  void build(const double* p, const double* m, int n_, double th, double soft, double g) {
+    pos = p; mass = m; n = n_; theta = th; soft2 = soft * soft; G = g;
+    nodes.clear(); leaf_idx.clear();
+    if (n < 1024) return;  // BRUTE_BELOW
+    double lo[3], hi[3];
+    for (int k = 0; k < 3; ++k) lo[k] = hi[k] = p[k];
+    for (int i = 1; i < n; ++i)
+      for (int k = 0; k < 3; ++k) {
+        lo[k] = std::min(lo[k], p[3 * i + k]);
+        hi[k] = std::max(hi[k], p[3 * i + k]);
+      }
+    double c[3], ext = 0.0;
+    for (int k = 0; k < 3; ++k) { c[k] = (lo[k] + hi[k]) * 0.5; ext = std::max(ext, hi[k] - lo[k]); }
+    const double half = std::max(ext * 0.5, 1.0e-9) * 1.0001;
+    std::vector<int> all(n);
+    std::iota(all.begin(), all.end(), 0);
+    nodes.reserve(2 * (size_t)n);
+    build_node(all, c, half, 0);
+  }
+  void accel_on(int i, int node, double* a) const {
+    const OctNode& nd = nodes[node];
+    const double* pi = pos + 3 * i;
+    if (nd.leaf_end > nd.leaf_begin) {
+      for (int s = nd.leaf_begin; s < nd.leaf_end; ++s) {
+        const int j = leaf_idx[s];
+        if (j == i) continue;
+        const double d[3] = {pos[3 * j] - pi[0], pos[3 * j + 1] - pi[1], pos[3 * j + 2] - pi[2]};
+        const double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2] + soft2;
+        const double g = G * mass[j] / (r2 * std::sqrt(r2));
+        for (int k = 0; k < 3; ++k) a[k] += d[k] * g;
+      }
+      return;
+    }
+    const double d[3] = {nd.com[0] - pi[0], nd.com[1] - pi[1], nd.com[2] - pi[2]};
+    const double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2] + soft2;
+    const double dist = std::sqrt(r2);
+    if ((2.0 * nd.half) / dist < theta) {
+      const double g = G * nd.mass / (r2 * dist);
+      for (int k = 0; k < 3; ++k) a[k] += d[k] * g;
+      return;
+    }
+    for (int o = 0; o < 8; ++o)
+      if (nd.children[o] >= 0) {
+        double b[3] = {0, 0, 0};
+        accel_on(i, nd.children[o], b);
+        for (int k = 0; k < 3; ++k) a[k] += b[k];
+      }
+  }
+  void accelerations(double* acc, int nthreads) const {
+    if (nodes.empty()) {  // brute force, bhtree.rs:118-131
+#pragma omp parallel for schedule(dynamic, 64) num_threads(nthreads)
+      for (int i = 0; i < n; ++i) {
+        double a[3] = {0, 0, 0};
+        for (int j = 0; j < n; ++j) {
+          if (i == j) continue;
+          const double d[3] = {pos[3 * j] - pos[3 * i], pos[3 * j + 1] - pos[3 * i + 1], pos[3 * j + 2] - pos[3 * i + 2]};
+          const double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2] + soft2;
+          const double g = G * mass[j] / (r2 * std::sqrt(r2));
+          for (int k = 0; k < 3; ++k) a[k] += d[k] * g;
+        }
+        for (int k = 0; k < 3; ++k) acc[3 * i + k] = a[k];
+      }
+      return;
+    }
+#pragma omp parallel for schedule(dynamic, 256) num_threads(nthreads)
+    for (int i = 0; i < n; ++i) {
+      double a[3] = {0, 0, 0};
+      accel_on(i, 0, a);
+      for (int k = 0; k < 3; ++k) acc[3 * i + k] = a[k];
+    }
+  }
+};
+
+// ---------------------------------------------------------------------------------------------------
+// HydroBody (crates/engine/src/hydrostatic.rs:241-374): the f64 CPU path of record and the timed baseline.
+// ---------------------------------------------------------------------------------------------------
+struct Hydro {
+  int n = 0, n_eos = 0;
+  std::vector<double> pos, vel, mass, u, h, rho, eos;  // eos: n_eos × 10
+  std::vector<int> mat;
+  double softening = 0.0, G = 6.674e-11, theta = 0.5, av_alpha = 1.0, av_beta = 2.0;
+  int kernel = 0;  // 0 cubic spline (reference), 1 Wendland C2
+
+  double W(double r, double hh) const { return kernel == 1 ? w_wendland64(r, hh) : w_cubic64(r, hh); }
+  double dW(double r, double hh) const { return kernel == 1 ? dw_wendland64(r, hh) : dw_cubic64(r, hh); }
+  double hmax() const { double m = 0.0; for (double x : h) m = std::max(m, x); return m; }
+
+  // compute_density, hydrostatic.rs:241-256. Single thread: the reference's symmetric i<j pair loop over
+  // the NeighborGrid (neighbors.rs:60-85). Multi-thread: a per-i gather over the same 27-cell candidates.
+  void compute_density(int nthreads) {
+    rho.assign(n, 0.0);
+    for (int i = 0; i < n; ++i) rho[i] = mass[i] * W(0.0, h[i]);
+    if (n < 512) {  // neighbors.rs:23 BRUTE_BELOW: all i<j pairs
+      for (int i = 0; i < n; ++i)
+        for (int j = i + 1; j < n; ++j) density_pair(i, j);
+      return;
+    }
+    CellList cl;
+    cl.build(n, hmax(), [&](int i, double* p) { for (int k = 0; k < 3; ++k) p[k] = pos[3 * i + k]; });
+    if (nthreads <= 1) {
+      for (int i = 0; i < n; ++i) cl.around(&pos[3 * i], [&](int j) { if (j > i) density_pair(i, j); });
+    } else {
+#pragma omp parallel for schedule(dynamic, 256) num_threads(nthreads)
+      for (int i = 0; i < n; ++i) {
+        double acc = 0.0;
+        cl.around(&pos[3 * i], [&](int j) {
+          if (j == i) return;
+          const double r = dist(i, j), hij = 0.5 * (h[i] + h[j]);
+          if (r < hij) acc += mass[j] * W(r, hij);
+        });
+        rho[i] += acc;
+      }
+    }
+  }
+  double dist(int i, int j) const {
+    const double d[3] = {pos[3 * i] - pos[3 * j], pos[3 * i + 1] - pos[3 * j + 1], pos[3 * i + 2] - pos[3 * j + 2]};
+    return std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+  }
+  void density_pair(int i, int j) {
+    const double r = dist(i, j), hij = 0.5 * (h[i] + h[j]);
+    if (r < hij) {
+      const double w = W(r, hij);
+      rho[i] += mass[j] * w;
+      rho[j] += mass[i] * w;
+    }
+  }
+
+  // forces_and_dudt, hydrostatic.rs:300-340: BH gravity + pressure + Monaghan AV + du/dt.
+  void forces(std::vector<double>& acc, std::vector<double>& dudt, int nthreads) {
+    acc.assign(3 * (size_t)n, 0.0);
+    dudt.assign(n, 0.0);
+    OctTree bh;
+    bh.build(pos.data(), mass.data(), n, theta, softening, G);
+    bh.accelerations(acc.data(), std::max(nthreads, 1));
+    std::vector<double> p(n), c(n);
+#pragma omp parallel for num_threads(std::max(nthreads, 1))
+    for (int i = 0; i < n; ++i) {
+      const double* e = &eos[10 * (size_t)mat[i]];
+      p[i] = pressure64(e, rho[i], u[i]);
+      c[i] = std::sqrt(sound_speed_sq64(e, rho[i], u[i]));
+    }
+    auto pair_terms = [&](int i, int j, double* ai, double& dui, double* aj, double& duj) -> bool {
+      const double dpos[3] = {pos[3 * i] - pos[3 * j], pos[3 * i + 1] - pos[3 * j + 1], pos[3 * i + 2] - pos[3 * j + 2]};
+      const double r = std::sqrt(dpos[0] * dpos[0] + dpos[1] * dpos[1] + dpos[2] * dpos[2]);
+      const double hij = 0.5 * (h[i] + h[j]);
+      if (r >= hij || r < 1.0e-9) return false;
+      const double dvel[3] = {vel[3 * i] - vel[3 * j], vel[3 * i + 1] - vel[3 * j + 1], vel[3 * i + 2] - vel[3 * j + 2]};
+      const double vr = dvel[0] * dpos[0] + dvel[1] * dpos[1] + dvel[2] * dpos[2];
+      double pi_ij = 0.0;
+      if (vr < 0.0) {
+        const double mu = hij * vr / (r * r + 0.01 * hij * hij);
+        const double c_bar = 0.5 * (c[i] + c[j]);
+        const double rho_bar = 0.5 * (rho[i] + rho[j]);
+        pi_ij = (-av_alpha * c_bar * mu + av_beta * mu * mu) / rho_bar;
+      }
+      const double coeff = p[i] / (rho[i] * rho[i]) + p[j] / (rho[j] * rho[j]) + pi_ij;
+      const double dw = dW(r, hij);
+      const double grad[3] = {dpos[0] / r * dw, dpos[1] / r * dw, dpos[2] / r * dw};
+      const double vdg = dvel[0] * grad[0] + dvel[1] * grad[1] + dvel[2] * grad[2];
+      for (int k = 0; k < 3; ++k) { ai[k] += grad[k] * (-coeff * mass[j]); if (aj) aj[k] += grad[k] * (coeff * mass[i]); }
+      dui += 0.5 * mass[j] * coeff * vdg;
+      duj += 0.5 * mass[i] * coeff * vdg;
+      return true;
+    };
+    if (n < 512) {
+      for (int i = 0; i < n; ++i)
+        for (int j = i + 1; j < n; ++j) pair_terms(i, j, &acc[3 * i], dudt[i], &acc[3 * j], dudt[j]);
+      return;
+    }
+    CellList cl;
+    cl.build(n, hmax(), [&](int i, double* q) { for (int k = 0; k < 3; ++k) q[k] = pos[3 * i + k]; });
+    if (nthreads <= 1) {
+      for (int i = 0; i < n; ++i)
+        cl.around(&pos[3 * i], [&](int j) { if (j > i) pair_terms(i, j, &acc[3 * i], dudt[i], &acc[3 * j], dudt[j]); });
+    } else {
+#pragma omp parallel for schedule(dynamic, 256) num_threads(nthreads)
+      for (int i = 0; i < n; ++i) {
+        double ai[3] = {0, 0, 0}, dui = 0.0, dummy = 0.0;
+        cl.around(&pos[3 * i], [&](int j) { if (j != i) pair_terms(i, j, ai, dui, nullptr, dummy); });
+        for (int k = 0; k < 3; ++k) acc[3 * i + k] += ai[k];
+        dudt[i] += dui;
+      }
+    }
+  }
+
+  // step, hydrostatic.rs:345-359 (KDK, two force evaluations, u clamped at 0).
+  void step(double dt, int nthreads) {
+    std::vector<double> a, du;
+    compute_density(nthreads);
+    forces(a, du, nthreads);
+    for (int i = 0; i < n; ++i) {
+      for (int k = 0; k < 3; ++k) vel[3 * i + k] += a[3 * i + k] * (0.5 * dt);
+      u[i] = std::max(u[i] + du[i] * (0.5 * dt), 0.0);
+      for (int k = 0; k < 3; ++k) pos[3 * i + k] += vel[3 * i + k] * dt;
+    }
+    compute_density(nthreads);
+    forces(a, du, nthreads);
+    for (int i = 0; i < n; ++i) {
+      for (int k = 0; k < 3; ++k) vel[3 * i + k] += a[3 * i + k] * (0.5 * dt);
+      u[i] = std::max(u[i] + du[i] * (0.5 * dt), 0.0);
+    }
+  }
+  // courant_dt, hydrostatic.rs:366-374 (assumes compute_density ran).
+  double courant_dt(double cfl, double sig_floor) const {
+    double dtm = INFINITY;
+    for (int i = 0; i < n; ++i) {
+      const double c = std::sqrt(sound_speed_sq64(&eos[10 * (size_t)mat[i]], rho[i], u[i]));
+      const double vv = std::sqrt(vel[3 * i] * vel[3 * i] + vel[3 * i + 1] * vel[3 * i + 1] + vel[3 * i + 2] * vel[3 * i + 2]);
+      dtm = std::min(dtm, h[i] / std::max(c + vv, sig_floor));
+    }
+    return cfl * dtm;
+  }
+};
+
+// ---------------------------------------------------------------------------------------------------
+// f32 SPH restatement of sph_step.wgsl cs_density (:120-149) and the SPH half of cs_forces (:153-211).
+// The neighbour SET is the reference's exact set {j != i : r < ½(h_i+h_j)} (the grid with its
+// cell-membership guard enumerates exactly this set, sph_step.wgsl:136-143); the sum runs over j ascending.
+// ---------------------------------------------------------------------------------------------------
+void neighbour_sets32(const float* pos4, int n, std::vector<std::vector<int>>& nb) {
+  nb.assign(n, {});
+  float hm = 0.0f;
+  for (int i = 0; i < n; ++i) hm = std::max(hm, pos4[4 * i + 3]);
+  CellList cl;
+  cl.build(n, (double)hm * (1.0 + 1.0e-6), [&](int i, double* p) { for (int k = 0; k < 3; ++k) p[k] = pos4[4 * i + k]; });
+  for (int i = 0; i < n; ++i) {
+    double p[3] = {pos4[4 * i], pos4[4 * i + 1], pos4[4 * i + 2]};
+    cl.around(p, [&](int j) {
+      if (j == i) return;
+      const float r = pair_r32(&pos4[4 * i], &pos4[4 * j]);
+      const float hij = 0.5f * (pos4[4 * i + 3] + pos4[4 * j + 3]);
+      if (r < hij) nb[i].push_back(j);
+    });
+    std::sort(nb[i].begin(), nb[i].end());
+  }
+}
+
+}  // namespace
+
+// =====================================================================================================
+// C ABI of the oracle (loaded by oracle/__init__.py through ctypes).
+// =====================================================================================================
+extern "C" {
+
+int orc_version() { return 1; }
+
+double orc_pressure64(const double* e, double rho, double u) { return pressure64(e, rho, u); }
+double orc_sound_speed_sq64(const double* e, double rho, double u) { return sound_speed_sq64(e, rho, u); }
+double orc_sound_speed64_wgsl(const double* e, double rho, double u, double du_floor) {
+  return sound_speed64_wgsl(e, rho, u, du_floor);
+}
+float orc_pressure32(const float* e, float rho, float u, float rho_floor) { return pressure32(e, rho, u, rho_floor); }
+float orc_sound_speed32(const float* e, float rho, float u, float du_floor, float rho_floor) {
+  return sound_speed32(e, rho, u, du_floor, rho_floor);
+}
+// Per-particle EOS over a material table (n_eos × 12 floats): P and c as sph_step.wgsl:158-159.
+void orc_eos32(const float* eos12, const uint32_t* mat, const float* rho, const float* u, int n, float du_floor,
+               float rho_floor, float* P, float* c) {
+  for (int i = 0; i < n; ++i) {
+    const float* e = eos12 + 12 * (size_t)mat[i];
+    P[i] = pressure32(e, rho[i], u[i], rho_floor);
+    c[i] = sound_speed32(e, rho[i], u[i], du_floor, rho_floor);
+  }
+}
+
+double orc_w64(int kind, double r, double h) { return kind == 1 ? w_wendland64(r, h) : w_cubic64(r, h); }
+double orc_dw64(int kind, double r, double h) { return kind == 1 ? dw_wendland64(r, h) : dw_cubic64(r, h); }
+float orc_w32(int kind, float r, float h) { return kern_w32(kind, r, h); }
+float orc_dw32(int kind, float r, float h) { return kern_dw32(kind, r, h); }
+
+// ---- Morton / sort / Karras / moments / traversal (bh_gravity.wgsl, gpu_gravity.rs) -----------------
+void orc_bbox32(const float* pos4, int n, float* lo, float* hi) {  // cs_bbox, bh_gravity.wgsl:68-78
+  for (int k = 0; k < 3; ++k) { lo[k] = INFINITY; hi[k] = -INFINITY; }
+  for (int i = 0; i < n; ++i)
+    for (int k = 0; k < 3; ++k) {
+      lo[k] = std::min(lo[k], pos4[4 * i + k]);
+      hi[k] = std::max(hi[k], pos4[4 * i + k]);
+    }
+}
+void orc_morton32(const float* pos4, int n, const float* lo, const float* hi, uint32_t* codes) {
+  for (int i = 0; i < n; ++i) codes[i] = morton32(&pos4[4 * i], lo, hi);
+}
+// gpu_gravity.rs:360 / gpu-bh-verify main.rs:383: sort the (code, index) pairs.
+void orc_sort_code_index(const uint32_t* codes, int n, uint32_t* order, uint32_t* sorted_codes) {
+  std::vector<uint32_t> o(n);
+  std::iota(o.begin(), o.end(), 0u);
+  std::sort(o.begin(), o.end(), [&](uint32_t a, uint32_t b) { return codes[a] != codes[b] ? codes[a] < codes[b] : a < b; });
+  for (int t = 0; t < n; ++t) { order[t] = o[t]; sorted_codes[t] = codes[o[t]]; }
+}
+// Cluster codes (gpu_gravity.rs:366) + Karras internal nodes (cs_tree). parent[] as cs_tree_reset/cs_tree.
+void orc_karras(const uint32_t* leaf_codes, int L, uint32_t* left, uint32_t* right, uint32_t* parent) {
+  const int nn = 2 * L - 1;
+  for (int i = 0; i < nn; ++i) parent[i] = 0xffffffffu;
+  for (int i = 0; i < L - 1; ++i) {
+    karras_node(leaf_codes, L, i, &left[i], &right[i]);
+    parent[left[i]] = (uint32_t)i;
+    parent[right[i]] = (uint32_t)i;
+  }
+}
+// Structural check of gpu-bh-verify main.rs:420-459 (verify_tree): 1 = valid.
+int orc_verify_tree(const uint32_t* left, const uint32_t* right, const uint32_t* parent, int L) {
+  if (L == 1) return 1;
+  const int ni = L - 1, nn = 2 * L - 1;
+  if (parent[0] != 0xffffffffu) return 0;
+  std::vector<int> visited(nn, 0);
+  std::vector<int> st{0};
+  int leaves = 0, internals = 0;
+  while (!st.empty()) {
+    const int idx = st.back();
+    st.pop_back();
+    if (idx >= nn) return 0;
+    if (++visited[idx] > 1) return 0;
+    if (idx >= ni) { ++leaves; continue; }
+    ++internals;
+    const int l = (int)left[idx], r = (int)right[idx];
+    if (l >= nn || r >= nn) return 0;
+    if ((int)parent[l] != idx || (int)parent[r] != idx) return 0;
+    st.push_back(l);
+    st.push_back(r);
+  }
+  return (leaves == L && internals == ni) ? 1 : 0;
+}
+// Bottom-up moments: leaf bucket sums (bh_gravity.wgsl:205-222) and the mass-weighted merge (:229-238).
+// Node arrays are float4 per node: com4 = (com.xyz, mass), bmin4/bmax4 = (xyz, 0).
+void orc_moments32(const float* sb4, int n, int K, int L, const uint32_t* left, const uint32_t* right,
+                   float* com4, float* bmin4, float* bmax4) {
+  const int leaf0 = L - 1;
+  for (int c = 0; c < L; ++c) {
+    const int li = leaf0 + c, s0 = c * K, s1 = std::min(s0 + K, n);
+    float m = 0.0f, mx[3] = {0, 0, 0}, lo[3] = {1.0e30f, 1.0e30f, 1.0e30f}, hi[3] = {-1.0e30f, -1.0e30f, -1.0e30f};
+    for (int s = s0; s < s1; ++s) {
+      const float* b = &sb4[4 * s];
+      m += b[3];
+      for (int k = 0; k < 3; ++k) {
+        mx[k] += b[k] * b[3];
+        lo[k] = std::min(lo[k], b[k]);
+        hi[k] = std::max(hi[k], b[k]);
+      }
+    }
+    for (int k = 0; k < 3; ++k) {
+      com4[4 * li + k] = m > 0.0f ? mx[k] / m : 0.0f;
+      bmin4[4 * li + k] = lo[k];
+      bmax4[4 * li + k] = hi[k];
+    }
+    com4[4 * li + 3] = m;
+    bmin4[4 * li + 3] = 0.0f;
+    bmax4[4 * li + 3] = 0.0f;
+  }
+  if (L < 2) return;
+  // Post-order over internal nodes (children before parents).
+  std::vector<int> post;
+  post.reserve(L);
+  std::vector<std::pair<int, int>> st{{0, 0}};
+  while (!st.empty()) {
+    auto& [node, state] = st.back();
+    if (node >= leaf0) { st.pop_back(); continue; }
+    if (state == 0) { state = 1; st.push_back({(int)left[node], 0}); }
+    else if (state == 1) { state = 2; st.push_back({(int)right[node], 0}); }
+    else { post.push_back(node); st.pop_back(); }
+  }
+  for (int node : post) {
+    const int l = (int)left[node], r = (int)right[node];
+    const float* cl = &com4[4 * l];
+    const float* cr = &com4[4 * r];
+    const float m = cl[3] + cr[3];
+    for (int k = 0; k < 3; ++k) {
+      com4[4 * node + k] = m > 0.0f ? (cl[k] * cl[3] + cr[k] * cr[3]) / m : 0.0f;
+      bmin4[4 * node + k] = std::min(bmin4[4 * l + k], bmin4[4 * r + k]);
+      bmax4[4 * node + k] = std::max(bmax4[4 * l + k], bmax4[4 * r + k]);
+    }
+    com4[4 * node + 3] = m;
+    bmin4[4 * node + 3] = 0.0f;
+    bmax4[4 * node + 3] = 0.0f;
+  }
+}
+// cs_gravity_bh, bh_gravity.wgsl:338-394: per-particle stack walk in sorted space, written to
+// acc4[order[t]]. Returns the number of dropped pushes (the reference's silent MAX_STACK guard).
+int orc_gravity_bh32(const float* sb4, int n, int K, int L, const uint32_t* left, const uint32_t* right,
+                     const float* com4, const float* bmin4, const float* bmax4, const uint32_t* order, float theta,
+                     float soft2, float G, float* acc4) {
+  const uint32_t leaf0 = (uint32_t)(L - 1);
+  int dropped = 0;
+  for (int t = 0; t < n; ++t) {
+    const float* pi = &sb4[4 * t];
+    float a[3] = {0, 0, 0};
+    uint32_t stack[64];
+    int sp = 0;
+    stack[sp++] = 0u;
+    while (sp > 0) {
+      const uint32_t ni = stack[--sp];
+      if (ni >= leaf0) {
+        const int c = (int)(ni - leaf0), s0 = c * K, s1 = std::min(s0 + K, n);
+        for (int s = s0; s < s1; ++s) {
+          if (s == t) continue;
+          const float* bj = &sb4[4 * s];
+          const float d[3] = {bj[0] - pi[0], bj[1] - pi[1], bj[2] - pi[2]};
+          const float r2 = ((d[0] * d[0] + d[1] * d[1]) + d[2] * d[2]) + soft2;
+          const float g = G * bj[3] / (r2 * std::sqrt(r2));
+          for (int k = 0; k < 3; ++k) a[k] = a[k] + d[k] * g;
+        }
+        continue;
+      }
+      const float* cm = &com4[4 * ni];
+      const float* bl = &bmin4[4 * ni];
+      const float* bh = &bmax4[4 * ni];
+      const float d[3] = {cm[0] - pi[0], cm[1] - pi[1], cm[2] - pi[2]};
+      const float r2 = ((d[0] * d[0] + d[1] * d[1]) + d[2] * d[2]) + soft2;
+      const float dist = std::sqrt(r2);
+      const float e[3] = {bh[0] - bl[0], bh[1] - bl[1], bh[2] - bl[2]};
+      const float size = std::sqrt((e[0] * e[0] + e[1] * e[1]) + e[2] * e[2]);
+      const float cd[3] = {0.5f * (bl[0] + bh[0]) - cm[0], 0.5f * (bl[1] + bh[1]) - cm[1], 0.5f * (bl[2] + bh[2]) - cm[2]};
+      const float delta = std::sqrt((cd[0] * cd[0] + cd[1] * cd[1]) + cd[2] * cd[2]);
+      if (dist >= size / theta + delta) {
+        const float g = G * cm[3] / (r2 * dist);
+        for (int k = 0; k < 3; ++k) a[k] = a[k] + d[k] * g;
+        continue;
+      }
+      if (sp + 2 <= 64) {
+        stack[sp++] = left[ni];
+        stack[sp++] = right[ni];
+      } else {
+        ++dropped;
+      }
+    }
+    for (int k = 0; k < 3; ++k) acc4[4 * order[t] + k] = a[k];
+    acc4[4 * order[t] + 3] = 0.0f;
+  }
+  return dropped;
+}
+// Softened direct sum in f32 (the leaf form r2·sqrt(r2), bh_gravity.wgsl:365-366).
+void orc_gravity_direct32(const float* b4, int n, float soft2, float G, float* acc4) {
+  for (int i = 0; i < n; ++i) {
+    float a[3] = {0, 0, 0};
+    for (int j = 0; j < n; ++j) {
+      if (j == i) continue;
+      const float d[3] = {b4[4 * j] - b4[4 * i], b4[4 * j + 1] - b4[4 * i + 1], b4[4 * j + 2] - b4[4 * i + 2]};
+      const float r2 = ((d[0] * d[0] + d[1] * d[1]) + d[2] * d[2]) + soft2;
+      const float g = G * b4[4 * j + 3] / (r2 * std::sqrt(r2));
+      for (int k = 0; k < 3; ++k) a[k] = a[k] + d[k] * g;
+    }
+    for (int k = 0; k < 3; ++k) acc4[4 * i + k] = a[k];
+    acc4[4 * i + 3] = 0.0f;
+  }
+}
+// f64 softened direct sum on a subset of targets (gpu-bh-verify main.rs:140-158; bhtree.rs:119-131).
+void orc_gravity_direct64(const double* pos3, const double* mass, int n, const int* targets, int nt, double soft,
+                          double G, double* acc3, int nthreads) {
+  const double s2 = soft * soft;
+#pragma omp parallel for schedule(dynamic, 16) num_threads(std::max(nthreads, 1))
+  for (int q = 0; q < nt; ++q) {
+    const int i = targets ? targets[q] : q;
+    double a[3] = {0, 0, 0};
+    for (int j = 0; j < n; ++j) {
+      if (j == i) continue;
+      const double d[3] = {pos3[3 * j] - pos3[3 * i], pos3[3 * j + 1] - pos3[3 * i + 1], pos3[3 * j + 2] - pos3[3 * i + 2]};
+      const double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2] + s2;
+      const double g = G * mass[j] / (r2 * std::sqrt(r2));
+      for (int k = 0; k < 3; ++k) a[k] += d[k] * g;
+    }
+    for (int k = 0; k < 3; ++k) acc3[3 * q + k] = a[k];
+  }
+}
+// f64 octree Barnes-Hut (bhtree.rs). Returns the node count (0 = brute-force mode below 1024 bodies).
+int orc_bhtree64(const double* pos3, const double* mass, int n, double theta, double soft, double G, double* acc3,
+                 int nthreads) {
+  OctTree t;
+  t.build(pos3, mass, n, theta, soft, G);
+  t.accelerations(acc3, std::max(nthreads, 1));
+  return (int)t.nodes.size();
+}
+
+// ---- neighbour sets and f32 SPH (sph_step.wgsl) ------------------------------------------------------
+// Exact neighbour sets, ascending per particle. Returns the total number of entries written, or -1 if a
+// particle has more than `cap` neighbours.
+long long orc_neighbours32(const float* pos4, int n, uint32_t* counts, uint32_t* lists, int cap) {
+  std::vector<std::vector<int>> nb;
+  neighbour_sets32(pos4, n, nb);
+  long long total = 0;
+  for (int i = 0; i < n; ++i) {
+    counts[i] = (uint32_t)nb[i].size();
+    if ((int)nb[i].size() > cap) return -1;
+    for (size_t k = 0; k < nb[i].size(); ++k) lists[(size_t)i * cap + k] = (uint32_t)nb[i][k];
+    total += (long long)nb[i].size();
+  }
+  return total;
+}
+// cs_density, sph_step.wgsl:120-149: rho_i = m_i W(0,h_i) + Σ_{j in set} m_j W(r, h_ij).
+void orc_density32(const float* pos4, const float* mass, int n, int kernel, float* rho) {
+  std::vector<std::vector<int>> nb;
+  neighbour_sets32(pos4, n, nb);
+  for (int i = 0; i < n; ++i) {
+    float r_i = mass[i] * kern_w32(kernel, 0.0f, pos4[4 * i + 3]);
+    for (int j : nb[i]) {
+      const float r = pair_r32(&pos4[4 * i], &pos4[4 * j]);
+      const float hij = 0.5f * (pos4[4 * i + 3] + pos4[4 * j + 3]);
+      r_i += mass[j] * kern_w32(kernel, r, hij);
+    }
+    rho[i] = r_i;
+  }
+}
+// The SPH half of cs_forces, sph_step.wgsl:171-210 (pressure + Monaghan AV + du/dt), with P and c taken
+// per particle (the reference recomputes the same pure function per pair, :188-190). out4 = (a.xyz, du/dt).
+void orc_sph_forces32(const float* pos4, const float* vel4, const float* mass, const float* rho, const float* P,
+                      const float* c, int n, float av_alpha, float av_beta, float r_min, int kernel, float* out4) {
+  std::vector<std::vector<int>> nb;
+  neighbour_sets32(pos4, n, nb);
+  for (int i = 0; i < n; ++i) {
+    float a[3] = {0, 0, 0}, de = 0.0f;
+    const float* pi = &pos4[4 * i];
+    const float* vi = &vel4[4 * i];
+    for (int j : nb[i]) {
+      const float* pj = &pos4[4 * j];
+      const float* vj = &vel4[4 * j];
+      const float dpos[3] = {pi[0] - pj[0], pi[1] - pj[1], pi[2] - pj[2]};
+      const float r = std::sqrt((dpos[0] * dpos[0] + dpos[1] * dpos[1]) + dpos[2] * dpos[2]);
+      const float hij = 0.5f * (pi[3] + pj[3]);
+      if (!(r < hij && r > r_min)) continue;
+      const float dvel[3] = {vi[0] - vj[0], vi[1] - vj[1], vi[2] - vj[2]};
+      const float vr = (dvel[0] * dpos[0] + dvel[1] * dpos[1]) + dvel[2] * dpos[2];
+      float pi_ij = 0.0f;
+      if (vr < 0.0f) {
+        const float mu = hij * vr / (r * r + 0.01f * hij * hij);
+        const float c_bar = 0.5f * (c[i] + c[j]);
+        const float rho_bar = 0.5f * (rho[i] + rho[j]);
+        pi_ij = (-av_alpha * c_bar * mu + av_beta * mu * mu) / rho_bar;
+      }
+      const float coeff = P[i] / (rho[i] * rho[i]) + P[j] / (rho[j] * rho[j]) + pi_ij;
+      const float dw = kern_dw32(kernel, r, hij);
+      const float grad[3] = {dpos[0] / r * dw, dpos[1] / r * dw, dpos[2] / r * dw};
+      for (int k = 0; k < 3; ++k) a[k] += grad[k] * (-coeff * mass[j]);
+      de += 0.5f * mass[j] * coeff * ((dvel[0] * grad[0] + dvel[1] * grad[1]) + dvel[2] * grad[2]);
+    }
+    for (int k = 0; k < 3; ++k) out4[4 * i + k] = a[k];
+    out4[4 * i + 3] = de;
+  }
+}
+
+// ---- f64 verifier physics (tools/sph-verify/src/main.rs:106-251) ----------------------------------
+// cpu_forces: O(N²) density, direct gravity (pow form) and SPH/AV/du-dt with P,c per pair (1e-3 steps).
+void orc_cpu_forces64(const double* pos3, const double* vel3, const double* h, const double* mass, const double* u,
+                      const int* mat, int n, const double* eos10, double soft, double G, double av_alpha,
+                      double av_beta, double du_floor, int kernel, double* rho, double* acc3, double* dudt) {
+  auto W = [&](double r, double hh) { return kernel == 1 ? w_wendland64(r, hh) : w_cubic64_verify(r, hh); };
+  auto dW = [&](double r, double hh) { return kernel == 1 ? dw_wendland64(r, hh) : dw_cubic64_verify(r, hh); };
+  for (int i = 0; i < n; ++i) {
+    rho[i] = mass[i] * W(0.0, h[i]);
+    for (int j = 0; j < n; ++j) {
+      if (i == j) continue;
+      const double d[3] = {pos3[3 * i] - pos3[3 * j], pos3[3 * i + 1] - pos3[3 * j + 1], pos3[3 * i + 2] - pos3[3 * j + 2]};
+      const double r = std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+      const double hij = 0.5 * (h[i] + h[j]);
+      if (r < hij) rho[i] += mass[j] * W(r, hij);
+    }
+  }
+  const double s2 = soft * soft;
+  std::vector<double> P(n), C(n);
+  for (int i = 0; i < n; ++i) {
+    const double* e = eos10 + 10 * (size_t)mat[i];
+    P[i] = pressure64(e, rho[i], u[i]);
+    C[i] = sound_speed64_wgsl(e, rho[i], u[i], du_floor);
+  }
+  for (int i = 0; i < n; ++i) {
+    double a[3] = {0, 0, 0}, de = 0.0;
+    for (int j = 0; j < n; ++j) {
+      if (i == j) continue;
+      const double d[3] = {pos3[3 * j] - pos3[3 * i], pos3[3 * j + 1] - pos3[3 * i + 1], pos3[3 * j + 2] - pos3[3 * i + 2]};
+      const double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+      const double g = G * mass[j] / std::pow(r2 + s2, 1.5);
+      for (int k = 0; k < 3; ++k) a[k] += d[k] * g;
+      const double r = std::sqrt(r2);
+      const double hij = 0.5 * (h[i] + h[j]);
+      if (r < hij && r > 1.0e-9) {
+        const double dvel[3] = {vel3[3 * i] - vel3[3 * j], vel3[3 * i + 1] - vel3[3 * j + 1], vel3[3 * i + 2] - vel3[3 * j + 2]};
+        const double dpos[3] = {-d[0], -d[1], -d[2]};
+        const double vr = dvel[0] * dpos[0] + dvel[1] * dpos[1] + dvel[2] * dpos[2];
+        double pi_ij = 0.0;
+        if (vr < 0.0) {
+          const double mu = hij * vr / (r * r + 0.01 * hij * hij);
+          pi_ij = (-av_alpha * 0.5 * (C[i] + C[j]) * mu + av_beta * mu * mu) / (0.5 * (rho[i] + rho[j]));
+        }
+        const double coeff = P[i] / (rho[i] * rho[i]) + P[j] / (rho[j] * rho[j]) + pi_ij;
+        const double dwdr = dW(r, hij);
+        const double grad[3] = {dpos[0] / r * dwdr, dpos[1] / r * dwdr, dpos[2] / r * dwdr};
+        for (int k = 0; k < 3; ++k) a[k] += grad[k] * (-coeff * mass[j]);
+        de += 0.5 * mass[j] * coeff * (dvel[0] * grad[0] + dvel[1] * grad[1] + dvel[2] * grad[2]);
+      }
+    }
+    for (int k = 0; k < 3; ++k) acc3[3 * i + k] = a[k];
+    dudt[i] = de;
+  }
+}
+// CpuState::step × steps (tools/sph-verify/src/main.rs:237-250), state updated in place.
+void orc_cpu_kdk64(double* pos3, double* vel3, const double* h, const double* mass, double* u, const int* mat, int n,
+                   const double* eos10, double soft, double G, double av_alpha, double av_beta, double du_floor,
+                   int kernel, double dt, int steps) {
+  std::vector<double> rho(n), a(3 * (size_t)n), du(n);
+  for (int s = 0; s < steps; ++s) {
+    orc_cpu_forces64(pos3, vel3, h, mass, u, mat, n, eos10, soft, G, av_alpha, av_beta, du_floor, kernel, rho.data(), a.data(), du.data());
+    for (int i = 0; i < n; ++i) {
+      for (int k = 0; k < 3; ++k) vel3[3 * i + k] += a[3 * i + k] * 0.5 * dt;
+      u[i] = std::max(u[i] + du[i] * 0.5 * dt, 0.0);
+      for (int k = 0; k < 3; ++k) pos3[3 * i + k] += vel3[3 * i + k] * dt;
+    }
+    orc_cpu_forces64(pos3, vel3, h, mass, u, mat, n, eos10, soft, G, av_alpha, av_beta, du_floor, kernel, rho.data(), a.data(), du.data());
+    for (int i = 0; i < n; ++i) {
+      for (int k = 0; k < 3; ++k) vel3[3 * i + k] += a[3 * i + k] * 0.5 * dt;
+      u[i] = std::max(u[i] + du[i] * 0.5 * dt, 0.0);
+    }
+  }
+}
+
+// ---- HydroBody handle (the timed CPU path) --------------------------------------------------------
+void* orc_hydro_new(int n, const double* pos3, const double* vel3, const double* mass, const double* u,
+                    const double* h, const int* mat, const double* eos10, int n_eos, double softening, double G,
+                    double theta, double av_alpha, double av_beta, int kernel) {
+  Hydro* hb = new Hydro();
+  hb->n = n;
+  hb->n_eos = n_eos;
+  hb->pos.assign(pos3, pos3 + 3 * (size_t)n);
+  hb->vel.assign(vel3, vel3 + 3 * (size_t)n);
+  hb->mass.assign(mass, mass + n);
+  hb->u.assign(u, u + n);
+  hb->h.assign(h, h + n);
+  hb->mat.assign(mat, mat + n);
+  hb->eos.assign(eos10, eos10 + 10 * (size_t)n_eos);
+  hb->softening = softening;
+  hb->G = G;
+  hb->theta = theta;
+  hb->av_alpha = av_alpha;
+  hb->av_beta = av_beta;
+  hb->kernel = kernel;
+  hb->rho.assign(n, 0.0);
+  return hb;
+}
+void orc_hydro_free(void* p) { delete static_cast<Hydro*>(p); }
+void orc_hydro_step(void* p, double dt, int nthreads) { static_cast<Hydro*>(p)->step(dt, nthreads); }
+void orc_hydro_density(void* p, int nthreads) { static_cast<Hydro*>(p)->compute_density(nthreads); }
+void orc_hydro_forces(void* p, double* acc3, double* dudt, int nthreads) {
+  Hydro* hb = static_cast<Hydro*>(p);
+  std::vector<double> a, du;
+  hb->forces(a, du, nthreads);
+  std::memcpy(acc3, a.data(), sizeof(double) * a.size());
+  std::memcpy(dudt, du.data(), sizeof(double) * du.size());
+}
+double orc_hydro_courant_dt(void* p, double cfl, double sig_floor) { return static_cast<Hydro*>(p)->courant_dt(cfl, sig_floor); }
+void orc_hydro_get(void* p, double* pos3, double* vel3, double* u, double* rho) {
+  Hydro* hb = static_cast<Hydro*>(p);
+  if (pos3) std::memcpy(pos3, hb->pos.data(), sizeof(double) * hb->pos.size());
+  if (vel3) std::memcpy(vel3, hb->vel.data(), sizeof(double) * hb->vel.size());
+  if (u) std::memcpy(u, hb->u.data(), sizeof(double) * hb->u.size());
+  if (rho) std::memcpy(rho, hb->rho.data(), sizeof(double) * hb->rho.size());
+}
+int orc_max_threads() {
+#ifdef _OPENMP
+  return omp_get_max_threads();
+#else
+  return 1;
+#endif
+}
+
+// ---- conservation sums (gpu_sph.rs:628-649; tools/impact-run/src/main.rs:195-205,528-536) ----------
+// out[0..2] = KE, IE, PE (PE O(N²) softened, skipped when with_pe == 0); out[3..5] = linear momentum;
+// out[6..8] = angular momentum about the origin.
+void orc_conservation64(const double* pos3, const double* vel3, const double* mass, const double* u, int n,
+                        double soft, double G, int with_pe, double* out) {
+  double ke = 0, ie = 0, pe = 0, p[3] = {0, 0, 0}, L[3] = {0, 0, 0};
+  for (int i = 0; i < n; ++i) {
+    const double* x = pos3 + 3 * i;
+    const double* v = vel3 + 3 * i;
+    ke += 0.5 * mass[i] * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    ie += mass[i] * u[i];
+    for (int k = 0; k < 3; ++k) p[k] += mass[i] * v[k];
+    L[0] += mass[i] * (x[1] * v[2] - x[2] * v[1]);
+    L[1] += mass[i] * (x[2] * v[0] - x[0] * v[2]);
+    L[2] += mass[i] * (x[0] * v[1] - x[1] * v[0]);
+  }
+  if (with_pe) {
+    const double s2 = soft * soft;
+    for (int i = 0; i < n; ++i)
+      for (int j = i + 1; j < n; ++j) {
+        const double d[3] = {pos3[3 * i] - pos3[3 * j], pos3[3 * i + 1] - pos3[3 * j + 1], pos3[3 * i + 2] - pos3[3 * j + 2]};
+        pe -= G * mass[i] * mass[j] / std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2] + s2);
+      }
+  }
+  out[0] = ke; out[1] = ie; out[2] = pe;
+  for (int k = 0; k < 3; ++k) { out[3 + k] = p[k]; out[6 + k] = L[k]; }
+}
+
+}  // extern "C"
