@@ -1,0 +1,324 @@
+#!/usr/bin/env python
+"""Benchmark: SPH + Barnes-Hut giant-impact particle-steps/s on one or more B200s.
+
+Default workload (N=1): the 1,048,576-particle impact (953,250 target + 95,326 impactor; 30 % iron /
+70 % basalt by mass; Tillotson; Wendland C2 with 64 neighbours and the smoothing-length solve; monopole +
+quadrupole Barnes-Hut at θ = 0.6 with 16-particle leaves; adaptive CFL 0.3 dt; FP32 SoA fields with FP64
+positions), seeded synthetic initial conditions. One step = one KDK leapfrog step (two force evaluations,
+as the reference's encode_kdk). Inputs are resident in HBM and the per-step working set (particle state,
+neighbour lists, tree) is larger than the 126 MB L2, so no flush is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload impact_1m|impact_4m|impact_10k]
+    python bench.py --impl reference ...    # the reference's CPU path (HydroBody::step) on the host cores
+
+Multi-GPU: replicas (one independent impact per rank, no collective on the data path); value is the sum
+over ranks divided by the slowest rank's time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "SPH+gravity particle-steps/s"
+UNIT = "particle-steps/s"
+
+from botheadstudios_b200.workloads import WORKLOADS  # noqa: E402
+
+# Algorithmic bytes per particle per phase execution (state read/written once, SoA f32/f64 layout):
+# sort = bbox/Morton 40 + radix (key,idx) 16 + permutation 132; tree = 20 + 304/L per particle;
+# gravity 32; neighbours 36 (pos 16 + list write 4·k_avg counted separately); density 28 + EOS 20;
+# forces 64; integrate: kick-drift 128 + kick 48 + CFL 36 per step (two phase executions).
+BYTES_PER_PARTICLE = dict(sort=188.0, tree=39.0, gravity=32.0, neighbours=16.0, hsolve=28.0, density=48.0,
+                          forces=64.0, integrate=106.0)
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return dict(hbm=float(d["hbm_gbs"]), bf16=float(d["bf16_tflops"]), src="measured")
+    return dict(hbm=6650.0, bf16=1590.0, src="fallback")
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=2)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return None
+        return dict(sm_mhz=statistics.median(sm), sm_max_mhz=smax, reasons=sorted(reasons), samples=len(sm))
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+        pg = dist
+    return world, rank, local, pg
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+def max_over_ranks(pg, v: float, local: int) -> float:
+    if pg is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{local}")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def build_workload(wl: dict, seed: int):
+    from botheadstudios_b200 import workloads
+    return workloads.build(wl, seed)
+
+
+def make_solver(wl: dict, I, device: int):
+    from botheadstudios_b200 import workloads
+    return workloads.solver(wl, I, device)
+
+
+# ---------------------------------------------------------------------------------------------------------
+# CPU baseline: the reference's CPU path of record (HydroBody::step, hydrostatic.rs:345: f64, octree
+# Barnes-Hut θ = 0.5, hash-grid neighbours, two force evaluations per KDK step) restated in C++ and run with
+# OpenMP on all host cores, in the reference's own SI units, on a bounded sample of the same generator.
+# ---------------------------------------------------------------------------------------------------------
+def cpu_reference_run(wl: dict, sample_n: int, steps: int, warmup: int, budget_s: float, nthreads: int = 0):
+    import oracle
+    from botheadstudios_b200 import ic
+    from botheadstudios_b200.materials import eos_table64, SI
+    frac = wl["n_impactor"] / (wl["n_target"] + wl["n_impactor"])
+    n_imp = max(int(round(sample_n * frac)), 1)
+    I = ic.impact(sample_n - n_imp, n_imp, n_ngb=wl["n_ngb"], seed=2)
+    U = I.units
+    p = I.particles
+    pos = I.pos64 * U.L
+    vel = p["vel"].astype(np.float64) * U.speed
+    mass = p["mass"].astype(np.float64) * U.M
+    u = p["u"].astype(np.float64) * U.energy
+    h = p["h"].astype(np.float64) * U.L
+    kernel = 1 if wl["kernel"] == "wendland" else 0
+    nthreads = nthreads or oracle.max_threads()
+    hb = oracle.HydroBody(pos, vel, mass, u, h, p["mat"].astype(np.int32), eos_table64(SI), I.softening * U.L,
+                          G=6.674e-11, theta=0.5, kernel=kernel)
+    hb.compute_density(nthreads)
+    dt = hb.courant_dt(0.3)
+    for _ in range(warmup):
+        hb.step(dt, nthreads)
+    done, t0 = 0, time.perf_counter()
+    while done < steps:
+        hb.step(dt, nthreads)
+        done += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    el = time.perf_counter() - t0
+    return dict(value=sample_n * done / el, steps_run=done, seconds=el, cores=nthreads, n=sample_n)
+
+
+def run_reference(args, wl, world, rank, local, pg):
+    if rank != 0:
+        return
+    r = cpu_reference_run(wl, sample_n=65_536, steps=args.steps, warmup=min(args.warmup, 1), budget_s=150.0)
+    sample = (f"HydroBody::step (f64, octree BH θ=0.5, hash grid, 2 force evals/step) on a 65,536-particle impact "
+              f"from the same generator, {r['steps_run']} timed steps in {r['seconds']:.1f} s, "
+              f"{r['cores']} OpenMP threads, SI units")
+    line = dict(metric=METRIC, value=r["value"], unit=UNIT, impl="reference", n_gpus=args.gpus, steps=args.steps,
+                warmup=args.warmup, ms_per_step=1000.0 * r["seconds"] / max(r["steps_run"], 1),
+                higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f64", data="synthetic",
+                config=dict(workload=args.workload, particles=wl["n_target"] + wl["n_impactor"]),
+                cpu_baseline=dict(value=r["value"], unit=UNIT, cores=r["cores"], kind="port", sample=sample),
+                e2e=dict(value=r["value"], unit=UNIT, h2d_bytes_per_step=0, d2h_bytes_per_step=0))
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, wl, world, rank, local, pg):
+    import torch
+
+    I = build_workload(wl, seed=1 + rank)
+    n = len(I.particles)
+    s = make_solver(wl, I, local)
+    s.upload(I.particles, I.eos, I.softening)
+    ext = torch.cuda.ExternalStream(s.stream(), device=f"cuda:{local}")
+    # warm-up (includes the first full force evaluation)
+    s.encode_kdk(args.warmup)
+    s.sync()
+    d0 = s.diag()
+    s.profile_enable(True)
+    barrier(pg)
+    torch.cuda.synchronize(local)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev0.record(ext)
+        s.encode_kdk(args.steps)
+        ev1.record(ext)
+        ev1.synchronize()
+    torch.cuda.synchronize(local)
+    barrier(pg)
+    ms = ev0.elapsed_time(ev1)
+    prof = s.profile_read()
+    s.profile_enable(False)
+    d1 = s.diag(check=False)
+    ms_max = max_over_ranks(pg, ms, local)
+    value = n * args.steps * world / (ms_max / 1000.0)
+
+    # ---- end to end through the public API: per step, upload the state from pinned host memory, one KDK
+    # step, read the state back into host memory ----
+    pin = torch.empty(n * 48, dtype=torch.uint8, pin_memory=True).numpy().view(I.particles.dtype)
+    state = s.readback()
+    pin[:] = state
+    e2e_steps = max(2, min(args.steps, 10))
+    barrier(pg)
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        s.upload(pin, I.eos, I.softening)
+        s.encode_kdk(1)
+        out = s.readback()
+        pin[:] = out
+    e2e_s = time.perf_counter() - t0
+    e2e_s = max_over_ranks(pg, e2e_s, local)
+    e2e_value = n * e2e_steps * world / e2e_s
+
+    if rank != 0:
+        return
+    # ---- roofline of the dominant phase (device-timed with CUDA events on the library's stream) ----
+    pk = peaks()
+    phases = {}
+    for k, t in prof["ms"].items():
+        calls = prof["calls"][k]
+        if calls == 0 or t <= 0:
+            continue
+        b = BYTES_PER_PARTICLE[k] * n * calls
+        phases[k] = dict(ms=round(t, 4), share=round(t / sum(prof["ms"].values()), 4), calls=calls,
+                         gbs=round(b / (t / 1000.0) / 1e9, 1))
+    dom = max(phases, key=lambda k: phases[k]["ms"])
+    dom_bytes = BYTES_PER_PARTICLE[dom] * n
+    dom_ms = phases[dom]["ms"] / phases[dom]["calls"]
+    achieved = dom_bytes / (dom_ms / 1000.0) / 1e9
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tf):
+        traffic = json.load(open(tf)).get(args.workload, {}).get(dom)
+    roof = dict(bound="hbm", kernel_phase=dom, achieved=round(achieved, 1), peak=pk["hbm"], unit="GB/s",
+                frac=round(achieved / pk["hbm"], 4), traffic=traffic, peak_source=pk["src"],
+                bytes_per_launch=dom_bytes, ms_per_launch=round(dom_ms, 4))
+    # ---- CPU baseline on the host cores (rank 0, N=1 only) ----
+    cpu = None
+    if world == 1 and not args.no_cpu:
+        r = cpu_reference_run(wl, sample_n=65_536, steps=50, warmup=0, budget_s=15.0)
+        cpu = dict(value=r["value"], unit=UNIT, cores=r["cores"], kind="port",
+                   sample=f"HydroBody::step restated in C++ (f64, octree θ=0.5), 65,536-particle impact of the same "
+                          f"generator, {r['steps_run']} steps in {r['seconds']:.1f} s")
+    dd = d1
+    energy0 = d0["kinetic"] + d0["internal"] + d0["potential"]
+    energy1 = dd["kinetic"] + dd["internal"] + dd["potential"]
+    line = dict(metric=METRIC, value=value, unit=UNIT, n_gpus=world, steps=args.steps, warmup=args.warmup,
+                ms_per_step=ms_max / args.steps, higher_is_better=True, scaling="weak", vs_baseline=None,
+                dtype="f32", data="synthetic (seeded lattice impact)",
+                config=dict(workload=args.workload, particles=n, kernel=wl["kernel"], neighbours=wl["n_ngb"],
+                            theta=wl["theta"], quadrupole=bool(wl["quad"]), leaf=wl["leaf"],
+                            h_solve=bool(wl["h_solve"]), dt="adaptive CFL 0.3", parallelism=f"replicas{world}",
+                            l2="working set > L2 (no flush needed)"),
+                e2e=dict(value=e2e_value, unit=UNIT, h2d_bytes_per_step=48 * n, d2h_bytes_per_step=48 * n,
+                         steps=e2e_steps),
+                gpu_launches=prof["kernel_launches"], roofline=roof, phases=phases, cpu_baseline=cpu,
+                clocks=clk.summary(),
+                physics=dict(energy_drift=(energy1 - energy0) / abs(d0["potential"]) if d0["potential"] else None,
+                             sim_time=dd["time"], dt=dd["dt"], max_neighbours=dd["max_neighbours_seen"],
+                             overflow_flags=dd["overflow_flags"], h_residual=dd["h_residual"]))
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="impact_1m", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
+    args = ap.parse_args()
+    wl = WORKLOADS[args.workload]
+    world, rank, local, pg = dist_setup(args)
+    try:
+        if args.impl == "reference":
+            run_reference(args, wl, world, rank, local, pg)
+        else:
+            run_ours(args, wl, world, rank, local, pg)
+    finally:
+        if pg is not None:
+            pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

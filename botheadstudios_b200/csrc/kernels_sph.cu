@@ -1,0 +1,448 @@
+// SPH on B200: neighbour lists from the LBVH, density + Tillotson EOS, smoothing-length solve, pressure +
+// Monaghan AV + du/dt forces with the Courant signal reduction fused in, KDK leapfrog with f64 positions
+// (bbox reduction fused into the drift), damped relaxation, exchange-format conversion and FP64 sums.
+//
+// Reference: shaders/sph_step.wgsl (cs_density :120-149, cs_forces :153-211, cs_kick_drift :221-228,
+// cs_kick :232-237, cs_relax :245-257, cs_signal :263-269). The reference finds neighbours with a spatial
+// hash over 27 cells plus a cell-membership guard; the set it produces is exactly {j != i : r_ij < h_ij},
+// h_ij = ½(h_i + h_j). Here that set is enumerated once per tree build by a warp-cooperative walk of the
+// LBVH (node AABBs carry the subtree's max h) and stored as interleaved per-particle lists; r_ij is
+// computed with single-rounded operations so the set is bit-identical to the reference predicate.
+#include "sph_kernels.cuh"
+
+namespace sphb {
+
+__device__ __forceinline__ float pair_r(float4 a, float4 b) {
+  return fsqrt(dot3_exact(fsub(a.x, b.x), fsub(a.y, b.y), fsub(a.z, b.z)));
+}
+__device__ __forceinline__ float pair_h(float hi, float hj) { return fmul(0.5f, fadd(hi, hj)); }
+
+// ---------------------------------------------------------------------------------------------------
+// Density (cs_density) with the EOS fused: rho_i = m_i W(0,h_i) + Σ m_j W(r, h_ij) over r < h_ij, then
+// P(rho,u), c(rho,u) and the per-particle force record (m, rho, P/rho², c). The reference re-evaluates P_j
+// and c_j for every pair (sph_step.wgsl:188-190); they are pure functions of (rho_j, u_j, mat_j), so one
+// evaluation per particle gives the same values.
+// ---------------------------------------------------------------------------------------------------
+__device__ __forceinline__ float4 eos_record(const Eos* __restrict__ eos, unsigned mat, float m, float rho,
+                                             float u, const DevParams* P) {
+  const Eos e = eos[mat];
+  const float p = tillotson_p(e, rho, u, P->rho_floor);
+  const float c = tillotson_c(e, rho, u, P->du_floor, P->rho_floor);
+  return make_float4(m, rho, p / (rho * rho), c);
+}
+
+template <int KERNEL>
+__global__ void k_density_eos(int n, State st, const unsigned* __restrict__ nbr,
+                              const unsigned* __restrict__ nbr_cnt, unsigned cap, const Eos* __restrict__ eos,
+                              const DevParams* __restrict__ P, float* __restrict__ rho, float4* __restrict__ fdata) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const float4 pi = st.pos_h[t];
+  const float m = st.mass[t];
+  float r_i = m * kern_w<KERNEL>(0.0f, pi.w);
+  const unsigned c = min(nbr_cnt[t], cap);
+  for (unsigned k = 0; k < c; ++k) {
+    const unsigned j = nbr[nbr_slot((unsigned)t, k, cap)];
+    const float4 pj = st.pos_h[j];
+    const float r = pair_r(pi, pj);
+    const float hij = pair_h(pi.w, pj.w);
+    if (r < hij) r_i += st.mass[j] * kern_w<KERNEL>(r, hij);
+  }
+  rho[t] = r_i;
+  fdata[t] = eos_record(eos, st.mat[t], m, r_i, st.vel_u[t].w, P);
+}
+
+int launch_density_eos(const Dev& d, const Cfg& c, cudaStream_t s) {
+  const int blocks = (d.n + 255) / 256;
+  if (c.kernel == 1)
+    k_density_eos<1><<<blocks, 256, 0, s>>>(d.n, d.s(), d.nbr, d.nbr_cnt, d.nbr_cap, d.eos, d.P, d.rho, d.fdata);
+  else
+    k_density_eos<0><<<blocks, 256, 0, s>>>(d.n, d.s(), d.nbr, d.nbr_cnt, d.nbr_cap, d.eos, d.P, d.rho, d.fdata);
+  return 1;
+}
+
+__global__ void k_eos_only(int n, State st, const float* __restrict__ rho, const Eos* __restrict__ eos,
+                           const DevParams* __restrict__ P, float4* __restrict__ fdata) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  fdata[t] = eos_record(eos, st.mat[t], st.mass[t], rho[t], st.vel_u[t].w, P);
+}
+int launch_eos_only(const Dev& d, cudaStream_t s) {
+  k_eos_only<<<(d.n + 255) / 256, 256, 0, s>>>(d.n, d.s(), d.rho, d.eos, d.P, d.fdata);
+  return 1;
+}
+
+// ---------------------------------------------------------------------------------------------------
+// Smoothing-length solve (new; the reference keeps h fixed, hydrostatic.rs:59-61). Jacobi-Newton on
+// f(h_i) = rho_i(h) − m_i (η/h_i)³ with rho_i from the reference's symmetric form (h_ij = ½(h_i+h_j)),
+// ∂rho_i/∂h_i = m_i ∂W(0,h_i)/∂h + Σ_j m_j ½ ∂W(r,h_ij)/∂h (Price 2012, J. Comput. Phys. 231, §3.2.1).
+// h may move inside the list's skin only; the residual |f|/rho is reduced to a device maximum.
+// ---------------------------------------------------------------------------------------------------
+template <int KERNEL>
+__global__ void k_h_iter(int n, State st, const unsigned* __restrict__ nbr, const unsigned* __restrict__ nbr_cnt,
+                         unsigned cap, const float* __restrict__ h0, float eta, float skin, DevParams* P,
+                         float* __restrict__ hnew, int last) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  float res = 0.0f;
+  if (t < n) {
+    const float4 pi = st.pos_h[t];
+    const float m = st.mass[t];
+    const float h = pi.w;
+    float rho = m * kern_w<KERNEL>(0.0f, h);
+    float drho = m * kern_dwdh<KERNEL>(0.0f, h);
+    const unsigned c = min(nbr_cnt[t], cap);
+    for (unsigned k = 0; k < c; ++k) {
+      const unsigned j = nbr[nbr_slot((unsigned)t, k, cap)];
+      const float4 pj = st.pos_h[j];
+      const float r = pair_r(pi, pj);
+      const float hij = pair_h(h, pj.w);
+      if (r < hij) {
+        const float mj = st.mass[j];
+        rho += mj * kern_w<KERNEL>(r, hij);
+        drho += mj * 0.5f * kern_dwdh<KERNEL>(r, hij);
+      }
+    }
+    const float e3 = eta * eta * eta;
+    const float rt = m * e3 / (h * h * h);
+    const float f = rho - rt;
+    res = fabsf(f) / fmaxf(rho, 1.0e-30f);
+    float hn = h;
+    if (!last) {
+      const float fp = drho + 3.0f * rt / h;
+      hn = fabsf(fp) > 0.0f ? h - f / fp : h;
+      if (!(hn == hn)) hn = h;  // NaN guard
+      hn = fminf(fmaxf(hn, 0.8f * h), 1.2f * h);
+      hn = fminf(hn, h0[t] * (1.0f + skin) * 0.999f);
+      hn = fmaxf(hn, h0[t] / ((1.0f + skin) * 1.001f));
+    }
+    hnew[t] = hn;
+  }
+  const float wres = warp_max(res);
+  if ((threadIdx.x & 31) == 0) atomicMax(&P->h_residual_bits, __float_as_uint(wres));
+}
+
+__global__ void k_h_commit(int n, State st, const float* __restrict__ hnew) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) st.pos_h[t].w = hnew[t];
+}
+__global__ void k_h_reset(DevParams* P, int iters) {
+  P->h_residual_bits = 0u;
+  P->h_iters_used = (unsigned)iters;
+}
+__global__ void k_h_publish(DevParams* P) { P->h_residual = __uint_as_float(P->h_residual_bits); }
+
+int launch_h_solve(const Dev& d, const Cfg& c, cudaStream_t s) {
+  const int blocks = (d.n + 255) / 256;
+  for (int it = 0; it <= c.h_iters; ++it) {
+    const int last = it == c.h_iters;
+    k_h_reset<<<1, 1, 0, s>>>(d.P, c.h_iters);
+    if (c.kernel == 1)
+      k_h_iter<1><<<blocks, 256, 0, s>>>(d.n, d.s(), d.nbr, d.nbr_cnt, d.nbr_cap, d.h0, c.h_eta, c.skin, d.P, d.hnew,
+                                          last);
+    else
+      k_h_iter<0><<<blocks, 256, 0, s>>>(d.n, d.s(), d.nbr, d.nbr_cnt, d.nbr_cap, d.h0, c.h_eta, c.skin, d.P, d.hnew,
+                                          last);
+    if (!last) k_h_commit<<<blocks, 256, 0, s>>>(d.n, d.s(), d.hnew);
+  }
+  k_h_publish<<<1, 1, 0, s>>>(d.P);
+  return (c.h_iters + 1) * 2 + c.h_iters + 1;
+}
+
+// ---------------------------------------------------------------------------------------------------
+// Forces (the SPH half of cs_forces, sph_step.wgsl:170-210) + gravity + the Courant signal (cs_signal
+// :263-269) reduced to a device minimum with one atomic per warp.
+// ---------------------------------------------------------------------------------------------------
+template <int KERNEL, bool GRAV>
+__global__ void k_forces(int n, State st, const float4* __restrict__ fdata, const unsigned* __restrict__ nbr,
+                         const unsigned* __restrict__ nbr_cnt, unsigned cap, const float4* __restrict__ grav,
+                         DevParams* P, float4* __restrict__ acc) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  float sig = __int_as_float(0x7f800000);
+  if (t < n) {
+    const float4 pi = st.pos_h[t];
+    const float4 vi = st.vel_u[t];
+    const float4 fi = fdata[t];
+    const float alpha = P->av_alpha, beta = P->av_beta, r_min = P->r_min;
+    float ax = 0.f, ay = 0.f, az = 0.f, de = 0.f;
+    const unsigned c = min(nbr_cnt[t], cap);
+    for (unsigned k = 0; k < c; ++k) {
+      const unsigned j = nbr[nbr_slot((unsigned)t, k, cap)];
+      const float4 pj = st.pos_h[j];
+      const float dx = fsub(pi.x, pj.x), dy = fsub(pi.y, pj.y), dz = fsub(pi.z, pj.z);
+      const float r = fsqrt(dot3_exact(dx, dy, dz));
+      const float hij = pair_h(pi.w, pj.w);
+      if (!(r < hij && r > r_min)) continue;
+      const float4 vj = st.vel_u[j];
+      const float4 fj = fdata[j];
+      const float vx = vi.x - vj.x, vy = vi.y - vj.y, vz = vi.z - vj.z;
+      const float vr = vx * dx + vy * dy + vz * dz;
+      float pij = 0.0f;
+      if (vr < 0.0f) {
+        const float mu = hij * vr / (r * r + 0.01f * hij * hij);
+        const float c_bar = 0.5f * (fi.w + fj.w);
+        const float rho_bar = 0.5f * (fi.y + fj.y);
+        pij = (-alpha * c_bar * mu + beta * mu * mu) / rho_bar;
+      }
+      const float coeff = fi.z + fj.z + pij;
+      const float dw = kern_dw<KERNEL>(r, hij);
+      const float gx = (dx / r) * dw, gy = (dy / r) * dw, gz = (dz / r) * dw;
+      const float s = -coeff * fj.x;
+      ax += gx * s;
+      ay += gy * s;
+      az += gz * s;
+      de += 0.5f * fj.x * coeff * (vx * gx + vy * gy + vz * gz);
+    }
+    if (GRAV) {
+      const float4 g = grav[t];
+      ax += g.x;
+      ay += g.y;
+      az += g.z;
+    }
+    acc[t] = make_float4(ax, ay, az, de);
+    const float vmag = sqrtf(vi.x * vi.x + vi.y * vi.y + vi.z * vi.z);
+    sig = pi.w / fmaxf(fi.w + vmag, P->sig_floor);
+  }
+  sig = warp_min(sig);
+  if ((threadIdx.x & 31) == 0 && sig < __int_as_float(0x7f800000)) atomicMin(&P->sig_min_bits, __float_as_uint(sig));
+}
+
+int launch_forces(const Dev& d, const Cfg& c, cudaStream_t s) {
+  const int blocks = (d.n + 255) / 256;
+  const bool g = c.gravity != 2;
+#define FARGS d.n, d.s(), d.fdata, d.nbr, d.nbr_cnt, d.nbr_cap, d.grav, d.P, d.acc
+  if (c.kernel == 1) {
+    if (g) k_forces<1, true><<<blocks, 256, 0, s>>>(FARGS);
+    else k_forces<1, false><<<blocks, 256, 0, s>>>(FARGS);
+  } else {
+    if (g) k_forces<0, true><<<blocks, 256, 0, s>>>(FARGS);
+    else k_forces<0, false><<<blocks, 256, 0, s>>>(FARGS);
+  }
+#undef FARGS
+  return 1;
+}
+
+// ---------------------------------------------------------------------------------------------------
+// Step control: dt = cfl·min signal (or the fixed dt), simulated time, reset of the reductions.
+// ---------------------------------------------------------------------------------------------------
+__global__ void k_finalize_dt(DevParams* P) {
+  double dt = P->dt_fixed;
+  if (P->cfl > 0.0f && P->sig_min_bits != 0x7f800000u) dt = (double)P->cfl * (double)__uint_as_float(P->sig_min_bits);
+  P->dt = dt;
+  P->time += dt;
+  P->steps += 1u;
+  P->sig_min_bits = 0x7f800000u;
+  P->bbox_keys[0] = P->bbox_keys[1] = P->bbox_keys[2] = 0xffffffffu;
+  P->bbox_keys[3] = P->bbox_keys[4] = P->bbox_keys[5] = 0u;
+}
+int launch_finalize_dt(const Dev& d, cudaStream_t s) { k_finalize_dt<<<1, 1, 0, s>>>(d.P);  return 1; }
+
+// First half-kick and drift (cs_kick_drift): v += a·dt/2, u = max(u + du·dt/2, 0), x += v·dt in f64,
+// plus the bounding box of the new positions for the next Morton pass.
+__global__ void k_kick_drift(int n, State st, const float4* __restrict__ acc, DevParams* P) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned lo[3] = {0xffffffffu, 0xffffffffu, 0xffffffffu}, hi[3] = {0u, 0u, 0u};
+  if (t < n) {
+    const double dt = P->dt;
+    const float hdt = (float)(0.5 * dt);
+    const float4 a = acc[t];
+    float4 v = st.vel_u[t];
+    v.x = v.x + a.x * hdt;
+    v.y = v.y + a.y * hdt;
+    v.z = v.z + a.z * hdt;
+    v.w = fmaxf(v.w + a.w * hdt, 0.0f);
+    st.vel_u[t] = v;
+    const double x = st.x[t] + (double)v.x * dt, y = st.y[t] + (double)v.y * dt, z = st.z[t] + (double)v.z * dt;
+    st.x[t] = x;
+    st.y[t] = y;
+    st.z[t] = z;
+    float4 p = st.pos_h[t];
+    p.x = (float)x;
+    p.y = (float)y;
+    p.z = (float)z;
+    st.pos_h[t] = p;
+    lo[0] = hi[0] = float_key(p.x);
+    lo[1] = hi[1] = float_key(p.y);
+    lo[2] = hi[2] = float_key(p.z);
+  }
+  __shared__ unsigned s_lo[3][32], s_hi[3][32];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    lo[k] = warp_min(lo[k]);
+    hi[k] = warp_max(hi[k]);
+    if (lane == 0) { s_lo[k][w] = lo[k]; s_hi[k][w] = hi[k]; }
+  }
+  __syncthreads();
+  if (w == 0) {
+    const int nw = blockDim.x >> 5;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      unsigned a = lane < nw ? s_lo[k][lane] : 0xffffffffu;
+      unsigned b = lane < nw ? s_hi[k][lane] : 0u;
+      a = warp_min(a);
+      b = warp_max(b);
+      if (lane == 0) {
+        atomicMin(&P->bbox_keys[k], a);
+        atomicMax(&P->bbox_keys[3 + k], b);
+      }
+    }
+  }
+}
+int launch_kick_drift(const Dev& d, cudaStream_t s) {
+  k_kick_drift<<<(d.n + 255) / 256, 256, 0, s>>>(d.n, d.s(), d.acc, d.P);
+  return 1;
+}
+
+// Final half-kick (cs_kick) with the EOS record refreshed for the new u (density is unchanged).
+__global__ void k_kick(int n, State st, const float4* __restrict__ acc, const float* __restrict__ rho,
+                       const Eos* __restrict__ eos, const DevParams* __restrict__ P, float4* __restrict__ fdata) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const float hdt = (float)(0.5 * P->dt);
+  const float4 a = acc[t];
+  float4 v = st.vel_u[t];
+  v.x = v.x + a.x * hdt;
+  v.y = v.y + a.y * hdt;
+  v.z = v.z + a.z * hdt;
+  v.w = fmaxf(v.w + a.w * hdt, 0.0f);
+  st.vel_u[t] = v;
+  fdata[t] = eos_record(eos, st.mat[t], st.mass[t], rho[t], v.w, P);
+}
+int launch_kick(const Dev& d, cudaStream_t s) {
+  k_kick<<<(d.n + 255) / 256, 256, 0, s>>>(d.n, d.s(), d.acc, d.rho, d.eos, d.P, d.fdata);
+  return 1;
+}
+
+// Damped relaxation (cs_relax, sph_step.wgsl:245-257): v = (v + (a + ω²(x,y,0))·dt)·damp; x += v·dt.
+__global__ void k_relax(int n, State st, const float4* __restrict__ acc, DevParams* P) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const double dt = P->dt_fixed;
+  const float fdt = (float)dt;
+  const float w2 = P->omega * P->omega;
+  const float4 a = acc[t];
+  float4 p = st.pos_h[t];
+  float4 v = st.vel_u[t];
+  v.x = (v.x + (a.x + w2 * p.x) * fdt) * P->damp;
+  v.y = (v.y + (a.y + w2 * p.y) * fdt) * P->damp;
+  v.z = (v.z + a.z * fdt) * P->damp;
+  st.vel_u[t] = v;
+  const double x = st.x[t] + (double)v.x * dt, y = st.y[t] + (double)v.y * dt, z = st.z[t] + (double)v.z * dt;
+  st.x[t] = x;
+  st.y[t] = y;
+  st.z[t] = z;
+  p.x = (float)x;
+  p.y = (float)y;
+  p.z = (float)z;
+  st.pos_h[t] = p;
+}
+int launch_relax(const Dev& d, cudaStream_t s) { k_relax<<<(d.n + 255) / 256, 256, 0, s>>>(d.n, d.s(), d.acc, d.P);  return 1; }
+
+// ---------------------------------------------------------------------------------------------------
+// 48-byte exchange layout (gpu_sph.rs:28) <-> internal state.
+// ---------------------------------------------------------------------------------------------------
+struct P48 {
+  float px, py, pz, h, vx, vy, vz, u, mass;
+  unsigned mat;
+  float rho;
+  unsigned prov;
+};
+static_assert(sizeof(P48) == 48, "SphParticle48 is 48 bytes");
+
+__global__ void k_from_aos(int n, const P48* __restrict__ aos, State st, float* __restrict__ rho) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const P48 p = aos[i];
+  st.pos_h[i] = make_float4(p.px, p.py, p.pz, p.h);
+  st.vel_u[i] = make_float4(p.vx, p.vy, p.vz, p.u);
+  st.x[i] = (double)p.px;
+  st.y[i] = (double)p.py;
+  st.z[i] = (double)p.pz;
+  st.mass[i] = p.mass;
+  st.mat[i] = p.mat;
+  st.prov[i] = p.prov;
+  st.id[i] = (unsigned)i;
+  rho[i] = p.rho;
+}
+int launch_from_aos(const Dev& d, cudaStream_t s) {
+  k_from_aos<<<(d.n + 255) / 256, 256, 0, s>>>(d.n, (const P48*)d.aos, d.s(), d.rho);
+  return 1;
+}
+
+__global__ void k_to_aos(int n, State st, const float* __restrict__ rho, P48* __restrict__ aos) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const float4 p = st.pos_h[t];
+  const float4 v = st.vel_u[t];
+  P48 o;
+  o.px = (float)st.x[t];
+  o.py = (float)st.y[t];
+  o.pz = (float)st.z[t];
+  o.h = p.w;
+  o.vx = v.x;
+  o.vy = v.y;
+  o.vz = v.z;
+  o.u = v.w;
+  o.mass = st.mass[t];
+  o.mat = st.mat[t];
+  o.rho = rho[t];
+  o.prov = st.prov[t];
+  aos[st.id[t]] = o;
+}
+int launch_to_aos(const Dev& d, cudaStream_t s) {
+  k_to_aos<<<(d.n + 255) / 256, 256, 0, s>>>(d.n, d.s(), d.rho, (P48*)d.aos);
+  return 1;
+}
+
+// ---------------------------------------------------------------------------------------------------
+// FP64 conservation sums, deterministic two-pass reduction: [mass, KE, IE, PE, p.xyz, L.xyz].
+// ---------------------------------------------------------------------------------------------------
+constexpr int DG_VALS = 10;
+__global__ void k_diag_partial(int n, State st, const float4* __restrict__ grav, double* __restrict__ part) {
+  double v[DG_VALS];
+#pragma unroll
+  for (int k = 0; k < DG_VALS; ++k) v[k] = 0.0;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    const double m = st.mass[t];
+    const float4 vu = st.vel_u[t];
+    const double vx = vu.x, vy = vu.y, vz = vu.z;
+    const double x = st.x[t], y = st.y[t], z = st.z[t];
+    v[0] += m;
+    v[1] += 0.5 * m * (vx * vx + vy * vy + vz * vz);
+    v[2] += m * (double)vu.w;
+    v[3] += grav ? 0.5 * m * (double)grav[t].w : 0.0;
+    v[4] += m * vx;
+    v[5] += m * vy;
+    v[6] += m * vz;
+    v[7] += m * (y * vz - z * vy);
+    v[8] += m * (z * vx - x * vz);
+    v[9] += m * (x * vy - y * vx);
+  }
+  __shared__ double s[DG_VALS][8];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+  for (int k = 0; k < DG_VALS; ++k) {
+    const double r = warp_sum(v[k]);
+    if (lane == 0) s[k][w] = r;
+  }
+  __syncthreads();
+  if (threadIdx.x < DG_VALS) {
+    double r = 0.0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) r += s[threadIdx.x][k];
+    part[blockIdx.x * 16 + threadIdx.x] = r;
+  }
+}
+__global__ void k_diag_final(const double* __restrict__ part, int blocks, double* __restrict__ out) {
+  if (threadIdx.x < DG_VALS) {
+    double r = 0.0;
+    for (int b = 0; b < blocks; ++b) r += part[b * 16 + threadIdx.x];
+    out[threadIdx.x] = r;
+  }
+}
+int launch_diag(const Dev& d, cudaStream_t s, double* out16) {
+  k_diag_partial<<<d.diag_blocks, 256, 0, s>>>(d.n, d.s(), d.grav, d.diag_part);
+  k_diag_final<<<1, 32, 0, s>>>(d.diag_part, d.diag_blocks, out16);
+  return 2;
+}
+
+}  // namespace sphb

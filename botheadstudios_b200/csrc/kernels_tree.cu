@@ -1,0 +1,509 @@
+// LBVH construction on B200: bounding box → 30-bit Morton keys → LSD radix sort → state permutation →
+// Karras internal nodes → single-pass bottom-up moments.
+//
+// Reference: shaders/bh_gravity.wgsl (cs_bbox :68, cs_morton :100, cs_tree :135, cs_com :201) and the CPU
+// sort of crates/engine/src/gpu_gravity.rs:336-368. The sort order is (Morton code, original index), made
+// exact by sorting 64-bit keys code<<idbits | index, so the permutation, the leaf codes and the Karras
+// topology are bit-identical to the reference's.
+#include <cuda/atomic>
+
+#include "sph_kernels.cuh"
+
+namespace sphb {
+
+// ---------------------------------------------------------------------------------------------------
+// Bounding box (cs_bbox): reduce order-preserving u32 keys per block, one atomic per block and axis.
+// ---------------------------------------------------------------------------------------------------
+__global__ void k_bbox_reset(DevParams* P) {
+  const int i = threadIdx.x;
+  if (i < 3) P->bbox_keys[i] = 0xffffffffu;
+  else if (i < 6) P->bbox_keys[i] = 0u;
+}
+
+__device__ __forceinline__ void block_bbox_commit(unsigned lo[3], unsigned hi[3], DevParams* P) {
+  __shared__ unsigned s_lo[3][32], s_hi[3][32];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    lo[k] = warp_min(lo[k]);
+    hi[k] = warp_max(hi[k]);
+    if (lane == 0) { s_lo[k][w] = lo[k]; s_hi[k][w] = hi[k]; }
+  }
+  __syncthreads();
+  if (w == 0) {
+    const int nw = blockDim.x >> 5;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      unsigned a = lane < nw ? s_lo[k][lane] : 0xffffffffu;
+      unsigned b = lane < nw ? s_hi[k][lane] : 0u;
+      a = warp_min(a);
+      b = warp_max(b);
+      if (lane == 0) {
+        atomicMin(&P->bbox_keys[k], a);
+        atomicMax(&P->bbox_keys[3 + k], b);
+      }
+    }
+  }
+}
+
+__global__ void k_bbox(const float4* __restrict__ pos, int n, DevParams* P) {
+  unsigned lo[3] = {0xffffffffu, 0xffffffffu, 0xffffffffu}, hi[3] = {0u, 0u, 0u};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const float4 p = pos[i];
+    const unsigned kx = float_key(p.x), ky = float_key(p.y), kz = float_key(p.z);
+    lo[0] = min(lo[0], kx); lo[1] = min(lo[1], ky); lo[2] = min(lo[2], kz);
+    hi[0] = max(hi[0], kx); hi[1] = max(hi[1], ky); hi[2] = max(hi[2], kz);
+  }
+  block_bbox_commit(lo, hi, P);
+}
+
+int launch_bbox_reset(const Dev& d, cudaStream_t s) { k_bbox_reset<<<1, 32, 0, s>>>(d.P);  return 1; }
+
+int launch_bbox(const Dev& d, cudaStream_t s) {
+  k_bbox_reset<<<1, 32, 0, s>>>(d.P);
+  const int threads = 256;
+  int blocks = (d.n + threads - 1) / threads;
+  blocks = blocks < 1 ? 1 : (blocks > 148 * 8 ? 148 * 8 : blocks);
+  k_bbox<<<blocks, threads, 0, s>>>(d.s().pos_h, d.n, d.P);
+  return 2;
+}
+
+// ---------------------------------------------------------------------------------------------------
+// Morton keys (cs_morton, bh_gravity.wgsl:91-108) with IEEE division, no contraction.
+// ---------------------------------------------------------------------------------------------------
+__global__ void k_keys(const float4* __restrict__ pos, const unsigned* __restrict__ id, int n, const DevParams* P,
+                       int idbits, unsigned long long* __restrict__ keys, unsigned* __restrict__ vals) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float lo[3], ext[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    lo[k] = key_float(P->bbox_keys[k]);
+    ext[k] = fmaxf(fsub(key_float(P->bbox_keys[3 + k]), lo[k]), 1.0e-30f);
+  }
+  const float4 p = pos[i];
+  const float pc[3] = {p.x, p.y, p.z};
+  unsigned q[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    float u = fdiv(fsub(pc[k], lo[k]), ext[k]);
+    u = fminf(fmaxf(u, 0.0f), 1.0f);
+    float f = floorf(fmul(u, 1024.0f));
+    f = fminf(fmaxf(f, 0.0f), 1023.0f);
+    q[k] = (unsigned)f;
+  }
+  const unsigned code = expand_bits(q[0]) * 4u + expand_bits(q[1]) * 2u + expand_bits(q[2]);
+  keys[i] = ((unsigned long long)code << idbits) | (unsigned long long)id[i];
+  vals[i] = (unsigned)i;
+}
+
+// ---------------------------------------------------------------------------------------------------
+// LSD radix sort, 8-bit digits, reduce-then-scan (no inter-block waits): upsweep histograms per tile,
+// per-digit scans over tiles, stable downsweep (warp match_any ranking, staged through shared memory).
+// ---------------------------------------------------------------------------------------------------
+constexpr int RS_THREADS = 256;
+constexpr int RS_ITEMS = 8;
+constexpr int RS_TILE = RS_THREADS * RS_ITEMS;  // 2048 keys per tile
+constexpr int RS_WARPS = RS_THREADS / 32;
+
+size_t radix_tiles(int n) { return (size_t)((n + RS_TILE - 1) / RS_TILE); }
+
+__global__ void __launch_bounds__(RS_THREADS) k_rs_upsweep(const unsigned long long* __restrict__ keys, int n,
+                                                           int shift, unsigned* __restrict__ hist, int T) {
+  __shared__ unsigned h[256];
+  h[threadIdx.x] = 0;
+  __syncthreads();
+  const int base = blockIdx.x * RS_TILE;
+#pragma unroll
+  for (int it = 0; it < RS_ITEMS; ++it) {
+    const int idx = base + it * RS_THREADS + threadIdx.x;
+    if (idx < n) atomicAdd(&h[(unsigned)(keys[idx] >> shift) & 255u], 1u);
+  }
+  __syncthreads();
+  hist[threadIdx.x * T + blockIdx.x] = h[threadIdx.x];
+}
+
+// Block-wide exclusive scan of one value per thread (blockDim.x <= 1024). Returns the block total.
+__device__ __forceinline__ unsigned block_exclusive_scan(unsigned v, unsigned* s_warp, unsigned& total) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  unsigned incl = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned t = __shfl_up_sync(SPH_FULL_MASK, incl, o);
+    if (lane >= o) incl += t;
+  }
+  if (lane == 31) s_warp[w] = incl;
+  __syncthreads();
+  if (w == 0) {
+    unsigned x = lane < nw ? s_warp[lane] : 0u;
+    unsigned xi = x;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned t = __shfl_up_sync(SPH_FULL_MASK, xi, o);
+      if (lane >= o) xi += t;
+    }
+    if (lane < nw) s_warp[lane] = xi - x;
+    if (lane == 31) s_warp[32] = xi;
+  }
+  __syncthreads();
+  const unsigned res = s_warp[w] + incl - v;
+  total = s_warp[32];
+  __syncthreads();
+  return res;
+}
+
+// One block per digit: exclusive scan of hist[d][0..T) in place; tot[d] = sum.
+__global__ void __launch_bounds__(1024) k_rs_scan(unsigned* __restrict__ hist, unsigned* __restrict__ tot, int T) {
+  __shared__ unsigned s_warp[33];
+  unsigned* h = hist + (size_t)blockIdx.x * T;
+  const int per = (T + blockDim.x - 1) / blockDim.x;
+  const int b0 = threadIdx.x * per;
+  unsigned sum = 0;
+  for (int i = 0; i < per; ++i)
+    if (b0 + i < T) sum += h[b0 + i];
+  unsigned total;
+  unsigned run = block_exclusive_scan(sum, s_warp, total);
+  for (int i = 0; i < per; ++i)
+    if (b0 + i < T) {
+      const unsigned v = h[b0 + i];
+      h[b0 + i] = run;
+      run += v;
+    }
+  if (threadIdx.x == 0) tot[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(RS_THREADS) k_rs_downsweep(const unsigned long long* __restrict__ kin,
+                                                             const unsigned* __restrict__ vin,
+                                                             unsigned long long* __restrict__ kout,
+                                                             unsigned* __restrict__ vout, int n, int shift,
+                                                             const unsigned* __restrict__ hist,
+                                                             const unsigned* __restrict__ tot, int T) {
+  __shared__ unsigned long long s_keys[RS_TILE];
+  __shared__ unsigned s_vals[RS_TILE];
+  __shared__ unsigned s_wcnt[RS_WARPS][256];
+  __shared__ unsigned s_gbin[256];     // global output start of digit d for this tile
+  __shared__ unsigned s_bstart[256];   // start of digit d inside the tile
+  __shared__ unsigned s_warp[33];
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const int base = blockIdx.x * RS_TILE;
+
+  // global digit starts: exclusive scan of the digit totals + this tile's prefix
+  unsigned total;
+  const unsigned dstart = block_exclusive_scan(tot[tid], s_warp, total);
+  s_gbin[tid] = dstart + hist[tid * T + blockIdx.x];
+#pragma unroll
+  for (int k = 0; k < RS_WARPS; ++k) s_wcnt[k][tid] = 0;
+  __syncthreads();
+
+  unsigned long long key[RS_ITEMS];
+  unsigned val[RS_ITEMS], dig[RS_ITEMS], loc[RS_ITEMS];
+  const unsigned lt_mask = (1u << lane) - 1u;
+#pragma unroll
+  for (int it = 0; it < RS_ITEMS; ++it) {
+    const int idx = base + (w * RS_ITEMS + it) * 32 + lane;
+    const bool ok = idx < n;
+    key[it] = ok ? kin[idx] : 0ull;
+    val[it] = ok ? vin[idx] : 0u;
+    const unsigned d = ok ? ((unsigned)(key[it] >> shift) & 255u) : 256u;
+    dig[it] = d;
+    const unsigned peers = __match_any_sync(SPH_FULL_MASK, d);
+    const int leader = __ffs(peers) - 1;
+    unsigned old = 0;
+    if (lane == leader && ok) {
+      old = s_wcnt[w][d];
+      s_wcnt[w][d] = old + __popc(peers);
+    }
+    old = __shfl_sync(SPH_FULL_MASK, old, leader);
+    loc[it] = old + __popc(peers & lt_mask);
+    __syncwarp();
+  }
+  __syncthreads();
+  // per digit: exclusive prefix over warps, then over digits within the tile
+  {
+    unsigned run = 0;
+#pragma unroll
+    for (int k = 0; k < RS_WARPS; ++k) {
+      const unsigned c = s_wcnt[k][tid];
+      s_wcnt[k][tid] = run;
+      run += c;
+    }
+    unsigned t2;
+    s_bstart[tid] = block_exclusive_scan(run, s_warp, t2);
+  }
+  __syncthreads();
+#pragma unroll
+  for (int it = 0; it < RS_ITEMS; ++it) {
+    if (dig[it] < 256u) {
+      const unsigned p = s_bstart[dig[it]] + s_wcnt[w][dig[it]] + loc[it];
+      s_keys[p] = key[it];
+      s_vals[p] = val[it];
+    }
+  }
+  __syncthreads();
+  const int cnt = min(RS_TILE, n - base);
+  for (int i = tid; i < cnt; i += RS_THREADS) {
+    const unsigned long long k = s_keys[i];
+    const unsigned d = (unsigned)(k >> shift) & 255u;
+    const unsigned g = s_gbin[d] + (unsigned)i - s_bstart[d];
+    kout[g] = k;
+    vout[g] = s_vals[i];
+  }
+}
+
+// ---------------------------------------------------------------------------------------------------
+// Permutation of the particle state into the new order; leaf cluster codes (gpu_gravity.rs:366).
+// ---------------------------------------------------------------------------------------------------
+__global__ void k_permute(int n, int K, int idbits, const unsigned* __restrict__ order,
+                          const unsigned long long* __restrict__ skeys, State in, State out,
+                          float4* __restrict__ body, unsigned* __restrict__ leaf_codes) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const unsigned o = order[t];
+  const float4 p = in.pos_h[o];
+  const float m = in.mass[o];
+  out.pos_h[t] = p;
+  out.vel_u[t] = in.vel_u[o];
+  out.x[t] = in.x[o];
+  out.y[t] = in.y[o];
+  out.z[t] = in.z[o];
+  out.mass[t] = m;
+  out.mat[t] = in.mat[o];
+  out.prov[t] = in.prov[o];
+  out.id[t] = in.id[o];
+  body[t] = make_float4(p.x, p.y, p.z, m);
+  if (t % K == 0) leaf_codes[t / K] = (unsigned)(skeys[t] >> idbits);
+}
+
+int launch_sort_permute(Dev& d, cudaStream_t s) {
+  const int n = d.n;
+  const int threads = 256;
+  const int blocks = (n + threads - 1) / threads;
+  const State& in = d.st[d.cur];
+  k_keys<<<blocks, threads, 0, s>>>(in.pos_h, in.id, n, d.P, d.idbits, d.keys[0], d.vals[0]);
+  const int T = (int)radix_tiles(n);
+  const int total_bits = 30 + d.idbits;
+  const int passes = (total_bits + 7) / 8;
+  int src = 0;
+  for (int shift = 0; shift < total_bits; shift += 8) {
+    k_rs_upsweep<<<T, RS_THREADS, 0, s>>>(d.keys[src], n, shift, d.rs_hist, T);
+    k_rs_scan<<<256, 1024, 0, s>>>(d.rs_hist, d.rs_tot, T);
+    k_rs_downsweep<<<T, RS_THREADS, 0, s>>>(d.keys[src], d.vals[src], d.keys[src ^ 1], d.vals[src ^ 1], n, shift,
+                                             d.rs_hist, d.rs_tot, T);
+    src ^= 1;
+  }
+  // vals[src] = old slot of each sorted position; keys[src] = sorted keys
+  const State& out = d.st[d.cur ^ 1];
+  k_permute<<<blocks, threads, 0, s>>>(n, d.K, d.idbits, d.vals[src], d.keys[src], in, out, d.body, d.leaf_codes);
+  d.cur ^= 1;
+  // keep the sorted keys in keys[0] for inspection
+  if (src != 0) cudaMemcpyAsync(d.keys[0], d.keys[src], sizeof(unsigned long long) * n, cudaMemcpyDeviceToDevice, s);
+  return 2 + 3 * passes;
+}
+
+// ---------------------------------------------------------------------------------------------------
+// Karras 2012 internal nodes over the leaf cluster codes (cs_tree, bh_gravity.wgsl:114-184).
+// ---------------------------------------------------------------------------------------------------
+__device__ __forceinline__ int kdelta(const unsigned* __restrict__ codes, int L, int i, int j) {
+  if (j < 0 || j >= L) return -1;
+  const unsigned ci = codes[i], cj = codes[j];
+  if (ci == cj) return 32 + __clz((unsigned)i ^ (unsigned)j);
+  return __clz(ci ^ cj);
+}
+
+// Particles covered by leaves [first, last] (the last leaf may be partial).
+__device__ __forceinline__ int range_count(int first, int last, int K, int n) {
+  return min((last + 1) * K, n) - first * K;
+}
+
+__global__ void k_karras(const unsigned* __restrict__ codes, int L, int K, int n, unsigned* __restrict__ left,
+                         unsigned* __restrict__ right, unsigned* __restrict__ parent, uint2* __restrict__ groups,
+                         unsigned* __restrict__ ngroups, int exact_dups) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= L - 1) return;
+  const int d = kdelta(codes, L, i, i + 1) > kdelta(codes, L, i, i - 1) ? 1 : -1;
+  const int dmin = kdelta(codes, L, i, i - d);
+  int lmax = 2;
+  while (kdelta(codes, L, i, i + lmax * d) > dmin) lmax *= 2;
+  int l = 0;
+  for (int t = lmax / 2; t >= 1; t /= 2)
+    if (kdelta(codes, L, i, i + (l + t) * d) > dmin) l += t;
+  const int j = i + l * d;
+  const int first = min(i, j), last = max(i, j);
+  int split = first;
+  const unsigned fc = codes[first], lc = codes[last];
+  if (fc == lc && !exact_dups) {
+    // the reference's split of a run of equal codes (bh_gravity.wgsl:159-160); it can disagree with the
+    // index-extended ranges the children compute for themselves, so such trees may be invalid
+    split = (first + last) >> 1;
+  } else if (fc == lc) {
+    // Karras 2012 §4: index-extended keys — binary search on the common prefix of the indices
+    const int cpfx = kdelta(codes, L, first, last);
+    int step = last - first;
+    for (;;) {
+      step = (step + 1) >> 1;
+      const int ns = split + step;
+      if (ns < last && kdelta(codes, L, first, ns) > cpfx) split = ns;
+      if (step <= 1) break;
+    }
+  } else {
+    const int cpfx = __clz(fc ^ lc);
+    int step = last - first;
+    for (;;) {
+      step = (step + 1) >> 1;
+      const int ns = split + step;
+      if (ns < last && __clz(fc ^ codes[ns]) > cpfx) split = ns;
+      if (step <= 1) break;
+    }
+  }
+  const unsigned lidx = (split == first) ? (unsigned)(L - 1 + split) : (unsigned)split;
+  const unsigned ridx = (split + 1 == last) ? (unsigned)(L - 1 + split + 1) : (unsigned)(split + 1);
+  left[i] = lidx;
+  right[i] = ridx;
+  parent[lidx] = (unsigned)i;
+  parent[ridx] = (unsigned)i;
+  // Walk groups: the maximal subtrees holding at most 32 particles. A node above the limit emits each child
+  // that fits; the root emits itself when the whole set fits. Subtrees share a Morton prefix, so every
+  // group's bounding box is compact.
+  if (range_count(first, last, K, n) > 32) {
+    if (range_count(first, split, K, n) <= 32) groups[atomicAdd(ngroups, 1u)] = make_uint2(first, split);
+    if (range_count(split + 1, last, K, n) <= 32) groups[atomicAdd(ngroups, 1u)] = make_uint2(split + 1, last);
+  } else if (i == 0) {
+    groups[atomicAdd(ngroups, 1u)] = make_uint2(first, last);
+  }
+}
+
+__global__ void k_single_group(uint2* groups, unsigned* ngroups, int L) {
+  groups[0] = make_uint2(0u, (unsigned)(L - 1));
+  *ngroups = 1u;
+}
+
+// ---------------------------------------------------------------------------------------------------
+// Bottom-up moments (cs_com, bh_gravity.wgsl:201-241), single pass: each leaf thread sums its bucket, then
+// climbs; the first child to arrive at a parent stops, the second merges. The arrival counter is an
+// acq_rel device-scope atomic, so the second arrival sees the sibling's node data (the ordering that WGSL
+// could not express and that made the reference fall back to a 33-dispatch sweep). The climb is bounded
+// by the tree height; nothing waits.
+// Node data: com.xyz/mass (mass-weighted merge, same f32 operations as the reference), AABB with the
+// subtree's max smoothing length, the opening radius diag/θ + |centre − COM| and, optionally, the
+// traceless quadrupole about the COM (parallel-axis merge).
+// ---------------------------------------------------------------------------------------------------
+template <bool QUAD>
+__global__ void k_leaf_climb(const float4* __restrict__ body, const float4* __restrict__ pos_h, int n, int K,
+                             int L, const unsigned* __restrict__ left, const unsigned* __restrict__ right,
+                             const unsigned* __restrict__ parent, unsigned* __restrict__ counters,
+                             float4* __restrict__ ncom, float4* __restrict__ nbmin, float4* __restrict__ nbmax,
+                             float4* __restrict__ nq0, float4* __restrict__ nq1, float theta, int side_mac) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= L) return;
+  const int li = L - 1 + c;
+  const int s0 = c * K, s1 = min(s0 + K, n);
+  float m = 0.0f, mx = 0.0f, my = 0.0f, mz = 0.0f, hmax = 0.0f;
+  float lo[3] = {1.0e30f, 1.0e30f, 1.0e30f}, hi[3] = {-1.0e30f, -1.0e30f, -1.0e30f};
+  for (int s = s0; s < s1; ++s) {
+    const float4 b = body[s];
+    m = fadd(m, b.w);
+    mx = fadd(mx, fmul(b.x, b.w));
+    my = fadd(my, fmul(b.y, b.w));
+    mz = fadd(mz, fmul(b.z, b.w));
+    lo[0] = fminf(lo[0], b.x); lo[1] = fminf(lo[1], b.y); lo[2] = fminf(lo[2], b.z);
+    hi[0] = fmaxf(hi[0], b.x); hi[1] = fmaxf(hi[1], b.y); hi[2] = fmaxf(hi[2], b.z);
+    hmax = fmaxf(hmax, pos_h[s].w);
+  }
+  float4 com = make_float4(m > 0.0f ? fdiv(mx, m) : 0.0f, m > 0.0f ? fdiv(my, m) : 0.0f,
+                           m > 0.0f ? fdiv(mz, m) : 0.0f, m);
+  {
+    const float ex = fsub(hi[0], lo[0]), ey = fsub(hi[1], lo[1]), ez = fsub(hi[2], lo[2]);
+    const float size = side_mac ? fmaxf(fmaxf(ex, ey), ez) : fsqrt(dot3_exact(ex, ey, ez));
+    const float cx = fsub(fmul(0.5f, fadd(lo[0], hi[0])), com.x), cy = fsub(fmul(0.5f, fadd(lo[1], hi[1])), com.y),
+                cz = fsub(fmul(0.5f, fadd(lo[2], hi[2])), com.z);
+    const float rc = fadd(fdiv(size, theta), fsqrt(dot3_exact(cx, cy, cz)));
+    ncom[li] = com;
+    nbmin[li] = make_float4(lo[0], lo[1], lo[2], hmax);
+    nbmax[li] = make_float4(hi[0], hi[1], hi[2], rc);
+  }
+  if (QUAD) {
+    float qxx = 0, qyy = 0, qzz = 0, qxy = 0, qxz = 0, qyz = 0;
+    for (int s = s0; s < s1; ++s) {
+      const float4 b = body[s];
+      const float dx = b.x - com.x, dy = b.y - com.y, dz = b.z - com.z;
+      const float r2 = dx * dx + dy * dy + dz * dz;
+      qxx += b.w * (3.0f * dx * dx - r2);
+      qyy += b.w * (3.0f * dy * dy - r2);
+      qzz += b.w * (3.0f * dz * dz - r2);
+      qxy += b.w * 3.0f * dx * dy;
+      qxz += b.w * 3.0f * dx * dz;
+      qyz += b.w * 3.0f * dy * dz;
+    }
+    nq0[li] = make_float4(qxx, qyy, qzz, qxy);
+    nq1[li] = make_float4(qxz, qyz, 0.0f, 0.0f);
+  }
+  unsigned node = parent[li];
+  while (node != SPH_NO_PARENT) {
+    cuda::atomic_ref<unsigned, cuda::thread_scope_device> cnt(counters[node]);
+    const unsigned arrived = cnt.fetch_add(1u, cuda::memory_order_acq_rel);
+    if (arrived == 0u) return;  // the sibling subtree finishes this node
+    const unsigned l = left[node], r = right[node];
+    const float4 cl = __ldcg(&ncom[l]), cr = __ldcg(&ncom[r]);
+    const float4 ll = __ldcg(&nbmin[l]), rl = __ldcg(&nbmin[r]);
+    const float4 lh = __ldcg(&nbmax[l]), rh = __ldcg(&nbmax[r]);
+    const float mm = fadd(cl.w, cr.w);
+    const float4 pc = make_float4(mm > 0.0f ? fdiv(fadd(fmul(cl.x, cl.w), fmul(cr.x, cr.w)), mm) : 0.0f,
+                                  mm > 0.0f ? fdiv(fadd(fmul(cl.y, cl.w), fmul(cr.y, cr.w)), mm) : 0.0f,
+                                  mm > 0.0f ? fdiv(fadd(fmul(cl.z, cl.w), fmul(cr.z, cr.w)), mm) : 0.0f, mm);
+    const float bl[3] = {fminf(ll.x, rl.x), fminf(ll.y, rl.y), fminf(ll.z, rl.z)};
+    const float bh[3] = {fmaxf(lh.x, rh.x), fmaxf(lh.y, rh.y), fmaxf(lh.z, rh.z)};
+    const float ex = fsub(bh[0], bl[0]), ey = fsub(bh[1], bl[1]), ez = fsub(bh[2], bl[2]);
+    const float size = side_mac ? fmaxf(fmaxf(ex, ey), ez) : fsqrt(dot3_exact(ex, ey, ez));
+    const float cx = fsub(fmul(0.5f, fadd(bl[0], bh[0])), pc.x), cy = fsub(fmul(0.5f, fadd(bl[1], bh[1])), pc.y),
+                cz = fsub(fmul(0.5f, fadd(bl[2], bh[2])), pc.z);
+    const float rc = fadd(fdiv(size, theta), fsqrt(dot3_exact(cx, cy, cz)));
+    ncom[node] = pc;
+    nbmin[node] = make_float4(bl[0], bl[1], bl[2], fmaxf(ll.w, rl.w));
+    nbmax[node] = make_float4(bh[0], bh[1], bh[2], rc);
+    if (QUAD) {
+      float4 q0 = make_float4(0, 0, 0, 0), q1 = make_float4(0, 0, 0, 0);
+      const float4 cc[2] = {cl, cr};
+      const unsigned ch[2] = {l, r};
+#pragma unroll
+      for (int k = 0; k < 2; ++k) {
+        const float4 a0 = __ldcg(&nq0[ch[k]]), a1 = __ldcg(&nq1[ch[k]]);
+        const float sx = cc[k].x - pc.x, sy = cc[k].y - pc.y, sz = cc[k].z - pc.z, w = cc[k].w;
+        const float s2 = sx * sx + sy * sy + sz * sz;
+        q0.x += a0.x + w * (3.0f * sx * sx - s2);
+        q0.y += a0.y + w * (3.0f * sy * sy - s2);
+        q0.z += a0.z + w * (3.0f * sz * sz - s2);
+        q0.w += a0.w + w * 3.0f * sx * sy;
+        q1.x += a1.x + w * 3.0f * sx * sz;
+        q1.y += a1.y + w * 3.0f * sy * sz;
+      }
+      nq0[node] = q0;
+      nq1[node] = q1;
+    }
+    node = parent[node];
+  }
+}
+
+int launch_tree(const Dev& d, const Cfg& c, float theta, cudaStream_t s) {
+  const int L = d.L;
+  cudaMemsetAsync(d.parent, 0xff, sizeof(unsigned) * (2 * (size_t)L - 1), s);
+  cudaMemsetAsync(d.ngroups, 0, sizeof(unsigned), s);
+  if (L > 1) {
+    cudaMemsetAsync(d.counters, 0, sizeof(unsigned) * (L - 1), s);
+    k_karras<<<(L - 1 + 255) / 256, 256, 0, s>>>(d.leaf_codes, L, d.K, d.n, d.left, d.right, d.parent, d.groups,
+                                                  d.ngroups, c.mac == 0 ? 1 : 0);
+  } else {
+    k_single_group<<<1, 1, 0, s>>>(d.groups, d.ngroups, L);
+  }
+  const State& st = d.s();
+  if (c.quad)
+    k_leaf_climb<true><<<(L + 127) / 128, 128, 0, s>>>(d.body, st.pos_h, d.n, d.K, L, d.left, d.right, d.parent,
+                                                       d.counters, d.ncom, d.nbmin, d.nbmax, d.nq0, d.nq1, theta,
+                                                       c.mac == 0 ? 1 : 0);
+  else
+    k_leaf_climb<false><<<(L + 127) / 128, 128, 0, s>>>(d.body, st.pos_h, d.n, d.K, L, d.left, d.right, d.parent,
+                                                        d.counters, d.ncom, d.nbmin, d.nbmax, d.nq0, d.nq1, theta,
+                                                       c.mac == 0 ? 1 : 0);
+  return 2;
+}
+
+}  // namespace sphb

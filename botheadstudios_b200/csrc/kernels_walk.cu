@@ -1,0 +1,368 @@
+// Fused LBVH group walk: Barnes-Hut gravity (group MAC, monopole + optional quadrupole) and the SPH
+// neighbour lists in ONE traversal per warp.
+//
+// A warp owns 32 Morton-consecutive particles (its "group") and walks the tree with a LIFO stack in shared
+// memory, popping up to 32 nodes at a time (one per lane) so node loads overlap instead of serialising.
+// Each popped node is classified for the whole group:
+//   * accepted  — the reference MAC (sqrt(d²+ε²) >= diag/θ + |centre−COM|, bh_gravity.wgsl:382) holds for
+//                 the nearest point of the group's bounding box, hence for every particle of the group, and
+//                 the node's box is outside the SPH reach: appended to the multipole list;
+//   * leaf      — appended to the direct list (pairwise gravity + the exact neighbour predicate);
+//   * opened    — children pushed (ballot + popc compaction).
+// Nodes whose box lies within ½(h_group,max + h_node,max) of the group are always opened, so every leaf
+// that can hold an SPH neighbour reaches the direct list: the neighbour set {j != i : r_ij < h_ij} is
+// complete and, with single-rounded arithmetic, identical to the reference predicate (sph_step.wgsl:141-143).
+// Lists are flushed through shared memory in chunks of 32 sources; every lane then runs the chunk against
+// its own particle with no dependent loads (the interaction loop is pure FP32 work).
+#include "sph_kernels.cuh"
+
+namespace sphb {
+
+constexpr int TW_WARPS = 4;
+constexpr int TW_STACK = 1536;  // per-warp node stack
+constexpr int TW_LIST = 64;     // per-warp list capacity (flushed once half full)
+
+struct WalkSmem {
+  unsigned stack[TW_WARPS][TW_STACK];
+  unsigned m2p[TW_WARPS][TW_LIST];
+  unsigned p2p[TW_WARPS][TW_LIST];
+  float4 src[TW_WARPS][32];   // staged sources: x, y, z, m
+  float4 q0[TW_WARPS][32];    // staged quadrupoles
+  float2 q1[TW_WARPS][32];
+  float hsrc[TW_WARPS][32];   // staged smoothing lengths (direct list)
+  int sidx[TW_WARPS][32];     // staged source indices (direct list)
+};
+
+// Compensated accumulator for the precision mode.
+struct Acc3 {
+  float x = 0.f, y = 0.f, z = 0.f, cx = 0.f, cy = 0.f, cz = 0.f;
+  template <bool KAHAN>
+  __device__ __forceinline__ void add(float ax, float ay, float az) {
+    if (KAHAN) {
+      float yy = ax - cx, t = x + yy;
+      cx = (t - x) - yy;
+      x = t;
+      yy = ay - cy;
+      t = y + yy;
+      cy = (t - y) - yy;
+      y = t;
+      yy = az - cz;
+      t = z + yy;
+      cz = (t - z) - yy;
+      z = t;
+    } else {
+      x += ax;
+      y += ay;
+      z += az;
+    }
+  }
+};
+
+template <bool GRAV, bool QUAD, bool NBR, bool HILO>
+__global__ void __launch_bounds__(TW_WARPS * 32, 6) k_tree_walk(
+    const float4* __restrict__ body, const float4* __restrict__ pos_h, const double* __restrict__ x64,
+    const double* __restrict__ y64, const double* __restrict__ z64, int n, int K, int L,
+    const unsigned* __restrict__ left, const unsigned* __restrict__ right, const float4* __restrict__ ncom,
+    const float4* __restrict__ nbmin, const float4* __restrict__ nbmax, const float4* __restrict__ nq0,
+    const float4* __restrict__ nq1, DevParams* P, float4* __restrict__ gout, unsigned* __restrict__ nbr,
+    unsigned* __restrict__ nbr_cnt, unsigned cap, float skin, float* __restrict__ h0,
+    const uint2* __restrict__ groups, const unsigned* __restrict__ ngroups) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  WalkSmem& S = *reinterpret_cast<WalkSmem*>(smem_raw);
+  const int w = threadIdx.x >> 5;
+  const unsigned lane = threadIdx.x & 31u;
+  const int warp = blockIdx.x * TW_WARPS + w;
+  if (warp >= (int)*ngroups) return;
+  // this warp's group: a maximal subtree of <= 32 particles (leaves g.x..g.y)
+  const uint2 grp = groups[warp];
+  const int s0 = (int)grp.x * K, s1 = min(((int)grp.y + 1) * K, n);
+  const int t = s0 + (int)lane;
+  const bool in_group = t < s1;
+  const int tl = in_group ? t : s0;
+  const float4 pi = pos_h[tl];  // x, y, z, h (same f32 coordinates as body)
+  float xlo = 0.f, ylo = 0.f, zlo = 0.f;
+  if (HILO && in_group) {
+    xlo = (float)(x64[t] - (double)pi.x);
+    ylo = (float)(y64[t] - (double)pi.y);
+    zlo = (float)(z64[t] - (double)pi.z);
+  }
+  if (NBR && in_group && h0) h0[t] = pi.w;
+  // Split the group where consecutive particles are far apart (a leaf bucket of K consecutive Morton
+  // particles can straddle a jump of the curve, e.g. between two bodies): each segment walks with its own
+  // compact box, so one straddling bucket cannot turn the walk into an all-pairs sum.
+  const float px = __shfl_up_sync(SPH_FULL_MASK, pi.x, 1), py = __shfl_up_sync(SPH_FULL_MASK, pi.y, 1),
+              pz = __shfl_up_sync(SPH_FULL_MASK, pi.z, 1), ph_ = __shfl_up_sync(SPH_FULL_MASK, pi.w, 1);
+  const float gap2 = (pi.x - px) * (pi.x - px) + (pi.y - py) * (pi.y - py) + (pi.z - pz) * (pi.z - pz);
+  const float hm = 3.0f * fmaxf(pi.w, ph_);
+  const unsigned brk = __ballot_sync(SPH_FULL_MASK, lane > 0 && in_group && gap2 > hm * hm);
+  const int nseg = __popc(brk) + 1;
+  const int myseg = __popc(brk & ((2u << lane) - 1u));
+  const float grow = (1.0f + skin) * (1.0f + 1.0e-5f);
+  const float G = P->G, soft2 = P->soft2;
+  const unsigned leaf0 = (unsigned)(L - 1);
+  const unsigned lt = (1u << lane) - 1u;
+
+  Acc3 acc;
+  float phi = 0.f;
+  unsigned cnt = 0;
+  unsigned overflow = 0;
+  unsigned* stack = S.stack[w];
+  unsigned long long st_visits = 0, st_pops = 0, st_m2p = 0, st_p2p = 0;
+
+  for (int seg = 0; seg < nseg; ++seg) {
+  const bool valid = in_group && myseg == seg;
+  const float big = 3.0e38f;
+  const float gx0 = warp_min(valid ? pi.x : big), gy0 = warp_min(valid ? pi.y : big),
+              gz0 = warp_min(valid ? pi.z : big);
+  const float gx1 = warp_max(valid ? pi.x : -big), gy1 = warp_max(valid ? pi.y : -big),
+              gz1 = warp_max(valid ? pi.z : -big);
+  const float ghmax = warp_max(valid ? pi.w : 0.0f);
+  int sp = 1, nm = 0, np = 0;
+  if (lane == 0) stack[0] = 0u;
+  __syncwarp();
+
+  // ---- multipole list: stage 32 nodes in shared memory, then every lane applies them -------------------
+  auto flush_m2p = [&](int count) {
+    for (int base = 0; base < count; base += 32) {
+      const int m = min(32, count - base);
+      if ((int)lane < m) {
+        const unsigned node = S.m2p[w][base + lane];
+        S.src[w][lane] = ncom[node];
+        if (QUAD) {
+          S.q0[w][lane] = nq0[node];
+          const float4 b = nq1[node];
+          S.q1[w][lane] = make_float2(b.x, b.y);
+        }
+      }
+      __syncwarp();
+      if (valid) {
+        for (int k = 0; k < m; ++k) {
+          const float4 c = S.src[w][k];
+          float dx = c.x - pi.x, dy = c.y - pi.y, dz = c.z - pi.z;
+          if (HILO) { dx -= xlo; dy -= ylo; dz -= zlo; }
+          const float r2 = dx * dx + dy * dy + dz * dz + soft2;
+          const float rinv = rsqrtf(r2);
+          const float rinv2 = rinv * rinv;
+          const float gm = G * c.w * rinv;
+          float fx = gm * rinv2 * dx, fy = gm * rinv2 * dy, fz = gm * rinv2 * dz;
+          float ph = -gm;
+          if (QUAD) {
+            const float4 a0 = S.q0[w][k];
+            const float2 a1 = S.q1[w][k];
+            const float ex = dx * rinv, ey = dy * rinv, ez = dz * rinv;
+            const float Qex = a0.x * ex + a0.w * ey + a1.x * ez;
+            const float Qey = a0.w * ex + a0.y * ey + a1.y * ez;
+            const float Qez = a1.x * ex + a1.y * ey + a0.z * ez;
+            const float eQe = ex * Qex + ey * Qey + ez * Qez;
+            const float s = G * rinv2;
+            fx += ((2.5f * eQe * ex - Qex) * rinv2) * s;
+            fy += ((2.5f * eQe * ey - Qey) * rinv2) * s;
+            fz += ((2.5f * eQe * ez - Qez) * rinv2) * s;
+            ph -= (0.5f * eQe * rinv2) * G * rinv;
+          }
+          acc.add<HILO>(fx, fy, fz);
+          phi += ph;
+        }
+      }
+      __syncwarp();
+    }
+  };
+
+  // ---- direct list: leaves of <= K sources (K divides 32), 32 sources per chunk ------------------------
+  auto flush_p2p = [&](int count) {
+    const int per = 32 / K;  // leaves per chunk
+    for (int base = 0; base < count; base += per) {
+      const int nl = min(per, count - base);
+      const int li = lane / K, off = lane % K;
+      int sidx = -1;
+      bool near_src = false;
+      if (li < nl) {
+        const unsigned e = S.p2p[w][base + li];
+        const int s = (int)(e & 0x7fffffffu) * K + off;
+        near_src = (e >> 31) != 0u;
+        if (s < n) sidx = s;
+      }
+      S.sidx[w][lane] = sidx;
+      if (sidx >= 0) {
+        S.src[w][lane] = body[sidx];
+        // smoothing length of sources inside the SPH reach; -1 marks a source that cannot be a neighbour
+        if (NBR) S.hsrc[w][lane] = near_src ? pos_h[sidx].w : -1.0f;
+      }
+      const unsigned have = __ballot_sync(SPH_FULL_MASK, sidx >= 0);
+      __syncwarp();
+      if (valid) {
+        unsigned m = have;
+        while (m) {
+          const int k = __ffs(m) - 1;
+          m &= m - 1;
+          const int s = S.sidx[w][k];
+          if (s == t) continue;
+          const float4 bj = S.src[w][k];
+          const float dx = fsub(bj.x, pi.x), dy = fsub(bj.y, pi.y), dz = fsub(bj.z, pi.z);
+          const float dd = dot3_exact(dx, dy, dz);
+          if (NBR) {
+            const float hj = S.hsrc[w][k];
+            if (hj >= 0.0f) {
+              const float r = fsqrt(dd);
+              float lim = fmul(0.5f, fadd(pi.w, hj));
+              if (skin > 0.0f) lim = lim * (1.0f + skin);
+              if (r < lim) {
+                if (cnt < cap) nbr[nbr_slot((unsigned)t, cnt, cap)] = (unsigned)s;
+                ++cnt;
+              }
+            }
+          }
+          if (GRAV) {
+            float ex = dx, ey = dy, ez = dz, d2 = dd;
+            if (HILO) {
+              ex -= xlo;
+              ey -= ylo;
+              ez -= zlo;
+              d2 = ex * ex + ey * ey + ez * ez;
+            }
+            const float r2 = d2 + soft2;
+            const float rinv = rsqrtf(r2);
+            const float gm = G * bj.w * rinv;
+            const float g = gm * rinv * rinv;
+            acc.add<HILO>(g * ex, g * ey, g * ez);
+            phi -= gm;
+          }
+        }
+      }
+      __syncwarp();
+    }
+  };
+
+  const unsigned nvalid = __popc(__ballot_sync(SPH_FULL_MASK, valid));
+  unsigned long long seg_m2p = 0, seg_p2p = 0;
+  while (sp > 0) {
+    const int take = min(sp, 32);
+    sp -= take;
+    st_visits += take;
+    ++st_pops;
+    const bool have = (int)lane < take;
+    const unsigned node = have ? stack[sp + lane] : 0u;
+    __syncwarp();
+    bool acc_node = false, leaf = false, open = false, near_leaf = false;
+    if (have) {
+      const float4 bl = nbmin[node], bh = nbmax[node];
+      const bool is_leaf = node >= leaf0;
+      bool near = false;
+      if (NBR) {
+        const float reach = 0.5f * (ghmax + bl.w) * grow;
+        near = (bl.x - reach <= gx1) && (bh.x + reach >= gx0) && (bl.y - reach <= gy1) && (bh.y + reach >= gy0) &&
+               (bl.z - reach <= gz1) && (bh.z + reach >= gz0);
+      }
+      bool mac = false;
+      if (GRAV) {
+        // leaves carry their own moments and may be accepted as well
+        const float4 c = ncom[node];
+        // distance from the COM to the nearest point of the group box
+        const float ddx = fmaxf(fmaxf(gx0 - c.x, c.x - gx1), 0.0f);
+        const float ddy = fmaxf(fmaxf(gy0 - c.y, c.y - gy1), 0.0f);
+        const float ddz = fmaxf(fmaxf(gz0 - c.z, c.z - gz1), 0.0f);
+        const float dmin = sqrtf(ddx * ddx + ddy * ddy + ddz * ddz + soft2);
+        mac = dmin >= bh.w * 1.00001f;
+      }
+      if (mac && !near) acc_node = true;
+      else if (is_leaf) leaf = GRAV || near;
+      else open = GRAV || near;
+      near_leaf = leaf && near;
+    }
+    const unsigned bm = __ballot_sync(SPH_FULL_MASK, acc_node);
+    const unsigned bf = __ballot_sync(SPH_FULL_MASK, leaf);
+    const unsigned bo = __ballot_sync(SPH_FULL_MASK, open);
+    if (acc_node) S.m2p[w][nm + __popc(bm & lt)] = node;
+    // direct-list entry: leaf index, bit 31 set when the leaf lies within the SPH reach
+    if (leaf) S.p2p[w][np + __popc(bf & lt)] = (node - leaf0) | (near_leaf ? 0x80000000u : 0u);
+    const int no = __popc(bo);
+    if (sp + 2 * no <= TW_STACK) {
+      if (open) {
+        const int r = sp + 2 * __popc(bo & lt);
+        stack[r] = left[node];
+        stack[r + 1] = right[node];
+      }
+      sp += 2 * no;
+    } else if (no) {
+      overflow = 1;
+    }
+    nm += __popc(bm);
+    np += __popc(bf);
+    seg_m2p += __popc(bm);
+    seg_p2p += __popc(bf);
+    __syncwarp();
+    if (nm > TW_LIST - 32) {
+      flush_m2p(nm);
+      nm = 0;
+    }
+    if (np > TW_LIST - 32) {
+      flush_p2p(np);
+      np = 0;
+    }
+  }
+  if (nm) flush_m2p(nm);
+  if (np) flush_p2p(np);
+  st_m2p += seg_m2p * nvalid;                             // node × particle interactions
+  st_p2p += seg_p2p * (unsigned long long)K * nvalid;     // leaf sources × particles (upper bound)
+  }  // segments
+
+  if (in_group && GRAV) gout[t] = make_float4(acc.x, acc.y, acc.z, phi);
+  if (NBR) {
+    if (in_group) nbr_cnt[t] = cnt;
+    const unsigned wmax = warp_max(in_group ? cnt : 0u);
+    if (lane == 0) {
+      atomicMax(&P->max_nbr_seen, wmax);
+      if (wmax > cap) atomicOr(&P->flags, kFlagNbrOverflow);
+    }
+  }
+  if (overflow && lane == 0) atomicOr(&P->flags, kFlagStackOverflow);
+  if (lane == 0) {
+    atomicAdd(&P->stat_visits, st_visits);
+    atomicAdd(&P->stat_pops, st_pops);
+    atomicAdd(&P->stat_m2p, st_m2p);
+    atomicAdd(&P->stat_p2p, st_p2p);
+  }
+}
+
+template <bool GRAV, bool QUAD, bool NBR, bool HILO>
+static void walk(const Dev& d, const Cfg& c, cudaStream_t s) {
+  const int warps = d.L;  // upper bound on the number of groups
+  const int blocks = (warps + TW_WARPS - 1) / TW_WARPS;
+  const size_t smem = sizeof(WalkSmem);
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_tree_walk<GRAV, QUAD, NBR, HILO>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    attr = true;
+  }
+  const State& st = d.s();
+  k_tree_walk<GRAV, QUAD, NBR, HILO><<<blocks, TW_WARPS * 32, smem, s>>>(
+      d.body, st.pos_h, st.x, st.y, st.z, d.n, d.K, d.L, d.left, d.right, d.ncom, d.nbmin, d.nbmax, d.nq0, d.nq1,
+      d.P, d.grav, d.nbr, d.nbr_cnt, d.nbr_cap, c.h_solve ? c.skin : 0.0f, d.h0, d.groups, d.ngroups);
+}
+
+// Gravity (group MAC) fused with the neighbour lists.
+int launch_walk(const Dev& d, const Cfg& c, cudaStream_t s) {
+  if (c.quad) {
+    if (c.hilo) walk<true, true, true, true>(d, c, s);
+    else walk<true, true, true, false>(d, c, s);
+  } else {
+    if (c.hilo) walk<true, false, true, true>(d, c, s);
+    else walk<true, false, true, false>(d, c, s);
+  }
+  return 1;
+}
+
+// Gravity only (group MAC), for point sets without SPH.
+int launch_gravity_group(const Dev& d, const Cfg& c, cudaStream_t s) {
+  if (c.quad) walk<true, true, false, false>(d, c, s);
+  else walk<true, false, false, false>(d, c, s);
+  return 1;
+}
+
+// Neighbour lists only (when gravity is not the tree).
+int launch_neighbours(const Dev& d, const Cfg& c, cudaStream_t s) {
+  walk<false, false, true, false>(d, c, s);
+  return 1;
+}
+
+}  // namespace sphb

@@ -1,0 +1,868 @@
+// Host side of the C ABI (include/sph_b200.h): the context that owns device memory, the CUDA stream and
+// the dispatch order of one KDK step. It mirrors the engine's GpuSph (crates/engine/src/gpu_sph.rs:742-922)
+// and ParticleStore (gpu_store.rs): capacity clamping on upload, enqueue-only stepping, a two-phase
+// non-blocking readback. Errors are status codes; nothing throws across the boundary.
+#include <cmath>
+#include <cstddef>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+#include <chrono>
+#include <thread>
+
+#include "../../include/sph_b200.h"
+#include "sph_kernels.cuh"
+
+using namespace sphb;
+
+struct sph_ctx {
+  sph_config cfg{};
+  Cfg kc{};
+  Dev d{};
+  Dev g{};                 // lazily allocated gravity-only state for sph_gravity
+  bool g_alloc = false;
+  cudaStream_t stream = nullptr;
+  uint32_t capacity = 0;
+  uint32_t n_eos = 0;
+  bool uploaded = false;
+  bool fresh = false;      // tree, neighbours, density, EOS and gravity are valid for the current positions
+  DevParams hp{};          // host copy of the host-owned fields
+  void* pinned_aos = nullptr;
+  cudaEvent_t rb_event = nullptr;
+  bool rb_inflight = false;
+  uint32_t rb_n = 0;
+  double* d_diag = nullptr;
+  std::string err;
+  int device = 0;
+  std::vector<void*> allocs;
+  // profiling
+  bool prof_on = false;
+  unsigned long long launches = 0;
+  struct Rec { int ph; cudaEvent_t a, b; };
+  std::vector<Rec> recs;
+  std::vector<cudaEvent_t> pool;
+  double prof_ms[SPH_PHASE_COUNT] = {0};
+  unsigned long long prof_calls[SPH_PHASE_COUNT] = {0};
+};
+
+namespace {
+
+sph_status cuda_fail(sph_ctx* c, cudaError_t e, const char* what) {
+  if (c) {
+    c->err = std::string(what) + ": " + cudaGetErrorString(e);
+  }
+  return e == cudaErrorMemoryAllocation ? SPH_ERR_OOM : SPH_ERR_CUDA;
+}
+#define CK(call)                                                       \
+  do {                                                                 \
+    cudaError_t _e = (call);                                           \
+    if (_e != cudaSuccess) return cuda_fail(ctx, _e, #call);           \
+  } while (0)
+
+template <typename T>
+sph_status dalloc(sph_ctx* ctx, T** p, size_t count) {
+  void* q = nullptr;
+  const size_t bytes = count * sizeof(T) > 0 ? count * sizeof(T) : 16;
+  cudaError_t e = cudaMalloc(&q, bytes);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMalloc");
+  ctx->allocs.push_back(q);
+  *p = static_cast<T*>(q);
+  return SPH_OK;
+}
+#define ALLOC(ptr, count)                                              \
+  do {                                                                 \
+    sph_status _s = dalloc(ctx, &(ptr), (count));                      \
+    if (_s != SPH_OK) return _s;                                       \
+  } while (0)
+
+sph_status alloc_dev(sph_ctx* ctx, Dev& d, uint32_t cap, uint32_t K, uint32_t nbr_cap, bool sph) {
+  d.cap = (int)cap;
+  d.K = (int)K;
+  const size_t capw = ((size_t)cap + 31) / 32 * 32;
+  const size_t Lmax = ((size_t)cap + K - 1) / K;
+  const size_t nodes = 2 * Lmax;
+  for (int b = 0; b < 2; ++b) {
+    State& s = d.st[b];
+    ALLOC(s.pos_h, capw);
+    ALLOC(s.vel_u, capw);
+    ALLOC(s.x, capw);
+    ALLOC(s.y, capw);
+    ALLOC(s.z, capw);
+    ALLOC(s.mass, capw);
+    ALLOC(s.mat, capw);
+    ALLOC(s.prov, capw);
+    ALLOC(s.id, capw);
+    ALLOC(d.keys[b], capw);
+    ALLOC(d.vals[b], capw);
+  }
+  ALLOC(d.body, capw);
+  d.rs_tiles_cap = (int)radix_tiles((int)cap);
+  ALLOC(d.rs_hist, 256 * (size_t)(d.rs_tiles_cap > 0 ? d.rs_tiles_cap : 1));
+  ALLOC(d.rs_tot, 256);
+  ALLOC(d.leaf_codes, Lmax);
+  ALLOC(d.left, Lmax);
+  ALLOC(d.right, Lmax);
+  ALLOC(d.parent, nodes);
+  ALLOC(d.counters, Lmax);
+  ALLOC(d.ncom, nodes);
+  ALLOC(d.nbmin, nodes);
+  ALLOC(d.nbmax, nodes);
+  ALLOC(d.nq0, nodes);
+  ALLOC(d.nq1, nodes);
+  ALLOC(d.grav, capw);
+  ALLOC(d.groups, Lmax);
+  ALLOC(d.ngroups, 1);
+  ALLOC(d.P, 1);
+  if (sph) {
+    d.nbr_cap = nbr_cap;
+    ALLOC(d.nbr, capw * nbr_cap);
+    ALLOC(d.nbr_cnt, capw);
+    ALLOC(d.rho, capw);
+    ALLOC(d.fdata, capw);
+    ALLOC(d.acc, capw);
+    ALLOC(d.hnew, capw);
+    ALLOC(d.h0, capw);
+    ALLOC(d.eos, kMaxMaterials);
+    d.diag_blocks = 148 * 2;
+    ALLOC(d.diag_part, (size_t)d.diag_blocks * 16);
+    uint8_t* aos = nullptr;
+    ALLOC(aos, capw * 48);
+    d.aos = aos;
+  }
+  return SPH_OK;
+}
+
+int bits_for(uint32_t n) {
+  int b = 1;
+  while (b < 32 && (1ull << b) < (unsigned long long)n) ++b;
+  return b;
+}
+
+cudaEvent_t pool_get(sph_ctx* ctx) {
+  if (!ctx->pool.empty()) {
+    cudaEvent_t e = ctx->pool.back();
+    ctx->pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+// Runs `f` (which returns the number of kernels it launched) as phase `ph`, bracketed by events when
+// profiling is on.
+template <typename F>
+void phase(sph_ctx* ctx, int ph, F&& f) {
+  cudaEvent_t a = nullptr, b = nullptr;
+  if (ctx->prof_on) {
+    a = pool_get(ctx);
+    b = pool_get(ctx);
+    cudaEventRecord(a, ctx->stream);
+  }
+  ctx->launches += (unsigned long long)f();
+  if (ctx->prof_on) {
+    cudaEventRecord(b, ctx->stream);
+    ctx->recs.push_back({ph, a, b});
+  }
+}
+
+// Push the host-owned DevParams fields (everything except the device-maintained reductions and counters).
+sph_status push_params(sph_ctx* ctx, Dev& d) {
+  DevParams& h = ctx->hp;
+  // copy [dt_fixed, ... sig_floor] contiguous block
+  const size_t off0 = offsetof(DevParams, dt_fixed);
+  const size_t off1 = offsetof(DevParams, time);
+  CK(cudaMemcpyAsync(reinterpret_cast<char*>(d.P) + off0, reinterpret_cast<char*>(&h) + off0, off1 - off0,
+                     cudaMemcpyHostToDevice, ctx->stream));
+  const size_t a0 = offsetof(DevParams, softening);
+  const size_t a1 = offsetof(DevParams, sig_min_bits);
+  CK(cudaMemcpyAsync(reinterpret_cast<char*>(d.P) + a0, reinterpret_cast<char*>(&h) + a0, a1 - a0,
+                     cudaMemcpyHostToDevice, ctx->stream));
+  return SPH_OK;
+}
+
+sph_status init_params(sph_ctx* ctx, Dev& d) {
+  DevParams p{};
+  p = ctx->hp;
+  p.dt = ctx->hp.dt_fixed;
+  p.time = 0.0;
+  p.sig_min_bits = 0x7f800000u;
+  for (int k = 0; k < 3; ++k) {
+    p.bbox_keys[k] = 0xffffffffu;
+    p.bbox_keys[3 + k] = 0u;
+  }
+  p.flags = 0;
+  p.max_nbr_seen = 0;
+  p.steps = 0;
+  CK(cudaMemcpyAsync(d.P, &p, sizeof(DevParams), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return SPH_OK;
+}
+
+// One tree build + everything that depends only on positions (and h): sort, LBVH, gravity, neighbour
+// lists, the smoothing-length solve, density and the EOS record.
+sph_status rebuild(sph_ctx* ctx, bool need_bbox) {
+  Dev& d = ctx->d;
+  cudaStream_t s = ctx->stream;
+  const Cfg& c = ctx->kc;
+  phase(ctx, SPH_PHASE_SORT, [&] { return (need_bbox ? launch_bbox(d, s) : 0) + launch_sort_permute(d, s); });
+  phase(ctx, SPH_PHASE_TREE, [&] { return launch_tree(d, c, ctx->cfg.theta, s); });
+  const bool fused = c.gravity == SPH_GRAVITY_TREE && c.mac == SPH_MAC_GROUP;
+  phase(ctx, SPH_PHASE_GRAVITY, [&] {
+    if (fused) return launch_walk(d, c, s);  // gravity + neighbour lists in one walk
+    if (c.gravity == SPH_GRAVITY_TREE) return launch_gravity_tree(d, c, s);
+    if (c.gravity == SPH_GRAVITY_DIRECT) return launch_gravity_direct(d, s);
+    cudaMemsetAsync(d.grav, 0, sizeof(float4) * (size_t)d.n, s);
+    return 0;
+  });
+  if (!fused) phase(ctx, SPH_PHASE_NEIGHBOURS, [&] { return launch_neighbours(d, c, s); });
+  if (c.h_solve) phase(ctx, SPH_PHASE_HSOLVE, [&] { return launch_h_solve(d, c, s); });
+  phase(ctx, SPH_PHASE_DENSITY, [&] { return launch_density_eos(d, c, s); });
+  CK(cudaGetLastError());
+  return SPH_OK;
+}
+
+void forces(sph_ctx* ctx) {
+  phase(ctx, SPH_PHASE_FORCES, [&] { return launch_forces(ctx->d, ctx->kc, ctx->stream); });
+}
+
+sph_status check_ready(sph_ctx* ctx) {
+  if (!ctx) return SPH_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  if (!ctx->uploaded || ctx->d.n == 0) {
+    ctx->err = "no particles uploaded";
+    return SPH_ERR_STATE;
+  }
+  return SPH_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* sph_status_string(sph_status s) {
+  switch (s) {
+    case SPH_OK: return "ok";
+    case SPH_CLAMPED: return "clamped to capacity";
+    case SPH_NOT_READY: return "not ready";
+    case SPH_ERR_INVALID: return "invalid argument";
+    case SPH_ERR_CUDA: return "CUDA error";
+    case SPH_ERR_OOM: return "out of device memory";
+    case SPH_ERR_TIMEOUT: return "timeout";
+    case SPH_ERR_OVERFLOW: return "device capacity overflow";
+    case SPH_ERR_STATE: return "call out of order";
+  }
+  return "unknown status";
+}
+
+sph_status sph_config_default(sph_config* cfg) {
+  if (!cfg) return SPH_ERR_INVALID;
+  std::memset(cfg, 0, sizeof(*cfg));
+  cfg->G = 6.674e-11;          // sph_step.wgsl:21
+  cfg->theta = 0.5f;           // gpu_gravity.rs:55
+  cfg->leaf_size = 1;          // gpu_gravity.rs:61
+  cfg->kernel = SPH_KERNEL_CUBIC;
+  cfg->gravity = SPH_GRAVITY_TREE;
+  cfg->multipole = SPH_MULTIPOLE_MONOPOLE;
+  cfg->precision = SPH_PRECISION_F32;
+  cfg->h_mode = SPH_H_FIXED;
+  cfg->h_neighbours = 64.0f;
+  cfg->h_tol = 1.0e-3f;
+  cfg->h_iters = 3;
+  cfg->max_neighbours = 256;   // the offline driver's deep buckets (tools/impact-run/src/main.rs:77)
+  cfg->cfl = 0.0f;
+  cfg->rho_floor = 1.0e-9f;
+  cfg->du_floor = 1.0f;
+  cfg->r_min = 1.0e-9f;
+  cfg->sig_floor = 1.0f;
+  cfg->device = -1;
+  return SPH_OK;
+}
+
+sph_status sph_create(const sph_config* cfg, uint32_t capacity, sph_ctx** out) {
+  if (!cfg || !out) return SPH_ERR_INVALID;
+  *out = nullptr;
+  if (cfg->leaf_size < 1 || cfg->leaf_size > 32 || !(cfg->theta > 0.0f) || cfg->kernel > 1 || cfg->gravity > 2 ||
+      cfg->multipole > 1 || cfg->precision > 1 || cfg->h_mode > 1 || cfg->max_neighbours < 1 ||
+      cfg->max_neighbours > 4096 || capacity > (1u << 26) || cfg->mac > 1 ||
+      (cfg->mac == SPH_MAC_GROUP && (cfg->leaf_size & (cfg->leaf_size - 1)) != 0))
+    return SPH_ERR_INVALID;
+  sph_ctx* ctx = new (std::nothrow) sph_ctx();
+  if (!ctx) return SPH_ERR_OOM;
+  ctx->cfg = *cfg;
+  ctx->capacity = capacity < 1 ? 1 : capacity;  // GpuSph::new: capacity.max(1)
+  ctx->kc.kernel = (int)cfg->kernel;
+  ctx->kc.gravity = (int)cfg->gravity;
+  ctx->kc.quad = cfg->multipole == SPH_MULTIPOLE_QUADRUPOLE;
+  ctx->kc.hilo = cfg->precision == SPH_PRECISION_HILO;
+  ctx->kc.h_solve = cfg->h_mode == SPH_H_SOLVE;
+  ctx->kc.h_eta = std::cbrt(3.0f * cfg->h_neighbours / (4.0f * 3.14159265358979f));
+  ctx->kc.h_tol = cfg->h_tol;
+  ctx->kc.h_iters = (int)cfg->h_iters;
+  ctx->kc.skin = ctx->kc.h_solve ? 0.15f : 0.0f;
+  ctx->kc.mac = (int)cfg->mac;
+  if (cfg->device >= 0) {
+    cudaError_t de = cudaSetDevice(cfg->device);
+    if (de != cudaSuccess) {
+      delete ctx;
+      return SPH_ERR_INVALID;
+    }
+  }
+  cudaGetDevice(&ctx->device);
+  cudaError_t e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    sph_status st = cuda_fail(ctx, e, "cudaStreamCreate");
+    delete ctx;
+    return st;
+  }
+  sph_status st = alloc_dev(ctx, ctx->d, ctx->capacity, cfg->leaf_size, cfg->max_neighbours, true);
+  if (st == SPH_OK) {
+    e = cudaMallocHost(&ctx->pinned_aos, (size_t)ctx->capacity * 48);
+    if (e != cudaSuccess) st = cuda_fail(ctx, e, "cudaMallocHost");
+  }
+  if (st == SPH_OK) {
+    e = cudaEventCreateWithFlags(&ctx->rb_event, cudaEventDisableTiming);
+    if (e != cudaSuccess) st = cuda_fail(ctx, e, "cudaEventCreate");
+  }
+  if (st == SPH_OK) st = dalloc(ctx, &ctx->d_diag, 16);
+  if (st == SPH_OK) {
+    DevParams& p = ctx->hp;
+    std::memset(&p, 0, sizeof(p));
+    p.dt_fixed = 0.0;
+    p.av_alpha = 1.0f;  // gpu_sph.rs:833 SphParams defaults
+    p.av_beta = 2.0f;
+    p.damp = 1.0f;
+    p.omega = 0.0f;
+    p.G = (float)cfg->G;
+    p.theta = cfg->theta;
+    p.cfl = cfg->cfl;
+    p.rho_floor = cfg->rho_floor;
+    p.du_floor = cfg->du_floor;
+    p.r_min = cfg->r_min;
+    p.sig_floor = cfg->sig_floor;
+    st = init_params(ctx, ctx->d);
+  }
+  if (st != SPH_OK) {
+    sph_destroy(ctx);
+    return st;
+  }
+  *out = ctx;
+  return SPH_OK;
+}
+
+void sph_destroy(sph_ctx* ctx) {
+  if (!ctx) return;
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  for (auto& r : ctx->recs) {
+    cudaEventDestroy(r.a);
+    cudaEventDestroy(r.b);
+  }
+  for (cudaEvent_t e : ctx->pool) cudaEventDestroy(e);
+  for (void* p : ctx->allocs) cudaFree(p);
+  if (ctx->pinned_aos) cudaFreeHost(ctx->pinned_aos);
+  if (ctx->rb_event) cudaEventDestroy(ctx->rb_event);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+sph_status sph_upload(sph_ctx* ctx, const SphParticle48* particles, uint32_t n, const SphEos48* eos, uint32_t n_eos,
+                      float softening) {
+  if (!ctx || (!particles && n) || (!eos && n_eos)) return SPH_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  sph_status ret = SPH_OK;
+  uint32_t nu = n;
+  if (nu > ctx->capacity) {
+    nu = ctx->capacity;
+    ret = SPH_CLAMPED;
+  }
+  uint32_t ne = n_eos;
+  if (ne > (uint32_t)kMaxMaterials) {
+    ne = kMaxMaterials;
+    ret = SPH_CLAMPED;
+  }
+  if (!std::isfinite(softening) || softening < 0.0f) return SPH_ERR_INVALID;
+  for (uint32_t i = 0; i < nu; ++i) {
+    const SphParticle48& p = particles[i];
+    if (p.mat >= ne || !std::isfinite(p.pos[0]) || !std::isfinite(p.pos[1]) || !std::isfinite(p.pos[2]) ||
+        !std::isfinite(p.vel[0]) || !std::isfinite(p.vel[1]) || !std::isfinite(p.vel[2]) || !std::isfinite(p.u) ||
+        !std::isfinite(p.mass) || !(p.h > 0.0f) || !std::isfinite(p.h) || p.mass < 0.0f) {
+      ctx->err = "particle " + std::to_string(i) + " has a material outside the table or a non-finite field";
+      return SPH_ERR_INVALID;
+    }
+  }
+  CK(cudaStreamSynchronize(ctx->stream));
+  Dev& d = ctx->d;
+  d.n = (int)nu;
+  d.cur = 0;
+  d.L = nu > 0 ? (int)((nu + d.K - 1) / d.K) : 0;
+  d.idbits = bits_for(nu);
+  ctx->n_eos = ne;
+  if (nu) CK(cudaMemcpyAsync(d.aos, particles, (size_t)nu * 48, cudaMemcpyHostToDevice, ctx->stream));
+  Eos table[kMaxMaterials];
+  std::memset(table, 0, sizeof(table));
+  if (ne) std::memcpy(table, eos, (size_t)ne * sizeof(Eos));
+  CK(cudaMemcpyAsync(d.eos, table, sizeof(table), cudaMemcpyHostToDevice, ctx->stream));
+  ctx->hp.softening = softening;
+  ctx->hp.soft2 = softening * softening;
+  sph_status st = push_params(ctx, d);
+  if (st != SPH_OK) return st;
+  if (nu) launch_from_aos(d, ctx->stream);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(ctx->stream));
+  ctx->uploaded = true;
+  ctx->fresh = false;
+  return ret;
+}
+
+sph_status sph_set_dt(sph_ctx* ctx, double dt, float damp) {
+  if (!ctx || !std::isfinite(dt) || dt < 0.0 || !std::isfinite(damp)) return SPH_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  ctx->hp.dt_fixed = dt;
+  ctx->hp.damp = damp;
+  return push_params(ctx, ctx->d);
+}
+
+sph_status sph_set_av(sph_ctx* ctx, float alpha, float beta) {
+  if (!ctx || !std::isfinite(alpha) || !std::isfinite(beta)) return SPH_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  ctx->hp.av_alpha = alpha;
+  ctx->hp.av_beta = beta;
+  return push_params(ctx, ctx->d);
+}
+
+sph_status sph_set_omega(sph_ctx* ctx, float omega) {
+  if (!ctx || !std::isfinite(omega)) return SPH_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  ctx->hp.omega = omega;
+  return push_params(ctx, ctx->d);
+}
+
+sph_status sph_eval_forces(sph_ctx* ctx) {
+  sph_status st = check_ready(ctx);
+  if (st != SPH_OK) return st;
+  st = rebuild(ctx, true);
+  if (st != SPH_OK) return st;
+  forces(ctx);
+  CK(cudaGetLastError());
+  ctx->fresh = true;
+  return SPH_OK;
+}
+
+sph_status sph_step_kdk(sph_ctx* ctx, uint32_t substeps) {
+  sph_status st = check_ready(ctx);
+  if (st != SPH_OK) return st;
+  Dev& d = ctx->d;
+  cudaStream_t s = ctx->stream;
+  for (uint32_t k = 0; k < substeps; ++k) {
+    // eval 1 at x_n (the tree, gravity and density of the previous eval 2 are still exact: a kick moves no
+    // particle), then dt, the half-kick + drift, eval 2 at x_{n+1}, the final half-kick.
+    if (!ctx->fresh) {
+      st = rebuild(ctx, true);
+      if (st != SPH_OK) return st;
+    }
+    forces(ctx);
+    phase(ctx, SPH_PHASE_INTEGRATE, [&] { return launch_finalize_dt(d, s) + launch_kick_drift(d, s); });
+    st = rebuild(ctx, false);
+    if (st != SPH_OK) return st;
+    forces(ctx);
+    phase(ctx, SPH_PHASE_INTEGRATE, [&] { return launch_kick(d, s); });
+    ctx->fresh = true;
+  }
+  CK(cudaGetLastError());
+  return SPH_OK;
+}
+
+sph_status sph_step_relax(sph_ctx* ctx, uint32_t steps) {
+  sph_status st = check_ready(ctx);
+  if (st != SPH_OK) return st;
+  for (uint32_t k = 0; k < steps; ++k) {
+    st = rebuild(ctx, true);
+    if (st != SPH_OK) return st;
+    forces(ctx);
+    phase(ctx, SPH_PHASE_INTEGRATE, [&] { return launch_relax(ctx->d, ctx->stream); });
+    ctx->fresh = false;
+  }
+  CK(cudaGetLastError());
+  return SPH_OK;
+}
+
+sph_status sph_readback_begin(sph_ctx* ctx) {
+  if (!ctx) return SPH_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  if (ctx->rb_inflight || ctx->d.n == 0) return SPH_OK;  // gpu_store.rs: no-op if empty or in flight
+  launch_to_aos(ctx->d, ctx->stream);
+  CK(cudaMemcpyAsync(ctx->pinned_aos, ctx->d.aos, (size_t)ctx->d.n * 48, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaEventRecord(ctx->rb_event, ctx->stream));
+  ctx->rb_inflight = true;
+  ctx->rb_n = (uint32_t)ctx->d.n;
+  return SPH_OK;
+}
+
+sph_status sph_readback_take(sph_ctx* ctx, SphParticle48* out, uint32_t cap, uint32_t* n_out, int* ready) {
+  if (!ctx || !out || !n_out || !ready) return SPH_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  *ready = 0;
+  *n_out = 0;
+  if (!ctx->rb_inflight) return SPH_NOT_READY;
+  cudaError_t e = cudaEventQuery(ctx->rb_event);
+  if (e == cudaErrorNotReady) return SPH_NOT_READY;
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaEventQuery");
+  const uint32_t m = ctx->rb_n < cap ? ctx->rb_n : cap;
+  std::memcpy(out, ctx->pinned_aos, (size_t)m * 48);
+  *n_out = m;
+  *ready = 1;
+  ctx->rb_inflight = false;
+  return m < ctx->rb_n ? SPH_CLAMPED : SPH_OK;
+}
+
+sph_status sph_sync(sph_ctx* ctx, uint32_t timeout_ms) {
+  if (!ctx) return SPH_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  if (timeout_ms == 0) {
+    CK(cudaStreamSynchronize(ctx->stream));
+    return SPH_OK;
+  }
+  const auto t0 = std::chrono::steady_clock::now();
+  for (;;) {
+    cudaError_t e = cudaStreamQuery(ctx->stream);
+    if (e == cudaSuccess) return SPH_OK;
+    if (e != cudaErrorNotReady) return cuda_fail(ctx, e, "cudaStreamQuery");
+    if (std::chrono::steady_clock::now() - t0 > std::chrono::milliseconds(timeout_ms)) {
+      ctx->err = "sph_sync timed out";
+      return SPH_ERR_TIMEOUT;
+    }
+    std::this_thread::sleep_for(std::chrono::microseconds(50));
+  }
+}
+
+uint32_t sph_count(const sph_ctx* ctx) { return ctx ? (uint32_t)ctx->d.n : 0u; }
+
+sph_status sph_particle_buffer(sph_ctx* ctx, void** device_ptr) {
+  if (!ctx || !device_ptr) return SPH_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  if (ctx->d.n) launch_to_aos(ctx->d, ctx->stream);
+  CK(cudaGetLastError());
+  *device_ptr = ctx->d.aos;
+  return SPH_OK;
+}
+
+void* sph_stream(sph_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+const char* sph_last_error(const sph_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+sph_status sph_diag(sph_ctx* ctx, sph_diag_out* out) {
+  if (!ctx || !out) return SPH_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  std::memset(out, 0, sizeof(*out));
+  if (ctx->d.n) launch_diag(ctx->d, ctx->stream, ctx->d_diag);
+  double v[16] = {0};
+  DevParams p;
+  if (ctx->d.n) CK(cudaMemcpyAsync(v, ctx->d_diag, sizeof(v), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaMemcpyAsync(&p, ctx->d.P, sizeof(p), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  out->mass = v[0];
+  out->kinetic = v[1];
+  out->internal = v[2];
+  out->potential = v[3];
+  for (int k = 0; k < 3; ++k) {
+    out->momentum[k] = v[4 + k];
+    out->angular_momentum[k] = v[7 + k];
+  }
+  out->dt = p.dt;
+  out->time = p.time;
+  out->steps = p.steps;
+  out->max_neighbours_seen = p.max_nbr_seen;
+  out->overflow_flags = p.flags;
+  out->h_iterations = p.h_iters_used;
+  out->h_residual = p.h_residual;
+  out->walk_nodes = p.stat_visits;
+  out->walk_pops = p.stat_pops;
+  out->m2p_interactions = p.stat_m2p;
+  out->p2p_interactions = p.stat_p2p;
+  if (p.flags & (kFlagNbrOverflow | kFlagStackOverflow)) {
+    ctx->err = "device capacity overflow (flags " + std::to_string(p.flags) + ")";
+    return SPH_ERR_OVERFLOW;
+  }
+  return SPH_OK;
+}
+
+sph_status sph_inspect(sph_ctx* ctx, uint32_t what, void* host_out, size_t bytes) {
+  if (!ctx || !host_out) return SPH_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  CK(cudaStreamSynchronize(ctx->stream));
+  Dev& d = ctx->d;
+  const size_t n = (size_t)d.n, L = (size_t)d.L;
+  const size_t nn = L ? 2 * L - 1 : 0;
+  auto need = [&](size_t b) { return bytes >= b; };
+  std::vector<unsigned> ids;
+  auto load_ids = [&]() -> sph_status {
+    ids.resize(n);
+    CK(cudaMemcpy(ids.data(), d.s().id, n * 4, cudaMemcpyDeviceToHost));
+    return SPH_OK;
+  };
+  auto scatter = [&](const void* dev, size_t elem) -> sph_status {
+    if (!need(n * elem)) return SPH_ERR_INVALID;
+    std::vector<char> tmp(n * elem);
+    CK(cudaMemcpy(tmp.data(), dev, n * elem, cudaMemcpyDeviceToHost));
+    sph_status st = load_ids();
+    if (st != SPH_OK) return st;
+    for (size_t t = 0; t < n; ++t) std::memcpy((char*)host_out + ids[t] * elem, tmp.data() + t * elem, elem);
+    return SPH_OK;
+  };
+  switch (what) {
+    case SPH_Q_BBOX: {
+      if (!need(24)) return SPH_ERR_INVALID;
+      DevParams p;
+      CK(cudaMemcpy(&p, d.P, sizeof(p), cudaMemcpyDeviceToHost));
+      float* f = (float*)host_out;
+      for (int k = 0; k < 6; ++k) {
+        const unsigned key = p.bbox_keys[k];
+        unsigned bits = (key >> 31) ? (key ^ 0x80000000u) : ~key;
+        std::memcpy(&f[k], &bits, 4);
+      }
+      return SPH_OK;
+    }
+    case SPH_Q_CODES: {
+      if (!need(n * 4)) return SPH_ERR_INVALID;
+      std::vector<unsigned long long> k(n);
+      CK(cudaMemcpy(k.data(), d.keys[0], n * 8, cudaMemcpyDeviceToHost));
+      for (size_t t = 0; t < n; ++t) ((unsigned*)host_out)[t] = (unsigned)(k[t] >> d.idbits);
+      return SPH_OK;
+    }
+    case SPH_Q_ORDER:
+      if (!need(n * 4)) return SPH_ERR_INVALID;
+      CK(cudaMemcpy(host_out, d.s().id, n * 4, cudaMemcpyDeviceToHost));
+      return SPH_OK;
+    case SPH_Q_LEFT:
+    case SPH_Q_RIGHT:
+      if (!need((L ? L - 1 : 0) * 4)) return SPH_ERR_INVALID;
+      if (L > 1) CK(cudaMemcpy(host_out, what == SPH_Q_LEFT ? d.left : d.right, (L - 1) * 4, cudaMemcpyDeviceToHost));
+      return SPH_OK;
+    case SPH_Q_PARENT:
+      if (!need(nn * 4)) return SPH_ERR_INVALID;
+      CK(cudaMemcpy(host_out, d.parent, nn * 4, cudaMemcpyDeviceToHost));
+      return SPH_OK;
+    case SPH_Q_NODE_COM:
+    case SPH_Q_NODE_BMIN:
+    case SPH_Q_NODE_BMAX: {
+      if (!need(nn * 16)) return SPH_ERR_INVALID;
+      const float4* src = what == SPH_Q_NODE_COM ? d.ncom : (what == SPH_Q_NODE_BMIN ? d.nbmin : d.nbmax);
+      CK(cudaMemcpy(host_out, src, nn * 16, cudaMemcpyDeviceToHost));
+      return SPH_OK;
+    }
+    case SPH_Q_NBR_COUNT:
+      return scatter(d.nbr_cnt, 4);
+    case SPH_Q_NBR_LIST: {
+      const size_t cap = d.nbr_cap;
+      if (!need(n * cap * 4)) return SPH_ERR_INVALID;
+      const size_t groups = (n + 31) / 32;
+      std::vector<unsigned> lst(groups * cap * 32), cnt(n);
+      CK(cudaMemcpy(lst.data(), d.nbr, lst.size() * 4, cudaMemcpyDeviceToHost));
+      CK(cudaMemcpy(cnt.data(), d.nbr_cnt, n * 4, cudaMemcpyDeviceToHost));
+      sph_status st = load_ids();
+      if (st != SPH_OK) return st;
+      unsigned* o = (unsigned*)host_out;
+      std::memset(o, 0xff, n * cap * 4);
+      for (size_t t = 0; t < n; ++t) {
+        const size_t c = cnt[t] < cap ? cnt[t] : cap;
+        for (size_t k = 0; k < c; ++k) o[ids[t] * cap + k] = ids[lst[((t >> 5) * cap + k) * 32 + (t & 31)]];
+      }
+      return SPH_OK;
+    }
+    case SPH_Q_RHO:
+      return scatter(d.rho, 4);
+    case SPH_Q_PRESSURE:
+    case SPH_Q_SOUND: {
+      if (!need(n * 4)) return SPH_ERR_INVALID;
+      std::vector<float4> f(n);
+      CK(cudaMemcpy(f.data(), d.fdata, n * 16, cudaMemcpyDeviceToHost));
+      sph_status st = load_ids();
+      if (st != SPH_OK) return st;
+      for (size_t t = 0; t < n; ++t) {
+        const float v = what == SPH_Q_PRESSURE ? f[t].z * (f[t].y * f[t].y) : f[t].w;
+        ((float*)host_out)[ids[t]] = v;
+      }
+      return SPH_OK;
+    }
+    case SPH_Q_ACC_SPH: {
+      // total acceleration minus gravity = the SPH part
+      if (!need(n * 16)) return SPH_ERR_INVALID;
+      std::vector<float4> a(n), g(n);
+      CK(cudaMemcpy(a.data(), d.acc, n * 16, cudaMemcpyDeviceToHost));
+      CK(cudaMemcpy(g.data(), d.grav, n * 16, cudaMemcpyDeviceToHost));
+      sph_status st = load_ids();
+      if (st != SPH_OK) return st;
+      const bool sub = ctx->kc.gravity != SPH_GRAVITY_NONE;
+      for (size_t t = 0; t < n; ++t) {
+        float4 v = a[t];
+        if (sub) {
+          v.x -= g[t].x;
+          v.y -= g[t].y;
+          v.z -= g[t].z;
+        }
+        ((float4*)host_out)[ids[t]] = v;
+      }
+      return SPH_OK;
+    }
+    case SPH_Q_ACC_GRAV:
+      return scatter(d.grav, 16);
+    case SPH_Q_H: {
+      if (!need(n * 4)) return SPH_ERR_INVALID;
+      std::vector<float4> p(n);
+      CK(cudaMemcpy(p.data(), d.s().pos_h, n * 16, cudaMemcpyDeviceToHost));
+      sph_status st = load_ids();
+      if (st != SPH_OK) return st;
+      for (size_t t = 0; t < n; ++t) ((float*)host_out)[ids[t]] = p[t].w;
+      return SPH_OK;
+    }
+    case SPH_Q_N_LEAVES:
+      if (!need(4)) return SPH_ERR_INVALID;
+      *(unsigned*)host_out = (unsigned)L;
+      return SPH_OK;
+  }
+  return SPH_ERR_INVALID;
+}
+
+sph_status sph_profile_enable(sph_ctx* ctx, int on) {
+  if (!ctx) return SPH_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  CK(cudaStreamSynchronize(ctx->stream));
+  for (auto& r : ctx->recs) {
+    ctx->pool.push_back(r.a);
+    ctx->pool.push_back(r.b);
+  }
+  ctx->recs.clear();
+  for (int k = 0; k < SPH_PHASE_COUNT; ++k) {
+    ctx->prof_ms[k] = 0.0;
+    ctx->prof_calls[k] = 0;
+  }
+  ctx->launches = 0;
+  ctx->prof_on = on != 0;
+  return SPH_OK;
+}
+
+sph_status sph_profile_read(sph_ctx* ctx, sph_profile* out) {
+  if (!ctx || !out) return SPH_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  CK(cudaStreamSynchronize(ctx->stream));
+  for (auto& r : ctx->recs) {
+    float ms = 0.0f;
+    CK(cudaEventElapsedTime(&ms, r.a, r.b));
+    ctx->prof_ms[r.ph] += ms;
+    ctx->prof_calls[r.ph] += 1;
+    ctx->pool.push_back(r.a);
+    ctx->pool.push_back(r.b);
+  }
+  ctx->recs.clear();
+  for (int k = 0; k < SPH_PHASE_COUNT; ++k) {
+    out->ms[k] = ctx->prof_ms[k];
+    out->calls[k] = ctx->prof_calls[k];
+  }
+  out->kernel_launches = ctx->launches;
+  return SPH_OK;
+}
+
+sph_status sph_gravity(sph_ctx* ctx, const double* pos3, const double* mass, uint32_t n, double softening,
+                       uint32_t gravity_mode, double* acc3) {
+  if (!ctx || (!pos3 && n) || (!mass && n) || (!acc3 && n) || gravity_mode > 1) return SPH_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  if (n > ctx->capacity) {
+    ctx->err = "sph_gravity: more points than the context capacity";
+    return SPH_ERR_INVALID;
+  }
+  if (n == 0) return SPH_OK;
+  if (!ctx->g_alloc) {
+    sph_status st = alloc_dev(ctx, ctx->g, ctx->capacity, ctx->cfg.leaf_size, 0, false);
+    if (st != SPH_OK) return st;
+    ctx->g_alloc = true;
+  }
+  Dev& g = ctx->g;
+  g.n = (int)n;
+  g.cur = 0;
+  g.L = (int)((n + g.K - 1) / g.K);
+  g.idbits = bits_for(n);
+  std::vector<float4> ph(n);
+  std::vector<double> xs(n), ys(n), zs(n);
+  std::vector<float> ms(n);
+  std::vector<unsigned> ids(n);
+  for (uint32_t i = 0; i < n; ++i) {
+    ph[i] = make_float4((float)pos3[3 * i], (float)pos3[3 * i + 1], (float)pos3[3 * i + 2], 0.0f);
+    xs[i] = pos3[3 * i];
+    ys[i] = pos3[3 * i + 1];
+    zs[i] = pos3[3 * i + 2];
+    ms[i] = (float)mass[i];
+    ids[i] = i;
+  }
+  cudaStream_t s = ctx->stream;
+  const State& st0 = g.st[0];
+  CK(cudaMemcpyAsync(st0.pos_h, ph.data(), n * 16, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(st0.x, xs.data(), n * 8, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(st0.y, ys.data(), n * 8, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(st0.z, zs.data(), n * 8, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(st0.mass, ms.data(), n * 4, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(st0.id, ids.data(), n * 4, cudaMemcpyHostToDevice, s));
+  CK(cudaMemsetAsync(st0.vel_u, 0, n * 16, s));
+  CK(cudaMemsetAsync(st0.mat, 0, n * 4, s));
+  CK(cudaMemsetAsync(st0.prov, 0, n * 4, s));
+  DevParams p = ctx->hp;
+  p.softening = (float)softening;
+  p.soft2 = (float)softening * (float)softening;
+  CK(cudaMemcpyAsync(g.P, &p, sizeof(p), cudaMemcpyHostToDevice, s));
+  launch_bbox(g, s);
+  launch_sort_permute(g, s);
+  if (gravity_mode == SPH_GRAVITY_TREE) {
+    launch_tree(g, ctx->kc, ctx->cfg.theta, s);
+    if (ctx->kc.mac == SPH_MAC_GROUP) launch_gravity_group(g, ctx->kc, s);
+    else launch_gravity_tree(g, ctx->kc, s);
+  } else {
+    launch_gravity_direct(g, s);
+  }
+  CK(cudaGetLastError());
+  std::vector<float4> acc(n);
+  std::vector<unsigned> sid(n);
+  CK(cudaMemcpyAsync(acc.data(), g.grav, n * 16, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(sid.data(), g.s().id, n * 4, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  for (uint32_t t = 0; t < n; ++t) {
+    acc3[3 * sid[t]] = acc[t].x;
+    acc3[3 * sid[t] + 1] = acc[t].y;
+    acc3[3 * sid[t] + 2] = acc[t].z;
+  }
+  return SPH_OK;
+}
+
+sph_status sph_gravity_direct64(sph_ctx* ctx, const double* pos3, const double* mass, uint32_t n,
+                                const uint32_t* targets, uint32_t n_targets, double softening, double* acc3) {
+  if (!ctx || !pos3 || !mass || !acc3 || n == 0) return SPH_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  const uint32_t nt = targets ? n_targets : n;
+  if (targets)
+    for (uint32_t q = 0; q < nt; ++q)
+      if (targets[q] >= n) return SPH_ERR_INVALID;
+  double *dp = nullptr, *dm = nullptr, *da = nullptr;
+  unsigned* dt = nullptr;
+  cudaStream_t s = ctx->stream;
+  cudaError_t e = cudaMallocAsync(&dp, (size_t)n * 24, s);
+  if (e == cudaSuccess) e = cudaMallocAsync(&dm, (size_t)n * 8, s);
+  if (e == cudaSuccess) e = cudaMallocAsync(&da, (size_t)nt * 24, s);
+  if (e == cudaSuccess && targets) e = cudaMallocAsync(&dt, (size_t)nt * 4, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dp, pos3, (size_t)n * 24, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dm, mass, (size_t)n * 8, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess && targets) e = cudaMemcpyAsync(dt, targets, (size_t)nt * 4, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) {
+    launch_gravity_direct64(dp, dm, (int)n, dt, (int)nt, softening * softening, ctx->cfg.G, da, s);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(acc3, da, (size_t)nt * 24, cudaMemcpyDeviceToHost, s);
+  if (dp) cudaFreeAsync(dp, s);
+  if (dm) cudaFreeAsync(dm, s);
+  if (da) cudaFreeAsync(da, s);
+  if (dt) cudaFreeAsync(dt, s);
+  cudaError_t e2 = cudaStreamSynchronize(s);
+  if (e == cudaSuccess) e = e2;
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "sph_gravity_direct64");
+  return SPH_OK;
+}
+
+}  // extern "C"

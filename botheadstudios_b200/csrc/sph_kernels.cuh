@@ -1,0 +1,108 @@
+// Internal device layout and host-side launchers of the SPH step kernels (not part of the C ABI).
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "sph_common.cuh"
+
+namespace sphb {
+
+// Particle state, structure-of-arrays, kept in Morton (LBVH leaf) order between force evaluations.
+// `id` is the particle's original index (its slot in the 48-byte exchange array).
+struct State {
+  float4* pos_h = nullptr;  // x, y, z (f32 copy of the f64 master), h
+  float4* vel_u = nullptr;  // vx, vy, vz, u
+  double* x = nullptr;      // f64 master positions
+  double* y = nullptr;
+  double* z = nullptr;
+  float* mass = nullptr;
+  unsigned* mat = nullptr;
+  unsigned* prov = nullptr;
+  unsigned* id = nullptr;
+};
+
+struct Dev {
+  int n = 0, cap = 0;
+  int K = 1;        // leaf size
+  int L = 0;        // number of leaves
+  int idbits = 1;   // bits of the particle index in the 64-bit sort key
+  State st[2];
+  int cur = 0;
+  float4* body = nullptr;  // x, y, z, m in sorted order (gravity sources)
+  unsigned long long* keys[2] = {nullptr, nullptr};
+  unsigned* vals[2] = {nullptr, nullptr};
+  unsigned* rs_hist = nullptr;  // [256][tiles]
+  unsigned* rs_tot = nullptr;   // [256]
+  int rs_tiles_cap = 0;
+  unsigned* leaf_codes = nullptr;
+  unsigned* left = nullptr;     // [L-1]
+  unsigned* right = nullptr;    // [L-1]
+  unsigned* parent = nullptr;   // [2L-1]
+  unsigned* counters = nullptr; // [L-1] climb arrival counters
+  float4* ncom = nullptr;       // [2L-1] com.xyz, mass
+  float4* nbmin = nullptr;      // [2L-1] bmin.xyz, max h
+  float4* nbmax = nullptr;      // [2L-1] bmax.xyz, opening radius
+  float4* nq0 = nullptr;        // [2L-1] Qxx, Qyy, Qzz, Qxy
+  float4* nq1 = nullptr;        // [2L-1] Qxz, Qyz, 0, 0
+  uint2* groups = nullptr;      // [L] walk groups: (first leaf, last leaf) of maximal subtrees with <= 32 particles
+  unsigned* ngroups = nullptr;  // [1] number of groups
+  unsigned* nbr = nullptr;      // interleaved neighbour lists [n/32][nbr_cap][32]
+  unsigned* nbr_cnt = nullptr;  // [n]
+  unsigned nbr_cap = 0;
+  float* rho = nullptr;         // [n]
+  float4* fdata = nullptr;      // [n] mass, rho, P/rho², c
+  float4* grav = nullptr;       // [n] gravity acc.xyz, potential
+  float4* acc = nullptr;        // [n] total acc.xyz, du/dt
+  float* hnew = nullptr;        // [n] smoothing-length solve scratch
+  float* h0 = nullptr;          // [n] smoothing length when the neighbour list was built
+  Eos* eos = nullptr;           // [16]
+  DevParams* P = nullptr;
+  double* diag_part = nullptr;  // [blocks][16]
+  int diag_blocks = 0;
+  void* aos = nullptr;          // [cap] 48-byte exchange buffer (original order)
+  const State& s() const { return st[cur]; }
+};
+
+struct Cfg {
+  int kernel = 0;       // 0 cubic, 1 Wendland C2
+  int gravity = 0;      // 0 tree, 1 direct, 2 none
+  int quad = 0;         // quadrupole moments
+  int hilo = 0;         // node-relative hi/lo + compensated sums
+  int h_solve = 0;
+  float h_eta = 0.0f;   // h = h_eta (m/ρ)^(1/3)
+  float h_tol = 1.0e-3f;
+  int h_iters = 4;
+  float skin = 0.0f;    // neighbour-list radius inflation (h-solve)
+  int mac = 0;          // 0 group walk, 1 per-particle reference walk
+};
+
+// ---- tree ------------------------------------------------------------------------------------------
+int launch_bbox_reset(const Dev& d, cudaStream_t s);
+int launch_bbox(const Dev& d, cudaStream_t s);
+int launch_sort_permute(Dev& d, cudaStream_t s);      // keys → radix sort → permute (swaps d.cur)
+int launch_tree(const Dev& d, const Cfg& c, float theta, cudaStream_t s);  // Karras + moments
+size_t radix_tiles(int n);
+
+// ---- gravity ---------------------------------------------------------------------------------------
+int launch_gravity_tree(const Dev& d, const Cfg& c, cudaStream_t s);
+int launch_gravity_direct(const Dev& d, cudaStream_t s);
+int launch_gravity_direct64(const double* pos3, const double* mass, int n, const unsigned* targets, int nt,
+                             double soft2, double G, double* acc3, cudaStream_t s);
+
+// ---- SPH -------------------------------------------------------------------------------------------
+int launch_neighbours(const Dev& d, const Cfg& c, cudaStream_t s);      // neighbour lists only
+int launch_walk(const Dev& d, const Cfg& c, cudaStream_t s);            // group-MAC gravity + neighbour lists
+int launch_gravity_group(const Dev& d, const Cfg& c, cudaStream_t s);   // group-MAC gravity only
+int launch_density_eos(const Dev& d, const Cfg& c, cudaStream_t s);
+int launch_h_solve(const Dev& d, const Cfg& c, cudaStream_t s);
+int launch_eos_only(const Dev& d, cudaStream_t s);
+int launch_forces(const Dev& d, const Cfg& c, cudaStream_t s);
+int launch_finalize_dt(const Dev& d, cudaStream_t s);
+int launch_kick_drift(const Dev& d, cudaStream_t s);
+int launch_kick(const Dev& d, cudaStream_t s);
+int launch_relax(const Dev& d, cudaStream_t s);
+int launch_from_aos(const Dev& d, cudaStream_t s);
+int launch_to_aos(const Dev& d, cudaStream_t s);
+int launch_diag(const Dev& d, cudaStream_t s, double* out16);
+
+}  // namespace sphb

@@ -1,0 +1,156 @@
+"""Seeded synthetic initial conditions for the giant-impact workloads.
+
+Bodies are differentiated: 30 % iron core / 70 % basalt mantle by mass, equal-mass particles, each region
+seeded on its own cubic lattice at the material's reference density (the reference's construction,
+``crates/engine/src/hydrostatic.rs:97-144`` ``new_differentiated``, uses equal-mass particles at the same
+densities on Fibonacci shells; a lattice is used here), with a uniform ±jitter·h displacement per axis.
+Smoothing lengths target a neighbour count inside the support radius h: (4π/3)(h/Δ)³ = N_ngb.
+Impacts: impactor mass ratio q, speed v_imp = f·v_esc at contact, impact angle from the contact normal,
+initial centre separation d0 (in target radii); the pair is placed on the straight-line approach that has
+that contact speed and impact parameter (energy and angular momentum of the two-body orbit), in the
+centre-of-mass frame. All values are in the unit system passed in (code units by default: G = M_t = R_t = 1).
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass
+
+import numpy as np
+
+from ._lib import PARTICLE_DTYPE
+from .materials import MAT_BASALT, MAT_IRON, TILLOTSON_SI, Units, code_units, eos_table
+
+
+def eta_for(n_ngb: float) -> float:
+    """h = eta·Δ such that (4π/3)(h/Δ)³ = n_ngb."""
+    return (3.0 * n_ngb / (4.0 * math.pi)) ** (1.0 / 3.0)
+
+
+def _lattice_ball(n: int, spacing: float, r_in: float, offset: float) -> np.ndarray:
+    """The n lattice points (spacing Δ, shifted by offset·Δ) closest to the origin outside radius r_in."""
+    r_out = (r_in ** 3 + n * spacing ** 3 * 3.0 / (4.0 * math.pi)) ** (1.0 / 3.0)
+    m = int(math.ceil(r_out * 1.08 / spacing)) + 2
+    while True:
+        ax = (np.arange(-m, m + 1, dtype=np.float64) + offset) * spacing
+        g = np.stack(np.meshgrid(ax, ax, ax, indexing="ij"), axis=-1).reshape(-1, 3)
+        r = np.sqrt((g * g).sum(1))
+        keep = r >= r_in
+        g, r = g[keep], r[keep]
+        if len(r) >= n:
+            break
+        m = int(m * 1.3) + 2
+    # deterministic: by radius, ties by lattice order (stable sort)
+    idx = np.argsort(r, kind="stable")[:n]
+    return g[idx]
+
+
+@dataclass
+class Body:
+    pos: np.ndarray
+    mass: np.ndarray
+    mat: np.ndarray
+    h: np.ndarray
+    radius: float
+    total_mass: float
+    spacing_min: float
+
+
+def differentiated_body(n: int, total_mass: float, units: Units, n_ngb: float, iron_frac: float = 0.3,
+                        jitter: float = 0.1, rng: np.random.Generator | None = None) -> Body:
+    rfe = TILLOTSON_SI["iron"][0] / units.density
+    rba = TILLOTSON_SI["basalt"][0] / units.density
+    m = total_mass / n
+    n_core = int(round(iron_frac * n))
+    n_mant = n - n_core
+    d_core = (m / rfe) ** (1.0 / 3.0)
+    d_mant = (m / rba) ** (1.0 / 3.0)
+    core = _lattice_ball(n_core, d_core, 0.0, 0.5) if n_core else np.zeros((0, 3))
+    r_core = float(np.sqrt((core * core).sum(1)).max()) + 0.5 * d_core if n_core else 0.0
+    mant = _lattice_ball(n_mant, d_mant, r_core, 0.25)
+    pos = np.concatenate([core, mant])
+    eta = eta_for(n_ngb)
+    h = np.concatenate([np.full(n_core, eta * d_core), np.full(n_mant, eta * d_mant)])
+    mat = np.concatenate([np.full(n_core, MAT_IRON, np.uint32), np.full(n_mant, MAT_BASALT, np.uint32)])
+    if jitter > 0.0:
+        rng = rng or np.random.default_rng(1)
+        pos = pos + rng.uniform(-jitter, jitter, size=pos.shape) * h[:, None]
+    radius = float(np.sqrt((pos * pos).sum(1)).max())
+    return Body(pos=pos, mass=np.full(n, m), mat=mat, h=h, radius=radius, total_mass=total_mass,
+                spacing_min=min(d_core, d_mant))
+
+
+@dataclass
+class Impact:
+    particles: np.ndarray  # PARTICLE_DTYPE
+    eos: np.ndarray        # [2, 12] float32
+    softening: float
+    units: Units
+    pos64: np.ndarray      # f64 positions (the exchange format holds f32)
+    n_target: int
+    n_impactor: int
+
+
+def impact(n_target: int, n_impactor: int, n_ngb: float = 48.0, mass_ratio: float = 0.1, v_factor: float = 1.1,
+           angle_deg: float = 45.0, separation: float = 3.0, seed: int = 1, jitter: float = 0.1,
+           u0_si: float = 1.0e6, units: Units | None = None) -> Impact:
+    """Two differentiated bodies on an oblique collision course (configs of the giant-impact benchmark)."""
+    units = units or code_units()
+    rng = np.random.default_rng(seed)
+    M_t = 1.0  # the target mass is the mass unit
+    if units.G != 1.0:
+        raise ValueError("impact() builds code-unit bodies (G = 1); pass code_units()")
+    tgt = differentiated_body(n_target, 1.0, units, n_ngb, jitter=jitter, rng=rng)
+    imp = differentiated_body(n_impactor, mass_ratio, units, n_ngb, jitter=jitter, rng=rng)
+    M_i = mass_ratio
+    R_sum = tgt.radius + imp.radius
+    mu = M_t + M_i
+    v_esc = math.sqrt(2.0 * mu / R_sum)
+    v_c = v_factor * v_esc
+    b_c = math.sin(math.radians(angle_deg)) * R_sum
+    d0 = separation * tgt.radius
+    v0 = math.sqrt(max(v_c * v_c - 2.0 * mu * (1.0 / R_sum - 1.0 / d0), 1e-12))
+    b0 = min(b_c * v_c / v0, 0.999 * d0)
+    rel_pos = np.array([math.sqrt(d0 * d0 - b0 * b0), b0, 0.0])
+    rel_vel = np.array([-v0, 0.0, 0.0])
+    # centre-of-mass frame
+    ft, fi = M_i / mu, M_t / mu
+    pos = np.concatenate([tgt.pos - ft * rel_pos, imp.pos + fi * rel_pos])
+    vel = np.concatenate([np.tile(-ft * rel_vel, (n_target, 1)), np.tile(fi * rel_vel, (n_impactor, 1))])
+    n = n_target + n_impactor
+    p = np.zeros(n, dtype=PARTICLE_DTYPE)
+    p["pos"] = pos.astype(np.float32)
+    p["h"] = np.concatenate([tgt.h, imp.h]).astype(np.float32)
+    p["vel"] = vel.astype(np.float32)
+    p["u"] = np.float32(u0_si / units.energy)
+    p["mass"] = np.concatenate([tgt.mass, imp.mass]).astype(np.float32)
+    p["mat"] = np.concatenate([tgt.mat, imp.mat])
+    rho0 = np.array([TILLOTSON_SI["basalt"][0], TILLOTSON_SI["iron"][0]]) / units.density
+    p["rho"] = rho0[p["mat"]].astype(np.float32)
+    p["prov"] = np.concatenate([np.zeros(n_target, np.uint32), np.ones(n_impactor, np.uint32)])
+    soft = 0.5 * min(tgt.spacing_min, imp.spacing_min)
+    return Impact(particles=p, eos=eos_table(units), softening=soft, units=units, pos64=pos, n_target=n_target,
+                  n_impactor=n_impactor)
+
+
+def planet(n: int, n_ngb: float = 64.0, seed: int = 3, jitter: float = 0.1, u0_si: float = 1.0e6,
+           units: Units | None = None) -> Impact:
+    """A single differentiated planet at rest (the equilibrium-planet precision workload)."""
+    units = units or code_units()
+    rng = np.random.default_rng(seed)
+    b = differentiated_body(n, 1.0, units, n_ngb, jitter=jitter, rng=rng)
+    p = np.zeros(n, dtype=PARTICLE_DTYPE)
+    p["pos"] = b.pos.astype(np.float32)
+    p["h"] = b.h.astype(np.float32)
+    p["u"] = np.float32(u0_si / units.energy)
+    p["mass"] = b.mass.astype(np.float32)
+    p["mat"] = b.mat
+    rho0 = np.array([TILLOTSON_SI["basalt"][0], TILLOTSON_SI["iron"][0]]) / units.density
+    p["rho"] = rho0[p["mat"]].astype(np.float32)
+    return Impact(particles=p, eos=eos_table(units), softening=0.5 * b.spacing_min, units=units, pos64=b.pos,
+                  n_target=n, n_impactor=0)
+
+
+def config_kwargs(units: Units) -> dict:
+    """The unit-dependent fields of sph_config for these initial conditions."""
+    return dict(G=units.G, rho_floor=units.rho_floor, du_floor=units.du_floor, r_min=units.r_min,
+                sig_floor=units.sig_floor)

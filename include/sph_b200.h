@@ -1,0 +1,221 @@
+/* sph_b200.h — C ABI of the B200-native SPH giant-impact step.
+ *
+ * A drop-in for the Integrity engine's GPU SPH path (sean-reid/BotheadStudios, project integrity-engine).
+ * The entry points replace the engine's `GpuSph` surface (crates/engine/src/gpu_sph.rs:742-922) and its
+ * gravity host (crates/engine/src/gpu_gravity.rs:181-230, 532-607). Every function is `extern "C"`, takes
+ * plain pointers and sizes, never throws and returns an sph_status. A context is owned by one thread at a
+ * time (the reference's GpuSph is single-owner); each context has its own CUDA stream.
+ *
+ * Units are the caller's: the reference runs in SI with G = 6.674e-11; the configuration carries G and the
+ * SI-valued guards of the reference shaders (density floor, sound-speed step floor, coincident-pair cut and
+ * signal-speed floor) so that G = 1 code units behave the same way.
+ */
+#ifndef SPH_B200_H
+#define SPH_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* The 48-byte particle exchange layout: gpu_sph.rs:25-37 `SphParticle` == sph_step.wgsl:38 `Particle`. */
+typedef struct SphParticle48 {
+  float pos[3];
+  float h;
+  float vel[3];
+  float u;
+  float mass;
+  uint32_t mat;
+  float rho;
+  uint32_t prov;
+} SphParticle48;
+
+/* The 48-byte material row: gpu_sph.rs:39-56 `SphEos` == sph_step.wgsl:43 `Eos` (Tillotson, SI). */
+typedef struct SphEos48 {
+  float rho0, a, b, cap_a;
+  float cap_b, e0, e_iv, e_cv;
+  float alpha, beta, _p0, _p1;
+} SphEos48;
+
+/* Status codes. No exception or abort crosses this boundary. */
+typedef enum sph_status {
+  SPH_OK = 0,
+  SPH_CLAMPED = 1,          /* upload held more particles/materials than capacity: the excess was dropped */
+  SPH_ERR_INVALID = -1,     /* bad argument (null pointer, size, material index, NaN input) */
+  SPH_ERR_CUDA = -2,        /* a CUDA runtime call failed; see sph_last_error() */
+  SPH_ERR_OOM = -3,         /* device allocation failed */
+  SPH_ERR_TIMEOUT = -4,     /* sph_sync timed out, or a bounded device wait gave up */
+  SPH_ERR_OVERFLOW = -5,    /* a device-side capacity was exceeded (neighbour list, traversal stack) */
+  SPH_ERR_STATE = -6,       /* call out of order (e.g. stepping before upload) */
+  SPH_NOT_READY = 2         /* readback in flight, not finished yet (sph_readback_take with ready=0) */
+} sph_status;
+
+enum { SPH_KERNEL_CUBIC = 0, SPH_KERNEL_WENDLAND_C2 = 1 };
+enum { SPH_GRAVITY_TREE = 0, SPH_GRAVITY_DIRECT = 1, SPH_GRAVITY_NONE = 2 };
+enum { SPH_MULTIPOLE_MONOPOLE = 0, SPH_MULTIPOLE_QUADRUPOLE = 1 };
+enum { SPH_H_FIXED = 0, SPH_H_SOLVE = 1 };
+enum { SPH_PRECISION_F32 = 0, SPH_PRECISION_HILO = 1 };
+
+/* Solver configuration. sph_config_default() fills the reference's values (SI, cubic spline, monopole
+ * Barnes-Hut at θ = 0.5 with one particle per leaf, fixed h, α = 1, β = 2). */
+typedef struct sph_config {
+  double G;               /* gravitational constant in the caller's units */
+  float theta;            /* Barnes-Hut opening angle; MAC: sqrt(d²+ε²) >= diag/θ + |centre-COM| */
+  uint32_t leaf_size;     /* particles per LBVH leaf bucket (1..32) */
+  uint32_t kernel;        /* SPH_KERNEL_* (support radius h in both) */
+  uint32_t gravity;       /* SPH_GRAVITY_* */
+  uint32_t multipole;     /* SPH_MULTIPOLE_* */
+  uint32_t precision;     /* SPH_PRECISION_*: HILO = node-relative hi/lo coordinates + compensated sums */
+  uint32_t h_mode;        /* SPH_H_*: FIXED keeps the uploaded h (the reference); SOLVE iterates h */
+  float h_neighbours;     /* SOLVE: target neighbour count inside the support radius */
+  float h_tol;            /* SOLVE: relative density residual that ends the iteration */
+  uint32_t h_iters;       /* SOLVE: maximum Newton iterations per force evaluation */
+  uint32_t max_neighbours;/* per-particle neighbour-list capacity */
+  float cfl;              /* > 0: adaptive dt = cfl·min h/max(c+|v|, sig_floor) each step; 0: fixed dt */
+  float rho_floor;        /* sph_step.wgsl:79  max(rho, 1e-9)   (SI value 1e-9) */
+  float du_floor;         /* sph_step.wgsl:91  |u|·1e-3 + 1     (SI value 1)    */
+  float r_min;            /* sph_step.wgsl:187 r > 1e-9         (SI value 1e-9) */
+  float sig_floor;        /* sph_step.wgsl:268 max(c+|v|, 1)    (SI value 1)    */
+  int32_t device;         /* CUDA device ordinal of the context; -1 = the calling thread's current device */
+  uint32_t mac;           /* SPH_MAC_*: GROUP (default) or PARTICLE (the reference's per-particle walk) */
+  uint32_t reserved[6];
+} sph_config;
+
+/* Barnes-Hut acceptance. PARTICLE: each particle walks with the reference MAC sqrt(d²+ε²) >= diag/θ + δ
+ * (bh_gravity.wgsl:382), reproducing cs_gravity_bh bit for bit. GROUP: a warp of 32 Morton-consecutive
+ * particles accepts a node only if the MAC holds for the nearest point of the group's bounding box, so every
+ * particle's own MAC holds too (never less accurate than PARTICLE at the same θ); its gravity walk also
+ * gathers the SPH neighbour candidates. leaf_size must then be a power of two. */
+enum { SPH_MAC_GROUP = 0, SPH_MAC_PARTICLE = 1 };
+
+/* Diagnostics: FP64 device sums over the live particles (gpu_sph.rs:628-649 total_energy;
+ * tools/impact-run/src/main.rs:528-536 angular momentum), plus device-side flags. */
+typedef struct sph_diag_out {
+  double kinetic, internal, potential;   /* potential from the gravity pass: ½ Σ m_i φ_i */
+  double momentum[3];
+  double angular_momentum[3];            /* about the origin */
+  double mass;
+  double dt;                             /* the dt of the last step (adaptive or fixed) */
+  double time;                           /* simulated time accumulated by sph_step_kdk */
+  uint32_t steps;
+  uint32_t max_neighbours_seen;
+  uint32_t overflow_flags;               /* bit0 neighbour list, bit1 traversal stack */
+  uint32_t h_iterations;                 /* SOLVE: iterations used by the last force evaluation */
+  float h_residual;                      /* SOLVE: max relative density residual after the last solve */
+  float pad;
+  /* cumulative tree-walk counters (group MAC): nodes visited, 32-wide pops, particle × multipole and
+   * particle × leaf-source interactions (the latter counts every source of a visited leaf) */
+  uint64_t walk_nodes, walk_pops, m2p_interactions, p2p_interactions;
+} sph_diag_out;
+
+typedef struct sph_ctx sph_ctx;
+
+/* Fill `cfg` with the reference's defaults. */
+sph_status sph_config_default(sph_config* cfg);
+
+/* GpuSph::new (gpu_sph.rs:767): allocate a context for up to `capacity` particles on the current device. */
+sph_status sph_create(const sph_config* cfg, uint32_t capacity, sph_ctx** out);
+void sph_destroy(sph_ctx* ctx);
+
+/* GpuSph::upload (gpu_sph.rs:839-851): copy particles (AoS, host) and the material table in. Like the
+ * reference's ParticleStore::replace it keeps the first `capacity` particles and the first 16 materials,
+ * and then returns SPH_CLAMPED. A particle whose mat is outside the table is SPH_ERR_INVALID. */
+sph_status sph_upload(sph_ctx* ctx, const SphParticle48* particles, uint32_t n, const SphEos48* eos,
+                      uint32_t n_eos, float softening);
+
+/* GpuSph::set_dt (gpu_sph.rs:855-859) and set_av (:865-869); SphParams.omega (gpu_sph.rs:60-79). */
+sph_status sph_set_dt(sph_ctx* ctx, double dt, float damp);
+sph_status sph_set_av(sph_ctx* ctx, float alpha, float beta);
+sph_status sph_set_omega(sph_ctx* ctx, float omega);
+
+/* GpuSph::encode_kdk (gpu_sph.rs:901-908): enqueue `substeps` KDK leapfrog steps (two force evaluations
+ * each, u clamped at 0) on the context's stream and return without waiting. */
+sph_status sph_step_kdk(sph_ctx* ctx, uint32_t substeps);
+/* GpuSph::encode_relax (gpu_sph.rs:893-898): enqueue damped relaxation steps (one evaluation each). */
+sph_status sph_step_relax(sph_ctx* ctx, uint32_t steps);
+/* One force evaluation on the current state without integrating (the verifier's run_gpu). */
+sph_status sph_eval_forces(sph_ctx* ctx);
+
+/* ParticleStore::begin_readback / take_readback (gpu_store.rs:126-213): a two-phase, non-blocking copy of
+ * the live particles (AoS, original order) to host memory the caller owns. Only one readback is in
+ * flight; take returns SPH_NOT_READY with *ready = 0 until it lands. */
+sph_status sph_readback_begin(sph_ctx* ctx);
+sph_status sph_readback_take(sph_ctx* ctx, SphParticle48* out, uint32_t cap, uint32_t* n_out, int* ready);
+
+/* Wait for all enqueued work (timeout_ms = 0 waits without limit). */
+sph_status sph_sync(sph_ctx* ctx, uint32_t timeout_ms);
+uint32_t sph_count(const sph_ctx* ctx);
+/* GpuSph::particle_buffer (gpu_sph.rs:876): a device buffer holding the live particles in the 48-byte
+ * layout in original order, refreshed by this call (the headless stand-in for the render vertex buffer). */
+sph_status sph_particle_buffer(sph_ctx* ctx, void** device_ptr);
+sph_status sph_diag(sph_ctx* ctx, sph_diag_out* out);
+/* The context's CUDA stream (cudaStream_t), for callers that order their own work after the step. */
+void* sph_stream(sph_ctx* ctx);
+const char* sph_last_error(const sph_ctx* ctx);
+const char* sph_status_string(sph_status s);
+
+/* Inspection of one force evaluation's intermediates, for staged verification (the checks of
+ * tools/gpu-bh-verify/src/main.rs and tools/sph-verify/src/main.rs). Sorted-space arrays come back in
+ * Morton order; per-particle physical quantities come back in original particle order. */
+enum {
+  SPH_Q_BBOX = 0,        /* float[6]   lo.xyz, hi.xyz (cs_bbox) */
+  SPH_Q_CODES = 1,       /* uint32[n]  sorted Morton codes */
+  SPH_Q_ORDER = 2,       /* uint32[n]  original index at each sorted position (the sort permutation) */
+  SPH_Q_LEFT = 3,        /* uint32[L-1] */
+  SPH_Q_RIGHT = 4,       /* uint32[L-1] */
+  SPH_Q_PARENT = 5,      /* uint32[2L-1] */
+  SPH_Q_NODE_COM = 6,    /* float4[2L-1] com.xyz, mass */
+  SPH_Q_NODE_BMIN = 7,   /* float4[2L-1] bmin.xyz, max h */
+  SPH_Q_NODE_BMAX = 8,   /* float4[2L-1] bmax.xyz, opening radius diag/θ+δ */
+  SPH_Q_NBR_COUNT = 9,   /* uint32[n]  neighbours of each particle (original order) */
+  SPH_Q_NBR_LIST = 10,   /* uint32[n*max_neighbours] original indices, row i = particle i, unsorted */
+  SPH_Q_RHO = 11,        /* float[n] */
+  SPH_Q_PRESSURE = 12,   /* float[n] */
+  SPH_Q_SOUND = 13,      /* float[n] */
+  SPH_Q_ACC_SPH = 14,    /* float4[n]  SPH acceleration xyz, du/dt */
+  SPH_Q_ACC_GRAV = 15,   /* float4[n]  gravity acceleration xyz, potential */
+  SPH_Q_H = 16,          /* float[n]   smoothing lengths */
+  SPH_Q_N_LEAVES = 17    /* uint32[1]  L */
+};
+sph_status sph_inspect(sph_ctx* ctx, uint32_t what, void* host_out, size_t bytes);
+
+/* Per-phase device timing (CUDA events recorded on the context's stream around each phase; the reference
+ * has none: gpu_sph.rs:879 passes `timestamp_writes: None`) and the count of kernels the library launched. */
+enum {
+  SPH_PHASE_SORT = 0,        /* bbox, Morton keys, radix sort, state permutation */
+  SPH_PHASE_TREE = 1,        /* Karras internal nodes + bottom-up moments */
+  SPH_PHASE_GRAVITY = 2,     /* Barnes-Hut traversal or direct sum */
+  SPH_PHASE_NEIGHBOURS = 3,  /* neighbour lists */
+  SPH_PHASE_HSOLVE = 4,      /* smoothing-length iterations */
+  SPH_PHASE_DENSITY = 5,     /* density + EOS */
+  SPH_PHASE_FORCES = 6,      /* pressure + AV + du/dt (+ Courant signal) */
+  SPH_PHASE_INTEGRATE = 7,   /* dt, kicks, drift, relaxation */
+  SPH_PHASE_COUNT = 8
+};
+typedef struct sph_profile {
+  double ms[SPH_PHASE_COUNT];
+  uint64_t calls[SPH_PHASE_COUNT];
+  uint64_t kernel_launches;  /* kernels launched since sph_profile_enable (counted whether or not timing is on) */
+} sph_profile;
+/* on != 0 starts recording phase events; any call resets the accumulators and the launch count. */
+sph_status sph_profile_enable(sph_ctx* ctx, int on);
+/* Waits for the stream, then reports the accumulated phase times since the last enable. */
+sph_status sph_profile_read(sph_ctx* ctx, sph_profile* out);
+
+/* GravityField::accelerations (gpu_gravity.rs:556) / cs_gravity_bh: softened self-gravity of a point set
+ * through the LBVH (gravity = SPH_GRAVITY_TREE) or the direct sum, using the context's G, θ, leaf size and
+ * multipole settings. Host arrays; acc3 receives the accelerations in input order. */
+sph_status sph_gravity(sph_ctx* ctx, const double* pos3, const double* mass, uint32_t n, double softening,
+                       uint32_t gravity_mode, double* acc3);
+
+/* FP64 softened direct sum on a subset of targets against all n sources, on the device (the precision
+ * oracle of the gravity tree). targets may be NULL (all particles). */
+sph_status sph_gravity_direct64(sph_ctx* ctx, const double* pos3, const double* mass, uint32_t n,
+                                const uint32_t* targets, uint32_t n_targets, double softening, double* acc3);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SPH_B200_H */

@@ -65,7 +65,7 @@ def lib():
     L.orc_bbox32.argtypes = [f32p, C.c_int, f32p, f32p]
     L.orc_morton32.argtypes = [f32p, C.c_int, f32p, f32p, u32p]
     L.orc_sort_code_index.argtypes = [u32p, C.c_int, u32p, u32p]
-    L.orc_karras.argtypes = [u32p, C.c_int, u32p, u32p, u32p]
+    L.orc_karras.argtypes = [u32p, C.c_int, u32p, u32p, u32p, C.c_int]
     L.orc_verify_tree.restype = C.c_int
     L.orc_verify_tree.argtypes = [u32p, u32p, u32p, C.c_int]
     L.orc_moments32.argtypes = [f32p, C.c_int, C.c_int, C.c_int, u32p, u32p, f32p, f32p, f32p]
@@ -160,14 +160,14 @@ def sort_code_index(codes):
     return order, sc
 
 
-def karras(leaf_codes):
+def karras(leaf_codes, exact_dups=False):
     lc = _c(leaf_codes, np.uint32)
     L = len(lc)
     nn = 2 * L - 1
     left = np.zeros(max(L - 1, 1), np.uint32)
     right = np.zeros(max(L - 1, 1), np.uint32)
     parent = np.zeros(nn, np.uint32)
-    lib().orc_karras(lc, L, left, right, parent)
+    lib().orc_karras(lc, L, left, right, parent, int(exact_dups))
     return left[: L - 1], right[: L - 1], parent
 
 
@@ -203,7 +203,7 @@ def gravity_bh32(sbodies4, K, left, right, com, bmin, bmax, order, theta, soft2,
     return acc, dropped
 
 
-def tree_pipeline32(bodies4, K=1, theta=0.5, soft=0.0, G=6.674e-11):
+def tree_pipeline32(bodies4, K=1, theta=0.5, soft=0.0, G=6.674e-11, exact_dups=False):
     """bbox → Morton → (code,index) sort → cluster codes → Karras → moments → traversal, all in f32.
 
     Mirrors the staged pipeline of tools/gpu-bh-verify (build_tree + cs_gravity_bh). Returns a dict with
@@ -216,7 +216,7 @@ def tree_pipeline32(bodies4, K=1, theta=0.5, soft=0.0, G=6.674e-11):
     order, scodes = sort_code_index(codes)
     L = (n + K - 1) // K
     leaf_codes = scodes[np.arange(L) * K]
-    left, right, parent = karras(leaf_codes)
+    left, right, parent = karras(leaf_codes, exact_dups)
     sb = np.ascontiguousarray(b[order])
     com, bmin, bmax = moments32(sb, K, left, right)
     acc, dropped = gravity_bh32(sb, K, left, right, com, bmin, bmax, order, theta,

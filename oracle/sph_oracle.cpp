@@ -220,7 +220,9 @@ inline int kdelta(const uint32_t* codes, int L, int i, int j) {
 }
 
 // One internal node of the Karras build, bh_gravity.wgsl:135-184. Returns (left, right).
-void karras_node(const uint32_t* codes, int L, int i, uint32_t* left, uint32_t* right) {
+// exact_dups = 0 reproduces the reference; 1 splits runs of equal codes on the index-extended key
+// (Karras 2012 §4), which the reference's midpoint split does not always agree with.
+void karras_node(const uint32_t* codes, int L, int i, uint32_t* left, uint32_t* right, int exact_dups) {
   const int d = kdelta(codes, L, i, i + 1) > kdelta(codes, L, i, i - 1) ? 1 : -1;
   const int dmin = kdelta(codes, L, i, i - d);
   int lmax = 2;
@@ -232,8 +234,17 @@ void karras_node(const uint32_t* codes, int L, int i, uint32_t* left, uint32_t* 
   const int first = std::min(i, j), last = std::max(i, j);
   int split = first;
   const uint32_t fc = codes[first], lc = codes[last];
-  if (fc == lc) {
+  if (fc == lc && !exact_dups) {
     split = (first + last) >> 1;
+  } else if (fc == lc) {
+    const int cpfx = kdelta(codes, L, first, last);
+    int step = last - first;
+    for (;;) {
+      step = (step + 1) >> 1;
+      const int ns = split + step;
+      if (ns < last && kdelta(codes, L, first, ns) > cpfx) split = ns;
+      if (step <= 1) break;
+    }
   } else {
     const int cpfx = clz32(fc ^ lc);
     int step = last - first;
@@ -645,11 +656,12 @@ void orc_sort_code_index(const uint32_t* codes, int n, uint32_t* order, uint32_t
   for (int t = 0; t < n; ++t) { order[t] = o[t]; sorted_codes[t] = codes[o[t]]; }
 }
 // Cluster codes (gpu_gravity.rs:366) + Karras internal nodes (cs_tree). parent[] as cs_tree_reset/cs_tree.
-void orc_karras(const uint32_t* leaf_codes, int L, uint32_t* left, uint32_t* right, uint32_t* parent) {
+void orc_karras(const uint32_t* leaf_codes, int L, uint32_t* left, uint32_t* right, uint32_t* parent,
+                int exact_dups) {
   const int nn = 2 * L - 1;
   for (int i = 0; i < nn; ++i) parent[i] = 0xffffffffu;
   for (int i = 0; i < L - 1; ++i) {
-    karras_node(leaf_codes, L, i, &left[i], &right[i]);
+    karras_node(leaf_codes, L, i, &left[i], &right[i], exact_dups);
     parent[left[i]] = (uint32_t)i;
     parent[right[i]] = (uint32_t)i;
   }
