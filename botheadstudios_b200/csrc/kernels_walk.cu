@@ -25,7 +25,8 @@ constexpr int TW_LIST = 64;     // per-warp list capacity (flushed once half ful
 struct WalkSmem {
   unsigned stack[TW_WARPS][TW_STACK];
   unsigned m2p[TW_WARPS][TW_LIST];
-  unsigned p2p[TW_WARPS][TW_LIST];
+  unsigned p2p[TW_WARPS][TW_LIST];   // near leaves: pairwise gravity + neighbour predicate
+  unsigned p2f[TW_WARPS][TW_LIST];   // far leaves: pairwise gravity only
   float4 src[TW_WARPS][32];   // staged sources: x, y, z, m
   float4 q0[TW_WARPS][32];    // staged quadrupoles
   float2 q1[TW_WARPS][32];
@@ -117,9 +118,43 @@ __global__ void __launch_bounds__(TW_WARPS * 32, 6) k_tree_walk(
   const float gx1 = warp_max(valid ? pi.x : -big), gy1 = warp_max(valid ? pi.y : -big),
               gz1 = warp_max(valid ? pi.z : -big);
   const float ghmax = warp_max(valid ? pi.w : 0.0f);
-  int sp = 1, nm = 0, np = 0;
+  int sp = 1, nm = 0, np = 0, nf = 0;
   if (lane == 0) stack[0] = 0u;
   __syncwarp();
+
+  // ---- far leaves: branch-free pairwise gravity, 32 staged sources per pass ---------------------------
+  auto flush_far = [&](int count) {
+    const int per = 32 / K;
+    for (int base = 0; base < count; base += per) {
+      const int nl = min(per, count - base);
+      const int li = lane / K, off = lane % K;
+      float4 src = make_float4(3.0e18f, 3.0e18f, 3.0e18f, 0.0f);  // padding: massless and far away
+      if (li < nl) {
+        const int s = (int)S.p2f[w][base + li] * K + off;
+        if (s < n) {
+          src = body[s];
+          src.w *= G;
+        }
+      }
+      S.src[w][lane] = src;
+      __syncwarp();
+      if (valid) {
+#pragma unroll 8
+        for (int k = 0; k < 32; ++k) {
+          const float4 bj = S.src[w][k];
+          float dx = bj.x - pi.x, dy = bj.y - pi.y, dz = bj.z - pi.z;
+          if (HILO) { dx -= xlo; dy -= ylo; dz -= zlo; }
+          const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, soft2)));
+          const float rinv = rsqrtf(r2);
+          const float gm = bj.w * rinv;
+          const float g = gm * rinv * rinv;
+          acc.add<HILO>(g * dx, g * dy, g * dz);
+          phi -= gm;
+        }
+      }
+      __syncwarp();
+    }
+  };
 
   // ---- multipole list: stage 32 nodes in shared memory, then every lane applies them -------------------
   auto flush_m2p = [&](int count) {
@@ -175,41 +210,40 @@ __global__ void __launch_bounds__(TW_WARPS * 32, 6) k_tree_walk(
       const int nl = min(per, count - base);
       const int li = lane / K, off = lane % K;
       int sidx = -1;
-      bool near_src = false;
       if (li < nl) {
-        const unsigned e = S.p2p[w][base + li];
-        const int s = (int)(e & 0x7fffffffu) * K + off;
-        near_src = (e >> 31) != 0u;
+        const int s = (int)S.p2p[w][base + li] * K + off;
         if (s < n) sidx = s;
       }
       S.sidx[w][lane] = sidx;
+      float4 src = make_float4(3.0e18f, 3.0e18f, 3.0e18f, 0.0f);  // padding: massless and far away
+      float hsrc = 0.0f;
       if (sidx >= 0) {
-        S.src[w][lane] = body[sidx];
-        // smoothing length of sources inside the SPH reach; -1 marks a source that cannot be a neighbour
-        if (NBR) S.hsrc[w][lane] = near_src ? pos_h[sidx].w : -1.0f;
+        src = body[sidx];
+        src.w *= G;
+        if (NBR) hsrc = pos_h[sidx].w;
       }
-      const unsigned have = __ballot_sync(SPH_FULL_MASK, sidx >= 0);
+      S.src[w][lane] = src;
+      if (NBR) S.hsrc[w][lane] = hsrc;
       __syncwarp();
       if (valid) {
-        unsigned m = have;
-        while (m) {
-          const int k = __ffs(m) - 1;
-          m &= m - 1;
+#pragma unroll 4
+        for (int k = 0; k < 32; ++k) {
           const int s = S.sidx[w][k];
-          if (s == t) continue;
+          const bool other = s >= 0 && s != t;
           const float4 bj = S.src[w][k];
           const float dx = fsub(bj.x, pi.x), dy = fsub(bj.y, pi.y), dz = fsub(bj.z, pi.z);
           const float dd = dot3_exact(dx, dy, dz);
-          if (NBR) {
-            const float hj = S.hsrc[w][k];
-            if (hj >= 0.0f) {
-              const float r = fsqrt(dd);
-              float lim = fmul(0.5f, fadd(pi.w, hj));
-              if (skin > 0.0f) lim = lim * (1.0f + skin);
-              if (r < lim) {
-                if (cnt < cap) nbr[nbr_slot((unsigned)t, cnt, cap)] = (unsigned)s;
-                ++cnt;
-              }
+          if (NBR && other) {
+            float lim = fmul(0.5f, fadd(pi.w, S.hsrc[w][k]));
+            if (skin > 0.0f) lim = lim * (1.0f + skin);
+            // sqrt_rn(dd) < lim, decided without the square root outside a 2^-19 band around lim²:
+            // dd < lim²(1-2^-19) ⇒ √dd < lim − 2 ulp(lim); dd > lim²(1+2^-19) ⇒ √dd > lim + 2 ulp(lim)
+            const float q = fmul(lim, lim);
+            bool inside = dd < fmul(q, 1.0f - 1.9073486e-6f);
+            if (!inside && !(dd > fmul(q, 1.0f + 1.9073486e-6f))) inside = fsqrt(dd) < lim;
+            if (inside) {
+              if (cnt < cap) nbr[nbr_slot((unsigned)t, cnt, cap)] = (unsigned)s;
+              ++cnt;
             }
           }
           if (GRAV) {
@@ -220,9 +254,9 @@ __global__ void __launch_bounds__(TW_WARPS * 32, 6) k_tree_walk(
               ez -= zlo;
               d2 = ex * ex + ey * ey + ez * ez;
             }
-            const float r2 = d2 + soft2;
+            const float r2 = other ? d2 + soft2 : 1.0f;
             const float rinv = rsqrtf(r2);
-            const float gm = G * bj.w * rinv;
+            const float gm = other ? bj.w * rinv : 0.0f;
             const float g = gm * rinv * rinv;
             acc.add<HILO>(g * ex, g * ey, g * ez);
             phi -= gm;
@@ -248,8 +282,10 @@ __global__ void __launch_bounds__(TW_WARPS * 32, 6) k_tree_walk(
       const float4 bl = nbmin[node], bh = nbmax[node];
       const bool is_leaf = node >= leaf0;
       bool near = false;
-      if (NBR) {
-        const float reach = 0.5f * (ghmax + bl.w) * grow;
+      {
+        // SPH reach (or, for gravity alone, plain overlap with the group box so that a group's own leaves
+        // take the careful path that skips self-pairs)
+        const float reach = NBR ? 0.5f * (ghmax + bl.w) * grow : 0.0f;
         near = (bl.x - reach <= gx1) && (bh.x + reach >= gx0) && (bl.y - reach <= gy1) && (bh.y + reach >= gy0) &&
                (bl.z - reach <= gz1) && (bh.z + reach >= gz0);
       }
@@ -266,15 +302,17 @@ __global__ void __launch_bounds__(TW_WARPS * 32, 6) k_tree_walk(
       }
       if (mac && !near) acc_node = true;
       else if (is_leaf) leaf = GRAV || near;
-      else open = GRAV || near;
+      else open = GRAV || (NBR && near);
       near_leaf = leaf && near;
     }
     const unsigned bm = __ballot_sync(SPH_FULL_MASK, acc_node);
     const unsigned bf = __ballot_sync(SPH_FULL_MASK, leaf);
     const unsigned bo = __ballot_sync(SPH_FULL_MASK, open);
+    const unsigned bn = __ballot_sync(SPH_FULL_MASK, near_leaf);
+    const unsigned bfar = bf & ~bn;
     if (acc_node) S.m2p[w][nm + __popc(bm & lt)] = node;
-    // direct-list entry: leaf index, bit 31 set when the leaf lies within the SPH reach
-    if (leaf) S.p2p[w][np + __popc(bf & lt)] = (node - leaf0) | (near_leaf ? 0x80000000u : 0u);
+    if (near_leaf) S.p2p[w][np + __popc(bn & lt)] = node - leaf0;
+    else if (leaf) S.p2f[w][nf + __popc(bfar & lt)] = node - leaf0;
     const int no = __popc(bo);
     if (sp + 2 * no <= TW_STACK) {
       if (open) {
@@ -287,7 +325,8 @@ __global__ void __launch_bounds__(TW_WARPS * 32, 6) k_tree_walk(
       overflow = 1;
     }
     nm += __popc(bm);
-    np += __popc(bf);
+    np += __popc(bn);
+    nf += __popc(bfar);
     seg_m2p += __popc(bm);
     seg_p2p += __popc(bf);
     __syncwarp();
@@ -299,9 +338,14 @@ __global__ void __launch_bounds__(TW_WARPS * 32, 6) k_tree_walk(
       flush_p2p(np);
       np = 0;
     }
+    if (nf > TW_LIST - 32) {
+      flush_far(nf);
+      nf = 0;
+    }
   }
   if (nm) flush_m2p(nm);
   if (np) flush_p2p(np);
+  if (nf) flush_far(nf);
   st_m2p += seg_m2p * nvalid;                             // node × particle interactions
   st_p2p += seg_p2p * (unsigned long long)K * nvalid;     // leaf sources × particles (upper bound)
   }  // segments

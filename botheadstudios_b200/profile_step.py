@@ -17,10 +17,18 @@ def main():
     ap.add_argument("--warmup", type=int, default=1)
     ap.add_argument("--steps", type=int, default=1)
     ap.add_argument("--mac", type=int, default=0)
+    ap.add_argument("--theta", type=float, default=None)
+    ap.add_argument("--precision", type=int, default=0, help="1 = node-relative hi/lo + compensated sums")
+    ap.add_argument("--accuracy", type=int, default=0,
+                    help="targets for an FP64 direct-sum check of the tree gravity (0 = skip)")
     args = ap.parse_args()
     wl = workloads.WORKLOADS[args.workload]
     I = workloads.build(wl)
-    with workloads.solver(wl, I, mac=args.mac) as s:
+    over = dict(mac=args.mac, precision=args.precision)
+    if args.theta is not None:
+        over["theta"] = args.theta
+    acc_err = None
+    with workloads.solver(wl, I, **over) as s:
         s.upload(I.particles, I.eos, I.softening)
         s.encode_kdk(args.warmup)
         s.sync()
@@ -29,12 +37,24 @@ def main():
         s.encode_kdk(args.steps)
         prof = s.profile_read()
         d1 = s.diag()
+        if args.accuracy:
+            import numpy as np
+            state = s.readback()
+            g = s.inspect("ACC_GRAV")[:, :3].astype(np.float64)
+            pos = state["pos"].astype(np.float64)
+            mass = state["mass"].astype(np.float64)
+            tg = np.random.default_rng(7).choice(len(mass), args.accuracy, replace=False).astype(np.uint32)
+            ref = s.gravity_direct64(pos, mass, I.softening, targets=tg)
+            e = np.linalg.norm(g[tg] - ref, axis=1) / np.linalg.norm(ref, axis=1)
+            acc_err = dict(targets=args.accuracy, rms_rel=float(np.sqrt(np.mean(e * e))),
+                           p99_rel=float(np.quantile(e, 0.99)), max_rel=float(e.max()),
+                           global_rms=float(np.sqrt(((g[tg] - ref) ** 2).sum() / (ref ** 2).sum())))
     n = len(I.particles)
     walks = max(prof["calls"]["gravity"], 1)
     stats = {k: (d1[k] - d0[k]) / walks for k in ("walk_nodes", "walk_pops", "m2p_interactions", "p2p_interactions")}
     print(json.dumps(dict(workload=args.workload, particles=n, steps=args.steps, phases_ms=prof["ms"],
                           calls=prof["calls"], launches=prof["kernel_launches"], per_walk=stats,
-                          per_particle={k: v / n for k, v in stats.items()})))
+                          per_particle={k: v / n for k, v in stats.items()}, gravity_error=acc_err)))
 
 
 if __name__ == "__main__":
