@@ -262,16 +262,42 @@ def run_ours(args, wl, world, rank, local, pg):
         phases[k] = dict(ms=round(t, 4), share=round(t / sum(prof["ms"].values()), 4), calls=calls,
                          gbs=round(b / (t / 1000.0) / 1e9, 1))
     dom = max(phases, key=lambda k: phases[k]["ms"])
-    dom_bytes = BYTES_PER_PARTICLE[dom] * n
     dom_ms = phases[dom]["ms"] / phases[dom]["calls"]
-    achieved = dom_bytes / (dom_ms / 1000.0) / 1e9
     traffic = None
     tf = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tf):
         traffic = json.load(open(tf)).get(args.workload, {}).get(dom)
-    roof = dict(bound="hbm", kernel_phase=dom, achieved=round(achieved, 1), peak=pk["hbm"], unit="GB/s",
-                frac=round(achieved / pk["hbm"], 4), traffic=traffic, peak_source=pk["src"],
-                bytes_per_launch=dom_bytes, ms_per_launch=round(dom_ms, 4))
+    if dom == "gravity" and wl.get("quad") is not None:
+        # The walk (group-MAC gravity fused with the neighbour lists) is FP32-pipe bound: algorithmic FLOPs
+        # from the device counters — 65 per quadrupole (20 per monopole) node interaction, 20 per pairwise
+        # interaction, 12 per node acceptance test — over its CUDA-event time. Peak: FP32 FMA throughput
+        # of 148 SMs × 128 lanes × 2 FLOP × the max SM clock (nominal; no measured FP32 peak exists here).
+        walks = max(phases["gravity"]["calls"], 1)
+        m2p = (d1["m2p_interactions"] - d0["m2p_interactions"]) / walks
+        p2p = (d1["p2p_interactions"] - d0["p2p_interactions"]) / walks
+        vis = (d1["walk_nodes"] - d0["walk_nodes"]) / walks
+        flops = (65.0 if wl["quad"] else 20.0) * m2p + 20.0 * p2p + 12.0 * vis
+        clk_max = (clk.summary() or {}).get("sm_max_mhz") or 1965.0
+        peak_tf = 148 * 128 * 2 * clk_max * 1e6 / 1e12
+        achieved = flops / (dom_ms / 1000.0) / 1e12
+        roof = dict(bound="fp32", kernel="k_tree_walk", achieved=round(achieved, 2), peak=round(peak_tf, 1),
+                    unit="TFLOP/s", frac=round(achieved / peak_tf, 4), traffic=traffic,
+                    peak_source="nominal FP32 FMA peak (148 SM x 128 lanes x 2 x max SM clock)",
+                    flops_per_launch=flops, ms_per_launch=round(dom_ms, 4),
+                    interactions_per_particle=dict(multipole=m2p / n, pairwise=p2p / n, nodes=vis / n))
+    else:
+        dom_bytes = BYTES_PER_PARTICLE[dom] * n
+        achieved = dom_bytes / (dom_ms / 1000.0) / 1e9
+        roof = dict(bound="hbm", kernel_phase=dom, achieved=round(achieved, 1), peak=pk["hbm"], unit="GB/s",
+                    frac=round(achieved / pk["hbm"], 4), traffic=traffic, peak_source=pk["src"],
+                    bytes_per_launch=dom_bytes, ms_per_launch=round(dom_ms, 4))
+    # memory-bound phases against the measured HBM copy bandwidth
+    mem = [k for k in ("sort", "tree", "density", "forces", "integrate", "hsolve") if k in phases]
+    mem_bytes = sum(BYTES_PER_PARTICLE[k] * n * phases[k]["calls"] for k in mem)
+    mem_ms = sum(phases[k]["ms"] for k in mem)
+    roof_hbm = dict(bound="hbm", phases=mem, achieved=round(mem_bytes / (mem_ms / 1000.0) / 1e9, 1),
+                    peak=pk["hbm"], unit="GB/s", frac=round(mem_bytes / (mem_ms / 1000.0) / 1e9 / pk["hbm"], 4),
+                    peak_source=pk["src"])
     # ---- CPU baseline on the host cores (rank 0, N=1 only) ----
     cpu = None
     if world == 1 and not args.no_cpu:
@@ -291,7 +317,7 @@ def run_ours(args, wl, world, rank, local, pg):
                             l2="working set > L2 (no flush needed)"),
                 e2e=dict(value=e2e_value, unit=UNIT, h2d_bytes_per_step=48 * n, d2h_bytes_per_step=48 * n,
                          steps=e2e_steps),
-                gpu_launches=prof["kernel_launches"], roofline=roof, phases=phases, cpu_baseline=cpu,
+                gpu_launches=prof["kernel_launches"], roofline=roof, roofline_hbm=roof_hbm, phases=phases, cpu_baseline=cpu,
                 clocks=clk.summary(),
                 physics=dict(energy_drift=(energy1 - energy0) / abs(d0["potential"]) if d0["potential"] else None,
                              sim_time=dd["time"], dt=dd["dt"], max_neighbours=dd["max_neighbours_seen"],

@@ -83,11 +83,16 @@ typedef struct sph_config {
   uint32_t reserved[6];
 } sph_config;
 
-/* Barnes-Hut acceptance. PARTICLE: each particle walks with the reference MAC sqrt(d²+ε²) >= diag/θ + δ
- * (bh_gravity.wgsl:382), reproducing cs_gravity_bh bit for bit. GROUP: a warp of 32 Morton-consecutive
- * particles accepts a node only if the MAC holds for the nearest point of the group's bounding box, so every
- * particle's own MAC holds too (never less accurate than PARTICLE at the same θ); its gravity walk also
- * gathers the SPH neighbour candidates. leaf_size must then be a power of two. */
+/* Barnes-Hut acceptance. PARTICLE: each particle walks with the GPU reference's MAC
+ * sqrt(d²+ε²) >= diag/θ + δ (bh_gravity.wgsl:382; diag = AABB diagonal, δ = |centre − COM|), reproducing
+ * cs_gravity_bh bit for bit, and uses the reference's split for runs of equal Morton codes.
+ * GROUP: a warp takes a group of <= 32 particles (a subtree of the LBVH) and accepts a node only when
+ * sqrt(d_box²+ε²) >= side/θ + δ holds for the nearest point of the group's bounding box, so it holds for
+ * every particle of the group. θ here measures the node's largest side, as in the reference's CPU octree
+ * (bhtree.rs:181, (2·half)/dist < θ), with Barnes' δ term added; at equal θ this is looser than the diagonal
+ * form. Leaves may be accepted as multipoles. The same walk gathers the SPH neighbour candidates, and runs
+ * of equal Morton codes are split on the index-extended key (always a valid tree). leaf_size must be a power
+ * of two. */
 enum { SPH_MAC_GROUP = 0, SPH_MAC_PARTICLE = 1 };
 
 /* Diagnostics: FP64 device sums over the live particles (gpu_sph.rs:628-649 total_energy;

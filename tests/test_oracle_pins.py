@@ -193,3 +193,21 @@ def test_conservation_sums_and_kdk_momentum():
     assert e0[0] > 0 and e0[1] > 0 and e0[2] < 0
     pscale = (mass * np.linalg.norm(v1, axis=1)).sum()
     assert np.linalg.norm(e1[3:6] - e0[3:6]) / pscale < 1e-9
+
+
+def test_reference_split_of_equal_codes_can_build_invalid_trees():
+    """bh_gravity.wgsl:159-160 splits a run of equal Morton codes at its midpoint, which can disagree with the
+    index-extended ranges the children determine for themselves: on duplicate-heavy inputs the reference's
+    tree is often invalid (a node reached twice or not at all). Splitting on the index-extended key
+    (Karras 2012) always gives a valid tree; that is what the default walk mode builds."""
+    bad_ref = bad_fix = 0
+    for seed in range(12):
+        rng = np.random.default_rng(seed)
+        b = rng.random((int(rng.integers(200, 2000)), 4)).astype(np.float32)
+        b[:, :3] = np.floor(b[:, :3] * float(rng.integers(2, 9))) / 8.0
+        for K in (1, 16):
+            t0 = oracle.tree_pipeline32(b, K=K, exact_dups=False)
+            t1 = oracle.tree_pipeline32(b, K=K, exact_dups=True)
+            bad_ref += not oracle.verify_tree(t0["left"], t0["right"], t0["parent"], t0["L"])
+            bad_fix += not oracle.verify_tree(t1["left"], t1["right"], t1["parent"], t1["L"])
+    assert bad_ref > 0 and bad_fix == 0
