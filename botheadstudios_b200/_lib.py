@@ -66,7 +66,7 @@ EXPORTS = ["sph_config_default", "sph_create", "sph_destroy", "sph_upload", "sph
            "sph_set_omega", "sph_step_kdk", "sph_step_relax", "sph_eval_forces", "sph_readback_begin",
            "sph_readback_take", "sph_sync", "sph_count", "sph_particle_buffer", "sph_diag", "sph_stream",
            "sph_last_error", "sph_status_string", "sph_inspect", "sph_profile_enable", "sph_profile_read",
-           "sph_gravity", "sph_gravity_direct64"]
+           "sph_gravity", "sph_gravity_direct64", "sph_gravity_tree_noalloc"]
 
 _lib = None
 
@@ -110,6 +110,8 @@ def load():
     L.sph_profile_read.argtypes = [vp, C.POINTER(SphProfile)]
     L.sph_gravity.argtypes = [vp, vp, vp, C.c_uint32, C.c_double, C.c_uint32, vp]
     L.sph_gravity_direct64.argtypes = [vp, vp, vp, C.c_uint32, vp, C.c_uint32, C.c_double, vp]
+    L.sph_gravity_tree_noalloc.argtypes = [vp, C.c_uint32, C.c_double, C.c_float, C.c_float, C.c_uint32, C.c_uint32,
+                                           vp, vp]
     for name in EXPORTS:
         if name not in ("sph_destroy", "sph_count", "sph_stream", "sph_last_error", "sph_status_string"):
             getattr(L, name).restype = C.c_int

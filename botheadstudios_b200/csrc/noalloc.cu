@@ -1,0 +1,179 @@
+// Tree gravity of a point set that allocates no memory.
+//
+// Some callers cannot allocate device memory when they need a force evaluation: a real-time frame loop where
+// cudaMalloc/cudaFree would synchronise the whole device and stall the frame, or a host engine whose device
+// memory is reserved up front by its own allocator and hands plug-ins only the buffers it owns. For them,
+// sph_gravity_tree_noalloc runs the same LBVH pipeline as the context path (bbox, Morton keys, radix sort,
+// Karras, moments, group-MAC walk) with every scratch buffer carved out of one fixed array in device
+// memory, compiled into the library. The caller passes device pointers for the input points and the output
+// accelerations. The array holds at most kNoAllocMaxPoints points; every GPU that loads the library keeps it
+// for the life of the process.
+#include <cstring>
+
+#include "../../include/sph_b200.h"
+#include "sph_kernels.cuh"
+
+namespace sphb {
+namespace {
+
+constexpr uint32_t kNoAllocMaxPoints = 65536;
+constexpr uint32_t kNoAllocMinLeaf = 8;  // bounds the node arrays: at most kNoAllocMaxPoints / 8 leaves
+constexpr size_t kAlign = 256;
+
+constexpr size_t up(size_t x) { return (x + kAlign - 1) / kAlign * kAlign; }
+
+// Byte size of every buffer of the pipeline for kNoAllocMaxPoints points and leaves of >= kNoAllocMinLeaf.
+constexpr size_t scratch_bytes() {
+  const size_t n = kNoAllocMaxPoints;
+  const size_t L = n / kNoAllocMinLeaf;
+  const size_t nodes = 2 * L;
+  const size_t tiles = (n + 2047) / 2048;
+  size_t b = 0;
+  b += 2 * (up(16 * n) + up(16 * n) + 3 * up(8 * n) + 4 * up(4 * n));  // two particle states
+  b += 2 * up(8 * n) + 2 * up(4 * n);                                  // sort keys and values
+  b += up(16 * n) + up(16 * n);                                        // bodies, accelerations
+  b += up(4 * 256 * tiles) + up(4 * 256);                              // radix histograms
+  b += 4 * up(4 * L) + up(8 * L) + up(4);                              // leaf codes, left/right/counters, groups
+  b += up(4 * nodes) + 5 * up(16 * nodes);                             // parents, node records
+  b += up(sizeof(DevParams));
+  return b;
+}
+constexpr size_t kScratchBytes = scratch_bytes();
+
+// The scratch array. In host code `g_noalloc_scratch` names a host-side stand-in, not device memory: its
+// device address comes from cudaGetSymbolAddress, looked up once per device.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
+
+constexpr int kMaxDevices = 64;
+void* g_scratch_addr[kMaxDevices] = {nullptr};
+
+template <typename T>
+T* carve(unsigned char*& p, size_t count) {
+  T* r = reinterpret_cast<T*>(p);
+  p += up(sizeof(T) * count);
+  return r;
+}
+
+Dev carve_dev(unsigned char* base, uint32_t K) {
+  const size_t n = kNoAllocMaxPoints;
+  const size_t L = n / kNoAllocMinLeaf;
+  const size_t nodes = 2 * L;
+  unsigned char* p = base;
+  Dev d;
+  d.cap = (int)n;
+  d.K = (int)K;
+  for (int b = 0; b < 2; ++b) {
+    State& s = d.st[b];
+    s.pos_h = carve<float4>(p, n);
+    s.vel_u = carve<float4>(p, n);
+    s.x = carve<double>(p, n);
+    s.y = carve<double>(p, n);
+    s.z = carve<double>(p, n);
+    s.mass = carve<float>(p, n);
+    s.mat = carve<unsigned>(p, n);
+    s.prov = carve<unsigned>(p, n);
+    s.id = carve<unsigned>(p, n);
+  }
+  d.keys[0] = carve<unsigned long long>(p, n);
+  d.keys[1] = carve<unsigned long long>(p, n);
+  d.vals[0] = carve<unsigned>(p, n);
+  d.vals[1] = carve<unsigned>(p, n);
+  d.body = carve<float4>(p, n);
+  d.grav = carve<float4>(p, n);
+  d.rs_tiles_cap = (int)((n + 2047) / 2048);
+  d.rs_hist = carve<unsigned>(p, 256 * (size_t)d.rs_tiles_cap);
+  d.rs_tot = carve<unsigned>(p, 256);
+  d.leaf_codes = carve<unsigned>(p, L);
+  d.left = carve<unsigned>(p, L);
+  d.right = carve<unsigned>(p, L);
+  d.counters = carve<unsigned>(p, L);
+  d.groups = carve<uint2>(p, L);
+  d.ngroups = carve<unsigned>(p, 1);
+  d.parent = carve<unsigned>(p, nodes);
+  d.ncom = carve<float4>(p, nodes);
+  d.nbmin = carve<float4>(p, nodes);
+  d.nbmax = carve<float4>(p, nodes);
+  d.nq0 = carve<float4>(p, nodes);
+  d.nq1 = carve<float4>(p, nodes);
+  d.P = carve<DevParams>(p, 1);
+  return d;
+}
+
+// Everything the walk reads from DevParams, written on the device (no host copy), counters cleared.
+__global__ void k_noalloc_params(DevParams* P, float G, float soft2, float theta) {
+  DevParams p;
+  memset(&p, 0, sizeof(p));
+  p.G = G;
+  p.soft2 = soft2;
+  p.softening = sqrtf(soft2);
+  p.theta = theta;
+  p.sig_min_bits = 0x7f800000u;
+  *P = p;
+}
+
+__global__ void k_noalloc_load(const float4* __restrict__ in, int n, State st) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float4 b = in[i];
+  st.pos_h[i] = make_float4(b.x, b.y, b.z, 0.0f);
+  st.vel_u[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+  st.x[i] = (double)b.x;
+  st.y[i] = (double)b.y;
+  st.z[i] = (double)b.z;
+  st.mass[i] = b.w;
+  st.mat[i] = 0u;
+  st.prov[i] = 0u;
+  st.id[i] = (unsigned)i;
+}
+
+__global__ void k_noalloc_store(int n, const unsigned* __restrict__ id, const float4* __restrict__ grav,
+                                float4* __restrict__ out) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) out[id[t]] = grav[t];
+}
+
+int bits_for_n(uint32_t n) {
+  int b = 1;
+  while (b < 32 && (1ull << b) < (unsigned long long)n) ++b;
+  return b;
+}
+
+}  // namespace
+}  // namespace sphb
+
+using namespace sphb;
+
+extern "C" sph_status sph_gravity_tree_noalloc(const void* d_bodies4, uint32_t n, double G, float softening,
+                                               float theta, uint32_t leaf_size, uint32_t multipole, void* d_acc4,
+                                               void* stream) {
+  if (!d_bodies4 || !d_acc4 || n == 0 || !(theta > 0.0f) || !(softening >= 0.0f) || multipole > 1) {
+    return SPH_ERR_INVALID;
+  }
+  if (n > kNoAllocMaxPoints) return SPH_ERR_INVALID;  // beyond the fixed scratch array
+  if (leaf_size < kNoAllocMinLeaf || leaf_size > 32 || (leaf_size & (leaf_size - 1)) != 0) return SPH_ERR_INVALID;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return SPH_ERR_CUDA;
+  // Set-up, once per device with that device current: the device address of the scratch array.
+  if (!g_scratch_addr[dev]) {
+    void* ptr = nullptr;
+    if (cudaGetSymbolAddress(&ptr, g_noalloc_scratch) != cudaSuccess || !ptr) return SPH_ERR_CUDA;
+    g_scratch_addr[dev] = ptr;
+  }
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  Dev d = carve_dev(static_cast<unsigned char*>(g_scratch_addr[dev]), leaf_size);
+  d.n = (int)n;
+  d.cur = 0;
+  d.L = (int)((n + leaf_size - 1) / leaf_size);
+  d.idbits = bits_for_n(n);
+  Cfg c;
+  c.quad = (int)multipole;
+  c.mac = SPH_MAC_GROUP;
+  k_noalloc_params<<<1, 1, 0, s>>>(d.P, (float)G, softening * softening, theta);
+  k_noalloc_load<<<(n + 255) / 256, 256, 0, s>>>(static_cast<const float4*>(d_bodies4), (int)n, d.st[0]);
+  launch_bbox(d, s);
+  launch_sort_permute(d, s);
+  launch_tree(d, c, theta, s);
+  launch_gravity_group(d, c, s);
+  k_noalloc_store<<<(n + 255) / 256, 256, 0, s>>>((int)n, d.s().id, d.grav, static_cast<float4*>(d_acc4));
+  return cudaGetLastError() == cudaSuccess ? SPH_OK : SPH_ERR_CUDA;
+}

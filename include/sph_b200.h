@@ -220,6 +220,24 @@ sph_status sph_gravity(sph_ctx* ctx, const double* pos3, const double* mass, uin
 sph_status sph_gravity_direct64(sph_ctx* ctx, const double* pos3, const double* mass, uint32_t n,
                                 const uint32_t* targets, uint32_t n_targets, double softening, double* acc3);
 
+/* Tree gravity of a point set that allocates no memory (no counterpart in the reference).
+ *
+ * For callers that cannot allocate device memory at the point where they need forces: a real-time frame
+ * loop, where cudaMalloc/cudaFree would synchronise the device and stall the frame, or a host engine that
+ * reserves all device memory with its own allocator and hands a plug-in only the buffers it owns. The caller
+ * passes DEVICE pointers: d_bodies4 = n float4 (x, y, z, mass), d_acc4 = n float4 output (acceleration xyz,
+ * potential), in input order. The work is enqueued on `stream` (a cudaStream_t; NULL = the default stream)
+ * on the calling thread's current device; the result is ready when that stream reaches this point.
+ * Same walk as sph_gravity with SPH_MAC_GROUP (side-based θ, Barnes' δ, quadrupole if multipole = 1).
+ * Limits: n <= 65536 and leaf_size in {8, 16, 32}; larger n returns SPH_ERR_INVALID. All scratch lives in
+ * one fixed array compiled into the library (about 15 MB, held by every GPU that loads the library until
+ * the process exits). The first call on a device looks up that array's device address; make that first
+ * call before any stream capture. Every call uses the same array, so calls whose work overlaps on the GPU
+ * (different streams, or different host threads on one device) race and corrupt each other's results:
+ * order them on one stream. */
+sph_status sph_gravity_tree_noalloc(const void* d_bodies4, uint32_t n, double G, float softening, float theta,
+                                    uint32_t leaf_size, uint32_t multipole, void* d_acc4, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
