@@ -64,9 +64,23 @@ class SphProfile(C.Structure):
 # Every symbol declared in include/sph_b200.h (checked by tests/test_abi.py).
 EXPORTS = ["sph_config_default", "sph_create", "sph_destroy", "sph_upload", "sph_set_dt", "sph_set_av",
            "sph_set_omega", "sph_step_kdk", "sph_step_relax", "sph_eval_forces", "sph_readback_begin",
-           "sph_readback_take", "sph_sync", "sph_count", "sph_particle_buffer", "sph_diag", "sph_stream",
+           "sph_readback_take", "sph_readback_into", "sph_sync", "sph_count", "sph_particle_buffer", "sph_diag", "sph_stream",
            "sph_last_error", "sph_status_string", "sph_inspect", "sph_profile_enable", "sph_profile_read",
-           "sph_gravity", "sph_gravity_direct64", "sph_gravity_tree_noalloc"]
+           "sph_gravity", "sph_gravity_direct64", "sph_gravity_tree_noalloc", "sph_dem_create", "sph_dem_destroy",
+           "sph_dem_replace", "sph_dem_set_params", "sph_dem_step", "sph_dem_readback", "sph_dem_contacts",
+           "sph_dem_count"]
+
+# 80-byte grain layout (particle_step.wgsl:127-137)
+GRAIN_DTYPE = np.dtype([("offset", "<f4", (3,)), ("u", "<f4"), ("vel", "<f4", (3,)), ("resting", "<f4"),
+                        ("color", "<f4", (3,)), ("material", "<f4"), ("emission", "<f4", (3,)), ("rho", "<f4"),
+                        ("radius", "<f4"), ("_p", "<f4", (3,))])
+assert GRAIN_DTYPE.itemsize == 80
+
+
+class DemParams(C.Structure):
+    _fields_ = [("gravity", C.c_float * 3), ("dt", C.c_float), ("c_stiffness", C.c_float),
+                ("c_normal_damp", C.c_float), ("c_friction", C.c_float), ("c_tangent_damp", C.c_float),
+                ("c_cohesion", C.c_float), ("reserved", C.c_float * 3)]
 
 _lib = None
 
@@ -94,6 +108,7 @@ def load():
     L.sph_eval_forces.argtypes = [vp]
     L.sph_readback_begin.argtypes = [vp]
     L.sph_readback_take.argtypes = [vp, vp, C.c_uint32, C.POINTER(C.c_uint32), C.POINTER(C.c_int)]
+    L.sph_readback_into.argtypes = [vp, vp, C.c_uint32, C.POINTER(C.c_uint32)]
     L.sph_sync.argtypes = [vp, C.c_uint32]
     L.sph_count.argtypes = [vp]
     L.sph_count.restype = C.c_uint32
@@ -112,8 +127,20 @@ def load():
     L.sph_gravity_direct64.argtypes = [vp, vp, vp, C.c_uint32, vp, C.c_uint32, C.c_double, vp]
     L.sph_gravity_tree_noalloc.argtypes = [vp, C.c_uint32, C.c_double, C.c_float, C.c_float, C.c_uint32, C.c_uint32,
                                            vp, vp]
+    L.sph_dem_create.argtypes = [C.c_uint32, C.c_int32, C.POINTER(vp)]
+    L.sph_dem_destroy.argtypes = [vp]
+    L.sph_dem_destroy.restype = None
+    L.sph_dem_replace.argtypes = [vp, vp, C.c_uint32]
+    L.sph_dem_set_params.argtypes = [vp, C.POINTER(DemParams)]
+    L.sph_dem_step.argtypes = [vp, C.c_uint32]
+    L.sph_dem_readback.argtypes = [vp, vp, C.c_uint32, C.POINTER(C.c_uint32)]
+    L.sph_dem_contacts.argtypes = [vp, vp, C.c_size_t]
+    L.sph_dem_count.argtypes = [vp]
+    L.sph_dem_count.restype = C.c_uint32
+    no_status = ("sph_destroy", "sph_count", "sph_stream", "sph_last_error", "sph_status_string", "sph_dem_destroy",
+                 "sph_dem_count")
     for name in EXPORTS:
-        if name not in ("sph_destroy", "sph_count", "sph_stream", "sph_last_error", "sph_status_string"):
+        if name not in no_status:
             getattr(L, name).restype = C.c_int
     _lib = L
     return L

@@ -81,7 +81,8 @@ int launch_eos_only(const Dev& d, cudaStream_t s) {
 template <int KERNEL>
 __global__ void k_h_iter(int n, State st, const unsigned* __restrict__ nbr, const unsigned* __restrict__ nbr_cnt,
                          unsigned cap, const float* __restrict__ h0, float eta, float skin, DevParams* P,
-                         float* __restrict__ hnew, int last) {
+                         float* __restrict__ hnew, int last, const Eos* __restrict__ eos, float* __restrict__ rho_out,
+                         float4* __restrict__ fdata) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   float res = 0.0f;
   if (t < n) {
@@ -107,7 +108,11 @@ __global__ void k_h_iter(int n, State st, const unsigned* __restrict__ nbr, cons
     const float f = rho - rt;
     res = fabsf(f) / fmaxf(rho, 1.0e-30f);
     float hn = h;
-    if (!last) {
+    if (last) {
+      // the final pass is the density pass: same sum, same order as k_density_eos
+      rho_out[t] = rho;
+      fdata[t] = eos_record(eos, st.mat[t], m, rho, st.vel_u[t].w, P);
+    } else {
       const float fp = drho + 3.0f * rt / h;
       hn = fabsf(fp) > 0.0f ? h - f / fp : h;
       if (!(hn == hn)) hn = h;  // NaN guard
@@ -138,10 +143,10 @@ int launch_h_solve(const Dev& d, const Cfg& c, cudaStream_t s) {
     k_h_reset<<<1, 1, 0, s>>>(d.P, c.h_iters);
     if (c.kernel == 1)
       k_h_iter<1><<<blocks, 256, 0, s>>>(d.n, d.s(), d.nbr, d.nbr_cnt, d.nbr_cap, d.h0, c.h_eta, c.skin, d.P, d.hnew,
-                                          last);
+                                          last, d.eos, d.rho, d.fdata);
     else
       k_h_iter<0><<<blocks, 256, 0, s>>>(d.n, d.s(), d.nbr, d.nbr_cnt, d.nbr_cap, d.h0, c.h_eta, c.skin, d.P, d.hnew,
-                                          last);
+                                          last, d.eos, d.rho, d.fdata);
     if (!last) k_h_commit<<<blocks, 256, 0, s>>>(d.n, d.s(), d.hnew);
   }
   k_h_publish<<<1, 1, 0, s>>>(d.P);

@@ -381,7 +381,7 @@ static void walk(const Dev& d, const Cfg& c, cudaStream_t s) {
   const State& st = d.s();
   k_tree_walk<GRAV, QUAD, NBR, HILO><<<blocks, TW_WARPS * 32, smem, s>>>(
       d.body, st.pos_h, st.x, st.y, st.z, d.n, d.K, d.L, d.left, d.right, d.ncom, d.nbmin, d.nbmax, d.nq0, d.nq1,
-      d.P, d.grav, d.nbr, d.nbr_cnt, d.nbr_cap, c.h_solve ? c.skin : 0.0f, d.h0, d.groups, d.ngroups);
+      d.P, d.grav, d.nbr, d.nbr_cnt, d.nbr_cap, c.h_solve ? c.skin : c.nbr_skin, d.h0, d.groups, d.ngroups);
 }
 
 // Gravity (group MAC) fused with the neighbour lists.

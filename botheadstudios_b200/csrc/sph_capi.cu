@@ -218,8 +218,9 @@ sph_status rebuild(sph_ctx* ctx, bool need_bbox) {
     return 0;
   });
   if (!fused) phase(ctx, SPH_PHASE_NEIGHBOURS, [&] { return launch_neighbours(d, c, s); });
+  // with the smoothing-length solve, its final (residual) pass is the density + EOS pass
   if (c.h_solve) phase(ctx, SPH_PHASE_HSOLVE, [&] { return launch_h_solve(d, c, s); });
-  phase(ctx, SPH_PHASE_DENSITY, [&] { return launch_density_eos(d, c, s); });
+  else phase(ctx, SPH_PHASE_DENSITY, [&] { return launch_density_eos(d, c, s); });
   CK(cudaGetLastError());
   return SPH_OK;
 }
@@ -515,6 +516,20 @@ sph_status sph_readback_take(sph_ctx* ctx, SphParticle48* out, uint32_t cap, uin
   *ready = 1;
   ctx->rb_inflight = false;
   return m < ctx->rb_n ? SPH_CLAMPED : SPH_OK;
+}
+
+sph_status sph_readback_into(sph_ctx* ctx, SphParticle48* out, uint32_t cap, uint32_t* n_out) {
+  if (!ctx || !out || !n_out) return SPH_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  *n_out = 0;
+  const uint32_t m = (uint32_t)ctx->d.n < cap ? (uint32_t)ctx->d.n : cap;
+  if (m) {
+    launch_to_aos(ctx->d, ctx->stream);
+    CK(cudaMemcpyAsync(out, ctx->d.aos, (size_t)m * 48, cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  CK(cudaStreamSynchronize(ctx->stream));
+  *n_out = m;
+  return m < (uint32_t)ctx->d.n ? SPH_CLAMPED : SPH_OK;
 }
 
 sph_status sph_sync(sph_ctx* ctx, uint32_t timeout_ms) {
@@ -862,6 +877,161 @@ sph_status sph_gravity_direct64(sph_ctx* ctx, const double* pos3, const double* 
   cudaError_t e2 = cudaStreamSynchronize(s);
   if (e == cudaSuccess) e = e2;
   if (e != cudaSuccess) return cuda_fail(ctx, e, "sph_gravity_direct64");
+  return SPH_OK;
+}
+
+}  // extern "C"
+
+// ---- granular contact context ---------------------------------------------------------------------------
+// A grain set rides on an SPH context's sorted state, tree and neighbour lists (h = 2r + COH_RANGE); the
+// 80-byte grain records stay resident in original order and receive positions/velocities on readback.
+struct sph_dem {
+  sph_ctx* base = nullptr;
+  DemParams p{};
+  void* grains = nullptr;   // [cap] SphGrain80, original order
+  float4* acc = nullptr;    // [cap][4] contact sums of the last substep (sorted order)
+  uint32_t capacity = 0;
+};
+
+extern "C" {
+
+sph_status sph_dem_create(uint32_t capacity, int32_t device, sph_dem** out) {
+  if (!out) return SPH_ERR_INVALID;
+  *out = nullptr;
+  sph_config cfg;
+  sph_config_default(&cfg);
+  cfg.leaf_size = 8;
+  cfg.gravity = SPH_GRAVITY_NONE;
+  cfg.mac = SPH_MAC_GROUP;
+  cfg.max_neighbours = 64;
+  cfg.device = device;
+  sph_dem* dem = new (std::nothrow) sph_dem();
+  if (!dem) return SPH_ERR_OOM;
+  sph_status st = sph_create(&cfg, capacity, &dem->base);
+  if (st != SPH_OK) {
+    delete dem;
+    return st;
+  }
+  sph_ctx* ctx = dem->base;
+  ctx->kc.nbr_skin = 1.0e-5f;  // contact candidates: a superset of the exact cut applied per pair
+  dem->capacity = ctx->capacity;
+  const size_t capw = ((size_t)dem->capacity + 31) / 32 * 32;
+  uint8_t* g = nullptr;
+  st = dalloc(ctx, &g, capw * 80);
+  if (st == SPH_OK) st = dalloc(ctx, &dem->acc, capw * 4);
+  if (st != SPH_OK) {
+    sph_dem_destroy(dem);
+    return st;
+  }
+  dem->grains = g;
+  dem->p.dt = 1.0f / 60.0f;
+  dem->p.gy = -9.81f;
+  *out = dem;
+  return SPH_OK;
+}
+
+void sph_dem_destroy(sph_dem* dem) {
+  if (!dem) return;
+  sph_destroy(dem->base);
+  delete dem;
+}
+
+uint32_t sph_dem_count(const sph_dem* dem) { return dem ? (uint32_t)dem->base->d.n : 0u; }
+
+sph_status sph_dem_set_params(sph_dem* dem, const sph_dem_params* p) {
+  if (!dem || !p || !(p->dt > 0.0f) || !std::isfinite(p->dt)) return SPH_ERR_INVALID;
+  DemParams& q = dem->p;
+  q.gx = p->gravity[0];
+  q.gy = p->gravity[1];
+  q.gz = p->gravity[2];
+  q.dt = p->dt;
+  q.stiffness = p->c_stiffness;
+  q.normal_damp = p->c_normal_damp;
+  q.friction = p->c_friction;
+  q.tangent_damp = p->c_tangent_damp;
+  q.cohesion = p->c_cohesion;
+  return SPH_OK;
+}
+
+sph_status sph_dem_replace(sph_dem* dem, const SphGrain80* grains, uint32_t n) {
+  if (!dem || (!grains && n)) return SPH_ERR_INVALID;
+  sph_ctx* ctx = dem->base;
+  cudaSetDevice(ctx->device);
+  sph_status ret = SPH_OK;
+  if (n > dem->capacity) {
+    n = dem->capacity;
+    ret = SPH_CLAMPED;
+  }
+  for (uint32_t i = 0; i < n; ++i) {
+    const SphGrain80& g = grains[i];
+    if (!std::isfinite(g.offset[0]) || !std::isfinite(g.offset[1]) || !std::isfinite(g.offset[2]) ||
+        !std::isfinite(g.vel[0]) || !std::isfinite(g.vel[1]) || !std::isfinite(g.vel[2]) || !(g.radius > 0.0f) ||
+        !std::isfinite(g.radius)) {
+      ctx->err = "grain " + std::to_string(i) + " has a non-finite field or a non-positive radius";
+      return SPH_ERR_INVALID;
+    }
+  }
+  CK(cudaStreamSynchronize(ctx->stream));
+  Dev& d = ctx->d;
+  d.n = (int)n;
+  d.cur = 0;
+  d.L = n ? (int)((n + d.K - 1) / d.K) : 0;
+  d.idbits = bits_for(n);
+  if (n) {
+    CK(cudaMemcpyAsync(dem->grains, grains, (size_t)n * 80, cudaMemcpyHostToDevice, ctx->stream));
+    launch_dem_load(d, dem->grains, ctx->stream);
+  }
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(ctx->stream));
+  ctx->uploaded = true;
+  ctx->fresh = false;
+  return ret;
+}
+
+sph_status sph_dem_step(sph_dem* dem, uint32_t substeps) {
+  if (!dem) return SPH_ERR_INVALID;
+  sph_ctx* ctx = dem->base;
+  sph_status st = check_ready(ctx);
+  if (st != SPH_OK) return st;
+  Dev& d = ctx->d;
+  cudaStream_t s = ctx->stream;
+  for (uint32_t k = 0; k < substeps; ++k) {
+    phase(ctx, SPH_PHASE_SORT, [&] { return launch_bbox(d, s) + launch_sort_permute(d, s); });
+    phase(ctx, SPH_PHASE_TREE, [&] { return launch_tree(d, ctx->kc, ctx->cfg.theta, s); });
+    phase(ctx, SPH_PHASE_NEIGHBOURS, [&] { return launch_neighbours(d, ctx->kc, s); });
+    phase(ctx, SPH_PHASE_FORCES, [&] { return launch_dem_contacts(d, dem->p, dem->acc, s); });
+    phase(ctx, SPH_PHASE_INTEGRATE, [&] { return launch_dem_integrate(d, dem->p, dem->acc, s); });
+  }
+  CK(cudaGetLastError());
+  return SPH_OK;
+}
+
+sph_status sph_dem_readback(sph_dem* dem, SphGrain80* out, uint32_t cap, uint32_t* n_out) {
+  if (!dem || !out || !n_out) return SPH_ERR_INVALID;
+  sph_ctx* ctx = dem->base;
+  cudaSetDevice(ctx->device);
+  const uint32_t n = (uint32_t)ctx->d.n;
+  const uint32_t m = n < cap ? n : cap;
+  *n_out = 0;
+  if (n) launch_dem_store(ctx->d, dem->grains, ctx->stream);
+  if (m) CK(cudaMemcpyAsync(out, dem->grains, (size_t)m * 80, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  *n_out = m;
+  return m < n ? SPH_CLAMPED : SPH_OK;
+}
+
+sph_status sph_dem_contacts(sph_dem* dem, float* out16, size_t bytes) {
+  if (!dem || !out16) return SPH_ERR_INVALID;
+  sph_ctx* ctx = dem->base;
+  cudaSetDevice(ctx->device);
+  const size_t n = (size_t)ctx->d.n;
+  if (bytes < n * 64) return SPH_ERR_INVALID;
+  CK(cudaStreamSynchronize(ctx->stream));
+  std::vector<float4> a(4 * n);
+  std::vector<unsigned> ids(n);
+  CK(cudaMemcpy(a.data(), dem->acc, n * 64, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(ids.data(), ctx->d.s().id, n * 4, cudaMemcpyDeviceToHost));
+  for (size_t t = 0; t < n; ++t) std::memcpy(out16 + 16 * (size_t)ids[t], &a[4 * t], 64);
   return SPH_OK;
 }
 

@@ -74,7 +74,18 @@ struct Cfg {
   int h_iters = 4;
   float skin = 0.0f;    // neighbour-list radius inflation (h-solve)
   int mac = 0;          // 0 group walk, 1 per-particle reference walk
+  float nbr_skin = 0.0f;  // list inflation without the h-solve (grain contacts: a superset, cut exactly later)
 };
+
+// Grain contact constants (the reference's GpuStepParams subset used by the contact law and solve).
+struct DemParams {
+  float gx, gy, gz, dt;
+  float stiffness, normal_damp, friction, tangent_damp, cohesion;
+};
+int launch_dem_load(const Dev& d, const void* grains, cudaStream_t s);
+int launch_dem_store(const Dev& d, void* grains, cudaStream_t s);
+int launch_dem_contacts(const Dev& d, const DemParams& p, float4* acc, cudaStream_t s);
+int launch_dem_integrate(const Dev& d, const DemParams& p, const float4* acc, cudaStream_t s);
 
 // ---- tree ------------------------------------------------------------------------------------------
 int launch_bbox_reset(const Dev& d, cudaStream_t s);

@@ -95,6 +95,13 @@ class GpuSph:
         self._check(st, "sph_readback_take")
         return out[: n.value]
 
+    def readback_into(self, out: np.ndarray) -> int:
+        """Blocking readback straight into `out` (a PARTICLE_DTYPE array, ideally in pinned memory)."""
+        assert out.dtype == PARTICLE_DTYPE and out.flags["C_CONTIGUOUS"]
+        n = C.c_uint32()
+        self._check(self._L.sph_readback_into(self._h, _ptr(out), len(out), C.byref(n)), "sph_readback_into")
+        return int(n.value)
+
     def readback(self) -> np.ndarray:
         """Blocking convenience: begin, sync, take."""
         self.begin_readback()

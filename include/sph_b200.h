@@ -126,7 +126,8 @@ void sph_destroy(sph_ctx* ctx);
 
 /* GpuSph::upload (gpu_sph.rs:839-851): copy particles (AoS, host) and the material table in. Like the
  * reference's ParticleStore::replace it keeps the first `capacity` particles and the first 16 materials,
- * and then returns SPH_CLAMPED. A particle whose mat is outside the table is SPH_ERR_INVALID. */
+ * and then returns SPH_CLAMPED. A particle whose mat is outside the table is SPH_ERR_INVALID. The next step
+ * rebuilds everything from the uploaded state. */
 sph_status sph_upload(sph_ctx* ctx, const SphParticle48* particles, uint32_t n, const SphEos48* eos,
                       uint32_t n_eos, float softening);
 
@@ -148,6 +149,10 @@ sph_status sph_eval_forces(sph_ctx* ctx);
  * flight; take returns SPH_NOT_READY with *ready = 0 until it lands. */
 sph_status sph_readback_begin(sph_ctx* ctx);
 sph_status sph_readback_take(sph_ctx* ctx, SphParticle48* out, uint32_t cap, uint32_t* n_out, int* ready);
+
+/* Blocking readback straight into caller memory (pinned memory gets a direct DMA): the live particles in
+ * original order. Same data as begin/take, without the library's staging copy. */
+sph_status sph_readback_into(sph_ctx* ctx, SphParticle48* out, uint32_t cap, uint32_t* n_out);
 
 /* Wait for all enqueued work (timeout_ms = 0 waits without limit). */
 sph_status sph_sync(sph_ctx* ctx, uint32_t timeout_ms);
@@ -219,6 +224,48 @@ sph_status sph_gravity(sph_ctx* ctx, const double* pos3, const double* mass, uin
  * oracle of the gravity tree). targets may be NULL (all particles). */
 sph_status sph_gravity_direct64(sph_ctx* ctx, const double* pos3, const double* mass, uint32_t n,
                                 const uint32_t* targets, uint32_t n_targets, double softening, double* acc3);
+
+/* ---- Granular (DEM) contact: GpuParticles (crates/engine/src/gpu_particles.rs:46-325) over the grain
+ * pipeline of shaders/particle_step.wgsl (contact_accel :167-211, cs_forces :273-336, the implicit velocity
+ * solve of cs_integrate :477-530). Terrain contact, air drag, cooling and render expansion (the ground
+ * scene) are not part of this path. */
+/* particle_step.wgsl:127-137 `Particle` (80 bytes). */
+typedef struct SphGrain80 {
+  float offset[3];
+  float u;
+  float vel[3];
+  float resting;
+  float color[3];
+  float material;
+  float emission[3];
+  float rho;
+  float radius;
+  float _p0, _p1, _p2;
+} SphGrain80;
+/* The contact constants of GpuStepParams (particle_step.wgsl:1-25) this path uses: per-mass stiffness (1/s²),
+ * normal damping (1/s), Coulomb μ, tangential damping (1/s), cohesion (1/s²), substep dt, gravity. */
+typedef struct sph_dem_params {
+  float gravity[3];
+  float dt;
+  float c_stiffness, c_normal_damp, c_friction, c_tangent_damp, c_cohesion;
+  float reserved[3];
+} sph_dem_params;
+typedef struct sph_dem sph_dem;
+/* GpuParticles::new (gpu_particles.rs:67). */
+sph_status sph_dem_create(uint32_t capacity, int32_t device, sph_dem** out);
+void sph_dem_destroy(sph_dem* dem);
+/* GpuParticles::replace (:325): clamps to capacity (SPH_CLAMPED). */
+sph_status sph_dem_replace(sph_dem* dem, const SphGrain80* grains, uint32_t n);
+/* GpuParticles::set_params (:304). */
+sph_status sph_dem_set_params(sph_dem* dem, const sph_dem_params* p);
+/* GpuParticles::dispatch (:255): `substeps` × (contact gather, implicit velocity solve, drift). */
+sph_status sph_dem_step(sph_dem* dem, uint32_t substeps);
+/* begin_readback/take_readback (:314-320), blocking: the grains in original order. */
+sph_status sph_dem_readback(sph_dem* dem, SphGrain80* out, uint32_t cap, uint32_t* n_out);
+/* The contact sums of the last substep (the reference's Accum: force.xyz, headroom, s_diag.xyz, 0,
+ * s_off.xyz, 0, sv_nbr.xyz, 0 — 16 floats per grain, original order), for verification. */
+sph_status sph_dem_contacts(sph_dem* dem, float* out16, size_t bytes);
+uint32_t sph_dem_count(const sph_dem* dem);
 
 /* Tree gravity of a point set that allocates no memory (no counterpart in the reference).
  *

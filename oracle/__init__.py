@@ -357,3 +357,30 @@ def conservation64(pos3, vel3, mass, u, soft=0.0, G=6.674e-11, with_pe=True):
     lib().orc_conservation64(_c(pos3, np.float64), _c(vel3, np.float64), _c(mass, np.float64), _c(u, np.float64),
                              len(mass), soft, G, int(with_pe), out)
     return out
+
+
+# ---- granular contact (particle_step.wgsl) ----------------------------------------------------------------
+def dem_params(stiffness, normal_damp, friction, tangent_damp, cohesion, dt, gravity=(0.0, -9.81, 0.0)):
+    return np.array([stiffness, normal_damp, friction, tangent_damp, cohesion, dt, *gravity], np.float32)
+
+
+def dem_contacts32(pos3, vel3, radius, prm):
+    L = lib()
+    L.orc_dem_contacts32.argtypes = [f32p, f32p, f32p, C.c_int, f32p, f32p]
+    n = len(radius)
+    acc = np.zeros((n, 16), np.float32)
+    L.orc_dem_contacts32(_c(pos3, np.float32), _c(vel3, np.float32), _c(radius, np.float32), n,
+                         _c(prm, np.float32), acc)
+    return acc
+
+
+def dem_step32(pos3, vel3, radius, prm, substeps=1):
+    """contacts + integrate, `substeps` times (the reference's dispatch without terrain/drag/cooling)."""
+    L = lib()
+    L.orc_dem_integrate32.argtypes = [f32p, f32p, f32p, C.c_int, f32p]
+    pos = np.array(pos3, np.float32, order="C")
+    vel = np.array(vel3, np.float32, order="C")
+    for _ in range(substeps):
+        acc = dem_contacts32(pos, vel, radius, prm)
+        L.orc_dem_integrate32(pos, vel, acc, len(radius), _c(prm, np.float32))
+    return pos, vel

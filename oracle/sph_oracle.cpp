@@ -1055,4 +1055,81 @@ void orc_conservation64(const double* pos3, const double* vel3, const double* ma
   for (int k = 0; k < 3; ++k) { out[3 + k] = p[k]; out[6 + k] = L[k]; }
 }
 
+// ---- granular contact (shaders/particle_step.wgsl:140-211 contact_accel, :273-336 cs_forces, :477-530
+// cs_integrate without terrain, drag, cooling and render state) ----------------------------------------
+// params: [c_stiffness, c_normal_damp, c_friction, c_tangent_damp, c_cohesion, dt, gx, gy, gz]
+// accum16 per grain: force.xyz, headroom, s_diag.xyz, 0, s_off.xyz (xy, xz, yz), 0, sv_nbr.xyz, 0
+static const float kDemTheta = 0.70f;                       // particle_step.wgsl:125
+static const float kDemCohRange = 0.15f;                    // particle_step.wgsl:163
+static void dem_contact32(const float* pi, const float* vi, float ri, const float* pj, const float* vj, float rj,
+                          const float* prm, float* acc) {
+  const float d[3] = {pi[0] - pj[0], pi[1] - pj[1], pi[2] - pj[2]};
+  const float dist = std::sqrt((d[0] * d[0] + d[1] * d[1]) + d[2] * d[2]);
+  const float touch = ri + rj;
+  if (dist >= touch + kDemCohRange || dist < 1.0e-9f) return;
+  const float nrm[3] = {d[0] / dist, d[1] / dist, d[2] / dist};
+  const float overlap = touch - dist;
+  const float vr[3] = {vi[0] - vj[0], vi[1] - vj[1], vi[2] - vj[2]};
+  const float v_n = (vr[0] * nrm[0] + vr[1] * nrm[1]) + vr[2] * nrm[2];
+  const float f_rep = prm[0] * std::max(overlap, 0.0f);
+  const float sep = std::max(-overlap, 0.0f);
+  const float f_coh = prm[4] * std::min(std::max(1.0f - sep / kDemCohRange, 0.0f), 1.0f);
+  const float normal_load = f_rep + f_coh;
+  const float vt[3] = {vr[0] - nrm[0] * v_n, vr[1] - nrm[1] * v_n, vr[2] - nrm[2] * v_n};
+  const float vt_mag = std::sqrt((vt[0] * vt[0] + vt[1] * vt[1]) + vt[2] * vt[2]);
+  float at[3] = {0, 0, 0};
+  if (vt_mag > 1.0e-9f) {
+    const float mag = std::min(std::min(prm[3] * vt_mag, prm[2] * normal_load), vt_mag / prm[5]);
+    for (int k = 0; k < 3; ++k) at[k] = -(vt[k] / vt_mag) * mag;
+  }
+  for (int k = 0; k < 3; ++k) acc[k] += nrm[k] * (f_rep - f_coh) + at[k];
+  if (overlap > 0.0f) {
+    const float dt = prm[5];
+    const float g = kDemTheta * kDemTheta * dt * dt * prm[0] + kDemTheta * dt * prm[1];
+    acc[4] += g * nrm[0] * nrm[0];
+    acc[5] += g * nrm[1] * nrm[1];
+    acc[6] += g * nrm[2] * nrm[2];
+    acc[8] += g * (nrm[0] * nrm[1]);
+    acc[9] += g * (nrm[0] * nrm[2]);
+    acc[10] += g * (nrm[1] * nrm[2]);
+    const float ndv = (nrm[0] * vj[0] + nrm[1] * vj[1]) + nrm[2] * vj[2];
+    for (int k = 0; k < 3; ++k) acc[12 + k] += g * ndv * nrm[k];
+  }
+}
+void orc_dem_contacts32(const float* pos3, const float* vel3, const float* radius, int n, const float* prm,
+                        float* accum16) {
+  for (int i = 0; i < n; ++i) {
+    float* acc = accum16 + 16 * (size_t)i;
+    for (int k = 0; k < 16; ++k) acc[k] = 0.0f;
+    acc[3] = 1.0e30f;
+    for (int j = 0; j < n; ++j)
+      if (j != i) dem_contact32(&pos3[3 * i], &vel3[3 * i], radius[i], &pos3[3 * j], &vel3[3 * j], radius[j], prm, acc);
+  }
+}
+// cs_integrate's directional trapezoidal solve (I+S)v' = v − ρSv + (1/θ)Σ S_c v_j + dt·a; x += dt(v+v')/2.
+void orc_dem_integrate32(float* pos3, float* vel3, const float* accum16, int n, const float* prm) {
+  const float rho_t = (1.0f - kDemTheta) / kDemTheta, dt = prm[5];
+  for (int i = 0; i < n; ++i) {
+    const float* a = accum16 + 16 * (size_t)i;
+    float* v = vel3 + 3 * i;
+    const float acc[3] = {prm[6] + a[0], prm[7] + a[1], prm[8] + a[2]};
+    const float sdx = a[4], sdy = a[5], sdz = a[6], sxy = a[8], sxz = a[9], syz = a[10];
+    const float sv[3] = {sdx * v[0] + sxy * v[1] + sxz * v[2], sxy * v[0] + sdy * v[1] + syz * v[2],
+                         sxz * v[0] + syz * v[1] + sdz * v[2]};
+    float rhs[3];
+    for (int k = 0; k < 3; ++k) rhs[k] = v[k] - rho_t * sv[k] + (1.0f / kDemTheta) * a[12 + k] + acc[k] * dt;
+    const float m00 = 1.0f + sdx, m11 = 1.0f + sdy, m22 = 1.0f + sdz, m01 = sxy, m02 = sxz, m12 = syz;
+    const float c00 = m11 * m22 - m12 * m12, c01 = m02 * m12 - m01 * m22, c02 = m01 * m12 - m02 * m11;
+    const float c11 = m00 * m22 - m02 * m02, c12 = m01 * m02 - m00 * m12, c22 = m00 * m11 - m01 * m01;
+    const float inv_det = 1.0f / (m00 * c00 + m01 * c01 + m02 * c02);
+    const float vn[3] = {(c00 * rhs[0] + c01 * rhs[1] + c02 * rhs[2]) * inv_det,
+                         (c01 * rhs[0] + c11 * rhs[1] + c12 * rhs[2]) * inv_det,
+                         (c02 * rhs[0] + c12 * rhs[1] + c22 * rhs[2]) * inv_det};
+    for (int k = 0; k < 3; ++k) {
+      pos3[3 * i + k] = pos3[3 * i + k] + (v[k] + vn[k]) * (0.5f * dt);
+      v[k] = vn[k];
+    }
+  }
+}
+
 }  // extern "C"

@@ -93,3 +93,25 @@ def test_ic_generator_counts_and_composition():
     assert np.abs(mom).max() < 1e-6
     r = np.linalg.norm(I.pos64[:8192] - I.pos64[:8192].mean(0), axis=1)
     assert 0.95 < r.max() < 1.1
+
+
+def test_grain_layouts_match_header():
+    prog = r"""
+#include <stdio.h>
+#include <stddef.h>
+#include "sph_b200.h"
+int main(void) {
+  printf("%zu %zu %zu %zu %zu %zu\n", sizeof(SphGrain80), offsetof(SphGrain80, radius), offsetof(SphGrain80, rho),
+         sizeof(sph_dem_params), offsetof(sph_dem_params, dt), offsetof(sph_dem_params, c_cohesion));
+  return 0;
+}
+"""
+    with tempfile.TemporaryDirectory() as d:
+        c = os.path.join(d, "g.c")
+        open(c, "w").write(prog)
+        exe = os.path.join(d, "g")
+        subprocess.run(["gcc", "-I", os.path.dirname(HEADER), c, "-o", exe], check=True)
+        vals = list(map(int, subprocess.run([exe], capture_output=True, text=True, check=True).stdout.split()))
+    g = _lib.GRAIN_DTYPE
+    assert vals == [80, g.fields["radius"][1], g.fields["rho"][1], C.sizeof(_lib.DemParams), _lib.DemParams.dt.offset,
+                    _lib.DemParams.c_cohesion.offset]
