@@ -14,10 +14,15 @@ WORKLOADS = {
     # the small plain-method impact: cubic spline, 48 neighbours, monopole θ = 0.5, one particle per leaf
     "impact_10k": dict(n_target=8_192, n_impactor=2_048, n_ngb=48.0, kernel="cubic", theta=0.5, quad=0, leaf=1,
                        h_solve=0, max_nbr=256),
+    # the precision-sweep body: a 4,194,304-particle differentiated planet at rest (θ swept by the caller)
+    "planet_4m": dict(kind="planet", n_target=4_194_304, n_impactor=0, n_ngb=64.0, kernel="wendland", theta=0.5,
+                      quad=1, leaf=16, h_solve=1, max_nbr=192),
 }
 
 
 def build(wl: dict, seed: int = 1) -> ic.Impact:
+    if wl.get("kind") == "planet":
+        return ic.planet(wl["n_target"], n_ngb=wl["n_ngb"], seed=seed)
     return ic.impact(wl["n_target"], wl["n_impactor"], n_ngb=wl["n_ngb"], seed=seed)
 
 
