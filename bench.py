@@ -8,7 +8,7 @@ positions), seeded synthetic initial conditions. One step = one KDK leapfrog ste
 as the reference's encode_kdk). Inputs are resident in HBM and the per-step working set (particle state,
 neighbour lists, tree) is larger than the 126 MB L2, so no flush is needed between steps.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload impact_1m|impact_4m|impact_10k]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload impact_1m|impact_4m|impact_10k|batch_256|...]
     python bench.py --impl reference ...    # the reference's CPU path (HydroBody::step) on the host cores
 
 Multi-GPU: replicas (one independent impact per rank, no collective on the data path); value is the sum
@@ -34,7 +34,7 @@ sys.path.insert(0, ROOT)
 METRIC = "SPH+gravity particle-steps/s"
 UNIT = "particle-steps/s"
 
-from botheadstudios_b200.workloads import WORKLOADS  # noqa: E402
+from botheadstudios_b200.workloads import WORKLOADS, n_particles  # noqa: E402
 
 # Algorithmic bytes per particle per phase execution (state read/written once, SoA f32/f64 layout):
 # sort = bbox/Morton 40 + radix (key,idx) 16 + permutation 132; tree = 20 + 304/L per particle;
@@ -157,7 +157,8 @@ def cpu_reference_run(wl: dict, sample_n: int, steps: int, warmup: int, budget_s
     import oracle
     from botheadstudios_b200 import ic
     from botheadstudios_b200.materials import eos_table64, SI
-    frac = wl["n_impactor"] / (wl["n_target"] + wl["n_impactor"])
+    from botheadstudios_b200.workloads import impactor_fraction
+    frac = impactor_fraction(wl)
     n_imp = max(int(round(sample_n * frac)), 1)
     I = ic.impact(sample_n - n_imp, n_imp, n_ngb=wl["n_ngb"], seed=2)
     U = I.units
@@ -195,7 +196,7 @@ def run_reference(args, wl, world, rank, local, pg):
     line = dict(metric=METRIC, value=r["value"], unit=UNIT, impl="reference", n_gpus=args.gpus, steps=args.steps,
                 warmup=args.warmup, ms_per_step=1000.0 * r["seconds"] / max(r["steps_run"], 1),
                 higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f64", data="synthetic",
-                config=dict(workload=args.workload, particles=wl["n_target"] + wl["n_impactor"]),
+                config=dict(workload=args.workload, particles=n_particles(wl)),
                 cpu_baseline=dict(value=r["value"], unit=UNIT, cores=r["cores"], kind="port", sample=sample),
                 e2e=dict(value=r["value"], unit=UNIT, h2d_bytes_per_step=0, d2h_bytes_per_step=0))
     print(json.dumps(line), flush=True)
@@ -204,16 +205,17 @@ def run_reference(args, wl, world, rank, local, pg):
 def run_ours(args, wl, world, rank, local, pg):
     import torch
 
+    from botheadstudios_b200.workloads import upload
     I = build_workload(wl, seed=1 + rank)
     n = len(I.particles)
     s = make_solver(wl, I, local)
-    s.upload(I.particles, I.eos, I.softening)
+    upload(s, I)
     ext = torch.cuda.ExternalStream(s.stream(), device=f"cuda:{local}")
-    # warm-up (includes the first full force evaluation)
+    # warm-up (includes the first full force evaluation, and the graph captures when graphs are on)
     s.encode_kdk(args.warmup)
     s.sync()
-    d0 = s.diag()
-    s.profile_enable(True)
+    dstart = s.diag()
+    s.profile_enable(False)  # launch count only: phase events off, so captured graphs replay
     barrier(pg)
     torch.cuda.synchronize(local)
     ev0 = torch.cuda.Event(enable_timing=True)
@@ -226,11 +228,16 @@ def run_ours(args, wl, world, rank, local, pg):
     torch.cuda.synchronize(local)
     barrier(pg)
     ms = ev0.elapsed_time(ev1)
+    launches = s.profile_read()["kernel_launches"]
+    ms_max = max_over_ranks(pg, ms, local)
+    value = n * args.steps * world / (ms_max / 1000.0)
+    # per-phase breakdown and walk counters: a few more steps with phase events (eager launches)
+    d0 = s.diag()
+    s.profile_enable(True)
+    s.encode_kdk(min(args.steps, 4))
     prof = s.profile_read()
     s.profile_enable(False)
     d1 = s.diag(check=False)
-    ms_max = max_over_ranks(pg, ms, local)
-    value = n * args.steps * world / (ms_max / 1000.0)
 
     # ---- end to end through the public API: per step, upload the state from pinned host memory, one KDK
     # step, read the state back into host memory ----
@@ -240,7 +247,10 @@ def run_ours(args, wl, world, rank, local, pg):
     barrier(pg)
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
-        s.upload(pin, I.eos, I.softening)  # H2D of the step's input state from pinned memory
+        if hasattr(I, "offsets"):          # H2D of the step's input state from pinned memory
+            s.upload_batch(pin, I.offsets, I.eos, I.softening)
+        else:
+            s.upload(pin, I.eos, I.softening)
         s.encode_kdk(1)
         s.readback_into(pin)               # D2H of the step's result into the same pinned buffer
     e2e_s = time.perf_counter() - t0
@@ -304,20 +314,21 @@ def run_ours(args, wl, world, rank, local, pg):
                    sample=f"HydroBody::step restated in C++ (f64, octree θ=0.5), 65,536-particle impact of the same "
                           f"generator, {r['steps_run']} steps in {r['seconds']:.1f} s")
     dd = d1
-    energy0 = d0["kinetic"] + d0["internal"] + d0["potential"]
+    energy0 = dstart["kinetic"] + dstart["internal"] + dstart["potential"]
     energy1 = dd["kinetic"] + dd["internal"] + dd["potential"]
     line = dict(metric=METRIC, value=value, unit=UNIT, n_gpus=world, steps=args.steps, warmup=args.warmup,
                 ms_per_step=ms_max / args.steps, higher_is_better=True, scaling="weak", vs_baseline=None,
                 dtype="f32", data="synthetic (seeded lattice impact)",
-                config=dict(workload=args.workload, particles=n, kernel=wl["kernel"], neighbours=wl["n_ngb"],
+                config=dict(workload=args.workload, particles=n, impacts=getattr(I, "n_impacts", 1),
+                            graph=bool(wl.get("graph", 0)), kernel=wl["kernel"], neighbours=wl["n_ngb"],
                             theta=wl["theta"], quadrupole=bool(wl["quad"]), leaf=wl["leaf"],
                             h_solve=bool(wl["h_solve"]), dt="adaptive CFL 0.3", parallelism=f"replicas{world}",
                             l2="working set > L2 (no flush needed)"),
                 e2e=dict(value=e2e_value, unit=UNIT, h2d_bytes_per_step=48 * n, d2h_bytes_per_step=48 * n,
                          steps=e2e_steps),
-                gpu_launches=prof["kernel_launches"], roofline=roof, roofline_hbm=roof_hbm, phases=phases, cpu_baseline=cpu,
+                gpu_launches=launches, roofline=roof, roofline_hbm=roof_hbm, phases=phases, cpu_baseline=cpu,
                 clocks=clk.summary(),
-                physics=dict(energy_drift=(energy1 - energy0) / abs(d0["potential"]) if d0["potential"] else None,
+                physics=dict(energy_drift=(energy1 - energy0) / abs(dstart["potential"]) if dstart["potential"] else None,
                              sim_time=dd["time"], dt=dd["dt"], max_neighbours=dd["max_neighbours_seen"],
                              overflow_flags=dd["overflow_flags"], h_residual=dd["h_residual"]))
     print(json.dumps(line), flush=True)

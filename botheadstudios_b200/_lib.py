@@ -25,7 +25,9 @@ SPH_ERR_STATE = -6
 
 # Inspection selectors (SPH_Q_*)
 Q = dict(BBOX=0, CODES=1, ORDER=2, LEFT=3, RIGHT=4, PARENT=5, NODE_COM=6, NODE_BMIN=7, NODE_BMAX=8,
-         NBR_COUNT=9, NBR_LIST=10, RHO=11, PRESSURE=12, SOUND=13, ACC_SPH=14, ACC_GRAV=15, H=16, N_LEAVES=17)
+         NBR_COUNT=9, NBR_LIST=10, RHO=11, PRESSURE=12, SOUND=13, ACC_SPH=14, ACC_GRAV=15, H=16, N_LEAVES=17,
+         IMPACT_DT=18, IMPACT_TIME=19)
+MAX_IMPACTS = 256  # SPH_MAX_IMPACTS
 
 KERNEL = dict(cubic=0, wendland=1)
 GRAVITY = dict(tree=0, direct=1, none=2)
@@ -42,7 +44,7 @@ class SphConfig(C.Structure):
                 ("h_mode", C.c_uint32), ("h_neighbours", C.c_float), ("h_tol", C.c_float),
                 ("h_iters", C.c_uint32), ("max_neighbours", C.c_uint32), ("cfl", C.c_float),
                 ("rho_floor", C.c_float), ("du_floor", C.c_float), ("r_min", C.c_float), ("sig_floor", C.c_float),
-                ("device", C.c_int32), ("mac", C.c_uint32), ("reserved", C.c_uint32 * 6)]
+                ("device", C.c_int32), ("mac", C.c_uint32), ("graph", C.c_uint32), ("reserved", C.c_uint32 * 5)]
 
 
 class SphDiag(C.Structure):
@@ -62,7 +64,8 @@ class SphProfile(C.Structure):
 
 
 # Every symbol declared in include/sph_b200.h (checked by tests/test_abi.py).
-EXPORTS = ["sph_config_default", "sph_create", "sph_destroy", "sph_upload", "sph_set_dt", "sph_set_av",
+EXPORTS = ["sph_config_default", "sph_create", "sph_destroy", "sph_upload", "sph_upload_batch", "sph_set_dt",
+           "sph_set_av",
            "sph_set_omega", "sph_step_kdk", "sph_step_relax", "sph_eval_forces", "sph_readback_begin",
            "sph_readback_take", "sph_readback_into", "sph_sync", "sph_count", "sph_particle_buffer", "sph_diag", "sph_stream",
            "sph_last_error", "sph_status_string", "sph_inspect", "sph_profile_enable", "sph_profile_read",
@@ -100,6 +103,7 @@ def load():
     L.sph_destroy.argtypes = [vp]
     L.sph_destroy.restype = None
     L.sph_upload.argtypes = [vp, vp, C.c_uint32, vp, C.c_uint32, C.c_float]
+    L.sph_upload_batch.argtypes = [vp, vp, vp, C.c_uint32, vp, C.c_uint32, vp]
     L.sph_set_dt.argtypes = [vp, C.c_double, C.c_float]
     L.sph_set_av.argtypes = [vp, C.c_float, C.c_float]
     L.sph_set_omega.argtypes = [vp, C.c_float]

@@ -30,6 +30,7 @@ __global__ void k_dem_load(int n, const G80* __restrict__ in, State st) {
   st.mat[i] = 0u;
   st.prov[i] = 0u;
   st.id[i] = (unsigned)i;
+  st.seg[i] = 0u;
 }
 
 __global__ void k_dem_store(int n, State st, G80* __restrict__ io) {

@@ -33,7 +33,8 @@ struct Comp3 {
 template <bool QUAD, bool HILO>
 __global__ void __launch_bounds__(GR_WARPS * 32) k_gravity_tree(
     const float4* __restrict__ body, const double* __restrict__ x64, const double* __restrict__ y64,
-    const double* __restrict__ z64, int n, int K, int L, const unsigned* __restrict__ left,
+    const double* __restrict__ z64, int n, int L, const unsigned* __restrict__ leaf_start,
+    const unsigned* __restrict__ seg, const Seg* __restrict__ segs, const unsigned* __restrict__ left,
     const unsigned* __restrict__ right, const float4* __restrict__ ncom, const float4* __restrict__ nbmax,
     const float4* __restrict__ nq0, const float4* __restrict__ nq1, const DevParams* __restrict__ P,
     float4* __restrict__ out) {
@@ -52,15 +53,23 @@ __global__ void __launch_bounds__(GR_WARPS * 32) k_gravity_tree(
     ylo = (float)(y64[t] - (double)pi.y);
     zlo = (float)(z64[t] - (double)pi.z);
   }
-  const float G = P->G, soft2 = P->soft2;
+  const unsigned sg = valid ? seg[t] : kNoSeg;
+  const float G = P->G, soft2 = valid ? segs[sg].soft2 : 0.0f;
   const unsigned leaf0 = (unsigned)(L - 1);
   float ax = 0.f, ay = 0.f, az = 0.f, phi = 0.f;
   Comp3 acc;
   uint2* stack = s_stack[wib];
   int sp = 0;
-  const unsigned all = __ballot_sync(SPH_FULL_MASK, valid);
-  if (lane == 0) stack[0] = make_uint2(0u, all);
-  sp = 1;
+  // one start entry per impact present in the warp: that impact's root with the mask of its lanes (a lane
+  // sees only its own impact's entry, so its walk is the one it would take alone)
+  unsigned todo = __ballot_sync(SPH_FULL_MASK, valid);
+  while (todo) {
+    const unsigned s = __shfl_sync(SPH_FULL_MASK, sg, __ffs(todo) - 1);
+    const unsigned m = __ballot_sync(SPH_FULL_MASK, valid && sg == s);
+    if (lane == 0) stack[sp] = make_uint2(segs[s].root, m);
+    ++sp;
+    todo &= ~m;
+  }
   __syncwarp();
   unsigned overflow = 0;
   while (sp > 0) {
@@ -71,7 +80,7 @@ __global__ void __launch_bounds__(GR_WARPS * 32) k_gravity_tree(
     if (node >= leaf0) {
       // leaf bucket: exact pairwise sum over its <= K sorted particles, skipping self
       const int c = (int)(node - leaf0);
-      const int s0 = c * K, s1 = min(s0 + K, n);
+      const int s0 = (int)leaf_start[c], s1 = (int)leaf_start[c + 1];
       if (in) {
         for (int s = s0; s < s1; ++s) {
           if (s == t) continue;
@@ -178,7 +187,8 @@ int launch_gravity_tree(const Dev& d, const Cfg& c, cudaStream_t s) {
   const int blocks = (warps + GR_WARPS - 1) / GR_WARPS;
   const State& st = d.s();
 #define GRAV_ARGS                                                                                           \
-  d.body, st.x, st.y, st.z, d.n, d.K, d.L, d.left, d.right, d.ncom, d.nbmax, d.nq0, d.nq1, d.P, d.grav
+  d.body, st.x, st.y, st.z, d.n, d.L, d.leaf_start, st.seg, d.segs, d.left, d.right, d.ncom, d.nbmax, d.nq0, d.nq1, \
+      d.P, d.grav
   if (c.quad) {
     if (c.hilo) k_gravity_tree<true, true><<<blocks, GR_WARPS * 32, 0, s>>>(GRAV_ARGS);
     else k_gravity_tree<true, false><<<blocks, GR_WARPS * 32, 0, s>>>(GRAV_ARGS);
@@ -196,21 +206,30 @@ int launch_gravity_tree(const Dev& d, const Cfg& c, cudaStream_t s) {
 // ---------------------------------------------------------------------------------------------------
 constexpr int DS_TILE = 256;
 
-__global__ void __launch_bounds__(DS_TILE) k_gravity_direct(const float4* __restrict__ body, int n,
+__global__ void __launch_bounds__(DS_TILE) k_gravity_direct(const float4* __restrict__ body,
+                                                           const unsigned* __restrict__ seg, int n,
+                                                           const Seg* __restrict__ segs,
                                                            const DevParams* __restrict__ P,
                                                            float4* __restrict__ out) {
   __shared__ float4 s_b[DS_TILE];
   const int i = blockIdx.x * DS_TILE + threadIdx.x;
+  // sources: the impacts of this block's targets (sorted order keeps impacts contiguous); each target sums
+  // over its own impact only
+  const int b0 = blockIdx.x * DS_TILE, b1 = min(b0 + DS_TILE, n) - 1;
+  const int j0 = (int)segs[seg[b0]].off, j1 = (int)segs[seg[b1] + 1].off;
+  const unsigned sg = i < n ? seg[i] : seg[b0];
+  const int m0 = (int)segs[sg].off, m1 = (int)segs[sg + 1].off;
   const float4 pi = i < n ? body[i] : make_float4(0, 0, 0, 0);
-  const float G = P->G, soft2 = P->soft2;
+  const float G = P->G, soft2 = segs[sg].soft2;
   float ax = 0, ay = 0, az = 0, phi = 0;
-  for (int base = 0; base < n; base += DS_TILE) {
+  for (int base = j0; base < j1; base += DS_TILE) {
     const int j = base + threadIdx.x;
-    s_b[threadIdx.x] = j < n ? body[j] : make_float4(0, 0, 0, 0);
+    s_b[threadIdx.x] = j < j1 ? body[j] : make_float4(0, 0, 0, 0);
     __syncthreads();
-    const int cnt = min(DS_TILE, n - base);
+    const int cnt = min(DS_TILE, j1 - base);
     for (int k = 0; k < cnt; ++k) {
-      if (base + k == i) continue;
+      const int jj = base + k;
+      if (jj == i || jj < m0 || jj >= m1) continue;
       const float4 bj = s_b[k];
       const float dx = bj.x - pi.x, dy = bj.y - pi.y, dz = bj.z - pi.z;
       const float r2 = dx * dx + dy * dy + dz * dz + soft2;
@@ -227,7 +246,7 @@ __global__ void __launch_bounds__(DS_TILE) k_gravity_direct(const float4* __rest
 }
 
 int launch_gravity_direct(const Dev& d, cudaStream_t s) {
-  k_gravity_direct<<<(d.n + DS_TILE - 1) / DS_TILE, DS_TILE, 0, s>>>(d.body, d.n, d.P, d.grav);
+  k_gravity_direct<<<(d.n + DS_TILE - 1) / DS_TILE, DS_TILE, 0, s>>>(d.body, d.s().seg, d.n, d.segs, d.P, d.grav);
   return 1;
 }
 

@@ -155,14 +155,16 @@ int launch_h_solve(const Dev& d, const Cfg& c, cudaStream_t s) {
 
 // ---------------------------------------------------------------------------------------------------
 // Forces (the SPH half of cs_forces, sph_step.wgsl:170-210) + gravity + the Courant signal (cs_signal
-// :263-269) reduced to a device minimum with one atomic per warp.
+// :263-269) reduced to each impact's minimum with one atomic per warp (per lane in a warp that straddles two
+// impacts).
 // ---------------------------------------------------------------------------------------------------
 template <int KERNEL, bool GRAV>
 __global__ void k_forces(int n, State st, const float4* __restrict__ fdata, const unsigned* __restrict__ nbr,
                          const unsigned* __restrict__ nbr_cnt, unsigned cap, const float4* __restrict__ grav,
-                         DevParams* P, float4* __restrict__ acc) {
+                         const DevParams* __restrict__ P, Seg* __restrict__ segs, float4* __restrict__ acc) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   float sig = __int_as_float(0x7f800000);
+  const unsigned sg = t < n ? st.seg[t] : kNoSeg;
   if (t < n) {
     const float4 pi = st.pos_h[t];
     const float4 vi = st.vel_u[t];
@@ -207,14 +209,21 @@ __global__ void k_forces(int n, State st, const float4* __restrict__ fdata, cons
     const float vmag = sqrtf(vi.x * vi.x + vi.y * vi.y + vi.z * vi.z);
     sig = pi.w / fmaxf(fi.w + vmag, P->sig_floor);
   }
-  sig = warp_min(sig);
-  if ((threadIdx.x & 31) == 0 && sig < __int_as_float(0x7f800000)) atomicMin(&P->sig_min_bits, __float_as_uint(sig));
+  const unsigned wlo = warp_min(sg), whi = warp_max(sg == kNoSeg ? 0u : sg);
+  if (wlo == kNoSeg) return;
+  if (wlo == whi) {
+    sig = warp_min(sig);
+    if ((threadIdx.x & 31) == 0 && sig < __int_as_float(0x7f800000))
+      atomicMin(&segs[wlo].sig_bits, __float_as_uint(sig));
+  } else if (sg != kNoSeg && sig < __int_as_float(0x7f800000)) {
+    atomicMin(&segs[sg].sig_bits, __float_as_uint(sig));
+  }
 }
 
 int launch_forces(const Dev& d, const Cfg& c, cudaStream_t s) {
   const int blocks = (d.n + 255) / 256;
   const bool g = c.gravity != 2;
-#define FARGS d.n, d.s(), d.fdata, d.nbr, d.nbr_cnt, d.nbr_cap, d.grav, d.P, d.acc
+#define FARGS d.n, d.s(), d.fdata, d.nbr, d.nbr_cnt, d.nbr_cap, d.grav, d.P, d.segs, d.acc
   if (c.kernel == 1) {
     if (g) k_forces<1, true><<<blocks, 256, 0, s>>>(FARGS);
     else k_forces<1, false><<<blocks, 256, 0, s>>>(FARGS);
@@ -227,27 +236,37 @@ int launch_forces(const Dev& d, const Cfg& c, cudaStream_t s) {
 }
 
 // ---------------------------------------------------------------------------------------------------
-// Step control: dt = cfl·min signal (or the fixed dt), simulated time, reset of the reductions.
+// Step control, per impact: dt = cfl·min signal (or the fixed dt), simulated time, reset of the reductions.
 // ---------------------------------------------------------------------------------------------------
-__global__ void k_finalize_dt(DevParams* P) {
+__global__ void k_finalize_dt(DevParams* P, Seg* segs, int nseg) {
+  const int k = threadIdx.x;
+  if (k == 0) P->steps += 1u;
+  if (k >= nseg) return;
+  Seg& S = segs[k];
   double dt = P->dt_fixed;
-  if (P->cfl > 0.0f && P->sig_min_bits != 0x7f800000u) dt = (double)P->cfl * (double)__uint_as_float(P->sig_min_bits);
-  P->dt = dt;
-  P->time += dt;
-  P->steps += 1u;
-  P->sig_min_bits = 0x7f800000u;
-  P->bbox_keys[0] = P->bbox_keys[1] = P->bbox_keys[2] = 0xffffffffu;
-  P->bbox_keys[3] = P->bbox_keys[4] = P->bbox_keys[5] = 0u;
+  if (P->cfl > 0.0f && S.sig_bits != 0x7f800000u) dt = (double)P->cfl * (double)__uint_as_float(S.sig_bits);
+  S.dt = dt;
+  S.time += dt;
+  S.sig_bits = 0x7f800000u;
+  for (int a = 0; a < 3; ++a) {
+    S.bbox[a] = 0xffffffffu;
+    S.bbox[3 + a] = 0u;
+  }
 }
-int launch_finalize_dt(const Dev& d, cudaStream_t s) { k_finalize_dt<<<1, 1, 0, s>>>(d.P);  return 1; }
+int launch_finalize_dt(const Dev& d, cudaStream_t s) {
+  k_finalize_dt<<<1, kMaxSegments, 0, s>>>(d.P, d.segs, d.nseg);
+  return 1;
+}
 
-// First half-kick and drift (cs_kick_drift): v += a·dt/2, u = max(u + du·dt/2, 0), x += v·dt in f64,
-// plus the bounding box of the new positions for the next Morton pass.
-__global__ void k_kick_drift(int n, State st, const float4* __restrict__ acc, DevParams* P) {
+// First half-kick and drift (cs_kick_drift): v += a·dt/2, u = max(u + du·dt/2, 0), x += v·dt in f64 with
+// the particle's impact dt, plus each impact's bounding box of the new positions for the next Morton pass.
+__global__ void k_kick_drift(int n, State st, const float4* __restrict__ acc, Seg* segs) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   unsigned lo[3] = {0xffffffffu, 0xffffffffu, 0xffffffffu}, hi[3] = {0u, 0u, 0u};
+  unsigned sg = kNoSeg;
   if (t < n) {
-    const double dt = P->dt;
+    sg = st.seg[t];
+    const double dt = segs[sg].dt;
     const float hdt = (float)(0.5 * dt);
     const float4 a = acc[t];
     float4 v = st.vel_u[t];
@@ -269,41 +288,20 @@ __global__ void k_kick_drift(int n, State st, const float4* __restrict__ acc, De
     lo[1] = hi[1] = float_key(p.y);
     lo[2] = hi[2] = float_key(p.z);
   }
-  __shared__ unsigned s_lo[3][32], s_hi[3][32];
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-#pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    lo[k] = warp_min(lo[k]);
-    hi[k] = warp_max(hi[k]);
-    if (lane == 0) { s_lo[k][w] = lo[k]; s_hi[k][w] = hi[k]; }
-  }
-  __syncthreads();
-  if (w == 0) {
-    const int nw = blockDim.x >> 5;
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      unsigned a = lane < nw ? s_lo[k][lane] : 0xffffffffu;
-      unsigned b = lane < nw ? s_hi[k][lane] : 0u;
-      a = warp_min(a);
-      b = warp_max(b);
-      if (lane == 0) {
-        atomicMin(&P->bbox_keys[k], a);
-        atomicMax(&P->bbox_keys[3 + k], b);
-      }
-    }
-  }
+  seg_bbox_commit(lo, hi, sg, segs);
 }
 int launch_kick_drift(const Dev& d, cudaStream_t s) {
-  k_kick_drift<<<(d.n + 255) / 256, 256, 0, s>>>(d.n, d.s(), d.acc, d.P);
+  k_kick_drift<<<(d.n + 255) / 256, 256, 0, s>>>(d.n, d.s(), d.acc, d.segs);
   return 1;
 }
 
 // Final half-kick (cs_kick) with the EOS record refreshed for the new u (density is unchanged).
 __global__ void k_kick(int n, State st, const float4* __restrict__ acc, const float* __restrict__ rho,
-                       const Eos* __restrict__ eos, const DevParams* __restrict__ P, float4* __restrict__ fdata) {
+                       const Eos* __restrict__ eos, const DevParams* __restrict__ P, const Seg* __restrict__ segs,
+                       float4* __restrict__ fdata) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
-  const float hdt = (float)(0.5 * P->dt);
+  const float hdt = (float)(0.5 * segs[st.seg[t]].dt);
   const float4 a = acc[t];
   float4 v = st.vel_u[t];
   v.x = v.x + a.x * hdt;
@@ -314,7 +312,7 @@ __global__ void k_kick(int n, State st, const float4* __restrict__ acc, const fl
   fdata[t] = eos_record(eos, st.mat[t], st.mass[t], rho[t], v.w, P);
 }
 int launch_kick(const Dev& d, cudaStream_t s) {
-  k_kick<<<(d.n + 255) / 256, 256, 0, s>>>(d.n, d.s(), d.acc, d.rho, d.eos, d.P, d.fdata);
+  k_kick<<<(d.n + 255) / 256, 256, 0, s>>>(d.n, d.s(), d.acc, d.rho, d.eos, d.P, d.segs, d.fdata);
   return 1;
 }
 
@@ -354,9 +352,17 @@ struct P48 {
 };
 static_assert(sizeof(P48) == 48, "SphParticle48 is 48 bytes");
 
-__global__ void k_from_aos(int n, const P48* __restrict__ aos, State st, float* __restrict__ rho) {
+__global__ void k_from_aos(int n, const P48* __restrict__ aos, const Seg* __restrict__ segs, int nseg, State st,
+                           float* __restrict__ rho) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
+  int lo = 0, hi = nseg - 1;  // the impact holding slot i: last segment starting at or before it
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (segs[mid].off <= (unsigned)i) lo = mid;
+    else hi = mid - 1;
+  }
+  st.seg[i] = (unsigned)lo;
   const P48 p = aos[i];
   st.pos_h[i] = make_float4(p.px, p.py, p.pz, p.h);
   st.vel_u[i] = make_float4(p.vx, p.vy, p.vz, p.u);
@@ -370,7 +376,7 @@ __global__ void k_from_aos(int n, const P48* __restrict__ aos, State st, float* 
   rho[i] = p.rho;
 }
 int launch_from_aos(const Dev& d, cudaStream_t s) {
-  k_from_aos<<<(d.n + 255) / 256, 256, 0, s>>>(d.n, (const P48*)d.aos, d.s(), d.rho);
+  k_from_aos<<<(d.n + 255) / 256, 256, 0, s>>>(d.n, (const P48*)d.aos, d.segs, d.nseg, d.s(), d.rho);
   return 1;
 }
 

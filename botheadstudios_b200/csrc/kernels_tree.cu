@@ -4,7 +4,9 @@
 // Reference: shaders/bh_gravity.wgsl (cs_bbox :68, cs_morton :100, cs_tree :135, cs_com :201) and the CPU
 // sort of crates/engine/src/gpu_gravity.rs:336-368. The sort order is (Morton code, original index), made
 // exact by sorting 64-bit keys code<<idbits | index, so the permutation, the leaf codes and the Karras
-// topology are bit-identical to the reference's.
+// topology are bit-identical to the reference's. A batch of impacts prefixes the code with the impact
+// (segment) index: every impact is quantised in its own box, sorted into its own contiguous range and
+// built into its own subtree, exactly as if it were alone.
 #include <cuda/atomic>
 
 #include "sph_kernels.cuh"
@@ -12,74 +14,106 @@
 namespace sphb {
 
 // ---------------------------------------------------------------------------------------------------
-// Bounding box (cs_bbox): reduce order-preserving u32 keys per block, one atomic per block and axis.
+// Segment table set-up: the first particle of every leaf (leaves are K-particle buckets counted from the
+// start of their segment; the last bucket of a segment may be partial).
 // ---------------------------------------------------------------------------------------------------
-__global__ void k_bbox_reset(DevParams* P) {
-  const int i = threadIdx.x;
-  if (i < 3) P->bbox_keys[i] = 0xffffffffu;
-  else if (i < 6) P->bbox_keys[i] = 0u;
+__global__ void k_leaf_start(const Seg* __restrict__ segs, int nseg, int K, int L, int n,
+                             unsigned* __restrict__ leaf_start) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c > L) return;
+  if (c == L) {
+    leaf_start[L] = (unsigned)n;
+    return;
+  }
+  int lo = 0, hi = nseg - 1;  // last segment whose first leaf is <= c
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (segs[mid].loff <= (unsigned)c) lo = mid;
+    else hi = mid - 1;
+  }
+  leaf_start[c] = segs[lo].off + (unsigned)(c - (int)segs[lo].loff) * (unsigned)K;
 }
 
-__device__ __forceinline__ void block_bbox_commit(unsigned lo[3], unsigned hi[3], DevParams* P) {
-  __shared__ unsigned s_lo[3][32], s_hi[3][32];
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-#pragma unroll
+int launch_segments(const Dev& d, cudaStream_t s) {
+  k_leaf_start<<<(d.L + 1 + 255) / 256, 256, 0, s>>>(d.segs, d.nseg, d.K, d.L, d.n, d.leaf_start);
+  return 1;
+}
+
+__global__ void k_segments_single(Seg* segs, int n, int L, float soft2, double dt) {
+  Seg a;
+  a.off = 0u;
+  a.loff = 0u;
+  a.root = 0u;
+  a.sig_bits = 0x7f800000u;
   for (int k = 0; k < 3; ++k) {
-    lo[k] = warp_min(lo[k]);
-    hi[k] = warp_max(hi[k]);
-    if (lane == 0) { s_lo[k][w] = lo[k]; s_hi[k][w] = hi[k]; }
+    a.bbox[k] = 0xffffffffu;
+    a.bbox[3 + k] = 0u;
   }
-  __syncthreads();
-  if (w == 0) {
-    const int nw = blockDim.x >> 5;
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      unsigned a = lane < nw ? s_lo[k][lane] : 0xffffffffu;
-      unsigned b = lane < nw ? s_hi[k][lane] : 0u;
-      a = warp_min(a);
-      b = warp_max(b);
-      if (lane == 0) {
-        atomicMin(&P->bbox_keys[k], a);
-        atomicMax(&P->bbox_keys[3 + k], b);
-      }
-    }
+  a.soft2 = soft2;
+  a.pad = 0u;
+  a.dt = dt;
+  a.time = 0.0;
+  segs[0] = a;
+  Seg e = a;
+  e.off = (unsigned)n;
+  e.loff = (unsigned)L;
+  segs[1] = e;
+}
+
+int launch_segments_single(const Dev& d, float soft2, double dt, cudaStream_t s) {
+  k_segments_single<<<1, 1, 0, s>>>(d.segs, d.n, d.L, soft2, dt);
+  return 1 + launch_segments(d, s);
+}
+
+// ---------------------------------------------------------------------------------------------------
+// Bounding box per segment (cs_bbox): order-preserving u32 keys, reduced per block (seg_bbox_commit).
+// ---------------------------------------------------------------------------------------------------
+__global__ void k_bbox_reset(Seg* segs, int nseg) {
+  const int k = threadIdx.x;
+  if (k >= nseg) return;
+  for (int a = 0; a < 3; ++a) {
+    segs[k].bbox[a] = 0xffffffffu;
+    segs[k].bbox[3 + a] = 0u;
   }
 }
 
-__global__ void k_bbox(const float4* __restrict__ pos, int n, DevParams* P) {
+__global__ void k_bbox(const float4* __restrict__ pos, const unsigned* __restrict__ seg, int n, Seg* segs) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
   unsigned lo[3] = {0xffffffffu, 0xffffffffu, 0xffffffffu}, hi[3] = {0u, 0u, 0u};
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+  unsigned sg = kNoSeg;
+  if (i < n) {
     const float4 p = pos[i];
-    const unsigned kx = float_key(p.x), ky = float_key(p.y), kz = float_key(p.z);
-    lo[0] = min(lo[0], kx); lo[1] = min(lo[1], ky); lo[2] = min(lo[2], kz);
-    hi[0] = max(hi[0], kx); hi[1] = max(hi[1], ky); hi[2] = max(hi[2], kz);
+    lo[0] = hi[0] = float_key(p.x);
+    lo[1] = hi[1] = float_key(p.y);
+    lo[2] = hi[2] = float_key(p.z);
+    sg = seg[i];
   }
-  block_bbox_commit(lo, hi, P);
+  seg_bbox_commit(lo, hi, sg, segs);
 }
-
-int launch_bbox_reset(const Dev& d, cudaStream_t s) { k_bbox_reset<<<1, 32, 0, s>>>(d.P);  return 1; }
 
 int launch_bbox(const Dev& d, cudaStream_t s) {
-  k_bbox_reset<<<1, 32, 0, s>>>(d.P);
-  const int threads = 256;
-  int blocks = (d.n + threads - 1) / threads;
-  blocks = blocks < 1 ? 1 : (blocks > 148 * 8 ? 148 * 8 : blocks);
-  k_bbox<<<blocks, threads, 0, s>>>(d.s().pos_h, d.n, d.P);
+  k_bbox_reset<<<1, kMaxSegments, 0, s>>>(d.segs, d.nseg);
+  k_bbox<<<(d.n + 255) / 256, 256, 0, s>>>(d.s().pos_h, d.s().seg, d.n, d.segs);
   return 2;
 }
 
 // ---------------------------------------------------------------------------------------------------
-// Morton keys (cs_morton, bh_gravity.wgsl:91-108) with IEEE division, no contraction.
+// Morton keys (cs_morton, bh_gravity.wgsl:91-108) with IEEE division, no contraction, each particle
+// quantised in its own segment's box. Sort key: (segment, code, original index), packed as
+// ((segment << 30 | code) << idbits) | index.
 // ---------------------------------------------------------------------------------------------------
-__global__ void k_keys(const float4* __restrict__ pos, const unsigned* __restrict__ id, int n, const DevParams* P,
-                       int idbits, unsigned long long* __restrict__ keys, unsigned* __restrict__ vals) {
+__global__ void k_keys(const float4* __restrict__ pos, const unsigned* __restrict__ id,
+                       const unsigned* __restrict__ seg, int n, const Seg* __restrict__ segs, int idbits,
+                       unsigned long long* __restrict__ keys, unsigned* __restrict__ vals) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
+  const unsigned sg = seg[i];
+  const unsigned* bb = segs[sg].bbox;
   float lo[3], ext[3];
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
-    lo[k] = key_float(P->bbox_keys[k]);
-    ext[k] = fmaxf(fsub(key_float(P->bbox_keys[3 + k]), lo[k]), 1.0e-30f);
+    lo[k] = key_float(bb[k]);
+    ext[k] = fmaxf(fsub(key_float(bb[3 + k]), lo[k]), 1.0e-30f);
   }
   const float4 p = pos[i];
   const float pc[3] = {p.x, p.y, p.z};
@@ -93,7 +127,7 @@ __global__ void k_keys(const float4* __restrict__ pos, const unsigned* __restric
     q[k] = (unsigned)f;
   }
   const unsigned code = expand_bits(q[0]) * 4u + expand_bits(q[1]) * 2u + expand_bits(q[2]);
-  keys[i] = ((unsigned long long)code << idbits) | (unsigned long long)id[i];
+  keys[i] = ((((unsigned long long)sg << 30) | code) << idbits) | (unsigned long long)id[i];
   vals[i] = (unsigned)i;
 }
 
@@ -253,9 +287,10 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_downsweep(const unsigned long
 // ---------------------------------------------------------------------------------------------------
 // Permutation of the particle state into the new order; leaf cluster codes (gpu_gravity.rs:366).
 // ---------------------------------------------------------------------------------------------------
-__global__ void k_permute(int n, int K, int idbits, const unsigned* __restrict__ order,
-                          const unsigned long long* __restrict__ skeys, State in, State out,
-                          float4* __restrict__ body, unsigned* __restrict__ leaf_codes) {
+__global__ void k_permute(int n, int L, int idbits, const unsigned* __restrict__ order,
+                          const unsigned long long* __restrict__ skeys, const unsigned* __restrict__ leaf_start,
+                          State in, State out, float4* __restrict__ body,
+                          unsigned long long* __restrict__ leaf_codes) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
   const unsigned o = order[t];
@@ -270,8 +305,9 @@ __global__ void k_permute(int n, int K, int idbits, const unsigned* __restrict__
   out.mat[t] = in.mat[o];
   out.prov[t] = in.prov[o];
   out.id[t] = in.id[o];
+  out.seg[t] = in.seg[o];
   body[t] = make_float4(p.x, p.y, p.z, m);
-  if (t % K == 0) leaf_codes[t / K] = (unsigned)(skeys[t] >> idbits);
+  if (t < L) leaf_codes[t] = skeys[leaf_start[t]] >> idbits;
 }
 
 int launch_sort_permute(Dev& d, cudaStream_t s) {
@@ -279,9 +315,9 @@ int launch_sort_permute(Dev& d, cudaStream_t s) {
   const int threads = 256;
   const int blocks = (n + threads - 1) / threads;
   const State& in = d.st[d.cur];
-  k_keys<<<blocks, threads, 0, s>>>(in.pos_h, in.id, n, d.P, d.idbits, d.keys[0], d.vals[0]);
+  k_keys<<<blocks, threads, 0, s>>>(in.pos_h, in.id, in.seg, n, d.segs, d.idbits, d.keys[0], d.vals[0]);
   const int T = (int)radix_tiles(n);
-  const int total_bits = 30 + d.idbits;
+  const int total_bits = 30 + d.segbits + d.idbits;
   const int passes = (total_bits + 7) / 8;
   int src = 0;
   for (int shift = 0; shift < total_bits; shift += 8) {
@@ -293,7 +329,8 @@ int launch_sort_permute(Dev& d, cudaStream_t s) {
   }
   // vals[src] = old slot of each sorted position; keys[src] = sorted keys
   const State& out = d.st[d.cur ^ 1];
-  k_permute<<<blocks, threads, 0, s>>>(n, d.K, d.idbits, d.vals[src], d.keys[src], in, out, d.body, d.leaf_codes);
+  k_permute<<<blocks, threads, 0, s>>>(n, d.L, d.idbits, d.vals[src], d.keys[src], d.leaf_start, in, out, d.body,
+                                       d.leaf_codes);
   d.cur ^= 1;
   // keep the sorted keys in keys[0] for inspection
   if (src != 0) cudaMemcpyAsync(d.keys[0], d.keys[src], sizeof(unsigned long long) * n, cudaMemcpyDeviceToDevice, s);
@@ -303,55 +340,80 @@ int launch_sort_permute(Dev& d, cudaStream_t s) {
 // ---------------------------------------------------------------------------------------------------
 // Karras 2012 internal nodes over the leaf cluster codes (cs_tree, bh_gravity.wgsl:114-184).
 // ---------------------------------------------------------------------------------------------------
-__device__ __forceinline__ int kdelta(const unsigned* __restrict__ codes, int L, int i, int j) {
+__device__ __forceinline__ unsigned code_seg(unsigned long long c) { return (unsigned)(c >> 30); }
+
+// Leaf codes are segment << 30 | Morton code: one impact's leaves share the top bits, so each impact is one
+// subtree. Equal codes (always within one impact) are told apart by the leaf index counted from the impact's
+// first leaf, so an impact's subtree is the tree it would get alone. With one segment every delta is the
+// reference's plus 32 (bh_gravity.wgsl:114-120), which leaves every comparison unchanged.
+__device__ __forceinline__ int kdelta(const unsigned long long* __restrict__ codes, const Seg* __restrict__ segs,
+                                      int L, int i, int j) {
   if (j < 0 || j >= L) return -1;
-  const unsigned ci = codes[i], cj = codes[j];
-  if (ci == cj) return 32 + __clz((unsigned)i ^ (unsigned)j);
-  return __clz(ci ^ cj);
+  const unsigned long long ci = codes[i], cj = codes[j];
+  if (ci == cj) {
+    const unsigned base = segs[code_seg(ci)].loff;
+    return 64 + __clz(((unsigned)i - base) ^ ((unsigned)j - base));
+  }
+  return __clzll(ci ^ cj);
 }
 
-// Particles covered by leaves [first, last] (the last leaf may be partial).
-__device__ __forceinline__ int range_count(int first, int last, int K, int n) {
-  return min((last + 1) * K, n) - first * K;
+// Particles covered by leaves [first, last].
+__device__ __forceinline__ int range_count(const unsigned* __restrict__ leaf_start, int first, int last) {
+  return (int)(leaf_start[last + 1] - leaf_start[first]);
 }
 
-__global__ void k_karras(const unsigned* __restrict__ codes, int L, int K, int n, unsigned* __restrict__ left,
-                         unsigned* __restrict__ right, unsigned* __restrict__ parent, uint2* __restrict__ groups,
-                         unsigned* __restrict__ ngroups, int exact_dups) {
+// Leaves [first, last] are exactly one segment.
+__device__ __forceinline__ bool whole_segment(const unsigned long long* __restrict__ codes, int L, int first,
+                                              int last) {
+  const unsigned sg = code_seg(codes[first]);
+  return code_seg(codes[last]) == sg && (first == 0 || code_seg(codes[first - 1]) != sg) &&
+         (last == L - 1 || code_seg(codes[last + 1]) != sg);
+}
+
+// A walk group: at most 32 particles of one segment.
+__device__ __forceinline__ bool group_fits(const unsigned long long* __restrict__ codes,
+                                           const unsigned* __restrict__ leaf_start, int first, int last) {
+  return range_count(leaf_start, first, last) <= 32 && code_seg(codes[first]) == code_seg(codes[last]);
+}
+
+__global__ void k_karras(const unsigned long long* __restrict__ codes, const unsigned* __restrict__ leaf_start,
+                         int L, unsigned* __restrict__ left, unsigned* __restrict__ right,
+                         unsigned* __restrict__ parent, uint2* __restrict__ groups, unsigned* __restrict__ ngroups,
+                         Seg* __restrict__ segs, int exact_dups) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= L - 1) return;
-  const int d = kdelta(codes, L, i, i + 1) > kdelta(codes, L, i, i - 1) ? 1 : -1;
-  const int dmin = kdelta(codes, L, i, i - d);
+  const int d = kdelta(codes, segs, L, i, i + 1) > kdelta(codes, segs, L, i, i - 1) ? 1 : -1;
+  const int dmin = kdelta(codes, segs, L, i, i - d);
   int lmax = 2;
-  while (kdelta(codes, L, i, i + lmax * d) > dmin) lmax *= 2;
+  while (kdelta(codes, segs, L, i, i + lmax * d) > dmin) lmax *= 2;
   int l = 0;
   for (int t = lmax / 2; t >= 1; t /= 2)
-    if (kdelta(codes, L, i, i + (l + t) * d) > dmin) l += t;
+    if (kdelta(codes, segs, L, i, i + (l + t) * d) > dmin) l += t;
   const int j = i + l * d;
   const int first = min(i, j), last = max(i, j);
   int split = first;
-  const unsigned fc = codes[first], lc = codes[last];
+  const unsigned long long fc = codes[first], lc = codes[last];
   if (fc == lc && !exact_dups) {
     // the reference's split of a run of equal codes (bh_gravity.wgsl:159-160); it can disagree with the
     // index-extended ranges the children compute for themselves, so such trees may be invalid
     split = (first + last) >> 1;
   } else if (fc == lc) {
     // Karras 2012 §4: index-extended keys — binary search on the common prefix of the indices
-    const int cpfx = kdelta(codes, L, first, last);
+    const int cpfx = kdelta(codes, segs, L, first, last);
     int step = last - first;
     for (;;) {
       step = (step + 1) >> 1;
       const int ns = split + step;
-      if (ns < last && kdelta(codes, L, first, ns) > cpfx) split = ns;
+      if (ns < last && kdelta(codes, segs, L, first, ns) > cpfx) split = ns;
       if (step <= 1) break;
     }
   } else {
-    const int cpfx = __clz(fc ^ lc);
+    const int cpfx = __clzll(fc ^ lc);
     int step = last - first;
     for (;;) {
       step = (step + 1) >> 1;
       const int ns = split + step;
-      if (ns < last && __clz(fc ^ codes[ns]) > cpfx) split = ns;
+      if (ns < last && __clzll(fc ^ codes[ns]) > cpfx) split = ns;
       if (step <= 1) break;
     }
   }
@@ -361,20 +423,26 @@ __global__ void k_karras(const unsigned* __restrict__ codes, int L, int K, int n
   right[i] = ridx;
   parent[lidx] = (unsigned)i;
   parent[ridx] = (unsigned)i;
-  // Walk groups: the maximal subtrees holding at most 32 particles. A node above the limit emits each child
-  // that fits; the root emits itself when the whole set fits. Subtrees share a Morton prefix, so every
-  // group's bounding box is compact.
-  if (range_count(first, last, K, n) > 32) {
-    if (range_count(first, split, K, n) <= 32) groups[atomicAdd(ngroups, 1u)] = make_uint2(first, split);
-    if (range_count(split + 1, last, K, n) <= 32) groups[atomicAdd(ngroups, 1u)] = make_uint2(split + 1, last);
+  // segment roots: the node spanning exactly one impact (a leaf when the impact has one leaf)
+  if (whole_segment(codes, L, first, last)) segs[code_seg(fc)].root = (unsigned)i;
+  if (split == first && whole_segment(codes, L, first, first)) segs[code_seg(fc)].root = lidx;
+  if (split + 1 == last && whole_segment(codes, L, last, last)) segs[code_seg(lc)].root = ridx;
+  // Walk groups: the maximal subtrees holding at most 32 particles of one segment. A node that does not fit
+  // emits each child that fits; the root emits itself when the whole set fits. Subtrees share a Morton
+  // prefix, so every group's bounding box is compact.
+  if (!group_fits(codes, leaf_start, first, last)) {
+    if (group_fits(codes, leaf_start, first, split)) groups[atomicAdd(ngroups, 1u)] = make_uint2(first, split);
+    if (group_fits(codes, leaf_start, split + 1, last))
+      groups[atomicAdd(ngroups, 1u)] = make_uint2(split + 1, last);
   } else if (i == 0) {
     groups[atomicAdd(ngroups, 1u)] = make_uint2(first, last);
   }
 }
 
-__global__ void k_single_group(uint2* groups, unsigned* ngroups, int L) {
+__global__ void k_single_group(uint2* groups, unsigned* ngroups, Seg* segs, int L) {
   groups[0] = make_uint2(0u, (unsigned)(L - 1));
   *ngroups = 1u;
+  segs[0].root = 0u;
 }
 
 // ---------------------------------------------------------------------------------------------------
@@ -388,15 +456,15 @@ __global__ void k_single_group(uint2* groups, unsigned* ngroups, int L) {
 // traceless quadrupole about the COM (parallel-axis merge).
 // ---------------------------------------------------------------------------------------------------
 template <bool QUAD>
-__global__ void k_leaf_climb(const float4* __restrict__ body, const float4* __restrict__ pos_h, int n, int K,
-                             int L, const unsigned* __restrict__ left, const unsigned* __restrict__ right,
+__global__ void k_leaf_climb(const float4* __restrict__ body, const float4* __restrict__ pos_h,
+                             const unsigned* __restrict__ leaf_start, int L, const unsigned* __restrict__ left, const unsigned* __restrict__ right,
                              const unsigned* __restrict__ parent, unsigned* __restrict__ counters,
                              float4* __restrict__ ncom, float4* __restrict__ nbmin, float4* __restrict__ nbmax,
                              float4* __restrict__ nq0, float4* __restrict__ nq1, float theta, int side_mac) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= L) return;
   const int li = L - 1 + c;
-  const int s0 = c * K, s1 = min(s0 + K, n);
+  const int s0 = (int)leaf_start[c], s1 = (int)leaf_start[c + 1];
   float m = 0.0f, mx = 0.0f, my = 0.0f, mz = 0.0f, hmax = 0.0f;
   float lo[3] = {1.0e30f, 1.0e30f, 1.0e30f}, hi[3] = {-1.0e30f, -1.0e30f, -1.0e30f};
   for (int s = s0; s < s1; ++s) {
@@ -489,20 +557,21 @@ int launch_tree(const Dev& d, const Cfg& c, float theta, cudaStream_t s) {
   cudaMemsetAsync(d.ngroups, 0, sizeof(unsigned), s);
   if (L > 1) {
     cudaMemsetAsync(d.counters, 0, sizeof(unsigned) * (L - 1), s);
-    k_karras<<<(L - 1 + 255) / 256, 256, 0, s>>>(d.leaf_codes, L, d.K, d.n, d.left, d.right, d.parent, d.groups,
-                                                  d.ngroups, c.mac == 0 ? 1 : 0);
+    k_karras<<<(L - 1 + 255) / 256, 256, 0, s>>>(d.leaf_codes, d.leaf_start, L, d.left, d.right, d.parent, d.groups,
+                                                  d.ngroups, d.segs, c.mac == 0 ? 1 : 0);
   } else {
-    k_single_group<<<1, 1, 0, s>>>(d.groups, d.ngroups, L);
+    k_single_group<<<1, 1, 0, s>>>(d.groups, d.ngroups, d.segs, L);
   }
   const State& st = d.s();
+  const int side_mac = c.mac == 0 ? 1 : 0;
   if (c.quad)
-    k_leaf_climb<true><<<(L + 127) / 128, 128, 0, s>>>(d.body, st.pos_h, d.n, d.K, L, d.left, d.right, d.parent,
+    k_leaf_climb<true><<<(L + 127) / 128, 128, 0, s>>>(d.body, st.pos_h, d.leaf_start, L, d.left, d.right, d.parent,
                                                        d.counters, d.ncom, d.nbmin, d.nbmax, d.nq0, d.nq1, theta,
-                                                       c.mac == 0 ? 1 : 0);
+                                                       side_mac);
   else
-    k_leaf_climb<false><<<(L + 127) / 128, 128, 0, s>>>(d.body, st.pos_h, d.n, d.K, L, d.left, d.right, d.parent,
+    k_leaf_climb<false><<<(L + 127) / 128, 128, 0, s>>>(d.body, st.pos_h, d.leaf_start, L, d.left, d.right, d.parent,
                                                         d.counters, d.ncom, d.nbmin, d.nbmax, d.nq0, d.nq1, theta,
-                                                       c.mac == 0 ? 1 : 0);
+                                                        side_mac);
   return 2;
 }
 

@@ -62,9 +62,10 @@ struct Acc3 {
 template <bool GRAV, bool QUAD, bool NBR, bool HILO>
 __global__ void __launch_bounds__(TW_WARPS * 32, 6) k_tree_walk(
     const float4* __restrict__ body, const float4* __restrict__ pos_h, const double* __restrict__ x64,
-    const double* __restrict__ y64, const double* __restrict__ z64, int n, int K, int L,
-    const unsigned* __restrict__ left, const unsigned* __restrict__ right, const float4* __restrict__ ncom,
-    const float4* __restrict__ nbmin, const float4* __restrict__ nbmax, const float4* __restrict__ nq0,
+    const double* __restrict__ y64, const double* __restrict__ z64, int K, int L,
+    const unsigned* __restrict__ leaf_start, const unsigned long long* __restrict__ leaf_codes,
+    const Seg* __restrict__ segs, const unsigned* __restrict__ left, const unsigned* __restrict__ right,
+    const float4* __restrict__ ncom, const float4* __restrict__ nbmin, const float4* __restrict__ nbmax, const float4* __restrict__ nq0,
     const float4* __restrict__ nq1, DevParams* P, float4* __restrict__ gout, unsigned* __restrict__ nbr,
     unsigned* __restrict__ nbr_cnt, unsigned cap, float skin, float* __restrict__ h0,
     const uint2* __restrict__ groups, const unsigned* __restrict__ ngroups) {
@@ -74,9 +75,12 @@ __global__ void __launch_bounds__(TW_WARPS * 32, 6) k_tree_walk(
   const unsigned lane = threadIdx.x & 31u;
   const int warp = blockIdx.x * TW_WARPS + w;
   if (warp >= (int)*ngroups) return;
-  // this warp's group: a maximal subtree of <= 32 particles (leaves g.x..g.y)
+  // this warp's group: a maximal subtree of <= 32 particles of one impact (leaves g.x..g.y); the walk starts
+  // at that impact's root
   const uint2 grp = groups[warp];
-  const int s0 = (int)grp.x * K, s1 = min(((int)grp.y + 1) * K, n);
+  const int s0 = (int)leaf_start[grp.x], s1 = (int)leaf_start[grp.y + 1];
+  const Seg& sgr = segs[(unsigned)(leaf_codes[grp.x] >> 30)];
+  const unsigned root = sgr.root;
   const int t = s0 + (int)lane;
   const bool in_group = t < s1;
   const int tl = in_group ? t : s0;
@@ -89,17 +93,17 @@ __global__ void __launch_bounds__(TW_WARPS * 32, 6) k_tree_walk(
   }
   if (NBR && in_group && h0) h0[t] = pi.w;
   // Split the group where consecutive particles are far apart (a leaf bucket of K consecutive Morton
-  // particles can straddle a jump of the curve, e.g. between two bodies): each segment walks with its own
+  // particles can straddle a jump of the curve, e.g. between two bodies): each part walks with its own
   // compact box, so one straddling bucket cannot turn the walk into an all-pairs sum.
   const float px = __shfl_up_sync(SPH_FULL_MASK, pi.x, 1), py = __shfl_up_sync(SPH_FULL_MASK, pi.y, 1),
               pz = __shfl_up_sync(SPH_FULL_MASK, pi.z, 1), ph_ = __shfl_up_sync(SPH_FULL_MASK, pi.w, 1);
   const float gap2 = (pi.x - px) * (pi.x - px) + (pi.y - py) * (pi.y - py) + (pi.z - pz) * (pi.z - pz);
   const float hm = 3.0f * fmaxf(pi.w, ph_);
   const unsigned brk = __ballot_sync(SPH_FULL_MASK, lane > 0 && in_group && gap2 > hm * hm);
-  const int nseg = __popc(brk) + 1;
-  const int myseg = __popc(brk & ((2u << lane) - 1u));
+  const int nparts = __popc(brk) + 1;
+  const int mypart = __popc(brk & ((2u << lane) - 1u));
   const float grow = (1.0f + skin) * (1.0f + 1.0e-5f);
-  const float G = P->G, soft2 = P->soft2;
+  const float G = P->G, soft2 = sgr.soft2;
   const unsigned leaf0 = (unsigned)(L - 1);
   const unsigned lt = (1u << lane) - 1u;
 
@@ -110,8 +114,8 @@ __global__ void __launch_bounds__(TW_WARPS * 32, 6) k_tree_walk(
   unsigned* stack = S.stack[w];
   unsigned long long st_visits = 0, st_pops = 0, st_m2p = 0, st_p2p = 0;
 
-  for (int seg = 0; seg < nseg; ++seg) {
-  const bool valid = in_group && myseg == seg;
+  for (int part = 0; part < nparts; ++part) {
+  const bool valid = in_group && mypart == part;
   const float big = 3.0e38f;
   const float gx0 = warp_min(valid ? pi.x : big), gy0 = warp_min(valid ? pi.y : big),
               gz0 = warp_min(valid ? pi.z : big);
@@ -119,7 +123,7 @@ __global__ void __launch_bounds__(TW_WARPS * 32, 6) k_tree_walk(
               gz1 = warp_max(valid ? pi.z : -big);
   const float ghmax = warp_max(valid ? pi.w : 0.0f);
   int sp = 1, nm = 0, np = 0, nf = 0;
-  if (lane == 0) stack[0] = 0u;
+  if (lane == 0) stack[0] = root;
   __syncwarp();
 
   // ---- far leaves: branch-free pairwise gravity, 32 staged sources per pass ---------------------------
@@ -130,8 +134,9 @@ __global__ void __launch_bounds__(TW_WARPS * 32, 6) k_tree_walk(
       const int li = lane / K, off = lane % K;
       float4 src = make_float4(3.0e18f, 3.0e18f, 3.0e18f, 0.0f);  // padding: massless and far away
       if (li < nl) {
-        const int s = (int)S.p2f[w][base + li] * K + off;
-        if (s < n) {
+        const unsigned lf = S.p2f[w][base + li];
+        const int s = (int)leaf_start[lf] + off;
+        if (s < (int)leaf_start[lf + 1]) {
           src = body[s];
           src.w *= G;
         }
@@ -211,8 +216,9 @@ __global__ void __launch_bounds__(TW_WARPS * 32, 6) k_tree_walk(
       const int li = lane / K, off = lane % K;
       int sidx = -1;
       if (li < nl) {
-        const int s = (int)S.p2p[w][base + li] * K + off;
-        if (s < n) sidx = s;
+        const unsigned lf = S.p2p[w][base + li];
+        const int s = (int)leaf_start[lf] + off;
+        if (s < (int)leaf_start[lf + 1]) sidx = s;
       }
       S.sidx[w][lane] = sidx;
       float4 src = make_float4(3.0e18f, 3.0e18f, 3.0e18f, 0.0f);  // padding: massless and far away
@@ -268,7 +274,7 @@ __global__ void __launch_bounds__(TW_WARPS * 32, 6) k_tree_walk(
   };
 
   const unsigned nvalid = __popc(__ballot_sync(SPH_FULL_MASK, valid));
-  unsigned long long seg_m2p = 0, seg_p2p = 0;
+  unsigned long long part_m2p = 0, part_p2p = 0;
   while (sp > 0) {
     const int take = min(sp, 32);
     sp -= take;
@@ -327,8 +333,8 @@ __global__ void __launch_bounds__(TW_WARPS * 32, 6) k_tree_walk(
     nm += __popc(bm);
     np += __popc(bn);
     nf += __popc(bfar);
-    seg_m2p += __popc(bm);
-    seg_p2p += __popc(bf);
+    part_m2p += __popc(bm);
+    part_p2p += __popc(bf);
     __syncwarp();
     if (nm > TW_LIST - 32) {
       flush_m2p(nm);
@@ -346,9 +352,9 @@ __global__ void __launch_bounds__(TW_WARPS * 32, 6) k_tree_walk(
   if (nm) flush_m2p(nm);
   if (np) flush_p2p(np);
   if (nf) flush_far(nf);
-  st_m2p += seg_m2p * nvalid;                             // node × particle interactions
-  st_p2p += seg_p2p * (unsigned long long)K * nvalid;     // leaf sources × particles (upper bound)
-  }  // segments
+  st_m2p += part_m2p * nvalid;                             // node × particle interactions
+  st_p2p += part_p2p * (unsigned long long)K * nvalid;     // leaf sources × particles (upper bound)
+  }  // parts
 
   if (in_group && GRAV) gout[t] = make_float4(acc.x, acc.y, acc.z, phi);
   if (NBR) {
@@ -380,8 +386,8 @@ static void walk(const Dev& d, const Cfg& c, cudaStream_t s) {
   }
   const State& st = d.s();
   k_tree_walk<GRAV, QUAD, NBR, HILO><<<blocks, TW_WARPS * 32, smem, s>>>(
-      d.body, st.pos_h, st.x, st.y, st.z, d.n, d.K, d.L, d.left, d.right, d.ncom, d.nbmin, d.nbmax, d.nq0, d.nq1,
-      d.P, d.grav, d.nbr, d.nbr_cnt, d.nbr_cap, c.h_solve ? c.skin : c.nbr_skin, d.h0, d.groups, d.ngroups);
+      d.body, st.pos_h, st.x, st.y, st.z, d.K, d.L, d.leaf_start, d.leaf_codes, d.segs, d.left, d.right, d.ncom,
+      d.nbmin, d.nbmax, d.nq0, d.nq1, d.P, d.grav, d.nbr, d.nbr_cnt, d.nbr_cap, c.h_solve ? c.skin : c.nbr_skin, d.h0, d.groups, d.ngroups);
 }
 
 // Gravity (group MAC) fused with the neighbour lists.

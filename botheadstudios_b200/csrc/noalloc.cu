@@ -29,11 +29,12 @@ constexpr size_t scratch_bytes() {
   const size_t nodes = 2 * L;
   const size_t tiles = (n + 2047) / 2048;
   size_t b = 0;
-  b += 2 * (up(16 * n) + up(16 * n) + 3 * up(8 * n) + 4 * up(4 * n));  // two particle states
+  b += 2 * (up(16 * n) + up(16 * n) + 3 * up(8 * n) + 5 * up(4 * n));  // two particle states
   b += 2 * up(8 * n) + 2 * up(4 * n);                                  // sort keys and values
   b += up(16 * n) + up(16 * n);                                        // bodies, accelerations
   b += up(4 * 256 * tiles) + up(4 * 256);                              // radix histograms
-  b += 4 * up(4 * L) + up(8 * L) + up(4);                              // leaf codes, left/right/counters, groups
+  b += up(8 * L) + 3 * up(4 * L) + up(8 * L) + up(4);                  // leaf codes, left/right/counters, groups
+  b += up(4 * (L + 1)) + up(2 * sizeof(Seg));                          // leaf starts, segment table
   b += up(4 * nodes) + 5 * up(16 * nodes);                             // parents, node records
   b += up(sizeof(DevParams));
   return b;
@@ -73,6 +74,7 @@ Dev carve_dev(unsigned char* base, uint32_t K) {
     s.mat = carve<unsigned>(p, n);
     s.prov = carve<unsigned>(p, n);
     s.id = carve<unsigned>(p, n);
+    s.seg = carve<unsigned>(p, n);
   }
   d.keys[0] = carve<unsigned long long>(p, n);
   d.keys[1] = carve<unsigned long long>(p, n);
@@ -83,12 +85,14 @@ Dev carve_dev(unsigned char* base, uint32_t K) {
   d.rs_tiles_cap = (int)((n + 2047) / 2048);
   d.rs_hist = carve<unsigned>(p, 256 * (size_t)d.rs_tiles_cap);
   d.rs_tot = carve<unsigned>(p, 256);
-  d.leaf_codes = carve<unsigned>(p, L);
+  d.leaf_codes = carve<unsigned long long>(p, L);
   d.left = carve<unsigned>(p, L);
   d.right = carve<unsigned>(p, L);
   d.counters = carve<unsigned>(p, L);
   d.groups = carve<uint2>(p, L);
   d.ngroups = carve<unsigned>(p, 1);
+  d.leaf_start = carve<unsigned>(p, L + 1);
+  d.segs = carve<Seg>(p, 2);
   d.parent = carve<unsigned>(p, nodes);
   d.ncom = carve<float4>(p, nodes);
   d.nbmin = carve<float4>(p, nodes);
@@ -100,14 +104,11 @@ Dev carve_dev(unsigned char* base, uint32_t K) {
 }
 
 // Everything the walk reads from DevParams, written on the device (no host copy), counters cleared.
-__global__ void k_noalloc_params(DevParams* P, float G, float soft2, float theta) {
+__global__ void k_noalloc_params(DevParams* P, float G, float theta) {
   DevParams p;
   memset(&p, 0, sizeof(p));
   p.G = G;
-  p.soft2 = soft2;
-  p.softening = sqrtf(soft2);
   p.theta = theta;
-  p.sig_min_bits = 0x7f800000u;
   *P = p;
 }
 
@@ -124,6 +125,7 @@ __global__ void k_noalloc_load(const float4* __restrict__ in, int n, State st) {
   st.mat[i] = 0u;
   st.prov[i] = 0u;
   st.id[i] = (unsigned)i;
+  st.seg[i] = 0u;
 }
 
 __global__ void k_noalloc_store(int n, const unsigned* __restrict__ id, const float4* __restrict__ grav,
@@ -168,8 +170,9 @@ extern "C" sph_status sph_gravity_tree_noalloc(const void* d_bodies4, uint32_t n
   Cfg c;
   c.quad = (int)multipole;
   c.mac = SPH_MAC_GROUP;
-  k_noalloc_params<<<1, 1, 0, s>>>(d.P, (float)G, softening * softening, theta);
+  k_noalloc_params<<<1, 1, 0, s>>>(d.P, (float)G, theta);
   k_noalloc_load<<<(n + 255) / 256, 256, 0, s>>>(static_cast<const float4*>(d_bodies4), (int)n, d.st[0]);
+  launch_segments_single(d, softening * softening, 0.0, s);
   launch_bbox(d, s);
   launch_sort_permute(d, s);
   launch_tree(d, c, theta, s);

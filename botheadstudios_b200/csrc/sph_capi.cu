@@ -2,6 +2,7 @@
 // the dispatch order of one KDK step. It mirrors the engine's GpuSph (crates/engine/src/gpu_sph.rs:742-922)
 // and ParticleStore (gpu_store.rs): capacity clamping on upload, enqueue-only stepping, a two-phase
 // non-blocking readback. Errors are status codes; nothing throws across the boundary.
+#include <algorithm>
 #include <cmath>
 #include <cstddef>
 #include <cstdio>
@@ -28,6 +29,9 @@ struct sph_ctx {
   uint32_t n_eos = 0;
   bool uploaded = false;
   bool fresh = false;      // tree, neighbours, density, EOS and gravity are valid for the current positions
+  // captured steady KDK sequence (two substeps), one per parity of the state double buffer
+  cudaGraphExec_t kdk_graph[2] = {nullptr, nullptr};
+  unsigned long long kdk_graph_launches = 0;  // kernels in one replay
   DevParams hp{};          // host copy of the host-owned fields
   void* pinned_aos = nullptr;
   cudaEvent_t rb_event = nullptr;
@@ -81,7 +85,8 @@ sph_status alloc_dev(sph_ctx* ctx, Dev& d, uint32_t cap, uint32_t K, uint32_t nb
   d.cap = (int)cap;
   d.K = (int)K;
   const size_t capw = ((size_t)cap + 31) / 32 * 32;
-  const size_t Lmax = ((size_t)cap + K - 1) / K;
+  // leaves: ceil(n_k / K) per impact, at most ceil(cap / K) + one partial leaf per extra impact
+  const size_t Lmax = ((size_t)cap + K - 1) / K + kMaxSegments;
   const size_t nodes = 2 * Lmax;
   for (int b = 0; b < 2; ++b) {
     State& s = d.st[b];
@@ -94,6 +99,7 @@ sph_status alloc_dev(sph_ctx* ctx, Dev& d, uint32_t cap, uint32_t K, uint32_t nb
     ALLOC(s.mat, capw);
     ALLOC(s.prov, capw);
     ALLOC(s.id, capw);
+    ALLOC(s.seg, capw);
     ALLOC(d.keys[b], capw);
     ALLOC(d.vals[b], capw);
   }
@@ -102,6 +108,8 @@ sph_status alloc_dev(sph_ctx* ctx, Dev& d, uint32_t cap, uint32_t K, uint32_t nb
   ALLOC(d.rs_hist, 256 * (size_t)(d.rs_tiles_cap > 0 ? d.rs_tiles_cap : 1));
   ALLOC(d.rs_tot, 256);
   ALLOC(d.leaf_codes, Lmax);
+  ALLOC(d.leaf_start, Lmax + 1);
+  ALLOC(d.segs, (size_t)kMaxSegments + 1);
   ALLOC(d.left, Lmax);
   ALLOC(d.right, Lmax);
   ALLOC(d.parent, nodes);
@@ -168,31 +176,16 @@ void phase(sph_ctx* ctx, int ph, F&& f) {
   }
 }
 
-// Push the host-owned DevParams fields (everything except the device-maintained reductions and counters).
+// Push the host-owned DevParams fields (the block before the device-maintained reductions and counters).
 sph_status push_params(sph_ctx* ctx, Dev& d) {
-  DevParams& h = ctx->hp;
-  // copy [dt_fixed, ... sig_floor] contiguous block
-  const size_t off0 = offsetof(DevParams, dt_fixed);
-  const size_t off1 = offsetof(DevParams, time);
-  CK(cudaMemcpyAsync(reinterpret_cast<char*>(d.P) + off0, reinterpret_cast<char*>(&h) + off0, off1 - off0,
-                     cudaMemcpyHostToDevice, ctx->stream));
-  const size_t a0 = offsetof(DevParams, softening);
-  const size_t a1 = offsetof(DevParams, sig_min_bits);
-  CK(cudaMemcpyAsync(reinterpret_cast<char*>(d.P) + a0, reinterpret_cast<char*>(&h) + a0, a1 - a0,
-                     cudaMemcpyHostToDevice, ctx->stream));
+  const size_t bytes = offsetof(DevParams, flags);
+  CK(cudaMemcpyAsync(d.P, &ctx->hp, bytes, cudaMemcpyHostToDevice, ctx->stream));
   return SPH_OK;
 }
 
 sph_status init_params(sph_ctx* ctx, Dev& d) {
   DevParams p{};
   p = ctx->hp;
-  p.dt = ctx->hp.dt_fixed;
-  p.time = 0.0;
-  p.sig_min_bits = 0x7f800000u;
-  for (int k = 0; k < 3; ++k) {
-    p.bbox_keys[k] = 0xffffffffu;
-    p.bbox_keys[3 + k] = 0u;
-  }
   p.flags = 0;
   p.max_nbr_seen = 0;
   p.steps = 0;
@@ -236,6 +229,130 @@ sph_status check_ready(sph_ctx* ctx) {
     ctx->err = "no particles uploaded";
     return SPH_ERR_STATE;
   }
+  return SPH_OK;
+}
+
+void drop_graphs(sph_ctx* ctx) {
+  for (auto& g : ctx->kdk_graph)
+    if (g) {
+      cudaGraphExecDestroy(g);
+      g = nullptr;
+    }
+}
+
+// Upload of `nimp` impacts (particles [off[k], off[k+1]) of `particles`, softening soft[k]); the impacts
+// are already validated as non-empty and within capacity.
+sph_status upload_impl(sph_ctx* ctx, const SphParticle48* particles, const uint32_t* off, uint32_t nimp,
+                       const SphEos48* eos, uint32_t n_eos, const float* soft) {
+  cudaSetDevice(ctx->device);
+  sph_status ret = SPH_OK;
+  const uint32_t nu = nimp ? off[nimp] : 0u;
+  uint32_t ne = n_eos;
+  if (ne > (uint32_t)kMaxMaterials) {
+    ne = kMaxMaterials;
+    ret = SPH_CLAMPED;
+  }
+  for (uint32_t k = 0; k < nimp; ++k)
+    if (!std::isfinite(soft[k]) || soft[k] < 0.0f) {
+      ctx->err = "impact " + std::to_string(k) + " has a negative or non-finite softening";
+      return SPH_ERR_INVALID;
+    }
+  for (uint32_t i = 0; i < nu; ++i) {
+    const SphParticle48& p = particles[i];
+    if (p.mat >= ne || !std::isfinite(p.pos[0]) || !std::isfinite(p.pos[1]) || !std::isfinite(p.pos[2]) ||
+        !std::isfinite(p.vel[0]) || !std::isfinite(p.vel[1]) || !std::isfinite(p.vel[2]) || !std::isfinite(p.u) ||
+        !std::isfinite(p.mass) || !(p.h > 0.0f) || !std::isfinite(p.h) || p.mass < 0.0f) {
+      ctx->err = "particle " + std::to_string(i) + " has a material outside the table or a non-finite field";
+      return SPH_ERR_INVALID;
+    }
+  }
+  CK(cudaStreamSynchronize(ctx->stream));
+  drop_graphs(ctx);
+  Dev& d = ctx->d;
+  d.n = (int)nu;
+  d.cur = 0;
+  d.nseg = nimp ? (int)nimp : 1;
+  d.segbits = nimp > 1 ? bits_for(nimp) : 0;
+  d.idbits = bits_for(nu);
+  // segment table: each impact's leaves are K-particle buckets from its first particle
+  std::vector<Seg> table((size_t)d.nseg + 1);
+  uint32_t L = 0;
+  for (uint32_t k = 0; k <= nimp; ++k) {
+    Seg& g = table[k];
+    std::memset(&g, 0, sizeof(g));
+    g.off = k < nimp ? off[k] : nu;
+    g.loff = L;
+    g.sig_bits = 0x7f800000u;
+    for (int a = 0; a < 3; ++a) g.bbox[a] = 0xffffffffu;
+    g.soft2 = k < nimp ? soft[k] * soft[k] : 0.0f;
+    g.dt = ctx->hp.dt_fixed;
+    if (k < nimp) L += (off[k + 1] - off[k] + (uint32_t)d.K - 1) / (uint32_t)d.K;
+  }
+  d.L = (int)L;
+  ctx->n_eos = ne;
+  if (nu) CK(cudaMemcpyAsync(d.aos, particles, (size_t)nu * 48, cudaMemcpyHostToDevice, ctx->stream));
+  Eos etab[kMaxMaterials];
+  std::memset(etab, 0, sizeof(etab));
+  if (ne) std::memcpy(etab, eos, (size_t)ne * sizeof(Eos));
+  CK(cudaMemcpyAsync(d.eos, etab, sizeof(etab), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(d.segs, table.data(), table.size() * sizeof(Seg), cudaMemcpyHostToDevice, ctx->stream));
+  sph_status st = push_params(ctx, d);
+  if (st != SPH_OK) return st;
+  if (nu) {
+    launch_from_aos(d, ctx->stream);
+    launch_segments(d, ctx->stream);
+  }
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(ctx->stream));
+  ctx->uploaded = true;
+  ctx->fresh = false;
+  return ret;
+}
+
+// One KDK substep from a fresh state (tree, gravity, neighbours and density valid for the positions). It
+// rebuilds once, so it flips the state double buffer.
+sph_status kdk_steady(sph_ctx* ctx) {
+  Dev& d = ctx->d;
+  cudaStream_t s = ctx->stream;
+  forces(ctx);
+  phase(ctx, SPH_PHASE_INTEGRATE, [&] { return launch_finalize_dt(d, s) + launch_kick_drift(d, s); });
+  sph_status st = rebuild(ctx, false);
+  if (st != SPH_OK) return st;
+  forces(ctx);
+  phase(ctx, SPH_PHASE_INTEGRATE, [&] { return launch_kick(d, s); });
+  return SPH_OK;
+}
+
+// Two steady substeps as one CUDA graph launch. Two substeps flip the double buffer twice, so a graph
+// captured with the buffer in one parity replays from that parity; one graph per parity is kept until the
+// next upload. Everything the kernels read that the host may change between replays (dt, AV, omega) is in
+// device memory, and every launch shape depends only on the uploaded particle and leaf counts.
+sph_status kdk_graph_launch(sph_ctx* ctx) {
+  Dev& d = ctx->d;
+  const int par = d.cur;
+  cudaStream_t s = ctx->stream;
+  if (!ctx->kdk_graph[par]) {
+    const unsigned long long l0 = ctx->launches;
+    CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    sph_status st = kdk_steady(ctx);
+    if (st == SPH_OK) st = kdk_steady(ctx);
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(s, &g);
+    if (st != SPH_OK) {
+      if (g) cudaGraphDestroy(g);
+      return st;
+    }
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaStreamEndCapture");
+    cudaGraphExec_t ex = nullptr;
+    const cudaError_t ei = cudaGraphInstantiate(&ex, g, 0);
+    cudaGraphDestroy(g);
+    if (ei != cudaSuccess) return cuda_fail(ctx, ei, "cudaGraphInstantiate");
+    ctx->kdk_graph[par] = ex;
+    ctx->kdk_graph_launches = ctx->launches - l0;
+    ctx->launches = l0;  // capture launched nothing
+  }
+  CK(cudaGraphLaunch(ctx->kdk_graph[par], s));
+  ctx->launches += ctx->kdk_graph_launches;
   return SPH_OK;
 }
 
@@ -361,6 +478,7 @@ void sph_destroy(sph_ctx* ctx) {
     cudaEventDestroy(r.b);
   }
   for (cudaEvent_t e : ctx->pool) cudaEventDestroy(e);
+  drop_graphs(ctx);
   for (void* p : ctx->allocs) cudaFree(p);
   if (ctx->pinned_aos) cudaFreeHost(ctx->pinned_aos);
   if (ctx->rb_event) cudaEventDestroy(ctx->rb_event);
@@ -371,50 +489,35 @@ void sph_destroy(sph_ctx* ctx) {
 sph_status sph_upload(sph_ctx* ctx, const SphParticle48* particles, uint32_t n, const SphEos48* eos, uint32_t n_eos,
                       float softening) {
   if (!ctx || (!particles && n) || (!eos && n_eos)) return SPH_ERR_INVALID;
-  cudaSetDevice(ctx->device);
+  if (!std::isfinite(softening) || softening < 0.0f) return SPH_ERR_INVALID;
   sph_status ret = SPH_OK;
   uint32_t nu = n;
   if (nu > ctx->capacity) {
     nu = ctx->capacity;
     ret = SPH_CLAMPED;
   }
-  uint32_t ne = n_eos;
-  if (ne > (uint32_t)kMaxMaterials) {
-    ne = kMaxMaterials;
-    ret = SPH_CLAMPED;
+  const uint32_t off[2] = {0u, nu};
+  const sph_status st = upload_impl(ctx, particles, off, nu ? 1u : 0u, eos, n_eos, &softening);
+  return st == SPH_OK ? ret : st;
+}
+
+sph_status sph_upload_batch(sph_ctx* ctx, const SphParticle48* particles, const uint32_t* offsets,
+                            uint32_t n_impacts, const SphEos48* eos, uint32_t n_eos, const float* softening) {
+  if (!ctx || !particles || !offsets || !softening || (!eos && n_eos)) return SPH_ERR_INVALID;
+  if (n_impacts < 1 || n_impacts > (uint32_t)kMaxSegments || offsets[0] != 0u) {
+    ctx->err = "sph_upload_batch: need 1..256 impacts and offsets[0] = 0";
+    return SPH_ERR_INVALID;
   }
-  if (!std::isfinite(softening) || softening < 0.0f) return SPH_ERR_INVALID;
-  for (uint32_t i = 0; i < nu; ++i) {
-    const SphParticle48& p = particles[i];
-    if (p.mat >= ne || !std::isfinite(p.pos[0]) || !std::isfinite(p.pos[1]) || !std::isfinite(p.pos[2]) ||
-        !std::isfinite(p.vel[0]) || !std::isfinite(p.vel[1]) || !std::isfinite(p.vel[2]) || !std::isfinite(p.u) ||
-        !std::isfinite(p.mass) || !(p.h > 0.0f) || !std::isfinite(p.h) || p.mass < 0.0f) {
-      ctx->err = "particle " + std::to_string(i) + " has a material outside the table or a non-finite field";
+  for (uint32_t k = 0; k < n_impacts; ++k)
+    if (offsets[k + 1] <= offsets[k]) {
+      ctx->err = "sph_upload_batch: impact " + std::to_string(k) + " is empty or the offsets decrease";
       return SPH_ERR_INVALID;
     }
+  if (offsets[n_impacts] > ctx->capacity) {
+    ctx->err = "sph_upload_batch: the batch holds more particles than the context capacity";
+    return SPH_ERR_INVALID;
   }
-  CK(cudaStreamSynchronize(ctx->stream));
-  Dev& d = ctx->d;
-  d.n = (int)nu;
-  d.cur = 0;
-  d.L = nu > 0 ? (int)((nu + d.K - 1) / d.K) : 0;
-  d.idbits = bits_for(nu);
-  ctx->n_eos = ne;
-  if (nu) CK(cudaMemcpyAsync(d.aos, particles, (size_t)nu * 48, cudaMemcpyHostToDevice, ctx->stream));
-  Eos table[kMaxMaterials];
-  std::memset(table, 0, sizeof(table));
-  if (ne) std::memcpy(table, eos, (size_t)ne * sizeof(Eos));
-  CK(cudaMemcpyAsync(d.eos, table, sizeof(table), cudaMemcpyHostToDevice, ctx->stream));
-  ctx->hp.softening = softening;
-  ctx->hp.soft2 = softening * softening;
-  sph_status st = push_params(ctx, d);
-  if (st != SPH_OK) return st;
-  if (nu) launch_from_aos(d, ctx->stream);
-  CK(cudaGetLastError());
-  CK(cudaStreamSynchronize(ctx->stream));
-  ctx->uploaded = true;
-  ctx->fresh = false;
-  return ret;
+  return upload_impl(ctx, particles, offsets, n_impacts, eos, n_eos, softening);
 }
 
 sph_status sph_set_dt(sph_ctx* ctx, double dt, float damp) {
@@ -454,22 +557,24 @@ sph_status sph_eval_forces(sph_ctx* ctx) {
 sph_status sph_step_kdk(sph_ctx* ctx, uint32_t substeps) {
   sph_status st = check_ready(ctx);
   if (st != SPH_OK) return st;
-  Dev& d = ctx->d;
-  cudaStream_t s = ctx->stream;
-  for (uint32_t k = 0; k < substeps; ++k) {
+  const bool graphs = ctx->cfg.graph != 0 && !ctx->prof_on;
+  for (uint32_t k = 0; k < substeps;) {
     // eval 1 at x_n (the tree, gravity and density of the previous eval 2 are still exact: a kick moves no
     // particle), then dt, the half-kick + drift, eval 2 at x_{n+1}, the final half-kick.
     if (!ctx->fresh) {
       st = rebuild(ctx, true);
       if (st != SPH_OK) return st;
+      ctx->fresh = true;
     }
-    forces(ctx);
-    phase(ctx, SPH_PHASE_INTEGRATE, [&] { return launch_finalize_dt(d, s) + launch_kick_drift(d, s); });
-    st = rebuild(ctx, false);
+    if (graphs && substeps - k >= 2) {
+      st = kdk_graph_launch(ctx);
+      if (st != SPH_OK) return st;
+      k += 2;
+      continue;
+    }
+    st = kdk_steady(ctx);
     if (st != SPH_OK) return st;
-    forces(ctx);
-    phase(ctx, SPH_PHASE_INTEGRATE, [&] { return launch_kick(d, s); });
-    ctx->fresh = true;
+    ++k;
   }
   CK(cudaGetLastError());
   return SPH_OK;
@@ -573,7 +678,10 @@ sph_status sph_diag(sph_ctx* ctx, sph_diag_out* out) {
   if (ctx->d.n) launch_diag(ctx->d, ctx->stream, ctx->d_diag);
   double v[16] = {0};
   DevParams p;
+  Seg s0;
+  std::memset(&s0, 0, sizeof(s0));
   if (ctx->d.n) CK(cudaMemcpyAsync(v, ctx->d_diag, sizeof(v), cudaMemcpyDeviceToHost, ctx->stream));
+  if (ctx->uploaded) CK(cudaMemcpyAsync(&s0, ctx->d.segs, sizeof(Seg), cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaMemcpyAsync(&p, ctx->d.P, sizeof(p), cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
   out->mass = v[0];
@@ -584,8 +692,8 @@ sph_status sph_diag(sph_ctx* ctx, sph_diag_out* out) {
     out->momentum[k] = v[4 + k];
     out->angular_momentum[k] = v[7 + k];
   }
-  out->dt = p.dt;
-  out->time = p.time;
+  out->dt = s0.dt;
+  out->time = s0.time;
   out->steps = p.steps;
   out->max_neighbours_seen = p.max_nbr_seen;
   out->overflow_flags = p.flags;
@@ -627,22 +735,34 @@ sph_status sph_inspect(sph_ctx* ctx, uint32_t what, void* host_out, size_t bytes
   };
   switch (what) {
     case SPH_Q_BBOX: {
-      if (!need(24)) return SPH_ERR_INVALID;
-      DevParams p;
-      CK(cudaMemcpy(&p, d.P, sizeof(p), cudaMemcpyDeviceToHost));
+      // as many impacts as the buffer holds
+      const size_t m = std::min(bytes / 24, (size_t)d.nseg);
+      if (m == 0) return SPH_ERR_INVALID;
+      std::vector<Seg> tab(m);
+      CK(cudaMemcpy(tab.data(), d.segs, m * sizeof(Seg), cudaMemcpyDeviceToHost));
       float* f = (float*)host_out;
-      for (int k = 0; k < 6; ++k) {
-        const unsigned key = p.bbox_keys[k];
-        unsigned bits = (key >> 31) ? (key ^ 0x80000000u) : ~key;
-        std::memcpy(&f[k], &bits, 4);
-      }
+      for (size_t g = 0; g < m; ++g)
+        for (int k = 0; k < 6; ++k) {
+          const unsigned key = tab[g].bbox[k];
+          unsigned bits = (key >> 31) ? (key ^ 0x80000000u) : ~key;
+          std::memcpy(&f[6 * g + k], &bits, 4);
+        }
       return SPH_OK;
     }
     case SPH_Q_CODES: {
       if (!need(n * 4)) return SPH_ERR_INVALID;
       std::vector<unsigned long long> k(n);
       CK(cudaMemcpy(k.data(), d.keys[0], n * 8, cudaMemcpyDeviceToHost));
-      for (size_t t = 0; t < n; ++t) ((unsigned*)host_out)[t] = (unsigned)(k[t] >> d.idbits);
+      for (size_t t = 0; t < n; ++t) ((unsigned*)host_out)[t] = (unsigned)(k[t] >> d.idbits) & 0x3fffffffu;
+      return SPH_OK;
+    }
+    case SPH_Q_IMPACT_DT:
+    case SPH_Q_IMPACT_TIME: {
+      const size_t m = (size_t)d.nseg;
+      if (!need(m * 8)) return SPH_ERR_INVALID;
+      std::vector<Seg> tab(m);
+      CK(cudaMemcpy(tab.data(), d.segs, m * sizeof(Seg), cudaMemcpyDeviceToHost));
+      for (size_t g = 0; g < m; ++g) ((double*)host_out)[g] = what == SPH_Q_IMPACT_DT ? tab[g].dt : tab[g].time;
       return SPH_OK;
     }
     case SPH_Q_ORDER:
@@ -796,6 +916,8 @@ sph_status sph_gravity(sph_ctx* ctx, const double* pos3, const double* mass, uin
   g.n = (int)n;
   g.cur = 0;
   g.L = (int)((n + g.K - 1) / g.K);
+  g.nseg = 1;
+  g.segbits = 0;
   g.idbits = bits_for(n);
   std::vector<float4> ph(n);
   std::vector<double> xs(n), ys(n), zs(n);
@@ -820,10 +942,10 @@ sph_status sph_gravity(sph_ctx* ctx, const double* pos3, const double* mass, uin
   CK(cudaMemsetAsync(st0.vel_u, 0, n * 16, s));
   CK(cudaMemsetAsync(st0.mat, 0, n * 4, s));
   CK(cudaMemsetAsync(st0.prov, 0, n * 4, s));
+  CK(cudaMemsetAsync(st0.seg, 0, n * 4, s));
   DevParams p = ctx->hp;
-  p.softening = (float)softening;
-  p.soft2 = (float)softening * (float)softening;
   CK(cudaMemcpyAsync(g.P, &p, sizeof(p), cudaMemcpyHostToDevice, s));
+  launch_segments_single(g, (float)softening * (float)softening, 0.0, s);
   launch_bbox(g, s);
   launch_sort_permute(g, s);
   if (gravity_mode == SPH_GRAVITY_TREE) {
@@ -976,10 +1098,13 @@ sph_status sph_dem_replace(sph_dem* dem, const SphGrain80* grains, uint32_t n) {
   d.n = (int)n;
   d.cur = 0;
   d.L = n ? (int)((n + d.K - 1) / d.K) : 0;
+  d.nseg = 1;
+  d.segbits = 0;
   d.idbits = bits_for(n);
   if (n) {
     CK(cudaMemcpyAsync(dem->grains, grains, (size_t)n * 80, cudaMemcpyHostToDevice, ctx->stream));
     launch_dem_load(d, dem->grains, ctx->stream);
+    launch_segments_single(d, 0.0f, 0.0, ctx->stream);
   }
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(ctx->stream));

@@ -21,21 +21,17 @@ struct Eos {
   float rho0, a, b, cap_a, cap_b, e0, e_iv, e_cv, alpha, beta, p0, p1;
 };
 
-// Physics scalars read by the kernels from device memory (so a captured graph sees host updates).
+// Physics scalars read by the kernels from device memory (so a captured graph sees host updates). The
+// per-impact quantities (dt, time, softening, bounding box, Courant signal) live in the segment table.
 struct DevParams {
-  double dt;          // dt of the current step (fixed dt, or cfl·min signal when cfl > 0)
   double dt_fixed;    // host-set dt (sph_set_dt)
-  double time;        // simulated time
-  float softening;
-  float soft2;
   float av_alpha, av_beta;
   float damp, omega;
   float G;            // f32 G for the force kernels
   float theta;
   float cfl;
   float rho_floor, du_floor, r_min, sig_floor;
-  unsigned sig_min_bits;  // atomicMin target: bits of the min Courant signal (positive floats order as uints)
-  unsigned bbox_keys[6];  // order-preserving u32 keys of lo.xyz, hi.xyz (bh_gravity.wgsl:49-57)
+  // ---- maintained by the device from here on --------------------------------------------------------
   unsigned flags;         // kFlag* bits
   unsigned max_nbr_seen;
   unsigned steps;

@@ -19,7 +19,87 @@ struct State {
   unsigned* mat = nullptr;
   unsigned* prov = nullptr;
   unsigned* id = nullptr;
+  unsigned* seg = nullptr;  // impact (segment) of the particle in a batch; 0 for a single impact
 };
+
+// A batch holds up to kMaxSegments independent impacts ("segments"). Sorted particles of segment k are
+// [segs[k].off, segs[k+1].off) and its leaves [segs[k].loff, segs[k+1].loff): a leaf holds <= K particles and
+// never crosses a segment boundary, so each segment is one subtree of the LBVH (its root in segs[k].root).
+// Entry nseg closes the ranges (off = n, loff = L). One impact is the batch of one segment.
+constexpr int kMaxSegments = 256;  // 8 sort-key bits above the 30-bit Morton code
+struct Seg {
+  unsigned off, loff;   // first sorted particle, first leaf
+  unsigned root;        // LBVH node spanning exactly this segment (rebuilt with the tree)
+  unsigned sig_bits;    // atomicMin target: bits of the segment's minimum Courant signal
+  unsigned bbox[6];     // order-preserving keys of lo.xyz, hi.xyz (bh_gravity.wgsl:49-57)
+  float soft2;          // softening² of this impact
+  unsigned pad;
+  double dt;            // dt of the current step
+  double time;          // simulated time
+};
+static_assert(sizeof(Seg) == 64, "Seg is one 64-byte record");
+constexpr unsigned kNoSeg = 0xffffffffu;
+
+// Reduce per-thread boxes (order-preserving keys, identity values when the thread holds no point) into the
+// segment table. Particles are contiguous per segment, so almost every block lies in one segment and commits
+// with one atomic per axis; a block that straddles segments commits per warp (warps inside one segment) or
+// per thread. `sg` is the thread's segment, kNoSeg when it holds no point. All threads of the block call it.
+__device__ __forceinline__ void seg_bbox_commit(unsigned lo[3], unsigned hi[3], unsigned sg, Seg* segs) {
+  __shared__ unsigned s_lo[3][32], s_hi[3][32], s_sg[2][32];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  const unsigned wmin = warp_min(sg), wmax = warp_max(sg == kNoSeg ? 0u : sg);
+  if (lane == 0) {
+    s_sg[0][w] = wmin;
+    s_sg[1][w] = wmax;
+  }
+  __syncthreads();
+  unsigned bmin = kNoSeg, bmax = 0u;
+  for (int k = 0; k < nw; ++k) {
+    bmin = min(bmin, s_sg[0][k]);
+    bmax = max(bmax, s_sg[1][k]);
+  }
+  if (bmin == kNoSeg) return;  // block-uniform: no point in this block
+  if (bmin == bmax) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      lo[k] = warp_min(lo[k]);
+      hi[k] = warp_max(hi[k]);
+      if (lane == 0) { s_lo[k][w] = lo[k]; s_hi[k][w] = hi[k]; }
+    }
+    __syncthreads();
+    if (w == 0) {
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        unsigned a = lane < nw ? s_lo[k][lane] : 0xffffffffu;
+        unsigned b = lane < nw ? s_hi[k][lane] : 0u;
+        a = warp_min(a);
+        b = warp_max(b);
+        if (lane == 0) {
+          atomicMin(&segs[bmin].bbox[k], a);
+          atomicMax(&segs[bmin].bbox[3 + k], b);
+        }
+      }
+    }
+    return;
+  }
+  if (wmin == kNoSeg) return;
+  if (wmin == wmax) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const unsigned a = warp_min(lo[k]), b = warp_max(hi[k]);
+      if (lane == 0) {
+        atomicMin(&segs[wmin].bbox[k], a);
+        atomicMax(&segs[wmin].bbox[3 + k], b);
+      }
+    }
+  } else if (sg != kNoSeg) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      atomicMin(&segs[sg].bbox[k], lo[k]);
+      atomicMax(&segs[sg].bbox[3 + k], hi[k]);
+    }
+  }
+}
 
 struct Dev {
   int n = 0, cap = 0;
@@ -34,7 +114,11 @@ struct Dev {
   unsigned* rs_hist = nullptr;  // [256][tiles]
   unsigned* rs_tot = nullptr;   // [256]
   int rs_tiles_cap = 0;
-  unsigned* leaf_codes = nullptr;
+  int nseg = 1;
+  int segbits = 0;                 // sort-key bits of the segment index (0 for one segment)
+  Seg* segs = nullptr;             // [kMaxSegments + 1]
+  unsigned* leaf_start = nullptr;  // [L+1] first sorted particle of each leaf
+  unsigned long long* leaf_codes = nullptr;  // segment << 30 | Morton code of each leaf's first particle
   unsigned* left = nullptr;     // [L-1]
   unsigned* right = nullptr;    // [L-1]
   unsigned* parent = nullptr;   // [2L-1]
@@ -87,8 +171,9 @@ int launch_dem_store(const Dev& d, void* grains, cudaStream_t s);
 int launch_dem_contacts(const Dev& d, const DemParams& p, float4* acc, cudaStream_t s);
 int launch_dem_integrate(const Dev& d, const DemParams& p, const float4* acc, cudaStream_t s);
 
-// ---- tree ------------------------------------------------------------------------------------------
-int launch_bbox_reset(const Dev& d, cudaStream_t s);
+// ---- segments and tree -----------------------------------------------------------------------------
+int launch_segments(const Dev& d, cudaStream_t s);        // leaf_start from the segment table
+int launch_segments_single(const Dev& d, float soft2, double dt, cudaStream_t s);  // one segment, on the device
 int launch_bbox(const Dev& d, cudaStream_t s);
 int launch_sort_permute(Dev& d, cudaStream_t s);      // keys → radix sort → permute (swaps d.cur)
 int launch_tree(const Dev& d, const Cfg& c, float theta, cudaStream_t s);  // Karras + moments

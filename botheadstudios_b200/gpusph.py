@@ -62,7 +62,37 @@ class GpuSph:
         if st == _lib.SPH_CLAMPED:
             warnings.warn("upload clamped to capacity / material table size")
         self.softening = float(softening)
+        self.n_impacts = 1
         return st
+
+    def upload_batch(self, particles: np.ndarray, offsets, eos: np.ndarray, softening) -> int:
+        """Independent impacts in one context: impact k = particles[offsets[k]:offsets[k+1]], each with its
+        own softening (a scalar applies to all). Every phase of a step is one launch over all impacts."""
+        p = np.ascontiguousarray(particles, dtype=PARTICLE_DTYPE)
+        off = np.ascontiguousarray(offsets, dtype=np.uint32)
+        k = len(off) - 1
+        soft = np.ascontiguousarray(np.broadcast_to(np.asarray(softening, np.float32), (k,)))
+        e = np.ascontiguousarray(eos, dtype=np.float32).reshape(-1, 12)
+        if k < 1 or int(off[-1]) != len(p):
+            raise ValueError("offsets must start at 0 and end at len(particles)")
+        st = self._check(self._L.sph_upload_batch(self._h, _ptr(p), _ptr(off), k, _ptr(e), len(e), _ptr(soft)),
+                         "sph_upload_batch")
+        self.n_impacts = k
+        self.softening = soft.copy()
+        return st
+
+    def impact_dt(self) -> np.ndarray:
+        """dt of each impact's last step."""
+        out = np.zeros(getattr(self, "n_impacts", 1), np.float64)
+        self._check(self._L.sph_inspect(self._h, Q["IMPACT_DT"], _ptr(out), out.nbytes), "sph_inspect(IMPACT_DT)")
+        return out
+
+    def impact_time(self) -> np.ndarray:
+        """Simulated time of each impact."""
+        out = np.zeros(getattr(self, "n_impacts", 1), np.float64)
+        self._check(self._L.sph_inspect(self._h, Q["IMPACT_TIME"], _ptr(out), out.nbytes),
+                    "sph_inspect(IMPACT_TIME)")
+        return out
 
     def set_dt(self, dt: float, damp: float = 1.0):
         self._check(self._L.sph_set_dt(self._h, float(dt), float(damp)), "sph_set_dt")
@@ -153,7 +183,8 @@ class GpuSph:
         L = self.n_leaves()
         nn = max(2 * L - 1, 0)
         cap = int(self.config.max_neighbours)
-        shapes = dict(BBOX=(np.float32, (6,)), CODES=(np.uint32, (n,)), ORDER=(np.uint32, (n,)),
+        k = getattr(self, "n_impacts", 1)
+        shapes = dict(BBOX=(np.float32, (6,) if k == 1 else (k, 6)), CODES=(np.uint32, (n,)), ORDER=(np.uint32, (n,)),
                       LEFT=(np.uint32, (max(L - 1, 0),)), RIGHT=(np.uint32, (max(L - 1, 0),)),
                       PARENT=(np.uint32, (nn,)), NODE_COM=(np.float32, (nn, 4)), NODE_BMIN=(np.float32, (nn, 4)),
                       NODE_BMAX=(np.float32, (nn, 4)), NBR_COUNT=(np.uint32, (n,)), NBR_LIST=(np.uint32, (n, cap)),

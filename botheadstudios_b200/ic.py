@@ -154,3 +154,55 @@ def config_kwargs(units: Units) -> dict:
     """The unit-dependent fields of sph_config for these initial conditions."""
     return dict(G=units.G, rho_floor=units.rho_floor, du_floor=units.du_floor, r_min=units.r_min,
                 sig_floor=units.sig_floor)
+
+
+@dataclass
+class Batch:
+    particles: np.ndarray  # PARTICLE_DTYPE, impacts concatenated
+    offsets: np.ndarray    # uint32 [n_impacts + 1]
+    softening: np.ndarray  # float32 [n_impacts]
+    eos: np.ndarray
+    units: Units
+    params: list           # per impact: dict(n, mass_ratio, angle_deg, v_factor, seed)
+
+    @property
+    def n_impacts(self) -> int:
+        return len(self.offsets) - 1
+
+    def impact(self, k: int) -> np.ndarray:
+        return self.particles[self.offsets[k]:self.offsets[k + 1]]
+
+
+def batch_draws(n_impacts: int, n_min: int, n_max: int, seed: int, mass_ratio=(0.05, 0.15), angle_deg=(0.0, 75.0),
+                v_factor=(1.0, 1.5)) -> list:
+    """The seeded per-impact draws of batch() (sizes and collision parameters) without building bodies."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n_impacts):
+        n = int(round(math.exp(rng.uniform(math.log(n_min), math.log(n_max)))))
+        q = float(rng.uniform(*mass_ratio))
+        ang = float(rng.uniform(*angle_deg))
+        vf = float(rng.uniform(*v_factor))
+        s = int(rng.integers(1, 2 ** 31 - 1))
+        out.append(dict(n=n, mass_ratio=q, angle_deg=ang, v_factor=vf, seed=s))
+    return out
+
+
+def batch(n_impacts: int, n_min: int = 20_000, n_max: int = 200_000, n_ngb: float = 64.0, seed: int = 11,
+          mass_ratio=(0.05, 0.15), angle_deg=(0.0, 75.0), v_factor=(1.0, 1.5)) -> Batch:
+    """Independent two-body impacts of uneven size (the batched workload): total particle counts log-uniform
+    in [n_min, n_max], impactor mass ratio, impact angle and v_imp/v_esc uniform in the given ranges, every
+    draw from one seeded generator. Particles have equal mass within an impact, so the impactor holds the
+    fraction q/(1+q) of them."""
+    parts, offs, soft, params = [], [0], [], []
+    I = None
+    for d in batch_draws(n_impacts, n_min, n_max, seed, mass_ratio, angle_deg, v_factor):
+        n, q, ang, vf, s = d["n"], d["mass_ratio"], d["angle_deg"], d["v_factor"], d["seed"]
+        n_i = max(1, int(round(n * q / (1.0 + q))))
+        I = impact(n - n_i, n_i, n_ngb=n_ngb, mass_ratio=q, v_factor=vf, angle_deg=ang, seed=s)
+        parts.append(I.particles)
+        offs.append(offs[-1] + len(I.particles))
+        soft.append(I.softening)
+        params.append(dict(n=n, mass_ratio=q, angle_deg=ang, v_factor=vf, seed=s))
+    return Batch(particles=np.concatenate(parts), offsets=np.asarray(offs, np.uint32),
+                 softening=np.asarray(soft, np.float32), eos=I.eos, units=I.units, params=params)

@@ -17,10 +17,41 @@ WORKLOADS = {
     # the precision-sweep body: a 4,194,304-particle differentiated planet at rest (θ swept by the caller)
     "planet_4m": dict(kind="planet", n_target=4_194_304, n_impactor=0, n_ngb=64.0, kernel="wendland", theta=0.5,
                       quad=1, leaf=16, h_solve=1, max_nbr=192),
+    # 256 independent impacts, total particle counts log-uniform in [20k, 200k] (about 2.0e7 particles), mass
+    # ratio 0.05-0.15, angle 0-75°, v_imp 1.0-1.5 v_esc; the 1M impact's method; one launch per phase for all
+    # impacts, steady steps replayed from a captured CUDA graph
+    "batch_256": dict(kind="batch", n_impacts=256, n_min=20_000, n_max=200_000, n_ngb=64.0, kernel="wendland",
+                      theta=0.6, quad=1, leaf=16, h_solve=1, max_nbr=192, graph=1),
+    # the same draw with 16 impacts (a quick check of the batched path)
+    "batch_16": dict(kind="batch", n_impacts=16, n_min=20_000, n_max=200_000, n_ngb=64.0, kernel="wendland",
+                     theta=0.6, quad=1, leaf=16, h_solve=1, max_nbr=192, graph=1),
 }
 
 
-def build(wl: dict, seed: int = 1) -> ic.Impact:
+def impactor_fraction(wl: dict) -> float:
+    """Fraction of a workload's particles in the impactor (the batch: mass ratio 0.1 at the range centre)."""
+    if wl.get("kind") == "batch":
+        return 0.1 / 1.1
+    return wl["n_impactor"] / (wl["n_target"] + wl["n_impactor"])
+
+
+def n_particles(wl: dict, seed: int = 1) -> int:
+    """Particles of the workload build(wl, seed) makes, without building it."""
+    if wl.get("kind") == "batch":
+        return sum(d["n"] for d in ic.batch_draws(wl["n_impacts"], wl["n_min"], wl["n_max"], 10 + seed))
+    return wl["n_target"] + wl["n_impactor"]
+
+
+def upload(s, I) -> int:
+    """Upload a built workload (one impact, or a batch) into a solver."""
+    if isinstance(I, ic.Batch):
+        return s.upload_batch(I.particles, I.offsets, I.eos, I.softening)
+    return s.upload(I.particles, I.eos, I.softening)
+
+
+def build(wl: dict, seed: int = 1):
+    if wl.get("kind") == "batch":
+        return ic.batch(wl["n_impacts"], wl["n_min"], wl["n_max"], n_ngb=wl["n_ngb"], seed=10 + seed)
     if wl.get("kind") == "planet":
         return ic.planet(wl["n_target"], n_ngb=wl["n_ngb"], seed=seed)
     return ic.impact(wl["n_target"], wl["n_impactor"], n_ngb=wl["n_ngb"], seed=seed)
@@ -30,6 +61,6 @@ def solver(wl: dict, I: ic.Impact, device: int = -1, **over):
     from .gpusph import GpuSph
     kw = dict(theta=wl["theta"], leaf_size=wl["leaf"], kernel=wl["kernel"], multipole=wl["quad"],
               h_mode=wl["h_solve"], h_neighbours=wl["n_ngb"], h_iters=2, max_neighbours=wl["max_nbr"], cfl=0.3,
-              device=device, **ic.config_kwargs(I.units))
+              graph=wl.get("graph", 0), device=device, **ic.config_kwargs(I.units))
     kw.update(over)
     return GpuSph(len(I.particles), **kw)

@@ -80,7 +80,9 @@ typedef struct sph_config {
   float sig_floor;        /* sph_step.wgsl:268 max(c+|v|, 1)    (SI value 1)    */
   int32_t device;         /* CUDA device ordinal of the context; -1 = the calling thread's current device */
   uint32_t mac;           /* SPH_MAC_*: GROUP (default) or PARTICLE (the reference's per-particle walk) */
-  uint32_t reserved[6];
+  uint32_t graph;         /* nonzero: sph_step_kdk captures its steady two-substep sequence once in a CUDA graph
+                             and replays it (phase timing is not recorded for replayed substeps) */
+  uint32_t reserved[5];
 } sph_config;
 
 /* Barnes-Hut acceptance. PARTICLE: each particle walks with the GPU reference's MAC
@@ -102,8 +104,8 @@ typedef struct sph_diag_out {
   double momentum[3];
   double angular_momentum[3];            /* about the origin */
   double mass;
-  double dt;                             /* the dt of the last step (adaptive or fixed) */
-  double time;                           /* simulated time accumulated by sph_step_kdk */
+  double dt;                             /* the dt of the last step (adaptive or fixed; impact 0 of a batch) */
+  double time;                           /* simulated time accumulated by sph_step_kdk (impact 0 of a batch) */
   uint32_t steps;
   uint32_t max_neighbours_seen;
   uint32_t overflow_flags;               /* bit0 neighbour list, bit1 traversal stack */
@@ -130,6 +132,19 @@ void sph_destroy(sph_ctx* ctx);
  * rebuilds everything from the uploaded state. */
 sph_status sph_upload(sph_ctx* ctx, const SphParticle48* particles, uint32_t n, const SphEos48* eos,
                       uint32_t n_eos, float softening);
+
+/* Batched impacts. No counterpart in the reference: its offline driver runs impacts one after another
+ * (tools/impact-run/src/main.rs:645-671). Uploads `n_impacts` independent impacts as one particle array,
+ * impact k being particles [offsets[k], offsets[k+1]) with softening softening[k]. Every phase of a step
+ * then runs as one launch over all impacts. Impacts never interact: each is quantised in its own box, sorted
+ * into its own range and built into its own subtree, so its neighbours and gravity come from itself alone,
+ * and each advances with its own adaptive dt (SPH_Q_IMPACT_DT). An impact gets the same result as a context
+ * that holds it alone. Particles keep their batch index (readback order). Requires 1 <= n_impacts <=
+ * SPH_MAX_IMPACTS, offsets[0] = 0, every impact non-empty, and offsets[n_impacts] <= capacity: an impact is
+ * never clamped. sph_upload is the batch of one impact. */
+#define SPH_MAX_IMPACTS 256
+sph_status sph_upload_batch(sph_ctx* ctx, const SphParticle48* particles, const uint32_t* offsets,
+                            uint32_t n_impacts, const SphEos48* eos, uint32_t n_eos, const float* softening);
 
 /* GpuSph::set_dt (gpu_sph.rs:855-859) and set_av (:865-869); SphParams.omega (gpu_sph.rs:60-79). */
 sph_status sph_set_dt(sph_ctx* ctx, double dt, float damp);
@@ -170,8 +185,8 @@ const char* sph_status_string(sph_status s);
  * tools/gpu-bh-verify/src/main.rs and tools/sph-verify/src/main.rs). Sorted-space arrays come back in
  * Morton order; per-particle physical quantities come back in original particle order. */
 enum {
-  SPH_Q_BBOX = 0,        /* float[6]   lo.xyz, hi.xyz (cs_bbox) */
-  SPH_Q_CODES = 1,       /* uint32[n]  sorted Morton codes */
+  SPH_Q_BBOX = 0,        /* float[6·n_impacts] lo.xyz, hi.xyz of each impact (cs_bbox) */
+  SPH_Q_CODES = 1,       /* uint32[n]  sorted Morton codes (each in its impact's box; impacts in order) */
   SPH_Q_ORDER = 2,       /* uint32[n]  original index at each sorted position (the sort permutation) */
   SPH_Q_LEFT = 3,        /* uint32[L-1] */
   SPH_Q_RIGHT = 4,       /* uint32[L-1] */
@@ -187,7 +202,9 @@ enum {
   SPH_Q_ACC_SPH = 14,    /* float4[n]  SPH acceleration xyz, du/dt */
   SPH_Q_ACC_GRAV = 15,   /* float4[n]  gravity acceleration xyz, potential */
   SPH_Q_H = 16,          /* float[n]   smoothing lengths */
-  SPH_Q_N_LEAVES = 17    /* uint32[1]  L */
+  SPH_Q_N_LEAVES = 17,   /* uint32[1]  L */
+  SPH_Q_IMPACT_DT = 18,  /* double[n_impacts] dt of each impact's last step */
+  SPH_Q_IMPACT_TIME = 19 /* double[n_impacts] simulated time of each impact */
 };
 sph_status sph_inspect(sph_ctx* ctx, uint32_t what, void* host_out, size_t bytes);
 
