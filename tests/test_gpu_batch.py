@@ -105,7 +105,8 @@ def test_graph_replay_matches_eager():
             s.upload_batch(B.particles, B.offsets, B.eos, B.softening)
             s.encode_kdk(1)                 # eager first step (fresh rebuild)
             s.profile_enable(False)         # reset the launch count; timing off so the graph is used
-            s.encode_kdk(5)                 # two replays (both parities) + one eager substep
+            s.encode_kdk(5)                 # two replays of one graph + one eager substep (flips the parity)
+            s.encode_kdk(2)                 # one replay of the graph captured at the other parity
             res.append((s.readback(), s.profile_read()["kernel_launches"], s.impact_time()))
     _same(res[0][0], res[1][0])
     assert res[0][1] == res[1][1] > 0
@@ -119,7 +120,7 @@ def test_batch_upload_rejects_bad_offsets():
         with pytest.raises(SphError):  # an empty impact
             s.upload_batch(B.particles, [0, 0, n], B.eos, 0.01)
         with pytest.raises(SphError):  # more impacts than the key has bits for
-            s.upload_batch(B.particles, np.arange(258), B.eos, 0.01)
+            s.upload_batch(B.particles[:257], np.arange(258), B.eos, 0.01)
     with GpuSph(n - 1, **_cfg(B.units)) as s:
         with pytest.raises(SphError):  # a batch is never clamped
             s.upload_batch(B.particles, B.offsets, B.eos, B.softening)
