@@ -143,9 +143,84 @@ def build_workload(wl: dict, seed: int):
     return workloads.build(wl, seed)
 
 
-def make_solver(wl: dict, I, device: int):
+class SingleRunner:
+    """One impact in one context (the interface of batching.BucketedBatch)."""
+
+    def __init__(self, wl: dict, I, device: int):
+        from botheadstudios_b200 import workloads
+        self.I = I
+        self.s = workloads.solver(wl, I, device)
+        self.ctxs = [self.s]
+        self.n = len(I.particles)
+        self.batch = I
+
+    def upload(self, particles=None):
+        p = self.I.particles if particles is None else particles
+        if hasattr(self.I, "offsets"):
+            self.s.upload_batch(p, self.I.offsets, self.I.eos, self.I.softening)
+        else:
+            self.s.upload(p, self.I.eos, self.I.softening)
+
+    def encode_kdk(self, k):
+        self.s.encode_kdk(k)
+
+    def sync(self):
+        self.s.sync()
+
+    def readback_into(self, out):
+        self.s.readback_into(out)
+
+
+def make_runner(wl: dict, I, device: int):
+    """The runner of a workload and, for a batch, the autotuner's choices and measurements."""
+    if wl.get("kind") != "batch":
+        return SingleRunner(wl, I, device), None
+    from botheadstudios_b200 import batching, workloads
+    base = workloads.config(wl, I)
+    tuned = None
+    choices = {}
+    if wl.get("autotune"):
+        choices, log = batching.tune_buckets(I, base, device=device)
+        tuned = dict(choices={str(b): c for b, c in choices.items()},
+                     measured=[dict(c["choice"], rate=round(c["rate"])) for c in log])
+    return batching.BucketedBatch(I, base, choices, device=device), tuned
+
+
+def timed(ctxs, encode, steps: int, local: int) -> float:
+    """Device time (ms) of encode(steps) over the contexts `ctxs`: an event on the current stream that every
+    context stream waits for, the steps, then an event after every context stream has finished."""
+    import torch
+    main = torch.cuda.current_stream(local)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    exts = [torch.cuda.ExternalStream(s.stream(), device=f"cuda:{local}") for s in ctxs]
+    e0.record(main)
+    for x in exts:
+        x.wait_event(e0)
+    encode(steps)
+    for x in exts:
+        ev = torch.cuda.Event()
+        ev.record(x)
+        main.wait_event(ev)
+    e1.record(main)
+    e1.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def plain_sequential(wl: dict, B, device: int, impacts: int = 16, steps: int = 2) -> dict:
+    """The plain GPU form on a batch's impacts: one impact at a time, each in its own context with the
+    workload's untuned configuration, no graph (the reference's offline driver runs impacts sequentially)."""
     from botheadstudios_b200 import workloads
-    return workloads.solver(wl, I, device)
+    from botheadstudios_b200.gpusph import GpuSph
+    tot_ps, tot_ms = 0, 0.0
+    for k in range(min(impacts, B.n_impacts)):
+        p = B.impact(k)
+        with GpuSph(len(p), device=device, **workloads.config(wl, B, graph=0)) as s:
+            s.upload(p, B.eos, float(B.softening[k]))
+            s.encode_kdk(1)
+            s.sync()
+            tot_ms += timed([s], s.encode_kdk, steps, max(device, 0))
+            tot_ps += len(p) * steps
+    return dict(value=tot_ps / (tot_ms / 1000.0), impacts=min(impacts, B.n_impacts), steps=steps)
 
 
 # ---------------------------------------------------------------------------------------------------------
@@ -205,57 +280,62 @@ def run_reference(args, wl, world, rank, local, pg):
 def run_ours(args, wl, world, rank, local, pg):
     import torch
 
-    from botheadstudios_b200.workloads import upload
     I = build_workload(wl, seed=1 + rank)
-    n = len(I.particles)
-    s = make_solver(wl, I, local)
-    upload(s, I)
-    ext = torch.cuda.ExternalStream(s.stream(), device=f"cuda:{local}")
+    runner, tuned = make_runner(wl, I, local)
+    n = runner.n
+    runner.upload()
     # warm-up (includes the first full force evaluation, and the graph captures when graphs are on)
-    s.encode_kdk(args.warmup)
-    s.sync()
-    dstart = s.diag()
-    s.profile_enable(False)  # launch count only: phase events off, so captured graphs replay
+    runner.encode_kdk(args.warmup)
+    runner.sync()
+    dstart = [s.diag() for s in runner.ctxs]
+    for s in runner.ctxs:
+        s.profile_enable(False)  # launch count only: phase events off, so captured graphs replay
     barrier(pg)
     torch.cuda.synchronize(local)
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
-        ev0.record(ext)
-        s.encode_kdk(args.steps)
-        ev1.record(ext)
-        ev1.synchronize()
+        ms = timed(runner.ctxs, runner.encode_kdk, args.steps, local)
     torch.cuda.synchronize(local)
     barrier(pg)
-    ms = ev0.elapsed_time(ev1)
-    launches = s.profile_read()["kernel_launches"]
+    launches = sum(s.profile_read()["kernel_launches"] for s in runner.ctxs)
     ms_max = max_over_ranks(pg, ms, local)
     value = n * args.steps * world / (ms_max / 1000.0)
-    # per-phase breakdown and walk counters: a few more steps with phase events (eager launches)
-    d0 = s.diag()
-    s.profile_enable(True)
-    s.encode_kdk(min(args.steps, 4))
-    prof = s.profile_read()
-    s.profile_enable(False)
-    d1 = s.diag(check=False)
+    # per-phase breakdown and walk counters: a few more steps with phase events (eager launches), one
+    # context at a time so that every kernel duration is its own
+    prof = dict(ms={}, calls={})
+    d0, d1 = [], []
+    for s in runner.ctxs:
+        d0.append(s.diag())
+        s.profile_enable(True)
+        s.encode_kdk(min(args.steps, 4))
+        pr = s.profile_read()
+        s.profile_enable(False)
+        d1.append(s.diag(check=False))
+        cnt = s.count()
+        for k, t in pr["ms"].items():
+            prof["ms"][k] = prof["ms"].get(k, 0.0) + t
+            prof["calls"][k] = prof["calls"].get(k, 0) + pr["calls"][k]
+            prof.setdefault("pcalls", {})[k] = prof.setdefault("pcalls", {}).get(k, 0) + pr["calls"][k] * cnt
+
+    def dsum(ds, key):
+        return sum(d[key] for d in ds)
 
     # ---- end to end through the public API: per step, upload the state from pinned host memory, one KDK
     # step, read the state back into host memory ----
-    pin = torch.empty(n * 48, dtype=torch.uint8, pin_memory=True).numpy().view(I.particles.dtype)
-    s.readback_into(pin)
+    pin = torch.empty(n * 48, dtype=torch.uint8, pin_memory=True).numpy().view(runner.batch.particles.dtype)
+    runner.readback_into(pin)
     e2e_steps = max(2, min(args.steps, 10))
     barrier(pg)
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
-        if hasattr(I, "offsets"):          # H2D of the step's input state from pinned memory
-            s.upload_batch(pin, I.offsets, I.eos, I.softening)
-        else:
-            s.upload(pin, I.eos, I.softening)
-        s.encode_kdk(1)
-        s.readback_into(pin)               # D2H of the step's result into the same pinned buffer
+        runner.upload(pin)          # H2D of the step's input state from pinned memory
+        runner.encode_kdk(1)
+        runner.readback_into(pin)   # D2H of the step's result into the same pinned buffer
     e2e_s = time.perf_counter() - t0
     e2e_s = max_over_ranks(pg, e2e_s, local)
     e2e_value = n * e2e_steps * world / e2e_s
+    plain = None
+    if wl.get("kind") == "batch" and rank == 0 and not args.no_plain:
+        plain = plain_sequential(wl, I, local)
 
     if rank != 0:
         return
@@ -266,11 +346,12 @@ def run_ours(args, wl, world, rank, local, pg):
         calls = prof["calls"][k]
         if calls == 0 or t <= 0:
             continue
-        b = BYTES_PER_PARTICLE[k] * n * calls
+        b = BYTES_PER_PARTICLE[k] * prof["pcalls"][k]  # particles processed over all calls
         phases[k] = dict(ms=round(t, 4), share=round(t / sum(prof["ms"].values()), 4), calls=calls,
                          gbs=round(b / (t / 1000.0) / 1e9, 1))
     dom = max(phases, key=lambda k: phases[k]["ms"])
     dom_ms = phases[dom]["ms"] / phases[dom]["calls"]
+    n_per_call = prof["pcalls"][dom] / phases[dom]["calls"]  # particles per launch of the dominant phase
     traffic = None
     tf = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tf):
@@ -281,9 +362,9 @@ def run_ours(args, wl, world, rank, local, pg):
         # interaction, 12 per node acceptance test — over its CUDA-event time. Peak: FP32 FMA throughput
         # of 148 SMs × 128 lanes × 2 FLOP × the max SM clock (nominal; no measured FP32 peak exists here).
         walks = max(phases["gravity"]["calls"], 1)
-        m2p = (d1["m2p_interactions"] - d0["m2p_interactions"]) / walks
-        p2p = (d1["p2p_interactions"] - d0["p2p_interactions"]) / walks
-        vis = (d1["walk_nodes"] - d0["walk_nodes"]) / walks
+        m2p = (dsum(d1, "m2p_interactions") - dsum(d0, "m2p_interactions")) / walks
+        p2p = (dsum(d1, "p2p_interactions") - dsum(d0, "p2p_interactions")) / walks
+        vis = (dsum(d1, "walk_nodes") - dsum(d0, "walk_nodes")) / walks
         flops = (65.0 if wl["quad"] else 20.0) * m2p + 20.0 * p2p + 12.0 * vis
         clk_max = (clk.summary() or {}).get("sm_max_mhz") or 1965.0
         peak_tf = 148 * 128 * 2 * clk_max * 1e6 / 1e12
@@ -292,16 +373,17 @@ def run_ours(args, wl, world, rank, local, pg):
                     unit="TFLOP/s", frac=round(achieved / peak_tf, 4), traffic=traffic,
                     peak_source="nominal FP32 FMA peak (148 SM x 128 lanes x 2 x max SM clock)",
                     flops_per_launch=flops, ms_per_launch=round(dom_ms, 4),
-                    interactions_per_particle=dict(multipole=m2p / n, pairwise=p2p / n, nodes=vis / n))
+                    interactions_per_particle=dict(multipole=m2p / n_per_call, pairwise=p2p / n_per_call,
+                                                   nodes=vis / n_per_call))
     else:
-        dom_bytes = BYTES_PER_PARTICLE[dom] * n
+        dom_bytes = BYTES_PER_PARTICLE[dom] * n_per_call
         achieved = dom_bytes / (dom_ms / 1000.0) / 1e9
         roof = dict(bound="hbm", kernel_phase=dom, achieved=round(achieved, 1), peak=pk["hbm"], unit="GB/s",
                     frac=round(achieved / pk["hbm"], 4), traffic=traffic, peak_source=pk["src"],
                     bytes_per_launch=dom_bytes, ms_per_launch=round(dom_ms, 4))
     # memory-bound phases against the measured HBM copy bandwidth
     mem = [k for k in ("sort", "tree", "density", "forces", "integrate", "hsolve") if k in phases]
-    mem_bytes = sum(BYTES_PER_PARTICLE[k] * n * phases[k]["calls"] for k in mem)
+    mem_bytes = sum(BYTES_PER_PARTICLE[k] * prof["pcalls"][k] for k in mem)
     mem_ms = sum(phases[k]["ms"] for k in mem)
     roof_hbm = dict(bound="hbm", phases=mem, achieved=round(mem_bytes / (mem_ms / 1000.0) / 1e9, 1),
                     peak=pk["hbm"], unit="GB/s", frac=round(mem_bytes / (mem_ms / 1000.0) / 1e9 / pk["hbm"], 4),
@@ -313,13 +395,15 @@ def run_ours(args, wl, world, rank, local, pg):
         cpu = dict(value=r["value"], unit=UNIT, cores=r["cores"], kind="port",
                    sample=f"HydroBody::step restated in C++ (f64, octree θ=0.5), 65,536-particle impact of the same "
                           f"generator, {r['steps_run']} steps in {r['seconds']:.1f} s")
-    dd = d1
-    energy0 = dstart["kinetic"] + dstart["internal"] + dstart["potential"]
-    energy1 = dd["kinetic"] + dd["internal"] + dd["potential"]
+    dd = d1[0]
+    energy0 = dsum(dstart, "kinetic") + dsum(dstart, "internal") + dsum(dstart, "potential")
+    energy1 = dsum(d1, "kinetic") + dsum(d1, "internal") + dsum(d1, "potential")
+    pot0 = dsum(dstart, "potential")
     line = dict(metric=METRIC, value=value, unit=UNIT, n_gpus=world, steps=args.steps, warmup=args.warmup,
                 ms_per_step=ms_max / args.steps, higher_is_better=True, scaling="weak", vs_baseline=None,
                 dtype="f32", data="synthetic (seeded lattice impact)",
                 config=dict(workload=args.workload, particles=n, impacts=getattr(I, "n_impacts", 1),
+                            contexts=len(runner.ctxs),
                             graph=bool(wl.get("graph", 0)), kernel=wl["kernel"], neighbours=wl["n_ngb"],
                             theta=wl["theta"], quadrupole=bool(wl["quad"]), leaf=wl["leaf"],
                             h_solve=bool(wl["h_solve"]), dt="adaptive CFL 0.3", parallelism=f"replicas{world}",
@@ -328,9 +412,12 @@ def run_ours(args, wl, world, rank, local, pg):
                          steps=e2e_steps),
                 gpu_launches=launches, roofline=roof, roofline_hbm=roof_hbm, phases=phases, cpu_baseline=cpu,
                 clocks=clk.summary(),
-                physics=dict(energy_drift=(energy1 - energy0) / abs(dstart["potential"]) if dstart["potential"] else None,
-                             sim_time=dd["time"], dt=dd["dt"], max_neighbours=dd["max_neighbours_seen"],
-                             overflow_flags=dd["overflow_flags"], h_residual=dd["h_residual"]))
+                autotune=tuned, plain_sequential=plain,
+                physics=dict(energy_drift=(energy1 - energy0) / abs(pot0) if pot0 else None,
+                             sim_time=dd["time"], dt=dd["dt"],
+                             max_neighbours=max(d["max_neighbours_seen"] for d in d1),
+                             overflow_flags=max(d["overflow_flags"] for d in d1),
+                             h_residual=max(d["h_residual"] for d in d1)))
     print(json.dumps(line), flush=True)
 
 
@@ -342,6 +429,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="impact_1m", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
+    ap.add_argument("--no-plain", action="store_true", help="batch workloads: skip the sequential plain-form leg")
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]
     world, rank, local, pg = dist_setup(args)

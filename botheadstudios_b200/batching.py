@@ -1,0 +1,184 @@
+"""Batched impacts by size bucket, with a launch-configuration autotuner.
+
+A batch of impacts of uneven size is split into size buckets; each bucket is one context (its own CUDA stream
+and tuned launch configuration) that advances all of its impacts with one launch per phase, and the buckets run
+concurrently on their streams. The autotuner picks, per bucket, the LBVH leaf size, the block size of the
+per-particle gather kernels (density, h-solve, forces) and the traversal tile of the fused walk (warps per
+block) by timing candidates on a probe batch drawn from that bucket. Choices are cached in a JSON file keyed
+by the GPU name and the bucket.
+
+The reference has no counterpart: its offline driver runs impacts one after another
+(tools/impact-run/src/main.rs:645-671).
+"""
+from __future__ import annotations
+
+import json
+import os
+
+import numpy as np
+
+from . import ic
+from .gpusph import GpuSph
+
+# particle-count buckets [lo, hi)
+BUCKETS = ((0, 45_000), (45_000, 100_000), (100_000, 1 << 31))
+CANDIDATES = dict(leaf_size=(8, 16, 32), walk_warps=(2, 4, 8), block_threads=(128, 256, 512))
+DEFAULT_CHOICE = dict(leaf_size=16, walk_warps=4, block_threads=256)
+
+
+def bucket_of(n: int) -> int:
+    for b, (lo, hi) in enumerate(BUCKETS):
+        if lo <= n < hi:
+            return b
+    raise ValueError(n)
+
+
+def subset(B: ic.Batch, idx) -> ic.Batch:
+    """The impacts `idx` of a batch, in that order, as a batch of their own."""
+    parts = [B.impact(k) for k in idx]
+    offs = np.concatenate([[0], np.cumsum([len(p) for p in parts])]).astype(np.uint32)
+    return ic.Batch(particles=np.concatenate(parts), offsets=offs, softening=B.softening[list(idx)].copy(),
+                    eos=B.eos, units=B.units, params=[B.params[k] for k in idx])
+
+
+def _time_steps(s: GpuSph, steps: int) -> float:
+    """Device time (ms) of `steps` KDK steps on the context's stream (CUDA events)."""
+    import torch
+    ext = torch.cuda.ExternalStream(s.stream())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(ext)
+    s.encode_kdk(steps)
+    e1.record(ext)
+    e1.synchronize()
+    return e0.elapsed_time(e1)
+
+
+class Autotuner:
+    """Coordinate search over CANDIDATES (leaf size, then walk tile, then block size), each candidate timed on
+    the same probe batch: a fresh context, one warm-up step (the full rebuild), `steps` timed steps."""
+
+    def __init__(self, base: dict, cache_path: str | None = None, steps: int = 2, device: int = -1):
+        self.base = dict(base)
+        self.cache_path = cache_path
+        self.steps = steps
+        self.device = device
+        self.cache = {}
+        if cache_path and os.path.exists(cache_path):
+            self.cache = json.load(open(cache_path))
+        self.log = []
+
+    def _key(self, bucket: int) -> str:
+        import torch
+        name = torch.cuda.get_device_name(self.device if self.device >= 0 else None)
+        return f"{name}|bucket{bucket}|{json.dumps(self.base, sort_keys=True, default=str)}"
+
+    def measure(self, probe: ic.Batch, choice: dict) -> float:
+        """Particle-steps/s of `choice` on the probe batch."""
+        cfg = dict(self.base, **choice)
+        with GpuSph(len(probe.particles), device=self.device, **cfg) as s:
+            s.upload_batch(probe.particles, probe.offsets, probe.eos, probe.softening)
+            s.encode_kdk(1)
+            s.sync()
+            ms = _time_steps(s, self.steps)
+        rate = len(probe.particles) * self.steps / (ms / 1000.0)
+        self.log.append(dict(choice=choice, rate=rate))
+        return rate
+
+    def tune(self, bucket: int, probe: ic.Batch) -> dict:
+        key = self._key(bucket)
+        if key in self.cache:
+            return dict(self.cache[key])
+        best = dict(DEFAULT_CHOICE)
+        best_rate = self.measure(probe, best)
+        for name in ("leaf_size", "walk_warps", "block_threads"):
+            for v in CANDIDATES[name]:
+                if v == best[name]:
+                    continue
+                trial = dict(best, **{name: v})
+                r = self.measure(probe, trial)
+                if r > best_rate:
+                    best, best_rate = trial, r
+        self.cache[key] = best
+        if self.cache_path:
+            json.dump(self.cache, open(self.cache_path, "w"), indent=1)
+        return dict(best)
+
+
+class BucketedBatch:
+    """A batch of impacts advanced as one context per size bucket (impacts reordered so that each bucket is a
+    contiguous range of the particle array; `order` maps back to the caller's impact order)."""
+
+    def __init__(self, B: ic.Batch, base: dict, choices: dict | None = None, device: int = -1):
+        sizes = np.diff(B.offsets).astype(np.int64)
+        buckets = np.array([bucket_of(int(n)) for n in sizes])
+        self.order = np.argsort(buckets, kind="stable")
+        self.batch = subset(B, self.order)
+        self.bucket_ids = sorted(set(buckets.tolist()))
+        self.ranges, self.ctxs, self.sub = [], [], []
+        choices = choices or {}
+        k0 = 0
+        for b in self.bucket_ids:
+            k1 = k0 + int((buckets == b).sum())
+            sub = subset(self.batch, range(k0, k1))
+            cfg = dict(base, **choices.get(b, DEFAULT_CHOICE))
+            s = GpuSph(len(sub.particles), device=device, **cfg)
+            self.ctxs.append(s)
+            self.sub.append(sub)
+            self.ranges.append((int(self.batch.offsets[k0]), int(self.batch.offsets[k1])))
+            k0 = k1
+        self.n = len(self.batch.particles)
+
+    def upload(self, particles: np.ndarray | None = None):
+        """Upload every bucket (from `particles`, a bucket-ordered array such as a pinned copy, or the batch)."""
+        p = self.batch.particles if particles is None else particles
+        for s, sub, (a, b) in zip(self.ctxs, self.sub, self.ranges):
+            s.upload_batch(p[a:b], sub.offsets, sub.eos, sub.softening)
+
+    def encode_kdk(self, substeps: int):
+        for s in self.ctxs:
+            s.encode_kdk(substeps)
+
+    def sync(self):
+        for s in self.ctxs:
+            s.sync()
+
+    def readback_into(self, out: np.ndarray):
+        for s, (a, b) in zip(self.ctxs, self.ranges):
+            s.readback_into(out[a:b])
+
+    def profile_enable(self, on: bool):
+        for s in self.ctxs:
+            s.profile_enable(on)
+
+    def profile_read(self) -> list:
+        return [s.profile_read() for s in self.ctxs]
+
+    def diag(self, check: bool = True) -> list:
+        return [s.diag(check) for s in self.ctxs]
+
+    def close(self):
+        for s in self.ctxs:
+            s.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
+def tune_buckets(B: ic.Batch, base: dict, cache_path: str | None = None, probe_particles: int = 600_000,
+                 device: int = -1) -> tuple[dict, list]:
+    """Autotune every bucket that `B` populates, on a probe of that bucket's impacts (about probe_particles
+    particles, the bucket's first impacts). Returns ({bucket: choice}, measurement log)."""
+    tuner = Autotuner(base, cache_path=cache_path, device=device)
+    sizes = np.diff(B.offsets).astype(np.int64)
+    choices = {}
+    for b in sorted({bucket_of(int(n)) for n in sizes}):
+        idx, tot = [], 0
+        for k, n in enumerate(sizes):
+            if bucket_of(int(n)) == b and tot < probe_particles:
+                idx.append(k)
+                tot += int(n)
+        choices[b] = tuner.tune(b, subset(B, idx))
+    return choices, tuner.log

@@ -53,11 +53,11 @@ __global__ void k_density_eos(int n, State st, const unsigned* __restrict__ nbr,
 }
 
 int launch_density_eos(const Dev& d, const Cfg& c, cudaStream_t s) {
-  const int blocks = (d.n + 255) / 256;
+  const int blocks = (d.n + c.blk - 1) / c.blk;
   if (c.kernel == 1)
-    k_density_eos<1><<<blocks, 256, 0, s>>>(d.n, d.s(), d.nbr, d.nbr_cnt, d.nbr_cap, d.eos, d.P, d.rho, d.fdata);
+    k_density_eos<1><<<blocks, c.blk, 0, s>>>(d.n, d.s(), d.nbr, d.nbr_cnt, d.nbr_cap, d.eos, d.P, d.rho, d.fdata);
   else
-    k_density_eos<0><<<blocks, 256, 0, s>>>(d.n, d.s(), d.nbr, d.nbr_cnt, d.nbr_cap, d.eos, d.P, d.rho, d.fdata);
+    k_density_eos<0><<<blocks, c.blk, 0, s>>>(d.n, d.s(), d.nbr, d.nbr_cnt, d.nbr_cap, d.eos, d.P, d.rho, d.fdata);
   return 1;
 }
 
@@ -137,17 +137,17 @@ __global__ void k_h_reset(DevParams* P, int iters) {
 __global__ void k_h_publish(DevParams* P) { P->h_residual = __uint_as_float(P->h_residual_bits); }
 
 int launch_h_solve(const Dev& d, const Cfg& c, cudaStream_t s) {
-  const int blocks = (d.n + 255) / 256;
+  const int blocks = (d.n + c.blk - 1) / c.blk;
   for (int it = 0; it <= c.h_iters; ++it) {
     const int last = it == c.h_iters;
     k_h_reset<<<1, 1, 0, s>>>(d.P, c.h_iters);
     if (c.kernel == 1)
-      k_h_iter<1><<<blocks, 256, 0, s>>>(d.n, d.s(), d.nbr, d.nbr_cnt, d.nbr_cap, d.h0, c.h_eta, c.skin, d.P, d.hnew,
+      k_h_iter<1><<<blocks, c.blk, 0, s>>>(d.n, d.s(), d.nbr, d.nbr_cnt, d.nbr_cap, d.h0, c.h_eta, c.skin, d.P, d.hnew,
                                           last, d.eos, d.rho, d.fdata);
     else
-      k_h_iter<0><<<blocks, 256, 0, s>>>(d.n, d.s(), d.nbr, d.nbr_cnt, d.nbr_cap, d.h0, c.h_eta, c.skin, d.P, d.hnew,
+      k_h_iter<0><<<blocks, c.blk, 0, s>>>(d.n, d.s(), d.nbr, d.nbr_cnt, d.nbr_cap, d.h0, c.h_eta, c.skin, d.P, d.hnew,
                                           last, d.eos, d.rho, d.fdata);
-    if (!last) k_h_commit<<<blocks, 256, 0, s>>>(d.n, d.s(), d.hnew);
+    if (!last) k_h_commit<<<blocks, c.blk, 0, s>>>(d.n, d.s(), d.hnew);
   }
   k_h_publish<<<1, 1, 0, s>>>(d.P);
   return (c.h_iters + 1) * 2 + c.h_iters + 1;
@@ -221,15 +221,15 @@ __global__ void k_forces(int n, State st, const float4* __restrict__ fdata, cons
 }
 
 int launch_forces(const Dev& d, const Cfg& c, cudaStream_t s) {
-  const int blocks = (d.n + 255) / 256;
+  const int blocks = (d.n + c.blk - 1) / c.blk;
   const bool g = c.gravity != 2;
 #define FARGS d.n, d.s(), d.fdata, d.nbr, d.nbr_cnt, d.nbr_cap, d.grav, d.P, d.segs, d.acc
   if (c.kernel == 1) {
-    if (g) k_forces<1, true><<<blocks, 256, 0, s>>>(FARGS);
-    else k_forces<1, false><<<blocks, 256, 0, s>>>(FARGS);
+    if (g) k_forces<1, true><<<blocks, c.blk, 0, s>>>(FARGS);
+    else k_forces<1, false><<<blocks, c.blk, 0, s>>>(FARGS);
   } else {
-    if (g) k_forces<0, true><<<blocks, 256, 0, s>>>(FARGS);
-    else k_forces<0, false><<<blocks, 256, 0, s>>>(FARGS);
+    if (g) k_forces<0, true><<<blocks, c.blk, 0, s>>>(FARGS);
+    else k_forces<0, false><<<blocks, c.blk, 0, s>>>(FARGS);
   }
 #undef FARGS
   return 1;

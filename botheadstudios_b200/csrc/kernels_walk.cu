@@ -18,20 +18,22 @@
 
 namespace sphb {
 
-constexpr int TW_WARPS = 4;
 constexpr int TW_STACK = 1536;  // per-warp node stack
 constexpr int TW_LIST = 64;     // per-warp list capacity (flushed once half full)
+constexpr int TW_WARPS_PER_SM = 24;  // resident walk warps per SM (80 registers, ~8.4 KB shared each)
 
+// Per-block shared memory of a W-warp walk block (the traversal tile: W groups of 32 particles).
+template <int W>
 struct WalkSmem {
-  unsigned stack[TW_WARPS][TW_STACK];
-  unsigned m2p[TW_WARPS][TW_LIST];
-  unsigned p2p[TW_WARPS][TW_LIST];   // near leaves: pairwise gravity + neighbour predicate
-  unsigned p2f[TW_WARPS][TW_LIST];   // far leaves: pairwise gravity only
-  float4 src[TW_WARPS][32];   // staged sources: x, y, z, m
-  float4 q0[TW_WARPS][32];    // staged quadrupoles
-  float2 q1[TW_WARPS][32];
-  float hsrc[TW_WARPS][32];   // staged smoothing lengths (direct list)
-  int sidx[TW_WARPS][32];     // staged source indices (direct list)
+  unsigned stack[W][TW_STACK];
+  unsigned m2p[W][TW_LIST];
+  unsigned p2p[W][TW_LIST];   // near leaves: pairwise gravity + neighbour predicate
+  unsigned p2f[W][TW_LIST];   // far leaves: pairwise gravity only
+  float4 src[W][32];   // staged sources: x, y, z, m
+  float4 q0[W][32];    // staged quadrupoles
+  float2 q1[W][32];
+  float hsrc[W][32];   // staged smoothing lengths (direct list)
+  int sidx[W][32];     // staged source indices (direct list)
 };
 
 // Compensated accumulator for the precision mode.
@@ -59,8 +61,8 @@ struct Acc3 {
   }
 };
 
-template <bool GRAV, bool QUAD, bool NBR, bool HILO>
-__global__ void __launch_bounds__(TW_WARPS * 32, 6) k_tree_walk(
+template <int W, bool GRAV, bool QUAD, bool NBR, bool HILO>
+__global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
     const float4* __restrict__ body, const float4* __restrict__ pos_h, const double* __restrict__ x64,
     const double* __restrict__ y64, const double* __restrict__ z64, int K, int L,
     const unsigned* __restrict__ leaf_start, const unsigned long long* __restrict__ leaf_codes,
@@ -70,10 +72,10 @@ __global__ void __launch_bounds__(TW_WARPS * 32, 6) k_tree_walk(
     unsigned* __restrict__ nbr_cnt, unsigned cap, float skin, float* __restrict__ h0,
     const uint2* __restrict__ groups, const unsigned* __restrict__ ngroups) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  WalkSmem& S = *reinterpret_cast<WalkSmem*>(smem_raw);
+  WalkSmem<W>& S = *reinterpret_cast<WalkSmem<W>*>(smem_raw);
   const int w = threadIdx.x >> 5;
   const unsigned lane = threadIdx.x & 31u;
-  const int warp = blockIdx.x * TW_WARPS + w;
+  const int warp = blockIdx.x * W + w;
   if (warp >= (int)*ngroups) return;
   // this warp's group: a maximal subtree of <= 32 particles of one impact (leaves g.x..g.y); the walk starts
   // at that impact's root
@@ -374,44 +376,54 @@ __global__ void __launch_bounds__(TW_WARPS * 32, 6) k_tree_walk(
   }
 }
 
-template <bool GRAV, bool QUAD, bool NBR, bool HILO>
+template <int W, bool GRAV, bool QUAD, bool NBR, bool HILO>
 static void walk(const Dev& d, const Cfg& c, cudaStream_t s) {
   const int warps = d.L;  // upper bound on the number of groups
-  const int blocks = (warps + TW_WARPS - 1) / TW_WARPS;
-  const size_t smem = sizeof(WalkSmem);
+  const int blocks = (warps + W - 1) / W;
+  const size_t smem = sizeof(WalkSmem<W>);
   static bool attr = false;
   if (!attr) {
-    cudaFuncSetAttribute(k_tree_walk<GRAV, QUAD, NBR, HILO>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_tree_walk<W, GRAV, QUAD, NBR, HILO>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)smem);
     attr = true;
   }
   const State& st = d.s();
-  k_tree_walk<GRAV, QUAD, NBR, HILO><<<blocks, TW_WARPS * 32, smem, s>>>(
+  k_tree_walk<W, GRAV, QUAD, NBR, HILO><<<blocks, W * 32, smem, s>>>(
       d.body, st.pos_h, st.x, st.y, st.z, d.K, d.L, d.leaf_start, d.leaf_codes, d.segs, d.left, d.right, d.ncom,
-      d.nbmin, d.nbmax, d.nq0, d.nq1, d.P, d.grav, d.nbr, d.nbr_cnt, d.nbr_cap, c.h_solve ? c.skin : c.nbr_skin, d.h0, d.groups, d.ngroups);
+      d.nbmin, d.nbmax, d.nq0, d.nq1, d.P, d.grav, d.nbr, d.nbr_cnt, d.nbr_cap, c.h_solve ? c.skin : c.nbr_skin,
+      d.h0, d.groups, d.ngroups);
 }
 
-// Gravity (group MAC) fused with the neighbour lists.
-int launch_walk(const Dev& d, const Cfg& c, cudaStream_t s) {
-  if (c.quad) {
-    if (c.hilo) walk<true, true, true, true>(d, c, s);
-    else walk<true, true, true, false>(d, c, s);
-  } else {
-    if (c.hilo) walk<true, false, true, true>(d, c, s);
-    else walk<true, false, true, false>(d, c, s);
+// Gravity (group MAC) fused with the neighbour lists; the traversal tile (warps per block) is a tuning choice.
+template <bool QUAD>
+static void walk_fused(const Dev& d, const Cfg& c, cudaStream_t s) {
+  if (c.hilo) {
+    walk<4, true, QUAD, true, true>(d, c, s);
+    return;
   }
+  switch (c.walk_warps) {
+    case 2: walk<2, true, QUAD, true, false>(d, c, s); break;
+    case 8: walk<8, true, QUAD, true, false>(d, c, s); break;
+    default: walk<4, true, QUAD, true, false>(d, c, s); break;
+  }
+}
+
+int launch_walk(const Dev& d, const Cfg& c, cudaStream_t s) {
+  if (c.quad) walk_fused<true>(d, c, s);
+  else walk_fused<false>(d, c, s);
   return 1;
 }
 
 // Gravity only (group MAC), for point sets without SPH.
 int launch_gravity_group(const Dev& d, const Cfg& c, cudaStream_t s) {
-  if (c.quad) walk<true, true, false, false>(d, c, s);
-  else walk<true, false, false, false>(d, c, s);
+  if (c.quad) walk<4, true, true, false, false>(d, c, s);
+  else walk<4, true, false, false, false>(d, c, s);
   return 1;
 }
 
 // Neighbour lists only (when gravity is not the tree).
 int launch_neighbours(const Dev& d, const Cfg& c, cudaStream_t s) {
-  walk<false, false, true, false>(d, c, s);
+  walk<4, false, false, true, false>(d, c, s);
   return 1;
 }
 

@@ -405,6 +405,8 @@ sph_status sph_create(const sph_config* cfg, uint32_t capacity, sph_ctx** out) {
   if (cfg->leaf_size < 1 || cfg->leaf_size > 32 || !(cfg->theta > 0.0f) || cfg->kernel > 1 || cfg->gravity > 2 ||
       cfg->multipole > 1 || cfg->precision > 1 || cfg->h_mode > 1 || cfg->max_neighbours < 1 ||
       cfg->max_neighbours > 4096 || capacity > (1u << 26) || cfg->mac > 1 ||
+      (cfg->block_threads != 0 && (cfg->block_threads < 64 || cfg->block_threads > 1024 || cfg->block_threads % 32)) ||
+      (cfg->walk_warps != 0 && cfg->walk_warps != 2 && cfg->walk_warps != 4 && cfg->walk_warps != 8) ||
       (cfg->mac == SPH_MAC_GROUP && (cfg->leaf_size & (cfg->leaf_size - 1)) != 0))
     return SPH_ERR_INVALID;
   sph_ctx* ctx = new (std::nothrow) sph_ctx();
@@ -421,6 +423,8 @@ sph_status sph_create(const sph_config* cfg, uint32_t capacity, sph_ctx** out) {
   ctx->kc.h_iters = (int)cfg->h_iters;
   ctx->kc.skin = ctx->kc.h_solve ? 0.15f : 0.0f;
   ctx->kc.mac = (int)cfg->mac;
+  ctx->kc.blk = cfg->block_threads ? (int)cfg->block_threads : 256;
+  ctx->kc.walk_warps = cfg->walk_warps ? (int)cfg->walk_warps : 4;
   if (cfg->device >= 0) {
     cudaError_t de = cudaSetDevice(cfg->device);
     if (de != cudaSuccess) {

@@ -159,6 +159,8 @@ struct Cfg {
   float skin = 0.0f;    // neighbour-list radius inflation (h-solve)
   int mac = 0;          // 0 group walk, 1 per-particle reference walk
   float nbr_skin = 0.0f;  // list inflation without the h-solve (grain contacts: a superset, cut exactly later)
+  int blk = 256;        // threads per block of the per-particle gather kernels (density, h-solve, forces)
+  int walk_warps = 4;   // warps per block of the fused walk (2, 4 or 8)
 };
 
 // Grain contact constants (the reference's GpuStepParams subset used by the contact law and solve).

@@ -18,13 +18,14 @@ WORKLOADS = {
     "planet_4m": dict(kind="planet", n_target=4_194_304, n_impactor=0, n_ngb=64.0, kernel="wendland", theta=0.5,
                       quad=1, leaf=16, h_solve=1, max_nbr=192),
     # 256 independent impacts, total particle counts log-uniform in [20k, 200k] (about 2.0e7 particles), mass
-    # ratio 0.05-0.15, angle 0-75°, v_imp 1.0-1.5 v_esc; the 1M impact's method; one launch per phase for all
-    # impacts, steady steps replayed from a captured CUDA graph
+    # ratio 0.05-0.15, angle 0-75°, v_imp 1.0-1.5 v_esc; the 1M impact's method; one context per size bucket
+    # (launch configuration autotuned per bucket) advancing its impacts with one launch per phase, steady steps
+    # replayed from a captured CUDA graph
     "batch_256": dict(kind="batch", n_impacts=256, n_min=20_000, n_max=200_000, n_ngb=64.0, kernel="wendland",
-                      theta=0.6, quad=1, leaf=16, h_solve=1, max_nbr=192, graph=1),
+                      theta=0.6, quad=1, leaf=16, h_solve=1, max_nbr=192, graph=1, autotune=1),
     # the same draw with 16 impacts (a quick check of the batched path)
     "batch_16": dict(kind="batch", n_impacts=16, n_min=20_000, n_max=200_000, n_ngb=64.0, kernel="wendland",
-                     theta=0.6, quad=1, leaf=16, h_solve=1, max_nbr=192, graph=1),
+                     theta=0.6, quad=1, leaf=16, h_solve=1, max_nbr=192, graph=1, autotune=1),
 }
 
 
@@ -57,10 +58,15 @@ def build(wl: dict, seed: int = 1):
     return ic.impact(wl["n_target"], wl["n_impactor"], n_ngb=wl["n_ngb"], seed=seed)
 
 
-def solver(wl: dict, I: ic.Impact, device: int = -1, **over):
-    from .gpusph import GpuSph
+def config(wl: dict, I, **over) -> dict:
+    """The solver configuration (sph_config fields) a workload runs with."""
     kw = dict(theta=wl["theta"], leaf_size=wl["leaf"], kernel=wl["kernel"], multipole=wl["quad"],
               h_mode=wl["h_solve"], h_neighbours=wl["n_ngb"], h_iters=2, max_neighbours=wl["max_nbr"], cfl=0.3,
-              graph=wl.get("graph", 0), device=device, **ic.config_kwargs(I.units))
+              graph=wl.get("graph", 0), **ic.config_kwargs(I.units))
     kw.update(over)
-    return GpuSph(len(I.particles), **kw)
+    return kw
+
+
+def solver(wl: dict, I, device: int = -1, **over):
+    from .gpusph import GpuSph
+    return GpuSph(len(I.particles), device=device, **config(wl, I, **over))

@@ -82,7 +82,10 @@ typedef struct sph_config {
   uint32_t mac;           /* SPH_MAC_*: GROUP (default) or PARTICLE (the reference's per-particle walk) */
   uint32_t graph;         /* nonzero: sph_step_kdk captures its steady two-substep sequence once in a CUDA graph
                              and replays it (phase timing is not recorded for replayed substeps) */
-  uint32_t reserved[5];
+  uint32_t block_threads; /* threads per block of the density, h-solve and force kernels: 64..1024, a multiple of
+                             32; 0 = 256 */
+  uint32_t walk_warps;    /* warps per block of the fused gravity + neighbour walk: 2, 4 or 8; 0 = 4 */
+  uint32_t reserved[3];
 } sph_config;
 
 /* Barnes-Hut acceptance. PARTICLE: each particle walks with the GPU reference's MAC

@@ -124,3 +124,27 @@ def test_batch_upload_rejects_bad_offsets():
     with GpuSph(n - 1, **_cfg(B.units)) as s:
         with pytest.raises(SphError):  # a batch is never clamped
             s.upload_batch(B.particles, B.offsets, B.eos, B.softening)
+
+
+def test_bucketed_batch_with_tuned_choices_equals_alone():
+    from botheadstudios_b200 import batching
+    B = ic.batch(4, 25_000, 130_000, seed=21)
+    base = _cfg(B.units, graph=1)
+    buckets = {batching.bucket_of(int(n)) for n in np.diff(B.offsets)}
+    assert len(buckets) >= 2
+    choices, log = batching.tune_buckets(B, base, probe_particles=60_000)
+    assert set(choices) == buckets and len(log) >= 7 * len(buckets)
+    for c in choices.values():
+        assert c["leaf_size"] in (8, 16, 32) and c["walk_warps"] in (2, 4, 8) and c["block_threads"] in (128, 256, 512)
+    with batching.BucketedBatch(B, base, choices) as bb:
+        bb.upload()
+        bb.encode_kdk(2)
+        out = np.zeros(len(B.particles), B.particles.dtype)
+        bb.sync()
+        bb.readback_into(out)
+        order = bb.order
+        offs = bb.batch.offsets
+    for j, k in enumerate(order):
+        b = batching.bucket_of(int(B.offsets[k + 1] - B.offsets[k]))
+        ref = _alone(B, int(k), 2, **dict(choices[b], graph=1))
+        _same(out[offs[j]:offs[j + 1]], ref["state"])
