@@ -53,7 +53,7 @@ class SphDiag(C.Structure):
                 ("momentum", C.c_double * 3), ("angular_momentum", C.c_double * 3), ("mass", C.c_double),
                 ("dt", C.c_double), ("time", C.c_double), ("steps", C.c_uint32),
                 ("max_neighbours_seen", C.c_uint32), ("overflow_flags", C.c_uint32), ("h_iterations", C.c_uint32),
-                ("h_residual", C.c_float), ("pad", C.c_float), ("walk_nodes", C.c_uint64),
+                ("h_residual", C.c_float), ("h_accepted", C.c_uint32), ("walk_nodes", C.c_uint64),
                 ("walk_pops", C.c_uint64), ("m2p_interactions", C.c_uint64), ("p2p_interactions", C.c_uint64)]
 
 
@@ -72,7 +72,17 @@ EXPORTS = ["sph_config_default", "sph_create", "sph_destroy", "sph_upload", "sph
            "sph_last_error", "sph_status_string", "sph_inspect", "sph_profile_enable", "sph_profile_read",
            "sph_gravity", "sph_gravity_direct64", "sph_gravity_tree_noalloc", "sph_dem_create", "sph_dem_destroy",
            "sph_dem_replace", "sph_dem_set_params", "sph_dem_step", "sph_dem_readback", "sph_dem_contacts",
-           "sph_dem_count"]
+           "sph_dem_count", "sph_mlp_set", "sph_mlp_record", "sph_mlp_features", "sph_set_progress",
+           "sph_mlp_forward", "sph_mlp_grad", "sph_mlp_train"]
+
+H_MODE = dict(fixed=0, solve=1, learned=2)
+MLP_PARAMS = 4819     # SPH_MLP_PARAMS
+MLP_TRAINABLE = 4801  # SPH_MLP_TRAINABLE
+
+
+class MlpTrainCfg(C.Structure):
+    _fields_ = [("epochs", C.c_uint32), ("batch", C.c_uint32), ("lr", C.c_float), ("beta1", C.c_float),
+                ("beta2", C.c_float), ("eps", C.c_float), ("weight_decay", C.c_float), ("seed", C.c_uint32)]
 
 # 80-byte grain layout (particle_step.wgsl:127-137)
 GRAIN_DTYPE = np.dtype([("offset", "<f4", (3,)), ("u", "<f4"), ("vel", "<f4", (3,)), ("resting", "<f4"),
@@ -140,6 +150,13 @@ def load():
     L.sph_dem_step.argtypes = [vp, C.c_uint32]
     L.sph_dem_readback.argtypes = [vp, vp, C.c_uint32, C.POINTER(C.c_uint32)]
     L.sph_dem_contacts.argtypes = [vp, vp, C.c_size_t]
+    L.sph_mlp_set.argtypes = [vp, vp, C.c_uint32]
+    L.sph_mlp_record.argtypes = [vp, C.c_int]
+    L.sph_mlp_features.argtypes = [vp, vp, vp, C.c_uint32]
+    L.sph_set_progress.argtypes = [vp, C.c_float]
+    L.sph_mlp_forward.argtypes = [vp, vp, C.c_uint32, vp]
+    L.sph_mlp_grad.argtypes = [vp, vp, vp, C.c_uint32, vp, vp]
+    L.sph_mlp_train.argtypes = [vp, vp, vp, C.c_uint32, C.POINTER(MlpTrainCfg), vp]
     L.sph_dem_count.argtypes = [vp]
     L.sph_dem_count.restype = C.c_uint32
     no_status = ("sph_destroy", "sph_count", "sph_stream", "sph_last_error", "sph_status_string", "sph_dem_destroy",
@@ -156,6 +173,6 @@ def default_config(**kw) -> SphConfig:
     load().sph_config_default(C.byref(cfg))
     for k, v in kw.items():
         if isinstance(v, str):
-            v = {**KERNEL, **GRAVITY}[v]
+            v = (H_MODE if k == "h_mode" else {**KERNEL, **GRAVITY})[v]
         setattr(cfg, k, v)
     return cfg

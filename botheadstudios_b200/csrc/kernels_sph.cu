@@ -78,6 +78,47 @@ int launch_eos_only(const Dev& d, cudaStream_t s) {
 // ∂rho_i/∂h_i = m_i ∂W(0,h_i)/∂h + Σ_j m_j ½ ∂W(r,h_ij)/∂h (Price 2012, J. Comput. Phys. 231, §3.2.1).
 // h may move inside the list's skin only; the residual |f|/rho is reduced to a device maximum.
 // ---------------------------------------------------------------------------------------------------
+// ρ_i and ∂ρ_i/∂h_i at the particle's current h over its neighbour list (the density sum of k_density_eos,
+// same terms in the same order).
+template <int KERNEL>
+__device__ __forceinline__ void h_sums(int t, const State& st, const unsigned* __restrict__ nbr,
+                                       const unsigned* __restrict__ nbr_cnt, unsigned cap, float& rho,
+                                       float& drho) {
+  const float4 pi = st.pos_h[t];
+  const float m = st.mass[t];
+  const float h = pi.w;
+  rho = m * kern_w<KERNEL>(0.0f, h);
+  drho = m * kern_dwdh<KERNEL>(0.0f, h);
+  const unsigned c = min(nbr_cnt[t], cap);
+  for (unsigned k = 0; k < c; ++k) {
+    const unsigned j = nbr[nbr_slot((unsigned)t, k, cap)];
+    const float4 pj = st.pos_h[j];
+    const float r = pair_r(pi, pj);
+    const float hij = pair_h(h, pj.w);
+    if (r < hij) {
+      const float mj = st.mass[j];
+      rho += mj * kern_w<KERNEL>(r, hij);
+      drho += mj * 0.5f * kern_dwdh<KERNEL>(r, hij);
+    }
+  }
+}
+
+// The Newton update of h from the residual f = ρ − m(η/h)³, limited to ±20 % and to the list's skin.
+__device__ __forceinline__ float h_newton(float h, float m, float rho, float drho, float eta, float h0, float skin,
+                                          float& res) {
+  const float e3 = eta * eta * eta;
+  const float rt = m * e3 / (h * h * h);
+  const float f = rho - rt;
+  res = fabsf(f) / fmaxf(rho, 1.0e-30f);
+  const float fp = drho + 3.0f * rt / h;
+  float hn = fabsf(fp) > 0.0f ? h - f / fp : h;
+  if (!(hn == hn)) hn = h;  // NaN guard
+  hn = fminf(fmaxf(hn, 0.8f * h), 1.2f * h);
+  hn = fminf(hn, h0 * (1.0f + skin) * 0.999f);
+  hn = fmaxf(hn, h0 / ((1.0f + skin) * 1.001f));
+  return hn;
+}
+
 template <int KERNEL>
 __global__ void k_h_iter(int n, State st, const unsigned* __restrict__ nbr, const unsigned* __restrict__ nbr_cnt,
                          unsigned cap, const float* __restrict__ h0, float eta, float skin, DevParams* P,
@@ -86,44 +127,82 @@ __global__ void k_h_iter(int n, State st, const unsigned* __restrict__ nbr, cons
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   float res = 0.0f;
   if (t < n) {
-    const float4 pi = st.pos_h[t];
-    const float m = st.mass[t];
-    const float h = pi.w;
-    float rho = m * kern_w<KERNEL>(0.0f, h);
-    float drho = m * kern_dwdh<KERNEL>(0.0f, h);
-    const unsigned c = min(nbr_cnt[t], cap);
-    for (unsigned k = 0; k < c; ++k) {
-      const unsigned j = nbr[nbr_slot((unsigned)t, k, cap)];
-      const float4 pj = st.pos_h[j];
-      const float r = pair_r(pi, pj);
-      const float hij = pair_h(h, pj.w);
-      if (r < hij) {
-        const float mj = st.mass[j];
-        rho += mj * kern_w<KERNEL>(r, hij);
-        drho += mj * 0.5f * kern_dwdh<KERNEL>(r, hij);
-      }
-    }
-    const float e3 = eta * eta * eta;
-    const float rt = m * e3 / (h * h * h);
-    const float f = rho - rt;
-    res = fabsf(f) / fmaxf(rho, 1.0e-30f);
-    float hn = h;
+    float rho, drho;
+    h_sums<KERNEL>(t, st, nbr, nbr_cnt, cap, rho, drho);
+    const float m = st.mass[t], h = st.pos_h[t].w;
+    float hn = h_newton(h, m, rho, drho, eta, h0[t], skin, res);
     if (last) {
       // the final pass is the density pass: same sum, same order as k_density_eos
       rho_out[t] = rho;
       fdata[t] = eos_record(eos, st.mat[t], m, rho, st.vel_u[t].w, P);
-    } else {
-      const float fp = drho + 3.0f * rt / h;
-      hn = fabsf(fp) > 0.0f ? h - f / fp : h;
-      if (!(hn == hn)) hn = h;  // NaN guard
-      hn = fminf(fmaxf(hn, 0.8f * h), 1.2f * h);
-      hn = fminf(hn, h0[t] * (1.0f + skin) * 0.999f);
-      hn = fmaxf(hn, h0[t] / ((1.0f + skin) * 1.001f));
+      hn = h;
     }
     hnew[t] = hn;
   }
   const float wres = warp_max(res);
   if ((threadIdx.x & 31) == 0) atomicMax(&P->h_residual_bits, __float_as_uint(wres));
+}
+
+// Learned h: check the proposed (or current) h of every listed particle. A particle whose relative density
+// residual is within tolerance (or that is on its last pass) is final: its density and EOS record are
+// written. Any other takes a Newton step (into hnew) and is appended to the next list. `list` null = all n.
+template <int KERNEL>
+__global__ void k_h_check(int n, const unsigned* __restrict__ list, const unsigned* __restrict__ list_n, State st,
+                          const unsigned* __restrict__ nbr, const unsigned* __restrict__ nbr_cnt, unsigned cap,
+                          const float* __restrict__ h0, float eta, float skin, float tol, DevParams* P,
+                          float* __restrict__ hnew, unsigned* __restrict__ next, unsigned* __restrict__ next_n,
+                          int last, const Eos* __restrict__ eos, float* __restrict__ rho_out,
+                          float4* __restrict__ fdata) {
+  const int count = list ? (int)*list_n : n;
+  const int lane = threadIdx.x & 31;
+  float wres = 0.0f;
+  unsigned acc = 0;
+  // whole warps step together (the append below is warp-aggregated)
+  for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < count; base += gridDim.x * blockDim.x) {
+    const int i = base + lane;
+    bool pend = false;
+    int t = -1;
+    if (i < count) {
+      t = list ? (int)list[i] : i;
+      float rho, drho, res;
+      h_sums<KERNEL>(t, st, nbr, nbr_cnt, cap, rho, drho);
+      const float m = st.mass[t], h = st.pos_h[t].w;
+      const float hn = h_newton(h, m, rho, drho, eta, h0[t], skin, res);
+      if (res <= tol || last) {
+        rho_out[t] = rho;
+        fdata[t] = eos_record(eos, st.mat[t], m, rho, st.vel_u[t].w, P);
+        wres = fmaxf(wres, res);
+        if (!list && res <= tol) ++acc;
+      } else {
+        hnew[t] = hn;
+        pend = true;
+      }
+    }
+    const unsigned bal = __ballot_sync(SPH_FULL_MASK, pend);
+    unsigned at = 0;
+    if (lane == 0 && bal) at = atomicAdd(next_n, (unsigned)__popc(bal));
+    at = __shfl_sync(SPH_FULL_MASK, at, 0);
+    if (pend) next[at + __popc(bal & ((1u << lane) - 1u))] = (unsigned)t;
+  }
+  wres = warp_max(wres);
+  acc += __shfl_xor_sync(SPH_FULL_MASK, acc, 16);
+  acc += __shfl_xor_sync(SPH_FULL_MASK, acc, 8);
+  acc += __shfl_xor_sync(SPH_FULL_MASK, acc, 4);
+  acc += __shfl_xor_sync(SPH_FULL_MASK, acc, 2);
+  acc += __shfl_xor_sync(SPH_FULL_MASK, acc, 1);
+  if (lane == 0) {
+    atomicMax(&P->h_residual_bits, __float_as_uint(wres));
+    if (acc) atomicAdd(&P->h_accepted, acc);
+  }
+}
+
+__global__ void k_h_commit_list(const unsigned* __restrict__ list, const unsigned* __restrict__ list_n, State st,
+                                const float* __restrict__ hnew) {
+  const int count = (int)*list_n;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+    const unsigned t = list[i];
+    st.pos_h[t].w = hnew[t];
+  }
 }
 
 __global__ void k_h_commit(int n, State st, const float* __restrict__ hnew) {
@@ -133,6 +212,7 @@ __global__ void k_h_commit(int n, State st, const float* __restrict__ hnew) {
 __global__ void k_h_reset(DevParams* P, int iters) {
   P->h_residual_bits = 0u;
   P->h_iters_used = (unsigned)iters;
+  P->h_accepted = 0u;
 }
 __global__ void k_h_publish(DevParams* P) { P->h_residual = __uint_as_float(P->h_residual_bits); }
 
@@ -153,6 +233,39 @@ int launch_h_solve(const Dev& d, const Cfg& c, cudaStream_t s) {
   return (c.h_iters + 1) * 2 + c.h_iters + 1;
 }
 
+// Learned h: the proposals written into pos_h.w before the tree build are checked in one pass over all
+// particles; only the rejected ones iterate (Jacobi-Newton over their own lists), at most h_iters times,
+// the last pass writing density and EOS whatever the residual. The residual maximum covers every particle.
+int launch_h_learned(const Dev& d, const Cfg& c, cudaStream_t s) {
+  const int full = (d.n + c.blk - 1) / c.blk;
+  const int part = full < 148 * 8 ? full : 148 * 8;
+  k_h_reset<<<1, 1, 0, s>>>(d.P, c.h_iters);
+  cudaMemsetAsync(d.pend_n, 0, 2 * sizeof(unsigned), s);
+  int launches = 2;
+#define HC_ARGS(list, ln, nx, nxn, last)                                                                   \
+  d.n, list, ln, d.s(), d.nbr, d.nbr_cnt, d.nbr_cap, d.h0, c.h_eta, c.skin, c.h_tol, d.P, d.hnew, nx, nxn, last, \
+      d.eos, d.rho, d.fdata
+  if (c.kernel == 1)
+    k_h_check<1><<<full, c.blk, 0, s>>>(HC_ARGS(nullptr, nullptr, d.pend[0], d.pend_n, c.h_iters == 0 ? 1 : 0));
+  else
+    k_h_check<0><<<full, c.blk, 0, s>>>(HC_ARGS(nullptr, nullptr, d.pend[0], d.pend_n, c.h_iters == 0 ? 1 : 0));
+  ++launches;
+  for (int it = 1; it <= c.h_iters; ++it) {
+    const int a = (it - 1) & 1, b = it & 1;
+    k_h_commit_list<<<part, 256, 0, s>>>(d.pend[a], d.pend_n + a, d.s(), d.hnew);
+    cudaMemsetAsync(d.pend_n + b, 0, sizeof(unsigned), s);
+    const int last = it == c.h_iters ? 1 : 0;
+    if (c.kernel == 1)
+      k_h_check<1><<<part, c.blk, 0, s>>>(HC_ARGS(d.pend[a], d.pend_n + a, d.pend[b], d.pend_n + b, last));
+    else
+      k_h_check<0><<<part, c.blk, 0, s>>>(HC_ARGS(d.pend[a], d.pend_n + a, d.pend[b], d.pend_n + b, last));
+    launches += 3;
+  }
+#undef HC_ARGS
+  k_h_publish<<<1, 1, 0, s>>>(d.P);
+  return launches + 1;
+}
+
 // ---------------------------------------------------------------------------------------------------
 // Forces (the SPH half of cs_forces, sph_step.wgsl:170-210) + gravity + the Courant signal (cs_signal
 // :263-269) reduced to each impact's minimum with one atomic per warp (per lane in a warp that straddles two
@@ -161,7 +274,8 @@ int launch_h_solve(const Dev& d, const Cfg& c, cudaStream_t s) {
 template <int KERNEL, bool GRAV>
 __global__ void k_forces(int n, State st, const float4* __restrict__ fdata, const unsigned* __restrict__ nbr,
                          const unsigned* __restrict__ nbr_cnt, unsigned cap, const float4* __restrict__ grav,
-                         const DevParams* __restrict__ P, Seg* __restrict__ segs, float4* __restrict__ acc) {
+                         const DevParams* __restrict__ P, Seg* __restrict__ segs, float4* __restrict__ acc,
+                         float* __restrict__ divv) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   float sig = __int_as_float(0x7f800000);
   const unsigned sg = t < n ? st.seg[t] : kNoSeg;
@@ -170,7 +284,7 @@ __global__ void k_forces(int n, State st, const float4* __restrict__ fdata, cons
     const float4 vi = st.vel_u[t];
     const float4 fi = fdata[t];
     const float alpha = P->av_alpha, beta = P->av_beta, r_min = P->r_min;
-    float ax = 0.f, ay = 0.f, az = 0.f, de = 0.f;
+    float ax = 0.f, ay = 0.f, az = 0.f, de = 0.f, dv = 0.f;
     const unsigned c = min(nbr_cnt[t], cap);
     for (unsigned k = 0; k < c; ++k) {
       const unsigned j = nbr[nbr_slot((unsigned)t, k, cap)];
@@ -197,7 +311,9 @@ __global__ void k_forces(int n, State st, const float4* __restrict__ fdata, cons
       ax += gx * s;
       ay += gy * s;
       az += gz * s;
-      de += 0.5f * fj.x * coeff * (vx * gx + vy * gy + vz * gz);
+      const float vg = vx * gx + vy * gy + vz * gz;
+      de += 0.5f * fj.x * coeff * vg;
+      dv += fj.x * vg;
     }
     if (GRAV) {
       const float4 g = grav[t];
@@ -206,6 +322,7 @@ __global__ void k_forces(int n, State st, const float4* __restrict__ fdata, cons
       az += g.z;
     }
     acc[t] = make_float4(ax, ay, az, de);
+    divv[t] = -dv / fi.y;  // ∇·v_i = −(1/ρ_i) Σ_j m_j v_ij·∇_i W_ij
     const float vmag = sqrtf(vi.x * vi.x + vi.y * vi.y + vi.z * vi.z);
     sig = pi.w / fmaxf(fi.w + vmag, P->sig_floor);
   }
@@ -223,7 +340,7 @@ __global__ void k_forces(int n, State st, const float4* __restrict__ fdata, cons
 int launch_forces(const Dev& d, const Cfg& c, cudaStream_t s) {
   const int blocks = (d.n + c.blk - 1) / c.blk;
   const bool g = c.gravity != 2;
-#define FARGS d.n, d.s(), d.fdata, d.nbr, d.nbr_cnt, d.nbr_cap, d.grav, d.P, d.segs, d.acc
+#define FARGS d.n, d.s(), d.fdata, d.nbr, d.nbr_cnt, d.nbr_cap, d.grav, d.P, d.segs, d.acc, d.divv
   if (c.kernel == 1) {
     if (g) k_forces<1, true><<<blocks, c.blk, 0, s>>>(FARGS);
     else k_forces<1, false><<<blocks, c.blk, 0, s>>>(FARGS);

@@ -1,0 +1,612 @@
+// Learned smoothing-length MLP on the tensor cores: 8 → 64 → 64 → 1 with GELU, BF16 operands and FP32
+// accumulation through mma.sync.m16n8k16 tiles. A CTA of 4 warps holds 128 rows (particles or training
+// samples); each warp owns 32 rows (two 16-row MMA tiles) and runs them through both hidden layers without
+// leaving shared memory. Training runs the backward pass on the same tiles (weight gradients as GEMMs over
+// the CTA's samples) and Adam on an FP32 master copy.
+//
+// Fragment layouts of m16n8k16 (row.col): lane = 4·g + q. A (16×16, row-major): a0 = (g, 2q..2q+1),
+// a1 = (g+8, 2q..), a2 = (g, 8+2q..), a3 = (g+8, 8+2q..). B (16×8, K×N): b0 = (k 2q..2q+1, n g),
+// b1 = (k 8+2q.., n g). C (16×8): c0,c1 = (g, 2q..2q+1), c2,c3 = (g+8, 2q..2q+1). Every operand is kept in
+// shared memory with its K index contiguous, so each fragment register is one aligned 32-bit load; row
+// strides of 24/72/136 elements put the 8 rows a fragment touches in distinct banks.
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+#include "../../include/sph_b200.h"
+#include "mlp.cuh"
+
+namespace sphb {
+
+namespace {
+
+constexpr int XS = 24;    // row stride of K=16 operands
+constexpr int HS = 72;    // row stride of K=64 operands
+constexpr int TS = 136;   // row stride of K=128 (sample-major) operands
+constexpr int ROWS = 128;
+
+__device__ __forceinline__ unsigned ld32(const __nv_bfloat16* p) { return *reinterpret_cast<const unsigned*>(p); }
+__device__ __forceinline__ void st32(__nv_bfloat16* p, float a, float b) {
+  *reinterpret_cast<__nv_bfloat162*>(p) = __floats2bfloat162_rn(a, b);
+}
+__device__ __forceinline__ void mma16816(float c[4], const unsigned a[4], unsigned b0, unsigned b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
+__device__ __forceinline__ float gelu_d(float z) {
+  return 0.5f * (1.0f + erff(z * 0.70710678118654752f)) + z * expf(-0.5f * z * z) * 0.39894228040143268f;
+}
+
+// Shared-memory weights of the forward pass.
+struct FwdW {
+  __nv_bfloat16 w1t[MLP_H * XS];
+  __nv_bfloat16 w2t[MLP_H * HS];
+  float b1[MLP_H], b2[MLP_H], w3[MLP_H];
+};
+
+__device__ void load_fwd(const MlpPacked* __restrict__ W, FwdW& s) {
+  for (int i = threadIdx.x; i < MLP_H * 16; i += blockDim.x) s.w1t[(i >> 4) * XS + (i & 15)] = W->w1t[i];
+  for (int i = threadIdx.x; i < MLP_H * MLP_H; i += blockDim.x) s.w2t[(i >> 6) * HS + (i & 63)] = W->w2t[i];
+  for (int i = threadIdx.x; i < MLP_H; i += blockDim.x) {
+    s.b1[i] = W->b1[i];
+    s.b2[i] = W->b2[i];
+    s.w3[i] = W->w3[i];
+  }
+}
+
+// Forward pass of one warp's 32 rows [r0, r0+32): x (bf16, [row][XS]) → h1 (bf16, [row][HS]) → y[row]
+// (FP32, without b3). Optionally keeps z1, z2 (FP32, [row][64]) and h1 transposed ([col][TS]).
+__device__ void mlp_rows(int r0, const __nv_bfloat16* sx, __nv_bfloat16* sh1, const FwdW& w, float* sy,
+                         float* z1o, float* z2o, __nv_bfloat16* h1t) {
+  const int lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
+#pragma unroll
+  for (int mt = 0; mt < 2; ++mt) {
+    const int ra = r0 + mt * 16;
+    unsigned a[4];
+    a[0] = ld32(sx + (ra + g) * XS + 2 * q);
+    a[1] = ld32(sx + (ra + g + 8) * XS + 2 * q);
+    a[2] = ld32(sx + (ra + g) * XS + 8 + 2 * q);
+    a[3] = ld32(sx + (ra + g + 8) * XS + 8 + 2 * q);
+#pragma unroll
+    for (int nt = 0; nt < 8; ++nt) {
+      const int c0 = nt * 8 + 2 * q;
+      float c[4] = {w.b1[c0], w.b1[c0 + 1], w.b1[c0], w.b1[c0 + 1]};
+      mma16816(c, a, ld32(w.w1t + (nt * 8 + g) * XS + 2 * q), ld32(w.w1t + (nt * 8 + g) * XS + 8 + 2 * q));
+      if (z1o) {
+        z1o[(ra + g) * MLP_H + c0] = c[0];
+        z1o[(ra + g) * MLP_H + c0 + 1] = c[1];
+        z1o[(ra + g + 8) * MLP_H + c0] = c[2];
+        z1o[(ra + g + 8) * MLP_H + c0 + 1] = c[3];
+      }
+      const float h0 = gelu(c[0]), h1 = gelu(c[1]), h2 = gelu(c[2]), h3 = gelu(c[3]);
+      st32(sh1 + (ra + g) * HS + c0, h0, h1);
+      st32(sh1 + (ra + g + 8) * HS + c0, h2, h3);
+      if (h1t) {
+        h1t[c0 * TS + ra + g] = __float2bfloat16_rn(h0);
+        h1t[(c0 + 1) * TS + ra + g] = __float2bfloat16_rn(h1);
+        h1t[c0 * TS + ra + g + 8] = __float2bfloat16_rn(h2);
+        h1t[(c0 + 1) * TS + ra + g + 8] = __float2bfloat16_rn(h3);
+      }
+    }
+  }
+  __syncwarp();
+#pragma unroll
+  for (int mt = 0; mt < 2; ++mt) {
+    const int ra = r0 + mt * 16;
+    unsigned a[4][4];
+#pragma unroll
+    for (int kt = 0; kt < 4; ++kt) {
+      a[kt][0] = ld32(sh1 + (ra + g) * HS + kt * 16 + 2 * q);
+      a[kt][1] = ld32(sh1 + (ra + g + 8) * HS + kt * 16 + 2 * q);
+      a[kt][2] = ld32(sh1 + (ra + g) * HS + kt * 16 + 8 + 2 * q);
+      a[kt][3] = ld32(sh1 + (ra + g + 8) * HS + kt * 16 + 8 + 2 * q);
+    }
+    float y0 = 0.0f, y1 = 0.0f;
+#pragma unroll
+    for (int nt = 0; nt < 8; ++nt) {
+      const int c0 = nt * 8 + 2 * q;
+      float c[4] = {w.b2[c0], w.b2[c0 + 1], w.b2[c0], w.b2[c0 + 1]};
+      const __nv_bfloat16* bp = w.w2t + (nt * 8 + g) * HS + 2 * q;
+#pragma unroll
+      for (int kt = 0; kt < 4; ++kt) mma16816(c, a[kt], ld32(bp + kt * 16), ld32(bp + kt * 16 + 8));
+      if (z2o) {
+        z2o[(ra + g) * MLP_H + c0] = c[0];
+        z2o[(ra + g) * MLP_H + c0 + 1] = c[1];
+        z2o[(ra + g + 8) * MLP_H + c0] = c[2];
+        z2o[(ra + g + 8) * MLP_H + c0 + 1] = c[3];
+      }
+      y0 += gelu(c[0]) * w.w3[c0] + gelu(c[1]) * w.w3[c0 + 1];
+      y1 += gelu(c[2]) * w.w3[c0] + gelu(c[3]) * w.w3[c0 + 1];
+    }
+    y0 += __shfl_xor_sync(SPH_FULL_MASK, y0, 1);
+    y0 += __shfl_xor_sync(SPH_FULL_MASK, y0, 2);
+    y1 += __shfl_xor_sync(SPH_FULL_MASK, y1, 1);
+    y1 += __shfl_xor_sync(SPH_FULL_MASK, y1, 2);
+    if (q == 0) {
+      sy[ra + g] = y0;
+      sy[ra + g + 8] = y1;
+    }
+  }
+  __syncwarp();
+}
+
+// One row of normalised features, rounded to bf16, into the A operand (K padded to 16 with zeros).
+__device__ __forceinline__ void put_row(__nv_bfloat16* sx, int r, const float f[MLP_IN], const MlpPacked* W) {
+#pragma unroll
+  for (int k = 0; k < MLP_IN; k += 2)
+    st32(sx + r * XS + k, (f[k] - W->xm[k]) * W->xs[k], (f[k + 1] - W->xm[k + 1]) * W->xs[k + 1]);
+#pragma unroll
+  for (int k = MLP_IN; k < 16; k += 2) st32(sx + r * XS + k, 0.0f, 0.0f);
+}
+
+// ---- feature definition (the solver's state at the start of the step's drift) ---------------------------
+__device__ __forceinline__ void features(int t, const State& st, const float* __restrict__ rho,
+                                         const unsigned* __restrict__ cnt, const float4* __restrict__ acc,
+                                         const float4* __restrict__ fdata, const float* __restrict__ divv,
+                                         const Eos* __restrict__ eos, const Seg* __restrict__ segs,
+                                         const DevParams* __restrict__ P, const MlpFeatureArgs& fa,
+                                         float f[MLP_IN]) {
+  const float4 p = st.pos_h[t];
+  const float m = st.mass[t];
+  const float r = fmaxf(rho[t], 1.0e-30f);
+  const unsigned mat = st.mat[t];
+  const float rho0 = eos[mat].rho0, e_iv = eos[mat].e_iv;
+  const float heq = fa.eta * cbrtf(m / r);
+  const float dt = (float)segs[st.seg[t]].dt;
+  const float4 a = acc[t];
+  const float c = fmaxf(fdata[t].w, 1.0e-30f);
+  f[0] = logf(p.w / heq);                                                      // log h relative to h(rho)
+  f[1] = logf(r / rho0);                                                       // log rho / rho0
+  f[2] = divv[t] * dt;                                                         // div v over the step
+  f[3] = (float)cnt[t] / fa.n_target;                                          // neighbours / target
+  f[4] = log1pf(sqrtf(a.x * a.x + a.y * a.y + a.z * a.z) * p.w / (c * c));     // |a| h / c²
+  f[5] = (float)mat;                                                           // material
+  f[6] = log1pf(fmaxf(st.vel_u[t].w, 0.0f) / e_iv);                            // u / E_iv
+  f[7] = P->progress;                                                          // step fraction
+}
+
+__global__ void __launch_bounds__(ROWS) k_mlp_propose(int n, State st, const float* __restrict__ rho,
+                                                     const unsigned* __restrict__ cnt,
+                                                     const float4* __restrict__ acc,
+                                                     const float4* __restrict__ fdata,
+                                                     const float* __restrict__ divv, const Eos* __restrict__ eos,
+                                                     const Seg* __restrict__ segs,
+                                                     const DevParams* __restrict__ P, MlpFeatureArgs fa,
+                                                     const MlpPacked* __restrict__ W, float* __restrict__ rec,
+                                                     float* __restrict__ dh, int apply) {
+  __shared__ __align__(16) FwdW w;
+  __shared__ __align__(16) __nv_bfloat16 sx[ROWS * XS];
+  __shared__ __align__(16) __nv_bfloat16 sh1[ROWS * HS];
+  __shared__ float sy[ROWS];
+  load_fwd(W, w);
+  const float b3 = W->b3, ym = W->ym, ys = W->ys;
+  __syncthreads();
+  const int r = threadIdx.x, r0 = (threadIdx.x >> 5) * 32;
+  for (int base = blockIdx.x * ROWS; base < n; base += gridDim.x * ROWS) {
+    const int t = base + r;
+    float f[MLP_IN] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    if (t < n) features(t, st, rho, cnt, acc, fdata, divv, eos, segs, P, fa, f);
+    put_row(sx, r, f, W);
+    __syncwarp();
+    mlp_rows(r0, sx, sh1, w, sy, nullptr, nullptr, nullptr);
+    if (t < n) {
+      const float d = (sy[r] + b3) * ys + ym;
+      const float dc = fminf(fmaxf(d, -0.1f), 0.1f);
+      if (apply) st.pos_h[t].w = st.pos_h[t].w * expf(dc);
+      if (rec) {
+        const unsigned id = st.id[t];
+#pragma unroll
+        for (int k = 0; k < MLP_IN; ++k) rec[(size_t)id * MLP_IN + k] = f[k];
+        dh[id] = d;
+      }
+    }
+    __syncwarp();
+  }
+}
+
+__global__ void __launch_bounds__(ROWS) k_mlp_forward(const MlpPacked* __restrict__ W, const float* __restrict__ x,
+                                                     int n, float* __restrict__ out) {
+  __shared__ __align__(16) FwdW w;
+  __shared__ __align__(16) __nv_bfloat16 sx[ROWS * XS];
+  __shared__ __align__(16) __nv_bfloat16 sh1[ROWS * HS];
+  __shared__ float sy[ROWS];
+  load_fwd(W, w);
+  __syncthreads();
+  const int r = threadIdx.x, r0 = (threadIdx.x >> 5) * 32;
+  for (int base = blockIdx.x * ROWS; base < n; base += gridDim.x * ROWS) {
+    const int t = base + r;
+    float f[MLP_IN] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    if (t < n)
+#pragma unroll
+      for (int k = 0; k < MLP_IN; ++k) f[k] = x[(size_t)t * MLP_IN + k];
+    put_row(sx, r, f, W);
+    __syncwarp();
+    mlp_rows(r0, sx, sh1, w, sy, nullptr, nullptr, nullptr);
+    if (t < n) out[t] = (sy[r] + W->b3) * W->ys + W->ym;
+    __syncwarp();
+  }
+}
+
+// ---- training: forward + backward of one 128-sample tile ----------------------------------------------
+struct TrainSmem {
+  FwdW w;
+  __nv_bfloat16 w2[MLP_H * HS];      // W2 [in][out] (B operand of dh1 = dz2 W2ᵀ)
+  __nv_bfloat16 sx[ROWS * XS];       // x' [row][k]
+  __nv_bfloat16 sxt[16 * TS];        // x' [k][row]
+  __nv_bfloat16 sh1[ROWS * HS];      // a1 [row][i]
+  __nv_bfloat16 sh1t[MLP_H * TS];    // a1 [i][row]
+  __nv_bfloat16 dz2[ROWS * HS];      // dz2 [row][j]
+  __nv_bfloat16 dz2t[MLP_H * TS];    // dz2 [j][row]
+  __nv_bfloat16 dz1t[MLP_H * TS];    // dz1 [i][row]
+  float z1[ROWS * MLP_H];            // z1, then dz1 (FP32)
+  float z2[ROWS * MLP_H];
+  float y[ROWS], dy[ROWS];
+};
+
+__global__ void __launch_bounds__(ROWS) k_mlp_train(const MlpPacked* __restrict__ W, const float* __restrict__ x,
+                                                   const float* __restrict__ tgt, const unsigned* __restrict__ idx,
+                                                   int m, float denom, float* __restrict__ grad,
+                                                   float* __restrict__ loss) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  TrainSmem& S = *reinterpret_cast<TrainSmem*>(smem_raw);
+  load_fwd(W, S.w);
+  for (int i = threadIdx.x; i < MLP_H * MLP_H; i += ROWS) S.w2[(i >> 6) * HS + (i & 63)] = W->w2[i];
+  const int r = threadIdx.x, wp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
+  const int s = blockIdx.x * ROWS + r;
+  const bool valid = s < m;
+  const unsigned j = valid ? idx[s] : 0u;
+  float f[MLP_IN] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  float tn = 0.0f;
+  if (valid) {
+#pragma unroll
+    for (int k = 0; k < MLP_IN; ++k) f[k] = x[(size_t)j * MLP_IN + k];
+    tn = (tgt[j] - W->ym) / W->ys;
+  }
+  put_row(S.sx, r, f, W);
+#pragma unroll
+  for (int k = 0; k < 16; ++k) S.sxt[k * TS + r] = S.sx[r * XS + k];
+  __syncthreads();
+  mlp_rows(wp * 32, S.sx, S.sh1, S.w, S.y, S.z1, S.z2, S.sh1t);
+  __syncthreads();
+  // output error: d(loss)/dy with loss = Σ (y − t)² / denom
+  {
+    const float e = valid ? (S.y[r] + W->b3 - tn) : 0.0f;
+    S.dy[r] = 2.0f * e / denom;
+    float e2 = e * e;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) e2 += __shfl_xor_sync(SPH_FULL_MASK, e2, o);
+    if (lane == 0) atomicAdd(loss, e2);
+  }
+  __syncthreads();
+  // dW3, db2 and dz2 (= dy w3 gelu'(z2)), one column per thread over half the rows
+  {
+    const int col = r & 63, h = r >> 6;
+    float gw3 = 0.f, gb2 = 0.f;
+    for (int rr = h * 64; rr < h * 64 + 64; ++rr) {
+      const float z = S.z2[rr * MLP_H + col];
+      gw3 += S.dy[rr] * gelu(z);
+      const float dz = S.dy[rr] * S.w.w3[col] * gelu_d(z);
+      gb2 += dz;
+      const __nv_bfloat16 b = __float2bfloat16_rn(dz);
+      S.dz2[rr * HS + col] = b;
+      S.dz2t[col * TS + rr] = b;
+    }
+    atomicAdd(&grad[MLP_W3 + col], gw3);
+    atomicAdd(&grad[MLP_B2 + col], gb2);
+    if (r == 0) {
+      float gb3 = 0.f;
+      for (int rr = 0; rr < ROWS; ++rr) gb3 += S.dy[rr];
+      atomicAdd(&grad[MLP_B3], gb3);
+    }
+  }
+  __syncthreads();
+  // dW2[i][j] = Σ_r a1[r][i] dz2[r][j]: warp wp takes rows i in [16wp, 16wp+16), all 8 column tiles
+#pragma unroll 1
+  for (int nt = 0; nt < 8; ++nt) {
+    float c[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+    for (int kt = 0; kt < 8; ++kt) {
+      unsigned a[4];
+      a[0] = ld32(S.sh1t + (16 * wp + g) * TS + kt * 16 + 2 * q);
+      a[1] = ld32(S.sh1t + (16 * wp + g + 8) * TS + kt * 16 + 2 * q);
+      a[2] = ld32(S.sh1t + (16 * wp + g) * TS + kt * 16 + 8 + 2 * q);
+      a[3] = ld32(S.sh1t + (16 * wp + g + 8) * TS + kt * 16 + 8 + 2 * q);
+      const __nv_bfloat16* bp = S.dz2t + (nt * 8 + g) * TS + kt * 16 + 2 * q;
+      mma16816(c, a, ld32(bp), ld32(bp + 8));
+    }
+    const int i0 = 16 * wp + g, c0 = nt * 8 + 2 * q;
+    atomicAdd(&grad[MLP_W2 + i0 * MLP_H + c0], c[0]);
+    atomicAdd(&grad[MLP_W2 + i0 * MLP_H + c0 + 1], c[1]);
+    atomicAdd(&grad[MLP_W2 + (i0 + 8) * MLP_H + c0], c[2]);
+    atomicAdd(&grad[MLP_W2 + (i0 + 8) * MLP_H + c0 + 1], c[3]);
+  }
+  // da1 = dz2 W2ᵀ for this warp's rows, then dz1 = da1 gelu'(z1) (FP32 into z1, bf16 transposed into dz1t)
+#pragma unroll 1
+  for (int mt = 0; mt < 2; ++mt) {
+    const int ra = wp * 32 + mt * 16;
+    unsigned a[4][4];
+#pragma unroll
+    for (int kt = 0; kt < 4; ++kt) {
+      a[kt][0] = ld32(S.dz2 + (ra + g) * HS + kt * 16 + 2 * q);
+      a[kt][1] = ld32(S.dz2 + (ra + g + 8) * HS + kt * 16 + 2 * q);
+      a[kt][2] = ld32(S.dz2 + (ra + g) * HS + kt * 16 + 8 + 2 * q);
+      a[kt][3] = ld32(S.dz2 + (ra + g + 8) * HS + kt * 16 + 8 + 2 * q);
+    }
+#pragma unroll
+    for (int nt = 0; nt < 8; ++nt) {
+      float c[4] = {0.f, 0.f, 0.f, 0.f};
+      const __nv_bfloat16* bp = S.w2 + (nt * 8 + g) * HS + 2 * q;
+#pragma unroll
+      for (int kt = 0; kt < 4; ++kt) mma16816(c, a[kt], ld32(bp + kt * 16), ld32(bp + kt * 16 + 8));
+      const int c0 = nt * 8 + 2 * q;
+      const int rows[2] = {ra + g, ra + g + 8};
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          float* zp = &S.z1[rows[h] * MLP_H + c0 + e];
+          const float dz = c[2 * h + e] * gelu_d(*zp);
+          *zp = dz;
+          S.dz1t[(c0 + e) * TS + rows[h]] = __float2bfloat16_rn(dz);
+        }
+      }
+    }
+  }
+  __syncthreads();
+  // db1: column sums of dz1
+  if (r < MLP_H) {
+    float gb1 = 0.f;
+    for (int rr = 0; rr < ROWS; ++rr) gb1 += S.z1[rr * MLP_H + r];
+    atomicAdd(&grad[MLP_B1 + r], gb1);
+  }
+  // dW1[k][i] = Σ_r x'[r][k] dz1[r][i]: one 16-row tile (k, padded), warp wp takes column tiles 2wp, 2wp+1
+#pragma unroll 1
+  for (int u = 0; u < 2; ++u) {
+    const int nt = 2 * wp + u;
+    float c[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+    for (int kt = 0; kt < 8; ++kt) {
+      unsigned a[4];
+      a[0] = ld32(S.sxt + g * TS + kt * 16 + 2 * q);
+      a[1] = ld32(S.sxt + (g + 8) * TS + kt * 16 + 2 * q);
+      a[2] = ld32(S.sxt + g * TS + kt * 16 + 8 + 2 * q);
+      a[3] = ld32(S.sxt + (g + 8) * TS + kt * 16 + 8 + 2 * q);
+      const __nv_bfloat16* bp = S.dz1t + (nt * 8 + g) * TS + kt * 16 + 2 * q;
+      mma16816(c, a, ld32(bp), ld32(bp + 8));
+    }
+    const int c0 = nt * 8 + 2 * q;  // rows g < 8 are the real inputs; rows g + 8 are the K padding
+    atomicAdd(&grad[MLP_W1 + g * MLP_H + c0], c[0]);
+    atomicAdd(&grad[MLP_W1 + g * MLP_H + c0 + 1], c[1]);
+  }
+}
+
+__global__ void k_mlp_pack(const float* __restrict__ P, MlpPacked* __restrict__ o) {
+  for (int i = threadIdx.x; i < MLP_H * 16; i += blockDim.x) {
+    const int out = i >> 4, in = i & 15;
+    o->w1t[i] = __float2bfloat16_rn(in < MLP_IN ? P[MLP_W1 + in * MLP_H + out] : 0.0f);
+  }
+  for (int i = threadIdx.x; i < MLP_H * MLP_H; i += blockDim.x) {
+    const int out = i >> 6, in = i & 63;
+    o->w2t[i] = __float2bfloat16_rn(P[MLP_W2 + in * MLP_H + out]);
+    o->w2[i] = __float2bfloat16_rn(P[MLP_W2 + i]);
+  }
+  for (int i = threadIdx.x; i < MLP_H; i += blockDim.x) {
+    o->w3[i] = __bfloat162float(__float2bfloat16_rn(P[MLP_W3 + i]));
+    o->b1[i] = P[MLP_B1 + i];
+    o->b2[i] = P[MLP_B2 + i];
+  }
+  if (threadIdx.x < MLP_IN) {
+    o->xm[threadIdx.x] = P[MLP_XM + threadIdx.x];
+    o->xs[threadIdx.x] = P[MLP_XS + threadIdx.x];
+  }
+  if (threadIdx.x == 0) {
+    o->b3 = P[MLP_B3];
+    o->ym = P[MLP_YM];
+    o->ys = P[MLP_YS];
+  }
+}
+
+__global__ void k_mlp_adam(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
+                           float* __restrict__ v, float lr, float b1, float b2, float eps, float wd, float c1,
+                           float c2) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= MLP_TRAIN) return;
+  const float gi = g[i] + wd * p[i];
+  const float mi = b1 * m[i] + (1.0f - b1) * gi;
+  const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+  m[i] = mi;
+  v[i] = vi;
+  p[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+}
+
+int propose_grid() {
+  static int grid = 0;
+  if (!grid) {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    grid = sms * 4;
+  }
+  return grid;
+}
+
+}  // namespace
+
+int launch_mlp_pack(const float* params, MlpPacked* out, cudaStream_t s) {
+  k_mlp_pack<<<1, 256, 0, s>>>(params, out);
+  return 1;
+}
+
+int launch_mlp_propose(const Dev& d, const MlpPacked* w, const MlpFeatureArgs& fa, const float* divv, float* rec,
+                       float* dh, bool apply, cudaStream_t s) {
+  const int tiles = (d.n + ROWS - 1) / ROWS;
+  const int grid = tiles < propose_grid() ? tiles : propose_grid();
+  k_mlp_propose<<<grid, ROWS, 0, s>>>(d.n, d.s(), d.rho, d.nbr_cnt, d.acc, d.fdata, divv, d.eos, d.segs, d.P, fa,
+                                      w, rec, dh, apply ? 1 : 0);
+  return 1;
+}
+
+int launch_mlp_forward(const MlpPacked* w, const float* x, int n, float* out, cudaStream_t s) {
+  const int tiles = (n + ROWS - 1) / ROWS;
+  const int grid = tiles < propose_grid() ? tiles : propose_grid();
+  k_mlp_forward<<<grid, ROWS, 0, s>>>(w, x, n, out);
+  return 1;
+}
+
+int launch_mlp_train_batch(const MlpPacked* w, const float* x, const float* t, const unsigned* idx, int m,
+                           float denom, float* grad, float* loss, cudaStream_t s) {
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_mlp_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TrainSmem));
+    attr = true;
+  }
+  k_mlp_train<<<(m + ROWS - 1) / ROWS, ROWS, sizeof(TrainSmem), s>>>(w, x, t, idx, m, denom, grad, loss);
+  return 1;
+}
+
+int launch_mlp_adam(float* params, const float* grad, float* m, float* v, int step, float lr, float b1, float b2,
+                    float eps, float wd, cudaStream_t s) {
+  const float c1 = 1.0f - powf(b1, (float)step), c2 = 1.0f - powf(b2, (float)step);
+  k_mlp_adam<<<(MLP_TRAIN + 255) / 256, 256, 0, s>>>(params, grad, m, v, lr, b1, b2, eps, wd, c1, c2);
+  return 1;
+}
+
+}  // namespace sphb
+
+// ---- the network on its own (host arrays, blocking, the calling thread's current device) ------------------
+using namespace sphb;
+
+namespace {
+
+struct DevBuf {
+  std::vector<void*> ptrs;
+  cudaError_t err = cudaSuccess;
+  template <typename T>
+  T* get(size_t count) {
+    void* p = nullptr;
+    if (err == cudaSuccess) err = cudaMalloc(&p, count * sizeof(T) > 0 ? count * sizeof(T) : 16);
+    if (err == cudaSuccess) ptrs.push_back(p);
+    return static_cast<T*>(p);
+  }
+  ~DevBuf() {
+    for (void* p : ptrs) cudaFree(p);
+  }
+};
+
+sph_status status_of(cudaError_t e) {
+  if (e == cudaSuccess) return SPH_OK;
+  return e == cudaErrorMemoryAllocation ? SPH_ERR_OOM : SPH_ERR_CUDA;
+}
+
+uint64_t splitmix(uint64_t& s) {
+  uint64_t z = (s += 0x9E3779B97F4A7C15ull);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+}  // namespace
+
+extern "C" {
+
+sph_status sph_mlp_forward(const float* params, const float* x, uint32_t n, float* out) {
+  if (!params || (!x && n) || (!out && n)) return SPH_ERR_INVALID;
+  if (n == 0) return SPH_OK;
+  DevBuf b;
+  float* dp = b.get<float>(MLP_TOTAL);
+  MlpPacked* w = b.get<MlpPacked>(1);
+  float* dx = b.get<float>((size_t)n * MLP_IN);
+  float* dy = b.get<float>(n);
+  if (b.err != cudaSuccess) return status_of(b.err);
+  cudaError_t e = cudaMemcpy(dp, params, MLP_TOTAL * sizeof(float), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(dx, x, (size_t)n * MLP_IN * sizeof(float), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return status_of(e);
+  launch_mlp_pack(dp, w, 0);
+  launch_mlp_forward(w, dx, (int)n, dy, 0);
+  e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpy(out, dy, (size_t)n * sizeof(float), cudaMemcpyDeviceToHost);
+  return status_of(e);
+}
+
+sph_status sph_mlp_grad(const float* params, const float* x, const float* t, uint32_t n, float* grad, float* loss) {
+  if (!params || !x || !t || !grad || !loss || n == 0) return SPH_ERR_INVALID;
+  DevBuf b;
+  float* dp = b.get<float>(MLP_TOTAL);
+  MlpPacked* w = b.get<MlpPacked>(1);
+  float* dx = b.get<float>((size_t)n * MLP_IN);
+  float* dt = b.get<float>(n);
+  unsigned* idx = b.get<unsigned>(n);
+  float* dg = b.get<float>(MLP_TRAIN + 1);  // gradient, then the summed squared error
+  if (b.err != cudaSuccess) return status_of(b.err);
+  std::vector<unsigned> id(n);
+  for (uint32_t i = 0; i < n; ++i) id[i] = i;
+  cudaError_t e = cudaMemcpy(dp, params, MLP_TOTAL * sizeof(float), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(dx, x, (size_t)n * MLP_IN * sizeof(float), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(dt, t, (size_t)n * sizeof(float), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(idx, id.data(), (size_t)n * sizeof(unsigned), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemset(dg, 0, (MLP_TRAIN + 1) * sizeof(float));
+  if (e != cudaSuccess) return status_of(e);
+  launch_mlp_pack(dp, w, 0);
+  launch_mlp_train_batch(w, dx, dt, idx, (int)n, (float)n, dg, dg + MLP_TRAIN, 0);
+  e = cudaGetLastError();
+  std::vector<float> h(MLP_TRAIN + 1);
+  if (e == cudaSuccess) e = cudaMemcpy(h.data(), dg, h.size() * sizeof(float), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return status_of(e);
+  std::memcpy(grad, h.data(), MLP_TRAIN * sizeof(float));
+  *loss = h[MLP_TRAIN] / (float)n;
+  return SPH_OK;
+}
+
+sph_status sph_mlp_train(float* params, const float* x, const float* t, uint32_t n, const sph_mlp_train_cfg* cfg,
+                         float* loss_per_epoch) {
+  if (!params || !x || !t || !cfg || n == 0 || cfg->batch == 0 || !(cfg->lr > 0.0f)) return SPH_ERR_INVALID;
+  DevBuf b;
+  float* dp = b.get<float>(MLP_TOTAL);
+  MlpPacked* w = b.get<MlpPacked>(1);
+  float* dx = b.get<float>((size_t)n * MLP_IN);
+  float* dt = b.get<float>(n);
+  unsigned* idx = b.get<unsigned>(n);
+  float* dg = b.get<float>(MLP_TRAIN + 1);
+  float* dm = b.get<float>(MLP_TRAIN);
+  float* dv = b.get<float>(MLP_TRAIN);
+  float* dl = b.get<float>(1);
+  if (b.err != cudaSuccess) return status_of(b.err);
+  cudaError_t e = cudaMemcpy(dp, params, MLP_TOTAL * sizeof(float), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(dx, x, (size_t)n * MLP_IN * sizeof(float), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(dt, t, (size_t)n * sizeof(float), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemset(dm, 0, MLP_TRAIN * sizeof(float));
+  if (e == cudaSuccess) e = cudaMemset(dv, 0, MLP_TRAIN * sizeof(float));
+  if (e != cudaSuccess) return status_of(e);
+  std::vector<unsigned> perm(n);
+  for (uint32_t i = 0; i < n; ++i) perm[i] = i;
+  uint64_t rs = cfg->seed * 0x2545F4914F6CDD1Dull + 1;
+  const float b1 = cfg->beta1 > 0.0f ? cfg->beta1 : 0.9f, b2 = cfg->beta2 > 0.0f ? cfg->beta2 : 0.999f;
+  const float eps = cfg->eps > 0.0f ? cfg->eps : 1.0e-8f;
+  int step = 0;
+  launch_mlp_pack(dp, w, 0);
+  for (uint32_t ep = 0; ep < cfg->epochs; ++ep) {
+    for (uint32_t i = n - 1; i > 0; --i) std::swap(perm[i], perm[splitmix(rs) % (i + 1)]);  // Fisher-Yates
+    e = cudaMemcpy(idx, perm.data(), (size_t)n * sizeof(unsigned), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(dl, 0, sizeof(float));
+    if (e != cudaSuccess) return status_of(e);
+    for (uint32_t off = 0; off < n; off += cfg->batch) {
+      const uint32_t m = n - off < cfg->batch ? n - off : cfg->batch;
+      cudaMemsetAsync(dg, 0, MLP_TRAIN * sizeof(float), 0);
+      launch_mlp_train_batch(w, dx, dt, idx + off, (int)m, (float)m, dg, dl, 0);
+      launch_mlp_adam(dp, dg, dm, dv, ++step, cfg->lr, b1, b2, eps, cfg->weight_decay, 0);
+      launch_mlp_pack(dp, w, 0);
+    }
+    float l = 0.0f;
+    e = cudaMemcpy(&l, dl, sizeof(float), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return status_of(e);
+    if (loss_per_epoch) loss_per_epoch[ep] = l / (float)n;
+  }
+  e = cudaMemcpy(params, dp, MLP_TRAIN * sizeof(float), cudaMemcpyDeviceToHost);
+  return status_of(e);
+}
+
+}  // extern "C"

@@ -14,6 +14,7 @@
 #include <thread>
 
 #include "../../include/sph_b200.h"
+#include "mlp.cuh"
 #include "sph_kernels.cuh"
 
 using namespace sphb;
@@ -32,6 +33,13 @@ struct sph_ctx {
   // captured steady KDK sequence (two substeps), one per parity of the state double buffer
   cudaGraphExec_t kdk_graph[2] = {nullptr, nullptr};
   unsigned long long kdk_graph_launches = 0;  // kernels in one replay
+  // learned smoothing lengths
+  float* mlp_params = nullptr;  // [SPH_MLP_PARAMS] FP32 on the device
+  MlpPacked* mlp_w = nullptr;
+  bool mlp_rec = false;
+  float* mlp_feat = nullptr;    // [cap][8] recorded features (original order)
+  float* mlp_dh = nullptr;      // [cap] recorded Δlog h
+  bool proposed = false;        // pos_h.w holds proposals for the next rebuild
   DevParams hp{};          // host copy of the host-owned fields
   void* pinned_aos = nullptr;
   cudaEvent_t rb_event = nullptr;
@@ -132,6 +140,10 @@ sph_status alloc_dev(sph_ctx* ctx, Dev& d, uint32_t cap, uint32_t K, uint32_t nb
     ALLOC(d.acc, capw);
     ALLOC(d.hnew, capw);
     ALLOC(d.h0, capw);
+    ALLOC(d.divv, capw);
+    ALLOC(d.pend[0], capw);
+    ALLOC(d.pend[1], capw);
+    ALLOC(d.pend_n, 2);
     ALLOC(d.eos, kMaxMaterials);
     d.diag_blocks = 148 * 2;
     ALLOC(d.diag_part, (size_t)d.diag_blocks * 16);
@@ -211,8 +223,12 @@ sph_status rebuild(sph_ctx* ctx, bool need_bbox) {
     return 0;
   });
   if (!fused) phase(ctx, SPH_PHASE_NEIGHBOURS, [&] { return launch_neighbours(d, c, s); });
-  // with the smoothing-length solve, its final (residual) pass is the density + EOS pass
-  if (c.h_solve) phase(ctx, SPH_PHASE_HSOLVE, [&] { return launch_h_solve(d, c, s); });
+  // with the smoothing-length solve, its final (residual) pass is the density + EOS pass; learned h checks
+  // the proposals written before this rebuild and iterates only the rejected particles
+  const bool learned = c.learned && ctx->proposed;
+  ctx->proposed = false;
+  if (c.h_solve)
+    phase(ctx, SPH_PHASE_HSOLVE, [&] { return learned ? launch_h_learned(d, c, s) : launch_h_solve(d, c, s); });
   else phase(ctx, SPH_PHASE_DENSITY, [&] { return launch_density_eos(d, c, s); });
   CK(cudaGetLastError());
   return SPH_OK;
@@ -316,6 +332,15 @@ sph_status kdk_steady(sph_ctx* ctx) {
   cudaStream_t s = ctx->stream;
   forces(ctx);
   phase(ctx, SPH_PHASE_INTEGRATE, [&] { return launch_finalize_dt(d, s) + launch_kick_drift(d, s); });
+  if (ctx->kc.learned || ctx->mlp_rec) {
+    // the network's Δlog h from the state at the start of the drift (counted with the smoothing-length phase)
+    const MlpFeatureArgs fa{ctx->kc.h_eta, ctx->cfg.h_neighbours};
+    phase(ctx, SPH_PHASE_HSOLVE, [&] {
+      return launch_mlp_propose(d, ctx->mlp_w, fa, d.divv, ctx->mlp_rec ? ctx->mlp_feat : nullptr,
+                                ctx->mlp_rec ? ctx->mlp_dh : nullptr, ctx->kc.learned != 0, s);
+    });
+    ctx->proposed = ctx->kc.learned != 0;
+  }
   sph_status st = rebuild(ctx, false);
   if (st != SPH_OK) return st;
   forces(ctx);
@@ -403,7 +428,7 @@ sph_status sph_create(const sph_config* cfg, uint32_t capacity, sph_ctx** out) {
   if (!cfg || !out) return SPH_ERR_INVALID;
   *out = nullptr;
   if (cfg->leaf_size < 1 || cfg->leaf_size > 32 || !(cfg->theta > 0.0f) || cfg->kernel > 1 || cfg->gravity > 2 ||
-      cfg->multipole > 1 || cfg->precision > 1 || cfg->h_mode > 1 || cfg->max_neighbours < 1 ||
+      cfg->multipole > 1 || cfg->precision > 1 || cfg->h_mode > 2 || cfg->max_neighbours < 1 ||
       cfg->max_neighbours > 4096 || capacity > (1u << 26) || cfg->mac > 1 ||
       (cfg->block_threads != 0 && (cfg->block_threads < 64 || cfg->block_threads > 1024 || cfg->block_threads % 32)) ||
       (cfg->walk_warps != 0 && cfg->walk_warps != 2 && cfg->walk_warps != 4 && cfg->walk_warps != 8) ||
@@ -417,7 +442,8 @@ sph_status sph_create(const sph_config* cfg, uint32_t capacity, sph_ctx** out) {
   ctx->kc.gravity = (int)cfg->gravity;
   ctx->kc.quad = cfg->multipole == SPH_MULTIPOLE_QUADRUPOLE;
   ctx->kc.hilo = cfg->precision == SPH_PRECISION_HILO;
-  ctx->kc.h_solve = cfg->h_mode == SPH_H_SOLVE;
+  ctx->kc.h_solve = cfg->h_mode == SPH_H_SOLVE || cfg->h_mode == SPH_H_LEARNED;
+  ctx->kc.learned = cfg->h_mode == SPH_H_LEARNED;
   ctx->kc.h_eta = std::cbrt(3.0f * cfg->h_neighbours / (4.0f * 3.14159265358979f));
   ctx->kc.h_tol = cfg->h_tol;
   ctx->kc.h_iters = (int)cfg->h_iters;
@@ -449,6 +475,20 @@ sph_status sph_create(const sph_config* cfg, uint32_t capacity, sph_ctx** out) {
     if (e != cudaSuccess) st = cuda_fail(ctx, e, "cudaEventCreate");
   }
   if (st == SPH_OK) st = dalloc(ctx, &ctx->d_diag, 16);
+  if (st == SPH_OK) st = dalloc(ctx, &ctx->mlp_params, (size_t)MLP_TOTAL);
+  if (st == SPH_OK) st = dalloc(ctx, &ctx->mlp_w, 1);
+  if (st == SPH_OK) {
+    // the zero network: Δlog h = 0 (unit scales so that the normalisation is well defined)
+    std::vector<float> z(MLP_TOTAL, 0.0f);
+    for (int k = 0; k < MLP_IN; ++k) z[MLP_XS + k] = 1.0f;
+    z[MLP_YS] = 1.0f;
+    cudaError_t e2 = cudaMemcpy(ctx->mlp_params, z.data(), z.size() * sizeof(float), cudaMemcpyHostToDevice);
+    if (e2 == cudaSuccess) {
+      launch_mlp_pack(ctx->mlp_params, ctx->mlp_w, ctx->stream);
+      e2 = cudaStreamSynchronize(ctx->stream);
+    }
+    if (e2 != cudaSuccess) st = cuda_fail(ctx, e2, "mlp init");
+  }
   if (st == SPH_OK) {
     DevParams& p = ctx->hp;
     std::memset(&p, 0, sizeof(p));
@@ -703,6 +743,7 @@ sph_status sph_diag(sph_ctx* ctx, sph_diag_out* out) {
   out->overflow_flags = p.flags;
   out->h_iterations = p.h_iters_used;
   out->h_residual = p.h_residual;
+  out->h_accepted = p.h_accepted;
   out->walk_nodes = p.stat_visits;
   out->walk_pops = p.stat_pops;
   out->m2p_interactions = p.stat_m2p;
@@ -1004,6 +1045,59 @@ sph_status sph_gravity_direct64(sph_ctx* ctx, const double* pos3, const double* 
   if (e == cudaSuccess) e = e2;
   if (e != cudaSuccess) return cuda_fail(ctx, e, "sph_gravity_direct64");
   return SPH_OK;
+}
+
+sph_status sph_mlp_set(sph_ctx* ctx, const float* params, uint32_t count) {
+  if (!ctx || !params || count != (uint32_t)MLP_TOTAL) return SPH_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  for (uint32_t k = 0; k < count; ++k)
+    if (!std::isfinite(params[k])) {
+      ctx->err = "sph_mlp_set: parameter " + std::to_string(k) + " is not finite";
+      return SPH_ERR_INVALID;
+    }
+  CK(cudaMemcpyAsync(ctx->mlp_params, params, count * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+  launch_mlp_pack(ctx->mlp_params, ctx->mlp_w, ctx->stream);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(ctx->stream));
+  return SPH_OK;
+}
+
+sph_status sph_mlp_record(sph_ctx* ctx, int on) {
+  if (!ctx) return SPH_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (on && !ctx->mlp_feat) {
+    sph_status st = dalloc(ctx, &ctx->mlp_feat, (size_t)ctx->capacity * MLP_IN);
+    if (st == SPH_OK) st = dalloc(ctx, &ctx->mlp_dh, (size_t)ctx->capacity);
+    if (st != SPH_OK) return st;
+  }
+  if (ctx->mlp_rec != (on != 0)) drop_graphs(ctx);  // the captured steps hold the recording pointers
+  ctx->mlp_rec = on != 0;
+  return SPH_OK;
+}
+
+sph_status sph_mlp_features(sph_ctx* ctx, float* features, float* dlogh, uint32_t cap) {
+  if (!ctx) return SPH_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  if (!ctx->mlp_feat) {
+    ctx->err = "sph_mlp_features: recording was never enabled";
+    return SPH_ERR_STATE;
+  }
+  const uint32_t n = (uint32_t)ctx->d.n < cap ? (uint32_t)ctx->d.n : cap;
+  if (features && n)
+    CK(cudaMemcpyAsync(features, ctx->mlp_feat, (size_t)n * MLP_IN * sizeof(float), cudaMemcpyDeviceToHost,
+                       ctx->stream));
+  if (dlogh && n)
+    CK(cudaMemcpyAsync(dlogh, ctx->mlp_dh, (size_t)n * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return n < (uint32_t)ctx->d.n ? SPH_CLAMPED : SPH_OK;
+}
+
+sph_status sph_set_progress(sph_ctx* ctx, float fraction) {
+  if (!ctx || !std::isfinite(fraction)) return SPH_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  ctx->hp.progress = fraction;
+  return push_params(ctx, ctx->d);
 }
 
 }  // extern "C"

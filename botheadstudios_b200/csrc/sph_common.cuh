@@ -31,6 +31,8 @@ struct DevParams {
   float theta;
   float cfl;
   float rho_floor, du_floor, r_min, sig_floor;
+  float progress;     // host-set fraction of the run completed (a learned-h input)
+  unsigned pad0;
   // ---- maintained by the device from here on --------------------------------------------------------
   unsigned flags;         // kFlag* bits
   unsigned max_nbr_seen;
@@ -38,7 +40,8 @@ struct DevParams {
   unsigned h_iters_used;
   float h_residual;
   unsigned h_residual_bits;
-  unsigned pad[2];
+  unsigned h_accepted;    // learned h: particles whose proposal passed the first residual check (last solve)
+  unsigned pad;
   // walk statistics, accumulated once per warp: node visits, 32-wide pops, multipole and pairwise
   // interactions (particle × source pairs)
   unsigned long long stat_visits, stat_pops, stat_m2p, stat_p2p;

@@ -139,6 +139,9 @@ struct Dev {
   float4* acc = nullptr;        // [n] total acc.xyz, du/dt
   float* hnew = nullptr;        // [n] smoothing-length solve scratch
   float* h0 = nullptr;          // [n] smoothing length when the neighbour list was built
+  float* divv = nullptr;        // [n] velocity divergence from the force pass (a learned-h input)
+  unsigned* pend[2] = {nullptr, nullptr};  // learned h: particles still iterating (two alternating lists)
+  unsigned* pend_n = nullptr;   // [2] list lengths
   Eos* eos = nullptr;           // [16]
   DevParams* P = nullptr;
   double* diag_part = nullptr;  // [blocks][16]
@@ -161,6 +164,7 @@ struct Cfg {
   float nbr_skin = 0.0f;  // list inflation without the h-solve (grain contacts: a superset, cut exactly later)
   int blk = 256;        // threads per block of the per-particle gather kernels (density, h-solve, forces)
   int walk_warps = 4;   // warps per block of the fused walk (2, 4 or 8)
+  int learned = 0;      // smoothing lengths proposed by the MLP, checked, iterated only where rejected
 };
 
 // Grain contact constants (the reference's GpuStepParams subset used by the contact law and solve).
@@ -193,6 +197,7 @@ int launch_walk(const Dev& d, const Cfg& c, cudaStream_t s);            // group
 int launch_gravity_group(const Dev& d, const Cfg& c, cudaStream_t s);   // group-MAC gravity only
 int launch_density_eos(const Dev& d, const Cfg& c, cudaStream_t s);
 int launch_h_solve(const Dev& d, const Cfg& c, cudaStream_t s);
+int launch_h_learned(const Dev& d, const Cfg& c, cudaStream_t s);   // check proposals, iterate the rejected
 int launch_eos_only(const Dev& d, cudaStream_t s);
 int launch_forces(const Dev& d, const Cfg& c, cudaStream_t s);
 int launch_finalize_dt(const Dev& d, cudaStream_t s);

@@ -94,6 +94,25 @@ class GpuSph:
                     "sph_inspect(IMPACT_TIME)")
         return out
 
+    # ---- learned smoothing lengths --------------------------------------------------------------------
+    def mlp_set(self, params: np.ndarray):
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        self._check(self._L.sph_mlp_set(self._h, _ptr(p), len(p)), "sph_mlp_set")
+
+    def mlp_record(self, on: bool = True):
+        self._check(self._L.sph_mlp_record(self._h, 1 if on else 0), "sph_mlp_record")
+
+    def mlp_features(self):
+        """(features[n][8], Δlog h[n]) of the last recorded step, in original particle order."""
+        n = self.count()
+        f = np.zeros((n, 8), np.float32)
+        d = np.zeros(n, np.float32)
+        self._check(self._L.sph_mlp_features(self._h, _ptr(f), _ptr(d), n), "sph_mlp_features")
+        return f, d
+
+    def set_progress(self, fraction: float):
+        self._check(self._L.sph_set_progress(self._h, float(fraction)), "sph_set_progress")
+
     def set_dt(self, dt: float, damp: float = 1.0):
         self._check(self._L.sph_set_dt(self._h, float(dt), float(damp)), "sph_set_dt")
 
@@ -162,7 +181,8 @@ class GpuSph:
         return dict(kinetic=d.kinetic, internal=d.internal, potential=d.potential, momentum=list(d.momentum),
                     angular_momentum=list(d.angular_momentum), mass=d.mass, dt=d.dt, time=d.time, steps=d.steps,
                     max_neighbours_seen=d.max_neighbours_seen, overflow_flags=d.overflow_flags,
-                    h_iterations=d.h_iterations, h_residual=d.h_residual, walk_nodes=d.walk_nodes,
+                    h_iterations=d.h_iterations, h_residual=d.h_residual, h_accepted=d.h_accepted,
+                    walk_nodes=d.walk_nodes,
                     walk_pops=d.walk_pops, m2p_interactions=d.m2p_interactions,
                     p2p_interactions=d.p2p_interactions, status=st)
 

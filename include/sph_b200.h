@@ -55,7 +55,7 @@ typedef enum sph_status {
 enum { SPH_KERNEL_CUBIC = 0, SPH_KERNEL_WENDLAND_C2 = 1 };
 enum { SPH_GRAVITY_TREE = 0, SPH_GRAVITY_DIRECT = 1, SPH_GRAVITY_NONE = 2 };
 enum { SPH_MULTIPOLE_MONOPOLE = 0, SPH_MULTIPOLE_QUADRUPOLE = 1 };
-enum { SPH_H_FIXED = 0, SPH_H_SOLVE = 1 };
+enum { SPH_H_FIXED = 0, SPH_H_SOLVE = 1, SPH_H_LEARNED = 2 };
 enum { SPH_PRECISION_F32 = 0, SPH_PRECISION_HILO = 1 };
 
 /* Solver configuration. sph_config_default() fills the reference's values (SI, cubic spline, monopole
@@ -68,7 +68,8 @@ typedef struct sph_config {
   uint32_t gravity;       /* SPH_GRAVITY_* */
   uint32_t multipole;     /* SPH_MULTIPOLE_* */
   uint32_t precision;     /* SPH_PRECISION_*: HILO = node-relative hi/lo coordinates + compensated sums */
-  uint32_t h_mode;        /* SPH_H_*: FIXED keeps the uploaded h (the reference); SOLVE iterates h */
+  uint32_t h_mode;        /* SPH_H_*: FIXED keeps the uploaded h (the reference); SOLVE iterates h; LEARNED
+                             checks the MLP's proposal and iterates only where it is rejected (sph_mlp_set) */
   float h_neighbours;     /* SOLVE: target neighbour count inside the support radius */
   float h_tol;            /* SOLVE: relative density residual that ends the iteration */
   uint32_t h_iters;       /* SOLVE: maximum Newton iterations per force evaluation */
@@ -114,7 +115,8 @@ typedef struct sph_diag_out {
   uint32_t overflow_flags;               /* bit0 neighbour list, bit1 traversal stack */
   uint32_t h_iterations;                 /* SOLVE: iterations used by the last force evaluation */
   float h_residual;                      /* SOLVE: max relative density residual after the last solve */
-  float pad;
+  uint32_t h_accepted;                   /* LEARNED: particles whose proposed h passed the first check (last
+                                            solve) */
   /* cumulative tree-walk counters (group MAC): nodes visited, 32-wide pops, particle × multipole and
    * particle × leaf-source interactions (the latter counts every source of a visited leaf) */
   uint64_t walk_nodes, walk_pops, m2p_interactions, p2p_interactions;
@@ -304,6 +306,45 @@ uint32_t sph_dem_count(const sph_dem* dem);
  * order them on one stream. */
 sph_status sph_gravity_tree_noalloc(const void* d_bodies4, uint32_t n, double G, float softening, float theta,
                                     uint32_t leaf_size, uint32_t multipole, void* d_acc4, void* stream);
+
+/* ---- Learned smoothing lengths (no counterpart in the reference, which keeps h fixed: hydrostatic.rs:59-61).
+ * A small MLP, 8 → 64 → 64 → 1 with GELU, proposes each particle's Δlog h for the coming step from its state
+ * at the start of the drift: log(h/h(ρ)) with h(ρ) = η(m/ρ)^(1/3), log(ρ/ρ0), ∇·v·dt, neighbours / target,
+ * log(1 + |a| h / c²), material, log(1 + u/E_iv) and the run's progress (sph_set_progress). In h_mode
+ * SPH_H_LEARNED the proposal (limited to ±0.1 in log h) replaces h before the tree build; one pass then checks
+ * every particle's density residual |ρ − m(η/h)³|/ρ against h_tol and only the rejected particles take the
+ * Newton iterations (at most h_iters). The network runs on the tensor cores with BF16 weights and activations
+ * and FP32 accumulation. Parameter block (SPH_MLP_PARAMS floats): W1[8][64] b1[64] W2[64][64] b2[64] W3[64]
+ * b3 (the SPH_MLP_TRAINABLE weights; W[i][o] by input row) then x_mean[8] x_scale[8] y_mean y_scale
+ * (x' = (x − x_mean)·x_scale; Δlog h = y·y_scale + y_mean). A new context holds the zero network (Δ = 0). */
+#define SPH_MLP_PARAMS 4819
+#define SPH_MLP_TRAINABLE 4801
+sph_status sph_mlp_set(sph_ctx* ctx, const float* params, uint32_t count);
+/* on != 0: every KDK step also keeps its 8 features per particle and the network's Δlog h (original order),
+ * for sph_mlp_features; the training data of the learned h. */
+sph_status sph_mlp_record(sph_ctx* ctx, int on);
+/* The last recorded step: features[n][8] and dlogh[n] (either may be NULL), cap = rows the buffers hold. */
+sph_status sph_mlp_features(sph_ctx* ctx, float* features, float* dlogh, uint32_t cap);
+/* The fraction of the run completed (the eighth input); read by the device at each step. */
+sph_status sph_set_progress(sph_ctx* ctx, float fraction);
+
+/* The network on its own, on the calling thread's current device (host arrays, blocking). */
+typedef struct sph_mlp_train_cfg {
+  uint32_t epochs;        /* passes over the samples */
+  uint32_t batch;         /* samples per Adam step */
+  float lr, beta1, beta2, eps, weight_decay;
+  uint32_t seed;          /* sample shuffling */
+} sph_mlp_train_cfg;
+/* Δlog h of feature rows x[n][8]. */
+sph_status sph_mlp_forward(const float* params, const float* x, uint32_t n, float* out);
+/* Mean squared error on the normalised targets (t − y_mean)/y_scale over all n rows and its gradient w.r.t.
+ * the SPH_MLP_TRAINABLE weights (FP32 sums of the BF16 tensor-core products). */
+sph_status sph_mlp_grad(const float* params, const float* x, const float* t, uint32_t n, float* grad,
+                        float* loss);
+/* Adam on minibatches of (x, t); params is updated in place (its normalisation entries are kept);
+ * loss_per_epoch (may be NULL) receives each epoch's mean training loss. */
+sph_status sph_mlp_train(float* params, const float* x, const float* t, uint32_t n, const sph_mlp_train_cfg* cfg,
+                         float* loss_per_epoch);
 
 #ifdef __cplusplus
 }

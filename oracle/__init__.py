@@ -384,3 +384,31 @@ def dem_step32(pos3, vel3, radius, prm, substeps=1):
         acc = dem_contacts32(pos, vel, radius, prm)
         L.orc_dem_integrate32(pos, vel, acc, len(radius), _c(prm, np.float32))
     return pos, vel
+
+
+# ---- learned smoothing-length MLP (FP64, optional BF16 operand rounding as in the product kernels) --------
+def mlp_param_count(trainable: bool = False) -> int:
+    L = lib()
+    L.orc_mlp_param_count.restype = C.c_int
+    return int(L.orc_mlp_param_count(1 if trainable else 0))
+
+
+def mlp_forward(params, x, bf16: bool = True) -> np.ndarray:
+    """De-normalised outputs (Δlog h) of the MLP for feature rows x[n][8]."""
+    L = lib()
+    L.orc_mlp_forward.argtypes = [f32p, f32p, C.c_int, C.c_int, f64p]
+    x = _c(x, np.float32).reshape(-1, 8)
+    out = np.zeros(len(x), np.float64)
+    L.orc_mlp_forward(_c(params, np.float32), x, len(x), 1 if bf16 else 0, out)
+    return out
+
+
+def mlp_grad(params, x, t, bf16: bool = True):
+    """(mean squared error on the normalised targets, its gradient w.r.t. the trainable parameters)."""
+    L = lib()
+    L.orc_mlp_grad.argtypes = [f32p, f32p, f32p, C.c_int, C.c_int, f64p]
+    L.orc_mlp_grad.restype = C.c_double
+    x = _c(x, np.float32).reshape(-1, 8)
+    g = np.zeros(mlp_param_count(True), np.float64)
+    loss = L.orc_mlp_grad(_c(params, np.float32), x, _c(t, np.float32), len(x), 1 if bf16 else 0, g)
+    return float(loss), g

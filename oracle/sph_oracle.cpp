@@ -1133,3 +1133,114 @@ void orc_dem_integrate32(float* pos3, float* vel3, const float* accum16, int n, 
 }
 
 }  // extern "C"
+
+namespace {
+
+// ---------------------------------------------------------------------------------------------------
+// Learned smoothing-length MLP (no reference counterpart): 8 → 64 → 64 → 1 with GELU, the FP64 statement of
+// the product's BF16-operand / FP32-accumulate kernels. Parameter block (floats):
+//   W1[8][64] b1[64] W2[64][64] b2[64] W3[64] b3 | x_mean[8] x_scale[8] y_mean y_scale
+// (W[i][o] row-major by input). x' = (x − x_mean)·x_scale; z1 = x'W1 + b1; a1 = gelu(z1); z2 = a1W2 + b2;
+// a2 = gelu(z2); y = a2·W3 + b3; the output is y·y_scale + y_mean. With `bf16` set, every tensor-core operand
+// is rounded to bfloat16 where the kernels round it: W1, W2, W3, x', a1 (forward); and in the backward pass
+// dz2 (for both dW2 and da1) and dz1 (for dW1). Gradients are of the mean squared error on the normalised
+// target (t − y_mean)/y_scale with respect to the first 4801 (trainable) parameters, rounding treated as
+// the identity (straight-through).
+// ---------------------------------------------------------------------------------------------------
+constexpr int kMlpIn = 8, kMlpH = 64;
+constexpr int kMlpW1 = 0, kMlpB1 = kMlpW1 + kMlpIn * kMlpH, kMlpW2 = kMlpB1 + kMlpH, kMlpB2 = kMlpW2 + kMlpH * kMlpH,
+              kMlpW3 = kMlpB2 + kMlpH, kMlpB3 = kMlpW3 + kMlpH, kMlpTrain = kMlpB3 + 1, kMlpXm = kMlpTrain,
+              kMlpXs = kMlpXm + kMlpIn, kMlpYm = kMlpXs + kMlpIn, kMlpYs = kMlpYm + 1, kMlpTotal = kMlpYs + 1;
+
+double bf16_round(double v) {
+  // to float, then to the nearest bfloat16 (ties to even), as __float2bfloat16_rn does on a float
+  float f = (float)v;
+  uint32_t u;
+  std::memcpy(&u, &f, 4);
+  u = (u + 0x7fffu + ((u >> 16) & 1u)) & 0xffff0000u;
+  std::memcpy(&f, &u, 4);
+  return (double)f;
+}
+double gelu(double z) { return 0.5 * z * (1.0 + std::erf(z / std::sqrt(2.0))); }
+double gelu_d(double z) {
+  return 0.5 * (1.0 + std::erf(z / std::sqrt(2.0))) + z * std::exp(-0.5 * z * z) / std::sqrt(2.0 * kPi);
+}
+
+struct MlpFwd {
+  double x[kMlpIn], z1[kMlpH], a1[kMlpH], z2[kMlpH], a2[kMlpH], y;
+};
+
+void mlp_forward1(const float* P, const float* xin, bool bf, MlpFwd& f) {
+  auto R = [&](double v) { return bf ? bf16_round(v) : v; };
+  for (int i = 0; i < kMlpIn; ++i) f.x[i] = R(((double)xin[i] - P[kMlpXm + i]) * P[kMlpXs + i]);
+  for (int o = 0; o < kMlpH; ++o) {
+    double z = 0.0;
+    for (int i = 0; i < kMlpIn; ++i) z += f.x[i] * R(P[kMlpW1 + i * kMlpH + o]);
+    f.z1[o] = z + P[kMlpB1 + o];
+    f.a1[o] = R(gelu(f.z1[o]));
+  }
+  for (int o = 0; o < kMlpH; ++o) {
+    double z = 0.0;
+    for (int i = 0; i < kMlpH; ++i) z += f.a1[i] * R(P[kMlpW2 + i * kMlpH + o]);
+    f.z2[o] = z + P[kMlpB2 + o];
+    f.a2[o] = gelu(f.z2[o]);
+  }
+  double y = 0.0;
+  for (int i = 0; i < kMlpH; ++i) y += f.a2[i] * R(P[kMlpW3 + i]);
+  f.y = y + P[kMlpB3];
+}
+
+}  // namespace
+
+extern "C" {
+
+int orc_mlp_param_count(int trainable) { return trainable ? kMlpTrain : kMlpTotal; }
+
+// Δlog h proposals (de-normalised network outputs) for n feature rows x[n][8].
+void orc_mlp_forward(const float* P, const float* x, int n, int bf, double* out) {
+  for (int s = 0; s < n; ++s) {
+    MlpFwd f;
+    mlp_forward1(P, x + (size_t)s * kMlpIn, bf != 0, f);
+    out[s] = f.y * P[kMlpYs] + P[kMlpYm];
+  }
+}
+
+// Mean-squared-error loss on the normalised targets and its gradient w.r.t. the trainable parameters.
+double orc_mlp_grad(const float* P, const float* x, const float* t, int n, int bf, double* grad) {
+  const bool B = bf != 0;
+  auto R = [&](double v) { return B ? bf16_round(v) : v; };
+  std::fill(grad, grad + kMlpTrain, 0.0);
+  double loss = 0.0;
+  double w2[kMlpH * kMlpH], w3[kMlpH];
+  for (int k = 0; k < kMlpH * kMlpH; ++k) w2[k] = R(P[kMlpW2 + k]);
+  for (int k = 0; k < kMlpH; ++k) w3[k] = R(P[kMlpW3 + k]);
+  for (int s = 0; s < n; ++s) {
+    MlpFwd f;
+    mlp_forward1(P, x + (size_t)s * kMlpIn, B, f);
+    const double tn = ((double)t[s] - P[kMlpYm]) / P[kMlpYs];
+    const double e = f.y - tn;
+    loss += e * e;
+    const double dy = 2.0 * e / n;
+    grad[kMlpB3] += dy;
+    double dz2[kMlpH], dz2r[kMlpH];
+    for (int j = 0; j < kMlpH; ++j) {
+      grad[kMlpW3 + j] += dy * f.a2[j];
+      dz2[j] = dy * w3[j] * gelu_d(f.z2[j]);
+      dz2r[j] = R(dz2[j]);
+      grad[kMlpB2 + j] += dz2[j];
+    }
+    for (int i = 0; i < kMlpH; ++i)
+      for (int j = 0; j < kMlpH; ++j) grad[kMlpW2 + i * kMlpH + j] += f.a1[i] * dz2r[j];
+    for (int i = 0; i < kMlpH; ++i) {
+      double da1 = 0.0;
+      for (int j = 0; j < kMlpH; ++j) da1 += dz2r[j] * w2[i * kMlpH + j];
+      const double dz1 = da1 * gelu_d(f.z1[i]);
+      grad[kMlpB1 + i] += dz1;
+      const double dz1r = R(dz1);
+      for (int k = 0; k < kMlpIn; ++k) grad[kMlpW1 + k * kMlpH + i] += f.x[k] * dz1r;
+    }
+  }
+  return loss / n;
+}
+
+}  // extern "C"
