@@ -158,7 +158,7 @@ __device__ __forceinline__ void features(int t, const State& st, const float* __
   const float heq = fa.eta * cbrtf(m / r);
   const float dt = (float)segs[st.seg[t]].dt;
   const float4 a = acc[t];
-  const float c = fmaxf(fdata[t].w, 1.0e-30f);
+  const float c = fmaxf(fdata[t].w, P->sig_floor);  // the Courant signal's floor keeps c² > 0
   f[0] = logf(p.w / heq);                                                      // log h relative to h(rho)
   f[1] = logf(r / rho0);                                                       // log rho / rho0
   f[2] = divv[t] * dt;                                                         // div v over the step
@@ -195,7 +195,7 @@ __global__ void __launch_bounds__(ROWS) k_mlp_propose(int n, State st, const flo
     mlp_rows(r0, sx, sh1, w, sy, nullptr, nullptr, nullptr);
     if (t < n) {
       const float d = (sy[r] + b3) * ys + ym;
-      const float dc = fminf(fmaxf(d, -0.1f), 0.1f);
+      const float dc = d == d ? fminf(fmaxf(d, -0.1f), 0.1f) : 0.0f;  // no proposal from a NaN
       if (apply) st.pos_h[t].w = st.pos_h[t].w * expf(dc);
       if (rec) {
         const unsigned id = st.id[t];

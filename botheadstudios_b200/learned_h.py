@@ -117,9 +117,10 @@ def solver_config(units, h_mode: int = 1, h_iters: int = 2, **over) -> dict:
 
 
 def collect(I, steps: int, every: int = 1, h_iters: int = 6, device: int = -1, max_rows: int | None = None,
-            seed: int = 0):
+            seed: int = 0, skip: int = 0):
     """Run the plain solver (a converged iterative solve) on initial conditions I for `steps` KDK steps and
-    record (features at the start of each step's drift, Δlog h the solve reached). Returns (X, T)."""
+    record (features at the start of each step's drift, Δlog h the solve reached), leaving out the first
+    `skip` steps (the settling of the initial lattice). Returns (X, T)."""
     from .gpusph import GpuSph
     rng = np.random.default_rng(seed)
     Xs, Ts = [], []
@@ -131,7 +132,7 @@ def collect(I, steps: int, every: int = 1, h_iters: int = 6, device: int = -1, m
             s.set_progress(k / max(steps - 1, 1))
             h0 = s.inspect("H").astype(np.float64)
             s.encode_kdk(1)
-            if k % every:
+            if k < skip or k % every:
                 continue
             f, _ = s.mlp_features()
             h1 = s.inspect("H").astype(np.float64)
@@ -147,18 +148,27 @@ def collect(I, steps: int, every: int = 1, h_iters: int = 6, device: int = -1, m
 def training_set(device: int = -1, quick: bool = False):
     """Trajectories of the two training shapes: the 10,240-particle two-body impact (8,192 + 2,048) and an
     equilibrium planet (131,072 particles; 16,384 for a quick set), both with the learned-h method's solver."""
-    steps_i, steps_p = (30, 10) if quick else (150, 60)
+    steps_i, steps_p = (30, 10) if quick else (300, 80)
     Ii = ic.impact(8192, 2048, n_ngb=64.0, seed=5)
     Ip = ic.planet(16_384 if quick else 131_072, n_ngb=64.0, seed=6)
-    Xa, Ta = collect(Ii, steps_i, device=device)
-    Xb, Tb = collect(Ip, steps_p, device=device, max_rows=None if quick else 32_768)
+    Xa, Ta = collect(Ii, steps_i, device=device, skip=3 if quick else 10)
+    Xb, Tb = collect(Ip, steps_p, device=device, max_rows=None if quick else 32_768, skip=2 if quick else 5)
     return np.concatenate([Xa, Xb]), np.concatenate([Ta, Tb])
 
 
-def fit(X, T, epochs: int = 30, batch: int = 4096, lr: float = 2e-3, seed: int = 0):
+# (epochs, learning rate) stages; Adam restarts at each stage
+SCHEDULE = ((80, 2e-3), (40, 5e-4), (20, 1.25e-4))
+
+
+def fit(X, T, schedule=SCHEDULE, batch: int = 4096, seed: int = 0):
+    """Train from a fresh initialisation through the stages of `schedule`; returns (params, losses)."""
     xm, xs, ym, ys = normalisation(X, T)
-    p0 = init_params(xm, xs, ym, ys, seed=seed)
-    return train(p0, X, T, epochs=epochs, batch=batch, lr=lr, seed=seed)
+    p = init_params(xm, xs, ym, ys, seed=seed)
+    losses = []
+    for k, (epochs, lr) in enumerate(schedule):
+        p, l = train(p, X, T, epochs=epochs, batch=batch, lr=lr, seed=seed + k)
+        losses.append(l)
+    return p, np.concatenate(losses)
 
 
 def save(params: np.ndarray, path: str = DEFAULT_PATH, **meta):
@@ -177,11 +187,10 @@ def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("cmd", choices=["train"])
     ap.add_argument("--out", default=DEFAULT_PATH)
-    ap.add_argument("--epochs", type=int, default=30)
     ap.add_argument("--quick", action="store_true")
     a = ap.parse_args(argv)
     X, T = training_set(quick=a.quick)
-    p, losses = fit(X, T, epochs=a.epochs)
+    p, losses = fit(X, T, schedule=((5, 2e-3),) if a.quick else SCHEDULE)
     save(p, a.out, losses=losses, rows=len(X))
     print(f"trained on {len(X)} rows: loss {losses[0]:.4g} -> {losses[-1]:.4g}; saved {a.out}")
 

@@ -51,7 +51,7 @@ def test_training_fits_a_smooth_target():
     rng = np.random.default_rng(9)
     x = rng.normal(size=(40_000, 8)).astype(np.float32)
     t = (0.004 + 0.01 * np.tanh(x[:, 2]) + 0.003 * x[:, 0] * x[:, 1]).astype(np.float32)
-    p, losses = learned_h.fit(x[:32_000], t[:32_000], epochs=25, batch=2048, lr=3e-3)
+    p, losses = learned_h.fit(x[:32_000], t[:32_000], schedule=((25, 3e-3),), batch=2048)
     assert losses[-1] < 0.05 * losses[0]
     pred = learned_h.forward(p, x[32_000:])
     err = np.sqrt(np.mean((pred - t[32_000:]) ** 2))
