@@ -206,6 +206,19 @@ def timed(ctxs, encode, steps: int, local: int) -> float:
     return e0.elapsed_time(e1)
 
 
+def plain_same(wl: dict, I, device: int, steps: int, warmup: int) -> dict:
+    """The plain GPU form (iterated h: SPH_H_SOLVE) on the same initial conditions, timed the same way: the
+    comparison of the learned form."""
+    from botheadstudios_b200 import workloads
+    with workloads.solver(wl, I, device, h_mode=1) as s:
+        workloads.upload(s, I)
+        s.encode_kdk(warmup)
+        s.sync()
+        ms = timed([s], s.encode_kdk, steps, max(device, 0))
+        d = s.diag()
+    return dict(value=len(I.particles) * steps / (ms / 1000.0), ms_per_step=ms / steps, h_residual=d["h_residual"])
+
+
 def plain_sequential(wl: dict, B, device: int, impacts: int = 16, steps: int = 2) -> dict:
     """The plain GPU form on a batch's impacts: one impact at a time, each in its own context with the
     workload's untuned configuration, no graph (the reference's offline driver runs impacts sequentially)."""
@@ -336,6 +349,8 @@ def run_ours(args, wl, world, rank, local, pg):
     plain = None
     if wl.get("kind") == "batch" and rank == 0 and not args.no_plain:
         plain = plain_sequential(wl, I, local)
+    elif wl.get("h_solve") == 2 and rank == 0 and not args.no_plain:
+        plain = plain_same(wl, I, local, args.steps, args.warmup)
 
     if rank != 0:
         return
@@ -406,17 +421,21 @@ def run_ours(args, wl, world, rank, local, pg):
                             contexts=len(runner.ctxs),
                             graph=bool(wl.get("graph", 0)), kernel=wl["kernel"], neighbours=wl["n_ngb"],
                             theta=wl["theta"], quadrupole=bool(wl["quad"]), leaf=wl["leaf"],
-                            h_solve=bool(wl["h_solve"]), dt="adaptive CFL 0.3", parallelism=f"replicas{world}",
+                            h_mode=["fixed", "solve", "learned"][wl["h_solve"]], dt="adaptive CFL 0.3",
+                            parallelism=f"replicas{world}",
                             l2="working set > L2 (no flush needed)"),
                 e2e=dict(value=e2e_value, unit=UNIT, h2d_bytes_per_step=48 * n, d2h_bytes_per_step=48 * n,
                          steps=e2e_steps),
                 gpu_launches=launches, roofline=roof, roofline_hbm=roof_hbm, phases=phases, cpu_baseline=cpu,
                 clocks=clk.summary(),
-                autotune=tuned, plain_sequential=plain,
+                autotune=tuned, **({"plain_sequential": plain} if wl.get("kind") == "batch" else
+                                   {"plain_form": plain} if plain else {}),
                 physics=dict(energy_drift=(energy1 - energy0) / abs(pot0) if pot0 else None,
                              sim_time=dd["time"], dt=dd["dt"],
                              max_neighbours=max(d["max_neighbours_seen"] for d in d1),
                              overflow_flags=max(d["overflow_flags"] for d in d1),
+                             h_accepted_fraction=(sum(d["h_accepted"] for d in d1) / n
+                                                  if wl.get("h_solve") == 2 else None),
                              h_residual=max(d["h_residual"] for d in d1)))
     print(json.dumps(line), flush=True)
 

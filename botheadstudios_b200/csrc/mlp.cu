@@ -24,6 +24,9 @@ constexpr int XS = 24;    // row stride of K=16 operands
 constexpr int HS = 72;    // row stride of K=64 operands
 constexpr int TS = 136;   // row stride of K=128 (sample-major) operands
 constexpr int ROWS = 128;
+// Largest proposed change of log h: an outlier proposal stays within reach of the fallback's Newton steps
+// (±20 % each, inside the list skin around the proposal).
+constexpr float kMaxStep = 0.03f;
 
 __device__ __forceinline__ unsigned ld32(const __nv_bfloat16* p) { return *reinterpret_cast<const unsigned*>(p); }
 __device__ __forceinline__ void st32(__nv_bfloat16* p, float a, float b) {
@@ -194,8 +197,10 @@ __global__ void __launch_bounds__(ROWS) k_mlp_propose(int n, State st, const flo
     __syncwarp();
     mlp_rows(r0, sx, sh1, w, sy, nullptr, nullptr, nullptr);
     if (t < n) {
-      const float d = (sy[r] + b3) * ys + ym;
-      const float dc = d == d ? fminf(fmaxf(d, -0.1f), 0.1f) : 0.0f;  // no proposal from a NaN
+      // the network gives log(h_next / h(rho)); the step from the current h subtracts log(h / h(rho)) = f[0],
+      // so a residual left by the previous solve is corrected whatever the network learned
+      const float d = (sy[r] + b3) * ys + ym - f[0];
+      const float dc = d == d ? fminf(fmaxf(d, -kMaxStep), kMaxStep) : 0.0f;  // no proposal from a NaN
       if (apply) st.pos_h[t].w = st.pos_h[t].w * expf(dc);
       if (rec) {
         const unsigned id = st.id[t];

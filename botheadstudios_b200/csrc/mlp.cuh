@@ -39,8 +39,9 @@ struct MlpFeatureArgs {
   float n_target;    // target neighbour count
 };
 
-// In-step proposal: features → MLP → h ← h·exp(clamp(Δlog h, ±0.1)) in pos_h.w (sorted order). With `rec`
-// non-null, also writes each particle's 8 features to rec[id] (original order) and its Δlog h to dh[id].
+// In-step proposal: features → MLP y = log(h_next/h(ρ)) → Δlog h = y − log(h/h(ρ)) → h ← h·exp(clamp(Δ, ±0.03))
+// in pos_h.w (sorted order). With `rec` non-null, also writes each particle's 8 features to rec[id]
+// (original order) and its Δlog h to dh[id].
 int launch_mlp_propose(const Dev& d, const MlpPacked* w, const MlpFeatureArgs& fa, const float* divv,
                        float* rec, float* dh, bool apply, cudaStream_t s);
 

@@ -2,7 +2,8 @@
 training on the GPU through the library's kernels, and the parameter file the solver loads.
 
 The network (8 → 64 → 64 → 1, GELU) proposes each particle's Δlog h for the coming step; see sph_b200.h for the
-features. Training targets are the smoothing lengths a converged iterative solve reaches at the next step,
+features. Training targets are log(h_next/h(ρ)): the smoothing lengths a converged iterative solve reaches at
+the next step, relative to the equilibrium h(ρ) = η(m/ρ)^(1/3) of the current density,
 recorded while the plain solver runs (SPH_H_SOLVE with many iterations), so the network learns to land where
 the iteration would. In SPH_H_LEARNED the solver checks every proposal's density residual and iterates only
 the rejected particles, so a poor proposal costs iterations, never accuracy.
@@ -136,7 +137,8 @@ def collect(I, steps: int, every: int = 1, h_iters: int = 6, device: int = -1, m
                 continue
             f, _ = s.mlp_features()
             h1 = s.inspect("H").astype(np.float64)
-            t = np.log(h1 / h0).astype(np.float32)
+            # the network's target: log(h_next / h(rho)) = log(h_next / h) + log(h / h(rho))
+            t = (np.log(h1 / h0) + f[:, 0]).astype(np.float32)
             if max_rows and len(t) > max_rows:
                 sel = rng.choice(len(t), max_rows, replace=False)
                 f, t = f[sel], t[sel]

@@ -17,6 +17,12 @@ WORKLOADS = {
     # the precision-sweep body: a 4,194,304-particle differentiated planet at rest (θ swept by the caller)
     "planet_4m": dict(kind="planet", n_target=4_194_304, n_impactor=0, n_ngb=64.0, kernel="wendland", theta=0.5,
                       quad=1, leaf=16, h_solve=1, max_nbr=192),
+    # the learned smoothing-length form of the 4M and 1M impacts: the network (trained on the 10k impact and the
+    # planet) proposes h, one residual check, Newton only for the rejected particles
+    "learned_4m": dict(n_target=3_813_004, n_impactor=381_300, n_ngb=64.0, kernel="wendland", theta=0.6, quad=1,
+                       leaf=16, h_solve=2, max_nbr=192),
+    "learned_1m": dict(n_target=953_250, n_impactor=95_326, n_ngb=64.0, kernel="wendland", theta=0.6, quad=1,
+                       leaf=16, h_solve=2, max_nbr=192),
     # 256 independent impacts, total particle counts log-uniform in [20k, 200k] (about 2.0e7 particles), mass
     # ratio 0.05-0.15, angle 0-75°, v_imp 1.0-1.5 v_esc; the 1M impact's method; one context per size bucket
     # (launch configuration autotuned per bucket) advancing its impacts with one launch per phase, steady steps
@@ -68,5 +74,11 @@ def config(wl: dict, I, **over) -> dict:
 
 
 def solver(wl: dict, I, device: int = -1, **over):
+    """A context for the workload; the learned form gets the trained network (progress held at 0.5)."""
     from .gpusph import GpuSph
-    return GpuSph(len(I.particles), device=device, **config(wl, I, **over))
+    s = GpuSph(len(I.particles), device=device, **config(wl, I, **over))
+    if config(wl, I, **over)["h_mode"] == 2:
+        from . import learned_h
+        s.mlp_set(learned_h.load())
+        s.set_progress(0.5)
+    return s
