@@ -23,7 +23,7 @@ from .gpusph import GpuSph
 # particle-count buckets [lo, hi)
 BUCKETS = ((0, 45_000), (45_000, 100_000), (100_000, 1 << 31))
 CANDIDATES = dict(leaf_size=(8, 16, 32), walk_warps=(2, 4, 8), block_threads=(128, 256, 512))
-DEFAULT_CHOICE = dict(leaf_size=16, walk_warps=4, block_threads=256)
+DEFAULT_CHOICE = dict(leaf_size=16, walk_warps=2, block_threads=256)
 
 
 def bucket_of(n: int) -> int:

@@ -271,7 +271,7 @@ int launch_h_learned(const Dev& d, const Cfg& c, cudaStream_t s) {
 // :263-269) reduced to each impact's minimum with one atomic per warp (per lane in a warp that straddles two
 // impacts).
 // ---------------------------------------------------------------------------------------------------
-template <int KERNEL, bool GRAV>
+template <int KERNEL, bool GRAV, bool DIVV>
 __global__ void k_forces(int n, State st, const float4* __restrict__ fdata, const unsigned* __restrict__ nbr,
                          const unsigned* __restrict__ nbr_cnt, unsigned cap, const float4* __restrict__ grav,
                          const DevParams* __restrict__ P, Seg* __restrict__ segs, float4* __restrict__ acc,
@@ -313,7 +313,7 @@ __global__ void k_forces(int n, State st, const float4* __restrict__ fdata, cons
       az += gz * s;
       const float vg = vx * gx + vy * gy + vz * gz;
       de += 0.5f * fj.x * coeff * vg;
-      dv += fj.x * vg;
+      if (DIVV) dv += fj.x * vg;
     }
     if (GRAV) {
       const float4 g = grav[t];
@@ -322,7 +322,7 @@ __global__ void k_forces(int n, State st, const float4* __restrict__ fdata, cons
       az += g.z;
     }
     acc[t] = make_float4(ax, ay, az, de);
-    divv[t] = -dv / fi.y;  // ∇·v_i = −(1/ρ_i) Σ_j m_j v_ij·∇_i W_ij
+    if (DIVV) divv[t] = -dv / fi.y;  // ∇·v_i = −(1/ρ_i) Σ_j m_j v_ij·∇_i W_ij (a learned-h input)
     const float vmag = sqrtf(vi.x * vi.x + vi.y * vi.y + vi.z * vi.z);
     sig = pi.w / fmaxf(fi.w + vmag, P->sig_floor);
   }
@@ -341,12 +341,20 @@ int launch_forces(const Dev& d, const Cfg& c, cudaStream_t s) {
   const int blocks = (d.n + c.blk - 1) / c.blk;
   const bool g = c.gravity != 2;
 #define FARGS d.n, d.s(), d.fdata, d.nbr, d.nbr_cnt, d.nbr_cap, d.grav, d.P, d.segs, d.acc, d.divv
-  if (c.kernel == 1) {
-    if (g) k_forces<1, true><<<blocks, c.blk, 0, s>>>(FARGS);
-    else k_forces<1, false><<<blocks, c.blk, 0, s>>>(FARGS);
+  if (c.divv) {
+    if (c.kernel == 1) {
+      if (g) k_forces<1, true, true><<<blocks, c.blk, 0, s>>>(FARGS);
+      else k_forces<1, false, true><<<blocks, c.blk, 0, s>>>(FARGS);
+    } else {
+      if (g) k_forces<0, true, true><<<blocks, c.blk, 0, s>>>(FARGS);
+      else k_forces<0, false, true><<<blocks, c.blk, 0, s>>>(FARGS);
+    }
+  } else if (c.kernel == 1) {
+    if (g) k_forces<1, true, false><<<blocks, c.blk, 0, s>>>(FARGS);
+    else k_forces<1, false, false><<<blocks, c.blk, 0, s>>>(FARGS);
   } else {
-    if (g) k_forces<0, true><<<blocks, c.blk, 0, s>>>(FARGS);
-    else k_forces<0, false><<<blocks, c.blk, 0, s>>>(FARGS);
+    if (g) k_forces<0, true, false><<<blocks, c.blk, 0, s>>>(FARGS);
+    else k_forces<0, false, false><<<blocks, c.blk, 0, s>>>(FARGS);
   }
 #undef FARGS
   return 1;

@@ -402,9 +402,9 @@ static void walk_fused(const Dev& d, const Cfg& c, cudaStream_t s) {
     return;
   }
   switch (c.walk_warps) {
-    case 2: walk<2, true, QUAD, true, false>(d, c, s); break;
+    case 4: walk<4, true, QUAD, true, false>(d, c, s); break;
     case 8: walk<8, true, QUAD, true, false>(d, c, s); break;
-    default: walk<4, true, QUAD, true, false>(d, c, s); break;
+    default: walk<2, true, QUAD, true, false>(d, c, s); break;
   }
 }
 

@@ -444,13 +444,14 @@ sph_status sph_create(const sph_config* cfg, uint32_t capacity, sph_ctx** out) {
   ctx->kc.hilo = cfg->precision == SPH_PRECISION_HILO;
   ctx->kc.h_solve = cfg->h_mode == SPH_H_SOLVE || cfg->h_mode == SPH_H_LEARNED;
   ctx->kc.learned = cfg->h_mode == SPH_H_LEARNED;
+  ctx->kc.divv = ctx->kc.learned;
   ctx->kc.h_eta = std::cbrt(3.0f * cfg->h_neighbours / (4.0f * 3.14159265358979f));
   ctx->kc.h_tol = cfg->h_tol;
   ctx->kc.h_iters = (int)cfg->h_iters;
   ctx->kc.skin = ctx->kc.h_solve ? 0.15f : 0.0f;
   ctx->kc.mac = (int)cfg->mac;
   ctx->kc.blk = cfg->block_threads ? (int)cfg->block_threads : 256;
-  ctx->kc.walk_warps = cfg->walk_warps ? (int)cfg->walk_warps : 4;
+  ctx->kc.walk_warps = cfg->walk_warps ? (int)cfg->walk_warps : 2;
   if (cfg->device >= 0) {
     cudaError_t de = cudaSetDevice(cfg->device);
     if (de != cudaSuccess) {
@@ -1073,6 +1074,7 @@ sph_status sph_mlp_record(sph_ctx* ctx, int on) {
   }
   if (ctx->mlp_rec != (on != 0)) drop_graphs(ctx);  // the captured steps hold the recording pointers
   ctx->mlp_rec = on != 0;
+  ctx->kc.divv = ctx->kc.learned || ctx->mlp_rec;
   return SPH_OK;
 }
 

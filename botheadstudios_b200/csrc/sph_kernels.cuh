@@ -163,8 +163,9 @@ struct Cfg {
   int mac = 0;          // 0 group walk, 1 per-particle reference walk
   float nbr_skin = 0.0f;  // list inflation without the h-solve (grain contacts: a superset, cut exactly later)
   int blk = 256;        // threads per block of the per-particle gather kernels (density, h-solve, forces)
-  int walk_warps = 4;   // warps per block of the fused walk (2, 4 or 8)
+  int walk_warps = 2;   // warps per block of the fused walk (2, 4 or 8)
   int learned = 0;      // smoothing lengths proposed by the MLP, checked, iterated only where rejected
+  int divv = 0;         // the force pass also writes ∇·v (the learned proposal or its recording needs it)
 };
 
 // Grain contact constants (the reference's GpuStepParams subset used by the contact law and solve).

@@ -19,17 +19,22 @@ def main():
     ap.add_argument("--mac", type=int, default=0)
     ap.add_argument("--theta", type=float, default=None)
     ap.add_argument("--precision", type=int, default=0, help="1 = node-relative hi/lo + compensated sums")
+    ap.add_argument("--leaf", type=int, default=None, help="LBVH leaf size (default: the workload's)")
+    ap.add_argument("--walk-warps", type=int, default=0, help="warps per walk block (2, 4, 8; 0 = 4)")
+    ap.add_argument("--block", type=int, default=0, help="threads per block of the gather kernels (0 = 256)")
     ap.add_argument("--accuracy", type=int, default=0,
                     help="targets for an FP64 direct-sum check of the tree gravity (0 = skip)")
     args = ap.parse_args()
     wl = workloads.WORKLOADS[args.workload]
     I = workloads.build(wl)
-    over = dict(mac=args.mac, precision=args.precision)
+    over = dict(mac=args.mac, precision=args.precision, walk_warps=args.walk_warps, block_threads=args.block)
+    if args.leaf is not None:
+        over["leaf_size"] = args.leaf
     if args.theta is not None:
         over["theta"] = args.theta
     acc_err = None
     with workloads.solver(wl, I, **over) as s:
-        s.upload(I.particles, I.eos, I.softening)
+        workloads.upload(s, I)
         s.encode_kdk(args.warmup)
         s.sync()
         d0 = s.diag()
@@ -52,7 +57,7 @@ def main():
     n = len(I.particles)
     walks = max(prof["calls"]["gravity"], 1)
     stats = {k: (d1[k] - d0[k]) / walks for k in ("walk_nodes", "walk_pops", "m2p_interactions", "p2p_interactions")}
-    print(json.dumps(dict(workload=args.workload, particles=n, steps=args.steps, phases_ms=prof["ms"],
+    print(json.dumps(dict(workload=args.workload, particles=n, steps=args.steps, config=over, phases_ms=prof["ms"],
                           calls=prof["calls"], launches=prof["kernel_launches"], per_walk=stats,
                           per_particle={k: v / n for k, v in stats.items()}, gravity_error=acc_err)))
 

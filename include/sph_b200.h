@@ -85,7 +85,7 @@ typedef struct sph_config {
                              and replays it (phase timing is not recorded for replayed substeps) */
   uint32_t block_threads; /* threads per block of the density, h-solve and force kernels: 64..1024, a multiple of
                              32; 0 = 256 */
-  uint32_t walk_warps;    /* warps per block of the fused gravity + neighbour walk: 2, 4 or 8; 0 = 4 */
+  uint32_t walk_warps;    /* warps per block of the fused gravity + neighbour walk: 2, 4 or 8; 0 = 2 */
   uint32_t reserved[3];
 } sph_config;
 
