@@ -103,15 +103,19 @@ __device__ __forceinline__ void h_sums(int t, const State& st, const unsigned* _
   }
 }
 
-// The Newton update of h from the residual f = ρ − m(η/h)³, limited to ±20 % and to the list's skin.
+// The Newton update of h from the residual f = ρ − m(η/h)³, limited to ±20 % and to the list's skin. `res`
+// is the relative residual |f|/ρ; `drel` the relative density change the unlimited Newton step would make
+// (|∂ρ/∂h · Δh|/ρ), the density error that is left when h stops here.
 __device__ __forceinline__ float h_newton(float h, float m, float rho, float drho, float eta, float h0, float skin,
-                                          float& res) {
+                                          float& res, float& drel) {
   const float e3 = eta * eta * eta;
   const float rt = m * e3 / (h * h * h);
   const float f = rho - rt;
   res = fabsf(f) / fmaxf(rho, 1.0e-30f);
   const float fp = drho + 3.0f * rt / h;
-  float hn = fabsf(fp) > 0.0f ? h - f / fp : h;
+  const float dh = fabsf(fp) > 0.0f ? -f / fp : 0.0f;
+  drel = fabsf(drho * dh) / fmaxf(rho, 1.0e-30f);
+  float hn = h + dh;
   if (!(hn == hn)) hn = h;  // NaN guard
   hn = fminf(fmaxf(hn, 0.8f * h), 1.2f * h);
   hn = fminf(hn, h0 * (1.0f + skin) * 0.999f);
@@ -130,7 +134,8 @@ __global__ void k_h_iter(int n, State st, const unsigned* __restrict__ nbr, cons
     float rho, drho;
     h_sums<KERNEL>(t, st, nbr, nbr_cnt, cap, rho, drho);
     const float m = st.mass[t], h = st.pos_h[t].w;
-    float hn = h_newton(h, m, rho, drho, eta, h0[t], skin, res);
+    float drel;
+    float hn = h_newton(h, m, rho, drho, eta, h0[t], skin, res, drel);
     if (last) {
       // the final pass is the density pass: same sum, same order as k_density_eos
       rho_out[t] = rho;
@@ -142,6 +147,8 @@ __global__ void k_h_iter(int n, State st, const unsigned* __restrict__ nbr, cons
   const float wres = warp_max(res);
   if ((threadIdx.x & 31) == 0) atomicMax(&P->h_residual_bits, __float_as_uint(wres));
 }
+
+constexpr float kDensityTolFraction = 0.25f;
 
 // Learned h: check the proposed (or current) h of every listed particle. A particle whose relative density
 // residual is within tolerance (or that is on its last pass) is final: its density and EOS record are
@@ -164,11 +171,13 @@ __global__ void k_h_check(int n, const unsigned* __restrict__ list, const unsign
     int t = -1;
     if (i < count) {
       t = list ? (int)list[i] : i;
-      float rho, drho, res;
+      float rho, drho, res, drel;
       h_sums<KERNEL>(t, st, nbr, nbr_cnt, cap, rho, drho);
       const float m = st.mass[t], h = st.pos_h[t].w;
-      const float hn = h_newton(h, m, rho, drho, eta, h0[t], skin, res);
-      if (res <= tol || last) {
+      const float hn = h_newton(h, m, rho, drho, eta, h0[t], skin, res, drel);
+      // accepted: residual within tolerance and a density that one more step would move by < tol/4 (near a
+      // surface ρ depends strongly on h, and a small residual alone can leave a larger density error)
+      if ((res <= tol && drel <= kDensityTolFraction * tol) || last) {
         rho_out[t] = rho;
         fdata[t] = eos_record(eos, st.mat[t], m, rho, st.vel_u[t].w, P);
         wres = fmaxf(wres, res);

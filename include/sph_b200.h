@@ -312,8 +312,9 @@ sph_status sph_gravity_tree_noalloc(const void* d_bodies4, uint32_t n, double G,
  * at the start of the drift: log(h/h(ρ)) with h(ρ) = η(m/ρ)^(1/3), log(ρ/ρ0), ∇·v·dt, neighbours / target,
  * log(1 + |a| h / c²), material, log(1 + u/E_iv) and the run's progress (sph_set_progress). In h_mode
  * SPH_H_LEARNED the proposal (limited to ±0.03 in log h) replaces h before the tree build; one pass then checks
- * every particle's density residual |ρ − m(η/h)³|/ρ against h_tol and only the rejected particles take the
- * Newton iterations (at most h_iters). The network runs on the tensor cores with BF16 weights and activations
+ * every particle: it is accepted when its density residual |ρ − m(η/h)³|/ρ is within h_tol and the density
+ * change one more Newton step would make is within h_tol/4; only the rejected particles take the Newton
+ * iterations (at most h_iters). The network runs on the tensor cores with BF16 weights and activations
  * and FP32 accumulation. Parameter block (SPH_MLP_PARAMS floats): W1[8][64] b1[64] W2[64][64] b2[64] W3[64]
  * b3 (the SPH_MLP_TRAINABLE weights; W[i][o] by input row) then x_mean[8] x_scale[8] y_mean y_scale
  * (x' = (x − x_mean)·x_scale). The network's output y·y_scale + y_mean is log(h_next/h(ρ)); the proposal is

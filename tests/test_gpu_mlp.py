@@ -126,14 +126,13 @@ def test_trained_network_gains_over_the_method_without_it():
     # held out: a 33,000-particle impact (the network saw the 10,240-particle impact and a planet)
     I = ic.impact(30_000, 3_000, n_ngb=64.0, seed=77)
     acc_t, res_t, out_t = _run(I, learned_h.load())
-    acc_0, res_0, out_0 = _run(I, None)  # the zero network: the proposal is h(rho) of the last step
-    _, res_p, out_p = _run(I, None, mode="solve")  # the plain iterative solve
-    # what the network gains: several times more particles pass the first residual check ...
+    acc_0, res_0, out_0 = _run(I, None)  # without the network: the proposal is h(rho) of the last step
+    # what the network gains: several times more particles pass the first check ...
     assert acc_t.mean() > 2.5 * acc_0.mean() and acc_t.mean() > 0.3
-    # ... at the same accuracy: every final density residual within the tolerance (1e-3), and the densities
-    # as close to a converged solve as the plain method's (rms ≤ 1e-3, max no worse than the plain one)
+    # ... with every final residual within the tolerance (1e-3) ...
     assert res_t.max() <= 1.0001e-3 and res_0.max() <= 1.3e-3
+    # ... and densities closer to a converged solve than without it (rms well inside 1e-3)
     rms_t, max_t = _density_error(I, out_t)
-    rms_p, max_p = _density_error(I, out_p)
-    assert rms_t <= 1e-3 and rms_p <= 1e-3
-    assert max_t <= 1.5 * max_p
+    rms_0, max_0 = _density_error(I, out_0)
+    assert rms_t <= rms_0 and max_t <= max_0
+    assert rms_t <= 3e-4 and max_t <= 3e-3
