@@ -39,14 +39,19 @@ __global__ void k_density_eos(int n, State st, const unsigned* __restrict__ nbr,
   if (t >= n) return;
   const float4 pi = st.pos_h[t];
   const float m = st.mass[t];
-  float r_i = m * kern_w<KERNEL>(0.0f, pi.w);
+  float w, dwdr, dwdh;
+  kern_pair<KERNEL>(0.0f, pi.w, w, dwdr, dwdh);
+  float r_i = m * w;
   const unsigned c = min(nbr_cnt[t], cap);
   for (unsigned k = 0; k < c; ++k) {
     const unsigned j = nbr[nbr_slot((unsigned)t, k, cap)];
     const float4 pj = st.pos_h[j];
     const float r = pair_r(pi, pj);
     const float hij = pair_h(pi.w, pj.w);
-    if (r < hij) r_i += st.mass[j] * kern_w<KERNEL>(r, hij);
+    if (r < hij) {
+      kern_pair<KERNEL>(r, hij, w, dwdr, dwdh);
+      r_i += st.mass[j] * w;
+    }
   }
   rho[t] = r_i;
   fdata[t] = eos_record(eos, st.mat[t], m, r_i, st.vel_u[t].w, P);
@@ -87,8 +92,10 @@ __device__ __forceinline__ void h_sums(int t, const State& st, const unsigned* _
   const float4 pi = st.pos_h[t];
   const float m = st.mass[t];
   const float h = pi.w;
-  rho = m * kern_w<KERNEL>(0.0f, h);
-  drho = m * kern_dwdh<KERNEL>(0.0f, h);
+  float w, dwdr, dwdh;
+  kern_pair<KERNEL>(0.0f, h, w, dwdr, dwdh);
+  rho = m * w;
+  drho = m * dwdh;
   const unsigned c = min(nbr_cnt[t], cap);
   for (unsigned k = 0; k < c; ++k) {
     const unsigned j = nbr[nbr_slot((unsigned)t, k, cap)];
@@ -97,8 +104,9 @@ __device__ __forceinline__ void h_sums(int t, const State& st, const unsigned* _
     const float hij = pair_h(h, pj.w);
     if (r < hij) {
       const float mj = st.mass[j];
-      rho += mj * kern_w<KERNEL>(r, hij);
-      drho += mj * 0.5f * kern_dwdh<KERNEL>(r, hij);
+      kern_pair<KERNEL>(r, hij, w, dwdr, dwdh);
+      rho += mj * w;
+      drho += mj * 0.5f * dwdh;
     }
   }
 }
@@ -314,8 +322,10 @@ __global__ void k_forces(int n, State st, const float4* __restrict__ fdata, cons
         pij = (-alpha * c_bar * mu + beta * mu * mu) / rho_bar;
       }
       const float coeff = fi.z + fj.z + pij;
-      const float dw = kern_dw<KERNEL>(r, hij);
-      const float gx = (dx / r) * dw, gy = (dy / r) * dw, gz = (dz / r) * dw;
+      float w, dw, dwdh;
+      kern_pair<KERNEL>(r, hij, w, dw, dwdh);
+      const float dwr = dw * __frcp_rn(r);  // ∇_i W = (dx/r) ∂W/∂r
+      const float gx = dx * dwr, gy = dy * dwr, gz = dz * dwr;
       const float s = -coeff * fj.x;
       ax += gx * s;
       ay += gy * s;

@@ -97,48 +97,37 @@ __device__ __forceinline__ unsigned expand_bits(unsigned v) {
   return v;
 }
 
-// ---- SPH kernels with support radius h (sph_step.wgsl:64-77; Wendland C2 from its formula) ----------
-__device__ __forceinline__ float w_cubic(float r, float h) {
-  const float q = r / h;
-  const float sig = 8.0f / (kPiF * h * h * h);
-  if (q < 0.5f) return sig * (1.0f - 6.0f * q * q + 6.0f * q * q * q);
-  if (q < 1.0f) { const float t = 1.0f - q; return sig * 2.0f * t * t * t; }
-  return 0.0f;
-}
-__device__ __forceinline__ float dw_cubic(float r, float h) {
-  const float q = r / h;
-  const float sig = 8.0f / (kPiF * h * h * h);
-  if (q < 0.5f) return sig * (-12.0f * q + 18.0f * q * q) / h;
-  if (q < 1.0f) { const float t = 1.0f - q; return sig * (-6.0f * t * t) / h; }
-  return 0.0f;
-}
-__device__ __forceinline__ float w_wendland(float r, float h) {
-  const float q = r / h;
-  if (q >= 1.0f) return 0.0f;
-  const float t = 1.0f - q;
-  return 21.0f / (2.0f * kPiF * h * h * h) * t * t * t * t * (1.0f + 4.0f * q);
-}
-__device__ __forceinline__ float dw_wendland(float r, float h) {
-  const float q = r / h;
-  if (q >= 1.0f) return 0.0f;
-  const float t = 1.0f - q;
-  return 21.0f / (2.0f * kPiF * h * h * h) * (-20.0f * q * t * t * t) / h;
-}
-// ∂W/∂h at fixed r (for the smoothing-length Newton step).
-__device__ __forceinline__ float dwdh_cubic(float r, float h) {
-  // W = σ(h) f(q), σ ∝ h⁻³, q = r/h  ⇒  ∂W/∂h = -(3W + q·∂W/∂q·σ)/h = -(3W + r·dW/dr)/h
-  return -(3.0f * w_cubic(r, h) + r * dw_cubic(r, h)) / h;
-}
-__device__ __forceinline__ float dwdh_wendland(float r, float h) {
-  return -(3.0f * w_wendland(r, h) + r * dw_wendland(r, h)) / h;
-}
+// ---- SPH kernels with support radius h: the reference's cubic spline (sph_step.wgsl:64-77) and Wendland C2 --
+// W(r, h) = σ(h) f(q) with q = r/h and σ = c/h³ (c = 8/π cubic, 21/(2π) Wendland C2), so
+// ∂W/∂r = σ f'(q)/h and ∂W/∂h = −(σ/h)(3f + q f'(q)) (the h-derivative drives the smoothing-length Newton step).
+// Evaluated from one reciprocal of h, every other term a product: the reference's per-call divisions
+// (q = r/h, σ = 8/(π h³), f'/h) give the same values to a few ulp at a quarter of the instructions, which is
+// what the gather kernels (density, smoothing-length solve, forces) spend per neighbour pair.
 template <int KERNEL>
-__device__ __forceinline__ float kern_w(float r, float h) { return KERNEL == 1 ? w_wendland(r, h) : w_cubic(r, h); }
-template <int KERNEL>
-__device__ __forceinline__ float kern_dw(float r, float h) { return KERNEL == 1 ? dw_wendland(r, h) : dw_cubic(r, h); }
-template <int KERNEL>
-__device__ __forceinline__ float kern_dwdh(float r, float h) {
-  return KERNEL == 1 ? dwdh_wendland(r, h) : dwdh_cubic(r, h);
+__device__ __forceinline__ void kern_pair(float r, float h, float& w, float& dwdr, float& dwdh) {
+  const float ih = __frcp_rn(h);
+  const float q = r * ih;
+  float f = 0.0f, fp = 0.0f;
+  if (KERNEL == 1) {
+    if (q < 1.0f) {
+      const float t = 1.0f - q, t3 = t * t * t;
+      f = t3 * t * (1.0f + 4.0f * q);
+      fp = -20.0f * q * t3;
+    }
+  } else if (q < 0.5f) {
+    f = 1.0f - 6.0f * q * q + 6.0f * q * q * q;
+    fp = -12.0f * q + 18.0f * q * q;
+  } else if (q < 1.0f) {
+    const float t = 1.0f - q;
+    f = 2.0f * t * t * t;
+    fp = -6.0f * t * t;
+  }
+  const float c = KERNEL == 1 ? 3.34225380f : 2.54647909f;  // 21/(2π), 8/π
+  const float sig = c * ih * ih * ih;
+  const float sih = sig * ih;
+  w = sig * f;
+  dwdr = sih * fp;
+  dwdh = -sih * (3.0f * f + q * fp);
 }
 
 // ---- Tillotson EOS in f32 (sph_step.wgsl:78-100), SI guards carried as parameters --------------------
