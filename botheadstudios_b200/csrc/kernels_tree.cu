@@ -3,8 +3,8 @@
 //
 // Reference: shaders/bh_gravity.wgsl (cs_bbox :68, cs_morton :100, cs_tree :135, cs_com :201) and the CPU
 // sort of crates/engine/src/gpu_gravity.rs:336-368. The sort order is (Morton code, original index), made
-// exact by sorting 64-bit keys code<<idbits | index, so the permutation, the leaf codes and the Karras
-// topology are bit-identical to the reference's. A batch of impacts prefixes the code with the impact
+// exact by a stable radix sort of the codes laid out in original-index order, so the permutation, the leaf
+// codes and the Karras topology are bit-identical to the reference's. A batch of impacts prefixes the code with the impact
 // (segment) index: every impact is quantised in its own box, sorted into its own contiguous range and
 // built into its own subtree, exactly as if it were alone.
 #include <cuda/atomic>
@@ -99,11 +99,12 @@ int launch_bbox(const Dev& d, cudaStream_t s) {
 
 // ---------------------------------------------------------------------------------------------------
 // Morton keys (cs_morton, bh_gravity.wgsl:91-108) with IEEE division, no contraction, each particle
-// quantised in its own segment's box. Sort key: (segment, code, original index), packed as
-// ((segment << 30 | code) << idbits) | index.
+// quantised in its own segment's box. The sort order is (segment, code, original index): each key
+// segment << 30 | code is written at its particle's original index, so a stable sort on the key alone leaves
+// equal keys in index order (30 + segment bits instead of 30 + segment + index bits: 4 passes, not 7, at 1M).
 // ---------------------------------------------------------------------------------------------------
 __global__ void k_keys(const float4* __restrict__ pos, const unsigned* __restrict__ id,
-                       const unsigned* __restrict__ seg, int n, const Seg* __restrict__ segs, int idbits,
+                       const unsigned* __restrict__ seg, int n, const Seg* __restrict__ segs,
                        unsigned long long* __restrict__ keys, unsigned* __restrict__ vals) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -127,8 +128,9 @@ __global__ void k_keys(const float4* __restrict__ pos, const unsigned* __restric
     q[k] = (unsigned)f;
   }
   const unsigned code = expand_bits(q[0]) * 4u + expand_bits(q[1]) * 2u + expand_bits(q[2]);
-  keys[i] = ((((unsigned long long)sg << 30) | code) << idbits) | (unsigned long long)id[i];
-  vals[i] = (unsigned)i;
+  const unsigned o = id[i];  // a permutation of [0, n)
+  keys[o] = ((unsigned long long)sg << 30) | code;
+  vals[o] = (unsigned)i;
 }
 
 // ---------------------------------------------------------------------------------------------------
@@ -287,7 +289,7 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_downsweep(const unsigned long
 // ---------------------------------------------------------------------------------------------------
 // Permutation of the particle state into the new order; leaf cluster codes (gpu_gravity.rs:366).
 // ---------------------------------------------------------------------------------------------------
-__global__ void k_permute(int n, int L, int idbits, const unsigned* __restrict__ order,
+__global__ void k_permute(int n, int L, const unsigned* __restrict__ order,
                           const unsigned long long* __restrict__ skeys, const unsigned* __restrict__ leaf_start,
                           State in, State out, float4* __restrict__ body,
                           unsigned long long* __restrict__ leaf_codes) {
@@ -307,7 +309,7 @@ __global__ void k_permute(int n, int L, int idbits, const unsigned* __restrict__
   out.id[t] = in.id[o];
   out.seg[t] = in.seg[o];
   body[t] = make_float4(p.x, p.y, p.z, m);
-  if (t < L) leaf_codes[t] = skeys[leaf_start[t]] >> idbits;
+  if (t < L) leaf_codes[t] = skeys[leaf_start[t]];
 }
 
 int launch_sort_permute(Dev& d, cudaStream_t s) {
@@ -315,9 +317,9 @@ int launch_sort_permute(Dev& d, cudaStream_t s) {
   const int threads = 256;
   const int blocks = (n + threads - 1) / threads;
   const State& in = d.st[d.cur];
-  k_keys<<<blocks, threads, 0, s>>>(in.pos_h, in.id, in.seg, n, d.segs, d.idbits, d.keys[0], d.vals[0]);
+  k_keys<<<blocks, threads, 0, s>>>(in.pos_h, in.id, in.seg, n, d.segs, d.keys[0], d.vals[0]);
   const int T = (int)radix_tiles(n);
-  const int total_bits = 30 + d.segbits + d.idbits;
+  const int total_bits = 30 + d.segbits;
   const int passes = (total_bits + 7) / 8;
   int src = 0;
   for (int shift = 0; shift < total_bits; shift += 8) {
@@ -329,7 +331,7 @@ int launch_sort_permute(Dev& d, cudaStream_t s) {
   }
   // vals[src] = old slot of each sorted position; keys[src] = sorted keys
   const State& out = d.st[d.cur ^ 1];
-  k_permute<<<blocks, threads, 0, s>>>(n, d.L, d.idbits, d.vals[src], d.keys[src], d.leaf_start, in, out, d.body,
+  k_permute<<<blocks, threads, 0, s>>>(n, d.L, d.vals[src], d.keys[src], d.leaf_start, in, out, d.body,
                                        d.leaf_codes);
   d.cur ^= 1;
   // keep the sorted keys in keys[0] for inspection

@@ -134,12 +134,6 @@ __global__ void k_noalloc_store(int n, const unsigned* __restrict__ id, const fl
   if (t < n) out[id[t]] = grav[t];
 }
 
-int bits_for_n(uint32_t n) {
-  int b = 1;
-  while (b < 32 && (1ull << b) < (unsigned long long)n) ++b;
-  return b;
-}
-
 }  // namespace
 }  // namespace sphb
 
@@ -166,7 +160,6 @@ extern "C" sph_status sph_gravity_tree_noalloc(const void* d_bodies4, uint32_t n
   d.n = (int)n;
   d.cur = 0;
   d.L = (int)((n + leaf_size - 1) / leaf_size);
-  d.idbits = bits_for_n(n);
   Cfg c;
   c.quad = (int)multipole;
   c.mac = SPH_MAC_GROUP;

@@ -289,7 +289,6 @@ sph_status upload_impl(sph_ctx* ctx, const SphParticle48* particles, const uint3
   d.cur = 0;
   d.nseg = nimp ? (int)nimp : 1;
   d.segbits = nimp > 1 ? bits_for(nimp) : 0;
-  d.idbits = bits_for(nu);
   // segment table: each impact's leaves are K-particle buckets from its first particle
   std::vector<Seg> table((size_t)d.nseg + 1);
   uint32_t L = 0;
@@ -799,7 +798,7 @@ sph_status sph_inspect(sph_ctx* ctx, uint32_t what, void* host_out, size_t bytes
       if (!need(n * 4)) return SPH_ERR_INVALID;
       std::vector<unsigned long long> k(n);
       CK(cudaMemcpy(k.data(), d.keys[0], n * 8, cudaMemcpyDeviceToHost));
-      for (size_t t = 0; t < n; ++t) ((unsigned*)host_out)[t] = (unsigned)(k[t] >> d.idbits) & 0x3fffffffu;
+      for (size_t t = 0; t < n; ++t) ((unsigned*)host_out)[t] = (unsigned)(k[t] & 0x3fffffffu);
       return SPH_OK;
     }
     case SPH_Q_IMPACT_DT:
@@ -964,7 +963,6 @@ sph_status sph_gravity(sph_ctx* ctx, const double* pos3, const double* mass, uin
   g.L = (int)((n + g.K - 1) / g.K);
   g.nseg = 1;
   g.segbits = 0;
-  g.idbits = bits_for(n);
   std::vector<float4> ph(n);
   std::vector<double> xs(n), ys(n), zs(n);
   std::vector<float> ms(n);
@@ -1200,7 +1198,6 @@ sph_status sph_dem_replace(sph_dem* dem, const SphGrain80* grains, uint32_t n) {
   d.L = n ? (int)((n + d.K - 1) / d.K) : 0;
   d.nseg = 1;
   d.segbits = 0;
-  d.idbits = bits_for(n);
   if (n) {
     CK(cudaMemcpyAsync(dem->grains, grains, (size_t)n * 80, cudaMemcpyHostToDevice, ctx->stream));
     launch_dem_load(d, dem->grains, ctx->stream);

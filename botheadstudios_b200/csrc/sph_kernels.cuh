@@ -105,7 +105,6 @@ struct Dev {
   int n = 0, cap = 0;
   int K = 1;        // leaf size
   int L = 0;        // number of leaves
-  int idbits = 1;   // bits of the particle index in the 64-bit sort key
   State st[2];
   int cur = 0;
   float4* body = nullptr;  // x, y, z, m in sorted order (gravity sources)
