@@ -17,6 +17,23 @@ __device__ __forceinline__ float pair_r(float4 a, float4 b) {
 }
 __device__ __forceinline__ float pair_h(float hi, float hj) { return fmul(0.5f, fadd(hi, hj)); }
 
+// The gather kernels walk a particle's list kGather entries at a time: all of a chunk's indices are loaded,
+// then all of its neighbour records, before any is used, so each thread keeps kGather gathers in flight
+// instead of one dependent chain. `lst` is the particle's first list slot (entries 32 apart, interleaved);
+// slots past the count read the particle itself (harmless filler, never summed).
+constexpr int kGather = 4;
+__device__ __forceinline__ void gather_pos_mass(const State& st, const unsigned* __restrict__ lst, unsigned k0,
+                                                unsigned c, unsigned self, float4 pj[kGather], float mj[kGather]) {
+  unsigned j[kGather];
+#pragma unroll
+  for (int u = 0; u < kGather; ++u) j[u] = k0 + u < c ? lst[(size_t)(k0 + u) * 32u] : self;
+#pragma unroll
+  for (int u = 0; u < kGather; ++u) {
+    pj[u] = st.pos_h[j[u]];
+    mj[u] = st.mass[j[u]];
+  }
+}
+
 // ---------------------------------------------------------------------------------------------------
 // Density (cs_density) with the EOS fused: rho_i = m_i W(0,h_i) + Σ m_j W(r, h_ij) over r < h_ij, then
 // P(rho,u), c(rho,u) and the per-particle force record (m, rho, P/rho², c). The reference re-evaluates P_j
@@ -43,14 +60,20 @@ __global__ void k_density_eos(int n, State st, const unsigned* __restrict__ nbr,
   kern_pair<KERNEL>(0.0f, pi.w, w, dwdr, dwdh);
   float r_i = m * w;
   const unsigned c = min(nbr_cnt[t], cap);
-  for (unsigned k = 0; k < c; ++k) {
-    const unsigned j = nbr[nbr_slot((unsigned)t, k, cap)];
-    const float4 pj = st.pos_h[j];
-    const float r = pair_r(pi, pj);
-    const float hij = pair_h(pi.w, pj.w);
-    if (r < hij) {
-      kern_pair<KERNEL>(r, hij, w, dwdr, dwdh);
-      r_i += st.mass[j] * w;
+  const unsigned* lst = nbr + nbr_slot((unsigned)t, 0u, cap);
+  for (unsigned k0 = 0; k0 < c; k0 += kGather) {
+    float4 pj[kGather];
+    float mj[kGather];
+    gather_pos_mass(st, lst, k0, c, (unsigned)t, pj, mj);
+#pragma unroll
+    for (int u = 0; u < kGather; ++u) {
+      if (k0 + u >= c) break;
+      const float r = pair_r(pi, pj[u]);
+      const float hij = pair_h(pi.w, pj[u].w);
+      if (r < hij) {
+        kern_pair<KERNEL>(r, hij, w, dwdr, dwdh);
+        r_i += mj[u] * w;
+      }
     }
   }
   rho[t] = r_i;
@@ -97,16 +120,21 @@ __device__ __forceinline__ void h_sums(int t, const State& st, const unsigned* _
   rho = m * w;
   drho = m * dwdh;
   const unsigned c = min(nbr_cnt[t], cap);
-  for (unsigned k = 0; k < c; ++k) {
-    const unsigned j = nbr[nbr_slot((unsigned)t, k, cap)];
-    const float4 pj = st.pos_h[j];
-    const float r = pair_r(pi, pj);
-    const float hij = pair_h(h, pj.w);
-    if (r < hij) {
-      const float mj = st.mass[j];
-      kern_pair<KERNEL>(r, hij, w, dwdr, dwdh);
-      rho += mj * w;
-      drho += mj * 0.5f * dwdh;
+  const unsigned* lst = nbr + nbr_slot((unsigned)t, 0u, cap);
+  for (unsigned k0 = 0; k0 < c; k0 += kGather) {
+    float4 pj[kGather];
+    float mj[kGather];
+    gather_pos_mass(st, lst, k0, c, (unsigned)t, pj, mj);
+#pragma unroll
+    for (int u = 0; u < kGather; ++u) {
+      if (k0 + u >= c) break;
+      const float r = pair_r(pi, pj[u]);
+      const float hij = pair_h(h, pj[u].w);
+      if (r < hij) {
+        kern_pair<KERNEL>(r, hij, w, dwdr, dwdh);
+        rho += mj[u] * w;
+        drho += mj[u] * 0.5f * dwdh;
+      }
     }
   }
 }
@@ -288,6 +316,8 @@ int launch_h_learned(const Dev& d, const Cfg& c, cudaStream_t s) {
 // :263-269) reduced to each impact's minimum with one atomic per warp (per lane in a warp that straddles two
 // impacts).
 // ---------------------------------------------------------------------------------------------------
+constexpr int kForceGather = 2;  // neighbours of a force chunk (three records each)
+
 template <int KERNEL, bool GRAV, bool DIVV>
 __global__ void k_forces(int n, State st, const float4* __restrict__ fdata, const unsigned* __restrict__ nbr,
                          const unsigned* __restrict__ nbr_cnt, unsigned cap, const float4* __restrict__ grav,
@@ -303,15 +333,29 @@ __global__ void k_forces(int n, State st, const float4* __restrict__ fdata, cons
     const float alpha = P->av_alpha, beta = P->av_beta, r_min = P->r_min;
     float ax = 0.f, ay = 0.f, az = 0.f, de = 0.f, dv = 0.f;
     const unsigned c = min(nbr_cnt[t], cap);
-    for (unsigned k = 0; k < c; ++k) {
-      const unsigned j = nbr[nbr_slot((unsigned)t, k, cap)];
-      const float4 pj = st.pos_h[j];
+    const unsigned* lst = nbr + nbr_slot((unsigned)t, 0u, cap);
+    for (unsigned k0 = 0; k0 < c; k0 += kForceGather) {
+      // a chunk's indices, then its positions, velocities and force records, all in flight together
+      unsigned jj[kForceGather];
+      float4 pjs[kForceGather], vjs[kForceGather], fjs[kForceGather];
+#pragma unroll
+      for (int u = 0; u < kForceGather; ++u) jj[u] = k0 + u < c ? lst[(size_t)(k0 + u) * 32u] : (unsigned)t;
+#pragma unroll
+      for (int u = 0; u < kForceGather; ++u) {
+        pjs[u] = st.pos_h[jj[u]];
+        vjs[u] = st.vel_u[jj[u]];
+        fjs[u] = fdata[jj[u]];
+      }
+#pragma unroll
+      for (int u = 0; u < kForceGather; ++u) {
+      if (k0 + u >= c) break;
+      const float4 pj = pjs[u];
       const float dx = fsub(pi.x, pj.x), dy = fsub(pi.y, pj.y), dz = fsub(pi.z, pj.z);
       const float r = fsqrt(dot3_exact(dx, dy, dz));
       const float hij = pair_h(pi.w, pj.w);
       if (!(r < hij && r > r_min)) continue;
-      const float4 vj = st.vel_u[j];
-      const float4 fj = fdata[j];
+      const float4 vj = vjs[u];
+      const float4 fj = fjs[u];
       const float vx = vi.x - vj.x, vy = vi.y - vj.y, vz = vi.z - vj.z;
       const float vr = vx * dx + vy * dy + vz * dz;
       float pij = 0.0f;
@@ -333,6 +377,7 @@ __global__ void k_forces(int n, State st, const float4* __restrict__ fdata, cons
       const float vg = vx * gx + vy * gy + vz * gz;
       de += 0.5f * fj.x * coeff * vg;
       if (DIVV) dv += fj.x * vg;
+      }
     }
     if (GRAV) {
       const float4 g = grav[t];
