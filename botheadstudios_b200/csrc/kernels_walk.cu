@@ -77,8 +77,8 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
   const unsigned lane = threadIdx.x & 31u;
   const int warp = blockIdx.x * W + w;
   if (warp >= (int)*ngroups) return;
-  // this warp's group: a maximal subtree of <= 32 particles of one impact (leaves g.x..g.y); the walk starts
-  // at that impact's root
+  // this warp's group: a run of <= 32 Morton-consecutive particles of one impact (leaves g.x..g.y); the walk
+  // starts at that impact's root
   const uint2 grp = groups[warp];
   const int s0 = (int)leaf_start[grp.x], s1 = (int)leaf_start[grp.y + 1];
   const Seg& sgr = segs[(unsigned)(leaf_codes[grp.x] >> 30)];

@@ -33,7 +33,7 @@ struct Seg {
   unsigned sig_bits;    // atomicMin target: bits of the segment's minimum Courant signal
   unsigned bbox[6];     // order-preserving keys of lo.xyz, hi.xyz (bh_gravity.wgsl:49-57)
   float soft2;          // softening² of this impact
-  unsigned pad;
+  unsigned pad;         // first walk group of the impact
   double dt;            // dt of the current step
   double time;          // simulated time
 };
@@ -127,7 +127,7 @@ struct Dev {
   float4* nbmax = nullptr;      // [2L-1] bmax.xyz, opening radius
   float4* nq0 = nullptr;        // [2L-1] Qxx, Qyy, Qzz, Qxy
   float4* nq1 = nullptr;        // [2L-1] Qxz, Qyz, 0, 0
-  uint2* groups = nullptr;      // [L] walk groups: (first leaf, last leaf) of maximal subtrees with <= 32 particles
+  uint2* groups = nullptr;      // [L] walk groups: (first leaf, last leaf) of runs of 32/K leaves of one impact
   unsigned* ngroups = nullptr;  // [1] number of groups
   unsigned* nbr = nullptr;      // interleaved neighbour lists [n/32][nbr_cap][32]
   unsigned* nbr_cnt = nullptr;  // [n]
