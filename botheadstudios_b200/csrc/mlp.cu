@@ -1,8 +1,9 @@
 // Learned smoothing-length MLP on the tensor cores: 8 → 64 → 64 → 1 with GELU, BF16 operands and FP32
-// accumulation through mma.sync.m16n8k16 tiles. A CTA of 4 warps holds 128 rows (particles or training
-// samples); each warp owns 32 rows (two 16-row MMA tiles) and runs them through both hidden layers without
-// leaving shared memory. Training runs the backward pass on the same tiles (weight gradients as GEMMs over
-// the CTA's samples) and Adam on an FP32 master copy.
+// accumulation. Inference (the in-step proposal and the standalone forward) runs on tcgen05: the two hidden
+// layers are M = 128 × N = 64 tcgen05.mma tiles with the accumulators in tensor memory (see the inference
+// section). Training uses mma.sync.m16n8k16 tiles: a CTA of 4 warps holds 128 samples, each warp owns 32 rows
+// (two 16-row MMA tiles) through both hidden layers, and the backward pass computes the weight gradients as
+// GEMMs over the CTA's samples; Adam updates an FP32 master copy.
 //
 // Fragment layouts of m16n8k16 (row.col): lane = 4·g + q. A (16×16, row-major): a0 = (g, 2q..2q+1),
 // a1 = (g+8, 2q..), a2 = (g, 8+2q..), a3 = (g+8, 8+2q..). B (16×8, K×N): b0 = (k 2q..2q+1, n g),
@@ -172,34 +173,213 @@ __device__ __forceinline__ void features(int t, const State& st, const float* __
   f[7] = P->progress;                                                          // step fraction
 }
 
+// ---- inference on the 5th-generation tensor cores (tcgen05) ---------------------------------------------
+// A CTA of 128 threads holds 128 rows. Each thread writes its row of x' (layer 1) or of a1 (layer 2) into
+// shared memory in the canonical no-swizzle K-major layout (8-row × 16-byte core matrices; core matrices
+// adjacent along K are 128 B apart, 8-row groups K·16 B apart); one thread issues tcgen05.mma (BF16 × BF16 →
+// FP32, M = 128, N = 64, K = 16 per instruction) with the weights as the K-major B operand, and commits to an
+// mbarrier. The accumulators live in tensor memory: row r of D is TMEM lane r, so after the barrier every
+// thread reads its own row (tcgen05.ld 32x32b) and applies bias, GELU and the next layer's input rounding,
+// and the 64 → 1 output layer is a per-thread dot product. Every barrier wait is bounded: on a timeout the
+// CTA stops issuing, raises an error flag, waits (bounded) for what it issued and frees its tensor memory.
+constexpr int TC_COLS = 128;            // TMEM columns per CTA: D1 [0, 64), D2 [64, 128)
+constexpr int TC_SMEM = 56 * 1024;      // dynamic shared memory per CTA: at most 4 CTAs (4 × 128 of 512 columns)
+constexpr unsigned kTcSpin = 1u << 16;  // barrier polls before giving up
+constexpr uint32_t kTcIdesc = (1u << 4)            // D: FP32
+                              | (1u << 7)          // A: BF16
+                              | (1u << 10)         // B: BF16 (A and B K-major: bits 15, 16 clear)
+                              | ((64u >> 3) << 17) // N = 64
+                              | ((128u >> 4) << 24);  // M = 128
+
+struct TcSmem {
+  __nv_bfloat16 a1[ROWS * 16];      // x' rows (K = 16, inputs 8..15 zero)
+  __nv_bfloat16 a2[ROWS * MLP_H];   // a1 rows (K = 64)
+  __nv_bfloat16 w1[MLP_H * 16];     // W1ᵀ [out][in] (K = 16)
+  __nv_bfloat16 w2[MLP_H * MLP_H];  // W2ᵀ [out][in] (K = 64)
+  float b1[MLP_H], b2[MLP_H], w3[MLP_H];
+  unsigned long long mbar;
+  unsigned tmem;
+  int ok;
+};
+static_assert(sizeof(TcSmem) <= TC_SMEM, "tcgen05 tile fits its shared memory");
+
+// element offset of (row r, k) in a K-major no-swizzle operand with K columns
+__device__ __forceinline__ int cm(int r, int k, int K) { return (r >> 3) * (K * 8) + (k >> 3) * 64 + (r & 7) * 8 + (k & 7); }
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+// shared-memory matrix descriptor: start, leading (K) and stride (8-row) byte offsets, sm100 version bits, no swizzle
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((saddr & 0x3FFFFu) >> 4) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+__device__ __forceinline__ void tc_mma(uint32_t d, uint64_t a, uint64_t b, uint32_t acc) {
+  asm volatile("{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
+               "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n"
+               :: "r"(d), "l"(a), "l"(b), "r"(kTcIdesc), "r"(acc) : "memory");
+}
+__device__ __forceinline__ void tc_commit(uint32_t mbar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" :: "r"(mbar) : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
+  for (unsigned i = 0; i < kTcSpin; ++i) {
+    uint32_t done;
+    asm volatile("{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\nselp.u32 %0, 1, 0, p;\n}\n"
+                 : "=r"(done) : "r"(mbar), "r"(parity) : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+// 16 consecutive FP32 columns of this warp's 32 TMEM lanes (one per thread)
+__device__ __forceinline__ void tc_ld16(uint32_t taddr, float v[16]) {
+  uint32_t r[16];
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                 "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+               : "r"(taddr));
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+__device__ __forceinline__ void tc_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ uint4 pack8(const float f[8]) {
+  __nv_bfloat162 h[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) h[i] = __floats2bfloat162_rn(f[2 * i], f[2 * i + 1]);
+  return *reinterpret_cast<uint4*>(h);
+}
+
+// CTA set-up: tensor memory, the barrier, the weights in the operand layout.
+__device__ void tc_setup(TcSmem& S, const MlpPacked* __restrict__ W) {
+  for (int i = threadIdx.x; i < MLP_H * 16; i += ROWS) S.w1[cm(i >> 4, i & 15, 16)] = W->w1t[i];
+  for (int i = threadIdx.x; i < MLP_H * MLP_H; i += ROWS) S.w2[cm(i >> 6, i & 63, 64)] = W->w2t[i];
+  for (int i = threadIdx.x; i < MLP_H; i += ROWS) {
+    S.b1[i] = W->b1[i];
+    S.b2[i] = W->b2[i];
+    S.w3[i] = W->w3[i];
+  }
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&S.mbar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    S.ok = 1;
+  }
+  if (threadIdx.x < 32) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                 :: "r"(smem_u32(&S.tmem)), "r"(TC_COLS) : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  fence_async_smem();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+}
+
+// One 128-row tile: this thread's normalised inputs in, its y (before b3) out (NaN after a barrier timeout).
+__device__ float tc_tile(TcSmem& S, const float xq[MLP_IN], uint32_t& phase) {
+  const int r = threadIdx.x, w = r >> 5;
+  const uint32_t mbar = smem_u32(&S.mbar);
+  const uint32_t trow = S.tmem + ((uint32_t)(w * 32) << 16);
+  const float zero8[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  *reinterpret_cast<uint4*>(S.a1 + cm(r, 0, 16)) = pack8(xq);
+  *reinterpret_cast<uint4*>(S.a1 + cm(r, 8, 16)) = pack8(zero8);
+  fence_async_smem();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (!S.ok) return __int_as_float(0x7fc00000);
+  if (r == 0) {
+    tc_mma(S.tmem, umma_desc(smem_u32(S.a1), 128, 256), umma_desc(smem_u32(S.w1), 128, 256), 0u);
+    tc_commit(mbar);
+  }
+  // on a timeout `phase` keeps the parity of the commit still outstanding, for the tear-down to wait on
+  bool got = mbar_wait(mbar, phase);
+  if (!__syncthreads_and(got)) {
+    if (r == 0) S.ok = 0;
+    return __int_as_float(0x7fc00000);
+  }
+  phase ^= 1u;
+  tc_fence_after();
+  // layer 1 → GELU → a1 (bf16) row
+  float z[64];
+#pragma unroll
+  for (int c = 0; c < 4; ++c) tc_ld16(trow + 16 * c, z + 16 * c);
+  tc_wait_ld();
+#pragma unroll
+  for (int kb = 0; kb < 8; ++kb) {
+    float h[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) h[i] = gelu(z[8 * kb + i] + S.b1[8 * kb + i]);
+    *reinterpret_cast<uint4*>(S.a2 + cm(r, 8 * kb, 64)) = pack8(h);
+  }
+  fence_async_smem();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (r == 0) {
+#pragma unroll
+    for (int kt = 0; kt < 4; ++kt)
+      tc_mma(S.tmem + 64, umma_desc(smem_u32(S.a2) + 256 * kt, 128, 1024), umma_desc(smem_u32(S.w2) + 256 * kt, 128, 1024),
+             kt > 0 ? 1u : 0u);
+    tc_commit(mbar);
+  }
+  got = mbar_wait(mbar, phase);
+  if (!__syncthreads_and(got)) {
+    if (r == 0) S.ok = 0;
+    return __int_as_float(0x7fc00000);
+  }
+  phase ^= 1u;
+  tc_fence_after();
+#pragma unroll
+  for (int c = 0; c < 4; ++c) tc_ld16(trow + 64 + 16 * c, z + 16 * c);
+  tc_wait_ld();
+  float y = 0.0f;
+#pragma unroll
+  for (int j = 0; j < MLP_H; ++j) y += gelu(z[j] + S.b2[j]) * S.w3[j];
+  tc_fence_before();
+  return y;
+}
+
+// CTA tear-down: after a timeout, wait (bounded) for the last commit; then free the tensor memory.
+__device__ bool tc_teardown(TcSmem& S, uint32_t phase) {
+  const bool failed = !S.ok;
+  if (failed) mbar_wait(smem_u32(&S.mbar), phase);  // what was issued before the timeout, if anything
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (threadIdx.x < 32)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(S.tmem), "r"(TC_COLS) : "memory");
+  return !failed;
+}
+
+__device__ __forceinline__ void normalise(const float f[MLP_IN], const MlpPacked* W, float xq[MLP_IN]) {
+#pragma unroll
+  for (int k = 0; k < MLP_IN; ++k) xq[k] = (f[k] - W->xm[k]) * W->xs[k];
+}
+
 __global__ void __launch_bounds__(ROWS) k_mlp_propose(int n, State st, const float* __restrict__ rho,
                                                      const unsigned* __restrict__ cnt,
                                                      const float4* __restrict__ acc,
                                                      const float4* __restrict__ fdata,
                                                      const float* __restrict__ divv, const Eos* __restrict__ eos,
-                                                     const Seg* __restrict__ segs,
-                                                     const DevParams* __restrict__ P, MlpFeatureArgs fa,
-                                                     const MlpPacked* __restrict__ W, float* __restrict__ rec,
-                                                     float* __restrict__ dh, int apply) {
-  __shared__ __align__(16) FwdW w;
-  __shared__ __align__(16) __nv_bfloat16 sx[ROWS * XS];
-  __shared__ __align__(16) __nv_bfloat16 sh1[ROWS * HS];
-  __shared__ float sy[ROWS];
-  load_fwd(W, w);
+                                                     const Seg* __restrict__ segs, DevParams* __restrict__ P,
+                                                     MlpFeatureArgs fa, const MlpPacked* __restrict__ W,
+                                                     float* __restrict__ rec, float* __restrict__ dh, int apply) {
+  extern __shared__ __align__(1024) unsigned char tc_raw[];
+  TcSmem& S = *reinterpret_cast<TcSmem*>(tc_raw);
+  tc_setup(S, W);
   const float b3 = W->b3, ym = W->ym, ys = W->ys;
-  __syncthreads();
-  const int r = threadIdx.x, r0 = (threadIdx.x >> 5) * 32;
+  uint32_t phase = 0;
+  const int r = threadIdx.x;
   for (int base = blockIdx.x * ROWS; base < n; base += gridDim.x * ROWS) {
     const int t = base + r;
-    float f[MLP_IN] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    float f[MLP_IN] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, xq[MLP_IN];
     if (t < n) features(t, st, rho, cnt, acc, fdata, divv, eos, segs, P, fa, f);
-    put_row(sx, r, f, W);
-    __syncwarp();
-    mlp_rows(r0, sx, sh1, w, sy, nullptr, nullptr, nullptr);
+    normalise(f, W, xq);
+    const float y = tc_tile(S, xq, phase);
     if (t < n) {
       // the network gives log(h_next / h(rho)); the step from the current h subtracts log(h / h(rho)) = f[0],
       // so a residual left by the previous solve is corrected whatever the network learned
-      const float d = (sy[r] + b3) * ys + ym - f[0];
+      const float d = (y + b3) * ys + ym - f[0];
       const float dc = d == d ? fminf(fmaxf(d, -kMaxStep), kMaxStep) : 0.0f;  // no proposal from a NaN
       if (apply) st.pos_h[t].w = st.pos_h[t].w * expf(dc);
       if (rec) {
@@ -209,31 +389,28 @@ __global__ void __launch_bounds__(ROWS) k_mlp_propose(int n, State st, const flo
         dh[id] = d;
       }
     }
-    __syncwarp();
   }
+  if (!tc_teardown(S, phase) && threadIdx.x == 0) atomicOr(&P->flags, kFlagTensorTimeout);
 }
 
 __global__ void __launch_bounds__(ROWS) k_mlp_forward(const MlpPacked* __restrict__ W, const float* __restrict__ x,
-                                                     int n, float* __restrict__ out) {
-  __shared__ __align__(16) FwdW w;
-  __shared__ __align__(16) __nv_bfloat16 sx[ROWS * XS];
-  __shared__ __align__(16) __nv_bfloat16 sh1[ROWS * HS];
-  __shared__ float sy[ROWS];
-  load_fwd(W, w);
-  __syncthreads();
-  const int r = threadIdx.x, r0 = (threadIdx.x >> 5) * 32;
+                                                     int n, float* __restrict__ out, unsigned* __restrict__ err) {
+  extern __shared__ __align__(1024) unsigned char tc_raw[];
+  TcSmem& S = *reinterpret_cast<TcSmem*>(tc_raw);
+  tc_setup(S, W);
+  uint32_t phase = 0;
+  const int r = threadIdx.x;
   for (int base = blockIdx.x * ROWS; base < n; base += gridDim.x * ROWS) {
     const int t = base + r;
-    float f[MLP_IN] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    float f[MLP_IN] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, xq[MLP_IN];
     if (t < n)
 #pragma unroll
       for (int k = 0; k < MLP_IN; ++k) f[k] = x[(size_t)t * MLP_IN + k];
-    put_row(sx, r, f, W);
-    __syncwarp();
-    mlp_rows(r0, sx, sh1, w, sy, nullptr, nullptr, nullptr);
-    if (t < n) out[t] = (sy[r] + W->b3) * W->ys + W->ym;
-    __syncwarp();
+    normalise(f, W, xq);
+    const float y = tc_tile(S, xq, phase);
+    if (t < n) out[t] = (y + W->b3) * W->ys + W->ym;
   }
+  if (!tc_teardown(S, phase) && threadIdx.x == 0) atomicOr(err, 1u);
 }
 
 // ---- training: forward + backward of one 128-sample tile ----------------------------------------------
@@ -448,17 +625,27 @@ int launch_mlp_pack(const float* params, MlpPacked* out, cudaStream_t s) {
 
 int launch_mlp_propose(const Dev& d, const MlpPacked* w, const MlpFeatureArgs& fa, const float* divv, float* rec,
                        float* dh, bool apply, cudaStream_t s) {
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_mlp_propose, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM);
+    attr = true;
+  }
   const int tiles = (d.n + ROWS - 1) / ROWS;
   const int grid = tiles < propose_grid() ? tiles : propose_grid();
-  k_mlp_propose<<<grid, ROWS, 0, s>>>(d.n, d.s(), d.rho, d.nbr_cnt, d.acc, d.fdata, divv, d.eos, d.segs, d.P, fa,
+  k_mlp_propose<<<grid, ROWS, TC_SMEM, s>>>(d.n, d.s(), d.rho, d.nbr_cnt, d.acc, d.fdata, divv, d.eos, d.segs, d.P, fa,
                                       w, rec, dh, apply ? 1 : 0);
   return 1;
 }
 
-int launch_mlp_forward(const MlpPacked* w, const float* x, int n, float* out, cudaStream_t s) {
+int launch_mlp_forward(const MlpPacked* w, const float* x, int n, float* out, unsigned* err, cudaStream_t s) {
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM);
+    attr = true;
+  }
   const int tiles = (n + ROWS - 1) / ROWS;
   const int grid = tiles < propose_grid() ? tiles : propose_grid();
-  k_mlp_forward<<<grid, ROWS, 0, s>>>(w, x, n, out);
+  k_mlp_forward<<<grid, ROWS, TC_SMEM, s>>>(w, x, n, out, err);
   return 1;
 }
 
@@ -526,14 +713,19 @@ sph_status sph_mlp_forward(const float* params, const float* x, uint32_t n, floa
   MlpPacked* w = b.get<MlpPacked>(1);
   float* dx = b.get<float>((size_t)n * MLP_IN);
   float* dy = b.get<float>(n);
+  unsigned* flag = b.get<unsigned>(1);
   if (b.err != cudaSuccess) return status_of(b.err);
   cudaError_t e = cudaMemcpy(dp, params, MLP_TOTAL * sizeof(float), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(dx, x, (size_t)n * MLP_IN * sizeof(float), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemset(flag, 0, sizeof(unsigned));
   if (e != cudaSuccess) return status_of(e);
   launch_mlp_pack(dp, w, 0);
-  launch_mlp_forward(w, dx, (int)n, dy, 0);
+  launch_mlp_forward(w, dx, (int)n, dy, flag, 0);
   e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaMemcpy(out, dy, (size_t)n * sizeof(float), cudaMemcpyDeviceToHost);
+  unsigned timeout = 0;
+  if (e == cudaSuccess) e = cudaMemcpy(&timeout, flag, sizeof(unsigned), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess && timeout) return SPH_ERR_TIMEOUT;
   return status_of(e);
 }
 

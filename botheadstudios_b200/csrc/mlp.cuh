@@ -45,8 +45,9 @@ struct MlpFeatureArgs {
 int launch_mlp_propose(const Dev& d, const MlpPacked* w, const MlpFeatureArgs& fa, const float* divv,
                        float* rec, float* dh, bool apply, cudaStream_t s);
 
-// Standalone forward over feature rows x[n][8] → de-normalised outputs.
-int launch_mlp_forward(const MlpPacked* w, const float* x, int n, float* out, cudaStream_t s);
+// Standalone forward over feature rows x[n][8] → de-normalised outputs; *err |= 1 if a tensor-core barrier
+// wait gave up (the outputs are then NaN).
+int launch_mlp_forward(const MlpPacked* w, const float* x, int n, float* out, unsigned* err, cudaStream_t s);
 
 // One training minibatch: forward + backward over rows idx[0..m) of (x, t), gradients of the mean squared
 // error on the normalised target (divided by `denom`) accumulated into grad[4801], the summed squared error

@@ -14,7 +14,7 @@ constexpr int kTravStack = 64;      // bh_gravity.wgsl:336 MAX_STACK
 constexpr float kPiF = 3.14159265359f;  // sph_step.wgsl:20
 
 // Device-side error/overflow flags (bit set, never cleared by kernels).
-enum : unsigned { kFlagNbrOverflow = 1u, kFlagStackOverflow = 2u, kFlagCandOverflow = 4u };
+enum : unsigned { kFlagNbrOverflow = 1u, kFlagStackOverflow = 2u, kFlagCandOverflow = 4u, kFlagTensorTimeout = 8u };
 
 // Material row as in SphEos48 (Tillotson, 12 floats).
 struct Eos {
