@@ -9,6 +9,7 @@ the iteration would. In SPH_H_LEARNED the solver checks every proposal's density
 the rejected particles, so a poor proposal costs iterations, never accuracy.
 
     python -m botheadstudios_b200.learned_h train [--out FILE]    # collect, train, save (needs a GPU)
+    python -m botheadstudios_b200.learned_h eval                  # held-out comparison with plain Newton
 """
 from __future__ import annotations
 
@@ -185,12 +186,53 @@ def load(path: str = DEFAULT_PATH) -> np.ndarray:
     return p
 
 
+def evaluate(I, params=None, mode: str = "learned", steps: int = 6, h_iters: int = 2, device: int = -1) -> dict:
+    """One held-out run: 2 steps to settle, then `steps` timed KDK steps; first-pass acceptance, residual,
+    smoothing-length phase time per rebuild, and the final densities' error against an 8-iteration solve on the
+    same positions."""
+    from .gpusph import GpuSph
+    with GpuSph(len(I.particles), device=device, **solver_config(I.units, h_mode=mode, h_iters=h_iters)) as s:
+        if params is not None:
+            s.mlp_set(params)
+        s.upload(I.particles, I.eos, I.softening)
+        s.encode_kdk(2)
+        s.sync()
+        acc, res = [], []
+        s.profile_enable(True)
+        for k in range(steps):
+            s.set_progress(k / steps)
+            s.encode_kdk(1)
+            d = s.diag()
+            acc.append(d["h_accepted"] / len(I.particles))
+            res.append(d["h_residual"])
+        pr = s.profile_read()
+        out = s.readback()
+    with GpuSph(len(I.particles), device=device, **solver_config(I.units, h_mode="solve", h_iters=8)) as s:
+        s.upload(out, I.eos, I.softening)
+        s.eval_forces()
+        rho_conv = s.inspect("RHO")
+    e = np.abs(out["rho"] / rho_conv - 1.0)
+    return dict(accepted=float(np.mean(acc)), residual=float(max(res)), hsolve_ms_per_step=pr["ms"]["hsolve"] / steps,
+                step_ms=sum(pr["ms"].values()) / steps, density_rms=float(np.sqrt(np.mean(e * e))),
+                density_max=float(e.max()))
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("cmd", choices=["train"])
+    ap.add_argument("cmd", choices=["train", "eval"])
     ap.add_argument("--out", default=DEFAULT_PATH)
     ap.add_argument("--quick", action="store_true")
     a = ap.parse_args(argv)
+    if a.cmd == "eval":
+        # held-out impacts (the network saw the 10,240-particle impact and the planet)
+        import json
+        p = load()
+        for nt, ni, seed in ((30_000, 3_000, 77), (953_250, 95_326, 79)):
+            I = ic.impact(nt, ni, n_ngb=64.0, seed=seed)
+            rows = dict(trained=evaluate(I, p), zero_network=evaluate(I, None),
+                        newton2=evaluate(I, None, mode="solve"), newton1=evaluate(I, None, mode="solve", h_iters=1))
+            print(json.dumps(dict(particles=nt + ni, **rows)), flush=True)
+        return
     X, T = training_set(quick=a.quick)
     p, losses = fit(X, T, schedule=((5, 2e-3),) if a.quick else SCHEDULE)
     save(p, a.out, losses=losses, rows=len(X))
