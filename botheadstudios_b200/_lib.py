@@ -45,7 +45,8 @@ class SphConfig(C.Structure):
                 ("h_iters", C.c_uint32), ("max_neighbours", C.c_uint32), ("cfl", C.c_float),
                 ("rho_floor", C.c_float), ("du_floor", C.c_float), ("r_min", C.c_float), ("sig_floor", C.c_float),
                 ("device", C.c_int32), ("mac", C.c_uint32), ("graph", C.c_uint32),
-                ("block_threads", C.c_uint32), ("walk_warps", C.c_uint32), ("reserved", C.c_uint32 * 3)]
+                ("block_threads", C.c_uint32), ("walk_warps", C.c_uint32), ("h_skin", C.c_float),
+                ("reserved", C.c_uint32 * 2)]
 
 
 class SphDiag(C.Structure):

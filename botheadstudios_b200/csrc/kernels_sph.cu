@@ -161,17 +161,18 @@ __device__ __forceinline__ float h_newton(float h, float m, float rho, float drh
 
 template <int KERNEL>
 __global__ void k_h_iter(int n, State st, const unsigned* __restrict__ nbr, const unsigned* __restrict__ nbr_cnt,
-                         unsigned cap, const float* __restrict__ h0, float eta, float skin, DevParams* P,
+                         unsigned cap, const float* __restrict__ h0, float eta, DevParams* P, Seg* __restrict__ segs,
                          float* __restrict__ hnew, int last, const Eos* __restrict__ eos, float* __restrict__ rho_out,
                          float4* __restrict__ fdata) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   float res = 0.0f;
+  const unsigned sg = t < n ? st.seg[t] : kNoSeg;
   if (t < n) {
     float rho, drho;
     h_sums<KERNEL>(t, st, nbr, nbr_cnt, cap, rho, drho);
     const float m = st.mass[t], h = st.pos_h[t].w;
     float drel;
-    float hn = h_newton(h, m, rho, drho, eta, h0[t], skin, res, drel);
+    float hn = h_newton(h, m, rho, drho, eta, h0[t], segs[sg].skin, res, drel);
     if (last) {
       // the final pass is the density pass: same sum, same order as k_density_eos
       rho_out[t] = rho;
@@ -180,8 +181,7 @@ __global__ void k_h_iter(int n, State st, const unsigned* __restrict__ nbr, cons
     }
     hnew[t] = hn;
   }
-  const float wres = warp_max(res);
-  if ((threadIdx.x & 31) == 0) atomicMax(&P->h_residual_bits, __float_as_uint(wres));
+  seg_res_max(segs, sg, res);
 }
 
 constexpr float kDensityTolFraction = 0.25f;
@@ -192,53 +192,53 @@ constexpr float kDensityTolFraction = 0.25f;
 template <int KERNEL>
 __global__ void k_h_check(int n, const unsigned* __restrict__ list, const unsigned* __restrict__ list_n, State st,
                           const unsigned* __restrict__ nbr, const unsigned* __restrict__ nbr_cnt, unsigned cap,
-                          const float* __restrict__ h0, float eta, float skin, float tol, DevParams* P,
+                          const float* __restrict__ h0, float eta, float tol, DevParams* P, Seg* __restrict__ segs,
                           float* __restrict__ hnew, unsigned* __restrict__ next, unsigned* __restrict__ next_n,
                           int last, const Eos* __restrict__ eos, float* __restrict__ rho_out,
                           float4* __restrict__ fdata) {
   const int count = list ? (int)*list_n : n;
   const int lane = threadIdx.x & 31;
-  float wres = 0.0f;
   unsigned acc = 0;
-  // whole warps step together (the append below is warp-aggregated)
+  // whole warps step together (the append and the residual maximum below are warp-collective)
   for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < count; base += gridDim.x * blockDim.x) {
     const int i = base + lane;
     bool pend = false;
     int t = -1;
+    unsigned sg = kNoSeg;
+    float fres = 0.0f;
     if (i < count) {
       t = list ? (int)list[i] : i;
       float rho, drho, res, drel;
       h_sums<KERNEL>(t, st, nbr, nbr_cnt, cap, rho, drho);
       const float m = st.mass[t], h = st.pos_h[t].w;
-      const float hn = h_newton(h, m, rho, drho, eta, h0[t], skin, res, drel);
+      const unsigned s = st.seg[t];
+      const float hn = h_newton(h, m, rho, drho, eta, h0[t], segs[s].skin, res, drel);
       // accepted: residual within tolerance and a density that one more step would move by < tol/4 (near a
       // surface ρ depends strongly on h, and a small residual alone can leave a larger density error)
       if ((res <= tol && drel <= kDensityTolFraction * tol) || last) {
         rho_out[t] = rho;
         fdata[t] = eos_record(eos, st.mat[t], m, rho, st.vel_u[t].w, P);
-        wres = fmaxf(wres, res);
+        sg = s;
+        fres = res;
         if (!list && res <= tol) ++acc;
       } else {
         hnew[t] = hn;
         pend = true;
       }
     }
+    seg_res_max(segs, sg, fres);
     const unsigned bal = __ballot_sync(SPH_FULL_MASK, pend);
     unsigned at = 0;
     if (lane == 0 && bal) at = atomicAdd(next_n, (unsigned)__popc(bal));
     at = __shfl_sync(SPH_FULL_MASK, at, 0);
     if (pend) next[at + __popc(bal & ((1u << lane) - 1u))] = (unsigned)t;
   }
-  wres = warp_max(wres);
   acc += __shfl_xor_sync(SPH_FULL_MASK, acc, 16);
   acc += __shfl_xor_sync(SPH_FULL_MASK, acc, 8);
   acc += __shfl_xor_sync(SPH_FULL_MASK, acc, 4);
   acc += __shfl_xor_sync(SPH_FULL_MASK, acc, 2);
   acc += __shfl_xor_sync(SPH_FULL_MASK, acc, 1);
-  if (lane == 0) {
-    atomicMax(&P->h_residual_bits, __float_as_uint(wres));
-    if (acc) atomicAdd(&P->h_accepted, acc);
-  }
+  if (lane == 0 && acc) atomicAdd(&P->h_accepted, acc);
 }
 
 __global__ void k_h_commit_list(const unsigned* __restrict__ list, const unsigned* __restrict__ list_n, State st,
@@ -254,27 +254,46 @@ __global__ void k_h_commit(int n, State st, const float* __restrict__ hnew) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t < n) st.pos_h[t].w = hnew[t];
 }
-__global__ void k_h_reset(DevParams* P, int iters) {
-  P->h_residual_bits = 0u;
-  P->h_iters_used = (unsigned)iters;
-  P->h_accepted = 0u;
+__global__ void k_h_reset(DevParams* P, Seg* segs, int nseg, int iters) {
+  if (threadIdx.x < nseg) segs[threadIdx.x].res_bits = 0u;
+  if (threadIdx.x == 0) {
+    P->h_iters_used = (unsigned)iters;
+    P->h_accepted = 0u;
+  }
 }
-__global__ void k_h_publish(DevParams* P) { P->h_residual = __uint_as_float(P->h_residual_bits); }
+// The solve's residual maximum (over all impacts); and each impact's next skin: wide while some particle of it
+// is still far from its smoothing length (right after an upload, or a shock), narrow once every one is near it.
+__global__ void k_h_publish(DevParams* P, Seg* segs, int nseg) {
+  __shared__ float s_max[kMaxSegments / 32];
+  float r = 0.0f;
+  if (threadIdx.x < nseg) {
+    r = __uint_as_float(segs[threadIdx.x].res_bits);
+    segs[threadIdx.x].skin = r > P->skin_reset ? P->skin_wide : P->skin_narrow;
+  }
+  r = warp_max(r);
+  if ((threadIdx.x & 31) == 0) s_max[threadIdx.x >> 5] = r;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float m = 0.0f;
+    for (int k = 0; k < kMaxSegments / 32; ++k) m = fmaxf(m, s_max[k]);
+    P->h_residual = m;
+  }
+}
 
 int launch_h_solve(const Dev& d, const Cfg& c, cudaStream_t s) {
   const int blocks = (d.n + c.blk - 1) / c.blk;
   for (int it = 0; it <= c.h_iters; ++it) {
     const int last = it == c.h_iters;
-    k_h_reset<<<1, 1, 0, s>>>(d.P, c.h_iters);
+    k_h_reset<<<1, kMaxSegments, 0, s>>>(d.P, d.segs, d.nseg, c.h_iters);
     if (c.kernel == 1)
-      k_h_iter<1><<<blocks, c.blk, 0, s>>>(d.n, d.s(), d.nbr, d.nbr_cnt, d.nbr_cap, d.h0, c.h_eta, c.skin, d.P, d.hnew,
+      k_h_iter<1><<<blocks, c.blk, 0, s>>>(d.n, d.s(), d.nbr, d.nbr_cnt, d.nbr_cap, d.h0, c.h_eta, d.P, d.segs, d.hnew,
                                           last, d.eos, d.rho, d.fdata);
     else
-      k_h_iter<0><<<blocks, c.blk, 0, s>>>(d.n, d.s(), d.nbr, d.nbr_cnt, d.nbr_cap, d.h0, c.h_eta, c.skin, d.P, d.hnew,
+      k_h_iter<0><<<blocks, c.blk, 0, s>>>(d.n, d.s(), d.nbr, d.nbr_cnt, d.nbr_cap, d.h0, c.h_eta, d.P, d.segs, d.hnew,
                                           last, d.eos, d.rho, d.fdata);
     if (!last) k_h_commit<<<blocks, c.blk, 0, s>>>(d.n, d.s(), d.hnew);
   }
-  k_h_publish<<<1, 1, 0, s>>>(d.P);
+  k_h_publish<<<1, kMaxSegments, 0, s>>>(d.P, d.segs, d.nseg);
   return (c.h_iters + 1) * 2 + c.h_iters + 1;
 }
 
@@ -284,11 +303,11 @@ int launch_h_solve(const Dev& d, const Cfg& c, cudaStream_t s) {
 int launch_h_learned(const Dev& d, const Cfg& c, cudaStream_t s) {
   const int full = (d.n + c.blk - 1) / c.blk;
   const int part = full < 148 * 8 ? full : 148 * 8;
-  k_h_reset<<<1, 1, 0, s>>>(d.P, c.h_iters);
+  k_h_reset<<<1, kMaxSegments, 0, s>>>(d.P, d.segs, d.nseg, c.h_iters);
   cudaMemsetAsync(d.pend_n, 0, 2 * sizeof(unsigned), s);
   int launches = 2;
 #define HC_ARGS(list, ln, nx, nxn, last)                                                                   \
-  d.n, list, ln, d.s(), d.nbr, d.nbr_cnt, d.nbr_cap, d.h0, c.h_eta, c.skin, c.h_tol, d.P, d.hnew, nx, nxn, last, \
+  d.n, list, ln, d.s(), d.nbr, d.nbr_cnt, d.nbr_cap, d.h0, c.h_eta, c.h_tol, d.P, d.segs, d.hnew, nx, nxn, last, \
       d.eos, d.rho, d.fdata
   if (c.kernel == 1)
     k_h_check<1><<<full, c.blk, 0, s>>>(HC_ARGS(nullptr, nullptr, d.pend[0], d.pend_n, c.h_iters == 0 ? 1 : 0));
@@ -307,7 +326,7 @@ int launch_h_learned(const Dev& d, const Cfg& c, cudaStream_t s) {
     launches += 3;
   }
 #undef HC_ARGS
-  k_h_publish<<<1, 1, 0, s>>>(d.P);
+  k_h_publish<<<1, kMaxSegments, 0, s>>>(d.P, d.segs, d.nseg);
   return launches + 1;
 }
 

@@ -51,6 +51,8 @@ __global__ void k_segments_single(Seg* segs, int n, int L, float soft2, double d
   }
   a.soft2 = soft2;
   a.pad = 0u;
+  a.res_bits = 0u;
+  a.skin = 0.0f;
   a.dt = dt;
   a.time = 0.0;
   segs[0] = a;

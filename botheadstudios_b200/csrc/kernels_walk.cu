@@ -104,6 +104,8 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
   const unsigned brk = __ballot_sync(SPH_FULL_MASK, lane > 0 && in_group && gap2 > hm * hm);
   const int nparts = __popc(brk) + 1;
   const int mypart = __popc(brk & ((2u << lane) - 1u));
+  // a negative skin: the impact's current smoothing-length skin (device-maintained)
+  if (NBR && skin < 0.0f) skin = sgr.skin;
   const float grow = (1.0f + skin) * (1.0f + 1.0e-5f);
   const float G = P->G, soft2 = sgr.soft2;
   const unsigned leaf0 = (unsigned)(L - 1);
@@ -390,7 +392,7 @@ static void walk(const Dev& d, const Cfg& c, cudaStream_t s) {
   const State& st = d.s();
   k_tree_walk<W, GRAV, QUAD, NBR, HILO><<<blocks, W * 32, smem, s>>>(
       d.body, st.pos_h, st.x, st.y, st.z, d.K, d.L, d.leaf_start, d.leaf_codes, d.segs, d.left, d.right, d.ncom,
-      d.nbmin, d.nbmax, d.nq0, d.nq1, d.P, d.grav, d.nbr, d.nbr_cnt, d.nbr_cap, c.h_solve ? c.skin : c.nbr_skin,
+      d.nbmin, d.nbmax, d.nq0, d.nq1, d.P, d.grav, d.nbr, d.nbr_cnt, d.nbr_cap, c.h_solve ? -1.0f : c.nbr_skin,
       d.h0, d.groups, d.ngroups);
 }
 

@@ -61,6 +61,10 @@ struct sph_ctx {
 
 namespace {
 
+// Neighbour-list skin after an upload or an unconverged smoothing-length solve (h may move up to 15 % per
+// rebuild); the configured h_skin applies once every particle is near its smoothing length.
+constexpr float kSkinWide = 0.15f;
+
 sph_status cuda_fail(sph_ctx* c, cudaError_t e, const char* what) {
   if (c) {
     c->err = std::string(what) + ": " + cudaGetErrorString(e);
@@ -300,6 +304,7 @@ sph_status upload_impl(sph_ctx* ctx, const SphParticle48* particles, const uint3
     g.sig_bits = 0x7f800000u;
     for (int a = 0; a < 3; ++a) g.bbox[a] = 0xffffffffu;
     g.soft2 = k < nimp ? soft[k] * soft[k] : 0.0f;
+    g.skin = ctx->hp.skin_wide;  // new positions: the first rebuild's solve gets the wide skin
     g.dt = ctx->hp.dt_fixed;
     if (k < nimp) L += (off[k + 1] - off[k] + (uint32_t)d.K - 1) / (uint32_t)d.K;
   }
@@ -431,6 +436,7 @@ sph_status sph_create(const sph_config* cfg, uint32_t capacity, sph_ctx** out) {
       cfg->max_neighbours > 4096 || capacity > (1u << 26) || cfg->mac > 1 ||
       (cfg->block_threads != 0 && (cfg->block_threads < 64 || cfg->block_threads > 1024 || cfg->block_threads % 32)) ||
       (cfg->walk_warps != 0 && cfg->walk_warps != 2 && cfg->walk_warps != 4 && cfg->walk_warps != 8) ||
+      !(cfg->h_skin >= 0.0f && cfg->h_skin <= 0.5f) ||
       (cfg->mac == SPH_MAC_GROUP && (cfg->leaf_size & (cfg->leaf_size - 1)) != 0))
     return SPH_ERR_INVALID;
   sph_ctx* ctx = new (std::nothrow) sph_ctx();
@@ -447,7 +453,7 @@ sph_status sph_create(const sph_config* cfg, uint32_t capacity, sph_ctx** out) {
   ctx->kc.h_eta = std::cbrt(3.0f * cfg->h_neighbours / (4.0f * 3.14159265358979f));
   ctx->kc.h_tol = cfg->h_tol;
   ctx->kc.h_iters = (int)cfg->h_iters;
-  ctx->kc.skin = ctx->kc.h_solve ? 0.15f : 0.0f;
+  ctx->kc.skin = ctx->kc.h_solve ? (cfg->h_skin > 0.0f ? cfg->h_skin : 0.05f) : 0.0f;
   ctx->kc.mac = (int)cfg->mac;
   ctx->kc.blk = cfg->block_threads ? (int)cfg->block_threads : 256;
   ctx->kc.walk_warps = cfg->walk_warps ? (int)cfg->walk_warps : 2;
@@ -504,6 +510,9 @@ sph_status sph_create(const sph_config* cfg, uint32_t capacity, sph_ctx** out) {
     p.du_floor = cfg->du_floor;
     p.r_min = cfg->r_min;
     p.sig_floor = cfg->sig_floor;
+    p.skin_narrow = ctx->kc.skin;
+    p.skin_wide = ctx->kc.skin > kSkinWide ? ctx->kc.skin : kSkinWide;
+    p.skin_reset = 10.0f * cfg->h_tol;
     st = init_params(ctx, ctx->d);
   }
   if (st != SPH_OK) {

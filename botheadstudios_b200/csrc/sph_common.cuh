@@ -32,6 +32,9 @@ struct DevParams {
   float cfl;
   float rho_floor, du_floor, r_min, sig_floor;
   float progress;     // host-set fraction of the run completed (a learned-h input)
+  float skin_narrow;  // neighbour-list skin of a rebuild after a converged smoothing-length solve
+  float skin_wide;    // ... after an upload, or after a solve that ended far from converged
+  float skin_reset;   // residual above which the next rebuild takes the wide skin
   unsigned pad0;
   // ---- maintained by the device from here on --------------------------------------------------------
   unsigned flags;         // kFlag* bits
@@ -39,7 +42,7 @@ struct DevParams {
   unsigned steps;
   unsigned h_iters_used;
   float h_residual;
-  unsigned h_residual_bits;
+  unsigned pad1;
   unsigned h_accepted;    // learned h: particles whose proposal passed the first residual check (last solve)
   unsigned pad;
   // walk statistics, accumulated once per warp: node visits, 32-wide pops, multipole and pairwise

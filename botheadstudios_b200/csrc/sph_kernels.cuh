@@ -34,10 +34,12 @@ struct Seg {
   unsigned bbox[6];     // order-preserving keys of lo.xyz, hi.xyz (bh_gravity.wgsl:49-57)
   float soft2;          // softening² of this impact
   unsigned pad;         // first walk group of the impact
+  unsigned res_bits;    // atomicMax target: the impact's smoothing-length residual maximum (float bits)
+  float skin;           // neighbour-list skin of the impact's next rebuild (smoothing-length solve)
   double dt;            // dt of the current step
   double time;          // simulated time
 };
-static_assert(sizeof(Seg) == 64, "Seg is one 64-byte record");
+static_assert(sizeof(Seg) == 72, "Seg is one 72-byte record");
 constexpr unsigned kNoSeg = 0xffffffffu;
 
 // Reduce per-thread boxes (order-preserving keys, identity values when the thread holds no point) into the
@@ -98,6 +100,19 @@ __device__ __forceinline__ void seg_bbox_commit(unsigned lo[3], unsigned hi[3], 
       atomicMin(&segs[sg].bbox[k], lo[k]);
       atomicMax(&segs[sg].bbox[3 + k], hi[k]);
     }
+  }
+}
+
+// Maximum of non-negative per-thread values into each thread's segment (res_bits): one atomic per warp when
+// the warp lies in one segment. `sg` = kNoSeg for a thread without a value. All lanes of the warp call it.
+__device__ __forceinline__ void seg_res_max(Seg* segs, unsigned sg, float v) {
+  const unsigned lo = warp_min(sg), hi = warp_max(sg == kNoSeg ? 0u : sg);
+  if (lo == kNoSeg) return;
+  if (lo == hi) {
+    const float m = warp_max(sg == kNoSeg ? 0.0f : v);
+    if ((threadIdx.x & 31) == 0) atomicMax(&segs[lo].res_bits, __float_as_uint(m));
+  } else if (sg != kNoSeg) {
+    atomicMax(&segs[sg].res_bits, __float_as_uint(v));
   }
 }
 

@@ -86,7 +86,10 @@ typedef struct sph_config {
   uint32_t block_threads; /* threads per block of the density, h-solve and force kernels: 64..1024, a multiple of
                              32; 0 = 256 */
   uint32_t walk_warps;    /* warps per block of the fused gravity + neighbour walk: 2, 4 or 8; 0 = 2 */
-  uint32_t reserved[3];
+  float h_skin;           /* SOLVE/LEARNED: neighbour lists are built at h·(1 + h_skin) and h moves at most that far
+                             per rebuild, once the previous solve converged (residual <= 10·h_tol); after an
+                             upload or an unconverged solve the skin is 0.15. 0 = 0.05 (at most 0.5) */
+  uint32_t reserved[2];
 } sph_config;
 
 /* Barnes-Hut acceptance. PARTICLE: each particle walks with the GPU reference's MAC
