@@ -32,8 +32,7 @@ struct WalkSmem {
   float4 src[W][32];   // staged sources: x, y, z, m
   float4 q0[W][32];    // staged quadrupoles
   float2 q1[W][32];
-  float hsrc[W][32];   // staged smoothing lengths (direct list)
-  int sidx[W][32];     // staged source indices (direct list)
+  float2 sh[W][32];    // staged source index (bits) and smoothing length (direct list)
 };
 
 // Compensated accumulator for the precision mode.
@@ -170,12 +169,16 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
     for (int base = 0; base < count; base += 32) {
       const int m = min(32, count - base);
       if ((int)lane < m) {
+        // staged with G folded in: (com, G·M) and G·Q
         const unsigned node = S.m2p[w][base + lane];
-        S.src[w][lane] = ncom[node];
+        float4 c = ncom[node];
+        c.w *= G;
+        S.src[w][lane] = c;
         if (QUAD) {
-          S.q0[w][lane] = nq0[node];
+          const float4 q = nq0[node];
           const float4 b = nq1[node];
-          S.q1[w][lane] = make_float2(b.x, b.y);
+          S.q0[w][lane] = make_float4(G * q.x, G * q.y, G * q.z, G * q.w);
+          S.q1[w][lane] = make_float2(G * b.x, G * b.y);
         }
       }
       __syncwarp();
@@ -187,10 +190,11 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
           const float r2 = dx * dx + dy * dy + dz * dz + soft2;
           const float rinv = rsqrtf(r2);
           const float rinv2 = rinv * rinv;
-          const float gm = G * c.w * rinv;
-          float fx = gm * rinv2 * dx, fy = gm * rinv2 * dy, fz = gm * rinv2 * dz;
-          float ph = -gm;
+          const float gm = c.w * rinv;           // G M / R
+          const float g = gm * rinv2;            // G M / R³
           if (QUAD) {
+            // a = G M d/R³ + (G/R⁴)(5/2 (eᵀQe) e − Q e), e = d/R (unit vector: Q·e and eᵀQe stay in f32 range
+            // in SI units) = d (G M/R³ + 5/2 eᵀQe/R⁵) − Q e/R⁴;  φ = −G M/R − ½ eᵀQe/R³
             const float4 a0 = S.q0[w][k];
             const float2 a1 = S.q1[w][k];
             const float ex = dx * rinv, ey = dy * rinv, ez = dz * rinv;
@@ -198,14 +202,14 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
             const float Qey = a0.w * ex + a0.y * ey + a1.y * ez;
             const float Qez = a1.x * ex + a1.y * ey + a0.z * ez;
             const float eQe = ex * Qex + ey * Qey + ez * Qez;
-            const float s = G * rinv2;
-            fx += ((2.5f * eQe * ex - Qex) * rinv2) * s;
-            fy += ((2.5f * eQe * ey - Qey) * rinv2) * s;
-            fz += ((2.5f * eQe * ez - Qez) * rinv2) * s;
-            ph -= (0.5f * eQe * rinv2) * G * rinv;
+            const float rinv4 = rinv2 * rinv2;
+            const float c1 = fmaf(2.5f * eQe, rinv4 * rinv, g);
+            acc.add<HILO>(c1 * dx - rinv4 * Qex, c1 * dy - rinv4 * Qey, c1 * dz - rinv4 * Qez);
+            phi -= fmaf(0.5f * eQe, rinv2, c.w) * rinv;
+          } else {
+            acc.add<HILO>(g * dx, g * dy, g * dz);
+            phi -= gm;
           }
-          acc.add<HILO>(fx, fy, fz);
-          phi += ph;
         }
       }
       __syncwarp();
@@ -224,7 +228,6 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
         const int s = (int)leaf_start[lf] + off;
         if (s < (int)leaf_start[lf + 1]) sidx = s;
       }
-      S.sidx[w][lane] = sidx;
       float4 src = make_float4(3.0e18f, 3.0e18f, 3.0e18f, 0.0f);  // padding: massless and far away
       float hsrc = 0.0f;
       if (sidx >= 0) {
@@ -233,18 +236,19 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
         if (NBR) hsrc = pos_h[sidx].w;
       }
       S.src[w][lane] = src;
-      if (NBR) S.hsrc[w][lane] = hsrc;
+      S.sh[w][lane] = make_float2(__int_as_float(sidx), hsrc);
       __syncwarp();
       if (valid) {
 #pragma unroll 4
         for (int k = 0; k < 32; ++k) {
-          const int s = S.sidx[w][k];
+          const float2 shk = S.sh[w][k];
+          const int s = __float_as_int(shk.x);
           const bool other = s >= 0 && s != t;
           const float4 bj = S.src[w][k];
           const float dx = fsub(bj.x, pi.x), dy = fsub(bj.y, pi.y), dz = fsub(bj.z, pi.z);
           const float dd = dot3_exact(dx, dy, dz);
           if (NBR && other) {
-            float lim = fmul(0.5f, fadd(pi.w, S.hsrc[w][k]));
+            float lim = fmul(0.5f, fadd(pi.w, shk.y));
             if (skin > 0.0f) lim = lim * (1.0f + skin);
             // sqrt_rn(dd) < lim, decided without the square root outside a 2^-19 band around lim²:
             // dd < lim²(1-2^-19) ⇒ √dd < lim − 2 ulp(lim); dd > lim²(1+2^-19) ⇒ √dd > lim + 2 ulp(lim)

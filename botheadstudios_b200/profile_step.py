@@ -22,6 +22,7 @@ def main():
     ap.add_argument("--leaf", type=int, default=None, help="LBVH leaf size (default: the workload's)")
     ap.add_argument("--walk-warps", type=int, default=0, help="warps per walk block (2, 4, 8; 0 = 4)")
     ap.add_argument("--block", type=int, default=0, help="threads per block of the gather kernels (0 = 256)")
+    ap.add_argument("--gravity", default=None, choices=["tree", "direct", "none"], help="override the gravity mode")
     ap.add_argument("--accuracy", type=int, default=0,
                     help="targets for an FP64 direct-sum check of the tree gravity (0 = skip)")
     args = ap.parse_args()
@@ -30,6 +31,8 @@ def main():
     over = dict(mac=args.mac, precision=args.precision, walk_warps=args.walk_warps, block_threads=args.block)
     if args.leaf is not None:
         over["leaf_size"] = args.leaf
+    if args.gravity is not None:
+        over["gravity"] = args.gravity
     if args.theta is not None:
         over["theta"] = args.theta
     acc_err = None
@@ -55,7 +58,7 @@ def main():
                            p99_rel=float(np.quantile(e, 0.99)), max_rel=float(e.max()),
                            global_rms=float(np.sqrt(((g[tg] - ref) ** 2).sum() / (ref ** 2).sum())))
     n = len(I.particles)
-    walks = max(prof["calls"]["gravity"], 1)
+    walks = max(prof["calls"]["gravity"], prof["calls"]["neighbours"], 1)
     stats = {k: (d1[k] - d0[k]) / walks for k in ("walk_nodes", "walk_pops", "m2p_interactions", "p2p_interactions")}
     print(json.dumps(dict(workload=args.workload, particles=n, steps=args.steps, config=over, phases_ms=prof["ms"],
                           calls=prof["calls"], launches=prof["kernel_launches"], per_walk=stats,
