@@ -74,11 +74,25 @@ EXPORTS = ["sph_config_default", "sph_create", "sph_destroy", "sph_upload", "sph
            "sph_gravity", "sph_gravity_direct64", "sph_gravity_tree_noalloc", "sph_dem_create", "sph_dem_destroy",
            "sph_dem_replace", "sph_dem_set_params", "sph_dem_step", "sph_dem_readback", "sph_dem_contacts",
            "sph_dem_count", "sph_mlp_set", "sph_mlp_record", "sph_mlp_features", "sph_set_progress",
-           "sph_mlp_forward", "sph_mlp_grad", "sph_mlp_train"]
+           "sph_mlp_forward", "sph_mlp_grad", "sph_mlp_train", "sph_measure_default", "sph_measure_disk"]
 
 H_MODE = dict(fixed=0, solve=1, learned=2)
 MLP_PARAMS = 4819     # SPH_MLP_PARAMS
 MLP_TRAINABLE = 4801  # SPH_MLP_TRAINABLE
+
+
+class MeasureCfg(C.Structure):
+    _fields_ = [("variant", C.c_int32), ("reserved", C.c_int32), ("G", C.c_double), ("remnant_frac", C.c_double),
+                ("link_factor", C.c_double), ("roche", C.c_double), ("rho_fallback", C.c_double),
+                ("pe_floor", C.c_double), ("pe_softening", C.c_double)]
+
+
+class DiskMeasure(C.Structure):
+    _fields_ = [("earth_frac", C.c_double), ("disk_mass", C.c_double), ("disk_target", C.c_double),
+                ("disk_impactor", C.c_double), ("remnant_target", C.c_double), ("remnant_impactor", C.c_double),
+                ("escaped_target", C.c_double), ("escaped_impactor", C.c_double), ("r_remnant", C.c_double),
+                ("m_remnant", C.c_double), ("clump_mass", C.c_double), ("clump_target_frac", C.c_double),
+                ("clump_n", C.c_uint32), ("n_clumps", C.c_uint32), ("n_bound", C.c_uint32), ("n_disk", C.c_uint32)]
 
 
 class MlpTrainCfg(C.Structure):
@@ -159,6 +173,8 @@ def load():
     L.sph_mlp_grad.argtypes = [vp, vp, vp, C.c_uint32, vp, vp]
     L.sph_mlp_train.argtypes = [vp, vp, vp, C.c_uint32, C.POINTER(MlpTrainCfg), vp]
     L.sph_dem_count.argtypes = [vp]
+    L.sph_measure_default.argtypes = [C.POINTER(MeasureCfg)]
+    L.sph_measure_disk.argtypes = [vp, C.c_uint32, C.POINTER(MeasureCfg), C.POINTER(DiskMeasure)]
     L.sph_dem_count.restype = C.c_uint32
     no_status = ("sph_destroy", "sph_count", "sph_stream", "sph_last_error", "sph_status_string", "sph_dem_destroy",
                  "sph_dem_count")

@@ -1,0 +1,795 @@
+// Disk measurement and the Moon candidate of one impact, on the device.
+//
+// The reference measures a finished impact on the host in two places: the impact-run tool
+// (tools/impact-run/src/main.rs:732-878, `measure` + `moon_candidate`) and the engine's HUD statistics
+// (crates/engine/src/gpu_sph.rs:399-469, `disk_stats_json` + accretion.rs:73-160 `find_clumps`). Both:
+//   1. mass, centre of mass and bulk velocity of the impact;
+//   2. the remnant radius: the smallest radius about the centre of mass enclosing 85 % of the mass (radius
+//      sort + running sum);
+//   3. each particle's two-body orbit about the remnant: escaping, remnant (periapsis inside it) or disk;
+//   4. friends-of-friends over the disk particles with a linking length of twice the mean smoothing length
+//      (the tool: an O(k²) pair loop; the engine: a cell grid), union-find;
+//   5. per clump of two or more: mass, centre of mass and velocity, volume, internal kinetic energy and the
+//      pairwise self-potential (O(s²)); bound when KE + PE < 0; outside the fluid Roche limit
+//      2.44 R (ρ_remnant / ρ_clump)^(1/3); the Moon candidate is the heaviest bound clump outside it.
+//
+// Here every step is a kernel over the impact's particle range of the state (already contiguous per impact):
+// deterministic two-pass f64 reductions; the radius sort is the tree's 8-bit LSD radix sort over the exact
+// f64 bit patterns of the radii; the 85 % crossing is a tile prefix walk; classification writes per-block
+// partials and an order-preserving compaction of the disk; the friends-of-friends search sorts the disk by
+// a lexicographic cell key (cell edge just above the linking length, so every linked pair lies in the 3 × 3
+// column of z-runs around a particle) and unites pairs with a lock-free union-find (hooking the larger root
+// under the smaller with atomicCAS, path halving; parent[i] <= i always, so every walk ends); clumps are
+// contiguous after a radix sort by root; the self-potential is split into units of two 128-particle rows of
+// the clump's upper pair triangle (rows u and T-1-u, so units carry equal work), each unit summing its pairs
+// in f64. The per-particle arithmetic that decides a classification (radii, periapsis, pair distances) is
+// written with explicitly rounded operations in the reference's order; the sums differ from the
+// reference's sequential ones only in association.
+#include <cstdint>
+#include <cstring>
+
+#include "sph_kernels.cuh"
+
+namespace sphb {
+
+struct DiskWork {
+  int cap = 0;
+  void* base = nullptr;
+  unsigned long long* keys[2] = {nullptr, nullptr};
+  unsigned* vals[2] = {nullptr, nullptr};
+  unsigned* hist = nullptr;
+  unsigned* tot = nullptr;
+  double* part = nullptr;   // [kDmBlocks][kDmVals] block partials
+  double* tsum = nullptr;   // [tiles] mass of each radius-sorted tile
+  double* scal = nullptr;   // [S_COUNT]
+  unsigned* cnt = nullptr;  // [C_COUNT]
+  unsigned* bcnt = nullptr; // [kDmBlocks] disk particles per block, then their output offsets
+  unsigned char* cat = nullptr;  // [cap] category of each particle
+  float4* dpos[2] = {nullptr, nullptr};  // disk particles: x, y, z, h
+  float4* dvel[2] = {nullptr, nullptr};  // vx, vy, vz, mass
+  float2* drp[2] = {nullptr, nullptr};   // rho, prov bits
+  unsigned* parent = nullptr;  // [cap] union-find forest over the cell-sorted disk
+  unsigned* gcnt = nullptr;    // [cap] members per root
+  uint4* clump = nullptr;      // [cap/2+1] first member, members, root, units
+  unsigned* uoff = nullptr;    // [cap/2+2] first unit of each clump
+  double* cstat = nullptr;     // [cap/2+1][8] mass, com xyz, volume, target mass, internal KE
+  double* upe = nullptr;       // [cap+1] unit sums Σ m_a m_b / r
+  double* out = nullptr;       // [16]
+};
+
+namespace {
+
+constexpr int kDmThreads = 256;
+constexpr int kDmBlocks = 592;  // 4 × 148 SMs; block b reduces the b-th contiguous chunk of the impact
+constexpr int kDmVals = 8;
+constexpr int kPeRows = 128;    // particles per self-potential row
+constexpr int kTile = 2048;     // radius-sorted tile of the crossing walk (the radix sort's tile)
+constexpr unsigned kCellBias = 1u << 20, kCellMax = (1u << 21) - 1u;
+constexpr int kUnionTries = 1 << 16;
+constexpr double kPiD = 3.14159265358979323846;
+
+enum { S_M = 0, S_COM = 1, S_VCOM = 4, S_RREM = 7, S_MREM = 8, S_LINK = 9, S_RHOREM = 10, S_CAT = 11, S_COUNT = 24 };
+enum { C_NDISK = 0, C_NCLUMP = 1, C_UNITS = 2, C_ERR = 3, C_COUNT = 8 };
+
+// Sum kDmVals doubles over the block in a fixed order (warp trees, then warps in order). Thread 0 gets them.
+__device__ __forceinline__ void block_sum(double* v, double (*s)[kDmVals]) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < kDmVals; ++k) {
+    const double x = warp_sum(v[k]);
+    if (lane == 0) s[w][k] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int nw = blockDim.x >> 5;
+#pragma unroll
+    for (int k = 0; k < kDmVals; ++k) {
+      double a = 0.0;
+      for (int j = 0; j < nw; ++j) a += s[j][k];
+      v[k] = a;
+    }
+  }
+  __syncthreads();
+}
+
+// Sum of nb partials of value k over a warp, fixed order.
+__device__ __forceinline__ double warp_sum_column(const double* part, int nb, int k) {
+  double a = 0.0;
+  for (int b = (int)(threadIdx.x & 31); b < nb; b += 32) a += part[b * kDmVals + k];
+  return warp_sum(a);
+}
+
+__device__ __forceinline__ double dsq3(double x, double y, double z) {
+  return __dadd_rn(__dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)), __dmul_rn(z, z));
+}
+
+// The particle's position as the 48-byte exchange record holds it (f32 of the f64 master).
+__device__ __forceinline__ float3 pos_f32(const State& st, unsigned t) {
+  return make_float3((float)st.x[t], (float)st.y[t], (float)st.z[t]);
+}
+
+// ---- 1. mass, centre of mass, bulk velocity ----------------------------------------------------------
+__global__ void __launch_bounds__(kDmThreads) k_dm_moments(State st, unsigned off, unsigned m, unsigned chunk,
+                                                           double* __restrict__ part) {
+  __shared__ double s[kDmThreads / 32][kDmVals];
+  double a[kDmVals] = {0, 0, 0, 0, 0, 0, 0, 0};
+  const unsigned b0 = blockIdx.x * chunk, b1 = min(m, b0 + chunk);
+  for (unsigned i = b0 + threadIdx.x; i < b1; i += kDmThreads) {
+    const unsigned t = off + i;
+    const float3 p = pos_f32(st, t);
+    const float4 v = st.vel_u[t];
+    const double mm = st.mass[t];
+    a[0] += mm;
+    a[1] += (double)p.x * mm;  // f32 × f32 products are exact in f64
+    a[2] += (double)p.y * mm;
+    a[3] += (double)p.z * mm;
+    a[4] += (double)v.x * mm;
+    a[5] += (double)v.y * mm;
+    a[6] += (double)v.z * mm;
+    a[7] += (double)st.pos_h[t].w;
+  }
+  block_sum(a, s);
+  if (threadIdx.x == 0)
+    for (int k = 0; k < kDmVals; ++k) part[blockIdx.x * kDmVals + k] = a[k];
+}
+
+__global__ void k_dm_moments_final(const double* __restrict__ part, int nb, double* __restrict__ scal) {
+  __shared__ double t[kDmVals];
+  const int w = threadIdx.x >> 5;
+  const double v = warp_sum_column(part, nb, w);
+  if ((threadIdx.x & 31) == 0) t[w] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const double M = t[0];
+    scal[S_M] = M;
+    for (int k = 0; k < 3; ++k) {
+      scal[S_COM + k] = t[1 + k] / M;
+      scal[S_VCOM + k] = t[4 + k] / M;
+    }
+    scal[S_CAT + 7] = t[7];  // Σ h over every particle (the engine's linking length)
+  }
+}
+
+// ---- 2. radii, their sort, the 85 % crossing -----------------------------------------------------------
+__global__ void k_dm_radius(State st, unsigned off, unsigned m, const double* __restrict__ scal,
+                            unsigned long long* __restrict__ keys, unsigned* __restrict__ vals) {
+  const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  const float3 p = pos_f32(st, off + i);
+  const double dx = __dsub_rn((double)p.x, scal[S_COM]), dy = __dsub_rn((double)p.y, scal[S_COM + 1]),
+               dz = __dsub_rn((double)p.z, scal[S_COM + 2]);
+  const double r = __dsqrt_rn(dsq3(dx, dy, dz));
+  keys[i] = (unsigned long long)__double_as_longlong(r);  // r >= 0: the bit pattern orders like the value
+  vals[i] = i;
+}
+
+__global__ void __launch_bounds__(kDmThreads) k_dm_tile_mass(State st, unsigned off, unsigned m,
+                                                             const unsigned* __restrict__ order,
+                                                             double* __restrict__ tsum) {
+  __shared__ double s[kDmThreads / 32][kDmVals];
+  double a[kDmVals] = {0, 0, 0, 0, 0, 0, 0, 0};
+  const unsigned b0 = blockIdx.x * kTile, b1 = min(m, b0 + kTile);
+  for (unsigned i = b0 + threadIdx.x; i < b1; i += kDmThreads) a[0] += (double)st.mass[off + order[i]];
+  block_sum(a, s);
+  if (threadIdx.x == 0) tsum[blockIdx.x] = a[0];
+}
+
+// One thread walks the tiles, then the crossing tile's particles in radius order.
+__global__ void k_dm_cross(State st, unsigned off, unsigned m, int tiles, const unsigned long long* __restrict__ keys,
+                           const unsigned* __restrict__ order, const double* __restrict__ tsum,
+                           double* __restrict__ scal, double frac) {
+  if (threadIdx.x != 0) return;
+  const double M = scal[S_M], thr = frac * M;
+  double cum = 0.0;
+  int t = 0;
+  while (t < tiles && cum + tsum[t] < thr) cum += tsum[t++];
+  double r_rem = __longlong_as_double((long long)keys[m - 1]), m_rem = M;
+  for (unsigned i = (unsigned)t * kTile; i < m; ++i) {
+    cum += (double)st.mass[off + order[i]];
+    if (cum >= thr) {
+      r_rem = __longlong_as_double((long long)keys[i]);
+      m_rem = cum;
+      break;
+    }
+  }
+  scal[S_RREM] = r_rem;
+  scal[S_MREM] = m_rem;
+  scal[S_RHOREM] = m_rem / (4.0 / 3.0 * kPiD * (r_rem * r_rem * r_rem));
+}
+
+// ---- 3. orbit classification ----------------------------------------------------------------------------
+// 0 escapes, 1 disk, 2 remnant: main.rs:232-247 (variant 0) or orbit.rs:91-116 (variant 1).
+__device__ __forceinline__ int classify(int variant, double px, double py, double pz, double vx, double vy,
+                                        double vz, double mu, double r_rem) {
+  const double r = __dsqrt_rn(dsq3(px, py, pz));
+  const double v2 = dsq3(vx, vy, vz);
+  const double hx = __dsub_rn(__dmul_rn(py, vz), __dmul_rn(pz, vy));
+  const double hy = __dsub_rn(__dmul_rn(pz, vx), __dmul_rn(px, vz));
+  const double hz = __dsub_rn(__dmul_rn(px, vy), __dmul_rn(py, vx));
+  const double h2 = dsq3(hx, hy, hz);
+  if (variant == 0 && r == 0.0) return 2;
+  if (variant == 1 && !(r > 0.0)) return 0;
+  const double energy = __dsub_rn(__dmul_rn(0.5, v2), __ddiv_rn(mu, r));
+  if (energy >= 0.0) return 0;
+  const double hl = __dsqrt_rn(h2);  // variant 1 multiplies by |h| twice: ((2E·|h|)·|h|)/μ²
+  const double num = variant == 0 ? __dmul_rn(__dmul_rn(2.0, energy), h2)
+                                  : __dmul_rn(__dmul_rn(__dmul_rn(2.0, energy), hl), hl);
+  const double q = __ddiv_rn(num, __dmul_rn(mu, mu));
+  const double e = __dsqrt_rn(fmax(__dadd_rn(1.0, q), 0.0));
+  const double a = __ddiv_rn(-mu, __dmul_rn(2.0, energy));
+  return __dmul_rn(a, __dsub_rn(1.0, e)) > r_rem ? 1 : 2;
+}
+
+// Categories: 0 target disk, 1 impactor disk, 2 target remnant, 3 impactor remnant, 4/5 escaping.
+__global__ void __launch_bounds__(kDmThreads) k_dm_classify(State st, unsigned off, unsigned m, unsigned chunk,
+                                                            int variant, double G, const double* __restrict__ scal,
+                                                            unsigned char* __restrict__ cat,
+                                                            double* __restrict__ part, unsigned* __restrict__ bcnt) {
+  __shared__ double s[kDmThreads / 32][kDmVals];
+  double a[kDmVals] = {0, 0, 0, 0, 0, 0, 0, 0};
+  const double cx = scal[S_COM], cy = scal[S_COM + 1], cz = scal[S_COM + 2];
+  const double ux = scal[S_VCOM], uy = scal[S_VCOM + 1], uz = scal[S_VCOM + 2];
+  const double mu = G * scal[S_MREM], r_rem = scal[S_RREM];
+  const unsigned b0 = blockIdx.x * chunk, b1 = min(m, b0 + chunk);
+  unsigned ndisk = 0;
+  for (unsigned base = b0; base < b1; base += kDmThreads) {
+    const unsigned i = base + threadIdx.x;
+    int is_disk = 0;
+    if (i < b1) {
+      const unsigned t = off + i;
+      const float3 p = pos_f32(st, t);
+      const float4 v = st.vel_u[t];
+      const int c = classify(variant, __dsub_rn((double)p.x, cx), __dsub_rn((double)p.y, cy),
+                             __dsub_rn((double)p.z, cz), __dsub_rn((double)v.x, ux), __dsub_rn((double)v.y, uy),
+                             __dsub_rn((double)v.z, uz), mu, r_rem);
+      const int k = (c == 1 ? 0 : c == 2 ? 2 : 4) + (st.prov[t] == 0u ? 0 : 1);
+      cat[i] = (unsigned char)k;
+      const double mm = st.mass[t];
+#pragma unroll
+      for (int j = 0; j < 6; ++j) a[j] += j == k ? mm : 0.0;
+      if (c == 1) a[6] += (double)st.pos_h[t].w;
+      is_disk = c == 1;
+    }
+    ndisk += (unsigned)__syncthreads_count(is_disk);
+  }
+  block_sum(a, s);
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < kDmVals; ++k) part[blockIdx.x * kDmVals + k] = a[k];
+    bcnt[blockIdx.x] = ndisk;
+  }
+}
+
+__global__ void __launch_bounds__(1024) k_dm_classify_final(const double* __restrict__ part, int nb, unsigned m,
+                                                            int variant, double link_factor,
+                                                            unsigned* __restrict__ bcnt, double* __restrict__ scal,
+                                                            unsigned* __restrict__ cnt, double* __restrict__ out) {
+  __shared__ unsigned s_warp[33];
+  __shared__ double t[kDmVals];
+  const int w = threadIdx.x >> 5;
+  if (w < kDmVals) {
+    const double v = warp_sum_column(part, nb, w);
+    if ((threadIdx.x & 31) == 0) t[w] = v;
+  }
+  unsigned total;
+  const unsigned c = threadIdx.x < (unsigned)nb ? bcnt[threadIdx.x] : 0u;
+  const unsigned o = block_exclusive_scan(c, s_warp, total);  // synchronises the block
+  if (threadIdx.x < (unsigned)nb) bcnt[threadIdx.x] = o;
+  if (threadIdx.x == 0) {
+    cnt[C_NDISK] = total;
+    for (int k = 0; k < 6; ++k) scal[S_CAT + k] = t[k];
+    const double mean_h = variant == 0 ? (total ? t[6] / (double)total : 0.0) : scal[S_CAT + 7] / (double)m;
+    scal[S_LINK] = link_factor * mean_h;
+    const double disk = t[0] + t[1];
+    out[0] = disk > 0.0 ? 100.0 * t[0] / disk : 0.0;
+    out[1] = disk;
+    for (int k = 0; k < 6; ++k) out[2 + k] = t[k];
+    out[8] = scal[S_RREM];
+    out[9] = scal[S_MREM];
+    for (int k = 10; k < 15; ++k) out[k] = 0.0;
+    out[15] = (double)total;
+  }
+}
+
+// ---- 4. friends-of-friends over the disk ----------------------------------------------------------------
+__device__ __forceinline__ unsigned cell_coord(double x, double c, double inv_cs) {
+  const double q = floor((x - c) * inv_cs) + (double)kCellBias;
+  if (!(q > 0.0)) return 0u;  // clamping only merges far cells: linked pairs stay within one cell per axis
+  return q >= (double)kCellMax ? kCellMax : (unsigned)q;
+}
+__device__ __forceinline__ unsigned long long cell_key(unsigned ix, unsigned iy, unsigned iz) {
+  return ((unsigned long long)ix << 42) | ((unsigned long long)iy << 21) | (unsigned long long)iz;
+}
+
+// Order-preserving compaction of the disk particles (block b writes from its offset in chunk order).
+__global__ void __launch_bounds__(kDmThreads) k_dm_compact(State st, const float* __restrict__ rho, unsigned off,
+                                                           unsigned m, unsigned chunk,
+                                                           const unsigned char* __restrict__ cat,
+                                                           const unsigned* __restrict__ boff,
+                                                           const double* __restrict__ scal, float4* __restrict__ dpos,
+                                                           float4* __restrict__ dvel, float2* __restrict__ drp,
+                                                           unsigned long long* __restrict__ keys,
+                                                           unsigned* __restrict__ vals) {
+  __shared__ unsigned s_warp[33];
+  const double cx = scal[S_COM], cy = scal[S_COM + 1], cz = scal[S_COM + 2];
+  // cell edge just above the linking length: a linked pair differs by at most one cell per axis even after
+  // the f32 subtraction of the tool's distance
+  const double inv_cs = 1.0 / (scal[S_LINK] * (1.0 + 0x1p-20));
+  const unsigned b0 = blockIdx.x * chunk, b1 = min(m, b0 + chunk);
+  unsigned run = boff[blockIdx.x];
+  for (unsigned base = b0; base < b1; base += kDmThreads) {
+    const unsigned i = base + threadIdx.x;
+    const unsigned f = (i < b1 && cat[i] < 2) ? 1u : 0u;
+    unsigned total;
+    const unsigned o = run + block_exclusive_scan(f, s_warp, total);
+    if (f) {
+      const unsigned t = off + i;
+      const float3 p = pos_f32(st, t);
+      const float4 v = st.vel_u[t];
+      dpos[o] = make_float4(p.x, p.y, p.z, st.pos_h[t].w);
+      dvel[o] = make_float4(v.x, v.y, v.z, st.mass[t]);
+      drp[o] = make_float2(rho[t], __uint_as_float(st.prov[t]));
+      keys[o] = cell_key(cell_coord(p.x, cx, inv_cs), cell_coord(p.y, cy, inv_cs), cell_coord(p.z, cz, inv_cs));
+      vals[o] = o;
+    }
+    run += total;
+  }
+}
+
+__global__ void k_dm_gather(unsigned n, const unsigned* __restrict__ order, const float4* __restrict__ p0,
+                            const float4* __restrict__ v0, const float2* __restrict__ r0, float4* __restrict__ p1,
+                            float4* __restrict__ v1, float2* __restrict__ r1, unsigned* __restrict__ parent,
+                            unsigned* __restrict__ gcnt) {
+  const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const unsigned j = order[i];
+  p1[i] = p0[j];
+  v1[i] = v0[j];
+  r1[i] = r0[j];
+  if (parent) {
+    parent[i] = i;
+    gcnt[i] = 0u;
+  }
+}
+
+// Root of x with path halving. parent[v] <= v for every v and the walk strictly decreases, so it ends.
+__device__ __forceinline__ unsigned uf_find(unsigned* parent, unsigned x) {
+  volatile unsigned* p = parent;
+  unsigned nx = p[x];
+  while (nx != x) {
+    const unsigned nn = p[nx];
+    if (nn != nx) p[x] = nn;  // nn is an ancestor of x
+    x = nx;
+    nx = nn;
+  }
+  return x;
+}
+
+__device__ __forceinline__ bool uf_unite(unsigned* parent, unsigned a, unsigned b) {
+  for (int k = 0; k < kUnionTries; ++k) {
+    a = uf_find(parent, a);
+    b = uf_find(parent, b);
+    if (a == b) return true;
+    const unsigned hi = a > b ? a : b, lo = a > b ? b : a;
+    if (atomicCAS(&parent[hi], hi, lo) == hi) return true;  // a failed hook means hi gained a parent
+  }
+  return false;
+}
+
+__device__ __forceinline__ double pair_d2(int variant, float4 a, float4 b) {
+  if (variant == 0)  // main.rs:823: f32 difference, widened, squared
+    return dsq3((double)__fsub_rn(a.x, b.x), (double)__fsub_rn(a.y, b.y), (double)__fsub_rn(a.z, b.z));
+  return dsq3(__dsub_rn((double)a.x, (double)b.x), __dsub_rn((double)a.y, (double)b.y),
+              __dsub_rn((double)a.z, (double)b.z));
+}
+
+__device__ __forceinline__ unsigned lower_bound_u64(const unsigned long long* k, unsigned n, unsigned long long x) {
+  unsigned lo = 0, hi = n;
+  while (lo < hi) {
+    const unsigned mid = (lo + hi) >> 1;
+    if (k[mid] < x) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+__global__ void k_dm_link(unsigned n, int variant, const unsigned long long* __restrict__ skeys,
+                          const float4* __restrict__ dpos, const double* __restrict__ scal,
+                          unsigned* __restrict__ parent, unsigned* __restrict__ cnt) {
+  const unsigned a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a + 1u >= n) return;  // partners come after a in the order, so each pair is tested once
+  const double link = scal[S_LINK], link2 = link * link;
+  const unsigned long long ka = skeys[a];
+  const unsigned ix = (unsigned)(ka >> 42), iy = (unsigned)(ka >> 21) & kCellMax, iz = (unsigned)ka & kCellMax;
+  const unsigned z0 = iz ? iz - 1u : 0u, z1 = iz < kCellMax ? iz + 1u : kCellMax;
+  const float4 pa = dpos[a];
+  bool ok = true;
+  for (int dx = -1; dx <= 1; ++dx) {
+    const int cx = (int)ix + dx;
+    if (cx < 0 || cx > (int)kCellMax) continue;
+    for (int dy = -1; dy <= 1; ++dy) {
+      const int cy = (int)iy + dy;
+      if (cy < 0 || cy > (int)kCellMax) continue;
+      const unsigned long long lo = cell_key((unsigned)cx, (unsigned)cy, z0);
+      const unsigned long long hi = cell_key((unsigned)cx, (unsigned)cy, z1);
+      if (hi < skeys[a + 1u]) continue;
+      unsigned j = max(lower_bound_u64(skeys, n, lo), a + 1u);
+      for (; j < n && skeys[j] <= hi; ++j)
+        if (pair_d2(variant, pa, dpos[j]) <= link2) ok &= uf_unite(parent, a, j);
+    }
+  }
+  if (!ok) atomicOr(&cnt[C_ERR], 1u);
+}
+
+__global__ void k_dm_roots(unsigned n, unsigned* __restrict__ parent, unsigned* __restrict__ gcnt,
+                           unsigned long long* __restrict__ keys, unsigned* __restrict__ vals) {
+  const unsigned a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= n) return;
+  const unsigned r = uf_find(parent, a);  // the smallest index of a's group
+  atomicAdd(&gcnt[r], 1u);
+  keys[a] = r;
+  vals[a] = a;
+}
+
+// ---- 5. clumps ------------------------------------------------------------------------------------------
+__global__ void k_dm_clumps(unsigned n, const unsigned long long* __restrict__ skeys,
+                            const unsigned* __restrict__ gcnt, uint4* __restrict__ clump,
+                            unsigned* __restrict__ cnt) {
+  const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const unsigned r = (unsigned)skeys[i];
+  if (i > 0 && (unsigned)skeys[i - 1] == r) return;
+  const unsigned s = gcnt[r];
+  if (s < 2u) return;
+  const unsigned c = atomicAdd(&cnt[C_NCLUMP], 1u);
+  const unsigned rows = (s + kPeRows - 1) / kPeRows;
+  clump[c] = make_uint4(i, s, r, (rows + 1) / 2);
+}
+
+// One warp per clump: mass, centre of mass, volume, target mass, then the internal kinetic energy.
+__global__ void __launch_bounds__(kDmThreads) k_dm_clump_stats(const unsigned* __restrict__ cnt,
+                                                               const uint4* __restrict__ clump, int variant,
+                                                               const float4* __restrict__ dpos,
+                                                               const float4* __restrict__ dvel,
+                                                               const float2* __restrict__ drp,
+                                                               double* __restrict__ cstat) {
+  const unsigned ncl = cnt[C_NCLUMP];
+  const unsigned lane = threadIdx.x & 31u;
+  for (unsigned c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < ncl; c += (gridDim.x * blockDim.x) >> 5) {
+    const uint4 cl = clump[c];
+    double a[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (unsigned j = lane; j < cl.y; j += 32u) {
+      const unsigned t = cl.x + j;
+      const float4 p = dpos[t], v = dvel[t];
+      const float2 rp = drp[t];
+      const double mm = v.w;
+      a[0] += mm;
+      a[1] += (double)v.x * mm;
+      a[2] += (double)v.y * mm;
+      a[3] += (double)v.z * mm;
+      a[4] += (double)p.x * mm;
+      a[5] += (double)p.y * mm;
+      a[6] += (double)p.z * mm;
+      const double rho = variant == 0 ? (double)rp.x : (double)fmaxf(rp.x, 1.0f);  // gpu_sph.rs:450
+      a[7] += mm / rho;
+      a[8] += __float_as_uint(rp.y) == 0u ? mm : 0.0;
+    }
+#pragma unroll
+    for (int k = 0; k < 9; ++k) a[k] = warp_sum(a[k]);
+    const double M = a[0];
+    const double cvx = a[1] / M, cvy = a[2] / M, cvz = a[3] / M;
+    double ke = 0.0;
+    for (unsigned j = lane; j < cl.y; j += 32u) {
+      const float4 v = dvel[cl.x + j];
+      const double dx = (double)v.x - cvx, dy = (double)v.y - cvy, dz = (double)v.z - cvz;
+      ke += 0.5 * (double)v.w * dsq3(dx, dy, dz);
+    }
+    ke = warp_sum(ke);
+    if (lane == 0) {
+      double* o = cstat + (size_t)c * 8;
+      o[0] = M;
+      o[1] = a[4] / M;
+      o[2] = a[5] / M;
+      o[3] = a[6] / M;
+      o[4] = a[7];
+      o[5] = a[8];
+      o[6] = ke;
+      o[7] = 0.0;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(1024) k_dm_unit_scan(unsigned* __restrict__ cnt, const uint4* __restrict__ clump,
+                                                       unsigned* __restrict__ uoff) {
+  __shared__ unsigned s_warp[33];
+  const unsigned ncl = cnt[C_NCLUMP];
+  const unsigned per = (ncl + blockDim.x - 1) / blockDim.x;
+  const unsigned c0 = threadIdx.x * per;
+  unsigned sum = 0;
+  for (unsigned k = 0; k < per; ++k)
+    if (c0 + k < ncl) sum += clump[c0 + k].w;
+  unsigned total;
+  unsigned run = block_exclusive_scan(sum, s_warp, total);
+  for (unsigned k = 0; k < per; ++k)
+    if (c0 + k < ncl) {
+      uoff[c0 + k] = run;
+      run += clump[c0 + k].w;
+    }
+  if (threadIdx.x == 0) {
+    uoff[ncl] = total;
+    cnt[C_UNITS] = total;
+  }
+}
+
+// Self-potential units: unit u of a clump with T rows covers rows u and T-1-u of the upper pair triangle.
+// upe[unit] = Σ_a m_a Σ_{b>a} m_b / r_ab with the reference's pair distance (floored or softened).
+__global__ void __launch_bounds__(kPeRows) k_dm_pe(const unsigned* __restrict__ cnt, const uint4* __restrict__ clump,
+                                                   const unsigned* __restrict__ uoff, int variant, double floor_r,
+                                                   double soft2, const float4* __restrict__ dpos,
+                                                   const float4* __restrict__ dvel, double* __restrict__ upe) {
+  __shared__ float4 sp[kPeRows];
+  __shared__ double s_red[kPeRows / 32];
+  const unsigned ncl = cnt[C_NCLUMP], units = cnt[C_UNITS];
+  for (unsigned u = blockIdx.x; u < units; u += gridDim.x) {
+    unsigned lo = 0, hi = ncl;  // the clump holding unit u: last c with uoff[c] <= u
+    while (hi - lo > 1) {
+      const unsigned mid = (lo + hi) >> 1;
+      if (uoff[mid] <= u) lo = mid;
+      else hi = mid;
+    }
+    const uint4 cl = clump[lo];
+    const unsigned rows = (cl.y + kPeRows - 1) / kPeRows;
+    const unsigned lu = u - uoff[lo];
+    double acc = 0.0;
+    for (int pass = 0; pass < 2; ++pass) {
+      const unsigned row = pass == 0 ? lu : rows - 1u - lu;
+      if (pass == 1 && row == lu) break;
+      const unsigned ia = row * kPeRows + threadIdx.x;
+      const bool va = ia < cl.y;
+      const float4 pa = va ? dpos[cl.x + ia] : make_float4(0.f, 0.f, 0.f, 0.f);
+      const double ma = va ? (double)dvel[cl.x + ia].w : 0.0;
+      double row_acc = 0.0;
+      for (unsigned tj = row; tj < rows; ++tj) {
+        const unsigned ib = tj * kPeRows + threadIdx.x;
+        __syncthreads();
+        if (ib < cl.y) {
+          float4 q = dpos[cl.x + ib];
+          q.w = dvel[cl.x + ib].w;
+          sp[threadIdx.x] = q;
+        }
+        __syncthreads();
+        const unsigned nb = min((unsigned)kPeRows, cl.y - tj * kPeRows);
+        if (va) {
+          const unsigned j0 = tj == row ? threadIdx.x + 1u : 0u;
+          for (unsigned j = j0; j < nb; ++j) {
+            const float4 q = sp[j];
+            const double d2 = pair_d2(variant, pa, q);
+            const double r = variant == 0 ? fmax(__dsqrt_rn(d2), floor_r) : __dsqrt_rn(__dadd_rn(d2, soft2));
+            row_acc += (double)q.w / r;
+          }
+        }
+      }
+      acc += ma * row_acc;
+    }
+    acc = warp_sum(acc);
+    if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int w = 0; w < kPeRows / 32; ++w) t += s_red[w];
+      upe[u] = t;
+    }
+    __syncthreads();
+  }
+}
+
+// Boundness, the Roche gate and the heaviest bound clump outside it (ties: the smaller root).
+__global__ void __launch_bounds__(kDmThreads) k_dm_select(const unsigned* __restrict__ cnt,
+                                                          const uint4* __restrict__ clump,
+                                                          const unsigned* __restrict__ uoff,
+                                                          const double* __restrict__ upe,
+                                                          const double* __restrict__ cstat,
+                                                          const double* __restrict__ scal, int variant, double G,
+                                                          double roche, double rho_fallback, double* __restrict__ out) {
+  __shared__ double s_m[kDmThreads], s_e[kDmThreads];
+  __shared__ unsigned s_root[kDmThreads], s_n[kDmThreads], s_bound[kDmThreads], s_cl[kDmThreads];
+  const unsigned ncl = cnt[C_NCLUMP];
+  const double cx = scal[S_COM], cy = scal[S_COM + 1], cz = scal[S_COM + 2];
+  const double r_rem = scal[S_RREM], rho_rem = scal[S_RHOREM];
+  double bm = 0.0, be = 0.0;
+  unsigned broot = 0xffffffffu, bn = 0, nb = 0, nc = 0;
+  for (unsigned c = threadIdx.x; c < ncl; c += blockDim.x) {
+    const double* st = cstat + (size_t)c * 8;
+    const double M = st[0];
+    if (variant == 1 && !(M > 0.0)) continue;  // accretion.rs:121 skips massless groups
+    ++nc;
+    double sum = 0.0;
+    for (unsigned u = uoff[c]; u < uoff[c + 1]; ++u) sum += upe[u];
+    const double pe = -G * sum;
+    const bool bound = st[6] + pe < 0.0;
+    const double rho_c = st[4] > 0.0 ? M / st[4] : rho_fallback;
+    const double d_roche = roche * r_rem * cbrt(rho_rem / rho_c);
+    const double dx = st[1] - cx, dy = st[2] - cy, dz = st[3] - cz;
+    const double dist = sqrt(dx * dx + dy * dy + dz * dz);
+    nb += bound ? 1u : 0u;
+    const uint4 cl = clump[c];
+    if (bound && dist > d_roche && (M > bm || (M == bm && M > 0.0 && cl.z < broot))) {
+      bm = M;
+      be = st[5];
+      broot = cl.z;
+      bn = cl.y;
+    }
+  }
+  s_m[threadIdx.x] = bm;
+  s_e[threadIdx.x] = be;
+  s_root[threadIdx.x] = broot;
+  s_n[threadIdx.x] = bn;
+  s_bound[threadIdx.x] = nb;
+  s_cl[threadIdx.x] = nc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = 1; k < kDmThreads; ++k) {
+      nb += s_bound[k];
+      nc += s_cl[k];
+      if (s_m[k] > bm || (s_m[k] == bm && s_m[k] > 0.0 && s_root[k] < broot)) {
+        bm = s_m[k];
+        be = s_e[k];
+        broot = s_root[k];
+        bn = s_n[k];
+      }
+    }
+    out[10] = bm;
+    out[11] = bm > 0.0 ? 100.0 * be / bm : 0.0;
+    out[12] = (double)bn;
+    out[13] = (double)nc;
+    out[14] = (double)nb;
+  }
+}
+
+int bits_of(unsigned v) {
+  int b = 0;
+  while (b < 32 && (v >> b)) ++b;
+  return b;
+}
+
+size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// Carve the workspace for m particles from one allocation.
+bool work_reserve(DiskWork* w, int m) {
+  if (w->cap >= m && w->base) return true;
+  if (w->base) cudaFree(w->base);
+  w->base = nullptr;
+  w->cap = 0;
+  const size_t n = (size_t)(m < 1 ? 1 : m), half = n / 2 + 2, tiles = radix_tiles((int)n);
+  size_t sz = 0;
+  auto take = [&](size_t bytes) {
+    const size_t o = sz;
+    sz += align256(bytes);
+    return o;
+  };
+  const size_t o_k0 = take(8 * n), o_k1 = take(8 * n), o_v0 = take(4 * n), o_v1 = take(4 * n);
+  const size_t o_hist = take(4 * 256 * tiles), o_tot = take(4 * 256), o_part = take(8 * kDmBlocks * kDmVals);
+  const size_t o_tsum = take(8 * tiles), o_scal = take(8 * S_COUNT), o_cnt = take(4 * C_COUNT);
+  const size_t o_bcnt = take(4 * kDmBlocks), o_cat = take(n);
+  const size_t o_p0 = take(16 * n), o_p1 = take(16 * n), o_u0 = take(16 * n), o_u1 = take(16 * n);
+  const size_t o_r0 = take(8 * n), o_r1 = take(8 * n), o_par = take(4 * n), o_g = take(4 * n);
+  const size_t o_cl = take(16 * half), o_uo = take(4 * (half + 1)), o_cs = take(64 * half), o_upe = take(8 * (n + 1));
+  const size_t o_out = take(8 * 16);
+  void* base = nullptr;
+  if (cudaMalloc(&base, sz) != cudaSuccess) return false;
+  char* b = (char*)base;
+  w->base = base;
+  w->cap = (int)n;
+  w->keys[0] = (unsigned long long*)(b + o_k0);
+  w->keys[1] = (unsigned long long*)(b + o_k1);
+  w->vals[0] = (unsigned*)(b + o_v0);
+  w->vals[1] = (unsigned*)(b + o_v1);
+  w->hist = (unsigned*)(b + o_hist);
+  w->tot = (unsigned*)(b + o_tot);
+  w->part = (double*)(b + o_part);
+  w->tsum = (double*)(b + o_tsum);
+  w->scal = (double*)(b + o_scal);
+  w->cnt = (unsigned*)(b + o_cnt);
+  w->bcnt = (unsigned*)(b + o_bcnt);
+  w->cat = (unsigned char*)(b + o_cat);
+  w->dpos[0] = (float4*)(b + o_p0);
+  w->dpos[1] = (float4*)(b + o_p1);
+  w->dvel[0] = (float4*)(b + o_u0);
+  w->dvel[1] = (float4*)(b + o_u1);
+  w->drp[0] = (float2*)(b + o_r0);
+  w->drp[1] = (float2*)(b + o_r1);
+  w->parent = (unsigned*)(b + o_par);
+  w->gcnt = (unsigned*)(b + o_g);
+  w->clump = (uint4*)(b + o_cl);
+  w->uoff = (unsigned*)(b + o_uo);
+  w->cstat = (double*)(b + o_cs);
+  w->upe = (double*)(b + o_upe);
+  w->out = (double*)(b + o_out);
+  return true;
+}
+
+}  // namespace
+
+void disk_work_free(DiskWork* w) {
+  if (!w) return;
+  if (w->base) cudaFree(w->base);
+  delete w;
+}
+
+int disk_measure(const Dev& d, unsigned off, unsigned m, const DiskCfg& c, DiskWork*& w, double* out,
+                 unsigned long long* launches, const char** err, cudaStream_t s) {
+  std::memset(out, 0, 16 * sizeof(double));
+  *launches = 0;
+  if (m == 0) return 0;
+  if (!w) w = new DiskWork();
+  if (!work_reserve(w, (int)m)) {
+    *err = "disk measure: workspace allocation failed";
+    return -3;
+  }
+  const State& st = d.s();
+  unsigned long long L = 0;
+  const unsigned chunk = ((m + kDmBlocks - 1) / kDmBlocks + kDmThreads - 1) / kDmThreads * kDmThreads;
+  const int nb = (int)((m + chunk - 1) / chunk);
+  cudaMemsetAsync(w->cnt, 0, 4 * C_COUNT, s);
+  k_dm_moments<<<nb, kDmThreads, 0, s>>>(st, off, m, chunk, w->part);
+  k_dm_moments_final<<<1, kDmThreads, 0, s>>>(w->part, nb, w->scal);
+  k_dm_radius<<<(m + 255) / 256, 256, 0, s>>>(st, off, m, w->scal, w->keys[0], w->vals[0]);
+  L += 3;
+  int src = 0;
+  L += launch_radix_sort(w->keys, w->vals, (int)m, 64, w->hist, w->tot, src, s);
+  const int tiles = (int)((m + kTile - 1) / kTile);
+  k_dm_tile_mass<<<tiles, kDmThreads, 0, s>>>(st, off, m, w->vals[src], w->tsum);
+  k_dm_cross<<<1, 32, 0, s>>>(st, off, m, tiles, w->keys[src], w->vals[src], w->tsum, w->scal, c.remnant_frac);
+  k_dm_classify<<<nb, kDmThreads, 0, s>>>(st, off, m, chunk, c.variant, c.G, w->scal, w->cat, w->part, w->bcnt);
+  k_dm_classify_final<<<1, 1024, 0, s>>>(w->part, nb, m, c.variant, c.link_factor, w->bcnt, w->scal, w->cnt, w->out);
+  L += 4;
+  unsigned nd = 0;
+  cudaMemcpyAsync(&nd, w->cnt + C_NDISK, 4, cudaMemcpyDeviceToHost, s);
+  cudaError_t e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) {
+    *err = cudaGetErrorString(e);
+    return -2;
+  }
+  if (nd >= 2) {
+    k_dm_compact<<<nb, kDmThreads, 0, s>>>(st, d.rho, off, m, chunk, w->cat, w->bcnt, w->scal, w->dpos[0],
+                                           w->dvel[0], w->drp[0], w->keys[0], w->vals[0]);
+    L += 1;
+    L += launch_radix_sort(w->keys, w->vals, (int)nd, 63, w->hist, w->tot, src, s);
+    const unsigned gb = (nd + 255) / 256;
+    k_dm_gather<<<gb, 256, 0, s>>>(nd, w->vals[src], w->dpos[0], w->dvel[0], w->drp[0], w->dpos[1], w->dvel[1],
+                                   w->drp[1], w->parent, w->gcnt);
+    k_dm_link<<<gb, 256, 0, s>>>(nd, c.variant, w->keys[src], w->dpos[1], w->scal, w->parent, w->cnt);
+    k_dm_roots<<<gb, 256, 0, s>>>(nd, w->parent, w->gcnt, w->keys[0], w->vals[0]);
+    L += 3;
+    L += launch_radix_sort(w->keys, w->vals, (int)nd, bits_of(nd), w->hist, w->tot, src, s);
+    k_dm_gather<<<gb, 256, 0, s>>>(nd, w->vals[src], w->dpos[1], w->dvel[1], w->drp[1], w->dpos[0], w->dvel[0],
+                                   w->drp[0], nullptr, nullptr);
+    k_dm_clumps<<<gb, 256, 0, s>>>(nd, w->keys[src], w->gcnt, w->clump, w->cnt);
+    const unsigned cb = (nd / 2 + 7) / 8;
+    k_dm_clump_stats<<<cb < 1184u ? (cb ? cb : 1u) : 1184u, kDmThreads, 0, s>>>(w->cnt, w->clump, c.variant,
+                                                                               w->dpos[0], w->dvel[0], w->drp[0],
+                                                                               w->cstat);
+    k_dm_unit_scan<<<1, 1024, 0, s>>>(w->cnt, w->clump, w->uoff);
+    k_dm_pe<<<nd < 1184u ? nd : 1184u, kPeRows, 0, s>>>(w->cnt, w->clump, w->uoff, c.variant, c.pe_floor,
+                                                        c.pe_soft * c.pe_soft, w->dpos[0], w->dvel[0], w->upe);
+    k_dm_select<<<1, kDmThreads, 0, s>>>(w->cnt, w->clump, w->uoff, w->upe, w->cstat, w->scal, c.variant, c.G,
+                                         c.roche, c.rho_fallback, w->out);
+    L += 7;
+  }
+  unsigned flags[C_COUNT];
+  cudaMemcpyAsync(out, w->out, 16 * sizeof(double), cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(flags, w->cnt, sizeof(flags), cudaMemcpyDeviceToHost, s);
+  e = cudaStreamSynchronize(s);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    *err = cudaGetErrorString(e);
+    return -2;
+  }
+  *launches = L;
+  if (flags[C_ERR]) {
+    *err = "disk measure: a union-find hook gave up after its retry limit";
+    return -5;
+  }
+  return 0;
+}
+
+}  // namespace sphb

@@ -161,35 +161,6 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_upsweep(const unsigned long l
   hist[threadIdx.x * T + blockIdx.x] = h[threadIdx.x];
 }
 
-// Block-wide exclusive scan of one value per thread (blockDim.x <= 1024). Returns the block total.
-__device__ __forceinline__ unsigned block_exclusive_scan(unsigned v, unsigned* s_warp, unsigned& total) {
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
-  unsigned incl = v;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const unsigned t = __shfl_up_sync(SPH_FULL_MASK, incl, o);
-    if (lane >= o) incl += t;
-  }
-  if (lane == 31) s_warp[w] = incl;
-  __syncthreads();
-  if (w == 0) {
-    unsigned x = lane < nw ? s_warp[lane] : 0u;
-    unsigned xi = x;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const unsigned t = __shfl_up_sync(SPH_FULL_MASK, xi, o);
-      if (lane >= o) xi += t;
-    }
-    if (lane < nw) s_warp[lane] = xi - x;
-    if (lane == 31) s_warp[32] = xi;
-  }
-  __syncthreads();
-  const unsigned res = s_warp[w] + incl - v;
-  total = s_warp[32];
-  __syncthreads();
-  return res;
-}
-
 // One block per digit: exclusive scan of hist[d][0..T) in place; tot[d] = sum.
 __global__ void __launch_bounds__(1024) k_rs_scan(unsigned* __restrict__ hist, unsigned* __restrict__ tot, int T) {
   __shared__ unsigned s_warp[33];
@@ -339,6 +310,25 @@ int launch_sort_permute(Dev& d, cudaStream_t s) {
   // keep the sorted keys in keys[0] for inspection
   if (src != 0) cudaMemcpyAsync(d.keys[0], d.keys[src], sizeof(unsigned long long) * n, cudaMemcpyDeviceToDevice, s);
   return 2 + 3 * passes;
+}
+
+// Stable LSD radix sort of n (key, value) pairs on the low `bits` key bits, ping-ponging between buf 0 and 1.
+// Returns the buffer holding the result in `src`; hist holds 256 × radix_tiles(n) counters.
+int launch_radix_sort(unsigned long long* keys[2], unsigned* vals[2], int n, int bits, unsigned* hist,
+                      unsigned* tot, int& src, cudaStream_t s) {
+  src = 0;
+  if (n <= 1) return 0;
+  const int T = (int)radix_tiles(n);
+  int launches = 0;
+  for (int shift = 0; shift < bits; shift += 8) {
+    k_rs_upsweep<<<T, RS_THREADS, 0, s>>>(keys[src], n, shift, hist, T);
+    k_rs_scan<<<256, 1024, 0, s>>>(hist, tot, T);
+    k_rs_downsweep<<<T, RS_THREADS, 0, s>>>(keys[src], vals[src], keys[src ^ 1], vals[src ^ 1], n, shift, hist,
+                                             tot, T);
+    src ^= 1;
+    launches += 3;
+  }
+  return launches;
 }
 
 // ---------------------------------------------------------------------------------------------------

@@ -46,6 +46,7 @@ struct sph_ctx {
   bool rb_inflight = false;
   uint32_t rb_n = 0;
   double* d_diag = nullptr;
+  DiskWork* disk = nullptr;  // disk-measurement workspace (allocated by the first measurement)
   std::string err;
   int device = 0;
   std::vector<void*> allocs;
@@ -532,6 +533,7 @@ void sph_destroy(sph_ctx* ctx) {
   }
   for (cudaEvent_t e : ctx->pool) cudaEventDestroy(e);
   drop_graphs(ctx);
+  disk_work_free(ctx->disk);
   for (void* p : ctx->allocs) cudaFree(p);
   if (ctx->pinned_aos) cudaFreeHost(ctx->pinned_aos);
   if (ctx->rb_event) cudaEventDestroy(ctx->rb_event);
@@ -723,6 +725,70 @@ sph_status sph_particle_buffer(sph_ctx* ctx, void** device_ptr) {
 
 void* sph_stream(sph_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
 const char* sph_last_error(const sph_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+sph_status sph_measure_default(sph_measure_cfg* cfg) {
+  if (!cfg) return SPH_ERR_INVALID;
+  std::memset(cfg, 0, sizeof(*cfg));
+  cfg->remnant_frac = 0.85;   // main.rs:744
+  cfg->link_factor = 2.0;     // main.rs:810
+  cfg->roche = 2.44;          // main.rs:840
+  cfg->rho_fallback = 2700.0; // main.rs:836
+  cfg->pe_floor = 1.0;        // main.rs:846
+  cfg->pe_softening = 1.0e4;  // gpu_sph.rs:458
+  return SPH_OK;
+}
+
+sph_status sph_measure_disk(sph_ctx* ctx, uint32_t impact, const sph_measure_cfg* cfg, sph_disk_measure* out) {
+  if (!ctx || !cfg || !out) return SPH_ERR_INVALID;
+  std::memset(out, 0, sizeof(*out));
+  if (!ctx->uploaded) {
+    ctx->err = "sph_measure_disk: nothing uploaded";
+    return SPH_ERR_STATE;
+  }
+  if (impact >= (uint32_t)ctx->d.nseg) {
+    ctx->err = "sph_measure_disk: impact " + std::to_string(impact) + " is outside the batch";
+    return SPH_ERR_INVALID;
+  }
+  if (cfg->variant < 0 || cfg->variant > 1 || !(cfg->remnant_frac > 0.0 && cfg->remnant_frac <= 1.0) ||
+      !(cfg->link_factor > 0.0) || !(cfg->roche >= 0.0) || !std::isfinite(cfg->G) || cfg->G < 0.0 ||
+      !(cfg->pe_floor >= 0.0) || !(cfg->pe_softening >= 0.0)) {
+    ctx->err = "sph_measure_disk: variant 0|1, remnant_frac in (0, 1], link_factor > 0, non-negative constants";
+    return SPH_ERR_INVALID;
+  }
+  cudaSetDevice(ctx->device);
+  Seg seg[2];
+  CK(cudaMemcpyAsync(seg, ctx->d.segs + impact, 2 * sizeof(Seg), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  const unsigned off = seg[0].off, m = seg[1].off - off;  // the table closes with entry nseg (off = n)
+  const DiskCfg dc{cfg->variant, cfg->G != 0.0 ? cfg->G : ctx->cfg.G, cfg->remnant_frac, cfg->link_factor,
+                   cfg->roche, cfg->rho_fallback, cfg->pe_floor, cfg->pe_softening};
+  double v[16];
+  unsigned long long launches = 0;
+  const char* msg = "";
+  const int rc = disk_measure(ctx->d, off, m, dc, ctx->disk, v, &launches, &msg, ctx->stream);
+  ctx->launches += launches;
+  if (rc) {
+    ctx->err = msg;
+    return (sph_status)rc;
+  }
+  out->earth_frac = v[0];
+  out->disk_mass = v[1];
+  out->disk_target = v[2];
+  out->disk_impactor = v[3];
+  out->remnant_target = v[4];
+  out->remnant_impactor = v[5];
+  out->escaped_target = v[6];
+  out->escaped_impactor = v[7];
+  out->r_remnant = v[8];
+  out->m_remnant = v[9];
+  out->clump_mass = v[10];
+  out->clump_target_frac = v[11];
+  out->clump_n = (uint32_t)v[12];
+  out->n_clumps = (uint32_t)v[13];
+  out->n_bound = (uint32_t)v[14];
+  out->n_disk = (uint32_t)v[15];
+  return SPH_OK;
+}
 
 sph_status sph_diag(sph_ctx* ctx, sph_diag_out* out) {
   if (!ctx || !out) return SPH_ERR_INVALID;

@@ -156,6 +156,35 @@ __device__ __forceinline__ float tillotson_c(const Eos& e, float rho, float u, f
   return sqrtf(fmaxf(dp + p / (r * r) * dfdu, 0.0f));
 }
 
+// Block-wide exclusive scan of one value per thread (blockDim.x <= 1024). Returns the block total.
+__device__ __forceinline__ unsigned block_exclusive_scan(unsigned v, unsigned* s_warp, unsigned& total) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  unsigned incl = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned t = __shfl_up_sync(SPH_FULL_MASK, incl, o);
+    if (lane >= o) incl += t;
+  }
+  if (lane == 31) s_warp[w] = incl;
+  __syncthreads();
+  if (w == 0) {
+    unsigned x = lane < nw ? s_warp[lane] : 0u;
+    unsigned xi = x;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned t = __shfl_up_sync(SPH_FULL_MASK, xi, o);
+      if (lane >= o) xi += t;
+    }
+    if (lane < nw) s_warp[lane] = xi - x;
+    if (lane == 31) s_warp[32] = xi;
+  }
+  __syncthreads();
+  const unsigned res = s_warp[w] + incl - v;
+  total = s_warp[32];
+  __syncthreads();
+  return res;
+}
+
 // Interleaved neighbour-list slot: warp-group g = t/32 owns a [cap][32] block so that entry k of all 32
 // lanes is one 128-byte line.
 __device__ __forceinline__ size_t nbr_slot(unsigned t, unsigned k, unsigned cap) {

@@ -199,6 +199,9 @@ int launch_bbox(const Dev& d, cudaStream_t s);
 int launch_sort_permute(Dev& d, cudaStream_t s);      // keys → radix sort → permute (swaps d.cur)
 int launch_tree(const Dev& d, const Cfg& c, float theta, cudaStream_t s);  // Karras + moments
 size_t radix_tiles(int n);
+// stable LSD radix sort of (keys, vals) on the low `bits` key bits; the result lands in buffer `src`
+int launch_radix_sort(unsigned long long* keys[2], unsigned* vals[2], int n, int bits, unsigned* hist,
+                      unsigned* tot, int& src, cudaStream_t s);
 
 // ---- gravity ---------------------------------------------------------------------------------------
 int launch_gravity_tree(const Dev& d, const Cfg& c, cudaStream_t s);
@@ -222,5 +225,17 @@ int launch_relax(const Dev& d, cudaStream_t s);
 int launch_from_aos(const Dev& d, cudaStream_t s);
 int launch_to_aos(const Dev& d, cudaStream_t s);
 int launch_diag(const Dev& d, cudaStream_t s, double* out16);
+
+// ---- disk measurement and the Moon candidate (disk.cu) ------------------------------------------------
+struct DiskCfg {
+  int variant;          // 0: the impact-run tool's measure, 1: the engine's disk statistics
+  double G, remnant_frac, link_factor, roche, rho_fallback, pe_floor, pe_soft;
+};
+struct DiskWork;        // device workspace, grown on demand
+void disk_work_free(DiskWork* w);
+// Measures the sorted particles [off, off + m) of the current state into out[16] (host memory; the call
+// synchronises the stream). Returns 0, or a negative status with a message in *err. *launches counts kernels.
+int disk_measure(const Dev& d, unsigned off, unsigned m, const DiskCfg& c, DiskWork*& w, double* out,
+                 unsigned long long* launches, const char** err, cudaStream_t s);
 
 }  // namespace sphb

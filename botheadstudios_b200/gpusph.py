@@ -94,6 +94,22 @@ class GpuSph:
                     "sph_inspect(IMPACT_TIME)")
         return out
 
+    # ---- disk measurement ----------------------------------------------------------------------------
+    def measure_disk(self, impact: int = 0, variant: int = 0, **kw) -> dict:
+        """Disk measurement and Moon candidate of one impact on the device (sph_measure_disk). variant 0 is the
+        impact-run tool's `measure`, 1 the engine's disk statistics; keyword arguments override the
+        sph_measure_cfg defaults (G, remnant_frac, link_factor, roche, rho_fallback, pe_floor, pe_softening)."""
+        cfg = _lib.MeasureCfg()
+        self._L.sph_measure_default(C.byref(cfg))
+        cfg.variant = variant
+        for k, v in kw.items():
+            if not hasattr(cfg, k):
+                raise TypeError(f"unknown measure option {k}")
+            setattr(cfg, k, v)
+        out = _lib.DiskMeasure()
+        self._check(self._L.sph_measure_disk(self._h, impact, C.byref(cfg), C.byref(out)), "sph_measure_disk")
+        return {name: getattr(out, name) for name, _ in out._fields_}
+
     # ---- learned smoothing lengths --------------------------------------------------------------------
     def mlp_set(self, params: np.ndarray):
         p = np.ascontiguousarray(params, dtype=np.float32)

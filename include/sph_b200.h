@@ -184,6 +184,45 @@ uint32_t sph_count(const sph_ctx* ctx);
  * layout in original order, refreshed by this call (the headless stand-in for the render vertex buffer). */
 sph_status sph_particle_buffer(sph_ctx* ctx, void** device_ptr);
 sph_status sph_diag(sph_ctx* ctx, sph_diag_out* out);
+
+/* ---- disk measurement and the Moon candidate of one impact ------------------------------------------------
+ * Replaces the host measurement of a finished impact: variant 0 follows the impact-run tool
+ * (tools/impact-run/src/main.rs:732-878, `measure` + `moon_candidate`), variant 1 the engine's statistics
+ * (crates/engine/src/gpu_sph.rs:399-469 `disk_stats_json` + accretion.rs:73-160 `find_clumps`). The remnant
+ * is the sphere about the centre of mass holding remnant_frac of the mass; each particle's two-body orbit
+ * about it is escaping, remnant (periapsis inside) or disk; friends-of-friends over the disk with a linking
+ * length of link_factor × the mean smoothing length (of the disk in variant 0, of every particle in variant
+ * 1); the Moon candidate is the heaviest self-bound clump (internal KE + pairwise PE < 0, two or more
+ * members) beyond the fluid Roche limit roche × R (ρ_remnant/ρ_clump)^(1/3). Provenance 0 is the target. */
+typedef struct sph_measure_cfg {
+  int32_t variant;         /* 0: the impact-run tool, 1: the engine's disk statistics */
+  int32_t reserved;
+  double G;                /* 0: the context's G */
+  double remnant_frac;     /* 0.85 */
+  double link_factor;      /* 2 */
+  double roche;            /* 2.44 */
+  double rho_fallback;     /* variant 0: clump density when its volume sum is zero (2700) */
+  double pe_floor;         /* variant 0: pair distance floor of the self-potential (1 m) */
+  double pe_softening;     /* variant 1: pair softening of the self-potential (1e4 m) */
+} sph_measure_cfg;
+
+typedef struct sph_disk_measure {
+  double earth_frac;                          /* % of the disk mass from the target (prov 0) */
+  double disk_mass, disk_target, disk_impactor;
+  double remnant_target, remnant_impactor;
+  double escaped_target, escaped_impactor;
+  double r_remnant, m_remnant;
+  double clump_mass;                          /* the Moon candidate, 0 when there is none */
+  double clump_target_frac;                   /* % of the candidate's mass from the target */
+  uint32_t clump_n;                           /* its particles */
+  uint32_t n_clumps;                          /* disk groups of two or more particles */
+  uint32_t n_bound;                           /* ... of which self-bound */
+  uint32_t n_disk;                            /* disk particles */
+} sph_disk_measure;
+
+sph_status sph_measure_default(sph_measure_cfg* cfg);
+/* Measures impact `impact` (0 for a single upload) of the current state. Synchronises the context's stream. */
+sph_status sph_measure_disk(sph_ctx* ctx, uint32_t impact, const sph_measure_cfg* cfg, sph_disk_measure* out);
 /* The context's CUDA stream (cudaStream_t), for callers that order their own work after the step. */
 void* sph_stream(sph_ctx* ctx);
 const char* sph_last_error(const sph_ctx* ctx);

@@ -412,3 +412,21 @@ def mlp_grad(params, x, t, bf16: bool = True):
     g = np.zeros(mlp_param_count(True), np.float64)
     loss = L.orc_mlp_grad(_c(params, np.float32), x, _c(t, np.float32), len(x), 1 if bf16 else 0, g)
     return float(loss), g
+
+
+# ---- disk measurement and the Moon candidate (tools/impact-run/src/main.rs:732-878) -------------------
+MEASURE_KEYS = ("earth_frac", "disk_mass", "disk_target", "disk_impactor", "remnant_target", "remnant_impactor",
+                "escaped_target", "escaped_impactor", "r_remnant", "m_remnant", "clump_mass", "clump_target_frac",
+                "clump_n", "n_clumps", "n_bound", "n_disk")
+
+
+def measure_disk(particles, G, variant=0, remnant_frac=0.85, link_factor=2.0, roche=2.44, rho_fallback=2700.0,
+                 pe_floor=1.0, pe_soft=1.0e4) -> dict:
+    """The reference's disk measurement of one impact's 48-byte particle array (a dict keyed by MEASURE_KEYS):
+    variant 0 = the impact-run tool's `measure`, variant 1 = the engine's `disk_stats_json`."""
+    L = lib()
+    L.orc_measure_disk.argtypes = [f32p, C.c_int, C.c_int] + [C.c_double] * 7 + [f64p]
+    p = np.ascontiguousarray(np.ascontiguousarray(particles).view(np.float32).reshape(-1, 12))
+    out = np.zeros(16, np.float64)
+    L.orc_measure_disk(p, len(p), variant, G, remnant_frac, link_factor, roche, rho_fallback, pe_floor, pe_soft, out)
+    return dict(zip(MEASURE_KEYS, out.tolist()))

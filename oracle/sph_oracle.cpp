@@ -1244,3 +1244,233 @@ double orc_mlp_grad(const float* P, const float* x, const float* t, int n, int b
 }
 
 }  // extern "C"
+
+namespace {
+
+// ---------------------------------------------------------------------------------------------------
+// Disk measurement and the Moon candidate, in the reference's two forms:
+//   variant 0: tools/impact-run/src/main.rs:732-878 (`measure`, `moon_candidate`) with `sum_oi` (:195),
+//              `com` (:207) and `perigee` (:232);
+//   variant 1: crates/engine/src/gpu_sph.rs:399-469 (`disk_stats_json`) with accretion.rs:73-160
+//              (`find_clumps`) and orbit.rs:91-116 (`is_bound`, `perigee`).
+// Provenance decides target vs impactor (prov 0 = the target; the tool's index test i < n_earth agrees with
+// it for the tool's particle layout). The union-find partition does not depend on the pair order, so the
+// tool's O(k²) loop stands in for the engine's grid pairs.
+// ---------------------------------------------------------------------------------------------------
+double sum_oi(std::vector<double>& t) {
+  std::sort(t.begin(), t.end(), [](double a, double b) { return std::fabs(a) < std::fabs(b); });
+  double s = 0.0, c = 0.0;
+  for (double x : t) {
+    const double y = x - c, z = s + y;
+    c = (z - s) - y;
+    s = z;
+  }
+  return s;
+}
+
+// 0 = escapes, 1 = disk (periapsis beyond the remnant), 2 = remnant
+int classify(int variant, const double p[3], const double v[3], double mu, double r_rem) {
+  const double r = std::sqrt(p[0] * p[0] + p[1] * p[1] + p[2] * p[2]);
+  const double v2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+  const double h[3] = {p[1] * v[2] - p[2] * v[1], p[2] * v[0] - p[0] * v[2], p[0] * v[1] - p[1] * v[0]};
+  const double h2 = h[0] * h[0] + h[1] * h[1] + h[2] * h[2];
+  if (variant == 0) {  // main.rs:232-247: r = 0 is Some(0); energy >= 0 is None
+    if (r == 0.0) return 2;
+    const double energy = 0.5 * v2 - mu / r;
+    if (energy >= 0.0) return 0;
+    const double a = -mu / (2.0 * energy);
+    const double e = std::sqrt(std::max(1.0 + 2.0 * energy * h2 / (mu * mu), 0.0));
+    return a * (1.0 - e) > r_rem ? 1 : 2;
+  }
+  // orbit.rs:91-116: bound needs r > 0; the bound periapsis uses |h|·|h|
+  if (!(r > 0.0 && 0.5 * v2 - mu / r < 0.0)) return 0;
+  const double energy = 0.5 * v2 - mu / r;
+  const double hl = std::sqrt(h2);
+  const double e = std::sqrt(std::max(1.0 + 2.0 * energy * hl * hl / (mu * mu), 0.0));
+  const double a = -mu / (2.0 * energy);
+  return a * (1.0 - e) > r_rem ? 1 : 2;
+}
+
+}  // namespace
+
+extern "C" {
+
+// P48 particles (x y z h vx vy vz u mass mat rho prov) of one impact. The reference's constants are
+// parameters: remnant_frac 0.85, link_factor 2, roche 2.44, and for variant 0 rho_fallback 2700 and a pair
+// distance floor of 1 m, for variant 1 a pair softening of 1e4 m. out[16]: earth_frac, disk, e_disk, t_disk,
+// e_rem, t_rem, e_esc, t_esc, r_remnant, m_remnant, clump_kg, clump_earth_frac, clump_n, n_clumps, n_bound, n_disk.
+void orc_measure_disk(const float* P, int n, int variant, double G, double remnant_frac, double link_factor,
+                      double roche, double rho_fallback, double pe_floor, double pe_soft, double* out) {
+  auto f = [&](int i, int k) { return P[12 * (size_t)i + k]; };
+  auto prov = [&](int i) { uint32_t u; std::memcpy(&u, &P[12 * (size_t)i + 11], 4); return u; };
+  std::fill(out, out + 16, 0.0);
+  if (n == 0) return;
+  double m_total = 0.0, com[3] = {0.0, 0.0, 0.0}, vcom[3] = {0.0, 0.0, 0.0};
+  if (variant == 0) {
+    std::vector<double> mv(n), vx(n), vy(n), vz(n);
+    for (int i = 0; i < n; ++i) {
+      const double m = f(i, 8);
+      mv[i] = m;
+      vx[i] = (double)f(i, 4) * m;
+      vy[i] = (double)f(i, 5) * m;
+      vz[i] = (double)f(i, 6) * m;
+    }
+    m_total = sum_oi(mv);
+    double mm = 0.0;
+    for (int i = 0; i < n; ++i) {
+      for (int k = 0; k < 3; ++k) com[k] += (double)f(i, k) * (double)f(i, 8);
+      mm += (double)f(i, 8);
+    }
+    for (int k = 0; k < 3; ++k) com[k] /= mm;
+    vcom[0] = sum_oi(vx) / m_total;
+    vcom[1] = sum_oi(vy) / m_total;
+    vcom[2] = sum_oi(vz) / m_total;
+  } else {
+    for (int i = 0; i < n; ++i) m_total += (double)f(i, 8);
+    for (int i = 0; i < n; ++i)
+      for (int k = 0; k < 3; ++k) {
+        com[k] += (double)f(i, k) * (double)f(i, 8);
+        vcom[k] += (double)f(i, 4 + k) * (double)f(i, 8);
+      }
+    for (int k = 0; k < 3; ++k) {
+      com[k] /= m_total;
+      vcom[k] /= m_total;
+    }
+  }
+  std::vector<std::pair<double, double>> radii(n);
+  for (int i = 0; i < n; ++i) {
+    const double d[3] = {(double)f(i, 0) - com[0], (double)f(i, 1) - com[1], (double)f(i, 2) - com[2]};
+    radii[i] = {std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]), (double)f(i, 8)};
+  }
+  std::stable_sort(radii.begin(), radii.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+  double cum = 0.0, r_rem = radii.back().first, m_rem = m_total;
+  for (const auto& rm : radii) {
+    cum += rm.second;
+    if (cum >= remnant_frac * m_total) {
+      r_rem = rm.first;
+      m_rem = cum;
+      break;
+    }
+  }
+  const double mu = G * m_rem;
+  std::vector<double> cat[6];  // e_disk, t_disk, e_rem, t_rem, e_esc, t_esc
+  std::vector<int> disk;
+  for (int i = 0; i < n; ++i) {
+    const double rp[3] = {(double)f(i, 0) - com[0], (double)f(i, 1) - com[1], (double)f(i, 2) - com[2]};
+    const double rv[3] = {(double)f(i, 4) - vcom[0], (double)f(i, 5) - vcom[1], (double)f(i, 6) - vcom[2]};
+    const int c = classify(variant, rp, rv, mu, r_rem);
+    const int slot = (c == 1 ? 0 : c == 2 ? 2 : 4) + (prov(i) == 0u ? 0 : 1);
+    cat[slot].push_back((double)f(i, 8));
+    if (c == 1) disk.push_back(i);
+  }
+  double sums[6];
+  for (int k = 0; k < 6; ++k) sums[k] = sum_oi(cat[k]);
+  const double dk = sums[0] + sums[1];
+  out[0] = dk > 0.0 ? 100.0 * sums[0] / dk : 0.0;
+  out[1] = dk;
+  for (int k = 0; k < 6; ++k) out[2 + k] = sums[k];
+  out[8] = r_rem;
+  out[9] = m_rem;
+  out[15] = (double)disk.size();
+  const int k = (int)disk.size();
+  if (k < 2) return;
+  // friends-of-friends over the disk particles, linking length = link_factor × mean smoothing length (of the
+  // disk in variant 0, of every particle in variant 1)
+  double mean_h = 0.0;
+  if (variant == 0) {
+    for (int i : disk) mean_h += (double)f(i, 3);
+    mean_h /= k;
+  } else {
+    for (int i = 0; i < n; ++i) mean_h += (double)f(i, 3);
+    mean_h /= n;
+  }
+  const double link = link_factor * mean_h, link2 = link * link;
+  auto dist2 = [&](int ia, int ib) {
+    double d2 = 0.0;
+    for (int c = 0; c < 3; ++c) {
+      // variant 0 subtracts in f32 and widens; variant 1 widens and subtracts in f64
+      const double dd = variant == 0 ? (double)(f(ia, c) - f(ib, c)) : (double)f(ia, c) - (double)f(ib, c);
+      d2 += dd * dd;
+    }
+    return d2;
+  };
+  std::vector<int> parent(k);
+  std::iota(parent.begin(), parent.end(), 0);
+  auto find = [&](int i) {
+    int r = i;
+    while (parent[r] != r) r = parent[r];
+    while (parent[i] != r) {
+      const int nx = parent[i];
+      parent[i] = r;
+      i = nx;
+    }
+    return r;
+  };
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int a = 0; a < k; ++a)
+    for (int b = a + 1; b < k; ++b)
+      if (dist2(disk[a], disk[b]) <= link2) {
+#pragma omp critical(orc_fof)
+        {
+          const int ra = find(a), rb = find(b);
+          if (ra != rb) parent[ra] = rb;
+        }
+      }
+  std::vector<std::vector<int>> groups(k);
+  for (int a = 0; a < k; ++a) groups[find(a)].push_back(disk[a]);
+  const double rho_rem = m_rem / (4.0 / 3.0 * kPi * r_rem * r_rem * r_rem);
+  double best_m = 0.0, best_e = 0.0;
+  int best_n = 0, n_bound = 0, n_clumps = 0;
+  for (const auto& mem : groups) {
+    if (mem.size() < 2) continue;
+    double m = 0.0, cv[3] = {0, 0, 0}, cp[3] = {0, 0, 0}, vol = 0.0;
+    for (int i : mem) m += (double)f(i, 8);
+    if (variant == 1 && m <= 0.0) continue;  // accretion.rs:121
+    ++n_clumps;
+    for (int i : mem) {
+      for (int c = 0; c < 3; ++c) {
+        cv[c] += (double)f(i, 4 + c) * (double)f(i, 8);
+        cp[c] += (double)f(i, c) * (double)f(i, 8);
+      }
+      const double rho = variant == 0 ? (double)f(i, 10) : (double)std::max(f(i, 10), 1.0f);
+      vol += (double)f(i, 8) / rho;
+    }
+    for (int c = 0; c < 3; ++c) {
+      cv[c] /= m;
+      cp[c] /= m;
+    }
+    const double rho_c = vol > 0.0 ? m / vol : rho_fallback;
+    double ke = 0.0, pe = 0.0;
+    for (int i : mem) {
+      const double dv[3] = {(double)f(i, 4) - cv[0], (double)f(i, 5) - cv[1], (double)f(i, 6) - cv[2]};
+      ke += 0.5 * (double)f(i, 8) * (dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2]);
+    }
+    const double s2 = pe_soft * pe_soft;
+#pragma omp parallel for reduction(+ : pe) schedule(dynamic, 16) if (mem.size() > 512)
+    for (size_t a = 0; a < mem.size(); ++a)
+      for (size_t b = a + 1; b < mem.size(); ++b) {
+        const double d2 = dist2(mem[a], mem[b]);
+        const double r = variant == 0 ? std::max(std::sqrt(d2), pe_floor) : std::sqrt(d2 + s2);
+        pe -= G * (double)f(mem[a], 8) * (double)f(mem[b], 8) / r;
+      }
+    const bool bound = ke + pe < 0.0;
+    const double d_roche = roche * r_rem * std::cbrt(rho_rem / rho_c);
+    const double dist = std::sqrt((cp[0] - com[0]) * (cp[0] - com[0]) + (cp[1] - com[1]) * (cp[1] - com[1]) +
+                                  (cp[2] - com[2]) * (cp[2] - com[2]));
+    if (bound) ++n_bound;
+    if (bound && dist > d_roche && m > best_m) {
+      best_m = m;
+      best_e = 0.0;
+      for (int i : mem)
+        if (prov(i) == 0u) best_e += (double)f(i, 8);
+      best_n = (int)mem.size();
+    }
+  }
+  out[10] = best_m;
+  out[11] = best_m > 0.0 ? 100.0 * best_e / best_m : 0.0;
+  out[12] = best_n;
+  out[13] = n_clumps;
+  out[14] = n_bound;
+}
+
+}  // extern "C"
