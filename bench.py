@@ -10,6 +10,7 @@ neighbour lists, tree) is larger than the 126 MB L2, so no flush is needed betwe
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--workload impact_1m|impact_4m|impact_10k|batch_256|...]
     python bench.py --impl reference ...    # the reference's CPU path (HydroBody::step) on the host cores
+    python bench.py --path measure [--measure-workload post_impact_1m] [--variant 0|1]   # disk measurement
 
 Multi-GPU: replicas (one independent impact per rank, no collective on the data path); value is the sum
 over ranks divided by the slowest rank's time.
@@ -440,6 +441,104 @@ def run_ours(args, wl, world, rank, local, pg):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------------------------------------------------
+# The disk measurement of a finished impact (sph_measure_disk; impact-run main.rs:732-878): one "step" is one
+# measurement of a post-impact field held on the device; e2e adds the upload of the field from host memory.
+# ---------------------------------------------------------------------------------------------------------
+MEASURE_METRIC = "disk-measurement particles/s"
+
+
+def _measure_field(args, rank):
+    from botheadstudios_b200 import ic, workloads
+    return ic.post_impact_scene(seed=1 + rank, **workloads.MEASURE_WORKLOADS[args.measure_workload])
+
+
+def run_measure(args, world, rank, local, pg):
+    import torch
+    from botheadstudios_b200 import ic
+    from botheadstudios_b200.gpusph import GpuSph
+    from botheadstudios_b200.materials import SI, eos_table
+
+    p = _measure_field(args, rank)
+    n, eos = len(p), eos_table()
+    flush = torch.empty(64 << 20, dtype=torch.float32, device=f"cuda:{local}")  # 256 MB > L2
+    with GpuSph(n, device=local, **ic.config_kwargs(SI)) as s:
+        ext = torch.cuda.ExternalStream(s.stream(), device=f"cuda:{local}")
+        s.upload(p, eos, 1.0e4)
+        for _ in range(args.warmup):
+            res = s.measure_disk(0, variant=args.variant)
+        launches0 = s.profile_read()["kernel_launches"]
+
+        def one(e2e: bool) -> float:
+            with torch.cuda.stream(ext):
+                flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(ext)
+            if e2e:
+                s.upload(p, eos, 1.0e4)
+            s.measure_disk(0, variant=args.variant)
+            e1.record(ext)
+            e1.synchronize()
+            return e0.elapsed_time(e1)
+
+        barrier(pg)
+        torch.cuda.synchronize(local)
+        dev = [one(False) for _ in range(args.steps)]
+        launches = (s.profile_read()["kernel_launches"] - launches0) // max(args.steps, 1)
+        e2e = [one(True) for _ in range(args.steps)]
+        barrier(pg)
+        res = s.measure_disk(0, variant=args.variant)
+    ms = max_over_ranks(pg, sum(dev) / len(dev), local)
+    ms_e2e = max_over_ranks(pg, sum(e2e) / len(e2e), local)
+    if rank != 0:
+        return
+    cpu = None
+    if not args.no_cpu and world == 1:
+        cpu = measure_reference_run(p, args.variant)
+    line = dict(metric=MEASURE_METRIC, value=n * world / (ms / 1000.0), unit="particles/s", n_gpus=world,
+                steps=args.steps, warmup=args.warmup, ms_per_step=ms, higher_is_better=True, scaling="weak",
+                vs_baseline=None, dtype="f64", data="synthetic",
+                config=dict(workload=args.measure_workload, particles=n, disk_particles=res["n_disk"],
+                            variant=args.variant, l2="flushed (256 MB write) before every measurement"),
+                e2e=dict(value=n * world / (ms_e2e / 1000.0), unit="particles/s", h2d_bytes_per_step=48 * n,
+                         d2h_bytes_per_step=112),
+                gpu_launches=int(launches), result=res)
+    if cpu is not None:
+        line["cpu_baseline"] = dict(value=n / cpu["seconds"], unit="particles/s", cores=cpu["cores"], kind="port",
+                                    sample=cpu["sample"])
+    print(json.dumps(line), flush=True)
+
+
+def measure_reference_run(p, variant: int) -> dict:
+    import oracle
+    from botheadstudios_b200.materials import G_SI
+    t0 = time.perf_counter()
+    oracle.measure_disk(p, G_SI, variant=variant)
+    el = time.perf_counter() - t0
+    cores = oracle.max_threads()
+    form = "impact-run measure + moon_candidate" if variant == 0 else "disk_stats_json + find_clumps"
+    return dict(seconds=el, cores=cores,
+                sample=f"{form} restated in C++ (O(k^2) friends-of-friends pairs on {cores} OpenMP threads) on "
+                       f"the whole {len(p):,}-particle field, one measurement in {el:.2f} s")
+
+
+def run_measure_reference(args, world, rank, local, pg):
+    if rank != 0:
+        return
+    p = _measure_field(args, 0)
+    runs = [measure_reference_run(p, args.variant) for _ in range(max(1, min(args.steps, 3)))]
+    sec = sum(r["seconds"] for r in runs) / len(runs)
+    v = len(p) / sec
+    line = dict(metric=MEASURE_METRIC, value=v, unit="particles/s", impl="reference", n_gpus=args.gpus,
+                steps=len(runs), warmup=0, ms_per_step=1000.0 * sec, higher_is_better=True, scaling="weak",
+                vs_baseline=None, dtype="f64", data="synthetic",
+                config=dict(workload=args.measure_workload, particles=len(p), variant=args.variant),
+                cpu_baseline=dict(value=v, unit="particles/s", cores=runs[0]["cores"], kind="port",
+                                  sample=runs[0]["sample"]),
+                e2e=dict(value=v, unit="particles/s", h2d_bytes_per_step=0, d2h_bytes_per_step=0))
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -449,11 +548,19 @@ def main():
     ap.add_argument("--workload", default="impact_1m", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
     ap.add_argument("--no-plain", action="store_true", help="batch workloads: skip the sequential plain-form leg")
+    ap.add_argument("--path", default="step", choices=["step", "measure"],
+                    help="measure: the disk measurement of a finished impact instead of the KDK step")
+    ap.add_argument("--measure-workload", default="post_impact_1m",
+                    choices=["post_impact_200k", "post_impact_1m", "post_impact_4m"])
+    ap.add_argument("--variant", type=int, default=0, choices=[0, 1],
+                    help="measure: 0 = the impact-run tool, 1 = the engine's disk statistics")
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]
     world, rank, local, pg = dist_setup(args)
     try:
-        if args.impl == "reference":
+        if args.path == "measure":
+            (run_measure_reference if args.impl == "reference" else run_measure)(args, world, rank, local, pg)
+        elif args.impl == "reference":
             run_reference(args, wl, world, rank, local, pg)
         else:
             run_ours(args, wl, world, rank, local, pg)

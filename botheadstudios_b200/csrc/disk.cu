@@ -15,16 +15,18 @@
 //
 // Here every step is a kernel over the impact's particle range of the state (already contiguous per impact):
 // deterministic two-pass f64 reductions; the radius sort is the tree's 8-bit LSD radix sort over the exact
-// f64 bit patterns of the radii; the 85 % crossing is a tile prefix walk; classification writes per-block
-// partials and an order-preserving compaction of the disk; the friends-of-friends search sorts the disk by
-// a lexicographic cell key (cell edge just above the linking length, so every linked pair lies in the 3 × 3
-// column of z-runs around a particle) and unites pairs with a lock-free union-find (hooking the larger root
+// f64 bit patterns of the radii; the 85 % crossing is a block prefix over tile masses, then over the crossing
+// tile's particles; classification writes per-block partials and an order-preserving compaction of the disk;
+// the friends-of-friends search sorts the disk by a lexicographic cell key (cell edge just above the linking
+// length, so every linked pair lies in the 3 × 3 column of z-runs around a particle), and one warp per
+// particle scans its partners and unites linked pairs with a lock-free union-find (hooking the larger root
 // under the smaller with atomicCAS, path halving; parent[i] <= i always, so every walk ends); clumps are
-// contiguous after a radix sort by root; the self-potential is split into units of two 128-particle rows of
-// the clump's upper pair triangle (rows u and T-1-u, so units carry equal work), each unit summing its pairs
-// in f64. The per-particle arithmetic that decides a classification (radii, periapsis, pair distances) is
-// written with explicitly rounded operations in the reference's order; the sums differ from the
-// reference's sequential ones only in association.
+// contiguous after a radix sort by root; one block per clump sums its moments; the self-potential is split
+// into 128 × 128 tile pairs of the clump's pair triangle, each summed in f64 by one block, then reduced per
+// clump in a fixed order. The per-particle arithmetic that decides a classification (radii, periapsis, pair
+// distances) is written with explicitly rounded operations in the reference's order; the sums differ from
+// the reference's sequential ones only in association. Two host reads size the work: the disk count and the
+// number of self-potential tile pairs.
 #include <cstdint>
 #include <cstring>
 
@@ -51,9 +53,10 @@ struct DiskWork {
   unsigned* parent = nullptr;  // [cap] union-find forest over the cell-sorted disk
   unsigned* gcnt = nullptr;    // [cap] members per root
   uint4* clump = nullptr;      // [cap/2+1] first member, members, root, units
-  unsigned* uoff = nullptr;    // [cap/2+2] first unit of each clump
-  double* cstat = nullptr;     // [cap/2+1][8] mass, com xyz, volume, target mass, internal KE
-  double* upe = nullptr;       // [cap+1] unit sums Σ m_a m_b / r
+  unsigned long long* uoff = nullptr;  // [cap/2+2] first self-potential unit of each clump
+  double* cstat = nullptr;     // [cap/2+1][8] mass, com xyz, volume, target mass, internal KE, Σ m m / r
+  double* upe = nullptr;       // [upe_cap] unit sums Σ m_a m_b / r (grown on demand)
+  unsigned long long upe_cap = 0;
   double* out = nullptr;       // [16]
 };
 
@@ -66,10 +69,11 @@ constexpr int kPeRows = 128;    // particles per self-potential row
 constexpr int kTile = 2048;     // radius-sorted tile of the crossing walk (the radix sort's tile)
 constexpr unsigned kCellBias = 1u << 20, kCellMax = (1u << 21) - 1u;
 constexpr int kUnionTries = 1 << 16;
+constexpr unsigned long long kMaxUnits = 1ull << 28;  // self-potential tile pairs (2 GB of partial sums)
 constexpr double kPiD = 3.14159265358979323846;
 
 enum { S_M = 0, S_COM = 1, S_VCOM = 4, S_RREM = 7, S_MREM = 8, S_LINK = 9, S_RHOREM = 10, S_CAT = 11, S_COUNT = 24 };
-enum { C_NDISK = 0, C_NCLUMP = 1, C_UNITS = 2, C_ERR = 3, C_COUNT = 8 };
+enum { C_NDISK = 0, C_NCLUMP = 1, C_ERR = 3, C_UNITS64 = 4, C_COUNT = 8 };  // C_UNITS64: a u64 in slots 4-5
 
 // Sum kDmVals doubles over the block in a fixed order (warp trees, then warps in order). Thread 0 gets them.
 __device__ __forceinline__ void block_sum(double* v, double (*s)[kDmVals]) {
@@ -174,27 +178,98 @@ __global__ void __launch_bounds__(kDmThreads) k_dm_tile_mass(State st, unsigned 
   if (threadIdx.x == 0) tsum[blockIdx.x] = a[0];
 }
 
-// One thread walks the tiles, then the crossing tile's particles in radius order.
-__global__ void k_dm_cross(State st, unsigned off, unsigned m, int tiles, const unsigned long long* __restrict__ keys,
-                           const unsigned* __restrict__ order, const double* __restrict__ tsum,
-                           double* __restrict__ scal, double frac) {
-  if (threadIdx.x != 0) return;
+// Block-wide exclusive scan of one double per thread (fixed association). Returns the block total in `total`.
+__device__ __forceinline__ double block_exclusive_scan_d(double v, double* s_warp, double& total) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  double incl = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const double t = __shfl_up_sync(SPH_FULL_MASK, incl, o);
+    if (lane >= o) incl += t;
+  }
+  if (lane == 31) s_warp[w] = incl;
+  __syncthreads();
+  if (w == 0) {
+    const double x = lane < nw ? s_warp[lane] : 0.0;
+    double xi = x;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const double t = __shfl_up_sync(SPH_FULL_MASK, xi, o);
+      if (lane >= o) xi += t;
+    }
+    if (lane < nw) s_warp[lane] = xi - x;
+    if (lane == 31) s_warp[32] = xi;
+  }
+  __syncthreads();
+  const double res = s_warp[w] + incl - v;
+  total = s_warp[32];
+  __syncthreads();
+  return res;
+}
+
+// The 85 % crossing in radius order: a prefix over the tile masses finds the crossing tile, a prefix over its
+// particles (two per thread) the first one whose running mass reaches frac·M. One block of 1024 threads.
+__global__ void __launch_bounds__(1024) k_dm_cross(State st, unsigned off, unsigned m, int tiles,
+                                                   const unsigned long long* __restrict__ keys,
+                                                   const unsigned* __restrict__ order, const double* __restrict__ tsum,
+                                                   double* __restrict__ scal, double frac) {
+  __shared__ double s_warp[33];
+  __shared__ unsigned s_tile, s_idx;
+  __shared__ double s_base, s_cum;
   const double M = scal[S_M], thr = frac * M;
-  double cum = 0.0;
-  int t = 0;
-  while (t < tiles && cum + tsum[t] < thr) cum += tsum[t++];
-  double r_rem = __longlong_as_double((long long)keys[m - 1]), m_rem = M;
-  for (unsigned i = (unsigned)t * kTile; i < m; ++i) {
-    cum += (double)st.mass[off + order[i]];
-    if (cum >= thr) {
-      r_rem = __longlong_as_double((long long)keys[i]);
-      m_rem = cum;
+  const unsigned per = ((unsigned)tiles + blockDim.x - 1) / blockDim.x, t0 = threadIdx.x * per;
+  double local = 0.0;
+  for (unsigned k = 0; k < per; ++k)
+    if (t0 + k < (unsigned)tiles) local += tsum[t0 + k];
+  if (threadIdx.x == 0) {
+    s_tile = 0xffffffffu;
+    s_idx = 0xffffffffu;
+  }
+  double total;
+  double cum = block_exclusive_scan_d(local, s_warp, total);  // synchronises, so s_tile is initialised
+  unsigned mine = 0xffffffffu;
+  for (unsigned k = 0; k < per && t0 + k < (unsigned)tiles; ++k) {
+    if (cum + tsum[t0 + k] >= thr) {
+      mine = t0 + k;
+      atomicMin(&s_tile, mine);
       break;
     }
+    cum += tsum[t0 + k];
   }
-  scal[S_RREM] = r_rem;
-  scal[S_MREM] = m_rem;
-  scal[S_RHOREM] = m_rem / (4.0 / 3.0 * kPiD * (r_rem * r_rem * r_rem));
+  __syncthreads();
+  // the crossing tile is the first crossing of its owner's run, so the owner's running mass is its base
+  if (mine != 0xffffffffu && mine == s_tile) s_base = cum;
+  if (threadIdx.x == 0 && s_tile == 0xffffffffu) s_base = total;
+  __syncthreads();
+  // walk the particles from the crossing tile on (normally within it; rounding may push it to the next)
+  double base = s_base;
+  for (unsigned start = (s_tile == 0xffffffffu ? (unsigned)tiles : s_tile) * kTile; start < m; start += kTile) {
+    const unsigned i0 = start + 2u * threadIdx.x;
+    const double v0 = i0 < m ? (double)st.mass[off + order[i0]] : 0.0;
+    const double v1 = i0 + 1u < m ? (double)st.mass[off + order[i0 + 1u]] : 0.0;
+    double tile_total;
+    const double ex = block_exclusive_scan_d(v0 + v1, s_warp, tile_total);
+    const double c0 = base + ex + v0, c1 = c0 + v1;
+    if (i0 < m && c0 >= thr) atomicMin(&s_idx, i0);
+    else if (i0 + 1u < m && c1 >= thr) atomicMin(&s_idx, i0 + 1u);
+    __syncthreads();
+    if (s_idx != 0xffffffffu) {
+      if (threadIdx.x == (s_idx - start) >> 1) s_cum = s_idx == i0 ? c0 : c1;
+      break;
+    }
+    base += tile_total;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double r_rem = __longlong_as_double((long long)keys[m - 1]), m_rem = M;
+    if (s_idx != 0xffffffffu) {
+      r_rem = __longlong_as_double((long long)keys[s_idx]);
+      m_rem = s_cum;
+    }
+    scal[S_RREM] = r_rem;
+    scal[S_MREM] = m_rem;
+    scal[S_RHOREM] = m_rem / (4.0 / 3.0 * kPiD * (r_rem * r_rem * r_rem));
+  }
 }
 
 // ---- 3. orbit classification ----------------------------------------------------------------------------
@@ -392,29 +467,42 @@ __device__ __forceinline__ unsigned lower_bound_u64(const unsigned long long* k,
   return lo;
 }
 
-__global__ void k_dm_link(unsigned n, int variant, const unsigned long long* __restrict__ skeys,
-                          const float4* __restrict__ dpos, const double* __restrict__ scal,
-                          unsigned* __restrict__ parent, unsigned* __restrict__ cnt) {
-  const unsigned a = blockIdx.x * blockDim.x + threadIdx.x;
-  if (a + 1u >= n) return;  // partners come after a in the order, so each pair is tested once
+// One warp per particle a: lanes 0-8 find the nine (x, y) columns' z-runs in the sorted cell keys, then the
+// warp scans each run's partners after a, 32 at a time; a linked partner whose root differs from a's is united.
+__global__ void __launch_bounds__(kDmThreads) k_dm_link(unsigned n, int variant,
+                                                        const unsigned long long* __restrict__ skeys,
+                                                        const float4* __restrict__ dpos,
+                                                        const double* __restrict__ scal,
+                                                        unsigned* __restrict__ parent, unsigned* __restrict__ cnt) {
+  const unsigned lane = threadIdx.x & 31u;
+  const unsigned nwarps = (gridDim.x * blockDim.x) >> 5;
   const double link = scal[S_LINK], link2 = link * link;
-  const unsigned long long ka = skeys[a];
-  const unsigned ix = (unsigned)(ka >> 42), iy = (unsigned)(ka >> 21) & kCellMax, iz = (unsigned)ka & kCellMax;
-  const unsigned z0 = iz ? iz - 1u : 0u, z1 = iz < kCellMax ? iz + 1u : kCellMax;
-  const float4 pa = dpos[a];
   bool ok = true;
-  for (int dx = -1; dx <= 1; ++dx) {
-    const int cx = (int)ix + dx;
-    if (cx < 0 || cx > (int)kCellMax) continue;
-    for (int dy = -1; dy <= 1; ++dy) {
-      const int cy = (int)iy + dy;
-      if (cy < 0 || cy > (int)kCellMax) continue;
-      const unsigned long long lo = cell_key((unsigned)cx, (unsigned)cy, z0);
-      const unsigned long long hi = cell_key((unsigned)cx, (unsigned)cy, z1);
-      if (hi < skeys[a + 1u]) continue;
-      unsigned j = max(lower_bound_u64(skeys, n, lo), a + 1u);
-      for (; j < n && skeys[j] <= hi; ++j)
-        if (pair_d2(variant, pa, dpos[j]) <= link2) ok &= uf_unite(parent, a, j);
+  for (unsigned a = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; a + 1u < n; a += nwarps) {
+    const unsigned long long ka = skeys[a], knext = skeys[a + 1u];
+    const unsigned ix = (unsigned)(ka >> 42), iy = (unsigned)(ka >> 21) & kCellMax, iz = (unsigned)ka & kCellMax;
+    unsigned j0 = 0, j1 = 0;
+    if (lane < 9u) {
+      const int cx = (int)ix + (int)(lane / 3u) - 1, cy = (int)iy + (int)(lane % 3u) - 1;
+      if (cx >= 0 && cx <= (int)kCellMax && cy >= 0 && cy <= (int)kCellMax) {
+        const unsigned long long lo = cell_key((unsigned)cx, (unsigned)cy, iz ? iz - 1u : 0u);
+        const unsigned long long hi = cell_key((unsigned)cx, (unsigned)cy, iz < kCellMax ? iz + 1u : kCellMax);
+        if (hi >= knext) {  // partners come after a in the order, so each pair is tested once
+          j0 = max(lower_bound_u64(skeys, n, lo), a + 1u);
+          j1 = lower_bound_u64(skeys, n, hi + 1ull);
+        }
+      }
+    }
+    const float4 pa = dpos[a];
+    const unsigned ra = uf_find(parent, a);
+    for (int c = 0; c < 9; ++c) {
+      const unsigned b0 = __shfl_sync(SPH_FULL_MASK, j0, c), b1 = __shfl_sync(SPH_FULL_MASK, j1, c);
+      for (unsigned j = b0 + lane; j < b1; j += 32u)
+        if (pair_d2(variant, pa, dpos[j]) <= link2) {
+          const unsigned rb = uf_find(parent, j);
+          // equal roots: already one group (a root never stops being one while its group is unmerged)
+          if (rb != ra) ok &= uf_unite(parent, ra, rb);
+        }
     }
   }
   if (!ok) atomicOr(&cnt[C_ERR], 1u);
@@ -441,23 +529,23 @@ __global__ void k_dm_clumps(unsigned n, const unsigned long long* __restrict__ s
   const unsigned s = gcnt[r];
   if (s < 2u) return;
   const unsigned c = atomicAdd(&cnt[C_NCLUMP], 1u);
-  const unsigned rows = (s + kPeRows - 1) / kPeRows;
-  clump[c] = make_uint4(i, s, r, (rows + 1) / 2);
+  clump[c] = make_uint4(i, s, r, 0u);
 }
 
-// One warp per clump: mass, centre of mass, volume, target mass, then the internal kinetic energy.
+// One block per clump: mass, centre of mass, volume, target mass, then the internal kinetic energy.
 __global__ void __launch_bounds__(kDmThreads) k_dm_clump_stats(const unsigned* __restrict__ cnt,
                                                                const uint4* __restrict__ clump, int variant,
                                                                const float4* __restrict__ dpos,
                                                                const float4* __restrict__ dvel,
                                                                const float2* __restrict__ drp,
                                                                double* __restrict__ cstat) {
+  __shared__ double s[kDmThreads / 32][kDmVals];
+  __shared__ double s_cv[3];
   const unsigned ncl = cnt[C_NCLUMP];
-  const unsigned lane = threadIdx.x & 31u;
-  for (unsigned c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < ncl; c += (gridDim.x * blockDim.x) >> 5) {
+  for (unsigned c = blockIdx.x; c < ncl; c += gridDim.x) {
     const uint4 cl = clump[c];
-    double a[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-    for (unsigned j = lane; j < cl.y; j += 32u) {
+    double a[kDmVals] = {0, 0, 0, 0, 0, 0, 0, 0}, b[kDmVals] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (unsigned j = threadIdx.x; j < cl.y; j += kDmThreads) {
       const unsigned t = cl.x + j;
       const float4 p = dpos[t], v = dvel[t];
       const float2 rp = drp[t];
@@ -471,104 +559,128 @@ __global__ void __launch_bounds__(kDmThreads) k_dm_clump_stats(const unsigned* _
       a[6] += (double)p.z * mm;
       const double rho = variant == 0 ? (double)rp.x : (double)fmaxf(rp.x, 1.0f);  // gpu_sph.rs:450
       a[7] += mm / rho;
-      a[8] += __float_as_uint(rp.y) == 0u ? mm : 0.0;
+      b[0] += __float_as_uint(rp.y) == 0u ? mm : 0.0;
     }
-#pragma unroll
-    for (int k = 0; k < 9; ++k) a[k] = warp_sum(a[k]);
-    const double M = a[0];
-    const double cvx = a[1] / M, cvy = a[2] / M, cvz = a[3] / M;
-    double ke = 0.0;
-    for (unsigned j = lane; j < cl.y; j += 32u) {
-      const float4 v = dvel[cl.x + j];
-      const double dx = (double)v.x - cvx, dy = (double)v.y - cvy, dz = (double)v.z - cvz;
-      ke += 0.5 * (double)v.w * dsq3(dx, dy, dz);
-    }
-    ke = warp_sum(ke);
-    if (lane == 0) {
+    block_sum(a, s);
+    block_sum(b, s);
+    if (threadIdx.x == 0) {
+      for (int k = 0; k < 3; ++k) s_cv[k] = a[1 + k] / a[0];
       double* o = cstat + (size_t)c * 8;
-      o[0] = M;
-      o[1] = a[4] / M;
-      o[2] = a[5] / M;
-      o[3] = a[6] / M;
+      o[0] = a[0];
+      o[1] = a[4] / a[0];
+      o[2] = a[5] / a[0];
+      o[3] = a[6] / a[0];
       o[4] = a[7];
-      o[5] = a[8];
-      o[6] = ke;
-      o[7] = 0.0;
+      o[5] = b[0];
     }
+    __syncthreads();
+    double k3[kDmVals] = {0, 0, 0, 0, 0, 0, 0, 0};
+    const double cvx = s_cv[0], cvy = s_cv[1], cvz = s_cv[2];
+    for (unsigned j = threadIdx.x; j < cl.y; j += kDmThreads) {
+      const float4 v = dvel[cl.x + j];
+      k3[0] += 0.5 * (double)v.w * dsq3((double)v.x - cvx, (double)v.y - cvy, (double)v.z - cvz);
+    }
+    block_sum(k3, s);
+    if (threadIdx.x == 0) cstat[(size_t)c * 8 + 6] = k3[0];
   }
+}
+
+// Self-potential units: the 128 × 128 tile pairs (i >= j) of a clump's lower pair triangle, T(T+1)/2 for
+// T = ceil(members / 128). Exclusive 64-bit prefix over the clumps; the total goes to cnt[C_UNITS64..+1].
+__device__ __forceinline__ unsigned long long clump_units(unsigned members) {
+  const unsigned long long t = (members + kPeRows - 1) / kPeRows;
+  return t * (t + 1ull) / 2ull;
 }
 
 __global__ void __launch_bounds__(1024) k_dm_unit_scan(unsigned* __restrict__ cnt, const uint4* __restrict__ clump,
-                                                       unsigned* __restrict__ uoff) {
-  __shared__ unsigned s_warp[33];
+                                                       unsigned long long* __restrict__ uoff) {
+  __shared__ unsigned long long s_warp[33];
   const unsigned ncl = cnt[C_NCLUMP];
   const unsigned per = (ncl + blockDim.x - 1) / blockDim.x;
   const unsigned c0 = threadIdx.x * per;
-  unsigned sum = 0;
+  unsigned long long sum = 0;
   for (unsigned k = 0; k < per; ++k)
-    if (c0 + k < ncl) sum += clump[c0 + k].w;
-  unsigned total;
-  unsigned run = block_exclusive_scan(sum, s_warp, total);
+    if (c0 + k < ncl) sum += clump_units(clump[c0 + k].y);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  unsigned long long incl = sum;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned long long t = __shfl_up_sync(SPH_FULL_MASK, incl, o);
+    if (lane >= o) incl += t;
+  }
+  if (lane == 31) s_warp[w] = incl;
+  __syncthreads();
+  if (w == 0) {
+    const unsigned long long x = lane < nw ? s_warp[lane] : 0ull;
+    unsigned long long xi = x;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned long long t = __shfl_up_sync(SPH_FULL_MASK, xi, o);
+      if (lane >= o) xi += t;
+    }
+    if (lane < nw) s_warp[lane] = xi - x;
+    if (lane == 31) s_warp[32] = xi;
+  }
+  __syncthreads();
+  unsigned long long run = s_warp[w] + incl - sum;
   for (unsigned k = 0; k < per; ++k)
     if (c0 + k < ncl) {
       uoff[c0 + k] = run;
-      run += clump[c0 + k].w;
+      run += clump_units(clump[c0 + k].y);
     }
   if (threadIdx.x == 0) {
-    uoff[ncl] = total;
-    cnt[C_UNITS] = total;
+    uoff[ncl] = s_warp[32];
+    *reinterpret_cast<unsigned long long*>(cnt + C_UNITS64) = s_warp[32];
   }
 }
 
-// Self-potential units: unit u of a clump with T rows covers rows u and T-1-u of the upper pair triangle.
-// upe[unit] = Σ_a m_a Σ_{b>a} m_b / r_ab with the reference's pair distance (floored or softened).
+// One 128 × 128 tile pair of a clump per unit: row tile j (thread t owns member a = 128 j + t) against column
+// tile i >= j staged in shared memory; on the diagonal only b > a. upe[unit] = Σ_a m_a Σ_b m_b / r_ab with the
+// reference's pair distance (floored, variant 0; softened, variant 1).
 __global__ void __launch_bounds__(kPeRows) k_dm_pe(const unsigned* __restrict__ cnt, const uint4* __restrict__ clump,
-                                                   const unsigned* __restrict__ uoff, int variant, double floor_r,
-                                                   double soft2, const float4* __restrict__ dpos,
+                                                   const unsigned long long* __restrict__ uoff, int variant,
+                                                   double floor_r, double soft2, const float4* __restrict__ dpos,
                                                    const float4* __restrict__ dvel, double* __restrict__ upe) {
   __shared__ float4 sp[kPeRows];
   __shared__ double s_red[kPeRows / 32];
-  const unsigned ncl = cnt[C_NCLUMP], units = cnt[C_UNITS];
-  for (unsigned u = blockIdx.x; u < units; u += gridDim.x) {
-    unsigned lo = 0, hi = ncl;  // the clump holding unit u: last c with uoff[c] <= u
+  const unsigned ncl = cnt[C_NCLUMP];
+  const unsigned long long units = *reinterpret_cast<const unsigned long long*>(cnt + C_UNITS64);
+  for (unsigned long long u = blockIdx.x; u < units; u += gridDim.x) {
+    unsigned lo = 0, hi = ncl;  // the clump holding unit u: the last c with uoff[c] <= u
     while (hi - lo > 1) {
       const unsigned mid = (lo + hi) >> 1;
       if (uoff[mid] <= u) lo = mid;
       else hi = mid;
     }
     const uint4 cl = clump[lo];
-    const unsigned rows = (cl.y + kPeRows - 1) / kPeRows;
-    const unsigned lu = u - uoff[lo];
+    const unsigned long long k = u - uoff[lo];
+    unsigned long long ti = (unsigned long long)((sqrt(8.0 * (double)k + 1.0) - 1.0) * 0.5);
+    while (ti > 0 && ti * (ti + 1ull) / 2ull > k) --ti;            // the estimate is off by at most one
+    while ((ti + 1ull) * (ti + 2ull) / 2ull <= k) ++ti;
+    const unsigned i = (unsigned)ti, j = (unsigned)(k - ti * (ti + 1ull) / 2ull);
+    const unsigned ia = j * kPeRows + threadIdx.x, ib = i * kPeRows + threadIdx.x;
+    __syncthreads();  // the previous unit's readers are done with sp
+    if (ib < cl.y) {
+      float4 q = dpos[cl.x + ib];
+      q.w = dvel[cl.x + ib].w;
+      sp[threadIdx.x] = q;
+    }
+    __syncthreads();
     double acc = 0.0;
-    for (int pass = 0; pass < 2; ++pass) {
-      const unsigned row = pass == 0 ? lu : rows - 1u - lu;
-      if (pass == 1 && row == lu) break;
-      const unsigned ia = row * kPeRows + threadIdx.x;
-      const bool va = ia < cl.y;
-      const float4 pa = va ? dpos[cl.x + ia] : make_float4(0.f, 0.f, 0.f, 0.f);
-      const double ma = va ? (double)dvel[cl.x + ia].w : 0.0;
-      double row_acc = 0.0;
-      for (unsigned tj = row; tj < rows; ++tj) {
-        const unsigned ib = tj * kPeRows + threadIdx.x;
-        __syncthreads();
-        if (ib < cl.y) {
-          float4 q = dpos[cl.x + ib];
-          q.w = dvel[cl.x + ib].w;
-          sp[threadIdx.x] = q;
-        }
-        __syncthreads();
-        const unsigned nb = min((unsigned)kPeRows, cl.y - tj * kPeRows);
-        if (va) {
-          const unsigned j0 = tj == row ? threadIdx.x + 1u : 0u;
-          for (unsigned j = j0; j < nb; ++j) {
-            const float4 q = sp[j];
-            const double d2 = pair_d2(variant, pa, q);
-            const double r = variant == 0 ? fmax(__dsqrt_rn(d2), floor_r) : __dsqrt_rn(__dadd_rn(d2, soft2));
-            row_acc += (double)q.w / r;
-          }
-        }
+    if (ia < cl.y) {
+      const float4 pa = dpos[cl.x + ia];
+      const unsigned nb = min((unsigned)kPeRows, cl.y - i * kPeRows);
+      double row = 0.0;
+      // 1 / max(r, floor) = min(1/r, 1/floor) and 1 / sqrt(r² + s²) from one f64 reciprocal square root
+      // (within an ulp of the divided form): the pair loop is bound by f64 issue, and this halves it
+      const double inv_floor = 1.0 / floor_r;
+      for (unsigned jj = i == j ? threadIdx.x + 1u : 0u; jj < nb; ++jj) {
+        const float4 q = sp[jj];
+        const double d2 = pair_d2(variant, pa, q);
+        const double ir = variant == 0 ? fmin(rsqrt(d2), inv_floor) : rsqrt(__dadd_rn(d2, soft2));
+        row += (double)q.w * ir;
       }
-      acc += ma * row_acc;
+      acc = (double)dvel[cl.x + ia].w * row;
     }
     acc = warp_sum(acc);
     if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = acc;
@@ -578,15 +690,27 @@ __global__ void __launch_bounds__(kPeRows) k_dm_pe(const unsigned* __restrict__ 
       for (int w = 0; w < kPeRows / 32; ++w) t += s_red[w];
       upe[u] = t;
     }
-    __syncthreads();
+  }
+}
+
+// One block per clump: its self-potential sum Σ_units, in a fixed order, into cstat[c][7].
+__global__ void __launch_bounds__(kDmThreads) k_dm_pe_reduce(const unsigned* __restrict__ cnt,
+                                                             const unsigned long long* __restrict__ uoff,
+                                                             const double* __restrict__ upe,
+                                                             double* __restrict__ cstat) {
+  __shared__ double s[kDmThreads / 32][kDmVals];
+  const unsigned ncl = cnt[C_NCLUMP];
+  for (unsigned c = blockIdx.x; c < ncl; c += gridDim.x) {
+    double a[kDmVals] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (unsigned long long u = uoff[c] + threadIdx.x; u < uoff[c + 1]; u += kDmThreads) a[0] += upe[u];
+    block_sum(a, s);
+    if (threadIdx.x == 0) cstat[(size_t)c * 8 + 7] = a[0];
   }
 }
 
 // Boundness, the Roche gate and the heaviest bound clump outside it (ties: the smaller root).
 __global__ void __launch_bounds__(kDmThreads) k_dm_select(const unsigned* __restrict__ cnt,
                                                           const uint4* __restrict__ clump,
-                                                          const unsigned* __restrict__ uoff,
-                                                          const double* __restrict__ upe,
                                                           const double* __restrict__ cstat,
                                                           const double* __restrict__ scal, int variant, double G,
                                                           double roche, double rho_fallback, double* __restrict__ out) {
@@ -602,9 +726,7 @@ __global__ void __launch_bounds__(kDmThreads) k_dm_select(const unsigned* __rest
     const double M = st[0];
     if (variant == 1 && !(M > 0.0)) continue;  // accretion.rs:121 skips massless groups
     ++nc;
-    double sum = 0.0;
-    for (unsigned u = uoff[c]; u < uoff[c + 1]; ++u) sum += upe[u];
-    const double pe = -G * sum;
+    const double pe = -G * st[7];
     const bool bound = st[6] + pe < 0.0;
     const double rho_c = st[4] > 0.0 ? M / st[4] : rho_fallback;
     const double d_roche = roche * r_rem * cbrt(rho_rem / rho_c);
@@ -672,7 +794,7 @@ bool work_reserve(DiskWork* w, int m) {
   const size_t o_bcnt = take(4 * kDmBlocks), o_cat = take(n);
   const size_t o_p0 = take(16 * n), o_p1 = take(16 * n), o_u0 = take(16 * n), o_u1 = take(16 * n);
   const size_t o_r0 = take(8 * n), o_r1 = take(8 * n), o_par = take(4 * n), o_g = take(4 * n);
-  const size_t o_cl = take(16 * half), o_uo = take(4 * (half + 1)), o_cs = take(64 * half), o_upe = take(8 * (n + 1));
+  const size_t o_cl = take(16 * half), o_uo = take(8 * (half + 1)), o_cs = take(64 * half);
   const size_t o_out = take(8 * 16);
   void* base = nullptr;
   if (cudaMalloc(&base, sz) != cudaSuccess) return false;
@@ -700,9 +822,8 @@ bool work_reserve(DiskWork* w, int m) {
   w->parent = (unsigned*)(b + o_par);
   w->gcnt = (unsigned*)(b + o_g);
   w->clump = (uint4*)(b + o_cl);
-  w->uoff = (unsigned*)(b + o_uo);
+  w->uoff = (unsigned long long*)(b + o_uo);
   w->cstat = (double*)(b + o_cs);
-  w->upe = (double*)(b + o_upe);
   w->out = (double*)(b + o_out);
   return true;
 }
@@ -712,6 +833,7 @@ bool work_reserve(DiskWork* w, int m) {
 void disk_work_free(DiskWork* w) {
   if (!w) return;
   if (w->base) cudaFree(w->base);
+  if (w->upe) cudaFree(w->upe);
   delete w;
 }
 
@@ -738,7 +860,7 @@ int disk_measure(const Dev& d, unsigned off, unsigned m, const DiskCfg& c, DiskW
   L += launch_radix_sort(w->keys, w->vals, (int)m, 64, w->hist, w->tot, src, s);
   const int tiles = (int)((m + kTile - 1) / kTile);
   k_dm_tile_mass<<<tiles, kDmThreads, 0, s>>>(st, off, m, w->vals[src], w->tsum);
-  k_dm_cross<<<1, 32, 0, s>>>(st, off, m, tiles, w->keys[src], w->vals[src], w->tsum, w->scal, c.remnant_frac);
+  k_dm_cross<<<1, 1024, 0, s>>>(st, off, m, tiles, w->keys[src], w->vals[src], w->tsum, w->scal, c.remnant_frac);
   k_dm_classify<<<nb, kDmThreads, 0, s>>>(st, off, m, chunk, c.variant, c.G, w->scal, w->cat, w->part, w->bcnt);
   k_dm_classify_final<<<1, 1024, 0, s>>>(w->part, nb, m, c.variant, c.link_factor, w->bcnt, w->scal, w->cnt, w->out);
   L += 4;
@@ -757,23 +879,53 @@ int disk_measure(const Dev& d, unsigned off, unsigned m, const DiskCfg& c, DiskW
     const unsigned gb = (nd + 255) / 256;
     k_dm_gather<<<gb, 256, 0, s>>>(nd, w->vals[src], w->dpos[0], w->dvel[0], w->drp[0], w->dpos[1], w->dvel[1],
                                    w->drp[1], w->parent, w->gcnt);
-    k_dm_link<<<gb, 256, 0, s>>>(nd, c.variant, w->keys[src], w->dpos[1], w->scal, w->parent, w->cnt);
+    const unsigned lb = (nd + 7) / 8;  // one warp per particle, grid-strided over at most 16 blocks per SM
+    k_dm_link<<<lb < 2368u ? lb : 2368u, kDmThreads, 0, s>>>(nd, c.variant, w->keys[src], w->dpos[1], w->scal,
+                                                             w->parent, w->cnt);
     k_dm_roots<<<gb, 256, 0, s>>>(nd, w->parent, w->gcnt, w->keys[0], w->vals[0]);
     L += 3;
     L += launch_radix_sort(w->keys, w->vals, (int)nd, bits_of(nd), w->hist, w->tot, src, s);
     k_dm_gather<<<gb, 256, 0, s>>>(nd, w->vals[src], w->dpos[1], w->dvel[1], w->drp[1], w->dpos[0], w->dvel[0],
                                    w->drp[0], nullptr, nullptr);
     k_dm_clumps<<<gb, 256, 0, s>>>(nd, w->keys[src], w->gcnt, w->clump, w->cnt);
-    const unsigned cb = (nd / 2 + 7) / 8;
-    k_dm_clump_stats<<<cb < 1184u ? (cb ? cb : 1u) : 1184u, kDmThreads, 0, s>>>(w->cnt, w->clump, c.variant,
-                                                                               w->dpos[0], w->dvel[0], w->drp[0],
-                                                                               w->cstat);
+    const unsigned cb = nd / 2 < 1184u ? nd / 2 : 1184u;  // clumps <= nd / 2; blocks stride over them
+    k_dm_clump_stats<<<cb, kDmThreads, 0, s>>>(w->cnt, w->clump, c.variant, w->dpos[0], w->dvel[0], w->drp[0],
+                                               w->cstat);
     k_dm_unit_scan<<<1, 1024, 0, s>>>(w->cnt, w->clump, w->uoff);
-    k_dm_pe<<<nd < 1184u ? nd : 1184u, kPeRows, 0, s>>>(w->cnt, w->clump, w->uoff, c.variant, c.pe_floor,
-                                                        c.pe_soft * c.pe_soft, w->dpos[0], w->dvel[0], w->upe);
-    k_dm_select<<<1, kDmThreads, 0, s>>>(w->cnt, w->clump, w->uoff, w->upe, w->cstat, w->scal, c.variant, c.G,
-                                         c.roche, c.rho_fallback, w->out);
-    L += 7;
+    L += 4;
+    // the self-potential's unit count sizes its partial sums: read it back once
+    unsigned long long units = 0;
+    cudaMemcpyAsync(&units, w->cnt + C_UNITS64, 8, cudaMemcpyDeviceToHost, s);
+    e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+      *err = cudaGetErrorString(e);
+      return -2;
+    }
+    if (units > kMaxUnits) {
+      *err = "disk measure: a clump's self-potential needs more than 2^28 tile pairs (a clump of ~3M particles)";
+      return -5;
+    }
+    if (units > w->upe_cap) {
+      if (w->upe) cudaFree(w->upe);
+      w->upe = nullptr;
+      w->upe_cap = 0;
+      const unsigned long long cap = units + units / 2 + 1024;
+      if (cudaMalloc(&w->upe, 8 * cap) != cudaSuccess) {
+        *err = "disk measure: self-potential workspace allocation failed";
+        return -3;
+      }
+      w->upe_cap = cap;
+    }
+    if (units) {
+      const unsigned pb = units < 4736ull ? (unsigned)units : 4736u;  // 32 blocks per SM, grid-strided
+      k_dm_pe<<<pb, kPeRows, 0, s>>>(w->cnt, w->clump, w->uoff, c.variant, c.pe_floor, c.pe_soft * c.pe_soft,
+                                     w->dpos[0], w->dvel[0], w->upe);
+      k_dm_pe_reduce<<<cb, kDmThreads, 0, s>>>(w->cnt, w->uoff, w->upe, w->cstat);
+      L += 2;
+    }
+    k_dm_select<<<1, kDmThreads, 0, s>>>(w->cnt, w->clump, w->cstat, w->scal, c.variant, c.G, c.roche,
+                                         c.rho_fallback, w->out);
+    L += 1;
   }
   unsigned flags[C_COUNT];
   cudaMemcpyAsync(out, w->out, 16 * sizeof(double), cudaMemcpyDeviceToHost, s);

@@ -34,6 +34,19 @@ WORKLOADS = {
                      theta=0.6, quad=1, leaf=16, h_solve=1, max_nbr=192, graph=1, autotune=1),
 }
 
+# Post-impact fields for the disk measurement (SI): a remnant of n_rem particles, a debris ring, escaping
+# particles and clumps (eight cold ones of 200-480 members between 3 and 5.8 R plus the four gate cases). The
+# 1M field's ring is 2 % of the particles, the share of a giant-impact disk at this resolution.
+_MEASURE_CLUMPS = tuple((200 + 40 * k, 3.0 + 0.4 * k, 5.0, 0.55 * k) for k in range(8)) + ic.SCENE_CLUMPS
+MEASURE_WORKLOADS = {
+    "post_impact_1m": dict(n_rem=1_000_000, n_ring=20_000, n_esc=2_000, clumps=_MEASURE_CLUMPS, m_rem=6.0e18,
+                           h_rem=2.5e5, h_debris=1.2e5, clump_radius=4.0e5),
+    "post_impact_4m": dict(n_rem=4_000_000, n_ring=80_000, n_esc=8_000, clumps=_MEASURE_CLUMPS, m_rem=1.5e18,
+                           h_rem=1.6e5, h_debris=0.8e5, clump_radius=2.6e5),
+    "post_impact_200k": dict(n_rem=200_000, n_ring=15_000, n_esc=2000, clumps=_MEASURE_CLUMPS, m_rem=3.0e19,
+                             h_rem=2.2e5, h_debris=1.2e5, clump_radius=4.0e5),
+}
+
 
 def impactor_fraction(wl: dict) -> float:
     """Fraction of a workload's particles in the impactor (the batch: mass ratio 0.1 at the range centre)."""
