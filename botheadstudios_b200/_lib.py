@@ -74,11 +74,16 @@ EXPORTS = ["sph_config_default", "sph_create", "sph_destroy", "sph_upload", "sph
            "sph_gravity", "sph_gravity_direct64", "sph_gravity_tree_noalloc", "sph_dem_create", "sph_dem_destroy",
            "sph_dem_replace", "sph_dem_set_params", "sph_dem_step", "sph_dem_readback", "sph_dem_contacts",
            "sph_dem_count", "sph_mlp_set", "sph_mlp_record", "sph_mlp_features", "sph_set_progress",
-           "sph_mlp_forward", "sph_mlp_grad", "sph_mlp_train", "sph_measure_default", "sph_measure_disk"]
+           "sph_mlp_forward", "sph_mlp_grad", "sph_mlp_train", "sph_measure_default", "sph_measure_disk",
+           "sph_body_bulk", "sph_assemble"]
 
 H_MODE = dict(fixed=0, solve=1, learned=2)
 MLP_PARAMS = 4819     # SPH_MLP_PARAMS
 MLP_TRAINABLE = 4801  # SPH_MLP_TRAINABLE
+
+
+class Placement(C.Structure):
+    _fields_ = [("offset", C.c_double * 3), ("vel", C.c_double * 3), ("spin", C.c_double * 3)]
 
 
 class MeasureCfg(C.Structure):
@@ -174,6 +179,8 @@ def load():
     L.sph_mlp_train.argtypes = [vp, vp, vp, C.c_uint32, C.POINTER(MlpTrainCfg), vp]
     L.sph_dem_count.argtypes = [vp]
     L.sph_measure_default.argtypes = [C.POINTER(MeasureCfg)]
+    L.sph_body_bulk.argtypes = [vp, C.c_uint32, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    L.sph_assemble.argtypes = [vp, C.POINTER(Placement), C.c_uint32, C.POINTER(C.c_float), C.POINTER(C.c_float)]
     L.sph_measure_disk.argtypes = [vp, C.c_uint32, C.POINTER(MeasureCfg), C.POINTER(DiskMeasure)]
     L.sph_dem_count.restype = C.c_uint32
     no_status = ("sph_destroy", "sph_count", "sph_stream", "sph_last_error", "sph_status_string", "sph_dem_destroy",

@@ -47,6 +47,7 @@ struct DiskWork {
   unsigned* cnt = nullptr;  // [C_COUNT]
   unsigned* bcnt = nullptr; // [kDmBlocks] disk particles per block, then their output offsets
   unsigned char* cat = nullptr;  // [cap] category of each particle
+  float4* pm = nullptr;                  // [cap] x, y, z, mass of the points whose radii are sorted
   float4* dpos[2] = {nullptr, nullptr};  // disk particles: x, y, z, h
   float4* dvel[2] = {nullptr, nullptr};  // vx, vy, vz, mass
   float2* drp[2] = {nullptr, nullptr};   // rho, prov bits
@@ -58,9 +59,20 @@ struct DiskWork {
   double* upe = nullptr;       // [upe_cap] unit sums Σ m_a m_b / r (grown on demand)
   unsigned long long upe_cap = 0;
   double* out = nullptr;       // [16]
+  double* bb = nullptr;        // [16] body bulk: centre, radius, new centre, new mass, new radius + mass, mass
+  double* place = nullptr;     // [kMaxPlacements][12] offset, vel, spin, centre of each source body
 };
 
 namespace {
+
+// The 48-byte exchange record (SphParticle, gpu_sph.rs:28).
+struct P48x {
+  float px, py, pz, h, vx, vy, vz, u, mass;
+  unsigned mat;
+  float rho;
+  unsigned prov;
+};
+static_assert(sizeof(P48x) == 48, "48-byte particle");
 
 constexpr int kDmThreads = 256;
 constexpr int kDmBlocks = 592;  // 4 × 148 SMs; block b reduces the b-th contiguous chunk of the impact
@@ -71,9 +83,13 @@ constexpr unsigned kCellBias = 1u << 20, kCellMax = (1u << 21) - 1u;
 constexpr int kUnionTries = 1 << 16;
 constexpr unsigned long long kMaxUnits = 1ull << 28;  // self-potential tile pairs (2 GB of partial sums)
 constexpr double kPiD = 3.14159265358979323846;
+constexpr unsigned kMaxPlacements = 256;
 
 enum { S_M = 0, S_COM = 1, S_VCOM = 4, S_RREM = 7, S_MREM = 8, S_LINK = 9, S_RHOREM = 10, S_CAT = 11, S_COUNT = 24 };
-enum { C_NDISK = 0, C_NCLUMP = 1, C_ERR = 3, C_UNITS64 = 4, C_COUNT = 8 };  // C_UNITS64: a u64 in slots 4-5
+enum { C_NDISK = 0, C_NCLUMP = 1, C_SEL = 2, C_ERR = 3, C_UNITS64 = 4, C_MINH = 6, C_COUNT = 8 };  // u64 in 4-5
+// body-bulk slots: the current centre and radius, the latest selection's centre and mass, its crossing radius
+// and running mass, the mass of every particle of the body
+enum { BB_C = 0, BB_R = 3, BB_CN = 4, BB_MN = 7, BB_RN = 8, BB_M = 10 };
 
 // Sum kDmVals doubles over the block in a fixed order (warp trees, then warps in order). Thread 0 gets them.
 __device__ __forceinline__ void block_sum(double* v, double (*s)[kDmVals]) {
@@ -114,7 +130,7 @@ __device__ __forceinline__ float3 pos_f32(const State& st, unsigned t) {
 
 // ---- 1. mass, centre of mass, bulk velocity ----------------------------------------------------------
 __global__ void __launch_bounds__(kDmThreads) k_dm_moments(State st, unsigned off, unsigned m, unsigned chunk,
-                                                           double* __restrict__ part) {
+                                                           double* __restrict__ part, float4* __restrict__ pm) {
   __shared__ double s[kDmThreads / 32][kDmVals];
   double a[kDmVals] = {0, 0, 0, 0, 0, 0, 0, 0};
   const unsigned b0 = blockIdx.x * chunk, b1 = min(m, b0 + chunk);
@@ -123,6 +139,7 @@ __global__ void __launch_bounds__(kDmThreads) k_dm_moments(State st, unsigned of
     const float3 p = pos_f32(st, t);
     const float4 v = st.vel_u[t];
     const double mm = st.mass[t];
+    pm[i] = make_float4(p.x, p.y, p.z, st.mass[t]);  // positions and masses for the remnant radius
     a[0] += mm;
     a[1] += (double)p.x * mm;  // f32 × f32 products are exact in f64
     a[2] += (double)p.y * mm;
@@ -154,26 +171,28 @@ __global__ void k_dm_moments_final(const double* __restrict__ part, int nb, doub
   }
 }
 
-// ---- 2. radii, their sort, the 85 % crossing -----------------------------------------------------------
-__global__ void k_dm_radius(State st, unsigned off, unsigned m, const double* __restrict__ scal,
+// ---- 2. radii about a centre, their sort, the mass-fraction crossing ------------------------------------
+// Shared by the remnant radius (85 % of an impact's mass) and the bulk radius of a body (98 %). pm holds the
+// points' f32 positions and masses; the radius is the exact f64 distance from the centre.
+__global__ void k_dm_radius(const float4* __restrict__ pm, unsigned m, const double* __restrict__ centre,
                             unsigned long long* __restrict__ keys, unsigned* __restrict__ vals) {
   const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= m) return;
-  const float3 p = pos_f32(st, off + i);
-  const double dx = __dsub_rn((double)p.x, scal[S_COM]), dy = __dsub_rn((double)p.y, scal[S_COM + 1]),
-               dz = __dsub_rn((double)p.z, scal[S_COM + 2]);
+  const float4 p = pm[i];
+  const double dx = __dsub_rn((double)p.x, centre[0]), dy = __dsub_rn((double)p.y, centre[1]),
+               dz = __dsub_rn((double)p.z, centre[2]);
   const double r = __dsqrt_rn(dsq3(dx, dy, dz));
   keys[i] = (unsigned long long)__double_as_longlong(r);  // r >= 0: the bit pattern orders like the value
   vals[i] = i;
 }
 
-__global__ void __launch_bounds__(kDmThreads) k_dm_tile_mass(State st, unsigned off, unsigned m,
+__global__ void __launch_bounds__(kDmThreads) k_dm_tile_mass(const float4* __restrict__ pm, unsigned m,
                                                              const unsigned* __restrict__ order,
                                                              double* __restrict__ tsum) {
   __shared__ double s[kDmThreads / 32][kDmVals];
   double a[kDmVals] = {0, 0, 0, 0, 0, 0, 0, 0};
   const unsigned b0 = blockIdx.x * kTile, b1 = min(m, b0 + kTile);
-  for (unsigned i = b0 + threadIdx.x; i < b1; i += kDmThreads) a[0] += (double)st.mass[off + order[i]];
+  for (unsigned i = b0 + threadIdx.x; i < b1; i += kDmThreads) a[0] += (double)pm[order[i]].w;
   block_sum(a, s);
   if (threadIdx.x == 0) tsum[blockIdx.x] = a[0];
 }
@@ -207,16 +226,19 @@ __device__ __forceinline__ double block_exclusive_scan_d(double v, double* s_war
   return res;
 }
 
-// The 85 % crossing in radius order: a prefix over the tile masses finds the crossing tile, a prefix over its
-// particles (two per thread) the first one whose running mass reaches frac·M. One block of 1024 threads.
-__global__ void __launch_bounds__(1024) k_dm_cross(State st, unsigned off, unsigned m, int tiles,
+// The mass-fraction crossing in radius order: a prefix over the tile masses finds the crossing tile, a prefix
+// over its points (two per thread) the first one whose running mass reaches frac·(*total). out[0] = its
+// radius, out[1] = the running mass there (the last radius and the total when rounding keeps the sum short).
+// One block of 1024 threads.
+__global__ void __launch_bounds__(1024) k_dm_cross(const float4* __restrict__ pm, unsigned m, int tiles,
                                                    const unsigned long long* __restrict__ keys,
                                                    const unsigned* __restrict__ order, const double* __restrict__ tsum,
-                                                   double* __restrict__ scal, double frac) {
+                                                   const double* __restrict__ total_mass, double frac,
+                                                   double* __restrict__ out) {
   __shared__ double s_warp[33];
   __shared__ unsigned s_tile, s_idx;
   __shared__ double s_base, s_cum;
-  const double M = scal[S_M], thr = frac * M;
+  const double M = *total_mass, thr = frac * M;
   const unsigned per = ((unsigned)tiles + blockDim.x - 1) / blockDim.x, t0 = threadIdx.x * per;
   double local = 0.0;
   for (unsigned k = 0; k < per; ++k)
@@ -245,8 +267,8 @@ __global__ void __launch_bounds__(1024) k_dm_cross(State st, unsigned off, unsig
   double base = s_base;
   for (unsigned start = (s_tile == 0xffffffffu ? (unsigned)tiles : s_tile) * kTile; start < m; start += kTile) {
     const unsigned i0 = start + 2u * threadIdx.x;
-    const double v0 = i0 < m ? (double)st.mass[off + order[i0]] : 0.0;
-    const double v1 = i0 + 1u < m ? (double)st.mass[off + order[i0 + 1u]] : 0.0;
+    const double v0 = i0 < m ? (double)pm[order[i0]].w : 0.0;
+    const double v1 = i0 + 1u < m ? (double)pm[order[i0 + 1u]].w : 0.0;
     double tile_total;
     const double ex = block_exclusive_scan_d(v0 + v1, s_warp, tile_total);
     const double c0 = base + ex + v0, c1 = c0 + v1;
@@ -266,9 +288,8 @@ __global__ void __launch_bounds__(1024) k_dm_cross(State st, unsigned off, unsig
       r_rem = __longlong_as_double((long long)keys[s_idx]);
       m_rem = s_cum;
     }
-    scal[S_RREM] = r_rem;
-    scal[S_MREM] = m_rem;
-    scal[S_RHOREM] = m_rem / (4.0 / 3.0 * kPiD * (r_rem * r_rem * r_rem));
+    out[0] = r_rem;
+    out[1] = m_rem;
   }
 }
 
@@ -351,6 +372,8 @@ __global__ void __launch_bounds__(1024) k_dm_classify_final(const double* __rest
   if (threadIdx.x < (unsigned)nb) bcnt[threadIdx.x] = o;
   if (threadIdx.x == 0) {
     cnt[C_NDISK] = total;
+    const double r_rem = scal[S_RREM];
+    scal[S_RHOREM] = scal[S_MREM] / (4.0 / 3.0 * kPiD * (r_rem * r_rem * r_rem));
     for (int k = 0; k < 6; ++k) scal[S_CAT + k] = t[k];
     const double mean_h = variant == 0 ? (total ? t[6] / (double)total : 0.0) : scal[S_CAT + 7] / (double)m;
     scal[S_LINK] = link_factor * mean_h;
@@ -767,6 +790,164 @@ __global__ void __launch_bounds__(kDmThreads) k_dm_select(const unsigned* __rest
   }
 }
 
+
+// ---------------------------------------------------------------------------------------------------------
+// Relaxed-body assembly: body_bulk (gpu_sph.rs:260-293) and assemble_from_relaxed_n (gpu_sph.rs:309-339).
+// A body's bulk: the centre of mass of its particles, the radius holding 98 % of their mass about it, then twice
+// the same over the particles within 1.5 × that radius of that centre (stray particles left by the relaxation
+// do not drag the centre). The assembly recentres each source body (prov k) on its bulk centre, places it at
+// offset k moving at vel k + spin k × (r − centre), keeps every other field, and drops particles whose prov has
+// no placement.
+// ---------------------------------------------------------------------------------------------------------
+__device__ __forceinline__ bool bb_take(const State& st, unsigned t, unsigned prov, int clip,
+                                        const double* __restrict__ bb) {
+  if (st.prov[t] != prov) return false;
+  if (!clip) return true;
+  const float3 p = pos_f32(st, t);
+  const double r = __dsqrt_rn(dsq3(__dsub_rn((double)p.x, bb[BB_C]), __dsub_rn((double)p.y, bb[BB_C + 1]),
+                                   __dsub_rn((double)p.z, bb[BB_C + 2])));
+  return r <= 1.5 * bb[BB_R];
+}
+
+__global__ void __launch_bounds__(kDmThreads) k_bb_count(State st, unsigned n, unsigned chunk, unsigned prov,
+                                                         int clip, const double* __restrict__ bb,
+                                                         double* __restrict__ part, unsigned* __restrict__ bcnt) {
+  __shared__ double s[kDmThreads / 32][kDmVals];
+  double a[kDmVals] = {0, 0, 0, 0, 0, 0, 0, 0};
+  const unsigned b0 = blockIdx.x * chunk, b1 = min(n, b0 + chunk);
+  unsigned cnt = 0;
+  for (unsigned base = b0; base < b1; base += kDmThreads) {
+    const unsigned t = base + threadIdx.x;
+    const bool take = t < b1 && bb_take(st, t, prov, clip, bb);
+    if (take) {
+      const float3 p = pos_f32(st, t);
+      const double mm = st.mass[t];
+      a[0] += mm;
+      a[1] += (double)p.x * mm;
+      a[2] += (double)p.y * mm;
+      a[3] += (double)p.z * mm;
+    }
+    cnt += (unsigned)__syncthreads_count(take);
+  }
+  block_sum(a, s);
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < kDmVals; ++k) part[blockIdx.x * kDmVals + k] = a[k];
+    bcnt[blockIdx.x] = cnt;
+  }
+}
+
+// Sums of the selection (centre of mass, zero for a massless one: gpu_sph.rs:266) and the block offsets.
+__global__ void __launch_bounds__(1024) k_bb_scan(const double* __restrict__ part, int nb, int first,
+                                                  unsigned* __restrict__ bcnt, double* __restrict__ bb,
+                                                  unsigned* __restrict__ cnt) {
+  __shared__ unsigned s_warp[33];
+  __shared__ double t[kDmVals];
+  const int w = threadIdx.x >> 5;
+  if (w < 4) {
+    const double v = warp_sum_column(part, nb, w);
+    if ((threadIdx.x & 31) == 0) t[w] = v;
+  }
+  unsigned total;
+  const unsigned c = threadIdx.x < (unsigned)nb ? bcnt[threadIdx.x] : 0u;
+  const unsigned o = block_exclusive_scan(c, s_warp, total);
+  if (threadIdx.x < (unsigned)nb) bcnt[threadIdx.x] = o;
+  if (threadIdx.x == 0) {
+    cnt[C_SEL] = total;
+    const double mm = t[0];
+    for (int k = 0; k < 3; ++k) bb[BB_CN + k] = mm > 0.0 ? t[1 + k] / mm : 0.0;
+    bb[BB_MN] = mm;
+    if (first) bb[BB_M] = mm;
+  }
+}
+
+__global__ void __launch_bounds__(kDmThreads) k_bb_write(State st, unsigned n, unsigned chunk, unsigned prov,
+                                                         int clip, const double* __restrict__ bb,
+                                                         const unsigned* __restrict__ boff, float4* __restrict__ pm) {
+  __shared__ unsigned s_warp[33];
+  const unsigned b0 = blockIdx.x * chunk, b1 = min(n, b0 + chunk);
+  unsigned run = boff[blockIdx.x];
+  for (unsigned base = b0; base < b1; base += kDmThreads) {
+    const unsigned t = base + threadIdx.x;
+    const unsigned f = (t < b1 && bb_take(st, t, prov, clip, bb)) ? 1u : 0u;
+    unsigned total;
+    const unsigned o = run + block_exclusive_scan(f, s_warp, total);
+    if (f) {
+      const float3 p = pos_f32(st, t);
+      pm[o] = make_float4(p.x, p.y, p.z, st.mass[t]);
+    }
+    run += total;
+  }
+}
+
+__global__ void k_bb_commit(double* __restrict__ bb) {
+  for (int k = 0; k < 3; ++k) bb[BB_C + k] = bb[BB_CN + k];
+  bb[BB_R] = bb[BB_RN];
+}
+
+// Assembly: count the kept particles per block (original order), then write them transformed.
+__global__ void __launch_bounds__(kDmThreads) k_asm_count(const P48x* __restrict__ aos, unsigned n, unsigned chunk,
+                                                          unsigned np, unsigned* __restrict__ bcnt) {
+  const unsigned b0 = blockIdx.x * chunk, b1 = min(n, b0 + chunk);
+  unsigned cnt = 0;
+  for (unsigned base = b0; base < b1; base += kDmThreads) {
+    const unsigned i = base + threadIdx.x;
+    cnt += (unsigned)__syncthreads_count(i < b1 && aos[i].prov < np);
+  }
+  if (threadIdx.x == 0) bcnt[blockIdx.x] = cnt;
+}
+
+__global__ void __launch_bounds__(1024) k_u32_offsets(unsigned* __restrict__ bcnt, int nb, unsigned* __restrict__ total_out) {
+  __shared__ unsigned s_warp[33];
+  unsigned total;
+  const unsigned c = threadIdx.x < (unsigned)nb ? bcnt[threadIdx.x] : 0u;
+  const unsigned o = block_exclusive_scan(c, s_warp, total);
+  if (threadIdx.x < (unsigned)nb) bcnt[threadIdx.x] = o;
+  if (threadIdx.x == 0) *total_out = total;
+}
+
+__global__ void __launch_bounds__(kDmThreads) k_asm_write(const P48x* __restrict__ aos, unsigned n, unsigned chunk,
+                                                          unsigned np, const double* __restrict__ place,
+                                                          const unsigned* __restrict__ boff, P48x* __restrict__ dst,
+                                                          unsigned* __restrict__ minh_key) {
+  __shared__ unsigned s_warp[33];
+  const unsigned b0 = blockIdx.x * chunk, b1 = min(n, b0 + chunk);
+  unsigned run = boff[blockIdx.x];
+  unsigned hk = 0xffffffffu;
+  for (unsigned base = b0; base < b1; base += kDmThreads) {
+    const unsigned i = base + threadIdx.x;
+    P48x p;
+    unsigned f = 0u;
+    if (i < b1) {
+      p = aos[i];
+      f = p.prov < np ? 1u : 0u;
+    }
+    unsigned total;
+    const unsigned o = run + block_exclusive_scan(f, s_warp, total);
+    if (f) {
+      const double* pl = place + (size_t)p.prov * 12;  // offset, vel, spin, centre
+      const double lx = __dsub_rn((double)p.px, pl[9]), ly = __dsub_rn((double)p.py, pl[10]),
+                   lz = __dsub_rn((double)p.pz, pl[11]);
+      const double qx = __dadd_rn(lx, pl[0]), qy = __dadd_rn(ly, pl[1]), qz = __dadd_rn(lz, pl[2]);
+      const double sx = pl[6], sy = pl[7], sz = pl[8];
+      const double vx = __dadd_rn(pl[3], __dsub_rn(__dmul_rn(sy, lz), __dmul_rn(ly, sz)));
+      const double vy = __dadd_rn(pl[4], __dsub_rn(__dmul_rn(sz, lx), __dmul_rn(lz, sx)));
+      const double vz = __dadd_rn(pl[5], __dsub_rn(__dmul_rn(sx, ly), __dmul_rn(lx, sy)));
+      P48x q = p;
+      q.px = (float)qx;
+      q.py = (float)qy;
+      q.pz = (float)qz;
+      q.vx = (float)vx;
+      q.vy = (float)vy;
+      q.vz = (float)vz;
+      dst[o] = q;
+      hk = min(hk, float_key(p.h));
+    }
+    run += total;
+  }
+  hk = warp_min(hk);
+  if ((threadIdx.x & 31) == 0 && hk != 0xffffffffu) atomicMin(minh_key, hk);
+}
+
 int bits_of(unsigned v) {
   int b = 0;
   while (b < 32 && (v >> b)) ++b;
@@ -792,10 +973,10 @@ bool work_reserve(DiskWork* w, int m) {
   const size_t o_hist = take(4 * 256 * tiles), o_tot = take(4 * 256), o_part = take(8 * kDmBlocks * kDmVals);
   const size_t o_tsum = take(8 * tiles), o_scal = take(8 * S_COUNT), o_cnt = take(4 * C_COUNT);
   const size_t o_bcnt = take(4 * kDmBlocks), o_cat = take(n);
-  const size_t o_p0 = take(16 * n), o_p1 = take(16 * n), o_u0 = take(16 * n), o_u1 = take(16 * n);
+  const size_t o_pm = take(16 * n), o_p0 = take(16 * n), o_p1 = take(16 * n), o_u0 = take(16 * n), o_u1 = take(16 * n);
   const size_t o_r0 = take(8 * n), o_r1 = take(8 * n), o_par = take(4 * n), o_g = take(4 * n);
   const size_t o_cl = take(16 * half), o_uo = take(8 * (half + 1)), o_cs = take(64 * half);
-  const size_t o_out = take(8 * 16);
+  const size_t o_out = take(8 * 16), o_bb = take(8 * 16), o_pl = take(8 * 12 * kMaxPlacements);
   void* base = nullptr;
   if (cudaMalloc(&base, sz) != cudaSuccess) return false;
   char* b = (char*)base;
@@ -813,6 +994,7 @@ bool work_reserve(DiskWork* w, int m) {
   w->cnt = (unsigned*)(b + o_cnt);
   w->bcnt = (unsigned*)(b + o_bcnt);
   w->cat = (unsigned char*)(b + o_cat);
+  w->pm = (float4*)(b + o_pm);
   w->dpos[0] = (float4*)(b + o_p0);
   w->dpos[1] = (float4*)(b + o_p1);
   w->dvel[0] = (float4*)(b + o_u0);
@@ -825,7 +1007,22 @@ bool work_reserve(DiskWork* w, int m) {
   w->uoff = (unsigned long long*)(b + o_uo);
   w->cstat = (double*)(b + o_cs);
   w->out = (double*)(b + o_out);
+  w->bb = (double*)(b + o_bb);
+  w->place = (double*)(b + o_pl);
   return true;
+}
+
+// Radius of the point whose running mass, in radius order about `centre`, first reaches frac·(*total)
+// (out[0]) and that running mass (out[1]); every pointer is device memory; n >= 1.
+int launch_radius_crossing(DiskWork* w, const float4* pm, unsigned n, const double* centre, const double* total,
+                           double frac, double* out, cudaStream_t s) {
+  k_dm_radius<<<(n + 255) / 256, 256, 0, s>>>(pm, n, centre, w->keys[0], w->vals[0]);
+  int src = 0;
+  int L = 1 + launch_radix_sort(w->keys, w->vals, (int)n, 64, w->hist, w->tot, src, s);
+  const int tiles = (int)((n + kTile - 1) / kTile);
+  k_dm_tile_mass<<<tiles, kDmThreads, 0, s>>>(pm, n, w->vals[src], w->tsum);
+  k_dm_cross<<<1, 1024, 0, s>>>(pm, n, tiles, w->keys[src], w->vals[src], w->tsum, total, frac, out);
+  return L + 2;
 }
 
 }  // namespace
@@ -852,18 +1049,13 @@ int disk_measure(const Dev& d, unsigned off, unsigned m, const DiskCfg& c, DiskW
   const unsigned chunk = ((m + kDmBlocks - 1) / kDmBlocks + kDmThreads - 1) / kDmThreads * kDmThreads;
   const int nb = (int)((m + chunk - 1) / chunk);
   cudaMemsetAsync(w->cnt, 0, 4 * C_COUNT, s);
-  k_dm_moments<<<nb, kDmThreads, 0, s>>>(st, off, m, chunk, w->part);
+  k_dm_moments<<<nb, kDmThreads, 0, s>>>(st, off, m, chunk, w->part, w->pm);
   k_dm_moments_final<<<1, kDmThreads, 0, s>>>(w->part, nb, w->scal);
-  k_dm_radius<<<(m + 255) / 256, 256, 0, s>>>(st, off, m, w->scal, w->keys[0], w->vals[0]);
-  L += 3;
-  int src = 0;
-  L += launch_radix_sort(w->keys, w->vals, (int)m, 64, w->hist, w->tot, src, s);
-  const int tiles = (int)((m + kTile - 1) / kTile);
-  k_dm_tile_mass<<<tiles, kDmThreads, 0, s>>>(st, off, m, w->vals[src], w->tsum);
-  k_dm_cross<<<1, 1024, 0, s>>>(st, off, m, tiles, w->keys[src], w->vals[src], w->tsum, w->scal, c.remnant_frac);
+  L += 2;
+  L += launch_radius_crossing(w, w->pm, m, w->scal + S_COM, w->scal + S_M, c.remnant_frac, w->scal + S_RREM, s);
   k_dm_classify<<<nb, kDmThreads, 0, s>>>(st, off, m, chunk, c.variant, c.G, w->scal, w->cat, w->part, w->bcnt);
   k_dm_classify_final<<<1, 1024, 0, s>>>(w->part, nb, m, c.variant, c.link_factor, w->bcnt, w->scal, w->cnt, w->out);
-  L += 4;
+  L += 2;
   unsigned nd = 0;
   cudaMemcpyAsync(&nd, w->cnt + C_NDISK, 4, cudaMemcpyDeviceToHost, s);
   cudaError_t e = cudaStreamSynchronize(s);
@@ -871,6 +1063,7 @@ int disk_measure(const Dev& d, unsigned off, unsigned m, const DiskCfg& c, DiskW
     *err = cudaGetErrorString(e);
     return -2;
   }
+  int src = 0;
   if (nd >= 2) {
     k_dm_compact<<<nb, kDmThreads, 0, s>>>(st, d.rho, off, m, chunk, w->cat, w->bcnt, w->scal, w->dpos[0],
                                            w->dvel[0], w->drp[0], w->keys[0], w->vals[0]);
@@ -941,6 +1134,115 @@ int disk_measure(const Dev& d, unsigned off, unsigned m, const DiskCfg& c, DiskW
     *err = "disk measure: a union-find hook gave up after its retry limit";
     return -5;
   }
+  return 0;
+}
+
+
+namespace {
+
+int reserve_or_fail(DiskWork*& w, unsigned m, const char** err) {
+  if (!w) w = new DiskWork();
+  if (!work_reserve(w, (int)(m ? m : 1u))) {
+    *err = "body measurement: workspace allocation failed";
+    return -3;
+  }
+  return 0;
+}
+
+int sync_or_fail(cudaStream_t s, const char** err) {
+  cudaError_t e = cudaStreamSynchronize(s);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    *err = cudaGetErrorString(e);
+    return -2;
+  }
+  return 0;
+}
+
+// body_bulk of one provenance into w->bb; on return out5 = {cx, cy, cz, mass, radius} (host).
+int body_bulk_impl(const Dev& d, unsigned prov, DiskWork* w, double* out5, unsigned long long* L,
+                   const char** err, cudaStream_t s) {
+  const unsigned n = (unsigned)d.n;
+  const State& st = d.s();
+  const unsigned chunk = ((n + kDmBlocks - 1) / kDmBlocks + kDmThreads - 1) / kDmThreads * kDmThreads;
+  const int nb = (int)((n + chunk - 1) / chunk);
+  cudaMemsetAsync(w->bb, 0, 16 * sizeof(double), s);
+  for (int round = 0; round < 3; ++round) {
+    const int clip = round > 0;
+    k_bb_count<<<nb, kDmThreads, 0, s>>>(st, n, chunk, prov, clip, w->bb, w->part, w->bcnt);
+    k_bb_scan<<<1, 1024, 0, s>>>(w->part, nb, round == 0, w->bcnt, w->bb, w->cnt);
+    unsigned sel = 0;
+    cudaMemcpyAsync(&sel, w->cnt + C_SEL, 4, cudaMemcpyDeviceToHost, s);
+    *L += 2;
+    if (int rc = sync_or_fail(s, err)) return rc;
+    if (sel == 0) break;  // nothing of this body (round 0), or nothing inside the clip sphere: keep the last
+    k_bb_write<<<nb, kDmThreads, 0, s>>>(st, n, chunk, prov, clip, w->bb, w->bcnt, w->pm);
+    *L += 1 + launch_radius_crossing(w, w->pm, sel, w->bb + BB_CN, w->bb + BB_MN, 0.98, w->bb + BB_RN, s);
+    k_bb_commit<<<1, 1, 0, s>>>(w->bb);
+    *L += 1;
+  }
+  double bb[16];
+  cudaMemcpyAsync(bb, w->bb, sizeof(bb), cudaMemcpyDeviceToHost, s);
+  if (int rc = sync_or_fail(s, err)) return rc;
+  out5[0] = bb[BB_C];
+  out5[1] = bb[BB_C + 1];
+  out5[2] = bb[BB_C + 2];
+  out5[3] = bb[BB_M];
+  out5[4] = bb[BB_R];
+  return 0;
+}
+
+}  // namespace
+
+int body_bulk(const Dev& d, unsigned prov, DiskWork*& w, double* out5, unsigned long long* launches,
+              const char** err, cudaStream_t s) {
+  *launches = 0;
+  for (int k = 0; k < 5; ++k) out5[k] = 0.0;
+  if (d.n == 0) return 0;
+  if (int rc = reserve_or_fail(w, (unsigned)d.n, err)) return rc;
+  return body_bulk_impl(d, prov, w, out5, launches, err, s);
+}
+
+int assemble_n(const Dev& d, const double* placements, unsigned np, void* dst, unsigned* n_out, float* min_h,
+               DiskWork*& w, unsigned long long* launches, const char** err, cudaStream_t s) {
+  *launches = 0;
+  *n_out = 0;
+  *min_h = __builtin_inff();
+  if (np > kMaxPlacements) {
+    *err = "assemble: at most 256 placements";
+    return -1;
+  }
+  const unsigned n = (unsigned)d.n;
+  if (n == 0 || np == 0) return 0;
+  if (int rc = reserve_or_fail(w, n, err)) return rc;
+  unsigned long long L = 0;
+  double place[kMaxPlacements * 12];
+  for (unsigned k = 0; k < np; ++k) {
+    double bulk[5];
+    if (int rc = body_bulk_impl(d, k, w, bulk, &L, err, s)) return rc;
+    for (int j = 0; j < 9; ++j) place[k * 12 + j] = placements[k * 9 + j];
+    for (int j = 0; j < 3; ++j) place[k * 12 + 9 + j] = bulk[j];
+  }
+  cudaMemcpyAsync(w->place, place, sizeof(double) * 12 * np, cudaMemcpyHostToDevice, s);
+  launch_to_aos(d, s);  // the state in original order, as the 48-byte records the reference assembles from
+  const unsigned chunk = ((n + kDmBlocks - 1) / kDmBlocks + kDmThreads - 1) / kDmThreads * kDmThreads;
+  const int nb = (int)((n + chunk - 1) / chunk);
+  cudaMemsetAsync(w->cnt + C_MINH, 0xff, 4, s);
+  k_asm_count<<<nb, kDmThreads, 0, s>>>((const P48x*)d.aos, n, chunk, np, w->bcnt);
+  k_u32_offsets<<<1, 1024, 0, s>>>(w->bcnt, nb, w->cnt + C_SEL);
+  k_asm_write<<<nb, kDmThreads, 0, s>>>((const P48x*)d.aos, n, chunk, np, w->place, w->bcnt, (P48x*)dst,
+                                        w->cnt + C_MINH);
+  L += 4;
+  unsigned cnts[C_COUNT];
+  cudaMemcpyAsync(cnts, w->cnt, sizeof(cnts), cudaMemcpyDeviceToHost, s);
+  if (int rc = sync_or_fail(s, err)) return rc;
+  *n_out = cnts[C_SEL];
+  if (cnts[C_MINH] != 0xffffffffu) {  // the order-preserving key back to the float
+    const unsigned k = cnts[C_MINH];
+    const unsigned b = (k >> 31) ? (k ^ 0x80000000u) : ~k;
+    std::memcpy(min_h, &b, 4);
+  }
+  *launches = L;
   return 0;
 }
 

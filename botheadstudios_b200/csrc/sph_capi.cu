@@ -262,13 +262,16 @@ void drop_graphs(sph_ctx* ctx) {
 }
 
 // Upload of `nimp` impacts (particles [off[k], off[k+1]) of `particles`, softening soft[k]); the impacts
-// are already validated as non-empty and within capacity.
+// are already validated as non-empty and within capacity. `on_device`: the particles are device memory
+// produced by the library itself (the assembly), so they skip the host validation, and eos == nullptr keeps
+// the material table.
 sph_status upload_impl(sph_ctx* ctx, const SphParticle48* particles, const uint32_t* off, uint32_t nimp,
-                       const SphEos48* eos, uint32_t n_eos, const float* soft) {
+                       const SphEos48* eos, uint32_t n_eos, const float* soft, bool on_device = false) {
   cudaSetDevice(ctx->device);
   sph_status ret = SPH_OK;
   const uint32_t nu = nimp ? off[nimp] : 0u;
-  uint32_t ne = n_eos;
+  const bool keep_eos = on_device && !eos;
+  uint32_t ne = keep_eos ? ctx->n_eos : n_eos;
   if (ne > (uint32_t)kMaxMaterials) {
     ne = kMaxMaterials;
     ret = SPH_CLAMPED;
@@ -278,7 +281,7 @@ sph_status upload_impl(sph_ctx* ctx, const SphParticle48* particles, const uint3
       ctx->err = "impact " + std::to_string(k) + " has a negative or non-finite softening";
       return SPH_ERR_INVALID;
     }
-  for (uint32_t i = 0; i < nu; ++i) {
+  for (uint32_t i = 0; i < (on_device ? 0u : nu); ++i) {
     const SphParticle48& p = particles[i];
     if (p.mat >= ne || !std::isfinite(p.pos[0]) || !std::isfinite(p.pos[1]) || !std::isfinite(p.pos[2]) ||
         !std::isfinite(p.vel[0]) || !std::isfinite(p.vel[1]) || !std::isfinite(p.vel[2]) || !std::isfinite(p.u) ||
@@ -311,11 +314,15 @@ sph_status upload_impl(sph_ctx* ctx, const SphParticle48* particles, const uint3
   }
   d.L = (int)L;
   ctx->n_eos = ne;
-  if (nu) CK(cudaMemcpyAsync(d.aos, particles, (size_t)nu * 48, cudaMemcpyHostToDevice, ctx->stream));
-  Eos etab[kMaxMaterials];
-  std::memset(etab, 0, sizeof(etab));
-  if (ne) std::memcpy(etab, eos, (size_t)ne * sizeof(Eos));
-  CK(cudaMemcpyAsync(d.eos, etab, sizeof(etab), cudaMemcpyHostToDevice, ctx->stream));
+  if (nu)
+    CK(cudaMemcpyAsync(d.aos, particles, (size_t)nu * 48,
+                       on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, ctx->stream));
+  if (!keep_eos) {
+    Eos etab[kMaxMaterials];
+    std::memset(etab, 0, sizeof(etab));
+    if (ne) std::memcpy(etab, eos, (size_t)ne * sizeof(Eos));
+    CK(cudaMemcpyAsync(d.eos, etab, sizeof(etab), cudaMemcpyHostToDevice, ctx->stream));
+  }
   CK(cudaMemcpyAsync(d.segs, table.data(), table.size() * sizeof(Seg), cudaMemcpyHostToDevice, ctx->stream));
   sph_status st = push_params(ctx, d);
   if (st != SPH_OK) return st;
@@ -725,6 +732,89 @@ sph_status sph_particle_buffer(sph_ctx* ctx, void** device_ptr) {
 
 void* sph_stream(sph_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
 const char* sph_last_error(const sph_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+sph_status sph_body_bulk(sph_ctx* ctx, uint32_t prov, double centre[3], double* mass, double* radius) {
+  if (!ctx || !centre || !mass || !radius) return SPH_ERR_INVALID;
+  if (!ctx->uploaded) {
+    ctx->err = "sph_body_bulk: nothing uploaded";
+    return SPH_ERR_STATE;
+  }
+  cudaSetDevice(ctx->device);
+  double v[5];
+  unsigned long long launches = 0;
+  const char* msg = "";
+  const int rc = body_bulk(ctx->d, prov, ctx->disk, v, &launches, &msg, ctx->stream);
+  ctx->launches += launches;
+  if (rc) {
+    ctx->err = msg;
+    return (sph_status)rc;
+  }
+  for (int k = 0; k < 3; ++k) centre[k] = v[k];
+  *mass = v[3];
+  *radius = v[4];
+  return SPH_OK;
+}
+
+sph_status sph_assemble(sph_ctx* ctx, const sph_placement* placements, uint32_t n_placements, float* softening,
+                        float* dt) {
+  if (!ctx || (!placements && n_placements) || !softening || !dt) return SPH_ERR_INVALID;
+  if (!ctx->uploaded) {
+    ctx->err = "sph_assemble: nothing uploaded";
+    return SPH_ERR_STATE;
+  }
+  if (n_placements > (uint32_t)kMaxSegments) {
+    ctx->err = "sph_assemble: at most 256 placements";
+    return SPH_ERR_INVALID;
+  }
+  for (uint32_t k = 0; k < n_placements; ++k)
+    for (int j = 0; j < 3; ++j)
+      if (!std::isfinite(placements[k].offset[j]) || !std::isfinite(placements[k].vel[j]) ||
+          !std::isfinite(placements[k].spin[j])) {
+        ctx->err = "sph_assemble: placement " + std::to_string(k) + " has a non-finite component";
+        return SPH_ERR_INVALID;
+      }
+  cudaSetDevice(ctx->device);
+  CK(cudaStreamSynchronize(ctx->stream));
+  const uint32_t n = (uint32_t)ctx->d.n;
+  void* dst = nullptr;
+  if (n) CK(cudaMalloc(&dst, (size_t)n * 48));
+  std::vector<double> pl((size_t)n_placements * 9);
+  for (uint32_t k = 0; k < n_placements; ++k)
+    for (int j = 0; j < 3; ++j) {
+      pl[k * 9 + j] = placements[k].offset[j];
+      pl[k * 9 + 3 + j] = placements[k].vel[j];
+      pl[k * 9 + 6 + j] = placements[k].spin[j];
+    }
+  unsigned n_out = 0;
+  float min_h = 0.0f;
+  unsigned long long launches = 0;
+  const char* msg = "";
+  int rc = assemble_n(ctx->d, pl.data(), n_placements, dst, &n_out, &min_h, ctx->disk, &launches, &msg,
+                      ctx->stream);
+  ctx->launches += launches;
+  sph_status st = SPH_OK;
+  if (rc) {
+    ctx->err = msg;
+    st = (sph_status)rc;
+  } else if (n_out == 0) {
+    ctx->err = "sph_assemble: no particle's prov has a placement";
+    st = SPH_ERR_INVALID;
+  } else {
+    // gpu_sph.rs:334-338: softening = a quarter of the finest h, dt shock-safe against the fastest approach
+    const float soft = 0.25f * min_h;
+    double vmax = 0.0;
+    for (uint32_t k = 0; k < n_placements; ++k) {
+      const double* v = placements[k].vel;
+      vmax = std::max(vmax, std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]));
+    }
+    *softening = soft;
+    *dt = (float)(0.01 * (double)min_h / (20000.0 + vmax));
+    const uint32_t off[2] = {0u, n_out};
+    st = upload_impl(ctx, (const SphParticle48*)dst, off, 1u, nullptr, 0u, &soft, true);
+  }
+  if (dst) cudaFree(dst);
+  return st;
+}
 
 sph_status sph_measure_default(sph_measure_cfg* cfg) {
   if (!cfg) return SPH_ERR_INVALID;

@@ -237,5 +237,14 @@ void disk_work_free(DiskWork* w);
 // synchronises the stream). Returns 0, or a negative status with a message in *err. *launches counts kernels.
 int disk_measure(const Dev& d, unsigned off, unsigned m, const DiskCfg& c, DiskWork*& w, double* out,
                  unsigned long long* launches, const char** err, cudaStream_t s);
+// body_bulk (gpu_sph.rs:260-293) of the state's particles with provenance `prov`: out5 = centre xyz, mass,
+// 98 %-mass radius (host memory; synchronises the stream).
+int body_bulk(const Dev& d, unsigned prov, DiskWork*& w, double* out5, unsigned long long* launches,
+              const char** err, cudaStream_t s);
+// assemble_from_relaxed_n (gpu_sph.rs:309-339): placements = np × {offset xyz, vel xyz, spin xyz} (host);
+// writes the kept particles, transformed, in original order into dst (device, room for d.n records) and returns
+// their count and smallest h. Overwrites d.aos.
+int assemble_n(const Dev& d, const double* placements, unsigned np, void* dst, unsigned* n_out, float* min_h,
+               DiskWork*& w, unsigned long long* launches, const char** err, cudaStream_t s);
 
 }  // namespace sphb

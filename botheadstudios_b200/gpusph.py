@@ -94,6 +94,28 @@ class GpuSph:
                     "sph_inspect(IMPACT_TIME)")
         return out
 
+    # ---- relaxed-body assembly --------------------------------------------------------------------------
+    def body_bulk(self, prov: int):
+        """body_bulk on the device: (centre[3], mass, 98 %-mass radius) of the particles with this provenance."""
+        c = (C.c_double * 3)()
+        m, r = C.c_double(), C.c_double()
+        self._check(self._L.sph_body_bulk(self._h, prov, c, C.byref(m), C.byref(r)), "sph_body_bulk")
+        return np.array(c[:], np.float64), m.value, r.value
+
+    def assemble(self, placements):
+        """assemble_from_relaxed_n on the device: placements[k] = (offset, vel, spin) for source body prov = k.
+        The state becomes the assembled impact; returns (softening, dt) as the reference does."""
+        arr = (_lib.Placement * max(len(placements), 1))()
+        for k, (o, v, w) in enumerate(placements):
+            arr[k].offset[:] = [float(x) for x in o]
+            arr[k].vel[:] = [float(x) for x in v]
+            arr[k].spin[:] = [float(x) for x in w]
+        soft, dt = C.c_float(), C.c_float()
+        self._check(self._L.sph_assemble(self._h, arr, len(placements), C.byref(soft), C.byref(dt)), "sph_assemble")
+        self.softening = soft.value
+        self.n_impacts = 1
+        return soft.value, dt.value
+
     # ---- disk measurement ----------------------------------------------------------------------------
     def measure_disk(self, impact: int = 0, variant: int = 0, **kw) -> dict:
         """Disk measurement and Moon candidate of one impact on the device (sph_measure_disk). variant 0 is the

@@ -185,6 +185,29 @@ uint32_t sph_count(const sph_ctx* ctx);
 sph_status sph_particle_buffer(sph_ctx* ctx, void** device_ptr);
 sph_status sph_diag(sph_ctx* ctx, sph_diag_out* out);
 
+/* ---- relaxed-body assembly (gpu_sph.rs:260-339) ------------------------------------------------------------
+ * body_bulk (gpu_sph.rs:260-293): the centre of mass of the particles with provenance `prov`, the radius holding
+ * 98 % of their mass about it, then twice again over the particles within 1.5 × that radius of that centre (so
+ * the strays a relaxation leaves do not drag the centre); also the body's total mass. */
+sph_status sph_body_bulk(sph_ctx* ctx, uint32_t prov, double centre[3], double* mass, double* radius);
+
+/* BodyPlacement (gpu_sph.rs:297-302): where source body prov = k goes, its bulk velocity and angular velocity. */
+typedef struct sph_placement {
+  double offset[3];
+  double vel[3];
+  double spin[3];   /* ω (rad/s, any axis): v = vel + ω × (r − centre) */
+} sph_placement;
+
+/* assemble_from_relaxed_n (gpu_sph.rs:309-339) on the context's state (the relaxed bodies, typically after
+ * sph_step_relax): each particle of prov k < n_placements is recentred on its body's bulk centre, moved to
+ * placements[k].offset and given placements[k].vel + spin × (r − centre); particles of other provenance are
+ * dropped; the rest of the record is kept. The result replaces the state as one impact (original order of the
+ * kept particles, the material table kept) with the returned softening (a quarter of the smallest h); *dt is the
+ * reference's shock-safe step 0.01 h_min / (20 km/s + the fastest placement speed), for sph_set_dt. At most 256
+ * placements; SPH_ERR_INVALID when no particle is kept. */
+sph_status sph_assemble(sph_ctx* ctx, const sph_placement* placements, uint32_t n_placements, float* softening,
+                        float* dt);
+
 /* ---- disk measurement and the Moon candidate of one impact ------------------------------------------------
  * Replaces the host measurement of a finished impact: variant 0 follows the impact-run tool
  * (tools/impact-run/src/main.rs:732-878, `measure` + `moon_candidate`), variant 1 the engine's statistics

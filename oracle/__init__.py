@@ -430,3 +430,28 @@ def measure_disk(particles, G, variant=0, remnant_frac=0.85, link_factor=2.0, ro
     out = np.zeros(16, np.float64)
     L.orc_measure_disk(p, len(p), variant, G, remnant_frac, link_factor, roche, rho_fallback, pe_floor, pe_soft, out)
     return dict(zip(MEASURE_KEYS, out.tolist()))
+
+
+# ---- relaxed-body assembly (gpu_sph.rs:260-339) ---------------------------------------------------------
+def body_bulk(particles, prov: int):
+    """body_bulk: (centre[3], mass, radius) of the particles with this provenance."""
+    L = lib()
+    L.orc_body_bulk.argtypes = [f32p, C.c_int, C.c_uint32, f64p]
+    p = np.ascontiguousarray(np.ascontiguousarray(particles).view(np.float32).reshape(-1, 12))
+    out = np.zeros(5, np.float64)
+    L.orc_body_bulk(p, len(p), prov, out)
+    return out[:3], float(out[3]), float(out[4])
+
+
+def assemble(particles, placements):
+    """assemble_from_relaxed_n: (particles, softening, dt); placements = [(offset, vel, spin), ...]."""
+    L = lib()
+    L.orc_assemble.argtypes = [f32p, C.c_int, f64p, C.c_int, f32p, C.POINTER(C.c_float), C.POINTER(C.c_float)]
+    L.orc_assemble.restype = C.c_int
+    src = np.ascontiguousarray(particles)
+    p = np.ascontiguousarray(src.view(np.float32).reshape(-1, 12))
+    pl = np.ascontiguousarray(np.asarray(placements, np.float64).reshape(-1, 9))
+    out = np.zeros_like(p)
+    soft, dt = C.c_float(), C.c_float()
+    m = L.orc_assemble(p, len(p), pl, len(pl), out, C.byref(soft), C.byref(dt))
+    return out[:m].copy().view(src.dtype).reshape(-1), soft.value, dt.value

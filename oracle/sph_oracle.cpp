@@ -1474,3 +1474,105 @@ void orc_measure_disk(const float* P, int n, int variant, double G, double remna
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------------------------------
+// Relaxed-body assembly: gpu_sph.rs:260-293 (`body_bulk`) and :309-339 (`assemble_from_relaxed_n`).
+// ---------------------------------------------------------------------------------------------------
+static void orc_bulk_impl(const float* P, int n, uint32_t prov, double* out5) {
+  auto f = [&](int i, int k) { return P[12 * (size_t)i + k]; };
+  auto pv = [&](int i) { uint32_t u; std::memcpy(&u, &P[12 * (size_t)i + 11], 4); return u; };
+  std::vector<int> ps;
+  for (int i = 0; i < n; ++i)
+    if (pv(i) == prov) ps.push_back(i);
+  double m = 0.0;
+  for (int i : ps) m += (double)f(i, 8);
+  auto com = [&](const std::vector<int>& sel, double c[3]) {
+    double mm = 0.0;
+    for (int i : sel) mm += (double)f(i, 8);
+    c[0] = c[1] = c[2] = 0.0;
+    if (mm <= 0.0) return;
+    for (int i : sel)
+      for (int k = 0; k < 3; ++k) c[k] += (double)f(i, k) * (double)f(i, 8);
+    for (int k = 0; k < 3; ++k) c[k] /= mm;
+  };
+  auto dist = [&](int i, const double c[3]) {
+    const double d[3] = {(double)f(i, 0) - c[0], (double)f(i, 1) - c[1], (double)f(i, 2) - c[2]};
+    return std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+  };
+  auto bulk_radius = [&](const std::vector<int>& sel, const double c[3]) {
+    double mm = 0.0;
+    for (int i : sel) mm += (double)f(i, 8);
+    std::vector<std::pair<double, double>> rr;
+    for (int i : sel) rr.push_back({dist(i, c), (double)f(i, 8)});
+    std::stable_sort(rr.begin(), rr.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+    double cum = 0.0, r = 0.0;
+    for (const auto& x : rr) {
+      cum += x.second;
+      r = x.first;
+      if (cum >= 0.98 * mm) break;
+    }
+    return r;
+  };
+  double c[3];
+  com(ps, c);
+  double r = bulk_radius(ps, c);
+  for (int it = 0; it < 2; ++it) {
+    std::vector<int> keep;
+    for (int i : ps)
+      if (dist(i, c) <= 1.5 * r) keep.push_back(i);
+    if (keep.empty()) break;
+    com(keep, c);
+    r = bulk_radius(keep, c);
+  }
+  out5[0] = c[0];
+  out5[1] = c[1];
+  out5[2] = c[2];
+  out5[3] = m;
+  out5[4] = r;
+}
+
+extern "C" {
+
+void orc_body_bulk(const float* P, int n, uint32_t prov, double* out5) { orc_bulk_impl(P, n, prov, out5); }
+
+// placements: np × {offset xyz, vel xyz, spin xyz}. out: room for n records; returns the kept count.
+int orc_assemble(const float* P, int n, const double* pl, int np, float* out, float* softening, float* dt) {
+  std::vector<double> coms((size_t)np * 3);
+  for (int k = 0; k < np; ++k) {
+    double b[5];
+    orc_bulk_impl(P, n, (uint32_t)k, b);
+    for (int j = 0; j < 3; ++j) coms[k * 3 + j] = b[j];
+  }
+  int m = 0;
+  float min_h = INFINITY;
+  for (int i = 0; i < n; ++i) {
+    const float* p = P + 12 * (size_t)i;
+    uint32_t prov;
+    std::memcpy(&prov, &p[11], 4);
+    if (prov >= (uint32_t)np) continue;
+    const double* o = pl + 9 * prov;
+    const double l[3] = {(double)p[0] - coms[prov * 3], (double)p[1] - coms[prov * 3 + 1],
+                         (double)p[2] - coms[prov * 3 + 2]};
+    const double q[3] = {l[0] + o[0], l[1] + o[1], l[2] + o[2]};
+    const double* w = o + 6;
+    const double v[3] = {o[3] + (w[1] * l[2] - l[1] * w[2]), o[4] + (w[2] * l[0] - l[2] * w[0]),
+                         o[5] + (w[0] * l[1] - l[0] * w[1])};
+    float* r = out + 12 * (size_t)m++;
+    std::memcpy(r, p, 48);
+    for (int k = 0; k < 3; ++k) {
+      r[k] = (float)q[k];
+      r[4 + k] = (float)v[k];
+    }
+    min_h = std::min(min_h, p[3]);
+  }
+  double vmax = 0.0;
+  for (int k = 0; k < np; ++k) {
+    const double* v = pl + 9 * k + 3;
+    vmax = std::max(vmax, std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]));
+  }
+  *softening = 0.25f * min_h;
+  *dt = (float)(0.01 * (double)min_h / (20000.0 + vmax));
+  return m;
+}
+
+}  // extern "C"
