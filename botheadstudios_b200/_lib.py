@@ -75,7 +75,7 @@ EXPORTS = ["sph_config_default", "sph_create", "sph_destroy", "sph_upload", "sph
            "sph_dem_replace", "sph_dem_set_params", "sph_dem_step", "sph_dem_readback", "sph_dem_contacts",
            "sph_dem_count", "sph_mlp_set", "sph_mlp_record", "sph_mlp_features", "sph_set_progress",
            "sph_mlp_forward", "sph_mlp_grad", "sph_mlp_train", "sph_measure_default", "sph_measure_disk",
-           "sph_body_bulk", "sph_assemble"]
+           "sph_body_bulk", "sph_assemble", "sph_dem_set_ground", "sph_dem_set_terrain"]
 
 H_MODE = dict(fixed=0, solve=1, learned=2)
 MLP_PARAMS = 4819     # SPH_MLP_PARAMS
@@ -109,6 +109,11 @@ GRAIN_DTYPE = np.dtype([("offset", "<f4", (3,)), ("u", "<f4"), ("vel", "<f4", (3
                         ("color", "<f4", (3,)), ("material", "<f4"), ("emission", "<f4", (3,)), ("rho", "<f4"),
                         ("radius", "<f4"), ("_p", "<f4", (3,))])
 assert GRAIN_DTYPE.itemsize == 80
+
+
+class DemGround(C.Structure):
+    _fields_ = [("center", C.c_float * 3), ("air_rho", C.c_float), ("drag_cd", C.c_float),
+                ("specific_heat", C.c_float), ("cool_rate", C.c_float), ("reserved", C.c_float)]
 
 
 class DemParams(C.Structure):
@@ -170,6 +175,8 @@ def load():
     L.sph_dem_step.argtypes = [vp, C.c_uint32]
     L.sph_dem_readback.argtypes = [vp, vp, C.c_uint32, C.POINTER(C.c_uint32)]
     L.sph_dem_contacts.argtypes = [vp, vp, C.c_size_t]
+    L.sph_dem_set_ground.argtypes = [vp, C.POINTER(DemGround)]
+    L.sph_dem_set_terrain.argtypes = [vp, vp, C.c_uint32, C.c_uint32]
     L.sph_mlp_set.argtypes = [vp, vp, C.c_uint32]
     L.sph_mlp_record.argtypes = [vp, C.c_int]
     L.sph_mlp_features.argtypes = [vp, vp, vp, C.c_uint32]

@@ -1273,6 +1273,8 @@ sph_status sph_set_progress(sph_ctx* ctx, float fraction) {
 struct sph_dem {
   sph_ctx* base = nullptr;
   DemParams p{};
+  int* terrain = nullptr;   // [wd][ww] heightfield (device), owned
+  bool stepped = false;     // a substep ran since the last replace (the glow is then the integrator's)
   void* grains = nullptr;   // [cap] SphGrain80, original order
   float4* acc = nullptr;    // [cap][4] contact sums of the last substep (sorted order)
   uint32_t capacity = 0;
@@ -1317,6 +1319,11 @@ sph_status sph_dem_create(uint32_t capacity, int32_t device, sph_dem** out) {
 
 void sph_dem_destroy(sph_dem* dem) {
   if (!dem) return;
+  if (dem->terrain) {
+    cudaSetDevice(dem->base->device);
+    cudaStreamSynchronize(dem->base->stream);
+    cudaFree(dem->terrain);
+  }
   sph_destroy(dem->base);
   delete dem;
 }
@@ -1335,6 +1342,43 @@ sph_status sph_dem_set_params(sph_dem* dem, const sph_dem_params* p) {
   q.friction = p->c_friction;
   q.tangent_damp = p->c_tangent_damp;
   q.cohesion = p->c_cohesion;
+  return SPH_OK;
+}
+
+sph_status sph_dem_set_ground(sph_dem* dem, const sph_dem_ground* g) {
+  if (!dem || !g) return SPH_ERR_INVALID;
+  const float v[7] = {g->center[0], g->center[1], g->center[2], g->air_rho, g->drag_cd, g->specific_heat,
+                      g->cool_rate};
+  for (float x : v)
+    if (!std::isfinite(x)) return SPH_ERR_INVALID;
+  if (g->air_rho < 0.0f || g->drag_cd < 0.0f || g->specific_heat < 0.0f || g->cool_rate < 0.0f)
+    return SPH_ERR_INVALID;
+  DemParams& q = dem->p;
+  q.cx = g->center[0];
+  q.cy = g->center[1];
+  q.cz = g->center[2];
+  q.air_rho = g->air_rho;
+  q.drag_cd = g->drag_cd;
+  q.specific_heat = g->specific_heat;
+  q.cool_rate = g->cool_rate;
+  return SPH_OK;
+}
+
+sph_status sph_dem_set_terrain(sph_dem* dem, const int32_t* heights, uint32_t w, uint32_t d) {
+  if (!dem || ((w || d) && (!heights || !w || !d))) return SPH_ERR_INVALID;
+  sph_ctx* ctx = dem->base;
+  cudaSetDevice(ctx->device);
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (dem->terrain) cudaFree(dem->terrain);
+  dem->terrain = nullptr;
+  dem->p.hf = nullptr;
+  dem->p.ww = dem->p.wd = 0;
+  if (!w) return SPH_OK;
+  CK(cudaMalloc(&dem->terrain, sizeof(int) * (size_t)w * d));
+  CK(cudaMemcpy(dem->terrain, heights, sizeof(int) * (size_t)w * d, cudaMemcpyHostToDevice));
+  dem->p.hf = dem->terrain;
+  dem->p.ww = w;
+  dem->p.wd = d;
   return SPH_OK;
 }
 
@@ -1363,6 +1407,7 @@ sph_status sph_dem_replace(sph_dem* dem, const SphGrain80* grains, uint32_t n) {
   d.L = n ? (int)((n + d.K - 1) / d.K) : 0;
   d.nseg = 1;
   d.segbits = 0;
+  dem->stepped = false;
   if (n) {
     CK(cudaMemcpyAsync(dem->grains, grains, (size_t)n * 80, cudaMemcpyHostToDevice, ctx->stream));
     launch_dem_load(d, dem->grains, ctx->stream);
@@ -1389,6 +1434,7 @@ sph_status sph_dem_step(sph_dem* dem, uint32_t substeps) {
     phase(ctx, SPH_PHASE_FORCES, [&] { return launch_dem_contacts(d, dem->p, dem->acc, s); });
     phase(ctx, SPH_PHASE_INTEGRATE, [&] { return launch_dem_integrate(d, dem->p, dem->acc, s); });
   }
+  if (substeps) dem->stepped = true;
   CK(cudaGetLastError());
   return SPH_OK;
 }
@@ -1400,7 +1446,7 @@ sph_status sph_dem_readback(sph_dem* dem, SphGrain80* out, uint32_t cap, uint32_
   const uint32_t n = (uint32_t)ctx->d.n;
   const uint32_t m = n < cap ? n : cap;
   *n_out = 0;
-  if (n) launch_dem_store(ctx->d, dem->grains, ctx->stream);
+  if (n) launch_dem_store(ctx->d, dem->p, dem->stepped, dem->grains, ctx->stream);
   if (m) CK(cudaMemcpyAsync(out, dem->grains, (size_t)m * 80, cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
   *n_out = m;

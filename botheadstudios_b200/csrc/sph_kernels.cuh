@@ -186,9 +186,14 @@ struct Cfg {
 struct DemParams {
   float gx, gy, gz, dt;
   float stiffness, normal_damp, friction, tangent_damp, cohesion;
+  // the ground scene (particle_step.wgsl Params): heightfield frame, medium, thermal relaxation
+  float cx, cy, cz;
+  float air_rho, drag_cd, specific_heat, cool_rate;
+  const int* hf = nullptr;  // [wd][ww] column tops (voxel units), nullptr without a terrain
+  unsigned ww = 0, wd = 0;
 };
 int launch_dem_load(const Dev& d, const void* grains, cudaStream_t s);
-int launch_dem_store(const Dev& d, void* grains, cudaStream_t s);
+int launch_dem_store(const Dev& d, const DemParams& p, bool stepped, void* grains, cudaStream_t s);
 int launch_dem_contacts(const Dev& d, const DemParams& p, float4* acc, cudaStream_t s);
 int launch_dem_integrate(const Dev& d, const DemParams& p, const float4* acc, cudaStream_t s);
 

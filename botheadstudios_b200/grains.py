@@ -1,5 +1,6 @@
 """Host-side mirror of the engine's granular pipeline ``GpuParticles`` (crates/engine/src/gpu_particles.rs:46-325)
-over the C ABI: ``new``/``replace``/``set_params``/``dispatch``/``readback``/``count``.
+over the C ABI: ``new``/``replace``/``set_params``/``dispatch``/``readback``/``count``, plus the ground scene's
+medium and terrain (``set_ground``, ``set_terrain``).
 """
 from __future__ import annotations
 
@@ -8,7 +9,7 @@ import ctypes as C
 import numpy as np
 
 from . import _lib
-from ._lib import GRAIN_DTYPE, DemParams
+from ._lib import GRAIN_DTYPE, DemGround, DemParams
 from .gpusph import SphError
 
 
@@ -36,6 +37,22 @@ class GpuGrains:
         p.dt, p.c_stiffness, p.c_normal_damp = dt, stiffness, normal_damp
         p.c_friction, p.c_tangent_damp, p.c_cohesion = friction, tangent_damp, cohesion
         self._check(self._L.sph_dem_set_params(self._h, C.byref(p)), "sph_dem_set_params")
+
+    def set_ground(self, center=(0.0, 0.0, 0.0), air_rho=0.0, drag_cd=0.0, specific_heat=0.0, cool_rate=0.0):
+        """The scene's heightfield frame, air (drag) and thermal relaxation (particle_step.wgsl Params)."""
+        g = DemGround()
+        g.center[:] = center
+        g.air_rho, g.drag_cd, g.specific_heat, g.cool_rate = air_rho, drag_cd, specific_heat, cool_rate
+        self._check(self._L.sph_dem_set_ground(self._h, C.byref(g)), "sph_dem_set_ground")
+
+    def set_terrain(self, heights):
+        """heights[z, x]: column tops in voxel units (None removes the terrain)."""
+        if heights is None:
+            self._check(self._L.sph_dem_set_terrain(self._h, None, 0, 0), "sph_dem_set_terrain")
+            return
+        h = np.ascontiguousarray(heights, dtype=np.int32)
+        d, w = h.shape
+        self._check(self._L.sph_dem_set_terrain(self._h, _ptr(h), w, d), "sph_dem_set_terrain")
 
     def replace(self, grains: np.ndarray) -> int:
         g = np.ascontiguousarray(grains, dtype=GRAIN_DTYPE)

@@ -345,7 +345,25 @@ void sph_dem_destroy(sph_dem* dem);
 sph_status sph_dem_replace(sph_dem* dem, const SphGrain80* grains, uint32_t n);
 /* GpuParticles::set_params (:304). */
 sph_status sph_dem_set_params(sph_dem* dem, const sph_dem_params* p);
-/* GpuParticles::dispatch (:255): `substeps` × (contact gather, implicit velocity solve, drift). */
+/* The ground scene's medium and thermal constants (particle_step.wgsl:16-50 Params: center, air_rho,
+ * drag_cd, specific_heat, cool_rate). All zero (the default) is vacuum without cooling. */
+typedef struct sph_dem_ground {
+  float center[3];       /* world.center(): centred coordinates + center = the heightfield's voxel coordinates */
+  float air_rho;         /* kg/m³ (0 = vacuum: no drag) */
+  float drag_cd;         /* drag coefficient */
+  float specific_heat;   /* J/(kg K): u = c·T; grains cool toward c·300 K */
+  float cool_rate;       /* 1/s */
+  float reserved;
+} sph_dem_ground;
+sph_status sph_dem_set_ground(sph_dem* dem, const sph_dem_ground* g);
+/* The terrain (binding 2 of particle_step.wgsl): a w × d heightfield of column tops in voxel units, row-major
+ * heights[z·w + x]; copied to the device. w = d = 0 removes it. With a terrain, each substep resolves terrain
+ * contact as the reference's non-injecting constraint (cs_integrate :477-576: into-surface velocity removed,
+ * Coulomb friction bounded by μ·Jn, a velocity-free position projection capped at 1 cm and by the headroom to
+ * the grain resting above) and counts grounded substeps in `resting`; without one, `resting` stays 0. */
+sph_status sph_dem_set_terrain(sph_dem* dem, const int32_t* heights, uint32_t w, uint32_t d);
+/* GpuParticles::dispatch (:255): `substeps` × (contact gather, implicit velocity solve, drift, then drag,
+ * cooling and terrain contact as set above). */
 sph_status sph_dem_step(sph_dem* dem, uint32_t substeps);
 /* begin_readback/take_readback (:314-320), blocking: the grains in original order. */
 sph_status sph_dem_readback(sph_dem* dem, SphGrain80* out, uint32_t cap, uint32_t* n_out);

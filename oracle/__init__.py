@@ -455,3 +455,31 @@ def assemble(particles, placements):
     soft, dt = C.c_float(), C.c_float()
     m = L.orc_assemble(p, len(p), pl, len(pl), out, C.byref(soft), C.byref(dt))
     return out[:m].copy().view(src.dtype).reshape(-1), soft.value, dt.value
+
+
+def dem_ground_step32(grains, prm, ground, heights=None, substeps=1):
+    """The ground scene's substeps (contacts + integrate with cooling, drag, terrain, settle counter, glow) on a
+    GRAIN_DTYPE array; ground = (center xyz, air_rho, drag_cd, specific_heat, cool_rate); heights[z, x] or None."""
+    L = lib()
+    i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+    L.orc_dem_ground_step32.argtypes = [f32p, f32p, f32p, f32p, f32p, f32p, f32p, C.c_int, f32p, f32p,
+                                        C.c_void_p, C.c_int, C.c_int]
+    g = np.array(grains, copy=True)
+    pos = np.ascontiguousarray(g["offset"], np.float32)
+    vel = np.ascontiguousarray(g["vel"], np.float32)
+    u = np.ascontiguousarray(g["u"], np.float32)
+    rest = np.ascontiguousarray(g["resting"], np.float32)
+    emis = np.ascontiguousarray(g["emission"], np.float32)
+    rad = np.ascontiguousarray(g["radius"], np.float32)
+    rho = np.ascontiguousarray(g["rho"], np.float32)
+    gr = np.ascontiguousarray(ground, np.float32)
+    if heights is None:
+        hp, w, d = None, 0, 0
+    else:
+        h = np.ascontiguousarray(heights, np.int32)
+        d, w = h.shape
+        hp = h.ctypes.data_as(C.c_void_p)
+    for _ in range(substeps):
+        L.orc_dem_ground_step32(pos, vel, rad, rho, u, rest, emis, len(g), _c(prm, np.float32), gr, hp, w, d)
+    g["offset"], g["vel"], g["u"], g["resting"], g["emission"] = pos, vel, u, rest, emis
+    return g

@@ -1056,7 +1056,7 @@ void orc_conservation64(const double* pos3, const double* vel3, const double* ma
 }
 
 // ---- granular contact (shaders/particle_step.wgsl:140-211 contact_accel, :273-336 cs_forces, :477-530
-// cs_integrate without terrain, drag, cooling and render state) ----------------------------------------
+// cs_integrate; the ground scene's terrain, drag, cooling and settle counter in orc_dem_ground_step32) -------
 // params: [c_stiffness, c_normal_damp, c_friction, c_tangent_damp, c_cohesion, dt, gx, gy, gz]
 // accum16 per grain: force.xyz, headroom, s_diag.xyz, 0, s_off.xyz (xy, xz, yz), 0, sv_nbr.xyz, 0
 static const float kDemTheta = 0.70f;                       // particle_step.wgsl:125
@@ -1573,6 +1573,144 @@ int orc_assemble(const float* P, int n, const double* pl, int np, float* out, fl
   *softening = 0.25f * min_h;
   *dt = (float)(0.01 * (double)min_h / (20000.0 + vmax));
   return m;
+}
+
+}  // extern "C"
+
+// ---- the ground scene: particle_step.wgsl:338-452 (terrain_top/_h/_surface, terrain_resolve), :282-336
+// (headroom), :477-576 (cs_integrate with cooling, drag, terrain contact, settle counter, incandescence) -----
+struct OrcGround {
+  float cx, cy, cz, air_rho, drag_cd, specific_heat, cool_rate;
+  const int* hf;
+  int w, d;
+};
+static float orc_terrain_top(const OrcGround& g, int cx, int cz) {
+  const int x = std::min(std::max(cx, 0), g.w - 1), z = std::min(std::max(cz, 0), g.d - 1);
+  return ((float)g.hf[z * g.w + x] - g.cy) - 0.5f;
+}
+static float orc_mix(float a, float b, float t) { return a * (1.0f - t) + b * t; }
+static void orc_terrain_surface(const OrcGround& g, float px, float pz, float s[3]) {
+  const float vx = px + g.cx, vz = pz + g.cz;
+  const int cx = (int)std::floor(vx), cz = (int)std::floor(vz);
+  const float h00 = orc_terrain_top(g, cx, cz), h10 = orc_terrain_top(g, cx + 1, cz);
+  const float h01 = orc_terrain_top(g, cx, cz + 1), h11 = orc_terrain_top(g, cx + 1, cz + 1);
+  const float fx = vx - (float)cx, fz = vz - (float)cz;
+  s[0] = orc_mix(orc_mix(h00, h10, fx), orc_mix(h01, h11, fx), fz);
+  s[1] = orc_mix(h10 - h00, h11 - h01, fz);
+  s[2] = orc_mix(h01 - h00, h11 - h10, fx);
+}
+static void orc_terrain_normal(const float s[3], float n[3]) {
+  const float nx = -s[1], nz = -s[2];
+  const float l = std::sqrt((nx * nx + 1.0f * 1.0f) + nz * nz);
+  n[0] = nx / l;
+  n[1] = 1.0f / l;
+  n[2] = nz / l;
+}
+
+extern "C" {
+
+// One substep of the ground scene for n grains (f32, as the shader). ground[7] = center xyz, air_rho, drag_cd,
+// specific_heat, cool_rate; hf = w × d heights or null. rho = grain densities; u, resting, emission3 updated.
+void orc_dem_ground_step32(float* pos3, float* vel3, const float* radius, const float* rho, float* u,
+                           float* resting, float* emission3, int n, const float* prm, const float* ground,
+                           const int* hf, int w, int d) {
+  const OrcGround g{ground[0], ground[1], ground[2], ground[3], ground[4], ground[5], ground[6], hf, w, d};
+  std::vector<float> acc((size_t)n * 16, 0.0f);
+  for (int i = 0; i < n; ++i) {
+    float* a = &acc[16 * (size_t)i];
+    a[3] = 1.0e30f;
+    float tn[3] = {0.0f, 1.0f, 0.0f};
+    if (hf) {
+      float s[3];
+      orc_terrain_surface(g, pos3[3 * i], pos3[3 * i + 2], s);
+      orc_terrain_normal(s, tn);
+    }
+    for (int j = 0; j < n; ++j) {
+      if (j == i) continue;
+      dem_contact32(&pos3[3 * i], &vel3[3 * i], radius[i], &pos3[3 * j], &vel3[3 * j], radius[j], prm, a);
+      if (hf) {
+        const float dj[3] = {pos3[3 * j] - pos3[3 * i], pos3[3 * j + 1] - pos3[3 * i + 1],
+                             pos3[3 * j + 2] - pos3[3 * i + 2]};
+        if ((dj[0] * tn[0] + dj[1] * tn[1]) + dj[2] * tn[2] > 0.0f)
+          a[3] = std::min(a[3], std::max(std::sqrt((dj[0] * dj[0] + dj[1] * dj[1]) + dj[2] * dj[2]) -
+                                             (radius[i] + radius[j]), 0.0f));
+      }
+    }
+  }
+  const float rho_t = (1.0f - kDemTheta) / kDemTheta, dt = prm[5];
+  for (int i = 0; i < n; ++i) {
+    const float* a = &acc[16 * (size_t)i];
+    float* v = vel3 + 3 * i;
+    float* p = pos3 + 3 * i;
+    const float u_amb = g.specific_heat * 300.0f;
+    u[i] = u_amb + (u[i] - u_amb) * std::exp(-g.cool_rate * dt);
+    float ax[3] = {prm[6] + a[0], prm[7] + a[1], prm[8] + a[2]};
+    const float sp = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    if (g.air_rho > 0.0f && sp > 1.0e-9f) {
+      const float s_grain = std::max(2.0f * radius[i], 1.0e-6f);
+      const float a_drag = 0.5f * g.air_rho * sp * sp * g.drag_cd / (std::max(rho[i], 1.0e-6f) * s_grain);
+      for (int k = 0; k < 3; ++k) ax[k] -= (a_drag / sp) * v[k];
+    }
+    const float sdx = a[4], sdy = a[5], sdz = a[6], sxy = a[8], sxz = a[9], syz = a[10];
+    const float sv[3] = {sdx * v[0] + sxy * v[1] + sxz * v[2], sxy * v[0] + sdy * v[1] + syz * v[2],
+                         sxz * v[0] + syz * v[1] + sdz * v[2]};
+    float rhs[3];
+    for (int k = 0; k < 3; ++k) rhs[k] = v[k] - rho_t * sv[k] + (1.0f / kDemTheta) * a[12 + k] + ax[k] * dt;
+    const float m00 = 1.0f + sdx, m11 = 1.0f + sdy, m22 = 1.0f + sdz, m01 = sxy, m02 = sxz, m12 = syz;
+    const float c00 = m11 * m22 - m12 * m12, c01 = m02 * m12 - m01 * m22, c02 = m01 * m12 - m02 * m11;
+    const float c11 = m00 * m22 - m02 * m02, c12 = m01 * m02 - m00 * m12, c22 = m00 * m11 - m01 * m01;
+    const float inv_det = 1.0f / (m00 * c00 + m01 * c01 + m02 * c02);
+    float vn[3] = {(c00 * rhs[0] + c01 * rhs[1] + c02 * rhs[2]) * inv_det,
+                   (c01 * rhs[0] + c11 * rhs[1] + c12 * rhs[2]) * inv_det,
+                   (c02 * rhs[0] + c12 * rhs[1] + c22 * rhs[2]) * inv_det};
+    float q[3];
+    for (int k = 0; k < 3; ++k) q[k] = p[k] + (v[k] + vn[k]) * (0.5f * dt);
+    float rest = 0.0f;
+    if (hf) {
+      float s[3];
+      orc_terrain_surface(g, q[0], q[2], s);
+      const float pen = s[0] - (q[1] - radius[i]);
+      if (pen > 0.0f) {
+        float nn[3];
+        orc_terrain_normal(s, nn);
+        const float vdn = vn[0] * nn[0] + vn[1] * nn[1] + vn[2] * nn[2];
+        float jn = 0.0f;
+        if (vdn < 0.0f) {
+          jn = -vdn;
+          for (int k = 0; k < 3; ++k) vn[k] += jn * nn[k];
+        }
+        const float vd = vn[0] * nn[0] + vn[1] * nn[1] + vn[2] * nn[2];
+        const float t[3] = {vn[0] - vd * nn[0], vn[1] - vd * nn[1], vn[2] - vd * nn[2]};
+        const float vt = std::sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
+        if (vt > 1.0e-9f) {
+          const float dv = std::min(prm[2] * jn, vt);
+          for (int k = 0; k < 3; ++k) vn[k] -= (t[k] / vt) * dv;
+        }
+        const float dp = std::min(std::min(pen, 0.01f), a[3]);
+        for (int k = 0; k < 3; ++k) q[k] += dp * nn[k];
+      }
+      float s2[3];
+      orc_terrain_surface(g, q[0], q[2], s2);
+      rest = q[1] - radius[i] <= s2[0] + 0.1f ? resting[i] + 1.0f : 0.0f;
+    }
+    resting[i] = rest;
+    for (int k = 0; k < 3; ++k) {
+      p[k] = q[k];
+      v[k] = vn[k];
+    }
+    const float temp = u[i] / std::max(g.specific_heat, 1.0f);
+    float* e = emission3 + 3 * i;
+    e[0] = e[1] = e[2] = 0.0f;
+    if (temp > 800.0f) {
+      const float x = temp - 800.0f;
+      const float inten = std::min(std::max(x / 2200.0f, 0.0f), 4.0f);
+      const float gg = std::min(std::max(x / 2200.0f, 0.0f), 1.0f);
+      const float bb = std::min(std::max((temp - 2600.0f) / 2400.0f, 0.0f), 1.0f);
+      e[0] = inten;
+      e[1] = gg * inten;
+      e[2] = bb * inten;
+    }
+  }
 }
 
 }  // extern "C"
