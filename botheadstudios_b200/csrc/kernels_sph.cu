@@ -19,14 +19,25 @@ __device__ __forceinline__ float pair_h(float hi, float hj) { return fmul(0.5f, 
 
 // The gather kernels walk a particle's list kGather entries at a time: all of a chunk's indices are loaded,
 // then all of its neighbour records, before any is used, so each thread keeps kGather gathers in flight
-// instead of one dependent chain. `lst` is the particle's first list slot (entries 32 apart, interleaved);
-// slots past the count read the particle itself (harmless filler, never summed).
+// instead of one dependent chain; the next chunk's indices are requested before this chunk's records, so the
+// list stream (HBM) overlaps the record gathers (mostly L1/L2) and the arithmetic. `lst` is the particle's
+// first list slot (entries 32 apart, interleaved); slots past the count read the particle itself (harmless
+// filler, never summed).
 constexpr int kGather = 4;
+template <int G>
+__device__ __forceinline__ void list_chunk(const unsigned* __restrict__ lst, unsigned k0, unsigned c, unsigned self,
+                                           unsigned j[G]) {
+#pragma unroll
+  for (int u = 0; u < G; ++u) j[u] = k0 + u < c ? lst[(size_t)(k0 + u) * 32u] : self;
+}
+// Records of the chunk whose indices are in `jn` (k0 = its first slot); on return jn holds the next chunk's.
 __device__ __forceinline__ void gather_pos_mass(const State& st, const unsigned* __restrict__ lst, unsigned k0,
-                                                unsigned c, unsigned self, float4 pj[kGather], float mj[kGather]) {
+                                                unsigned c, unsigned self, unsigned jn[kGather],
+                                                float4 pj[kGather], float mj[kGather]) {
   unsigned j[kGather];
 #pragma unroll
-  for (int u = 0; u < kGather; ++u) j[u] = k0 + u < c ? lst[(size_t)(k0 + u) * 32u] : self;
+  for (int u = 0; u < kGather; ++u) j[u] = jn[u];
+  list_chunk<kGather>(lst, k0 + kGather, c, self, jn);
 #pragma unroll
   for (int u = 0; u < kGather; ++u) {
     pj[u] = st.pos_h[j[u]];
@@ -61,10 +72,12 @@ __global__ void k_density_eos(int n, State st, const unsigned* __restrict__ nbr,
   float r_i = m * w;
   const unsigned c = min(nbr_cnt[t], cap);
   const unsigned* lst = nbr + nbr_slot((unsigned)t, 0u, cap);
+  unsigned jn[kGather];
+  list_chunk<kGather>(lst, 0u, c, (unsigned)t, jn);
   for (unsigned k0 = 0; k0 < c; k0 += kGather) {
     float4 pj[kGather];
     float mj[kGather];
-    gather_pos_mass(st, lst, k0, c, (unsigned)t, pj, mj);
+    gather_pos_mass(st, lst, k0, c, (unsigned)t, jn, pj, mj);
 #pragma unroll
     for (int u = 0; u < kGather; ++u) {
       if (k0 + u >= c) break;
@@ -121,10 +134,12 @@ __device__ __forceinline__ void h_sums(int t, const State& st, const unsigned* _
   drho = m * dwdh;
   const unsigned c = min(nbr_cnt[t], cap);
   const unsigned* lst = nbr + nbr_slot((unsigned)t, 0u, cap);
+  unsigned jn[kGather];
+  list_chunk<kGather>(lst, 0u, c, (unsigned)t, jn);
   for (unsigned k0 = 0; k0 < c; k0 += kGather) {
     float4 pj[kGather];
     float mj[kGather];
-    gather_pos_mass(st, lst, k0, c, (unsigned)t, pj, mj);
+    gather_pos_mass(st, lst, k0, c, (unsigned)t, jn, pj, mj);
 #pragma unroll
     for (int u = 0; u < kGather; ++u) {
       if (k0 + u >= c) break;
@@ -353,12 +368,16 @@ __global__ void k_forces(int n, State st, const float4* __restrict__ fdata, cons
     float ax = 0.f, ay = 0.f, az = 0.f, de = 0.f, dv = 0.f;
     const unsigned c = min(nbr_cnt[t], cap);
     const unsigned* lst = nbr + nbr_slot((unsigned)t, 0u, cap);
+    unsigned jn[kForceGather];
+    list_chunk<kForceGather>(lst, 0u, c, (unsigned)t, jn);
     for (unsigned k0 = 0; k0 < c; k0 += kForceGather) {
-      // a chunk's indices, then its positions, velocities and force records, all in flight together
+      // a chunk's positions, velocities and force records in flight together, the next chunk's indices
+      // requested ahead of them
       unsigned jj[kForceGather];
       float4 pjs[kForceGather], vjs[kForceGather], fjs[kForceGather];
 #pragma unroll
-      for (int u = 0; u < kForceGather; ++u) jj[u] = k0 + u < c ? lst[(size_t)(k0 + u) * 32u] : (unsigned)t;
+      for (int u = 0; u < kForceGather; ++u) jj[u] = jn[u];
+      list_chunk<kForceGather>(lst, k0 + kForceGather, c, (unsigned)t, jn);
 #pragma unroll
       for (int u = 0; u < kForceGather; ++u) {
         pjs[u] = st.pos_h[jj[u]];
