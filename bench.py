@@ -225,16 +225,19 @@ def plain_sequential(wl: dict, B, device: int, impacts: int = 16, steps: int = 2
     workload's untuned configuration, no graph (the reference's offline driver runs impacts sequentially)."""
     from botheadstudios_b200 import workloads
     from botheadstudios_b200.gpusph import GpuSph
-    tot_ps, tot_ms = 0, 0.0
+    tot_ps, tot_ms, res = 0, 0.0, 0.0
     for k in range(min(impacts, B.n_impacts)):
         p = B.impact(k)
-        with GpuSph(len(p), device=device, **workloads.config(wl, B, graph=0)) as s:
+        # the plain form is the iterated smoothing-length solve, whatever the workload's own form
+        with GpuSph(len(p), device=device, **workloads.config(wl, B, graph=0, h_mode=1)) as s:
             s.upload(p, B.eos, float(B.softening[k]))
             s.encode_kdk(1)
             s.sync()
             tot_ms += timed([s], s.encode_kdk, steps, max(device, 0))
             tot_ps += len(p) * steps
-    return dict(value=tot_ps / (tot_ms / 1000.0), impacts=min(impacts, B.n_impacts), steps=steps)
+            res = max(res, s.diag()["h_residual"])
+    return dict(value=tot_ps / (tot_ms / 1000.0), impacts=min(impacts, B.n_impacts), steps=steps,
+                h_residual_max=res)
 
 
 # ---------------------------------------------------------------------------------------------------------

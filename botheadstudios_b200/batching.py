@@ -53,6 +53,14 @@ def _time_steps(s: GpuSph, steps: int) -> float:
     return e0.elapsed_time(e1)
 
 
+def _load_network(s, cfg: dict):
+    """The learned smoothing-length form needs the trained network in every context (progress held at 0.5)."""
+    if cfg.get("h_mode") in (2, "learned"):
+        from . import learned_h
+        s.mlp_set(learned_h.load())
+        s.set_progress(0.5)
+
+
 class Autotuner:
     """Coordinate search over CANDIDATES (leaf size, then walk tile, then block size), each candidate timed on
     the same probe batch: a fresh context, one warm-up step (the full rebuild), `steps` timed steps."""
@@ -76,6 +84,7 @@ class Autotuner:
         """Particle-steps/s of `choice` on the probe batch."""
         cfg = dict(self.base, **choice)
         with GpuSph(len(probe.particles), device=self.device, **cfg) as s:
+            _load_network(s, cfg)
             s.upload_batch(probe.particles, probe.offsets, probe.eos, probe.softening)
             s.encode_kdk(1)
             s.sync()
@@ -122,6 +131,7 @@ class BucketedBatch:
             sub = subset(self.batch, range(k0, k1))
             cfg = dict(base, **choices.get(b, DEFAULT_CHOICE))
             s = GpuSph(len(sub.particles), device=device, **cfg)
+            _load_network(s, cfg)
             self.ctxs.append(s)
             self.sub.append(sub)
             self.ranges.append((int(self.batch.offsets[k0]), int(self.batch.offsets[k1])))

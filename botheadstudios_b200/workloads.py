@@ -29,6 +29,11 @@ WORKLOADS = {
     # replayed from a captured CUDA graph
     "batch_256": dict(kind="batch", n_impacts=256, n_min=20_000, n_max=200_000, n_ngb=64.0, kernel="wendland",
                       theta=0.6, quad=1, leaf=16, h_solve=1, max_nbr=192, graph=1, autotune=1),
+    # the learned smoothing-length form of the same 256 impacts (the network proposes h, Newton only where the
+    # proposal's residual check fails), batched and graphed as above
+    "batch_256_learned": dict(kind="batch", n_impacts=256, n_min=20_000, n_max=200_000, n_ngb=64.0,
+                              kernel="wendland", theta=0.6, quad=1, leaf=16, h_solve=2, max_nbr=192, graph=1,
+                              autotune=1),
     # the same draw with 16 impacts (a quick check of the batched path)
     "batch_16": dict(kind="batch", n_impacts=16, n_min=20_000, n_max=200_000, n_ngb=64.0, kernel="wendland",
                      theta=0.6, quad=1, leaf=16, h_solve=1, max_nbr=192, graph=1, autotune=1),
