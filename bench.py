@@ -40,9 +40,20 @@ from botheadstudios_b200.workloads import WORKLOADS, n_particles  # noqa: E402
 # Algorithmic bytes per particle per phase execution (state read/written once, SoA f32/f64 layout):
 # sort = bbox/Morton 40 + radix (key,idx) 16 + permutation 132; tree = 20 + 304/L per particle;
 # gravity 32; neighbours 36 (pos 16 + list write 4·k_avg counted separately); density 28 + EOS 20;
-# forces 64; integrate: kick-drift 128 + kick 48 + CFL 36 per step (two phase executions).
+# forces 64; integrate: kick-drift 128 + kick 48 + CFL 36 per step (two phase executions). The gather phases
+# also stream each particle's neighbour list from HBM (4 B per entry, once per gather pass): LIST_PASSES.
 BYTES_PER_PARTICLE = dict(sort=188.0, tree=39.0, gravity=32.0, neighbours=16.0, hsolve=28.0, density=48.0,
                           forces=64.0, integrate=106.0)
+
+
+def list_passes(wl: dict) -> dict:
+    """Neighbour-list reads per particle per phase call: one per gather pass (the plain smoothing-length solve
+    makes h_iters + 1 = 3; the learned form's first check is counted alone, a lower bound)."""
+    return dict(forces=1, density=1, hsolve=3 if wl.get("h_solve") == 1 else 1)
+
+
+def phase_bytes(k: str, wl: dict, lbar: float) -> float:
+    return BYTES_PER_PARTICLE[k] + 4.0 * lbar * list_passes(wl).get(k, 0)
 
 
 def peaks():
@@ -336,6 +347,14 @@ def run_ours(args, wl, world, rank, local, pg):
     def dsum(ds, key):
         return sum(d[key] for d in ds)
 
+    # mean neighbour-list length (the lists the gather phases stream)
+    lsum, lcnt = 0.0, 0
+    for s in runner.ctxs:
+        c = s.inspect("NBR_COUNT").astype(np.float64)
+        lsum += float(c.sum())
+        lcnt += len(c)
+    lbar = lsum / max(lcnt, 1)
+
     # ---- end to end through the public API: per step, upload the state from pinned host memory, one KDK
     # step, read the state back into host memory ----
     pin = torch.empty(n * 48, dtype=torch.uint8, pin_memory=True).numpy().view(runner.batch.particles.dtype)
@@ -365,7 +384,7 @@ def run_ours(args, wl, world, rank, local, pg):
         calls = prof["calls"][k]
         if calls == 0 or t <= 0:
             continue
-        b = BYTES_PER_PARTICLE[k] * prof["pcalls"][k]  # particles processed over all calls
+        b = phase_bytes(k, wl, lbar) * prof["pcalls"][k]  # particles processed over all calls
         phases[k] = dict(ms=round(t, 4), share=round(t / sum(prof["ms"].values()), 4), calls=calls,
                          gbs=round(b / (t / 1000.0) / 1e9, 1))
     dom = max(phases, key=lambda k: phases[k]["ms"])
@@ -395,18 +414,19 @@ def run_ours(args, wl, world, rank, local, pg):
                     interactions_per_particle=dict(multipole=m2p / n_per_call, pairwise=p2p / n_per_call,
                                                    nodes=vis / n_per_call))
     else:
-        dom_bytes = BYTES_PER_PARTICLE[dom] * n_per_call
+        dom_bytes = phase_bytes(dom, wl, lbar) * n_per_call
         achieved = dom_bytes / (dom_ms / 1000.0) / 1e9
         roof = dict(bound="hbm", kernel_phase=dom, achieved=round(achieved, 1), peak=pk["hbm"], unit="GB/s",
                     frac=round(achieved / pk["hbm"], 4), traffic=traffic, peak_source=pk["src"],
                     bytes_per_launch=dom_bytes, ms_per_launch=round(dom_ms, 4))
     # memory-bound phases against the measured HBM copy bandwidth
     mem = [k for k in ("sort", "tree", "density", "forces", "integrate", "hsolve") if k in phases]
-    mem_bytes = sum(BYTES_PER_PARTICLE[k] * prof["pcalls"][k] for k in mem)
+    mem_bytes = sum(phase_bytes(k, wl, lbar) * prof["pcalls"][k] for k in mem)
     mem_ms = sum(phases[k]["ms"] for k in mem)
     roof_hbm = dict(bound="hbm", phases=mem, achieved=round(mem_bytes / (mem_ms / 1000.0) / 1e9, 1),
                     peak=pk["hbm"], unit="GB/s", frac=round(mem_bytes / (mem_ms / 1000.0) / 1e9 / pk["hbm"], 4),
-                    peak_source=pk["src"])
+                    peak_source=pk["src"], mean_list_entries=round(lbar, 1),
+                    per_phase={k: round(phases[k]["gbs"] / pk["hbm"], 4) for k in mem})
     # ---- CPU baseline on the host cores (rank 0, N=1 only) ----
     cpu = None
     if world == 1 and not args.no_cpu:
