@@ -141,13 +141,30 @@ def barrier(pg):
         pg.barrier()
 
 
-def max_over_ranks(pg, v: float, local: int) -> float:
+def _reduce(pg, v: float, local: int, op: str) -> float:
+    """All-reduce one number over the ranks (NCCL on the rank's GPU; gloo on the host)."""
     if pg is None:
         return v
     import torch
-    t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{local}")
-    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    dev = "cpu" if pg.get_backend() == "gloo" else f"cuda:{local}"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
+    pg.all_reduce(t, op=getattr(pg.ReduceOp, op))
     return float(t.item())
+
+
+def max_over_ranks(pg, v: float, local: int) -> float:
+    """The slowest rank's time: replicas are timed on the device, the job takes the maximum."""
+    return _reduce(pg, v, local, "MAX")
+
+
+def sum_over_ranks(pg, v: float, local: int) -> float:
+    """Work summed over the replicas (each rank's workload is its own seeded draw, so sizes may differ)."""
+    return _reduce(pg, v, local, "SUM")
+
+
+def replica_value(pg, units_local: float, ms_local: float, local: int) -> float:
+    """Whole-job throughput of independent replicas: the units all ranks processed ÷ the slowest rank's time."""
+    return sum_over_ranks(pg, units_local, local) / (max_over_ranks(pg, ms_local, local) / 1000.0)
 
 
 def build_workload(wl: dict, seed: int):
@@ -326,7 +343,7 @@ def run_ours(args, wl, world, rank, local, pg):
     barrier(pg)
     launches = sum(s.profile_read()["kernel_launches"] for s in runner.ctxs)
     ms_max = max_over_ranks(pg, ms, local)
-    value = n * args.steps * world / (ms_max / 1000.0)
+    value = replica_value(pg, n * args.steps, ms, local)
     # per-phase breakdown and walk counters: a few more steps with phase events (eager launches), one
     # context at a time so that every kernel duration is its own
     prof = dict(ms={}, calls={})
@@ -360,15 +377,16 @@ def run_ours(args, wl, world, rank, local, pg):
     pin = torch.empty(n * 48, dtype=torch.uint8, pin_memory=True).numpy().view(runner.batch.particles.dtype)
     runner.readback_into(pin)
     e2e_steps = max(2, min(args.steps, 10))
+
+    def e2e_run(k):
+        for _ in range(k):
+            runner.upload(pin)          # H2D of the step's input state from pinned memory
+            runner.encode_kdk(1)
+            runner.readback_into(pin)   # D2H of the step's result into the same pinned buffer
+
     barrier(pg)
-    t0 = time.perf_counter()
-    for _ in range(e2e_steps):
-        runner.upload(pin)          # H2D of the step's input state from pinned memory
-        runner.encode_kdk(1)
-        runner.readback_into(pin)   # D2H of the step's result into the same pinned buffer
-    e2e_s = time.perf_counter() - t0
-    e2e_s = max_over_ranks(pg, e2e_s, local)
-    e2e_value = n * e2e_steps * world / e2e_s
+    e2e_ms = timed(runner.ctxs, e2e_run, e2e_steps, local)  # device events around the whole sequence
+    e2e_value = replica_value(pg, n * e2e_steps, e2e_ms, local)
     plain = None
     if wl.get("kind") == "batch" and rank == 0 and not args.no_plain:
         plain = plain_sequential(wl, I, local)
@@ -511,19 +529,20 @@ def run_measure(args, world, rank, local, pg):
         e2e = [one(True) for _ in range(args.steps)]
         barrier(pg)
         res = s.measure_disk(0, variant=args.variant)
+    value = replica_value(pg, n, sum(dev) / len(dev), local)
+    value_e2e = replica_value(pg, n, sum(e2e) / len(e2e), local)
     ms = max_over_ranks(pg, sum(dev) / len(dev), local)
-    ms_e2e = max_over_ranks(pg, sum(e2e) / len(e2e), local)
     if rank != 0:
         return
     cpu = None
     if not args.no_cpu and world == 1:
         cpu = measure_reference_run(p, args.variant)
-    line = dict(metric=MEASURE_METRIC, value=n * world / (ms / 1000.0), unit="particles/s", n_gpus=world,
+    line = dict(metric=MEASURE_METRIC, value=value, unit="particles/s", n_gpus=world,
                 steps=args.steps, warmup=args.warmup, ms_per_step=ms, higher_is_better=True, scaling="weak",
                 vs_baseline=None, dtype="f64", data="synthetic",
                 config=dict(workload=args.measure_workload, particles=n, disk_particles=res["n_disk"],
                             variant=args.variant, l2="flushed (256 MB write) before every measurement"),
-                e2e=dict(value=n * world / (ms_e2e / 1000.0), unit="particles/s", h2d_bytes_per_step=48 * n,
+                e2e=dict(value=value_e2e, unit="particles/s", h2d_bytes_per_step=48 * n,
                          d2h_bytes_per_step=112),
                 gpu_launches=int(launches), result=res)
     if cpu is not None:
