@@ -137,10 +137,9 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
       const int li = lane / K, off = lane % K;
       float4 src = make_float4(3.0e18f, 3.0e18f, 3.0e18f, 0.0f);  // padding: massless and far away
       if (li < nl) {
-        const unsigned lf = S.p2f[w][base + li];
-        const int s = (int)leaf_start[lf] + off;
-        if (s < (int)leaf_start[lf + 1]) {
-          src = body[s];
+        const unsigned e = S.p2f[w][base + li];  // first source << 5 | (sources − 1)
+        if (off <= (int)(e & 31u)) {
+          src = body[(e >> 5) + off];
           src.w *= G;
         }
       }
@@ -224,9 +223,8 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
       const int li = lane / K, off = lane % K;
       int sidx = -1;
       if (li < nl) {
-        const unsigned lf = S.p2p[w][base + li];
-        const int s = (int)leaf_start[lf] + off;
-        if (s < (int)leaf_start[lf + 1]) sidx = s;
+        const unsigned e = S.p2p[w][base + li];  // first source << 5 | (sources − 1)
+        if (off <= (int)(e & 31u)) sidx = (int)(e >> 5) + off;
       }
       float4 src = make_float4(3.0e18f, 3.0e18f, 3.0e18f, 0.0f);  // padding: massless and far away
       float hsrc = 0.0f;
@@ -292,9 +290,14 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
     const unsigned node = have ? stack[sp + lane] : 0u;
     __syncwarp();
     bool acc_node = false, leaf = false, open = false, near_leaf = false;
+    unsigned ls0 = 0u, ls1 = 1u;  // a leaf's source range, loaded alongside its box
     if (have) {
       const float4 bl = nbmin[node], bh = nbmax[node];
       const bool is_leaf = node >= leaf0;
+      if (is_leaf) {
+        ls0 = leaf_start[node - leaf0];
+        ls1 = leaf_start[node - leaf0 + 1];
+      }
       bool near = false;
       {
         // SPH reach (or, for gravity alone, plain overlap with the group box so that a group's own leaves
@@ -317,6 +320,7 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
       if (mac && !near) acc_node = true;
       else if (is_leaf) leaf = GRAV || near;
       else open = GRAV || (NBR && near);
+      if (is_leaf && ls1 <= ls0) acc_node = leaf = false;  // an empty leaf (none are built) adds nothing
       near_leaf = leaf && near;
     }
     const unsigned bm = __ballot_sync(SPH_FULL_MASK, acc_node);
@@ -325,8 +329,12 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
     const unsigned bn = __ballot_sync(SPH_FULL_MASK, near_leaf);
     const unsigned bfar = bf & ~bn;
     if (acc_node) S.m2p[w][nm + __popc(bm & lt)] = node;
-    if (near_leaf) S.p2p[w][np + __popc(bn & lt)] = node - leaf0;
-    else if (leaf) S.p2f[w][nf + __popc(bfar & lt)] = node - leaf0;
+    if (leaf) {
+      // list entries carry the leaf's source range (capacity <= 2^26 particles, leaves <= 32 sources)
+      const unsigned e = (ls0 << 5) | min(ls1 - ls0 - 1u, 31u);
+      if (near_leaf) S.p2p[w][np + __popc(bn & lt)] = e;
+      else S.p2f[w][nf + __popc(bfar & lt)] = e;
+    }
     const int no = __popc(bo);
     if (sp + 2 * no <= TW_STACK) {
       if (open) {
