@@ -130,19 +130,25 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
   __syncwarp();
 
   // ---- far leaves: branch-free pairwise gravity, 32 staged sources per pass ---------------------------
+  // The next chunk's sources are loaded into registers before this chunk is evaluated, so the gather
+  // overlaps the arithmetic.
+  auto far_source = [&](int base, int count) {
+    const int per = 32 / K;
+    const int li = lane / K, off = lane % K;
+    float4 src = make_float4(3.0e18f, 3.0e18f, 3.0e18f, 0.0f);  // padding: massless and far away
+    if (li < min(per, count - base)) {
+      const unsigned e = S.p2f[w][base + li];  // first source << 5 | (sources − 1)
+      if (off <= (int)(e & 31u)) src = body[(e >> 5) + off];
+    }
+    return src;
+  };
   auto flush_far = [&](int count) {
     const int per = 32 / K;
+    float4 nxt = far_source(0, count);
     for (int base = 0; base < count; base += per) {
-      const int nl = min(per, count - base);
-      const int li = lane / K, off = lane % K;
-      float4 src = make_float4(3.0e18f, 3.0e18f, 3.0e18f, 0.0f);  // padding: massless and far away
-      if (li < nl) {
-        const unsigned e = S.p2f[w][base + li];  // first source << 5 | (sources − 1)
-        if (off <= (int)(e & 31u)) {
-          src = body[(e >> 5) + off];
-          src.w *= G;
-        }
-      }
+      float4 src = nxt;
+      if (base + per < count) nxt = far_source(base + per, count);
+      src.w *= G;
       S.src[w][lane] = src;
       __syncwarp();
       if (valid) {
@@ -216,23 +222,33 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
   };
 
   // ---- direct list: leaves of <= K sources (K divides 32), 32 sources per chunk ------------------------
+  auto near_source = [&](int base, int count, float4& src, float& hsrc) {
+    const int per = 32 / K;  // leaves per chunk
+    const int li = lane / K, off = lane % K;
+    int sidx = -1;
+    if (li < min(per, count - base)) {
+      const unsigned e = S.p2p[w][base + li];  // first source << 5 | (sources − 1)
+      if (off <= (int)(e & 31u)) sidx = (int)(e >> 5) + off;
+    }
+    src = make_float4(3.0e18f, 3.0e18f, 3.0e18f, 0.0f);  // padding: massless and far away
+    hsrc = 0.0f;
+    if (sidx >= 0) {
+      src = body[sidx];
+      if (NBR) hsrc = pos_h[sidx].w;
+    }
+    return sidx;
+  };
   auto flush_p2p = [&](int count) {
     const int per = 32 / K;  // leaves per chunk
+    float4 nsrc;
+    float nh;
+    int nidx = near_source(0, count, nsrc, nh);
     for (int base = 0; base < count; base += per) {
-      const int nl = min(per, count - base);
-      const int li = lane / K, off = lane % K;
-      int sidx = -1;
-      if (li < nl) {
-        const unsigned e = S.p2p[w][base + li];  // first source << 5 | (sources − 1)
-        if (off <= (int)(e & 31u)) sidx = (int)(e >> 5) + off;
-      }
-      float4 src = make_float4(3.0e18f, 3.0e18f, 3.0e18f, 0.0f);  // padding: massless and far away
-      float hsrc = 0.0f;
-      if (sidx >= 0) {
-        src = body[sidx];
-        src.w *= G;
-        if (NBR) hsrc = pos_h[sidx].w;
-      }
+      float4 src = nsrc;
+      const float hsrc = nh;
+      const int sidx = nidx;
+      if (base + per < count) nidx = near_source(base + per, count, nsrc, nh);
+      src.w *= G;
       S.src[w][lane] = src;
       S.sh[w][lane] = make_float2(__int_as_float(sidx), hsrc);
       __syncwarp();
