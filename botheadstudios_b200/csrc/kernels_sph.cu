@@ -607,6 +607,22 @@ int launch_from_aos(const Dev& d, cudaStream_t s) {
   return 1;
 }
 
+// Upload validation on the device (the host would walk every record): the first particle whose material is
+// outside the table or that has a non-finite field, a non-positive h or a negative mass.
+__global__ void k_validate_aos(int n, const P48* __restrict__ aos, unsigned ne, unsigned* __restrict__ first_bad) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const P48 p = aos[i];
+  const bool ok = p.mat < ne && isfinite(p.px) && isfinite(p.py) && isfinite(p.pz) && isfinite(p.vx) &&
+                  isfinite(p.vy) && isfinite(p.vz) && isfinite(p.u) && isfinite(p.mass) && p.h > 0.0f &&
+                  isfinite(p.h) && p.mass >= 0.0f;
+  if (!ok) atomicMin(first_bad, (unsigned)i);
+}
+int launch_validate_aos(const Dev& d, int n, unsigned ne, unsigned* first_bad, cudaStream_t s) {
+  k_validate_aos<<<(n + 255) / 256, 256, 0, s>>>(n, (const P48*)d.aos, ne, first_bad);
+  return 1;
+}
+
 __global__ void k_to_aos(int n, State st, const float* __restrict__ rho, P48* __restrict__ aos) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;

@@ -46,6 +46,7 @@ struct sph_ctx {
   bool rb_inflight = false;
   uint32_t rb_n = 0;
   double* d_diag = nullptr;
+  unsigned* d_flag = nullptr;  // upload validation: the first invalid particle
   DiskWork* disk = nullptr;  // disk-measurement workspace (allocated by the first measurement)
   std::string err;
   int device = 0;
@@ -281,16 +282,23 @@ sph_status upload_impl(sph_ctx* ctx, const SphParticle48* particles, const uint3
       ctx->err = "impact " + std::to_string(k) + " has a negative or non-finite softening";
       return SPH_ERR_INVALID;
     }
-  for (uint32_t i = 0; i < (on_device ? 0u : nu); ++i) {
-    const SphParticle48& p = particles[i];
-    if (p.mat >= ne || !std::isfinite(p.pos[0]) || !std::isfinite(p.pos[1]) || !std::isfinite(p.pos[2]) ||
-        !std::isfinite(p.vel[0]) || !std::isfinite(p.vel[1]) || !std::isfinite(p.vel[2]) || !std::isfinite(p.u) ||
-        !std::isfinite(p.mass) || !(p.h > 0.0f) || !std::isfinite(p.h) || p.mass < 0.0f) {
-      ctx->err = "particle " + std::to_string(i) + " has a material outside the table or a non-finite field";
+  CK(cudaStreamSynchronize(ctx->stream));
+  // the records go to the exchange buffer first and are checked there, before any state changes
+  Dev& dv = ctx->d;
+  if (nu)
+    CK(cudaMemcpyAsync(dv.aos, particles, (size_t)nu * 48,
+                       on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, ctx->stream));
+  if (nu && !on_device) {
+    unsigned bad = 0xffffffffu;
+    CK(cudaMemsetAsync(ctx->d_flag, 0xff, sizeof(unsigned), ctx->stream));
+    launch_validate_aos(dv, (int)nu, ne, ctx->d_flag, ctx->stream);
+    CK(cudaMemcpyAsync(&bad, ctx->d_flag, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (bad != 0xffffffffu) {
+      ctx->err = "particle " + std::to_string(bad) + " has a material outside the table or a non-finite field";
       return SPH_ERR_INVALID;
     }
   }
-  CK(cudaStreamSynchronize(ctx->stream));
   drop_graphs(ctx);
   Dev& d = ctx->d;
   d.n = (int)nu;
@@ -314,9 +322,6 @@ sph_status upload_impl(sph_ctx* ctx, const SphParticle48* particles, const uint3
   }
   d.L = (int)L;
   ctx->n_eos = ne;
-  if (nu)
-    CK(cudaMemcpyAsync(d.aos, particles, (size_t)nu * 48,
-                       on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, ctx->stream));
   if (!keep_eos) {
     Eos etab[kMaxMaterials];
     std::memset(etab, 0, sizeof(etab));
@@ -489,6 +494,7 @@ sph_status sph_create(const sph_config* cfg, uint32_t capacity, sph_ctx** out) {
     if (e != cudaSuccess) st = cuda_fail(ctx, e, "cudaEventCreate");
   }
   if (st == SPH_OK) st = dalloc(ctx, &ctx->d_diag, 16);
+  if (st == SPH_OK) st = dalloc(ctx, &ctx->d_flag, 1);
   if (st == SPH_OK) st = dalloc(ctx, &ctx->mlp_params, (size_t)MLP_TOTAL);
   if (st == SPH_OK) st = dalloc(ctx, &ctx->mlp_w, 1);
   if (st == SPH_OK) {

@@ -229,6 +229,8 @@ int launch_kick(const Dev& d, cudaStream_t s);
 int launch_relax(const Dev& d, cudaStream_t s);
 int launch_from_aos(const Dev& d, cudaStream_t s);
 int launch_to_aos(const Dev& d, cudaStream_t s);
+// first invalid record of the n 48-byte particles in d.aos into *first_bad (left at 0xffffffff when all pass)
+int launch_validate_aos(const Dev& d, int n, unsigned ne, unsigned* first_bad, cudaStream_t s);
 int launch_diag(const Dev& d, cudaStream_t s, double* out16);
 
 // ---- disk measurement and the Moon candidate (disk.cu) ------------------------------------------------
