@@ -12,8 +12,14 @@
 
 namespace sphb {
 
-__device__ __forceinline__ float pair_r(float4 a, float4 b) {
-  return fsqrt(dot3_exact(fsub(a.x, b.x), fsub(a.y, b.y), fsub(a.z, b.z)));
+// Pair distance in the gather kernels from one reciprocal square root (MUFU, within 2 ulp): the sums they
+// form are continuous at the support edge (W and ∇W vanish at q = 1), so a pair whose r rounds across h_ij
+// changes nothing, and the exact predicate is needed only where the neighbour set is decided (the walk).
+__device__ __forceinline__ float pair_r(float4 a, float4 b, float& rinv) {
+  const float dx = a.x - b.x, dy = a.y - b.y, dz = a.z - b.z;
+  const float dd = dx * dx + dy * dy + dz * dz;
+  rinv = rsqrtf(dd);
+  return dd > 0.0f ? dd * rinv : 0.0f;
 }
 __device__ __forceinline__ float pair_h(float hi, float hj) { return fmul(0.5f, fadd(hi, hj)); }
 
@@ -22,13 +28,14 @@ __device__ __forceinline__ float pair_h(float hi, float hj) { return fmul(0.5f, 
 // instead of one dependent chain; the next chunk's indices are requested before this chunk's records, so the
 // list stream (HBM) overlaps the record gathers (mostly L1/L2) and the arithmetic. `lst` is the particle's
 // first list slot (entries 32 apart, interleaved); slots past the count read the particle itself (harmless
-// filler, never summed).
+// filler, never summed). The lists are read once per pass and streamed past the cache (evict-first), so they
+// do not push the neighbours' records out of L2.
 constexpr int kGather = 4;
 template <int G>
 __device__ __forceinline__ void list_chunk(const unsigned* __restrict__ lst, unsigned k0, unsigned c, unsigned self,
                                            unsigned j[G]) {
 #pragma unroll
-  for (int u = 0; u < G; ++u) j[u] = k0 + u < c ? lst[(size_t)(k0 + u) * 32u] : self;
+  for (int u = 0; u < G; ++u) j[u] = k0 + u < c ? __ldcs(&lst[(size_t)(k0 + u) * 32u]) : self;
 }
 // Records of the chunk whose indices are in `jn` (k0 = its first slot); on return jn holds the next chunk's.
 __device__ __forceinline__ void gather_pos_mass(const State& st, const unsigned* __restrict__ lst, unsigned k0,
@@ -81,7 +88,8 @@ __global__ void k_density_eos(int n, State st, const unsigned* __restrict__ nbr,
 #pragma unroll
     for (int u = 0; u < kGather; ++u) {
       if (k0 + u >= c) break;
-      const float r = pair_r(pi, pj[u]);
+      float ri;
+      const float r = pair_r(pi, pj[u], ri);
       const float hij = pair_h(pi.w, pj[u].w);
       if (r < hij) {
         kern_pair<KERNEL>(r, hij, w, dwdr, dwdh);
@@ -143,7 +151,8 @@ __device__ __forceinline__ void h_sums(int t, const State& st, const unsigned* _
 #pragma unroll
     for (int u = 0; u < kGather; ++u) {
       if (k0 + u >= c) break;
-      const float r = pair_r(pi, pj[u]);
+      float ri;
+      const float r = pair_r(pi, pj[u], ri);
       const float hij = pair_h(h, pj[u].w);
       if (r < hij) {
         kern_pair<KERNEL>(r, hij, w, dwdr, dwdh);
@@ -388,8 +397,10 @@ __global__ void k_forces(int n, State st, const float4* __restrict__ fdata, cons
       for (int u = 0; u < kForceGather; ++u) {
       if (k0 + u >= c) break;
       const float4 pj = pjs[u];
-      const float dx = fsub(pi.x, pj.x), dy = fsub(pi.y, pj.y), dz = fsub(pi.z, pj.z);
-      const float r = fsqrt(dot3_exact(dx, dy, dz));
+      const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+      const float dd = dx * dx + dy * dy + dz * dz;
+      const float rinv = rsqrtf(dd);
+      const float r = dd > 0.0f ? dd * rinv : 0.0f;
       const float hij = pair_h(pi.w, pj.w);
       if (!(r < hij && r > r_min)) continue;
       const float4 vj = vjs[u];
@@ -406,7 +417,7 @@ __global__ void k_forces(int n, State st, const float4* __restrict__ fdata, cons
       const float coeff = fi.z + fj.z + pij;
       float w, dw, dwdh;
       kern_pair<KERNEL>(r, hij, w, dw, dwdh);
-      const float dwr = dw * __frcp_rn(r);  // ∇_i W = (dx/r) ∂W/∂r
+      const float dwr = dw * rinv;  // ∇_i W = (dx/r) ∂W/∂r
       const float gx = dx * dwr, gy = dy * dwr, gz = dz * dwr;
       const float s = -coeff * fj.x;
       ax += gx * s;

@@ -103,12 +103,12 @@ __device__ __forceinline__ unsigned expand_bits(unsigned v) {
 // ---- SPH kernels with support radius h: the reference's cubic spline (sph_step.wgsl:64-77) and Wendland C2 --
 // W(r, h) = σ(h) f(q) with q = r/h and σ = c/h³ (c = 8/π cubic, 21/(2π) Wendland C2), so
 // ∂W/∂r = σ f'(q)/h and ∂W/∂h = −(σ/h)(3f + q f'(q)) (the h-derivative drives the smoothing-length Newton step).
-// Evaluated from one reciprocal of h, every other term a product: the reference's per-call divisions
-// (q = r/h, σ = 8/(π h³), f'/h) give the same values to a few ulp at a quarter of the instructions, which is
-// what the gather kernels (density, smoothing-length solve, forces) spend per neighbour pair.
+// Evaluated from one approximate reciprocal of h (within 2 ulp), every other term a product: the reference's
+// per-call divisions (q = r/h, σ = 8/(π h³), f'/h) give the same values to a few ulp at a fraction of the
+// instructions, which is what the gather kernels (density, smoothing-length solve, forces) spend per pair.
 template <int KERNEL>
 __device__ __forceinline__ void kern_pair(float r, float h, float& w, float& dwdr, float& dwdh) {
-  const float ih = __frcp_rn(h);
+  const float ih = __fdividef(1.0f, h);
   const float q = r * ih;
   float f = 0.0f, fp = 0.0f;
   if (KERNEL == 1) {
