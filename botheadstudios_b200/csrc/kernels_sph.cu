@@ -409,10 +409,11 @@ __global__ void k_forces(int n, State st, const float4* __restrict__ fdata, cons
       const float vr = vx * dx + vy * dy + vz * dz;
       float pij = 0.0f;
       if (vr < 0.0f) {
-        const float mu = hij * vr / (r * r + 0.01f * hij * hij);
+        // approximate divisions (within 2 ulp): both denominators are positive and far from the limits
+        const float mu = __fdividef(hij * vr, dd + 0.01f * hij * hij);
         const float c_bar = 0.5f * (fi.w + fj.w);
         const float rho_bar = 0.5f * (fi.y + fj.y);
-        pij = (-alpha * c_bar * mu + beta * mu * mu) / rho_bar;
+        pij = __fdividef(-alpha * c_bar * mu + beta * mu * mu, rho_bar);
       }
       const float coeff = fi.z + fj.z + pij;
       float w, dw, dwdh;
