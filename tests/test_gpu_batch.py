@@ -97,6 +97,30 @@ def test_tiny_impacts_share_warps_without_mixing(over):
         assert np.array_equal(acc[a:b], ref["acc"]) and np.array_equal(rho[a:b], ref["rho"]), k
 
 
+def test_learned_batch_equals_each_impact_alone():
+    """The learned smoothing length in a batch: proposals, the residual check, the rejected particles' Newton
+    steps and the per-impact skin and residual give every impact what it gets alone, bit for bit."""
+    from botheadstudios_b200 import learned_h
+    B = ic.batch(3, 1500, 4000, seed=6)
+    params = learned_h.load()
+    with GpuSph(len(B.particles), **_cfg(B.units, h_mode=2)) as s:
+        s.mlp_set(params)
+        s.set_progress(0.5)
+        s.upload_batch(B.particles, B.offsets, B.eos, B.softening)
+        s.encode_kdk(3)
+        out = s.readback()
+        dts = s.impact_dt()
+    for k in range(B.n_impacts):
+        p = B.impact(k)
+        with GpuSph(len(p), **_cfg(B.units, h_mode=2)) as a:
+            a.mlp_set(params)
+            a.set_progress(0.5)
+            a.upload(p, B.eos, float(B.softening[k]))
+            a.encode_kdk(3)
+            _same(out[B.offsets[k]:B.offsets[k + 1]], a.readback())
+            assert dts[k] == a.diag()["dt"]
+
+
 def test_graph_replay_matches_eager():
     B = ic.batch(3, 1000, 3000, seed=4)
     res = []
