@@ -209,8 +209,14 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
             const float eQe = ex * Qex + ey * Qey + ez * Qez;
             const float rinv4 = rinv2 * rinv2;
             const float c1 = fmaf(2.5f * eQe, rinv4 * rinv, g);
-            acc.add<HILO>(c1 * dx - rinv4 * Qex, c1 * dy - rinv4 * Qey, c1 * dz - rinv4 * Qez);
-            phi -= fmaf(0.5f * eQe, rinv2, c.w) * rinv;
+            if (HILO) {
+              acc.add<HILO>(c1 * dx - rinv4 * Qex, c1 * dy - rinv4 * Qey, c1 * dz - rinv4 * Qez);
+            } else {  // two fused multiply-adds per axis straight into the sums
+              acc.x = fmaf(-rinv4, Qex, fmaf(c1, dx, acc.x));
+              acc.y = fmaf(-rinv4, Qey, fmaf(c1, dy, acc.y));
+              acc.z = fmaf(-rinv4, Qez, fmaf(c1, dz, acc.z));
+            }
+            phi = fmaf(-fmaf(0.5f * eQe, rinv2, c.w), rinv, phi);
           } else {
             acc.add<HILO>(g * dx, g * dy, g * dz);
             phi -= gm;

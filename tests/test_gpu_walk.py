@@ -82,6 +82,27 @@ def test_group_walk_gravity_bounds(K, quad):
         assert rms < bound, (theta, rms)
 
 
+@pytest.mark.parametrize("mac", [0, 1])
+def test_gravity_and_sph_bitwise_repeatable(mac):
+    """gpu_gravity.rs:655-880 asks for bitwise repeatability: the same input gives the same bits, in a fresh
+    context and on a second evaluation in the same context (no order-dependent atomics on the force path)."""
+    bodies, pos, mass = cloud(3000, 11)
+    n = len(bodies)
+    p = particles_from_arrays(bodies[:, :3], np.full(n, 2.0e5, np.float32), np.zeros((n, 3), np.float32),
+                              np.full(n, 1.0e5, np.float32), bodies[:, 3], np.zeros(n, np.uint32))
+    runs = []
+    for _ in range(2):
+        with GpuSph(n, G=G, theta=0.6, leaf_size=16 if mac == 0 else 1, multipole=1 if mac == 0 else 0, mac=mac,
+                    max_neighbours=256) as s:
+            s.upload(p, M.eos_table(), softening=5.0e3)
+            for _ in range(2):
+                s.eval_forces()
+                runs.append([s.inspect(q).copy() for q in ("ACC_GRAV", "RHO", "ACC_SPH")])
+    for r in runs[1:]:
+        for a, b in zip(runs[0], r):
+            assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+
+
 def test_point_set_gravity_api_matches_direct():
     """sph_gravity (GravityField::accelerations): tree and direct modes against the f64 direct sum."""
     _, pos, mass = cloud(3000, 11)
