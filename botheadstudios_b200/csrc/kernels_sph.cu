@@ -18,7 +18,7 @@ namespace sphb {
 __device__ __forceinline__ float pair_r(float4 a, float4 b, float& rinv) {
   const float dx = a.x - b.x, dy = a.y - b.y, dz = a.z - b.z;
   const float dd = dx * dx + dy * dy + dz * dz;
-  rinv = rsqrtf(dd);
+  rinv = rsqrt_ftz(dd);
   return dd > 0.0f ? dd * rinv : 0.0f;
 }
 __device__ __forceinline__ float pair_h(float hi, float hj) { return fmul(0.5f, fadd(hi, hj)); }
@@ -399,7 +399,7 @@ __global__ void k_forces(int n, State st, const float4* __restrict__ fdata, cons
       const float4 pj = pjs[u];
       const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
       const float dd = dx * dx + dy * dy + dz * dz;
-      const float rinv = rsqrtf(dd);
+      const float rinv = rsqrt_ftz(dd);
       const float r = dd > 0.0f ? dd * rinv : 0.0f;
       const float hij = pair_h(pi.w, pj.w);
       if (!(r < hij && r > r_min)) continue;
@@ -410,10 +410,10 @@ __global__ void k_forces(int n, State st, const float4* __restrict__ fdata, cons
       float pij = 0.0f;
       if (vr < 0.0f) {
         // approximate divisions (within 2 ulp): both denominators are positive and far from the limits
-        const float mu = __fdividef(hij * vr, dd + 0.01f * hij * hij);
+        const float mu = div_ftz(hij * vr, dd + 0.01f * hij * hij);
         const float c_bar = 0.5f * (fi.w + fj.w);
         const float rho_bar = 0.5f * (fi.y + fj.y);
-        pij = __fdividef(-alpha * c_bar * mu + beta * mu * mu, rho_bar);
+        pij = div_ftz(-alpha * c_bar * mu + beta * mu * mu, rho_bar);
       }
       const float coeff = fi.z + fj.z + pij;
       float w, dw, dwdh;

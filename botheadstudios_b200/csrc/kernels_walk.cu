@@ -158,7 +158,7 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
           float dx = bj.x - pi.x, dy = bj.y - pi.y, dz = bj.z - pi.z;
           if (HILO) { dx -= xlo; dy -= ylo; dz -= zlo; }
           const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, soft2)));
-          const float rinv = rsqrtf(r2);
+          const float rinv = rsqrt_ftz(r2);
           const float gm = bj.w * rinv;
           const float g = gm * rinv * rinv;
           acc.add<HILO>(g * dx, g * dy, g * dz);
@@ -193,7 +193,7 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
           float dx = c.x - pi.x, dy = c.y - pi.y, dz = c.z - pi.z;
           if (HILO) { dx -= xlo; dy -= ylo; dz -= zlo; }
           const float r2 = dx * dx + dy * dy + dz * dz + soft2;
-          const float rinv = rsqrtf(r2);
+          const float rinv = rsqrt_ftz(r2);
           const float rinv2 = rinv * rinv;
           const float gm = c.w * rinv;           // G M / R
           const float g = gm * rinv2;            // G M / R³
@@ -289,7 +289,7 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
               d2 = ex * ex + ey * ey + ez * ez;
             }
             const float r2 = other ? d2 + soft2 : 1.0f;
-            const float rinv = rsqrtf(r2);
+            const float rinv = rsqrt_ftz(r2);
             const float gm = other ? bj.w * rinv : 0.0f;
             const float g = gm * rinv * rinv;
             acc.add<HILO>(g * ex, g * ey, g * ez);

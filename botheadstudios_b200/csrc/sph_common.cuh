@@ -50,6 +50,26 @@ struct DevParams {
   unsigned long long stat_visits, stat_pops, stat_m2p, stat_p2p;
 };
 
+// ---- approximate reciprocal square root, reciprocal and division on the special-function unit alone ------
+// The .ftz forms flush subnormal operands and results to zero, so they compile to the bare unit operation; the
+// operands they get here are never subnormal (softened squared distances, squared pair distances of distinct
+// particles, smoothing lengths, densities). Each result is within 2 ulp of the exact one.
+__device__ __forceinline__ float rsqrt_ftz(float x) {
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float rcp_ftz(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float div_ftz(float a, float b) {
+  float y;
+  asm("div.approx.ftz.f32 %0, %1, %2;" : "=f"(y) : "f"(a), "f"(b));
+  return y;
+}
+
 // ---- exact single-rounding arithmetic (no FMA contraction) -----------------------------------------
 __device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b); }
 __device__ __forceinline__ float fsub(float a, float b) { return __fsub_rn(a, b); }
@@ -108,7 +128,7 @@ __device__ __forceinline__ unsigned expand_bits(unsigned v) {
 // instructions, which is what the gather kernels (density, smoothing-length solve, forces) spend per pair.
 template <int KERNEL>
 __device__ __forceinline__ void kern_pair(float r, float h, float& w, float& dwdr, float& dwdh) {
-  const float ih = __fdividef(1.0f, h);
+  const float ih = rcp_ftz(h);
   const float q = r * ih;
   float f = 0.0f, fp = 0.0f;
   if (KERNEL == 1) {
