@@ -313,8 +313,11 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
     __syncwarp();
     bool acc_node = false, leaf = false, open = false, near_leaf = false;
     unsigned ls0 = 0u, ls1 = 1u;  // a leaf's source range, loaded alongside its box
+    float4 lbl = make_float4(0.f, 0.f, 0.f, 0.f), lbh = lbl;  // the node's box (and max h), for the lane test
     if (have) {
       const float4 bl = nbmin[node], bh = nbmax[node];
+      lbl = bl;
+      lbh = bh;
       const bool is_leaf = node >= leaf0;
       if (is_leaf) {
         ls0 = leaf_start[node - leaf0];
@@ -344,6 +347,25 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
       else open = GRAV || (NBR && near);
       if (is_leaf && ls1 <= ls0) acc_node = leaf = false;  // an empty leaf (none are built) adds nothing
       near_leaf = leaf && near;
+    }
+    if (NBR && GRAV) {
+      // A leaf near the group box may still be out of every particle's own reach: then it can hold no
+      // neighbour and takes the cheaper far path. The test is conservative (reach with the list's skin and a
+      // margin), and a leaf holding a particle of the part is at distance 0, so self-pairs stay on the near path.
+      const unsigned cand = __ballot_sync(SPH_FULL_MASK, near_leaf);
+      unsigned keep = 0;
+      for (unsigned b = cand; b; b &= b - 1) {
+        const int k = __ffs(b) - 1;
+        const float x0 = __shfl_sync(SPH_FULL_MASK, lbl.x, k), y0 = __shfl_sync(SPH_FULL_MASK, lbl.y, k),
+                    z0 = __shfl_sync(SPH_FULL_MASK, lbl.z, k), hm = __shfl_sync(SPH_FULL_MASK, lbl.w, k);
+        const float x1 = __shfl_sync(SPH_FULL_MASK, lbh.x, k), y1 = __shfl_sync(SPH_FULL_MASK, lbh.y, k),
+                    z1 = __shfl_sync(SPH_FULL_MASK, lbh.z, k);
+        const float ex = fmaxf(fmaxf(x0 - pi.x, pi.x - x1), 0.0f), ey = fmaxf(fmaxf(y0 - pi.y, pi.y - y1), 0.0f),
+                    ez = fmaxf(fmaxf(z0 - pi.z, pi.z - z1), 0.0f);
+        const float r = 0.5f * (pi.w + hm) * grow * 1.0001f;
+        if (__any_sync(SPH_FULL_MASK, valid && ex * ex + ey * ey + ez * ez <= r * r)) keep |= 1u << k;
+      }
+      if (near_leaf && !((keep >> lane) & 1u)) near_leaf = false;
     }
     const unsigned bm = __ballot_sync(SPH_FULL_MASK, acc_node);
     const unsigned bf = __ballot_sync(SPH_FULL_MASK, leaf);
