@@ -7,13 +7,16 @@
 //   * accepted  — the reference MAC (sqrt(d²+ε²) >= diag/θ + |centre−COM|, bh_gravity.wgsl:382) holds for
 //                 the nearest point of the group's bounding box, hence for every particle of the group, and
 //                 the node's box is outside the SPH reach: appended to the multipole list;
-//   * leaf      — appended to the direct list (pairwise gravity + the exact neighbour predicate);
+//   * leaf      — appended to the near list (pairwise gravity + the exact neighbour predicate) when some
+//                 particle of the group can reach it with its own smoothing length (a per-lane test after
+//                 the group test), otherwise to the far list (pairwise gravity only);
 //   * opened    — children pushed (ballot + popc compaction).
 // Nodes whose box lies within ½(h_group,max + h_node,max) of the group are always opened, so every leaf
 // that can hold an SPH neighbour reaches the direct list: the neighbour set {j != i : r_ij < h_ij} is
 // complete and, with single-rounded arithmetic, identical to the reference predicate (sph_step.wgsl:141-143).
-// Lists are flushed through shared memory in chunks of 32 sources; every lane then runs the chunk against
-// its own particle with no dependent loads (the interaction loop is pure FP32 work).
+// Lists are flushed through shared memory in chunks of 32 sources (the next chunk's loads issued before the
+// current chunk is evaluated); every lane then runs the chunk against its own particle with no dependent loads
+// (the interaction loop is pure FP32 work, its reciprocal square root the bare special-function operation).
 #include "sph_kernels.cuh"
 
 namespace sphb {
