@@ -95,9 +95,10 @@ typedef struct sph_config {
 /* Barnes-Hut acceptance. PARTICLE: each particle walks with the GPU reference's MAC
  * sqrt(d²+ε²) >= diag/θ + δ (bh_gravity.wgsl:382; diag = AABB diagonal, δ = |centre − COM|), reproducing
  * cs_gravity_bh bit for bit, and uses the reference's split for runs of equal Morton codes.
- * GROUP: a warp takes a group of <= 32 particles (a subtree of the LBVH) and accepts a node only when
- * sqrt(d_box²+ε²) >= side/θ + δ holds for the nearest point of the group's bounding box, so it holds for
- * every particle of the group. θ here measures the node's largest side, as in the reference's CPU octree
+ * GROUP: a warp takes a group of <= 32 Morton-consecutive particles of one impact (whole leaves; split into
+ * parts where consecutive particles are more than 6 h apart) and accepts a node only when
+ * sqrt(d_box²+ε²) >= side/θ + δ holds for the nearest point of the part's bounding box, so it holds for
+ * every particle of the part. θ here measures the node's largest side, as in the reference's CPU octree
  * (bhtree.rs:181, (2·half)/dist < θ), with Barnes' δ term added; at equal θ this is looser than the diagonal
  * form. Leaves may be accepted as multipoles. The same walk gathers the SPH neighbour candidates, and runs
  * of equal Morton codes are split on the index-extended key (always a valid tree). leaf_size must be a power
@@ -314,8 +315,9 @@ sph_status sph_gravity_direct64(sph_ctx* ctx, const double* pos3, const double* 
 
 /* ---- Granular (DEM) contact: GpuParticles (crates/engine/src/gpu_particles.rs:46-325) over the grain
  * pipeline of shaders/particle_step.wgsl (contact_accel :167-211, cs_forces :273-336, the implicit velocity
- * solve of cs_integrate :477-530). Terrain contact, air drag, cooling and render expansion (the ground
- * scene) are not part of this path. */
+ * solve of cs_integrate :477-530), plus the ground scene of cs_integrate :338-576 (terrain contact, air drag,
+ * cooling: sph_dem_set_ground, sph_dem_set_terrain). The draw-only sub-cube expansion (cs_expand) is
+ * rendering and is not part of this path. */
 /* particle_step.wgsl:127-137 `Particle` (80 bytes). */
 typedef struct SphGrain80 {
   float offset[3];
