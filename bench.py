@@ -167,6 +167,33 @@ def replica_value(pg, units_local: float, ms_local: float, local: int) -> float:
     return sum_over_ranks(pg, units_local, local) / (max_over_ranks(pg, ms_local, local) / 1000.0)
 
 
+def conservation_drifts(start: list, end: list) -> dict:
+    """Drifts over a run from the FP64 device sums of each context (`GpuSph.diag` at its start and end):
+    total energy change ÷ |potential| at the start; |ΔP| ÷ sqrt(2·M·KE) at the start (momentum against the
+    system's kinetic momentum scale); |ΔL| ÷ |L| at the start (L about the origin). Each context's impacts are
+    isolated systems, so the sums over contexts are conserved too; None where the scale is zero."""
+    def tot(ds, k):
+        return sum(d[k] for d in ds)
+
+    def vec(ds, k):
+        return [sum(d[k][i] for d in ds) for i in range(3)]
+
+    def norm(v):
+        return math.sqrt(sum(x * x for x in v))
+
+    e0 = tot(start, "kinetic") + tot(start, "internal") + tot(start, "potential")
+    e1 = tot(end, "kinetic") + tot(end, "internal") + tot(end, "potential")
+    pot0 = abs(tot(start, "potential"))
+    p0, p1 = vec(start, "momentum"), vec(end, "momentum")
+    l0, l1 = vec(start, "angular_momentum"), vec(end, "angular_momentum")
+    pscale = math.sqrt(2.0 * tot(start, "mass") * tot(start, "kinetic"))
+    dp = norm([b - a for a, b in zip(p0, p1)])
+    dl = norm([b - a for a, b in zip(l0, l1)])
+    return dict(energy_drift=(e1 - e0) / pot0 if pot0 else None,
+                momentum_drift=dp / pscale if pscale else None,
+                angular_momentum_drift=dl / norm(l0) if norm(l0) else None)
+
+
 def build_workload(wl: dict, seed: int):
     from botheadstudios_b200 import workloads
     return workloads.build(wl, seed)
@@ -453,9 +480,6 @@ def run_ours(args, wl, world, rank, local, pg):
                    sample=f"HydroBody::step restated in C++ (f64, octree θ=0.5), 65,536-particle impact of the same "
                           f"generator, {r['steps_run']} steps in {r['seconds']:.1f} s")
     dd = d1[0]
-    energy0 = dsum(dstart, "kinetic") + dsum(dstart, "internal") + dsum(dstart, "potential")
-    energy1 = dsum(d1, "kinetic") + dsum(d1, "internal") + dsum(d1, "potential")
-    pot0 = dsum(dstart, "potential")
     line = dict(metric=METRIC, value=value, unit=UNIT, n_gpus=world, steps=args.steps, warmup=args.warmup,
                 ms_per_step=ms_max / args.steps, higher_is_better=True, scaling="weak", vs_baseline=None,
                 dtype="f32", data="synthetic (seeded lattice impact)",
@@ -472,7 +496,7 @@ def run_ours(args, wl, world, rank, local, pg):
                 clocks=clk.summary(),
                 autotune=tuned, **({"plain_sequential": plain} if wl.get("kind") == "batch" else
                                    {"plain_form": plain} if plain else {}),
-                physics=dict(energy_drift=(energy1 - energy0) / abs(pot0) if pot0 else None,
+                physics=dict(**conservation_drifts(dstart, d1),
                              sim_time=dd["time"], dt=dd["dt"],
                              max_neighbours=max(d["max_neighbours_seen"] for d in d1),
                              overflow_flags=max(d["overflow_flags"] for d in d1),

@@ -2,6 +2,7 @@
 and the job's throughput is the units all ranks processed over the slowest rank's device time. The host logic of
 that (bench.py's reductions over ranks, the per-rank seeds) runs here as two gloo ranks on the CPU."""
 import json
+import math
 import os
 import socket
 import sys
@@ -56,3 +57,27 @@ def test_replica_reductions_over_two_gloo_ranks(tmp_path):
         assert r["value"] == pytest.approx(300.0 / 0.020)  # all units ÷ the slowest time (20 ms)
         assert r["n_total"] == res[0]["n_local"] + res[1]["n_local"]
     assert res[0]["n_local"] != res[1]["n_local"]  # the replicas are different draws
+
+
+def _diag(ke, ie, pe, p, L, m=2.0):
+    return dict(kinetic=ke, internal=ie, potential=pe, momentum=list(p), angular_momentum=list(L), mass=m)
+
+
+def test_conservation_drifts_over_contexts():
+    """The drifts bench.py reports: energy change over |PE|, |ΔP| over sqrt(2 M KE), |ΔL| over |L|, each summed
+    over the contexts (isolated impacts) before the ratio."""
+    sys.path.insert(0, ROOT)
+    import bench
+    start = [_diag(1.0, 2.0, -4.0, (1.0, 0.0, 0.0), (0.0, 0.0, 3.0)),
+             _diag(1.0, 1.0, -4.0, (-1.0, 0.0, 0.0), (0.0, 0.0, 1.0))]
+    end = [_diag(1.5, 2.0, -4.0, (1.0, 0.3, 0.0), (0.0, 0.0, 3.0)),
+           _diag(1.0, 0.9, -4.0, (-1.0, 0.1, 0.0), (0.0, 0.04, 1.0))]
+    d = bench.conservation_drifts(start, end)
+    assert d["energy_drift"] == pytest.approx(0.4 / 8.0)
+    assert d["momentum_drift"] == pytest.approx(0.4 / math.sqrt(2.0 * 4.0 * 2.0))
+    assert d["angular_momentum_drift"] == pytest.approx(0.04 / 4.0)
+    still = bench.conservation_drifts(start, start)
+    assert still == dict(energy_drift=0.0, momentum_drift=0.0, angular_momentum_drift=0.0)
+    zero = [_diag(0.0, 0.0, 0.0, (0.0, 0.0, 0.0), (0.0, 0.0, 0.0))]
+    assert bench.conservation_drifts(zero, zero) == dict(energy_drift=None, momentum_drift=None,
+                                                         angular_momentum_drift=None)
