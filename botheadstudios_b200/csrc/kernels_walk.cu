@@ -444,12 +444,8 @@ static void walk(const Dev& d, const Cfg& c, cudaStream_t s) {
   const int warps = d.L;  // upper bound on the number of groups
   const int blocks = (warps + W - 1) / W;
   const size_t smem = sizeof(WalkSmem<W>);
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_tree_walk<W, GRAV, QUAD, NBR, HILO>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)smem);
-    attr = true;
-  }
+  static std::atomic<unsigned long long> attr{0};
+  smem_limit_per_device(k_tree_walk<W, GRAV, QUAD, NBR, HILO>, (int)smem, attr);
   const State& st = d.s();
   k_tree_walk<W, GRAV, QUAD, NBR, HILO><<<blocks, W * 32, smem, s>>>(
       d.body, st.pos_h, st.x, st.y, st.z, d.K, d.L, d.leaf_start, d.leaf_codes, d.segs, d.left, d.right, d.ncom,

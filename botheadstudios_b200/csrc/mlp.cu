@@ -605,15 +605,11 @@ __global__ void k_mlp_adam(float* __restrict__ p, const float* __restrict__ g, f
   p[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
 }
 
-int propose_grid() {
-  static int grid = 0;
-  if (!grid) {
-    int dev = 0, sms = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    grid = sms * 4;
-  }
-  return grid;
+int propose_grid() {  // 4 blocks per SM of the current device
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  return sms * 4;
 }
 
 }  // namespace
@@ -625,37 +621,30 @@ int launch_mlp_pack(const float* params, MlpPacked* out, cudaStream_t s) {
 
 int launch_mlp_propose(const Dev& d, const MlpPacked* w, const MlpFeatureArgs& fa, const float* divv, float* rec,
                        float* dh, bool apply, cudaStream_t s) {
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_mlp_propose, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM);
-    attr = true;
-  }
+  static std::atomic<unsigned long long> attr{0};
+  smem_limit_per_device(k_mlp_propose, TC_SMEM, attr);
   const int tiles = (d.n + ROWS - 1) / ROWS;
-  const int grid = tiles < propose_grid() ? tiles : propose_grid();
+  const int cap = propose_grid();
+  const int grid = tiles < cap ? tiles : cap;
   k_mlp_propose<<<grid, ROWS, TC_SMEM, s>>>(d.n, d.s(), d.rho, d.nbr_cnt, d.acc, d.fdata, divv, d.eos, d.segs, d.P, fa,
                                       w, rec, dh, apply ? 1 : 0);
   return 1;
 }
 
 int launch_mlp_forward(const MlpPacked* w, const float* x, int n, float* out, unsigned* err, cudaStream_t s) {
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM);
-    attr = true;
-  }
+  static std::atomic<unsigned long long> attr{0};
+  smem_limit_per_device(k_mlp_forward, TC_SMEM, attr);
   const int tiles = (n + ROWS - 1) / ROWS;
-  const int grid = tiles < propose_grid() ? tiles : propose_grid();
+  const int cap = propose_grid();
+  const int grid = tiles < cap ? tiles : cap;
   k_mlp_forward<<<grid, ROWS, TC_SMEM, s>>>(w, x, n, out, err);
   return 1;
 }
 
 int launch_mlp_train_batch(const MlpPacked* w, const float* x, const float* t, const unsigned* idx, int m,
                            float denom, float* grad, float* loss, cudaStream_t s) {
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_mlp_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TrainSmem));
-    attr = true;
-  }
+  static std::atomic<unsigned long long> attr{0};
+  smem_limit_per_device(k_mlp_train, (int)sizeof(TrainSmem), attr);
   k_mlp_train<<<(m + ROWS - 1) / ROWS, ROWS, sizeof(TrainSmem), s>>>(w, x, t, idx, m, denom, grad, loss);
   return 1;
 }

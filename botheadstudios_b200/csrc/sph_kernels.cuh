@@ -1,11 +1,25 @@
 // Internal device layout and host-side launchers of the SPH step kernels (not part of the C ABI).
 #pragma once
 #include <cuda_runtime.h>
+#include <atomic>
 #include <cstdint>
 
 #include "sph_common.cuh"
 
 namespace sphb {
+
+// Raises a kernel's dynamic shared-memory limit on the calling thread's current device, once per device: the
+// attribute belongs to the device, so contexts on several GPUs in one process each need it. `done` holds one
+// bit per device ordinal (below 64); two threads racing here both set the same value, which is harmless.
+template <typename Kernel>
+inline void smem_limit_per_device(Kernel kernel, int bytes, std::atomic<unsigned long long>& done) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return;
+  const unsigned long long bit = 1ull << (dev & 63);
+  if (done.load(std::memory_order_acquire) & bit) return;
+  if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) == cudaSuccess)
+    done.fetch_or(bit, std::memory_order_release);
+}
 
 // Particle state, structure-of-arrays, kept in Morton (LBVH leaf) order between force evaluations.
 // `id` is the particle's original index (its slot in the 48-byte exchange array).
