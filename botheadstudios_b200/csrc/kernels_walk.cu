@@ -17,6 +17,8 @@
 // Lists are flushed through shared memory in chunks of 32 sources (the next chunk's loads issued before the
 // current chunk is evaluated); every lane then runs the chunk against its own particle with no dependent loads
 // (the interaction loop is pure FP32 work, its reciprocal square root the bare special-function operation).
+#include <type_traits>
+
 #include "sph_kernels.cuh"
 
 namespace sphb {
@@ -111,6 +113,9 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
   // a negative skin: the impact's current smoothing-length skin (device-maintained)
   if (NBR && skin < 0.0f) skin = sgr.skin;
   const float grow = (1.0f + skin) * (1.0f + 1.0e-5f);
+  // the conservative neighbour test of a list with a skin: lim = ½(h_i + h_j)(1 + skin)(1 + 2^-19)
+  const float lim_j = 0.5f * (1.0f + skin) * (1.0f + 1.9073486e-6f);
+  const float lim_i = pi.w * lim_j;
   const float G = P->G, soft2 = sgr.soft2;
   const unsigned leaf0 = (unsigned)(L - 1);
   const unsigned lt = (1u << lane) - 1u;
@@ -249,6 +254,50 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
     }
     return sidx;
   };
+  auto near_sources = [&](auto loose) {
+#pragma unroll 4
+    for (int k = 0; k < 32; ++k) {
+      const float2 shk = S.sh[w][k];
+      const int s = __float_as_int(shk.x);
+      const bool other = s >= 0 && s != t;
+      const float4 bj = S.src[w][k];
+      const float dx = fsub(bj.x, pi.x), dy = fsub(bj.y, pi.y), dz = fsub(bj.z, pi.z);
+      const float dd = dot3_exact(dx, dy, dz);
+      if (NBR && other) {
+        bool inside;
+        if constexpr (decltype(loose)::value) {
+          const float lim = fmaf(shk.y, lim_j, lim_i);
+          inside = dd < lim * lim;
+        } else {
+          const float lim = fmul(0.5f, fadd(pi.w, shk.y));
+          // sqrt_rn(dd) < lim, decided without the square root outside a 2^-19 band around lim²:
+          // dd < lim²(1-2^-19) ⇒ √dd < lim − 2 ulp(lim); dd > lim²(1+2^-19) ⇒ √dd > lim + 2 ulp(lim)
+          const float q = fmul(lim, lim);
+          inside = dd < fmul(q, 1.0f - 1.9073486e-6f);
+          if (!inside && !(dd > fmul(q, 1.0f + 1.9073486e-6f))) inside = fsqrt(dd) < lim;
+        }
+        if (inside) {
+          if (cnt < cap) nbr[nbr_slot((unsigned)t, cnt, cap)] = (unsigned)s;
+          ++cnt;
+        }
+      }
+      if (GRAV) {
+        float ex = dx, ey = dy, ez = dz, d2 = dd;
+        if (HILO) {
+          ex -= xlo;
+          ey -= ylo;
+          ez -= zlo;
+          d2 = ex * ex + ey * ey + ez * ez;
+        }
+        const float r2 = other ? d2 + soft2 : 1.0f;
+        const float rinv = rsqrt_ftz(r2);
+        const float gm = other ? bj.w * rinv : 0.0f;
+        const float g = gm * rinv * rinv;
+        acc.add<HILO>(g * ex, g * ey, g * ez);
+        phi -= gm;
+      }
+    }
+  };
   auto flush_p2p = [&](int count) {
     const int per = 32 / K;  // leaves per chunk
     float4 nsrc;
@@ -264,43 +313,13 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
       S.sh[w][lane] = make_float2(__int_as_float(sidx), hsrc);
       __syncwarp();
       if (valid) {
-#pragma unroll 4
-        for (int k = 0; k < 32; ++k) {
-          const float2 shk = S.sh[w][k];
-          const int s = __float_as_int(shk.x);
-          const bool other = s >= 0 && s != t;
-          const float4 bj = S.src[w][k];
-          const float dx = fsub(bj.x, pi.x), dy = fsub(bj.y, pi.y), dz = fsub(bj.z, pi.z);
-          const float dd = dot3_exact(dx, dy, dz);
-          if (NBR && other) {
-            float lim = fmul(0.5f, fadd(pi.w, shk.y));
-            if (skin > 0.0f) lim = lim * (1.0f + skin);
-            // sqrt_rn(dd) < lim, decided without the square root outside a 2^-19 band around lim²:
-            // dd < lim²(1-2^-19) ⇒ √dd < lim − 2 ulp(lim); dd > lim²(1+2^-19) ⇒ √dd > lim + 2 ulp(lim)
-            const float q = fmul(lim, lim);
-            bool inside = dd < fmul(q, 1.0f - 1.9073486e-6f);
-            if (!inside && !(dd > fmul(q, 1.0f + 1.9073486e-6f))) inside = fsqrt(dd) < lim;
-            if (inside) {
-              if (cnt < cap) nbr[nbr_slot((unsigned)t, cnt, cap)] = (unsigned)s;
-              ++cnt;
-            }
-          }
-          if (GRAV) {
-            float ex = dx, ey = dy, ez = dz, d2 = dd;
-            if (HILO) {
-              ex -= xlo;
-              ey -= ylo;
-              ez -= zlo;
-              d2 = ex * ex + ey * ey + ez * ez;
-            }
-            const float r2 = other ? d2 + soft2 : 1.0f;
-            const float rinv = rsqrt_ftz(r2);
-            const float gm = other ? bj.w * rinv : 0.0f;
-            const float g = gm * rinv * rinv;
-            acc.add<HILO>(g * ex, g * ey, g * ez);
-            phi -= gm;
-          }
-        }
+        // A list built with a skin is a candidate set: the gather kernels keep r < h_ij at the current h,
+        // and the smoothing-length solve holds h below h0·(1 + skin)·0.999, so every superset of the exact
+        // predicate gives the same sums in the same order. With a skin the test is therefore a conservative
+        // one (lim padded by 2^-19, more than the rounding of either form); without one (fixed h) it is the
+        // reference's exact predicate.
+        if (NBR && skin > 0.0f) near_sources(std::true_type{});
+        else near_sources(std::false_type{});
       }
       __syncwarp();
     }
