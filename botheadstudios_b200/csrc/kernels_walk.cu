@@ -65,7 +65,12 @@ struct Acc3 {
   }
 };
 
-template <int W, bool GRAV, bool QUAD, bool NBR, bool HILO>
+// What a gravity walk writes: the acceleration alone (a step's walk: the KDK integrator needs no potential),
+// the acceleration and the potential φ, or φ alone (into .w of the gravity record, for the energy diagnostic
+// of a state whose step walk left it out).
+enum { kWalkAcc = 0, kWalkAccPhi = 1, kWalkPhi = 2 };
+
+template <int W, bool GRAV, bool QUAD, bool NBR, bool HILO, int OUT>
 __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
     const float4* __restrict__ body, const float4* __restrict__ pos_h, const double* __restrict__ x64,
     const double* __restrict__ y64, const double* __restrict__ z64, int K, int L,
@@ -172,7 +177,7 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
           const float gm = bj.w * rinv;
           const float g = gm * rinv * rinv;
           acc.add<HILO>(g * dx, g * dy, g * dz);
-          phi -= gm;
+          if (OUT != kWalkAcc) phi -= gm;
         }
       }
       __syncwarp();
@@ -226,10 +231,10 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
               acc.y = fmaf(-rinv4, Qey, fmaf(c1, dy, acc.y));
               acc.z = fmaf(-rinv4, Qez, fmaf(c1, dz, acc.z));
             }
-            phi = fmaf(-fmaf(0.5f * eQe, rinv2, c.w), rinv, phi);
+            if (OUT != kWalkAcc) phi = fmaf(-fmaf(0.5f * eQe, rinv2, c.w), rinv, phi);
           } else {
             acc.add<HILO>(g * dx, g * dy, g * dz);
-            phi -= gm;
+            if (OUT != kWalkAcc) phi -= gm;
           }
         }
       }
@@ -294,7 +299,7 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
         const float gm = other ? bj.w * rinv : 0.0f;
         const float g = gm * rinv * rinv;
         acc.add<HILO>(g * ex, g * ey, g * ez);
-        phi -= gm;
+        if (OUT != kWalkAcc) phi -= gm;
       }
     }
   };
@@ -440,7 +445,10 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
   st_p2p += part_p2p * (unsigned long long)K * nvalid;     // leaf sources × particles (upper bound)
   }  // parts
 
-  if (in_group && GRAV) gout[t] = make_float4(acc.x, acc.y, acc.z, phi);
+  if (in_group && GRAV) {
+    if (OUT == kWalkPhi) reinterpret_cast<float*>(gout)[4 * (size_t)t + 3] = phi;
+    else gout[t] = make_float4(acc.x, acc.y, acc.z, OUT == kWalkAccPhi ? phi : 0.0f);
+  }
   if (NBR) {
     if (in_group) nbr_cnt[t] = cnt;
     const unsigned wmax = warp_max(in_group ? cnt : 0u);
@@ -450,7 +458,7 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
     }
   }
   if (overflow && lane == 0) atomicOr(&P->flags, kFlagStackOverflow);
-  if (lane == 0) {
+  if (lane == 0 && OUT != kWalkPhi) {  // a diagnostic's potential walk is not a step's walk
     atomicAdd(&P->stat_visits, st_visits);
     atomicAdd(&P->stat_pops, st_pops);
     atomicAdd(&P->stat_m2p, st_m2p);
@@ -458,50 +466,69 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
   }
 }
 
-template <int W, bool GRAV, bool QUAD, bool NBR, bool HILO>
+template <int W, bool GRAV, bool QUAD, bool NBR, bool HILO, int OUT>
 static void walk(const Dev& d, const Cfg& c, cudaStream_t s) {
   const int warps = d.L;  // upper bound on the number of groups
   const int blocks = (warps + W - 1) / W;
   const size_t smem = sizeof(WalkSmem<W>);
   static std::atomic<unsigned long long> attr{0};
-  smem_limit_per_device(k_tree_walk<W, GRAV, QUAD, NBR, HILO>, (int)smem, attr);
+  smem_limit_per_device(k_tree_walk<W, GRAV, QUAD, NBR, HILO, OUT>, (int)smem, attr);
   const State& st = d.s();
-  k_tree_walk<W, GRAV, QUAD, NBR, HILO><<<blocks, W * 32, smem, s>>>(
+  k_tree_walk<W, GRAV, QUAD, NBR, HILO, OUT><<<blocks, W * 32, smem, s>>>(
       d.body, st.pos_h, st.x, st.y, st.z, d.K, d.L, d.leaf_start, d.leaf_codes, d.segs, d.left, d.right, d.ncom,
       d.nbmin, d.nbmax, d.nq0, d.nq1, d.P, d.grav, d.nbr, d.nbr_cnt, d.nbr_cap, c.h_solve ? -1.0f : c.nbr_skin,
       d.h0, d.groups, d.ngroups);
 }
 
 // Gravity (group MAC) fused with the neighbour lists; the traversal tile (warps per block) is a tuning choice.
-template <bool QUAD>
+template <bool QUAD, int OUT>
 static void walk_fused(const Dev& d, const Cfg& c, cudaStream_t s) {
   if (c.hilo) {
-    walk<4, true, QUAD, true, true>(d, c, s);
+    walk<4, true, QUAD, true, true, OUT>(d, c, s);
     return;
   }
   switch (c.walk_warps) {
-    case 4: walk<4, true, QUAD, true, false>(d, c, s); break;
-    case 8: walk<8, true, QUAD, true, false>(d, c, s); break;
-    default: walk<2, true, QUAD, true, false>(d, c, s); break;
+    case 4: walk<4, true, QUAD, true, false, OUT>(d, c, s); break;
+    case 8: walk<8, true, QUAD, true, false, OUT>(d, c, s); break;
+    default: walk<2, true, QUAD, true, false, OUT>(d, c, s); break;
   }
 }
 
-int launch_walk(const Dev& d, const Cfg& c, cudaStream_t s) {
-  if (c.quad) walk_fused<true>(d, c, s);
-  else walk_fused<false>(d, c, s);
+int launch_walk(const Dev& d, const Cfg& c, bool potential, cudaStream_t s) {
+  if (potential) {
+    if (c.quad) walk_fused<true, kWalkAccPhi>(d, c, s);
+    else walk_fused<false, kWalkAccPhi>(d, c, s);
+  } else {
+    if (c.quad) walk_fused<true, kWalkAcc>(d, c, s);
+    else walk_fused<false, kWalkAcc>(d, c, s);
+  }
+  return 1;
+}
+
+// The potential alone, into .w of the gravity record, on the tree of the last evaluation (the energy
+// diagnostic after steps whose walks left it out). The group MAC and quadrupoles of the step's walk; without
+// the neighbour lists a node is near only when it overlaps the part's box.
+int launch_potential(const Dev& d, const Cfg& c, cudaStream_t s) {
+  if (c.hilo) {
+    if (c.quad) walk<4, true, true, false, true, kWalkPhi>(d, c, s);
+    else walk<4, true, false, false, true, kWalkPhi>(d, c, s);
+  } else {
+    if (c.quad) walk<4, true, true, false, false, kWalkPhi>(d, c, s);
+    else walk<4, true, false, false, false, kWalkPhi>(d, c, s);
+  }
   return 1;
 }
 
 // Gravity only (group MAC), for point sets without SPH.
 int launch_gravity_group(const Dev& d, const Cfg& c, cudaStream_t s) {
-  if (c.quad) walk<4, true, true, false, false>(d, c, s);
-  else walk<4, true, false, false, false>(d, c, s);
+  if (c.quad) walk<4, true, true, false, false, kWalkAccPhi>(d, c, s);
+  else walk<4, true, false, false, false, kWalkAccPhi>(d, c, s);
   return 1;
 }
 
 // Neighbour lists only (when gravity is not the tree).
 int launch_neighbours(const Dev& d, const Cfg& c, cudaStream_t s) {
-  walk<4, false, false, true, false>(d, c, s);
+  walk<4, false, false, true, false, kWalkAcc>(d, c, s);
   return 1;
 }
 

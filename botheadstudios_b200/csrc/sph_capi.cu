@@ -30,6 +30,8 @@ struct sph_ctx {
   uint32_t n_eos = 0;
   bool uploaded = false;
   bool fresh = false;      // tree, neighbours, density, EOS and gravity are valid for the current positions
+  bool evaluated = false;  // the tree, sorted state and gravity record are those of an evaluation of this state
+  bool phi_valid = false;  // the gravity record's .w holds the potential of that evaluation
   // captured steady KDK sequence (two substeps), one per parity of the state double buffer
   cudaGraphExec_t kdk_graph[2] = {nullptr, nullptr};
   unsigned long long kdk_graph_launches = 0;  // kernels in one replay
@@ -212,17 +214,25 @@ sph_status init_params(sph_ctx* ctx, Dev& d) {
   return SPH_OK;
 }
 
+bool fused_walk(const sph_ctx* ctx) {
+  return ctx->kc.gravity == SPH_GRAVITY_TREE && ctx->kc.mac == SPH_MAC_GROUP;
+}
+
 // One tree build + everything that depends only on positions (and h): sort, LBVH, gravity, neighbour
-// lists, the smoothing-length solve, density and the EOS record.
-sph_status rebuild(sph_ctx* ctx, bool need_bbox) {
+// lists, the smoothing-length solve, density and the EOS record. `potential`: the fused walk also sums the
+// potential φ (the energy diagnostic's); a KDK step's walks leave it out (the reference computes the
+// potential energy on demand, not in the step: gpu_sph.rs:628), and sph_diag fills it in when asked.
+sph_status rebuild(sph_ctx* ctx, bool need_bbox, bool potential) {
   Dev& d = ctx->d;
   cudaStream_t s = ctx->stream;
   const Cfg& c = ctx->kc;
   phase(ctx, SPH_PHASE_SORT, [&] { return (need_bbox ? launch_bbox(d, s) : 0) + launch_sort_permute(d, s); });
   phase(ctx, SPH_PHASE_TREE, [&] { return launch_tree(d, c, ctx->cfg.theta, s); });
-  const bool fused = c.gravity == SPH_GRAVITY_TREE && c.mac == SPH_MAC_GROUP;
+  const bool fused = fused_walk(ctx);
+  ctx->evaluated = true;
+  ctx->phi_valid = !fused || potential;  // the other gravity paths always write φ (or zero without gravity)
   phase(ctx, SPH_PHASE_GRAVITY, [&] {
-    if (fused) return launch_walk(d, c, s);  // gravity + neighbour lists in one walk
+    if (fused) return launch_walk(d, c, potential, s);  // gravity + neighbour lists in one walk
     if (c.gravity == SPH_GRAVITY_TREE) return launch_gravity_tree(d, c, s);
     if (c.gravity == SPH_GRAVITY_DIRECT) return launch_gravity_direct(d, s);
     cudaMemsetAsync(d.grav, 0, sizeof(float4) * (size_t)d.n, s);
@@ -339,6 +349,8 @@ sph_status upload_impl(sph_ctx* ctx, const SphParticle48* particles, const uint3
   CK(cudaStreamSynchronize(ctx->stream));
   ctx->uploaded = true;
   ctx->fresh = false;
+  ctx->evaluated = false;
+  ctx->phi_valid = false;
   return ret;
 }
 
@@ -358,11 +370,19 @@ sph_status kdk_steady(sph_ctx* ctx) {
     });
     ctx->proposed = ctx->kc.learned != 0;
   }
-  sph_status st = rebuild(ctx, false);
+  sph_status st = rebuild(ctx, false, false);
   if (st != SPH_OK) return st;
   forces(ctx);
   phase(ctx, SPH_PHASE_INTEGRATE, [&] { return launch_kick(d, s); });
   return SPH_OK;
+}
+
+// The potential φ of the last evaluation, when its walk left it out: one potential-only walk over that
+// evaluation's tree (the positions have not moved since: a KDK step ends with a kick). Enqueued on the stream.
+void ensure_potential(sph_ctx* ctx) {
+  if (ctx->phi_valid || !ctx->evaluated || !ctx->d.n) return;
+  ctx->launches += launch_potential(ctx->d, ctx->kc, ctx->stream);
+  ctx->phi_valid = true;
 }
 
 // Two steady substeps as one CUDA graph launch. Two substeps flip the double buffer twice, so a graph
@@ -614,7 +634,7 @@ sph_status sph_set_omega(sph_ctx* ctx, float omega) {
 sph_status sph_eval_forces(sph_ctx* ctx) {
   sph_status st = check_ready(ctx);
   if (st != SPH_OK) return st;
-  st = rebuild(ctx, true);
+  st = rebuild(ctx, true, true);
   if (st != SPH_OK) return st;
   forces(ctx);
   CK(cudaGetLastError());
@@ -630,7 +650,7 @@ sph_status sph_step_kdk(sph_ctx* ctx, uint32_t substeps) {
     // eval 1 at x_n (the tree, gravity and density of the previous eval 2 are still exact: a kick moves no
     // particle), then dt, the half-kick + drift, eval 2 at x_{n+1}, the final half-kick.
     if (!ctx->fresh) {
-      st = rebuild(ctx, true);
+      st = rebuild(ctx, true, false);
       if (st != SPH_OK) return st;
       ctx->fresh = true;
     }
@@ -644,6 +664,8 @@ sph_status sph_step_kdk(sph_ctx* ctx, uint32_t substeps) {
     if (st != SPH_OK) return st;
     ++k;
   }
+  // graph replays run the captured walks without passing through rebuild(): mark the potential stale here
+  if (substeps && fused_walk(ctx)) ctx->phi_valid = false;
   CK(cudaGetLastError());
   return SPH_OK;
 }
@@ -652,7 +674,8 @@ sph_status sph_step_relax(sph_ctx* ctx, uint32_t steps) {
   sph_status st = check_ready(ctx);
   if (st != SPH_OK) return st;
   for (uint32_t k = 0; k < steps; ++k) {
-    st = rebuild(ctx, true);
+    // the relaxation moves the particles after this evaluation: its walk sums the potential
+    st = rebuild(ctx, true, true);
     if (st != SPH_OK) return st;
     forces(ctx);
     phase(ctx, SPH_PHASE_INTEGRATE, [&] { return launch_relax(ctx->d, ctx->stream); });
@@ -890,6 +913,7 @@ sph_status sph_diag(sph_ctx* ctx, sph_diag_out* out) {
   if (!ctx || !out) return SPH_ERR_INVALID;
   cudaSetDevice(ctx->device);
   std::memset(out, 0, sizeof(*out));
+  ensure_potential(ctx);
   if (ctx->d.n) launch_diag(ctx->d, ctx->stream, ctx->d_diag);
   double v[16] = {0};
   DevParams p;
@@ -929,6 +953,7 @@ sph_status sph_diag(sph_ctx* ctx, sph_diag_out* out) {
 sph_status sph_inspect(sph_ctx* ctx, uint32_t what, void* host_out, size_t bytes) {
   if (!ctx || !host_out) return SPH_ERR_INVALID;
   cudaSetDevice(ctx->device);
+  if (what == SPH_Q_ACC_GRAV) ensure_potential(ctx);
   CK(cudaStreamSynchronize(ctx->stream));
   Dev& d = ctx->d;
   const size_t n = (size_t)d.n, L = (size_t)d.L;
@@ -1423,6 +1448,8 @@ sph_status sph_dem_replace(sph_dem* dem, const SphGrain80* grains, uint32_t n) {
   CK(cudaStreamSynchronize(ctx->stream));
   ctx->uploaded = true;
   ctx->fresh = false;
+  ctx->evaluated = false;
+  ctx->phi_valid = false;
   return ret;
 }
 

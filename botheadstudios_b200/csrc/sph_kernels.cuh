@@ -230,7 +230,9 @@ int launch_gravity_direct64(const double* pos3, const double* mass, int n, const
 
 // ---- SPH -------------------------------------------------------------------------------------------
 int launch_neighbours(const Dev& d, const Cfg& c, cudaStream_t s);      // neighbour lists only
-int launch_walk(const Dev& d, const Cfg& c, cudaStream_t s);            // group-MAC gravity + neighbour lists
+// group-MAC gravity + neighbour lists; potential: also the potential φ (the steps' walks leave it out)
+int launch_walk(const Dev& d, const Cfg& c, bool potential, cudaStream_t s);
+int launch_potential(const Dev& d, const Cfg& c, cudaStream_t s);      // φ alone on the current tree
 int launch_gravity_group(const Dev& d, const Cfg& c, cudaStream_t s);   // group-MAC gravity only
 int launch_density_eos(const Dev& d, const Cfg& c, cudaStream_t s);
 int launch_h_solve(const Dev& d, const Cfg& c, cudaStream_t s);

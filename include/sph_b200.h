@@ -108,7 +108,9 @@ enum { SPH_MAC_GROUP = 0, SPH_MAC_PARTICLE = 1 };
 /* Diagnostics: FP64 device sums over the live particles (gpu_sph.rs:628-649 total_energy;
  * tools/impact-run/src/main.rs:528-536 angular momentum), plus device-side flags. */
 typedef struct sph_diag_out {
-  double kinetic, internal, potential;   /* potential from the gravity pass: ½ Σ m_i φ_i */
+  double kinetic, internal, potential;   /* ½ Σ m_i φ_i with φ from the tree gravity of the last evaluation
+                                            (KDK steps leave φ out of their walks, as the reference's step
+                                            does; sph_diag then sums it in one potential-only walk) */
   double momentum[3];
   double angular_momentum[3];            /* about the origin */
   double mass;
@@ -271,7 +273,7 @@ enum {
   SPH_Q_PRESSURE = 12,   /* float[n] */
   SPH_Q_SOUND = 13,      /* float[n] */
   SPH_Q_ACC_SPH = 14,    /* float4[n]  SPH acceleration xyz, du/dt */
-  SPH_Q_ACC_GRAV = 15,   /* float4[n]  gravity acceleration xyz, potential */
+  SPH_Q_ACC_GRAV = 15,   /* float4[n]  gravity acceleration xyz, potential (filled in on demand, as sph_diag) */
   SPH_Q_H = 16,          /* float[n]   smoothing lengths */
   SPH_Q_N_LEAVES = 17,   /* uint32[1]  L */
   SPH_Q_IMPACT_DT = 18,  /* double[n_impacts] dt of each impact's last step */
