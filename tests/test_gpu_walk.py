@@ -161,3 +161,31 @@ def test_full_size_conservation_and_accuracy(impact1m):
     ref = s.gravity_direct64(st["pos"].astype(np.float64), st["mass"].astype(np.float64), I.softening, targets=tg)
     rms = math.sqrt(((g[tg] - ref) ** 2).sum() / (ref ** 2).sum())
     assert rms < 1e-3, rms
+
+
+@pytest.mark.parametrize("graph", [0, 1])
+def test_potential_on_demand_after_steps(graph):
+    """KDK walks leave the potential out; sph_diag sums it in a potential-only walk over the last evaluation's
+    tree. Its PE agrees with the FP64 direct sum of the state, repeated calls agree exactly, the per-particle φ
+    of the inspection is what it summed, and a diagnostic between steps changes nothing: the trajectory and the
+    final PE equal those of a run without it, bit for bit (eager steps and graph replays)."""
+    from botheadstudios_b200 import ic
+    I = ic.impact(16_000, 2_000, n_ngb=48, seed=4)
+    kw = dict(kernel="wendland", multipole=1, leaf_size=16, theta=0.6, h_mode=1, h_neighbours=48, cfl=0.3,
+              graph=graph, **ic.config_kwargs(I.units))
+    n = len(I.particles)
+    with GpuSph(n, **kw) as a, GpuSph(n, **kw) as b:
+        for s in (a, b):
+            s.upload(I.particles, I.eos, I.softening)
+        a.encode_kdk(2)
+        d1, d2 = a.diag(), a.diag()
+        g1 = a.inspect("ACC_GRAV")
+        st = a.readback()
+        a.encode_kdk(2)
+        b.encode_kdk(4)
+        assert np.array_equal(a.readback().view(np.uint8), b.readback().view(np.uint8))
+        assert a.diag()["potential"] == b.diag()["potential"]
+    assert d1["potential"] == d2["potential"] and d1["potential"] < 0.0
+    assert 0.5 * (st["mass"].astype(np.float64) * g1[:, 3]).sum() == pytest.approx(d1["potential"], rel=1e-6)
+    pe = oracle.conservation64(st["pos"], st["vel"], st["mass"], st["u"], soft=I.softening, G=I.units.G)[2]
+    assert d1["potential"] == pytest.approx(pe, rel=1e-3)
