@@ -264,7 +264,8 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
     for (int k = 0; k < 32; ++k) {
       const float2 shk = S.sh[w][k];
       const int s = __float_as_int(shk.x);
-      const bool other = s >= 0 && s != t;
+      // padding (s = −1) sits massless at 3e18: it passes no neighbour test and adds no gravity
+      const bool other = s != t;
       const float4 bj = S.src[w][k];
       const float dx = fsub(bj.x, pi.x), dy = fsub(bj.y, pi.y), dz = fsub(bj.z, pi.z);
       const float dd = dot3_exact(dx, dy, dz);
@@ -342,6 +343,7 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
     __syncwarp();
     bool acc_node = false, leaf = false, open = false, near_leaf = false;
     unsigned ls0 = 0u, ls1 = 1u;  // a leaf's source range, loaded alongside its box
+    unsigned lc = 0u, rc = 0u;    // an internal node's children, loaded alongside its box (no second round trip)
     float4 lbl = make_float4(0.f, 0.f, 0.f, 0.f), lbh = lbl;  // the node's box (and max h), for the lane test
     if (have) {
       const float4 bl = nbmin[node], bh = nbmax[node];
@@ -351,6 +353,9 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
       if (is_leaf) {
         ls0 = leaf_start[node - leaf0];
         ls1 = leaf_start[node - leaf0 + 1];
+      } else {
+        lc = left[node];
+        rc = right[node];
       }
       bool near = false;
       {
@@ -412,8 +417,8 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
     if (sp + 2 * no <= TW_STACK) {
       if (open) {
         const int r = sp + 2 * __popc(bo & lt);
-        stack[r] = left[node];
-        stack[r + 1] = right[node];
+        stack[r] = lc;
+        stack[r + 1] = rc;
       }
       sp += 2 * no;
     } else if (no) {
