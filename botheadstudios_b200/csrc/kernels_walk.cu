@@ -167,7 +167,7 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
       S.src[w][lane] = src;
       __syncwarp();
       if (valid) {
-#pragma unroll 8
+#pragma unroll 4
         for (int k = 0; k < 32; ++k) {
           const float4 bj = S.src[w][k];
           float dx = bj.x - pi.x, dy = bj.y - pi.y, dz = bj.z - pi.z;
