@@ -99,11 +99,13 @@ class Autotuner:
             return dict(self.cache[key])
         best = dict(DEFAULT_CHOICE)
         best_rate = self.measure(probe, best)
+        timed = [dict(best)]  # each configuration is timed once (a coordinate's first value may already be)
         for name in ("leaf_size", "walk_warps", "block_threads"):
             for v in CANDIDATES[name]:
-                if v == best[name]:
-                    continue
                 trial = dict(best, **{name: v})
+                if trial in timed:
+                    continue
+                timed.append(trial)
                 r = self.measure(probe, trial)
                 if r > best_rate:
                     best, best_rate = trial, r
