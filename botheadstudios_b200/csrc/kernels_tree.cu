@@ -451,7 +451,8 @@ __global__ void k_single_leaf_root(Seg* segs) { segs[0].root = 0u; }
 // could not express and that made the reference fall back to a 33-dispatch sweep). The climb is bounded
 // by the tree height; nothing waits.
 // Node data: com.xyz/mass (mass-weighted merge, same f32 operations as the reference), AABB with the
-// subtree's max smoothing length, the opening radius diag/θ + |centre − COM| and, optionally, the
+// subtree's max smoothing length, the opening radius size/θ + |centre − COM| (size: the largest side for the
+// group walk, the diagonal for the reference's per-particle walk) and, optionally, the
 // traceless quadrupole about the COM (parallel-axis merge).
 // ---------------------------------------------------------------------------------------------------
 template <bool QUAD>

@@ -4,16 +4,18 @@
 // A warp owns 32 Morton-consecutive particles (its "group") and walks the tree with a LIFO stack in shared
 // memory, popping up to 32 nodes at a time (one per lane) so node loads overlap instead of serialising.
 // Each popped node is classified for the whole group:
-//   * accepted  — the reference MAC (sqrt(d²+ε²) >= diag/θ + |centre−COM|, bh_gravity.wgsl:382) holds for
-//                 the nearest point of the group's bounding box, hence for every particle of the group, and
-//                 the node's box is outside the SPH reach: appended to the multipole list;
-//   * leaf      — appended to the near list (pairwise gravity + the exact neighbour predicate) when some
-//                 particle of the group can reach it with its own smoothing length (a per-lane test after
-//                 the group test), otherwise to the far list (pairwise gravity only);
+//   * accepted  — the MAC sqrt(d²+ε²) >= side/θ + |centre−COM| (the node's largest side, as the reference's
+//                 CPU octree measures it, bhtree.rs:181, with the δ term of bh_gravity.wgsl:382) holds for the
+//                 nearest point of the group's bounding box, hence for every particle of the group, and the
+//                 node's box is outside the SPH reach: appended to the multipole list;
+//   * leaf      — appended to the near list (pairwise gravity + the neighbour test) when some particle of the
+//                 group can reach it with its own smoothing length (a per-lane test after the group test),
+//                 otherwise to the far list (pairwise gravity only);
 //   * opened    — children pushed (ballot + popc compaction).
 // Nodes whose box lies within ½(h_group,max + h_node,max) of the group are always opened, so every leaf
 // that can hold an SPH neighbour reaches the direct list: the neighbour set {j != i : r_ij < h_ij} is
-// complete and, with single-rounded arithmetic, identical to the reference predicate (sph_step.wgsl:141-143).
+// complete. Without a skin (fixed h) the test is the reference predicate, single-rounded, so the set is
+// identical to it (sph_step.wgsl:141-143); with a skin the list is a candidate set that contains it.
 // Lists are flushed through shared memory in chunks of 32 sources (the next chunk's loads issued before the
 // current chunk is evaluated); every lane then runs the chunk against its own particle with no dependent loads
 // (the interaction loop is pure FP32 work, its reciprocal square root the bare special-function operation).

@@ -266,7 +266,8 @@ enum {
   SPH_Q_PARENT = 5,      /* uint32[2L-1] */
   SPH_Q_NODE_COM = 6,    /* float4[2L-1] com.xyz, mass */
   SPH_Q_NODE_BMIN = 7,   /* float4[2L-1] bmin.xyz, max h */
-  SPH_Q_NODE_BMAX = 8,   /* float4[2L-1] bmax.xyz, opening radius diag/θ+δ */
+  SPH_Q_NODE_BMAX = 8,   /* float4[2L-1] bmax.xyz, opening radius size/θ+δ (size: largest side in GROUP mode,
+                            diagonal in PARTICLE mode) */
   SPH_Q_NBR_COUNT = 9,   /* uint32[n]  neighbours of each particle (original order) */
   SPH_Q_NBR_LIST = 10,   /* uint32[n*max_neighbours] original indices, row i = particle i, unsorted */
   SPH_Q_RHO = 11,        /* float[n] */
