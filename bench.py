@@ -475,7 +475,7 @@ def run_ours(args, wl, world, rank, local, pg):
     # ---- CPU baseline on the host cores (rank 0, N=1 only) ----
     cpu = None
     if world == 1 and not args.no_cpu:
-        r = cpu_reference_run(wl, sample_n=65_536, steps=50, warmup=0, budget_s=15.0)
+        r = cpu_reference_run(wl, sample_n=65_536, steps=1000, warmup=0, budget_s=15.0)  # ~15 s of CPU work
         cpu = dict(value=r["value"], unit=UNIT, cores=r["cores"], kind="port",
                    sample=f"HydroBody::step restated in C++ (f64, octree θ=0.5), 65,536-particle impact of the same "
                           f"generator, {r['steps_run']} steps in {r['seconds']:.1f} s")
