@@ -8,7 +8,11 @@
 // memory, compiled into the library. The caller passes device pointers for the input points and the output
 // accelerations. The array holds at most kNoAllocMaxPoints points; every GPU that loads the library keeps it
 // for the life of the process.
+#include <cuda.h>  // driver-API types only (CUcontext, CUresult); the functions come from the runtime's lookup
+
+#include <cstdint>
 #include <cstring>
+#include <mutex>
 
 #include "../../include/sph_b200.h"
 #include "sph_kernels.cuh"
@@ -42,11 +46,87 @@ constexpr size_t scratch_bytes() {
 constexpr size_t kScratchBytes = scratch_bytes();
 
 // The scratch array. In host code `g_noalloc_scratch` names a host-side stand-in, not device memory: its
-// device address comes from cudaGetSymbolAddress, looked up once per device.
+// device address comes from cudaGetSymbolAddress, looked up once per device context.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
+// The address is cached per device together with the unique id of the context it was looked up in. A
+// cudaDeviceReset (or another context on the same device) loads the module again at another address; its
+// context id differs, so the next call looks the address up again instead of using a stale one. The cache is
+// read and written under a mutex: several host threads may make their first call at the same time.
 constexpr int kMaxDevices = 64;
-void* g_scratch_addr[kMaxDevices] = {nullptr};
+struct ScratchSlot {
+  unsigned long long ctx_id = 0;  // 0: no lookup yet (driver context ids start at 1)
+  void* addr = nullptr;
+};
+ScratchSlot g_scratch[kMaxDevices];
+std::mutex g_scratch_mu;
+
+using PfnCtxGetCurrent = CUresult (*)(CUcontext*);
+using PfnCtxGetId = CUresult (*)(CUcontext, unsigned long long*);
+struct CtxFns {
+  PfnCtxGetCurrent get_current = nullptr;
+  PfnCtxGetId get_id = nullptr;
+};
+// cuCtxGetCurrent / cuCtxGetId through the runtime's driver entry-point lookup (no link against libcuda).
+const CtxFns& ctx_fns() {
+  static const CtxFns fns = [] {
+    CtxFns f;
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      f.get_current = reinterpret_cast<PfnCtxGetCurrent>(p);
+    p = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      f.get_id = reinterpret_cast<PfnCtxGetId>(p);
+    return f;
+  }();
+  return fns;
+}
+
+// Id of the calling thread's current context, 0 when there is none (or the driver cannot say).
+unsigned long long current_ctx_id() {
+  const CtxFns& f = ctx_fns();
+  if (!f.get_current || !f.get_id) return 0;
+  CUcontext c = nullptr;
+  if (f.get_current(&c) != CUDA_SUCCESS || !c) return 0;
+  unsigned long long id = 0;
+  return f.get_id(c, &id) == CUDA_SUCCESS ? id : 0;
+}
+
+// Device address of the scratch array for the current device and context. The lookup runs with the device
+// current, on the first call in each context; during a stream capture no lookup is made (the capture must
+// come after a first call in the same context). Returns nullptr with *status set on failure.
+void* scratch_address(int dev, cudaStream_t s, sph_status* status) {
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &cap) != cudaSuccess) {
+    *status = SPH_ERR_CUDA;
+    return nullptr;
+  }
+  std::lock_guard<std::mutex> lock(g_scratch_mu);
+  ScratchSlot& slot = g_scratch[dev];
+  unsigned long long id = current_ctx_id();
+  if (slot.addr && id != 0 && slot.ctx_id == id) return slot.addr;
+  if (cap != cudaStreamCaptureStatusNone) {
+    *status = SPH_ERR_STATE;  // first call in this context inside a capture: nothing may be looked up here
+    return nullptr;
+  }
+  void* ptr = nullptr;
+  if (cudaGetSymbolAddress(&ptr, g_noalloc_scratch) != cudaSuccess || !ptr) {
+    *status = SPH_ERR_CUDA;
+    return nullptr;
+  }
+  if (id == 0) id = current_ctx_id();  // the lookup made the device's primary context current
+  if (id == 0) {
+    // without a context id a cached address could go stale unseen: use the fresh lookup, cache nothing
+    slot = ScratchSlot{};
+    return ptr;
+  }
+  slot.ctx_id = id;
+  slot.addr = ptr;
+  return ptr;
+}
 
 template <typename T>
 T* carve(unsigned char*& p, size_t count) {
@@ -128,10 +208,14 @@ __global__ void k_noalloc_load(const float4* __restrict__ in, int n, State st) {
   st.seg[i] = 0u;
 }
 
+// The results in input order. If the walk's traversal stack overflowed (it then skips subtrees), every
+// output is NaN: the caller has no context whose flags it could read, so the result itself says it is invalid.
 __global__ void k_noalloc_store(int n, const unsigned* __restrict__ id, const float4* __restrict__ grav,
-                                float4* __restrict__ out) {
+                                const DevParams* __restrict__ P, float4* __restrict__ out) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t < n) out[id[t]] = grav[t];
+  if (t >= n) return;
+  const float nan = __int_as_float(0x7fc00000);
+  out[id[t]] = (P->flags & kFlagStackOverflow) ? make_float4(nan, nan, nan, nan) : grav[t];
 }
 
 }  // namespace
@@ -145,18 +229,20 @@ extern "C" sph_status sph_gravity_tree_noalloc(const void* d_bodies4, uint32_t n
   if (!d_bodies4 || !d_acc4 || n == 0 || !(theta > 0.0f) || !(softening >= 0.0f) || multipole > 1) {
     return SPH_ERR_INVALID;
   }
+  // the kernels read and write whole float4 records
+  if (((uintptr_t)d_bodies4 | (uintptr_t)d_acc4) & 15u) return SPH_ERR_INVALID;
   if (n > kNoAllocMaxPoints) return SPH_ERR_INVALID;  // beyond the fixed scratch array
   if (leaf_size < kNoAllocMinLeaf || leaf_size > 32 || (leaf_size & (leaf_size - 1)) != 0) return SPH_ERR_INVALID;
+  // an error left pending by the caller's own earlier work is not this call's to report or to clear
+  if (cudaPeekAtLastError() != cudaSuccess) return SPH_ERR_CUDA;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return SPH_ERR_CUDA;
-  // Set-up, once per device with that device current: the device address of the scratch array.
-  if (!g_scratch_addr[dev]) {
-    void* ptr = nullptr;
-    if (cudaGetSymbolAddress(&ptr, g_noalloc_scratch) != cudaSuccess || !ptr) return SPH_ERR_CUDA;
-    g_scratch_addr[dev] = ptr;
-  }
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  Dev d = carve_dev(static_cast<unsigned char*>(g_scratch_addr[dev]), leaf_size);
+  // Set-up, once per device context with that device current: the device address of the scratch array.
+  sph_status st = SPH_OK;
+  void* base = scratch_address(dev, s, &st);
+  if (!base) return st;
+  Dev d = carve_dev(static_cast<unsigned char*>(base), leaf_size);
   d.n = (int)n;
   d.cur = 0;
   d.L = (int)((n + leaf_size - 1) / leaf_size);
@@ -170,6 +256,7 @@ extern "C" sph_status sph_gravity_tree_noalloc(const void* d_bodies4, uint32_t n
   launch_sort_permute(d, s);
   launch_tree(d, c, theta, s);
   launch_gravity_group(d, c, s);
-  k_noalloc_store<<<(n + 255) / 256, 256, 0, s>>>((int)n, d.s().id, d.grav, static_cast<float4*>(d_acc4));
+  k_noalloc_store<<<(n + 255) / 256, 256, 0, s>>>((int)n, d.s().id, d.grav, d.P, static_cast<float4*>(d_acc4));
+  // no error was pending on entry, so one pending now comes from these launches: report it (and clear it)
   return cudaGetLastError() == cudaSuccess ? SPH_OK : SPH_ERR_CUDA;
 }

@@ -386,12 +386,15 @@ uint32_t sph_dem_count(const sph_dem* dem);
  * potential), in input order. The work is enqueued on `stream` (a cudaStream_t; NULL = the default stream)
  * on the calling thread's current device; the result is ready when that stream reaches this point.
  * Same walk as sph_gravity with SPH_MAC_GROUP (side-based θ, Barnes' δ, quadrupole if multipole = 1).
- * Limits: n <= 65536 and leaf_size in {8, 16, 32}; larger n returns SPH_ERR_INVALID. All scratch lives in
- * one fixed array compiled into the library (about 15 MB, held by every GPU that loads the library until
- * the process exits). The first call on a device looks up that array's device address; make that first
- * call before any stream capture. Every call uses the same array, so calls whose work overlaps on the GPU
- * (different streams, or different host threads on one device) race and corrupt each other's results:
- * order them on one stream. */
+ * Limits: n <= 65536 and leaf_size in {8, 16, 32}; larger n returns SPH_ERR_INVALID. Both pointers must be
+ * 16-byte aligned (SPH_ERR_INVALID otherwise). All scratch lives in one fixed array compiled into the library
+ * (about 15 MB, held by every GPU that loads the library until the process exits). The first call in each
+ * device context (and the first after a cudaDeviceReset) looks up that array's device address; make that
+ * first call before any stream capture (a first call inside a capture returns SPH_ERR_STATE). Every call
+ * uses the same array, so calls whose work overlaps on the GPU (different streams, or different host threads
+ * on one device) race and corrupt each other's results: order them on one stream. If the traversal stack
+ * (1,536 nodes per warp) overflows, every output is NaN. A CUDA error already pending on the calling thread
+ * is left in place and returns SPH_ERR_CUDA before any work is enqueued. */
 sph_status sph_gravity_tree_noalloc(const void* d_bodies4, uint32_t n, double G, float softening, float theta,
                                     uint32_t leaf_size, uint32_t multipole, void* d_acc4, void* stream);
 
