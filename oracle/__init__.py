@@ -93,11 +93,19 @@ def lib():
     L.orc_hydro_step.argtypes = [C.c_void_p, C.c_double, C.c_int]
     L.orc_hydro_density.argtypes = [C.c_void_p, C.c_int]
     L.orc_hydro_forces.argtypes = [C.c_void_p, f64p, f64p, C.c_int]
+    L.orc_hydro_eval_sampled.argtypes = [C.c_void_p, C.c_int, f64p]
     L.orc_hydro_courant_dt.restype = C.c_double
     L.orc_hydro_courant_dt.argtypes = [C.c_void_p, C.c_double, C.c_double]
     L.orc_hydro_get.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     L.orc_max_threads.restype = C.c_int
     L.orc_conservation64.argtypes = [f64p, f64p, f64p, f64p, C.c_int, C.c_double, C.c_double, C.c_int, f64p]
+    L.orc_h_solve32.restype = C.c_float
+    L.orc_h_solve32.argtypes = [f32p, f32p, C.c_int, C.c_int, C.c_float, C.c_float, C.c_int, f32p, f32p, f32p]
+    L.orc_h_solve64.restype = C.c_int
+    L.orc_h_solve64.argtypes = [f64p, f64p, f64p, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_int,
+                                f64p, f64p, f64p]
+    L.orc_relax32.argtypes = [f32p, f32p, f32p, C.c_int, C.c_float, C.c_float, C.c_float]
+    L.orc_signal32.argtypes = [f32p, f32p, f32p, C.c_int, C.c_float, f32p]
     _lib = L
     return L
 
@@ -283,6 +291,47 @@ def sph_forces32(pos4, vel4, mass, rho, P, c, av_alpha=1.0, av_beta=2.0, r_min=1
     return out
 
 
+def h_solve32(pos4, mass, eta, skin, iters, kernel=1):
+    """The smoothing-length solve in f32: `iters` Jacobi-Newton steps from h0 = pos4[:, 3] inside the list skin,
+    then the density at the final h. Returns (h, rho, residual) per particle."""
+    p = _c(pos4, np.float32)
+    n = len(p)
+    h = np.empty(n, np.float32)
+    rho = np.empty(n, np.float32)
+    res = np.empty(n, np.float32)
+    lib().orc_h_solve32(p, _c(mass, np.float32), n, kernel, eta, skin, int(iters), h, rho, res)
+    return h, rho, res
+
+
+def h_solve64(pos3, h0, mass, eta, skin, kernel=1, step_tol=1e-12, max_iter=200):
+    """The same solve in f64, iterated until no h moves by more than step_tol in a step (Price 2012 Newton on
+    rho(h) = m (eta/h)^3 with the symmetric h_ij). Returns (h, rho, residual, steps); steps > max_iter means it
+    did not settle."""
+    n = len(mass)
+    h = np.empty(n)
+    rho = np.empty(n)
+    res = np.empty(n)
+    it = lib().orc_h_solve64(_c(pos3, np.float64), _c(h0, np.float64), _c(mass, np.float64), n, kernel, eta, skin,
+                             step_tol, int(max_iter), h, rho, res)
+    return h, rho, res, it
+
+
+def relax32(pos4, vel4, acc4, dt, damp, omega):
+    """One cs_relax step (sph_step.wgsl:245-257) in f32 on copies of pos4/vel4; returns (pos4, vel4)."""
+    p = np.array(pos4, np.float32, order="C")
+    v = np.array(vel4, np.float32, order="C")
+    lib().orc_relax32(p, v, _c(acc4, np.float32), len(p), dt, damp, omega)
+    return p, v
+
+
+def signal32(pos4, vel4, c, floor=1.0):
+    """cs_signal (sph_step.wgsl:263-269): h / max(c + |v|, floor) per particle; the adaptive dt is cfl * min."""
+    p = _c(pos4, np.float32)
+    sig = np.empty(len(p), np.float32)
+    lib().orc_signal32(p, _c(vel4, np.float32), _c(c, np.float32), len(p), floor, sig)
+    return sig
+
+
 def cpu_forces64(pos3, vel3, h, mass, u, mat, eos10_table, soft, G=6.674e-11, av_alpha=1.0, av_beta=2.0,
                  du_floor=1.0, kernel=0):
     n = len(h)
@@ -329,6 +378,14 @@ class HydroBody:
         du = np.empty(self.n)
         self._L.orc_hydro_forces(self._h, acc, du, nthreads)
         return acc, du
+
+    def eval_sampled(self, stride):
+        """One force evaluation of the single-threaded path at full size with its per-particle loops run for
+        every stride-th block of 512 consecutive particles: returns (seconds of the full-size parts, seconds of
+        the sampled loops); a full evaluation takes about the first + stride x the second."""
+        t = np.zeros(2)
+        self._L.orc_hydro_eval_sampled(self._h, int(stride), t)
+        return float(t[0]), float(t[1])
 
     def courant_dt(self, cfl, sig_floor=1.0):
         return self._L.orc_hydro_courant_dt(self._h, cfl, sig_floor)

@@ -25,6 +25,7 @@
 #include <cstring>
 #include <numeric>
 #include <vector>
+#include <chrono>
 #ifdef _OPENMP
 #include <omp.h>
 #endif
@@ -493,6 +494,44 @@ struct Hydro {
     }
   }
 
+  // Pressure and sound speed of every particle (eos.rs:52-96), once per force evaluation.
+  void eos_all(int nthreads, std::vector<double>& p, std::vector<double>& c) const {
+    p.resize(n);
+    c.resize(n);
+#pragma omp parallel for num_threads(std::max(nthreads, 1))
+    for (int i = 0; i < n; ++i) {
+      const double* e = &eos[10 * (size_t)mat[i]];
+      p[i] = pressure64(e, rho[i], u[i]);
+      c[i] = std::sqrt(sound_speed_sq64(e, rho[i], u[i]));
+    }
+  }
+  // The pair terms of forces_and_dudt (hydrostatic.rs:300-340): pressure + Monaghan AV + du/dt of the pair
+  // (i, j), added to i and, when aj is given, with the opposite sign to j.
+  bool pair_terms(int i, int j, const std::vector<double>& p, const std::vector<double>& c, double* ai, double& dui,
+                  double* aj, double& duj) const {
+    const double dpos[3] = {pos[3 * i] - pos[3 * j], pos[3 * i + 1] - pos[3 * j + 1], pos[3 * i + 2] - pos[3 * j + 2]};
+    const double r = std::sqrt(dpos[0] * dpos[0] + dpos[1] * dpos[1] + dpos[2] * dpos[2]);
+    const double hij = 0.5 * (h[i] + h[j]);
+    if (r >= hij || r < 1.0e-9) return false;
+    const double dvel[3] = {vel[3 * i] - vel[3 * j], vel[3 * i + 1] - vel[3 * j + 1], vel[3 * i + 2] - vel[3 * j + 2]};
+    const double vr = dvel[0] * dpos[0] + dvel[1] * dpos[1] + dvel[2] * dpos[2];
+    double pi_ij = 0.0;
+    if (vr < 0.0) {
+      const double mu = hij * vr / (r * r + 0.01 * hij * hij);
+      const double c_bar = 0.5 * (c[i] + c[j]);
+      const double rho_bar = 0.5 * (rho[i] + rho[j]);
+      pi_ij = (-av_alpha * c_bar * mu + av_beta * mu * mu) / rho_bar;
+    }
+    const double coeff = p[i] / (rho[i] * rho[i]) + p[j] / (rho[j] * rho[j]) + pi_ij;
+    const double dw = dW(r, hij);
+    const double grad[3] = {dpos[0] / r * dw, dpos[1] / r * dw, dpos[2] / r * dw};
+    const double vdg = dvel[0] * grad[0] + dvel[1] * grad[1] + dvel[2] * grad[2];
+    for (int k = 0; k < 3; ++k) { ai[k] += grad[k] * (-coeff * mass[j]); if (aj) aj[k] += grad[k] * (coeff * mass[i]); }
+    dui += 0.5 * mass[j] * coeff * vdg;
+    duj += 0.5 * mass[i] * coeff * vdg;
+    return true;
+  }
+
   // forces_and_dudt, hydrostatic.rs:300-340: BH gravity + pressure + Monaghan AV + du/dt.
   void forces(std::vector<double>& acc, std::vector<double>& dudt, int nthreads) {
     acc.assign(3 * (size_t)n, 0.0);
@@ -500,55 +539,78 @@ struct Hydro {
     OctTree bh;
     bh.build(pos.data(), mass.data(), n, theta, softening, G);
     bh.accelerations(acc.data(), std::max(nthreads, 1));
-    std::vector<double> p(n), c(n);
-#pragma omp parallel for num_threads(std::max(nthreads, 1))
-    for (int i = 0; i < n; ++i) {
-      const double* e = &eos[10 * (size_t)mat[i]];
-      p[i] = pressure64(e, rho[i], u[i]);
-      c[i] = std::sqrt(sound_speed_sq64(e, rho[i], u[i]));
-    }
-    auto pair_terms = [&](int i, int j, double* ai, double& dui, double* aj, double& duj) -> bool {
-      const double dpos[3] = {pos[3 * i] - pos[3 * j], pos[3 * i + 1] - pos[3 * j + 1], pos[3 * i + 2] - pos[3 * j + 2]};
-      const double r = std::sqrt(dpos[0] * dpos[0] + dpos[1] * dpos[1] + dpos[2] * dpos[2]);
-      const double hij = 0.5 * (h[i] + h[j]);
-      if (r >= hij || r < 1.0e-9) return false;
-      const double dvel[3] = {vel[3 * i] - vel[3 * j], vel[3 * i + 1] - vel[3 * j + 1], vel[3 * i + 2] - vel[3 * j + 2]};
-      const double vr = dvel[0] * dpos[0] + dvel[1] * dpos[1] + dvel[2] * dpos[2];
-      double pi_ij = 0.0;
-      if (vr < 0.0) {
-        const double mu = hij * vr / (r * r + 0.01 * hij * hij);
-        const double c_bar = 0.5 * (c[i] + c[j]);
-        const double rho_bar = 0.5 * (rho[i] + rho[j]);
-        pi_ij = (-av_alpha * c_bar * mu + av_beta * mu * mu) / rho_bar;
-      }
-      const double coeff = p[i] / (rho[i] * rho[i]) + p[j] / (rho[j] * rho[j]) + pi_ij;
-      const double dw = dW(r, hij);
-      const double grad[3] = {dpos[0] / r * dw, dpos[1] / r * dw, dpos[2] / r * dw};
-      const double vdg = dvel[0] * grad[0] + dvel[1] * grad[1] + dvel[2] * grad[2];
-      for (int k = 0; k < 3; ++k) { ai[k] += grad[k] * (-coeff * mass[j]); if (aj) aj[k] += grad[k] * (coeff * mass[i]); }
-      dui += 0.5 * mass[j] * coeff * vdg;
-      duj += 0.5 * mass[i] * coeff * vdg;
-      return true;
-    };
+    std::vector<double> p, c;
+    eos_all(nthreads, p, c);
     if (n < 512) {
       for (int i = 0; i < n; ++i)
-        for (int j = i + 1; j < n; ++j) pair_terms(i, j, &acc[3 * i], dudt[i], &acc[3 * j], dudt[j]);
+        for (int j = i + 1; j < n; ++j) pair_terms(i, j, p, c, &acc[3 * i], dudt[i], &acc[3 * j], dudt[j]);
       return;
     }
     CellList cl;
     cl.build(n, hmax(), [&](int i, double* q) { for (int k = 0; k < 3; ++k) q[k] = pos[3 * i + k]; });
     if (nthreads <= 1) {
       for (int i = 0; i < n; ++i)
-        cl.around(&pos[3 * i], [&](int j) { if (j > i) pair_terms(i, j, &acc[3 * i], dudt[i], &acc[3 * j], dudt[j]); });
+        cl.around(&pos[3 * i], [&](int j) { if (j > i) pair_terms(i, j, p, c, &acc[3 * i], dudt[i], &acc[3 * j], dudt[j]); });
     } else {
 #pragma omp parallel for schedule(dynamic, 256) num_threads(nthreads)
       for (int i = 0; i < n; ++i) {
         double ai[3] = {0, 0, 0}, dui = 0.0, dummy = 0.0;
-        cl.around(&pos[3 * i], [&](int j) { if (j != i) pair_terms(i, j, ai, dui, nullptr, dummy); });
+        cl.around(&pos[3 * i], [&](int j) { if (j != i) pair_terms(i, j, p, c, ai, dui, nullptr, dummy); });
         for (int k = 0; k < 3; ++k) acc[3 * i + k] += ai[k];
         dudt[i] += dui;
       }
     }
+  }
+
+  // One force evaluation of the single-threaded path (the reference's own: symmetric i < j pair loops over
+  // the neighbour grid, a per-particle octree walk) timed at full size with its per-particle loops run over
+  // every `stride`-th block of 512 consecutive particles only (blocks keep the cache reuse that consecutive,
+  // spatially close particles give the full loops). t[0] = seconds of the parts that run in full (grid and
+  // octree builds, the EOS of every particle), t[1] = seconds of the sampled loops (density pairs, gravity
+  // walks, force pairs). A full evaluation takes about t[0] + stride · t[1]. The state is left unchanged.
+  void eval_sampled(int stride, double* t) {
+    constexpr int kBlock = 512;
+    auto sampled = [&](auto&& f) {
+      for (int b0 = 0; b0 < n; b0 += kBlock * stride)
+        for (int i = b0; i < std::min(b0 + kBlock, n); ++i) f(i);
+    };
+    using clk = std::chrono::steady_clock;
+    auto sec = [](clk::time_point a, clk::time_point b) { return std::chrono::duration<double>(b - a).count(); };
+    std::vector<double> rho_s(n);
+    auto t0 = clk::now();
+    for (int i = 0; i < n; ++i) rho_s[i] = mass[i] * W(0.0, h[i]);
+    CellList cl;
+    cl.build(n, hmax(), [&](int i, double* q) { for (int k = 0; k < 3; ++k) q[k] = pos[3 * i + k]; });
+    auto t1 = clk::now();
+    sampled([&](int i) {
+      cl.around(&pos[3 * i], [&](int j) {
+        if (j <= i) return;
+        const double r = dist(i, j), hij = 0.5 * (h[i] + h[j]);
+        if (r < hij) {
+          const double w = W(r, hij);
+          rho_s[i] += mass[j] * w;
+          rho_s[j] += mass[i] * w;
+        }
+      });
+    });
+    auto t2 = clk::now();
+    OctTree bh;
+    bh.build(pos.data(), mass.data(), n, theta, softening, G);
+    auto t3 = clk::now();
+    std::vector<double> acc(3 * (size_t)n, 0.0), dudt(n, 0.0);
+    sampled([&](int i) { bh.accel_on(i, 0, &acc[3 * i]); });
+    auto t4 = clk::now();
+    std::vector<double> p, c;
+    eos_all(1, p, c);
+    CellList cl2;
+    cl2.build(n, hmax(), [&](int i, double* q) { for (int k = 0; k < 3; ++k) q[k] = pos[3 * i + k]; });
+    auto t5 = clk::now();
+    sampled([&](int i) {
+      cl2.around(&pos[3 * i], [&](int j) { if (j > i) pair_terms(i, j, p, c, &acc[3 * i], dudt[i], &acc[3 * j], dudt[j]); });
+    });
+    auto t6 = clk::now();
+    t[0] = sec(t0, t1) + sec(t2, t3) + sec(t4, t5);
+    t[1] = sec(t1, t2) + sec(t3, t4) + sec(t5, t6);
   }
 
   // step, hydrostatic.rs:345-359 (KDK, two force evaluations, u clamped at 0).
@@ -904,6 +966,193 @@ void orc_sph_forces32(const float* pos4, const float* vel4, const float* mass, c
   }
 }
 
+}  // extern "C"
+
+// ---- smoothing-length solve (no reference counterpart: the reference keeps h fixed, hydrostatic.rs:59-61) --
+// The density is the reference's symmetric sum (sph_step.wgsl:120-149: self term m_i W(0,h_i), pairs r < h_ij
+// with h_ij = ½(h_i+h_j)); the solve drives f(h_i) = ρ_i(h) − m_i(η/h_i)³ to zero by Newton–Raphson (Price
+// 2012, J. Comput. Phys. 231, §3.2.1), with ∂ρ_i/∂h_i = m_i ∂W(0,h_i)/∂h + Σ_j m_j ½ ∂W(r,h_ij)/∂h (h_ij moves
+// by ½ dh_i). W = σ(h) f(q), σ = c/h³, q = r/h ⇒ ∂W/∂h = −(σ/h)(3f + q f'(q)), written from the formula.
+// Every particle steps from the same iterate (Jacobi). A step is limited to ±20 % and to the box the
+// neighbour-list skin allows around the smoothing length h0 the list was built with:
+// h ≤ h0(1+skin)·0.999 and h ≥ h0/((1+skin)·1.001).
+// orc_h_solve32 runs a fixed number of such steps in f32 and then the density pass at the final h (the
+// product's sequence); orc_h_solve64 iterates in f64 until the iterate settles (the converged solution).
+// ---------------------------------------------------------------------------------------------------
+namespace {
+template <typename T>
+T kern_f(int kind, T q, T& fp) {  // f(q), f'(q) of the two kernels (support radius h)
+  fp = T(0);
+  if (q >= T(1)) return T(0);
+  if (kind == 1) {
+    const T t = T(1) - q, t3 = t * t * t;
+    fp = T(-20) * q * t3;
+    return t3 * t * (T(1) + T(4) * q);
+  }
+  if (q < T(0.5)) {
+    fp = T(-12) * q + T(18) * q * q;
+    return T(1) - T(6) * q * q + T(6) * q * q * q;
+  }
+  const T t = T(1) - q;
+  fp = T(-6) * t * t;
+  return T(2) * t * t * t;
+}
+template <typename T>
+void kern_w_dwdh(int kind, T r, T h, T& w, T& dwdh) {
+  const T c = kind == 1 ? T(21) / (T(2) * T(kPi)) : T(8) / T(kPi);
+  const T q = r / h;
+  T fp;
+  const T f = kern_f<T>(kind, q, fp);
+  const T sig = c / (h * h * h);
+  w = sig * f;
+  dwdh = -(sig / h) * (T(3) * f + q * fp);
+}
+template <typename T>
+T h_newton_step(T h, T m, T rho, T drho, T eta, T h0, T skin, T& res) {
+  const T rt = m * (eta * eta * eta) / (h * h * h);
+  const T f = rho - rt;
+  res = std::fabs(f) / std::max(rho, T(1e-30));
+  const T fp = drho + T(3) * rt / h;
+  const T dh = std::fabs(fp) > T(0) ? -f / fp : T(0);
+  T hn = h + dh;
+  if (!(hn == hn)) hn = h;
+  hn = std::min(std::max(hn, T(0.8) * h), T(1.2) * h);
+  hn = std::min(hn, h0 * (T(1) + skin) * T(0.999));
+  hn = std::max(hn, h0 / ((T(1) + skin) * T(1.001)));
+  return hn;
+}
+// Candidate pairs of the solve: everything within the largest h_ij the skin allows, exact test per pass.
+template <typename T>
+void hsolve_candidates(const T* pos, int stride, const T* h0, int n, T skin, std::vector<std::vector<int>>& cand) {
+  T hm = T(0);
+  for (int i = 0; i < n; ++i) hm = std::max(hm, h0[i]);
+  const double reach = (double)hm * (1.0 + (double)skin) * (1.0 + 1.0e-6);
+  CellList cl;
+  cl.build(n, reach, [&](int i, double* p) { for (int k = 0; k < 3; ++k) p[k] = (double)pos[stride * i + k]; });
+  cand.assign(n, {});
+  for (int i = 0; i < n; ++i) {
+    double p[3] = {(double)pos[stride * i], (double)pos[stride * i + 1], (double)pos[stride * i + 2]};
+    cl.around(p, [&](int j) {
+      if (j == i) return;
+      double d2 = 0.0;
+      for (int k = 0; k < 3; ++k) {
+        const double d = (double)pos[stride * i + k] - (double)pos[stride * j + k];
+        d2 += d * d;
+      }
+      if (d2 < reach * reach) cand[i].push_back(j);
+    });
+    std::sort(cand[i].begin(), cand[i].end());
+  }
+}
+// ρ_i, ∂ρ_i/∂h_i at the current h over the candidates (f32: the product's single-rounded pair distance).
+template <typename T>
+void hsolve_sums(const T* pos, int stride, const T* mass, const T* h, int i, int kind,
+                 const std::vector<int>& cand, T& rho, T& drho) {
+  T w, dwdh;
+  kern_w_dwdh<T>(kind, T(0), h[i], w, dwdh);
+  rho = mass[i] * w;
+  drho = mass[i] * dwdh;
+  for (int j : cand) {
+    const T dx = pos[stride * i] - pos[stride * j], dy = pos[stride * i + 1] - pos[stride * j + 1],
+            dz = pos[stride * i + 2] - pos[stride * j + 2];
+    const T r = std::sqrt((dx * dx + dy * dy) + dz * dz);
+    const T hij = T(0.5) * (h[i] + h[j]);
+    if (!(r < hij)) continue;
+    kern_w_dwdh<T>(kind, r, hij, w, dwdh);
+    rho += mass[j] * w;
+    drho += mass[j] * T(0.5) * dwdh;
+  }
+}
+}  // namespace
+
+extern "C" {
+// f32: `iters` Jacobi-Newton steps from h0 = pos4[.w], then the density at the final h. h_out, rho_out,
+// res_out (relative residual |ρ − m(η/h)³|/ρ at the final h) per particle. Returns the largest residual.
+float orc_h_solve32(const float* pos4, const float* mass, int n, int kernel, float eta, float skin, int iters,
+                    float* h_out, float* rho_out, float* res_out) {
+  std::vector<float> h0(n), h(n), hn(n);
+  for (int i = 0; i < n; ++i) h0[i] = h[i] = pos4[4 * i + 3];
+  std::vector<std::vector<int>> cand;
+  hsolve_candidates<float>(pos4, 4, h0.data(), n, skin, cand);
+  for (int it = 0; it < iters; ++it) {
+#pragma omp parallel for schedule(dynamic, 256)
+    for (int i = 0; i < n; ++i) {
+      float rho, drho, res;
+      hsolve_sums<float>(pos4, 4, mass, h.data(), i, kernel, cand[i], rho, drho);
+      hn[i] = h_newton_step<float>(h[i], mass[i], rho, drho, eta, h0[i], skin, res);
+    }
+    h.swap(hn);
+  }
+  float rmax = 0.0f;
+  for (int i = 0; i < n; ++i) {
+    float rho, drho;
+    hsolve_sums<float>(pos4, 4, mass, h.data(), i, kernel, cand[i], rho, drho);
+    const float rt = mass[i] * (eta * eta * eta) / (h[i] * h[i] * h[i]);
+    const float res = std::fabs(rho - rt) / std::max(rho, 1e-30f);
+    h_out[i] = h[i];
+    rho_out[i] = rho;
+    res_out[i] = res;
+    rmax = std::max(rmax, res);
+  }
+  return rmax;
+}
+// f64: Jacobi-Newton from h0 until no smoothing length moves by more than step_tol (relative) in a step, or
+// max_iter steps. The clamps make a fixed point of the limited iteration the solution (a particle held at
+// its skin bound stops moving). Returns the steps taken (max_iter + 1 when it did not settle); h_out, rho_out
+// and res_out (the relative residual at h_out) per particle.
+int orc_h_solve64(const double* pos3, const double* h0, const double* mass, int n, int kernel, double eta,
+                  double skin, double step_tol, int max_iter, double* h_out, double* rho_out, double* res_out) {
+  std::vector<double> h(h0, h0 + n), hn(n);
+  std::vector<std::vector<int>> cand;
+  hsolve_candidates<double>(pos3, 3, h0, n, skin, cand);
+  int it = 0;
+  bool settled = false;
+  for (; it <= max_iter; ++it) {
+    double move = 0.0;
+#pragma omp parallel for schedule(dynamic, 256) reduction(max : move)
+    for (int i = 0; i < n; ++i) {
+      double rho, drho;
+      hsolve_sums<double>(pos3, 3, mass, h.data(), i, kernel, cand[i], rho, drho);
+      hn[i] = h_newton_step<double>(h[i], mass[i], rho, drho, eta, h0[i], skin, res_out[i]);
+      rho_out[i] = rho;
+      move = std::max(move, std::fabs(hn[i] - h[i]) / h[i]);
+    }
+    if (move <= step_tol) {
+      settled = true;
+      break;
+    }
+    if (it < max_iter) h.swap(hn);
+  }
+  for (int i = 0; i < n; ++i) h_out[i] = h[i];
+  return settled ? it : max_iter + 1;
+}
+
+// cs_relax, sph_step.wgsl:245-257, in f32: a_cf = ω²(x, y, 0); v = (v + (a + a_cf)·dt)·damp; x = x + v·dt.
+// pos4/vel4 are updated in place (h and u untouched); acc4 = (a.xyz, du/dt) of the evaluation at x.
+void orc_relax32(float* pos4, float* vel4, const float* acc4, int n, float dt, float damp, float omega) {
+  const float w2 = omega * omega;
+  for (int i = 0; i < n; ++i) {
+    float* p = pos4 + 4 * i;
+    float* v = vel4 + 4 * i;
+    const float* a = acc4 + 4 * i;
+    const float cf[3] = {w2 * p[0], w2 * p[1], 0.0f};
+    for (int k = 0; k < 3; ++k) {
+      v[k] = (v[k] + (a[k] + cf[k]) * dt) * damp;
+      p[k] = p[k] + v[k] * dt;
+    }
+  }
+}
+
+// cs_signal, sph_step.wgsl:263-269: signal_i = h_i / max(c_i + |v_i|, floor) (the shader's floor is 1 m/s);
+// the adaptive dt is cfl · min_i signal_i (the host reduction of impact-run main.rs:345-356).
+void orc_signal32(const float* pos4, const float* vel4, const float* c, int n, float floor, float* sig) {
+  for (int i = 0; i < n; ++i) {
+    const float* v = vel4 + 4 * i;
+    const float vmag = std::sqrt((v[0] * v[0] + v[1] * v[1]) + v[2] * v[2]);
+    sig[i] = pos4[4 * i + 3] / std::max(c[i] + vmag, floor);
+  }
+}
+
 // ---- f64 verifier physics (tools/sph-verify/src/main.rs:106-251) ----------------------------------
 // cpu_forces: O(N²) density, direct gravity (pow form) and SPH/AV/du-dt with P,c per pair (1e-3 steps).
 void orc_cpu_forces64(const double* pos3, const double* vel3, const double* h, const double* mass, const double* u,
@@ -1011,6 +1260,7 @@ void orc_hydro_forces(void* p, double* acc3, double* dudt, int nthreads) {
   std::memcpy(acc3, a.data(), sizeof(double) * a.size());
   std::memcpy(dudt, du.data(), sizeof(double) * du.size());
 }
+void orc_hydro_eval_sampled(void* p, int stride, double* t) { static_cast<Hydro*>(p)->eval_sampled(std::max(stride, 1), t); }
 double orc_hydro_courant_dt(void* p, double cfl, double sig_floor) { return static_cast<Hydro*>(p)->courant_dt(cfl, sig_floor); }
 void orc_hydro_get(void* p, double* pos3, double* vel3, double* u, double* rho) {
   Hydro* hb = static_cast<Hydro*>(p);
