@@ -46,7 +46,7 @@ class SphConfig(C.Structure):
                 ("rho_floor", C.c_float), ("du_floor", C.c_float), ("r_min", C.c_float), ("sig_floor", C.c_float),
                 ("device", C.c_int32), ("mac", C.c_uint32), ("graph", C.c_uint32),
                 ("block_threads", C.c_uint32), ("walk_warps", C.c_uint32), ("h_skin", C.c_float),
-                ("reserved", C.c_uint32 * 2)]
+                ("walk_stack", C.c_uint32), ("reserved", C.c_uint32)]
 
 
 class SphDiag(C.Structure):

@@ -37,7 +37,7 @@ __global__ void __launch_bounds__(GR_WARPS * 32) k_gravity_tree(
     const unsigned* __restrict__ seg, const Seg* __restrict__ segs, const unsigned* __restrict__ left,
     const unsigned* __restrict__ right, const float4* __restrict__ ncom, const float4* __restrict__ nbmax,
     const float4* __restrict__ nq0, const float4* __restrict__ nq1, const DevParams* __restrict__ P,
-    float4* __restrict__ out) {
+    float4* __restrict__ out, int stack_cap) {
   __shared__ uint2 s_stack[GR_WARPS][kTravStack];
   const int wib = threadIdx.x >> 5;
   const unsigned lane = threadIdx.x & 31u;
@@ -163,7 +163,7 @@ __global__ void __launch_bounds__(GR_WARPS * 32) k_gravity_tree(
     }
     const unsigned om = __ballot_sync(SPH_FULL_MASK, open);
     if (om) {
-      if (sp + 2 <= kTravStack) {
+      if (sp + 2 <= stack_cap) {
         if (lane == 0) {
           stack[sp] = make_uint2(left[node], om);
           stack[sp + 1] = make_uint2(right[node], om);
@@ -188,7 +188,7 @@ int launch_gravity_tree(const Dev& d, const Cfg& c, cudaStream_t s) {
   const State& st = d.s();
 #define GRAV_ARGS                                                                                           \
   d.body, st.x, st.y, st.z, d.n, d.L, d.leaf_start, st.seg, d.segs, d.left, d.right, d.ncom, d.nbmax, d.nq0, d.nq1, \
-      d.P, d.grav
+      d.P, d.grav, c.walk_stack > 0 && c.walk_stack < kTravStack ? c.walk_stack : kTravStack
   if (c.quad) {
     if (c.hilo) k_gravity_tree<true, true><<<blocks, GR_WARPS * 32, 0, s>>>(GRAV_ARGS);
     else k_gravity_tree<true, false><<<blocks, GR_WARPS * 32, 0, s>>>(GRAV_ARGS);

@@ -81,7 +81,7 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
     const float4* __restrict__ ncom, const float4* __restrict__ nbmin, const float4* __restrict__ nbmax, const float4* __restrict__ nq0,
     const float4* __restrict__ nq1, DevParams* P, float4* __restrict__ gout, unsigned* __restrict__ nbr,
     unsigned* __restrict__ nbr_cnt, unsigned cap, float skin, float* __restrict__ h0,
-    const uint2* __restrict__ groups, const unsigned* __restrict__ ngroups) {
+    const uint2* __restrict__ groups, const unsigned* __restrict__ ngroups, int stack_cap) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   WalkSmem<W>& S = *reinterpret_cast<WalkSmem<W>*>(smem_raw);
   const int w = threadIdx.x >> 5;
@@ -416,7 +416,7 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
       else S.p2f[w][nf + __popc(bfar & lt)] = e;
     }
     const int no = __popc(bo);
-    if (sp + 2 * no <= TW_STACK) {
+    if (sp + 2 * no <= stack_cap) {
       if (open) {
         const int r = sp + 2 * __popc(bo & lt);
         stack[r] = lc;
@@ -484,7 +484,7 @@ static void walk(const Dev& d, const Cfg& c, cudaStream_t s) {
   k_tree_walk<W, GRAV, QUAD, NBR, HILO, OUT><<<blocks, W * 32, smem, s>>>(
       d.body, st.pos_h, st.x, st.y, st.z, d.K, d.L, d.leaf_start, d.leaf_codes, d.segs, d.left, d.right, d.ncom,
       d.nbmin, d.nbmax, d.nq0, d.nq1, d.P, d.grav, d.nbr, d.nbr_cnt, d.nbr_cap, c.h_solve ? -1.0f : c.nbr_skin,
-      d.h0, d.groups, d.ngroups);
+      d.h0, d.groups, d.ngroups, c.walk_stack > 0 && c.walk_stack < TW_STACK ? c.walk_stack : TW_STACK);
 }
 
 // Gravity (group MAC) fused with the neighbour lists; the traversal tile (warps per block) is a tuning choice.

@@ -486,6 +486,7 @@ sph_status sph_create(const sph_config* cfg, uint32_t capacity, sph_ctx** out) {
   ctx->kc.h_eta = std::cbrt(3.0f * cfg->h_neighbours / (4.0f * 3.14159265358979f));
   ctx->kc.h_tol = cfg->h_tol;
   ctx->kc.h_iters = (int)cfg->h_iters;
+  ctx->kc.walk_stack = (int)std::min<uint32_t>(cfg->walk_stack, 1u << 20);
   ctx->kc.skin = ctx->kc.h_solve ? (cfg->h_skin > 0.0f ? cfg->h_skin : 0.05f) : 0.0f;
   ctx->kc.mac = (int)cfg->mac;
   ctx->kc.blk = cfg->block_threads ? (int)cfg->block_threads : 256;

@@ -194,6 +194,7 @@ struct Cfg {
   int walk_warps = 2;   // warps per block of the fused walk (2, 4 or 8)
   int learned = 0;      // smoothing lengths proposed by the MLP, checked, iterated only where rejected
   int divv = 0;         // the force pass also writes ∇·v (the learned proposal or its recording needs it)
+  int walk_stack = 0;   // traversal-stack limit of the walks (0: their full stacks); for testing the overflow path
 };
 
 // Grain contact constants (the reference's GpuStepParams subset used by the contact law and solve).

@@ -89,7 +89,12 @@ typedef struct sph_config {
   float h_skin;           /* SOLVE/LEARNED: neighbour lists are built at h·(1 + h_skin) and h moves at most that far
                              per rebuild, once the previous solve converged (residual <= 10·h_tol); after an
                              upload or an unconverged solve the skin is 0.15. 0 = 0.05 (at most 0.5) */
-  uint32_t reserved[2];
+  uint32_t walk_stack;    /* traversal-stack entries a walk may use (per warp in GROUP mode, 1,536 there; per
+                             particle in PARTICLE mode, 64 there as in bh_gravity.wgsl:336); 0 = all of them. A
+                             smaller limit is for testing the overflow path: children that do not fit are
+                             skipped and SPH_ERR_OVERFLOW is raised through sph_diag (the reference drops them
+                             silently, bh_gravity.wgsl:388-391) */
+  uint32_t reserved;
 } sph_config;
 
 /* Barnes-Hut acceptance. PARTICLE: each particle walks with the GPU reference's MAC

@@ -85,3 +85,29 @@ def verify_config(n: int = 300):
         mat[i] = m
         rho[i] = rho0
     return pos4, vel4, mass, mat, rho
+
+
+def splitmix_subsample(n_total: int, n: int, seed: int = 2) -> np.ndarray:
+    """n distinct indices of range(n_total), ascending, drawn by a partial Fisher-Yates shuffle whose random
+    numbers are the splitmix64 stream (bhtree.rs:197-203) started at `seed`."""
+    idx = np.arange(n_total, dtype=np.int64)
+    s = seed
+    for k in range(n):
+        s, u = splitmix(s)
+        j = k + min(int(u * (n_total - k)), n_total - k - 1)
+        idx[k], idx[j] = idx[j], idx[k]
+    return np.sort(idx[:n])
+
+
+def subsample_impact(I, n: int, seed: int = 2):
+    """A seeded n-particle subsample of a built impact as a self-consistent body: the chosen particles keep
+    their positions, velocities, u and materials; mass and smoothing length scale by N/n and (N/n)^(1/3) so the
+    density and the neighbour count stay those of the full impact (the softening scales with h).
+    Returns (particles, softening)."""
+    N = len(I.particles)
+    sel = splitmix_subsample(N, n, seed)
+    p = I.particles[sel].copy()
+    f = N / n
+    p["mass"] = (p["mass"].astype(np.float64) * f).astype(np.float32)
+    p["h"] = (p["h"].astype(np.float64) * f ** (1.0 / 3.0)).astype(np.float32)
+    return p, float(I.softening * f ** (1.0 / 3.0))

@@ -1,0 +1,195 @@
+"""The benchmark impact's method against the oracle on a 65,536-particle subsample of the 1,048,576-particle
+impact (indices drawn by splitmix64 from seed 2; mass and h rescaled so the density and the 64-neighbour count
+stay those of the full impact): Wendland C2, the smoothing-length solve (2 Newton iterations), θ = 0.6 with
+quadrupole moments, 16-particle leaves, the group walk, the 192-entry neighbour lists, all through the C ABI.
+
+Staged like the reference's gpu-bh-verify (tools/gpu-bh-verify/src/main.rs:461-568):
+* bit for bit: Morton codes, the (code, index) sort permutation, the Karras topology (index-extended split),
+  node COM / mass / AABB, each node's largest h and opening radius;
+* bit for bit: neighbour sets — the device's candidate lists (built with the solve's skin) filtered by the
+  reference predicate r < ½(h_i + h_j) (sph_step.wgsl:130-143) at the solved h equal the oracle's exact sets;
+* within stated tolerances: h after the solve (the oracle's f32 solve with the same iterations; a converged
+  device solve against the f64 Newton solve), density (sph_step.wgsl:120-149), forces and du/dt
+  (sph_step.wgsl:153-211), gravity against the FP64 direct sum;
+* the same neighbour / density / force checks again after KDK steps (rebuilds with the narrowed skin).
+"""
+import math
+
+import numpy as np
+import pytest
+
+import oracle
+from botheadstudios_b200 import workloads
+from botheadstudios_b200.gpusph import GpuSph
+from refcases import subsample_impact
+
+pytestmark = pytest.mark.gpu
+N_SUB = 65536
+WL = workloads.WORKLOADS["impact_1m"]
+KERNEL = 1  # Wendland C2
+
+
+@pytest.fixture(scope="module")
+def sub():
+    I = workloads.build(WL)
+    p, soft = subsample_impact(I, N_SUB, seed=2)
+    return I, p, soft
+
+
+def _cfg(I, **over):
+    return workloads.config(WL, I, **over)
+
+
+def _eta(cfg):
+    # the context's η, computed as the library computes it (f32)
+    return float(np.cbrt(np.float32(3.0) * np.float32(cfg["h_neighbours"]) / (np.float32(4.0) * np.float32(math.pi))))
+
+
+def _pos4(p, h):
+    return np.ascontiguousarray(np.concatenate([p["pos"], np.asarray(h, np.float32)[:, None]], axis=1),
+                                dtype=np.float32)
+
+
+def _exact_sets_from_lists(pos4, cnt, lst):
+    """The device's candidate lists filtered by the reference predicate in f32 (single-rounded, no FMA)."""
+    out = []
+    for i in range(len(pos4)):
+        c = lst[i, : cnt[i]].astype(np.int64)
+        d = pos4[c, :3] - pos4[i, :3]
+        r = np.sqrt((d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1]) + d[:, 2] * d[:, 2])
+        hij = np.float32(0.5) * (pos4[i, 3] + pos4[c, 3])
+        out.append(np.sort(c[r < hij]).astype(np.uint32))
+    return out
+
+
+def _node_w_fields(tp, h0, K, theta):
+    """Each node's largest h (bmin.w) and its opening radius size/θ + |centre − COM| (bmax.w, size = the
+    largest side), in f32 with the library's single-rounded operations."""
+    L = tp["L"]
+    nn = 2 * L - 1
+    hs = h0[tp["order"]].astype(np.float32)
+    hmax = np.zeros(nn, np.float32)
+    n = len(hs)
+    for c in range(L):
+        hmax[L - 1 + c] = hs[c * K: min((c + 1) * K, n)].max()
+    left, right = tp["left"], tp["right"]
+    # internal nodes: children have larger indices in no fixed order, so iterate a post-order
+    order, stack = [], [0]
+    while stack:
+        v = stack.pop()
+        if v < L - 1:
+            order.append(v)
+            stack.extend((int(left[v]), int(right[v])))
+    for v in reversed(order):
+        hmax[v] = max(hmax[left[v]], hmax[right[v]])
+    lo, hi, com = tp["bmin"][:, :3], tp["bmax"][:, :3], tp["com"][:, :3]
+    ext = hi - lo
+    size = np.maximum(np.maximum(ext[:, 0], ext[:, 1]), ext[:, 2])
+    cen = np.float32(0.5) * (lo + hi) - com
+    rc = size / np.float32(theta) + np.sqrt((cen[:, 0] * cen[:, 0] + cen[:, 1] * cen[:, 1]) + cen[:, 2] * cen[:, 2])
+    return hmax, rc.astype(np.float32)
+
+
+def _compare_sph(s, p_state, eos, tol_rho=2e-6, tol_acc=1e-4, tol_du=1e-3):
+    """Neighbour sets, density, EOS, SPH acceleration and du/dt of the context's last evaluation against the
+    oracle, at the state `p_state` (48-byte particles, original order) and the device's smoothing lengths."""
+    h = s.inspect("H")
+    pos4 = _pos4(p_state, h)
+    cnt, lst = s.inspect("NBR_COUNT"), s.inspect("NBR_LIST")
+    cap = int(s.config.max_neighbours)
+    assert cnt.max() <= cap, cnt.max()
+    got = _exact_sets_from_lists(pos4, cnt, lst)
+    want = oracle.neighbours32(pos4, cap=cap)
+    bad = [i for i in range(len(pos4)) if not np.array_equal(got[i], want[i])]
+    assert not bad, (len(bad), bad[:5])
+    mass = p_state["mass"]
+    rho = s.inspect("RHO")
+    rho_o = oracle.density32(pos4, mass, kernel=KERNEL)
+    assert np.max(np.abs(rho - rho_o) / rho_o) < tol_rho
+    P_o, c_o = oracle.eos32(eos, p_state["mat"], rho_o, p_state["u"])
+    vel4 = np.ascontiguousarray(np.concatenate([p_state["vel"], p_state["u"][:, None]], axis=1), dtype=np.float32)
+    f_o = oracle.sph_forces32(pos4, vel4, mass, rho_o, P_o, c_o, kernel=KERNEL)
+    acc = s.inspect("ACC_SPH")
+    da = acc[:, :3].astype(np.float64) - f_o[:, :3]
+    assert math.sqrt((da ** 2).sum() / (f_o[:, :3].astype(np.float64) ** 2).sum()) < tol_acc
+    du_scale = float((f_o[:, 3].astype(np.float64) ** 2).sum())
+    du = acc[:, 3].astype(np.float64) - f_o[:, 3]
+    if du_scale == 0.0:
+        assert np.all(acc[:, 3] == 0.0)  # no approaching pairs yet: no work term on either side
+    else:
+        assert math.sqrt((du ** 2).sum() / du_scale) < tol_du
+    return h
+
+
+def test_config2_subsample_tree_neighbours_density_forces(sub):
+    I, p, soft = sub
+    cfg = _cfg(I)
+    K, theta = cfg["leaf_size"], cfg["theta"]
+    n = len(p)
+    with GpuSph(n, **cfg) as s:
+        s.upload(p, I.eos, soft)
+        s.eval_forces()
+        d = s.diag()
+        assert d["overflow_flags"] == 0
+        # ---- tree: bit for bit against the oracle's staged pipeline on the uploaded (f32) positions --------
+        bodies = np.ascontiguousarray(np.concatenate([p["pos"], p["mass"][:, None]], axis=1), dtype=np.float32)
+        tp = oracle.tree_pipeline32(bodies, K=K, theta=theta, soft=soft, G=cfg["G"], exact_dups=True)
+        assert np.array_equal(s.inspect("CODES"), tp["sorted_codes"])
+        assert np.array_equal(s.inspect("ORDER"), tp["order"])
+        assert s.n_leaves() == tp["L"]
+        assert np.array_equal(s.inspect("LEFT"), tp["left"])
+        assert np.array_equal(s.inspect("RIGHT"), tp["right"])
+        assert np.array_equal(s.inspect("PARENT"), tp["parent"])
+        com, bmin, bmax = s.inspect("NODE_COM"), s.inspect("NODE_BMIN"), s.inspect("NODE_BMAX")
+        assert np.array_equal(com, tp["com"])
+        assert np.array_equal(bmin[:, :3], tp["bmin"][:, :3]) and np.array_equal(bmax[:, :3], tp["bmax"][:, :3])
+        hmax, rc = _node_w_fields(tp, p["h"], K, theta)
+        assert np.array_equal(bmin[:, 3], hmax)
+        assert np.array_equal(bmax[:, 3], rc)
+        # ---- the smoothing-length solve: the oracle's f32 solve with the same iterations and skin --------
+        h_dev = s.inspect("H")
+        h_o, rho_so, res_o = oracle.h_solve32(_pos4(p, p["h"]), p["mass"], _eta(cfg), 0.15, cfg["h_iters"],
+                                              kernel=KERNEL)
+        rel = np.abs(h_dev.astype(np.float64) / h_o - 1.0)
+        assert rel.max() < 1e-5, rel.max()
+        # the device's residual maximum is the oracle's at the device's h
+        assert d["h_residual"] == pytest.approx(float(res_o.max()), rel=1e-3)
+        # ---- neighbour sets, density, forces at the solved h ------------------------------------------
+        _compare_sph(s, p, I.eos)
+        # ---- gravity (θ = 0.6, quadrupoles) against the FP64 direct sum ---------------------------------
+        g = s.inspect("ACC_GRAV")[:, :3].astype(np.float64)
+        tg = np.random.default_rng(2).choice(n, 4096, replace=False)
+        ref = oracle.gravity_direct64(p["pos"].astype(np.float64), p["mass"].astype(np.float64), soft, cfg["G"],
+                                      targets=tg)
+        assert math.sqrt(((g[tg] - ref) ** 2).sum() / (ref ** 2).sum()) < 1e-3
+
+
+def test_config2_subsample_converged_solve_matches_f64_newton(sub):
+    """With enough iterations the device solve reaches the f64 Newton solution of ρ(h) = m(η/h)³ (the same
+    symmetric h_ij, step limits and skin box) everywhere."""
+    I, p, soft = sub
+    cfg = _cfg(I, h_iters=8)
+    with GpuSph(len(p), **cfg) as s:
+        s.upload(p, I.eos, soft)
+        s.eval_forces()
+        h_dev = s.inspect("H").astype(np.float64)
+    h64, _, res64, steps = oracle.h_solve64(p["pos"].astype(np.float64), p["h"].astype(np.float64),
+                                            p["mass"].astype(np.float64), _eta(cfg), 0.15, kernel=KERNEL)
+    assert steps <= 200
+    rel = np.abs(h_dev / h64 - 1.0)
+    assert rel.max() < 3e-4 and np.percentile(rel, 99) < 1e-5, (rel.max(), np.percentile(rel, 99))
+
+
+def test_config2_subsample_after_kdk_steps(sub):
+    """The rebuilds of a run (after the first solve the skin narrows): neighbour sets, density and forces
+    against the oracle at the state after the steps, re-evaluated in place."""
+    I, p, soft = sub
+    cfg = _cfg(I)
+    with GpuSph(len(p), **cfg) as s:
+        s.upload(p, I.eos, soft)
+        s.encode_kdk(3)
+        s.eval_forces()
+        st = s.readback()
+        d = s.diag()
+        assert d["overflow_flags"] == 0 and d["steps"] == 3
+        _compare_sph(s, st, I.eos)
