@@ -297,56 +297,138 @@ def plain_sequential(wl: dict, B, device: int, impacts: int = 16, steps: int = 2
 
 # ---------------------------------------------------------------------------------------------------------
 # CPU baseline: the reference's CPU path of record (HydroBody::step, hydrostatic.rs:345: f64, octree
-# Barnes-Hut θ = 0.5, hash-grid neighbours, two force evaluations per KDK step) restated in C++ and run with
-# OpenMP on all host cores, in the reference's own SI units, on a bounded sample of the same generator.
+# Barnes-Hut θ = 0.5, hash-grid neighbours, two force evaluations per KDK step) restated in C++, in the
+# reference's own SI units, on the benchmark's own initial conditions (the same seeded workload the GPU arm
+# runs). All host cores: OpenMP over the per-particle loops, full KDK steps. One core (the reference's own
+# path is single-threaded: no rayon in its Cargo.lock): one force evaluation at full size whose builds run in
+# full and whose per-particle loops run on every 64th block of 512 particles, scaled up.
 # ---------------------------------------------------------------------------------------------------------
-def cpu_reference_run(wl: dict, sample_n: int, steps: int, warmup: int, budget_s: float, nthreads: int = 0):
+CPU_STRIDE = 64
+
+
+def host_info() -> dict:
+    model = ""
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    try:
+        usable = len(os.sched_getaffinity(0))
+    except AttributeError:
+        usable = os.cpu_count()
+    return dict(nproc=usable, cpus=os.cpu_count(), model=model)
+
+
+def cpu_bodies(wl: dict, seed: int = 1, sample_impacts: int = 8):
+    """HydroBody handles on the workload's own initial conditions in SI units: the impact itself, or for a
+    batch its first `sample_impacts` impacts (a seeded sample, labelled as such). Returns (bodies, counts)."""
     import oracle
-    from botheadstudios_b200 import ic
     from botheadstudios_b200.materials import eos_table64, SI
-    from botheadstudios_b200.workloads import impactor_fraction
-    frac = impactor_fraction(wl)
-    n_imp = max(int(round(sample_n * frac)), 1)
-    I = ic.impact(sample_n - n_imp, n_imp, n_ngb=wl["n_ngb"], seed=2)
+    I = build_workload(wl, seed)
     U = I.units
-    p = I.particles
-    pos = I.pos64 * U.L
-    vel = p["vel"].astype(np.float64) * U.speed
-    mass = p["mass"].astype(np.float64) * U.M
-    u = p["u"].astype(np.float64) * U.energy
-    h = p["h"].astype(np.float64) * U.L
     kernel = 1 if wl["kernel"] == "wendland" else 0
-    nthreads = nthreads or oracle.max_threads()
-    hb = oracle.HydroBody(pos, vel, mass, u, h, p["mat"].astype(np.int32), eos_table64(SI), I.softening * U.L,
-                          G=6.674e-11, theta=0.5, kernel=kernel)
-    hb.compute_density(nthreads)
-    dt = hb.courant_dt(0.3)
-    for _ in range(warmup):
-        hb.step(dt, nthreads)
+    p_all = I.particles
+    if hasattr(I, "offsets"):
+        spans = [(int(I.offsets[k]), int(I.offsets[k + 1]), float(I.softening[k]))
+                 for k in range(min(sample_impacts, I.n_impacts))]
+        pos_all = p_all["pos"].astype(np.float64)
+    else:
+        spans = [(0, len(p_all), float(I.softening))]
+        pos_all = I.pos64
+    out, counts = [], []
+    for a, b, soft in spans:
+        p = p_all[a:b]
+        hb = oracle.HydroBody(pos_all[a:b] * U.L, p["vel"].astype(np.float64) * U.speed,
+                              p["mass"].astype(np.float64) * U.M, p["u"].astype(np.float64) * U.energy,
+                              p["h"].astype(np.float64) * U.L, p["mat"].astype(np.int32), eos_table64(SI),
+                              soft * U.L, G=6.674e-11, theta=0.5, kernel=kernel)
+        out.append(hb)
+        counts.append(b - a)
+    return out, counts
+
+
+def cpu_full_steps(bodies, counts, nthreads: int, max_steps: int, budget_s: float):
+    """Full KDK steps (HydroBody::step) at the Courant dt, all bodies per step, until max_steps or the budget
+    (at least one step). Returns particle-steps/s and the steps run."""
+    dts = []
+    for hb in bodies:
+        hb.compute_density(nthreads)
+        dts.append(hb.courant_dt(0.3))
     done, t0 = 0, time.perf_counter()
-    while done < steps:
-        hb.step(dt, nthreads)
+    while done < max(max_steps, 1):
+        for hb, dt in zip(bodies, dts):
+            hb.step(dt, nthreads)
         done += 1
         if time.perf_counter() - t0 > budget_s:
             break
     el = time.perf_counter() - t0
-    return dict(value=sample_n * done / el, steps_run=done, seconds=el, cores=nthreads, n=sample_n)
+    return dict(value=sum(counts) * done / el, steps_run=done, seconds=el)
+
+
+def cpu_single_thread(bodies, counts, stride: int = CPU_STRIDE):
+    """One core: a step is two force evaluations, each estimated from one sampled evaluation at full size."""
+    t_step = 0.0
+    for hb in bodies:
+        full, sampled = hb.eval_sampled(stride)
+        t_step += 2.0 * (full + stride * sampled)
+    return dict(value=sum(counts) / t_step, seconds_per_step=t_step)
+
+
+def cpu_sample_text(wl, counts, r, nthreads):
+    what = (f"the first {len(counts)} impacts ({sum(counts):,} particles) of the workload's seeded draw"
+            if wl.get("kind") == "batch" else f"the workload's own {sum(counts):,}-particle initial conditions")
+    return (f"HydroBody::step restated in C++ (f64, octree Barnes-Hut theta=0.5, hash-grid neighbours, 2 force "
+            f"evaluations per KDK step, SI units) on {what}: {r['steps_run']} full KDK step(s) in "
+            f"{r['seconds']:.1f} s on {nthreads} OpenMP threads")
+
+
+def cpu_baseline_leg(wl: dict, budget_s: float = 30.0, max_steps: int = 2) -> dict:
+    import oracle
+    bodies, counts = cpu_bodies(wl)
+    nthreads = oracle.max_threads()
+    r = cpu_full_steps(bodies, counts, nthreads, max_steps, budget_s)
+    one = cpu_single_thread(bodies, counts)
+    return dict(value=r["value"], unit=UNIT, cores=nthreads, kind="port",
+                sample=cpu_sample_text(wl, counts, r, nthreads),
+                single_thread=dict(value=one["value"], unit=UNIT, cores=1, kind="port",
+                                   sample=f"the reference's single-threaded loops (symmetric pair loops, per-particle "
+                                          f"octree walk) on the same state: grid/octree builds and the EOS at full "
+                                          f"size, per-particle loops on every {CPU_STRIDE}th block of 512 particles, "
+                                          f"scaled by {CPU_STRIDE}; {one['seconds_per_step']:.1f} s per step"),
+                host=host_info())
 
 
 def run_reference(args, wl, world, rank, local, pg):
+    """The reference arm: the CPU path of record on this configuration, full KDK steps on all host cores,
+    until --steps steps or 150 s (its warm-up is none: a CPU step needs no compilation or cache warm-up, and
+    one more 1M-particle step would cost tens of seconds). Rank 0 alone runs it."""
     if rank != 0:
         return
-    r = cpu_reference_run(wl, sample_n=65_536, steps=args.steps, warmup=min(args.warmup, 1), budget_s=150.0)
-    sample = (f"HydroBody::step (f64, octree BH θ=0.5, hash grid, 2 force evals/step) on a 65,536-particle impact "
-              f"from the same generator, {r['steps_run']} timed steps in {r['seconds']:.1f} s, "
-              f"{r['cores']} OpenMP threads, SI units")
+    import oracle
+    bodies, counts = cpu_bodies(wl)
+    nthreads = oracle.max_threads()
+    r = cpu_full_steps(bodies, counts, nthreads, args.steps, budget_s=150.0)
+    n = n_particles(wl)
     line = dict(metric=METRIC, value=r["value"], unit=UNIT, impl="reference", n_gpus=args.gpus, steps=args.steps,
-                warmup=args.warmup, ms_per_step=1000.0 * r["seconds"] / max(r["steps_run"], 1),
+                steps_run=r["steps_run"], warmup=args.warmup, warmup_run=0,
+                ms_per_step=1000.0 * r["seconds"] / max(r["steps_run"], 1),
                 higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f64", data="synthetic",
-                config=dict(workload=args.workload, particles=n_particles(wl)),
-                cpu_baseline=dict(value=r["value"], unit=UNIT, cores=r["cores"], kind="port", sample=sample),
+                config=bench_config(args, wl, n, world),
+                cpu_baseline=dict(value=r["value"], unit=UNIT, cores=nthreads, kind="port",
+                                  sample=cpu_sample_text(wl, counts, r, nthreads), host=host_info()),
                 e2e=dict(value=r["value"], unit=UNIT, h2d_bytes_per_step=0, d2h_bytes_per_step=0))
     print(json.dumps(line), flush=True)
+
+
+def bench_config(args, wl: dict, n: int, world: int) -> dict:
+    """The workload as both arms name it (the same dict in the GPU line and the reference line)."""
+    return dict(workload=args.workload, particles=n, impacts=wl.get("n_impacts", 1), kernel=wl["kernel"],
+                neighbours=wl["n_ngb"], theta=wl["theta"], quadrupole=bool(wl["quad"]), leaf=wl["leaf"],
+                h_mode=["fixed", "solve", "learned"][wl["h_solve"]], dt="adaptive CFL 0.3",
+                parallelism=f"replicas{world}", l2="working set > L2 (no flush needed)")
 
 
 def run_ours(args, wl, world, rank, local, pg):
@@ -475,21 +557,13 @@ def run_ours(args, wl, world, rank, local, pg):
     # ---- CPU baseline on the host cores (rank 0, N=1 only) ----
     cpu = None
     if world == 1 and not args.no_cpu:
-        r = cpu_reference_run(wl, sample_n=65_536, steps=1000, warmup=0, budget_s=15.0)  # ~15 s of CPU work
-        cpu = dict(value=r["value"], unit=UNIT, cores=r["cores"], kind="port",
-                   sample=f"HydroBody::step restated in C++ (f64, octree θ=0.5), 65,536-particle impact of the same "
-                          f"generator, {r['steps_run']} steps in {r['seconds']:.1f} s")
+        cpu = cpu_baseline_leg(wl)
     dd = d1[0]
     line = dict(metric=METRIC, value=value, unit=UNIT, n_gpus=world, steps=args.steps, warmup=args.warmup,
                 ms_per_step=ms_max / args.steps, higher_is_better=True, scaling="weak", vs_baseline=None,
                 dtype="f32", data="synthetic (seeded lattice impact)",
-                config=dict(workload=args.workload, particles=n, impacts=getattr(I, "n_impacts", 1),
-                            contexts=len(runner.ctxs),
-                            graph=bool(wl.get("graph", 0)), kernel=wl["kernel"], neighbours=wl["n_ngb"],
-                            theta=wl["theta"], quadrupole=bool(wl["quad"]), leaf=wl["leaf"],
-                            h_mode=["fixed", "solve", "learned"][wl["h_solve"]], dt="adaptive CFL 0.3",
-                            parallelism=f"replicas{world}",
-                            l2="working set > L2 (no flush needed)"),
+                config=bench_config(args, wl, n, world),
+                runner=dict(contexts=len(runner.ctxs), graph=bool(wl.get("graph", 0))),
                 e2e=dict(value=e2e_value, unit=UNIT, h2d_bytes_per_step=48 * n, d2h_bytes_per_step=48 * n,
                          steps=e2e_steps),
                 gpu_launches=launches, roofline=roof, roofline_hbm=roof_hbm, phases=phases, cpu_baseline=cpu,

@@ -81,3 +81,19 @@ def test_conservation_drifts_over_contexts():
     zero = [_diag(0.0, 0.0, 0.0, (0.0, 0.0, 0.0), (0.0, 0.0, 0.0))]
     assert bench.conservation_drifts(zero, zero) == dict(energy_drift=None, momentum_drift=None,
                                                          angular_momentum_drift=None)
+
+
+def test_cpu_legs_on_a_small_impact():
+    """The CPU baseline legs on a small impact of the benchmark's generator: full KDK steps on all cores, the
+    sampled single-thread estimate, the host record, and one config dict shared by both arms."""
+    import argparse
+    sys.path.insert(0, ROOT)
+    import bench
+    wl = dict(bench.WORKLOADS["impact_1m"], n_target=3000, n_impactor=300)
+    leg = bench.cpu_baseline_leg(wl, budget_s=5.0, max_steps=1)
+    assert leg["value"] > 0 and leg["single_thread"]["value"] > 0 and leg["single_thread"]["cores"] == 1
+    assert leg["cores"] >= 1 and leg["host"]["nproc"] >= 1
+    assert "3,300-particle" in leg["sample"]
+    args = argparse.Namespace(workload="impact_1m", gpus=1)
+    cfg = bench.bench_config(args, wl, 3300, 1)
+    assert cfg["particles"] == 3300 and cfg["workload"] == "impact_1m" and cfg["leaf"] == 16
