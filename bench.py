@@ -523,14 +523,21 @@ def run_ours(args, wl, world, rank, local, pg):
         traffic = json.load(open(tf)).get(args.workload, {}).get(dom)
     if dom == "gravity" and wl.get("quad") is not None:
         # The walk (group-MAC gravity fused with the neighbour lists) is FP32-pipe bound: algorithmic FLOPs
-        # from the device counters — 65 per quadrupole (20 per monopole) node interaction, 20 per pairwise
-        # interaction, 12 per node acceptance test — over its CUDA-event time. Peak: FP32 FMA throughput
-        # of 148 SMs × 128 lanes × 2 FLOP × the max SM clock (nominal; no measured FP32 peak exists here).
+        # from the device counters — 65 per quadrupole (20 per monopole) multipole evaluation at a particle,
+        # 20 per particle × source-particle pair (real sources only: the padding slots of partial leaves are
+        # reported beside it, not counted), 12 per node acceptance test, 180 (80 monopole) per node expanded
+        # about a group's centre and 60 per particle evaluating that expansion — over its CUDA-event time.
+        # Peak: FP32 FMA throughput of 148 SMs × 128 lanes × 2 FLOP × the max SM clock (nominal; no measured
+        # FP32 peak exists here).
         walks = max(phases["gravity"]["calls"], 1)
-        m2p = (dsum(d1, "m2p_interactions") - dsum(d0, "m2p_interactions")) / walks
-        p2p = (dsum(d1, "p2p_interactions") - dsum(d0, "p2p_interactions")) / walks
-        vis = (dsum(d1, "walk_nodes") - dsum(d0, "walk_nodes")) / walks
-        flops = (65.0 if wl["quad"] else 20.0) * m2p + 20.0 * p2p + 12.0 * vis
+
+        def per_walk(key):
+            return (dsum(d1, key) - dsum(d0, key)) / walks
+        m2p, p2p, vis = per_walk("m2p_interactions"), per_walk("p2p_interactions"), per_walk("walk_nodes")
+        m2l, slots = per_walk("local_expansions"), per_walk("p2p_slots")
+        quad = bool(wl["quad"])
+        flops = ((65.0 if quad else 20.0) * m2p + 20.0 * p2p + 12.0 * vis + (180.0 if quad else 80.0) * m2l +
+                 (60.0 * n_per_call if m2l > 0 else 0.0))
         clk_max = (clk.summary() or {}).get("sm_max_mhz") or 1965.0
         peak_tf = 148 * 128 * 2 * clk_max * 1e6 / 1e12
         achieved = flops / (dom_ms / 1000.0) / 1e12
@@ -539,7 +546,8 @@ def run_ours(args, wl, world, rank, local, pg):
                     peak_source="nominal FP32 FMA peak (148 SM x 128 lanes x 2 x max SM clock)",
                     flops_per_launch=flops, ms_per_launch=round(dom_ms, 4),
                     interactions_per_particle=dict(multipole=m2p / n_per_call, pairwise=p2p / n_per_call,
-                                                   nodes=vis / n_per_call))
+                                                   pairwise_slots=slots / n_per_call, nodes=vis / n_per_call,
+                                                   local_expansions_per_group=m2l / max(n_per_call / 32.0, 1.0)))
     else:
         dom_bytes = phase_bytes(dom, wl, lbar) * n_per_call
         achieved = dom_bytes / (dom_ms / 1000.0) / 1e9

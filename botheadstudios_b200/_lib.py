@@ -46,7 +46,7 @@ class SphConfig(C.Structure):
                 ("rho_floor", C.c_float), ("du_floor", C.c_float), ("r_min", C.c_float), ("sig_floor", C.c_float),
                 ("device", C.c_int32), ("mac", C.c_uint32), ("graph", C.c_uint32),
                 ("block_threads", C.c_uint32), ("walk_warps", C.c_uint32), ("h_skin", C.c_float),
-                ("walk_stack", C.c_uint32), ("reserved", C.c_uint32)]
+                ("walk_stack", C.c_uint32), ("local_theta", C.c_float)]
 
 
 class SphDiag(C.Structure):
@@ -55,7 +55,8 @@ class SphDiag(C.Structure):
                 ("dt", C.c_double), ("time", C.c_double), ("steps", C.c_uint32),
                 ("max_neighbours_seen", C.c_uint32), ("overflow_flags", C.c_uint32), ("h_iterations", C.c_uint32),
                 ("h_residual", C.c_float), ("h_accepted", C.c_uint32), ("walk_nodes", C.c_uint64),
-                ("walk_pops", C.c_uint64), ("m2p_interactions", C.c_uint64), ("p2p_interactions", C.c_uint64)]
+                ("walk_pops", C.c_uint64), ("m2p_interactions", C.c_uint64), ("p2p_interactions", C.c_uint64),
+                ("local_expansions", C.c_uint64), ("p2p_slots", C.c_uint64)]
 
 
 PHASES = ["sort", "tree", "gravity", "neighbours", "hsolve", "density", "forces", "integrate"]

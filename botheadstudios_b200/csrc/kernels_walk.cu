@@ -34,6 +34,7 @@ template <int W>
 struct WalkSmem {
   unsigned stack[W][TW_STACK];
   unsigned m2p[W][TW_LIST];
+  unsigned m2l[W][TW_LIST];   // accepted nodes far from the group: into the group's local expansion
   unsigned p2p[W][TW_LIST];   // near leaves: pairwise gravity + neighbour predicate
   unsigned p2f[W][TW_LIST];   // far leaves: pairwise gravity only
   float4 src[W][32];   // staged sources: x, y, z, m
@@ -67,6 +68,111 @@ struct Acc3 {
   }
 };
 
+// ---- the group's local expansion --------------------------------------------------------------------------
+// An accepted node far from the group (|COM − z| >= r_g/θ_L, z the centre of the group's box and r_g its
+// half-diagonal) does not go through a per-particle multipole evaluation: its potential is expanded about z,
+//   φ(z + y) ≈ φ0 + g·y + ½ yᵀH y + ⅙ T:yyy,   a(z + y) = −(g + H y + ½ T:yy),
+// with the monopole to third order and the quadrupole to second order in y (Cartesian Taylor coefficients of
+// the softened 1/R; R² = |u|² + ε², u = COM − z, e = u/R so that Q·e stays in f32 range in SI units). Each lane
+// expands a different node, the warp sums the 20 coefficients (lane k ends up holding coefficient k), and each
+// particle evaluates the expansion once. Coefficient order: φ0; g x, y, z; H xx, yy, zz, xy, xz, yz;
+// T xxx, yyy, zzz, xxy, xxz, xyy, yyz, xzz, yzz, xyz.
+constexpr int kLocal = 20;
+
+template <bool QUAD>
+__device__ __forceinline__ void local_coeffs(float4 c, float4 q0, float2 q1, float G, float zx, float zy, float zz,
+                                             float soft2, float v[32]) {
+  const float ux = c.x - zx, uy = c.y - zy, uz = c.z - zz;
+  const float iR = rsqrt_ftz(fmaf(ux, ux, fmaf(uy, uy, fmaf(uz, uz, soft2))));
+  const float ex = ux * iR, ey = uy * iR, ez = uz * iR;
+  const float s0 = G * c.w * iR, s1 = s0 * iR, s2 = s1 * iR, s3 = s2 * iR;
+  const float xx = ex * ex, yy = ey * ey, zz2 = ez * ez;
+  v[0] = -s0;
+  v[1] = -s1 * ex;
+  v[2] = -s1 * ey;
+  v[3] = -s1 * ez;
+  v[4] = -s2 * fmaf(3.0f, xx, -1.0f);
+  v[5] = -s2 * fmaf(3.0f, yy, -1.0f);
+  v[6] = -s2 * fmaf(3.0f, zz2, -1.0f);
+  const float m3s2 = -3.0f * s2;
+  v[7] = m3s2 * ex * ey;
+  v[8] = m3s2 * ex * ez;
+  v[9] = m3s2 * ey * ez;
+  const float ax = fmaf(-15.0f, xx, 3.0f), ay = fmaf(-15.0f, yy, 3.0f), az = fmaf(-15.0f, zz2, 3.0f);
+  v[10] = s3 * ex * (ax + 6.0f);
+  v[11] = s3 * ey * (ay + 6.0f);
+  v[12] = s3 * ez * (az + 6.0f);
+  v[13] = s3 * ey * ax;  // xxy
+  v[14] = s3 * ez * ax;  // xxz
+  v[15] = s3 * ex * ay;  // xyy
+  v[16] = s3 * ez * ay;  // yyz
+  v[17] = s3 * ex * az;  // xzz
+  v[18] = s3 * ey * az;  // yzz
+  v[19] = -15.0f * s3 * ex * ey * ez;
+  if (QUAD) {
+    // q = G·Q (traceless, about the COM): φ = −½ eQe/R³; g = (Qe − 5/2 eQe e)/R⁴;
+    // H = −(Q − 5(Qe eᵀ + e Qeᵀ) − 5/2 eQe I + 35/2 eQe e eᵀ)/R⁵
+    const float qxx = G * q0.x, qyy = G * q0.y, qzz = G * q0.z, qxy = G * q0.w, qxz = G * q1.x, qyz = G * q1.y;
+    const float Qx = fmaf(qxx, ex, fmaf(qxy, ey, qxz * ez));
+    const float Qy = fmaf(qxy, ex, fmaf(qyy, ey, qyz * ez));
+    const float Qz = fmaf(qxz, ex, fmaf(qyz, ey, qzz * ez));
+    const float eQe = fmaf(ex, Qx, fmaf(ey, Qy, ez * Qz));
+    const float iR2 = iR * iR, iR3 = iR2 * iR, iR4 = iR2 * iR2, iR5 = iR4 * iR;
+    v[0] = fmaf(-0.5f * eQe, iR3, v[0]);
+    const float k25 = 2.5f * eQe;
+    v[1] = fmaf(iR4, fmaf(-k25, ex, Qx), v[1]);
+    v[2] = fmaf(iR4, fmaf(-k25, ey, Qy), v[2]);
+    v[3] = fmaf(iR4, fmaf(-k25, ez, Qz), v[3]);
+    const float k175 = 17.5f * eQe;
+    v[4] = fmaf(-iR5, fmaf(k175, xx, fmaf(-10.0f * Qx, ex, qxx - k25)), v[4]);
+    v[5] = fmaf(-iR5, fmaf(k175, yy, fmaf(-10.0f * Qy, ey, qyy - k25)), v[5]);
+    v[6] = fmaf(-iR5, fmaf(k175, zz2, fmaf(-10.0f * Qz, ez, qzz - k25)), v[6]);
+    v[7] = fmaf(-iR5, fmaf(k175 * ex, ey, fmaf(-5.0f, fmaf(Qx, ey, Qy * ex), qxy)), v[7]);
+    v[8] = fmaf(-iR5, fmaf(k175 * ex, ez, fmaf(-5.0f, fmaf(Qx, ez, Qz * ex), qxz)), v[8]);
+    v[9] = fmaf(-iR5, fmaf(k175 * ey, ez, fmaf(-5.0f, fmaf(Qy, ez, Qz * ey), qyz)), v[9]);
+  }
+}
+
+// Sums v[0..31] over the warp in 31 shuffles: lane k returns the total of v[k] (recursive halving: at each
+// step a lane keeps the half of its values whose index bit matches its lane bit and adds its partner's copy).
+__device__ __forceinline__ float warp_transpose_sum32(float v[32]) {
+  const unsigned lane = threadIdx.x & 31u;
+#pragma unroll
+  for (int off = 16; off >= 1; off >>= 1) {
+    const bool up = (lane & (unsigned)off) != 0u;
+#pragma unroll
+    for (int k = 0; k < off; ++k) {
+      const float send = up ? v[k] : v[k + off];
+      const float keep = up ? v[k + off] : v[k];
+      v[k] = keep + __shfl_xor_sync(SPH_FULL_MASK, send, off);
+    }
+  }
+  return v[0];
+}
+
+// The expansion at offset y from its centre: a += −(g + H y + ½ T:yy), φ += φ0 + g·y + ½ yHy + ⅙ T:yyy.
+template <bool PHI>
+__device__ __forceinline__ void local_eval(const float cf[kLocal], float yx, float yy, float yz, float& ax,
+                                           float& ay, float& az, float& phi) {
+  const float hx = fmaf(cf[4], yx, fmaf(cf[7], yy, cf[8] * yz));
+  const float hy = fmaf(cf[7], yx, fmaf(cf[5], yy, cf[9] * yz));
+  const float hz = fmaf(cf[8], yx, fmaf(cf[9], yy, cf[6] * yz));
+  const float xx = 0.5f * yx * yx, yy2 = 0.5f * yy * yy, zz = 0.5f * yz * yz;
+  const float xy = yx * yy, xz = yx * yz, yz2 = yy * yz;
+  const float tx = fmaf(cf[10], xx, fmaf(cf[15], yy2, fmaf(cf[17], zz, fmaf(cf[13], xy, fmaf(cf[14], xz, cf[19] * yz2)))));
+  const float ty = fmaf(cf[13], xx, fmaf(cf[11], yy2, fmaf(cf[18], zz, fmaf(cf[15], xy, fmaf(cf[19], xz, cf[16] * yz2)))));
+  const float tz = fmaf(cf[14], xx, fmaf(cf[16], yy2, fmaf(cf[12], zz, fmaf(cf[19], xy, fmaf(cf[17], xz, cf[18] * yz2)))));
+  ax = -(cf[1] + hx + tx);
+  ay = -(cf[2] + hy + ty);
+  az = -(cf[3] + hz + tz);
+  if (PHI) {
+    // ⅙ T:yyy = ⅓ (y · (½ T:yy)), ½ yHy = ½ y·(H y)
+    const float third = 1.0f / 3.0f;
+    phi += cf[0] + fmaf(cf[1], yx, fmaf(cf[2], yy, cf[3] * yz)) + 0.5f * fmaf(yx, hx, fmaf(yy, hy, yz * hz)) +
+           third * fmaf(yx, tx, fmaf(yy, ty, yz * tz));
+  }
+}
+
 // What a gravity walk writes: the acceleration alone (a step's walk: the KDK integrator needs no potential),
 // the acceleration and the potential φ, or φ alone (into .w of the gravity record, for the energy diagnostic
 // of a state whose step walk left it out).
@@ -81,7 +187,7 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
     const float4* __restrict__ ncom, const float4* __restrict__ nbmin, const float4* __restrict__ nbmax, const float4* __restrict__ nq0,
     const float4* __restrict__ nq1, DevParams* P, float4* __restrict__ gout, unsigned* __restrict__ nbr,
     unsigned* __restrict__ nbr_cnt, unsigned cap, float skin, float* __restrict__ h0,
-    const uint2* __restrict__ groups, const unsigned* __restrict__ ngroups, int stack_cap) {
+    const uint2* __restrict__ groups, const unsigned* __restrict__ ngroups, int stack_cap, float local_theta) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   WalkSmem<W>& S = *reinterpret_cast<WalkSmem<W>*>(smem_raw);
   const int w = threadIdx.x >> 5;
@@ -132,7 +238,7 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
   unsigned cnt = 0;
   unsigned overflow = 0;
   unsigned* stack = S.stack[w];
-  unsigned long long st_visits = 0, st_pops = 0, st_m2p = 0, st_p2p = 0;
+  unsigned long long st_visits = 0, st_pops = 0, st_m2p = 0, st_p2p = 0, st_m2l = 0, st_slots = 0;
 
   for (int part = 0; part < nparts; ++part) {
   const bool valid = in_group && mypart == part;
@@ -142,7 +248,12 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
   const float gx1 = warp_max(valid ? pi.x : -big), gy1 = warp_max(valid ? pi.y : -big),
               gz1 = warp_max(valid ? pi.z : -big);
   const float ghmax = warp_max(valid ? pi.w : 0.0f);
-  int sp = 1, nm = 0, np = 0, nf = 0;
+  // the part's local expansion: centre z, and the distance beyond which an accepted node's COM joins it
+  const float zx = 0.5f * (gx0 + gx1), zy = 0.5f * (gy0 + gy1), zz = 0.5f * (gz0 + gz1);
+  const float rg2 = 0.25f * ((gx1 - gx0) * (gx1 - gx0) + (gy1 - gy0) * (gy1 - gy0) + (gz1 - gz0) * (gz1 - gz0));
+  const float far2 = (GRAV && local_theta > 0.0f) ? rg2 / (local_theta * local_theta) : big;
+  float loc = 0.0f;  // lane k < kLocal: coefficient k of the part's expansion
+  int sp = 1, nm = 0, np = 0, nf = 0, nl = 0;
   if (lane == 0) stack[0] = root;
   __syncwarp();
 
@@ -183,6 +294,28 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
         }
       }
       __syncwarp();
+    }
+  };
+
+  // ---- far multipoles: each lane expands its own node about z, the warp sums the coefficients -------------
+  auto flush_m2l = [&](int count) {
+    for (int base = 0; base < count; base += 32) {
+      float v[32];
+#pragma unroll
+      for (int k = 0; k < 32; ++k) v[k] = 0.0f;
+      if ((int)lane < count - base) {
+        const unsigned node = S.m2l[w][base + lane];
+        const float4 c = ncom[node];
+        float4 q0 = make_float4(0.f, 0.f, 0.f, 0.f);
+        float2 q1 = make_float2(0.f, 0.f);
+        if (QUAD) {
+          q0 = nq0[node];
+          const float4 b = nq1[node];
+          q1 = make_float2(b.x, b.y);
+        }
+        local_coeffs<QUAD>(c, q0, q1, G, zx, zy, zz, soft2, v);
+      }
+      loc += warp_transpose_sum32(v);
     }
   };
 
@@ -334,7 +467,7 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
   };
 
   const unsigned nvalid = __popc(__ballot_sync(SPH_FULL_MASK, valid));
-  unsigned long long part_m2p = 0, part_p2p = 0;
+  unsigned long long part_m2p = 0, part_p2p = 0, part_m2l = 0, part_src = 0;
   while (sp > 0) {
     const int take = min(sp, 32);
     sp -= take;
@@ -343,7 +476,7 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
     const bool have = (int)lane < take;
     const unsigned node = have ? stack[sp + lane] : 0u;
     __syncwarp();
-    bool acc_node = false, leaf = false, open = false, near_leaf = false;
+    bool acc_node = false, leaf = false, open = false, near_leaf = false, far_l = false;
     unsigned ls0 = 0u, ls1 = 1u;  // a leaf's source range, loaded alongside its box
     unsigned lc = 0u, rc = 0u;    // an internal node's children, loaded alongside its box (no second round trip)
     float4 lbl = make_float4(0.f, 0.f, 0.f, 0.f), lbh = lbl;  // the node's box (and max h), for the lane test
@@ -377,6 +510,8 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
         const float ddz = fmaxf(fmaxf(gz0 - c.z, c.z - gz1), 0.0f);
         const float dmin = sqrtf(ddx * ddx + ddy * ddy + ddz * ddz + soft2);
         mac = dmin >= bh.w * 1.00001f;
+        const float ux = c.x - zx, uy = c.y - zy, uz = c.z - zz;
+        far_l = ux * ux + uy * uy + uz * uz >= far2;
       }
       if (mac && !near) acc_node = true;
       else if (is_leaf) leaf = GRAV || near;
@@ -403,12 +538,16 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
       }
       if (near_leaf && !((keep >> lane) & 1u)) near_leaf = false;
     }
+    const bool acc_l = acc_node && far_l;
+    acc_node = acc_node && !far_l;
+    const unsigned bl = __ballot_sync(SPH_FULL_MASK, acc_l);
     const unsigned bm = __ballot_sync(SPH_FULL_MASK, acc_node);
     const unsigned bf = __ballot_sync(SPH_FULL_MASK, leaf);
     const unsigned bo = __ballot_sync(SPH_FULL_MASK, open);
     const unsigned bn = __ballot_sync(SPH_FULL_MASK, near_leaf);
     const unsigned bfar = bf & ~bn;
     if (acc_node) S.m2p[w][nm + __popc(bm & lt)] = node;
+    if (acc_l) S.m2l[w][nl + __popc(bl & lt)] = node;
     if (leaf) {
       // list entries carry the leaf's source range (capacity <= 2^26 particles, leaves <= 32 sources)
       const unsigned e = (ls0 << 5) | min(ls1 - ls0 - 1u, 31u);
@@ -427,14 +566,27 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
       overflow = 1;
     }
     nm += __popc(bm);
+    nl += __popc(bl);
     np += __popc(bn);
     nf += __popc(bfar);
     part_m2p += __popc(bm);
+    part_m2l += __popc(bl);
     part_p2p += __popc(bf);
+    {
+      // real source particles of this pop's leaves (the slots above include the padding of partial leaves)
+      unsigned srcs = leaf ? ls1 - ls0 : 0u;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) srcs += __shfl_xor_sync(SPH_FULL_MASK, srcs, o);
+      part_src += srcs;
+    }
     __syncwarp();
     if (nm > TW_LIST - 32) {
       flush_m2p(nm);
       nm = 0;
+    }
+    if (nl > TW_LIST - 32) {
+      flush_m2l(nl);
+      nl = 0;
     }
     if (np > TW_LIST - 32) {
       flush_p2p(np);
@@ -446,10 +598,26 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
     }
   }
   if (nm) flush_m2p(nm);
+  if (nl) flush_m2l(nl);
   if (np) flush_p2p(np);
   if (nf) flush_far(nf);
+  if (GRAV && part_m2l) {
+    // the part's expansion (lane k holds coefficient k) evaluated by every particle of the part
+    float cf[kLocal];
+#pragma unroll
+    for (int k = 0; k < kLocal; ++k) cf[k] = __shfl_sync(SPH_FULL_MASK, loc, k);
+    if (valid) {
+      float yx = pi.x - zx, yy = pi.y - zy, yz = pi.z - zz;
+      if (HILO) { yx += xlo; yy += ylo; yz += zlo; }
+      float lx, ly, lz;
+      local_eval<OUT != kWalkAcc>(cf, yx, yy, yz, lx, ly, lz, phi);
+      acc.add<HILO>(lx, ly, lz);
+    }
+  }
   st_m2p += part_m2p * nvalid;                             // node × particle interactions
-  st_p2p += part_p2p * (unsigned long long)K * nvalid;     // leaf sources × particles (upper bound)
+  st_m2l += part_m2l;                                      // nodes expanded about a part's centre
+  st_p2p += part_src * nvalid;                             // source particles × particles
+  st_slots += part_p2p * (unsigned long long)K * nvalid;   // ... counting every leaf as K sources
   }  // parts
 
   if (in_group && GRAV) {
@@ -470,6 +638,8 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
     atomicAdd(&P->stat_pops, st_pops);
     atomicAdd(&P->stat_m2p, st_m2p);
     atomicAdd(&P->stat_p2p, st_p2p);
+    atomicAdd(&P->stat_m2l, st_m2l);
+    atomicAdd(&P->stat_p2p_slots, st_slots);
   }
 }
 
@@ -484,7 +654,8 @@ static void walk(const Dev& d, const Cfg& c, cudaStream_t s) {
   k_tree_walk<W, GRAV, QUAD, NBR, HILO, OUT><<<blocks, W * 32, smem, s>>>(
       d.body, st.pos_h, st.x, st.y, st.z, d.K, d.L, d.leaf_start, d.leaf_codes, d.segs, d.left, d.right, d.ncom,
       d.nbmin, d.nbmax, d.nq0, d.nq1, d.P, d.grav, d.nbr, d.nbr_cnt, d.nbr_cap, c.h_solve ? -1.0f : c.nbr_skin,
-      d.h0, d.groups, d.ngroups, c.walk_stack > 0 && c.walk_stack < TW_STACK ? c.walk_stack : TW_STACK);
+      d.h0, d.groups, d.ngroups, c.walk_stack > 0 && c.walk_stack < TW_STACK ? c.walk_stack : TW_STACK,
+      GRAV ? c.local_theta : 0.0f);
 }
 
 // Gravity (group MAC) fused with the neighbour lists; the traversal tile (warps per block) is a tuning choice.

@@ -249,6 +249,7 @@ extern "C" sph_status sph_gravity_tree_noalloc(const void* d_bodies4, uint32_t n
   Cfg c;
   c.quad = (int)multipole;
   c.mac = SPH_MAC_GROUP;
+  c.local_theta = kLocalThetaDefault;  // the walk sph_gravity runs with the default configuration
   k_noalloc_params<<<1, 1, 0, s>>>(d.P, (float)G, theta);
   k_noalloc_load<<<(n + 255) / 256, 256, 0, s>>>(static_cast<const float4*>(d_bodies4), (int)n, d.st[0]);
   launch_segments_single(d, softening * softening, 0.0, s);

@@ -458,6 +458,7 @@ sph_status sph_config_default(sph_config* cfg) {
   cfg->r_min = 1.0e-9f;
   cfg->sig_floor = 1.0f;
   cfg->device = -1;
+  cfg->local_theta = kLocalThetaDefault;
   return SPH_OK;
 }
 
@@ -469,7 +470,7 @@ sph_status sph_create(const sph_config* cfg, uint32_t capacity, sph_ctx** out) {
       cfg->max_neighbours > 4096 || capacity > (1u << 26) || cfg->mac > 1 ||
       (cfg->block_threads != 0 && (cfg->block_threads < 64 || cfg->block_threads > 1024 || cfg->block_threads % 32)) ||
       (cfg->walk_warps != 0 && cfg->walk_warps != 2 && cfg->walk_warps != 4 && cfg->walk_warps != 8) ||
-      !(cfg->h_skin >= 0.0f && cfg->h_skin <= 0.5f) ||
+      !(cfg->h_skin >= 0.0f && cfg->h_skin <= 0.5f) || !(cfg->local_theta >= 0.0f && cfg->local_theta < 1.0f) ||
       (cfg->mac == SPH_MAC_GROUP && (cfg->leaf_size & (cfg->leaf_size - 1)) != 0))
     return SPH_ERR_INVALID;
   sph_ctx* ctx = new (std::nothrow) sph_ctx();
@@ -487,6 +488,7 @@ sph_status sph_create(const sph_config* cfg, uint32_t capacity, sph_ctx** out) {
   ctx->kc.h_tol = cfg->h_tol;
   ctx->kc.h_iters = (int)cfg->h_iters;
   ctx->kc.walk_stack = (int)std::min<uint32_t>(cfg->walk_stack, 1u << 20);
+  ctx->kc.local_theta = cfg->local_theta;
   ctx->kc.skin = ctx->kc.h_solve ? (cfg->h_skin > 0.0f ? cfg->h_skin : 0.05f) : 0.0f;
   ctx->kc.mac = (int)cfg->mac;
   ctx->kc.blk = cfg->block_threads ? (int)cfg->block_threads : 256;
@@ -944,6 +946,8 @@ sph_status sph_diag(sph_ctx* ctx, sph_diag_out* out) {
   out->walk_pops = p.stat_pops;
   out->m2p_interactions = p.stat_m2p;
   out->p2p_interactions = p.stat_p2p;
+  out->local_expansions = p.stat_m2l;
+  out->p2p_slots = p.stat_p2p_slots;
   if (p.flags & (kFlagNbrOverflow | kFlagStackOverflow)) {
     ctx->err = "device capacity overflow (flags " + std::to_string(p.flags) + ")";
     return SPH_ERR_OVERFLOW;

@@ -46,8 +46,10 @@ struct DevParams {
   unsigned h_accepted;    // learned h: particles whose proposal passed the first residual check (last solve)
   unsigned pad;
   // walk statistics, accumulated once per warp: node visits, 32-wide pops, multipole and pairwise
-  // interactions (particle × source pairs)
+  // interactions (particle × node, particle × source particle)
   unsigned long long stat_visits, stat_pops, stat_m2p, stat_p2p;
+  unsigned long long stat_m2l;        // accepted nodes taken into a group's local expansion (per node and part)
+  unsigned long long stat_p2p_slots;  // pairwise slots evaluated: every leaf counted as leaf_size sources
 };
 
 // ---- approximate reciprocal square root, reciprocal and division on the special-function unit alone ------

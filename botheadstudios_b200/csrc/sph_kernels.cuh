@@ -178,6 +178,9 @@ struct Dev {
   const State& s() const { return st[cur]; }
 };
 
+// The group walk's local-expansion opening parameter (r_group / distance) that sph_config_default sets.
+constexpr float kLocalThetaDefault = 0.0f;
+
 struct Cfg {
   int kernel = 0;       // 0 cubic, 1 Wendland C2
   int gravity = 0;      // 0 tree, 1 direct, 2 none
@@ -195,6 +198,7 @@ struct Cfg {
   int learned = 0;      // smoothing lengths proposed by the MLP, checked, iterated only where rejected
   int divv = 0;         // the force pass also writes ∇·v (the learned proposal or its recording needs it)
   int walk_stack = 0;   // traversal-stack limit of the walks (0: their full stacks); for testing the overflow path
+  float local_theta = 0.0f;  // group walk: accepted nodes beyond r_group/local_theta join the local expansion
 };
 
 // Grain contact constants (the reference's GpuStepParams subset used by the contact law and solve).

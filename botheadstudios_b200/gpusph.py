@@ -222,7 +222,8 @@ class GpuSph:
                     h_iterations=d.h_iterations, h_residual=d.h_residual, h_accepted=d.h_accepted,
                     walk_nodes=d.walk_nodes,
                     walk_pops=d.walk_pops, m2p_interactions=d.m2p_interactions,
-                    p2p_interactions=d.p2p_interactions, status=st)
+                    p2p_interactions=d.p2p_interactions, local_expansions=d.local_expansions,
+                    p2p_slots=d.p2p_slots, status=st)
 
     # ---- profiling ------------------------------------------------------------------------------------
     def profile_enable(self, on: bool = True):

@@ -18,6 +18,8 @@ def main():
     ap.add_argument("--steps", type=int, default=1)
     ap.add_argument("--mac", type=int, default=0)
     ap.add_argument("--theta", type=float, default=None)
+    ap.add_argument("--local-theta", type=float, default=None,
+                    help="group walk: the local expansion's opening parameter (0 = off; default: the library's)")
     ap.add_argument("--precision", type=int, default=0, help="1 = node-relative hi/lo + compensated sums")
     ap.add_argument("--leaf", type=int, default=None, help="LBVH leaf size (default: the workload's)")
     ap.add_argument("--walk-warps", type=int, default=0, help="warps per walk block (2, 4, 8; 0 = 4)")
@@ -35,6 +37,8 @@ def main():
         over["gravity"] = args.gravity
     if args.theta is not None:
         over["theta"] = args.theta
+    if args.local_theta is not None:
+        over["local_theta"] = args.local_theta
     acc_err = None
     with workloads.solver(wl, I, **over) as s:
         workloads.upload(s, I)
@@ -59,7 +63,8 @@ def main():
                            global_rms=float(np.sqrt(((g[tg] - ref) ** 2).sum() / (ref ** 2).sum())))
     n = len(I.particles)
     walks = max(prof["calls"]["gravity"], prof["calls"]["neighbours"], 1)
-    stats = {k: (d1[k] - d0[k]) / walks for k in ("walk_nodes", "walk_pops", "m2p_interactions", "p2p_interactions")}
+    stats = {k: (d1[k] - d0[k]) / walks for k in ("walk_nodes", "walk_pops", "m2p_interactions", "p2p_interactions",
+                                                "local_expansions", "p2p_slots")}
     print(json.dumps(dict(workload=args.workload, particles=n, steps=args.steps, config=over, phases_ms=prof["ms"],
                           calls=prof["calls"], launches=prof["kernel_launches"], per_walk=stats,
                           per_particle={k: v / n for k, v in stats.items()}, gravity_error=acc_err)))

@@ -94,7 +94,10 @@ typedef struct sph_config {
                              smaller limit is for testing the overflow path: children that do not fit are
                              skipped and SPH_ERR_OVERFLOW is raised through sph_diag (the reference drops them
                              silently, bh_gravity.wgsl:388-391) */
-  uint32_t reserved;
+  float local_theta;      /* GROUP mode: an accepted node whose COM lies beyond r_g/local_theta of the group's
+                             box centre (r_g: the box's half-diagonal) is not evaluated per particle but expanded
+                             once about the centre (monopole to third, quadrupole to second order in the offset)
+                             and the expansion is evaluated per particle; 0 = every accepted node per particle */
 } sph_config;
 
 /* Barnes-Hut acceptance. PARTICLE: each particle walks with the GPU reference's MAC
@@ -128,9 +131,13 @@ typedef struct sph_diag_out {
   float h_residual;                      /* SOLVE: max relative density residual after the last solve */
   uint32_t h_accepted;                   /* LEARNED: particles whose proposed h passed the first check (last
                                             solve) */
-  /* cumulative tree-walk counters (group MAC): nodes visited, 32-wide pops, particle × multipole and
-   * particle × leaf-source interactions (the latter counts every source of a visited leaf) */
+  /* cumulative tree-walk counters of the steps' walks (GROUP mode): nodes visited, 32-wide pops,
+   * particle × multipole and particle × source-particle interactions */
   uint64_t walk_nodes, walk_pops, m2p_interactions, p2p_interactions;
+  uint64_t local_expansions;             /* accepted nodes expanded about a group's centre (one per node and
+                                            group part) */
+  uint64_t p2p_slots;                    /* pairwise slots the lanes ran: p2p_interactions with every leaf
+                                            counted as leaf_size sources (the padding of partial leaves) */
 } sph_diag_out;
 
 typedef struct sph_ctx sph_ctx;

@@ -59,7 +59,7 @@ int main(void) {
          offsetof(SphParticle48, prov));
   printf("%zu %zu %zu %zu %zu %zu\n", offsetof(sph_config, theta), offsetof(sph_config, max_neighbours),
          offsetof(sph_config, cfl), offsetof(sph_config, sig_floor), offsetof(sph_config, walk_stack),
-         offsetof(sph_config, reserved));
+         offsetof(sph_config, local_theta));
   printf("%zu %zu %zu\n", offsetof(sph_diag_out, dt), offsetof(sph_diag_out, steps),
          offsetof(sph_diag_out, h_residual));
   return 0;
@@ -77,7 +77,7 @@ int main(void) {
     assert list(map(int, lines[1].split())) == [p.fields[k][1] for k in ("h", "vel", "u", "mat", "rho", "prov")]
     sc = _lib.SphConfig
     assert list(map(int, lines[2].split())) == [sc.theta.offset, sc.max_neighbours.offset, sc.cfl.offset,
-                                                sc.sig_floor.offset, sc.walk_stack.offset, sc.reserved.offset]
+                                                sc.sig_floor.offset, sc.walk_stack.offset, sc.local_theta.offset]
     sd = _lib.SphDiag
     assert list(map(int, lines[3].split())) == [sd.dt.offset, sd.steps.offset, sd.h_residual.offset]
 
