@@ -90,9 +90,11 @@ def _node_w_fields(tp, h0, K, theta):
     return hmax, rc.astype(np.float32)
 
 
-def _compare_sph(s, p_state, eos, tol_rho=2e-6, tol_acc=1e-4, tol_du=1e-3):
+def _compare_sph(s, p_state, I, tol_rho=2e-6, tol_acc=1e-4, tol_du=1e-3):
     """Neighbour sets, density, EOS, SPH acceleration and du/dt of the context's last evaluation against the
-    oracle, at the state `p_state` (48-byte particles, original order) and the device's smoothing lengths."""
+    oracle, at the state `p_state` (48-byte particles, original order) and the device's smoothing lengths, with
+    the unit system's guards (density floor, sound-speed step floor, coincident-pair cut) on both sides."""
+    u = I.units
     h = s.inspect("H")
     pos4 = _pos4(p_state, h)
     cnt, lst = s.inspect("NBR_COUNT"), s.inspect("NBR_LIST")
@@ -106,9 +108,10 @@ def _compare_sph(s, p_state, eos, tol_rho=2e-6, tol_acc=1e-4, tol_du=1e-3):
     rho = s.inspect("RHO")
     rho_o = oracle.density32(pos4, mass, kernel=KERNEL)
     assert np.max(np.abs(rho - rho_o) / rho_o) < tol_rho
-    P_o, c_o = oracle.eos32(eos, p_state["mat"], rho_o, p_state["u"])
+    P_o, c_o = oracle.eos32(I.eos, p_state["mat"], rho_o, p_state["u"], du_floor=u.du_floor, rho_floor=u.rho_floor)
+    assert np.max(np.abs(s.inspect("SOUND") - c_o) / c_o) < 2e-3
     vel4 = np.ascontiguousarray(np.concatenate([p_state["vel"], p_state["u"][:, None]], axis=1), dtype=np.float32)
-    f_o = oracle.sph_forces32(pos4, vel4, mass, rho_o, P_o, c_o, kernel=KERNEL)
+    f_o = oracle.sph_forces32(pos4, vel4, mass, rho_o, P_o, c_o, r_min=u.r_min, kernel=KERNEL)
     acc = s.inspect("ACC_SPH")
     da = acc[:, :3].astype(np.float64) - f_o[:, :3]
     assert math.sqrt((da ** 2).sum() / (f_o[:, :3].astype(np.float64) ** 2).sum()) < tol_acc
@@ -155,7 +158,7 @@ def test_config2_subsample_tree_neighbours_density_forces(sub):
         # the device's residual maximum is the oracle's at the device's h
         assert d["h_residual"] == pytest.approx(float(res_o.max()), rel=1e-3)
         # ---- neighbour sets, density, forces at the solved h ------------------------------------------
-        _compare_sph(s, p, I.eos)
+        _compare_sph(s, p, I)
         # ---- gravity (θ = 0.6, quadrupoles) against the FP64 direct sum ---------------------------------
         g = s.inspect("ACC_GRAV")[:, :3].astype(np.float64)
         tg = np.random.default_rng(2).choice(n, 4096, replace=False)
@@ -192,4 +195,4 @@ def test_config2_subsample_after_kdk_steps(sub):
         st = s.readback()
         d = s.diag()
         assert d["overflow_flags"] == 0 and d["steps"] == 3
-        _compare_sph(s, st, I.eos)
+        _compare_sph(s, st, I)
