@@ -179,7 +179,9 @@ struct Dev {
 };
 
 // The group walk's local-expansion opening parameter (r_group / distance) that sph_config_default sets.
-constexpr float kLocalThetaDefault = 0.0f;
+// Measured on the 1M impact (θ = 0.6, quadrupoles): 0.3 cuts the walk 12 % and moves the gravity error against
+// FP64 direct sums from 3.8e-4 to 4.8e-4 RMS.
+constexpr float kLocalThetaDefault = 0.3f;
 
 struct Cfg {
   int kernel = 0;       // 0 cubic, 1 Wendland C2

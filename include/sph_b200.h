@@ -97,7 +97,8 @@ typedef struct sph_config {
   float local_theta;      /* GROUP mode: an accepted node whose COM lies beyond r_g/local_theta of the group's
                              box centre (r_g: the box's half-diagonal) is not evaluated per particle but expanded
                              once about the centre (monopole to third, quadrupole to second order in the offset)
-                             and the expansion is evaluated per particle; 0 = every accepted node per particle */
+                             and the expansion is evaluated per particle; 0 = every accepted node per particle.
+                             sph_config_default: 0.3 */
 } sph_config;
 
 /* Barnes-Hut acceptance. PARTICLE: each particle walks with the GPU reference's MAC
