@@ -460,7 +460,9 @@ __global__ void k_leaf_climb(const float4* __restrict__ body, const float4* __re
                              const unsigned* __restrict__ leaf_start, int L, const unsigned* __restrict__ left, const unsigned* __restrict__ right,
                              const unsigned* __restrict__ parent, unsigned* __restrict__ counters,
                              float4* __restrict__ ncom, float4* __restrict__ nbmin, float4* __restrict__ nbmax,
-                             float4* __restrict__ nq0, float4* __restrict__ nq1, float theta, int side_mac) {
+                             float4* __restrict__ nq0, float4* __restrict__ nq1, float theta, int side_mac,
+                             int half, float4* __restrict__ hcom, float4* __restrict__ hq0,
+                             float2* __restrict__ hq1, float2* __restrict__ hrc) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= L) return;
   const int li = L - 1 + c;
@@ -488,6 +490,52 @@ __global__ void k_leaf_climb(const float4* __restrict__ body, const float4* __re
     ncom[li] = com;
     nbmin[li] = make_float4(lo[0], lo[1], lo[2], hmax);
     nbmax[li] = make_float4(hi[0], hi[1], hi[2], rc);
+  }
+  if (half > 0) {
+    // the leaf's two halves as multipoles of their own (the far field of the group walk): COM, mass, the
+    // traceless quadrupole about that COM, and the opening radius largest side/θ + |centre − COM|
+    float rcs[2] = {0.0f, 0.0f};
+    for (int b = 0; b < 2; ++b) {
+      const int a0 = s0 + b * half, a1 = min(s0 + (b + 1) * half, s1);
+      float hm = 0.0f, hx = 0.0f, hy = 0.0f, hz = 0.0f;
+      float l3[3] = {1.0e30f, 1.0e30f, 1.0e30f}, u3[3] = {-1.0e30f, -1.0e30f, -1.0e30f};
+      for (int s = a0; s < a1; ++s) {
+        const float4 q = body[s];
+        hm += q.w;
+        hx = fmaf(q.x, q.w, hx);
+        hy = fmaf(q.y, q.w, hy);
+        hz = fmaf(q.z, q.w, hz);
+        l3[0] = fminf(l3[0], q.x); l3[1] = fminf(l3[1], q.y); l3[2] = fminf(l3[2], q.z);
+        u3[0] = fmaxf(u3[0], q.x); u3[1] = fmaxf(u3[1], q.y); u3[2] = fmaxf(u3[2], q.z);
+      }
+      const float inv = hm > 0.0f ? 1.0f / hm : 0.0f;
+      const float4 hc = make_float4(hx * inv, hy * inv, hz * inv, hm);
+      if (a1 > a0) {
+        const float ex = u3[0] - l3[0], ey = u3[1] - l3[1], ez = u3[2] - l3[2];
+        const float size = fmaxf(fmaxf(ex, ey), ez);
+        const float cx = 0.5f * (l3[0] + u3[0]) - hc.x, cy = 0.5f * (l3[1] + u3[1]) - hc.y,
+                    cz = 0.5f * (l3[2] + u3[2]) - hc.z;
+        rcs[b] = size / theta + sqrtf(cx * cx + cy * cy + cz * cz);
+      }
+      float qxx = 0, qyy = 0, qzz = 0, qxy = 0, qxz = 0, qyz = 0;
+      if (QUAD) {
+        for (int s = a0; s < a1; ++s) {
+          const float4 q = body[s];
+          const float dx = q.x - hc.x, dy = q.y - hc.y, dz = q.z - hc.z;
+          const float r2 = dx * dx + dy * dy + dz * dz;
+          qxx += q.w * (3.0f * dx * dx - r2);
+          qyy += q.w * (3.0f * dy * dy - r2);
+          qzz += q.w * (3.0f * dz * dz - r2);
+          qxy += q.w * 3.0f * dx * dy;
+          qxz += q.w * 3.0f * dx * dz;
+          qyz += q.w * 3.0f * dy * dz;
+        }
+      }
+      hcom[2 * c + b] = hc;
+      hq0[2 * c + b] = make_float4(qxx, qyy, qzz, qxy);
+      hq1[2 * c + b] = make_float2(qxz, qyz);
+    }
+    hrc[c] = make_float2(rcs[0], rcs[1]);
   }
   if (QUAD) {
     float qxx = 0, qyy = 0, qzz = 0, qxy = 0, qxz = 0, qyz = 0;
@@ -566,15 +614,22 @@ int launch_tree(const Dev& d, const Cfg& c, float theta, cudaStream_t s) {
   k_run_groups<<<(L + 255) / 256, 256, 0, s>>>(d.segs, d.nseg, 32 / d.K, L, d.groups);
   const State& st = d.s();
   const int side_mac = c.mac == 0 ? 1 : 0;
+  const int half = half_leaf(d, c);
   if (c.quad)
     k_leaf_climb<true><<<(L + 127) / 128, 128, 0, s>>>(d.body, st.pos_h, d.leaf_start, L, d.left, d.right, d.parent,
                                                        d.counters, d.ncom, d.nbmin, d.nbmax, d.nq0, d.nq1, theta,
-                                                       side_mac);
+                                                       side_mac, half, d.hcom, d.hq0, d.hq1, d.hrc);
   else
     k_leaf_climb<false><<<(L + 127) / 128, 128, 0, s>>>(d.body, st.pos_h, d.leaf_start, L, d.left, d.right, d.parent,
                                                         d.counters, d.ncom, d.nbmin, d.nbmax, d.nq0, d.nq1, theta,
-                                                        side_mac);
+                                                        side_mac, half, d.hcom, d.hq0, d.hq1, d.hrc);
   return 2;
+}
+
+// Far leaves are split in the group walk when a half holds at least 8 particles: one quadrupole evaluation
+// (~50 instructions) then replaces 8 pairwise ones (~14 each); halves of 4 would not pay.
+int half_leaf(const Dev& d, const Cfg& c) {
+  return (c.mac == 0 && c.gravity == 0 && d.K >= 16 && d.hcom) ? d.K / 2 : 0;
 }
 
 }  // namespace sphb

@@ -26,7 +26,7 @@
 namespace sphb {
 
 constexpr int TW_STACK = 1536;  // per-warp node stack
-constexpr int TW_LIST = 64;     // per-warp list capacity (flushed once half full)
+constexpr int TW_LIST = 96;     // per-warp list capacity (a pop adds <= 64 entries; flushed above 32)
 constexpr int TW_WARPS_PER_SM = 24;  // resident walk warps per SM (80 registers, ~8.4 KB shared each)
 
 // Per-block shared memory of a W-warp walk block (the traversal tile: W groups of 32 particles).
@@ -187,7 +187,9 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
     const float4* __restrict__ ncom, const float4* __restrict__ nbmin, const float4* __restrict__ nbmax, const float4* __restrict__ nq0,
     const float4* __restrict__ nq1, DevParams* P, float4* __restrict__ gout, unsigned* __restrict__ nbr,
     unsigned* __restrict__ nbr_cnt, unsigned cap, float skin, float* __restrict__ h0,
-    const uint2* __restrict__ groups, const unsigned* __restrict__ ngroups, int stack_cap, float local_theta) {
+    const uint2* __restrict__ groups, const unsigned* __restrict__ ngroups, int stack_cap, float local_theta,
+    int half, const float4* __restrict__ hcom, const float4* __restrict__ hq0, const float2* __restrict__ hq1,
+    const float2* __restrict__ hrc) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   WalkSmem<W>& S = *reinterpret_cast<WalkSmem<W>*>(smem_raw);
   const int w = threadIdx.x >> 5;
@@ -260,9 +262,11 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
   // ---- far leaves: branch-free pairwise gravity, 32 staged sources per pass ---------------------------
   // The next chunk's sources are loaded into registers before this chunk is evaluated, so the gather
   // overlaps the arithmetic.
+  // far entries hold at most KF sources: half leaves when far leaves are split, whole leaves otherwise
+  const int KF = half > 0 ? half : K;
   auto far_source = [&](int base, int count) {
-    const int per = 32 / K;
-    const int li = lane / K, off = lane % K;
+    const int per = 32 / KF;
+    const int li = lane / KF, off = lane % KF;
     float4 src = make_float4(3.0e18f, 3.0e18f, 3.0e18f, 0.0f);  // padding: massless and far away
     if (li < min(per, count - base)) {
       const unsigned e = S.p2f[w][base + li];  // first source << 5 | (sources − 1)
@@ -271,7 +275,7 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
     return src;
   };
   auto flush_far = [&](int count) {
-    const int per = 32 / K;
+    const int per = 32 / KF;
     float4 nxt = far_source(0, count);
     for (int base = 0; base < count; base += per) {
       float4 src = nxt;
@@ -297,6 +301,27 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
     }
   };
 
+  // A multipole-list entry: a node index, or a half leaf (bit 31 set, index 2·leaf + half).
+  auto load_multipole = [&](unsigned e, float4& c, float4& q0, float2& q1) {
+    q0 = make_float4(0.f, 0.f, 0.f, 0.f);
+    q1 = make_float2(0.f, 0.f);
+    if (e & 0x80000000u) {
+      const unsigned hi = e & 0x7fffffffu;
+      c = hcom[hi];
+      if (QUAD) {
+        q0 = hq0[hi];
+        q1 = hq1[hi];
+      }
+    } else {
+      c = ncom[e];
+      if (QUAD) {
+        q0 = nq0[e];
+        const float4 b = nq1[e];
+        q1 = make_float2(b.x, b.y);
+      }
+    }
+  };
+
   // ---- far multipoles: each lane expands its own node about z, the warp sums the coefficients -------------
   auto flush_m2l = [&](int count) {
     for (int base = 0; base < count; base += 32) {
@@ -304,15 +329,9 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
 #pragma unroll
       for (int k = 0; k < 32; ++k) v[k] = 0.0f;
       if ((int)lane < count - base) {
-        const unsigned node = S.m2l[w][base + lane];
-        const float4 c = ncom[node];
-        float4 q0 = make_float4(0.f, 0.f, 0.f, 0.f);
-        float2 q1 = make_float2(0.f, 0.f);
-        if (QUAD) {
-          q0 = nq0[node];
-          const float4 b = nq1[node];
-          q1 = make_float2(b.x, b.y);
-        }
+        float4 c, q0;
+        float2 q1;
+        load_multipole(S.m2l[w][base + lane], c, q0, q1);
         local_coeffs<QUAD>(c, q0, q1, G, zx, zy, zz, soft2, v);
       }
       loc += warp_transpose_sum32(v);
@@ -325,13 +344,12 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
       const int m = min(32, count - base);
       if ((int)lane < m) {
         // staged with G folded in: (com, G·M) and G·Q
-        const unsigned node = S.m2p[w][base + lane];
-        float4 c = ncom[node];
+        float4 c, q;
+        float2 b;
+        load_multipole(S.m2p[w][base + lane], c, q, b);
         c.w *= G;
         S.src[w][lane] = c;
         if (QUAD) {
-          const float4 q = nq0[node];
-          const float4 b = nq1[node];
           S.q0[w][lane] = make_float4(G * q.x, G * q.y, G * q.z, G * q.w);
           S.q1[w][lane] = make_float2(G * b.x, G * b.y);
         }
@@ -540,20 +558,63 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
     }
     const bool acc_l = acc_node && far_l;
     acc_node = acc_node && !far_l;
-    const unsigned bl = __ballot_sync(SPH_FULL_MASK, acc_l);
-    const unsigned bm = __ballot_sync(SPH_FULL_MASK, acc_node);
-    const unsigned bf = __ballot_sync(SPH_FULL_MASK, leaf);
+    // Entries of this lane: a node for the multipole lists (m0 per particle, l0 into the group's expansion), a
+    // near leaf, or a far leaf; with half leaves a far leaf becomes two entries, each half accepted as a
+    // multipole when the MAC holds for its own moments, else its <= half sources go to the far list.
+    bool m0 = acc_node, m1 = false, l0 = acc_l, l1 = false, f0 = leaf && !near_leaf, f1 = false;
+    unsigned v0 = node, v1 = 0u;                                 // multipole entries
+    unsigned fe0 = (ls0 << 5) | min(ls1 - ls0 - 1u, 31u), fe1 = 0u;  // far entries: first << 5 | (count − 1)
+    unsigned fs0 = ls1 - ls0, fs1 = 0u, fk = (unsigned)K;           // their sources, slots per far entry
+    if (GRAV && half > 0 && f0) {
+      const unsigned cl = node - leaf0, mid = ls0 + (unsigned)half;
+      const float2 rch = hrc[cl];
+      fk = (unsigned)half;
+      auto classify = [&](unsigned hidx, float rc_h, bool& m, bool& l, bool& f) {
+        const float4 hc = hcom[hidx];
+        const float ddx = fmaxf(fmaxf(gx0 - hc.x, hc.x - gx1), 0.0f);
+        const float ddy = fmaxf(fmaxf(gy0 - hc.y, hc.y - gy1), 0.0f);
+        const float ddz = fmaxf(fmaxf(gz0 - hc.z, hc.z - gz1), 0.0f);
+        const bool mac_h = sqrtf(ddx * ddx + ddy * ddy + ddz * ddz + soft2) >= rc_h * 1.00001f;
+        const float ux = hc.x - zx, uy = hc.y - zy, uz = hc.z - zz;
+        const bool far_h = ux * ux + uy * uy + uz * uz >= far2;
+        m = mac_h && !far_h;
+        l = mac_h && far_h;
+        f = !mac_h;
+      };
+      classify(2u * cl, rch.x, m0, l0, f0);
+      v0 = 0x80000000u | (2u * cl);
+      fe0 = (ls0 << 5) | (min(ls1, mid) - ls0 - 1u);
+      fs0 = min(ls1, mid) - ls0;
+      if (ls1 > mid) {
+        classify(2u * cl + 1u, rch.y, m1, l1, f1);
+        v1 = 0x80000000u | (2u * cl + 1u);
+        fe1 = (mid << 5) | (ls1 - mid - 1u);
+        fs1 = ls1 - mid;
+      }
+    }
+    const unsigned bm0 = __ballot_sync(SPH_FULL_MASK, m0), bm1 = __ballot_sync(SPH_FULL_MASK, m1);
+    const unsigned bl0 = __ballot_sync(SPH_FULL_MASK, l0), bl1 = __ballot_sync(SPH_FULL_MASK, l1);
+    const unsigned bf0 = __ballot_sync(SPH_FULL_MASK, f0), bf1 = __ballot_sync(SPH_FULL_MASK, f1);
     const unsigned bo = __ballot_sync(SPH_FULL_MASK, open);
     const unsigned bn = __ballot_sync(SPH_FULL_MASK, near_leaf);
-    const unsigned bfar = bf & ~bn;
-    if (acc_node) S.m2p[w][nm + __popc(bm & lt)] = node;
-    if (acc_l) S.m2l[w][nl + __popc(bl & lt)] = node;
-    if (leaf) {
-      // list entries carry the leaf's source range (capacity <= 2^26 particles, leaves <= 32 sources)
-      const unsigned e = (ls0 << 5) | min(ls1 - ls0 - 1u, 31u);
-      if (near_leaf) S.p2p[w][np + __popc(bn & lt)] = e;
-      else S.p2f[w][nf + __popc(bfar & lt)] = e;
+    // two entries per lane: lanes below this one come first, then this lane's first and second entry
+    if (m0 || m1) {
+      const int k = nm + __popc(bm0 & lt) + __popc(bm1 & lt);
+      if (m0) S.m2p[w][k] = v0;
+      if (m1) S.m2p[w][k + (m0 ? 1 : 0)] = v1;
     }
+    if (l0 || l1) {
+      const int k = nl + __popc(bl0 & lt) + __popc(bl1 & lt);
+      if (l0) S.m2l[w][k] = v0;
+      if (l1) S.m2l[w][k + (l0 ? 1 : 0)] = v1;
+    }
+    if (f0 || f1) {
+      const int k = nf + __popc(bf0 & lt) + __popc(bf1 & lt);
+      if (f0) S.p2f[w][k] = fe0;
+      if (f1) S.p2f[w][k + (f0 ? 1 : 0)] = fe1;
+    }
+    // list entries carry the leaf's source range (capacity <= 2^26 particles, leaves <= 32 sources)
+    if (near_leaf) S.p2p[w][np + __popc(bn & lt)] = (ls0 << 5) | min(ls1 - ls0 - 1u, 31u);
     const int no = __popc(bo);
     if (sp + 2 * no <= stack_cap) {
       if (open) {
@@ -565,34 +626,36 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
     } else if (no) {
       overflow = 1;
     }
-    nm += __popc(bm);
-    nl += __popc(bl);
+    nm += __popc(bm0) + __popc(bm1);
+    nl += __popc(bl0) + __popc(bl1);
     np += __popc(bn);
-    nf += __popc(bfar);
-    part_m2p += __popc(bm);
-    part_m2l += __popc(bl);
-    part_p2p += __popc(bf);
+    nf += __popc(bf0) + __popc(bf1);
+    part_m2p += __popc(bm0) + __popc(bm1);
+    part_m2l += __popc(bl0) + __popc(bl1);
     {
-      // real source particles of this pop's leaves (the slots above include the padding of partial leaves)
-      unsigned srcs = leaf ? ls1 - ls0 : 0u;
+      // source particles of this pop's pairwise entries (low half) and the slots the lanes run for them
+      // (high half: K per near leaf, KF per far entry, the padding of partial leaves included); <= 1,024 each
+      unsigned pk = (near_leaf ? ls1 - ls0 + ((unsigned)K << 16) : 0u) + (f0 ? fs0 + (fk << 16) : 0u) +
+                    (f1 ? fs1 + (fk << 16) : 0u);
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) srcs += __shfl_xor_sync(SPH_FULL_MASK, srcs, o);
-      part_src += srcs;
+      for (int o = 16; o > 0; o >>= 1) pk += __shfl_xor_sync(SPH_FULL_MASK, pk, o);
+      part_src += pk & 0xffffu;
+      part_p2p += pk >> 16;
     }
     __syncwarp();
-    if (nm > TW_LIST - 32) {
+    if (nm > TW_LIST - 64) {
       flush_m2p(nm);
       nm = 0;
     }
-    if (nl > TW_LIST - 32) {
+    if (nl > TW_LIST - 64) {
       flush_m2l(nl);
       nl = 0;
     }
-    if (np > TW_LIST - 32) {
+    if (np > TW_LIST - 64) {
       flush_p2p(np);
       np = 0;
     }
-    if (nf > TW_LIST - 32) {
+    if (nf > TW_LIST - 64) {
       flush_far(nf);
       nf = 0;
     }
@@ -617,7 +680,7 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
   st_m2p += part_m2p * nvalid;                             // node × particle interactions
   st_m2l += part_m2l;                                      // nodes expanded about a part's centre
   st_p2p += part_src * nvalid;                             // source particles × particles
-  st_slots += part_p2p * (unsigned long long)K * nvalid;   // ... counting every leaf as K sources
+  st_slots += part_p2p * nvalid;                           // ... counting the slots the lanes ran
   }  // parts
 
   if (in_group && GRAV) {
@@ -655,7 +718,7 @@ static void walk(const Dev& d, const Cfg& c, cudaStream_t s) {
       d.body, st.pos_h, st.x, st.y, st.z, d.K, d.L, d.leaf_start, d.leaf_codes, d.segs, d.left, d.right, d.ncom,
       d.nbmin, d.nbmax, d.nq0, d.nq1, d.P, d.grav, d.nbr, d.nbr_cnt, d.nbr_cap, c.h_solve ? -1.0f : c.nbr_skin,
       d.h0, d.groups, d.ngroups, c.walk_stack > 0 && c.walk_stack < TW_STACK ? c.walk_stack : TW_STACK,
-      GRAV ? c.local_theta : 0.0f);
+      GRAV ? c.local_theta : 0.0f, GRAV ? half_leaf(d, c) : 0, d.hcom, d.hq0, d.hq1, d.hrc);
 }
 
 // Gravity (group MAC) fused with the neighbour lists; the traversal tile (warps per block) is a tuning choice.

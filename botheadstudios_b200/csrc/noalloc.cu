@@ -40,6 +40,7 @@ constexpr size_t scratch_bytes() {
   b += up(8 * L) + 3 * up(4 * L) + up(8 * L) + up(4);                  // leaf codes, left/right/counters, groups
   b += up(4 * (L + 1)) + up(2 * sizeof(Seg));                          // leaf starts, segment table
   b += up(4 * nodes) + 5 * up(16 * nodes);                             // parents, node records
+  b += 2 * up(16 * L) + 2 * up(8 * L);                                 // half-leaf moments (leaves of >= 16)
   b += up(sizeof(DevParams));
   return b;
 }
@@ -179,6 +180,11 @@ Dev carve_dev(unsigned char* base, uint32_t K) {
   d.nbmax = carve<float4>(p, nodes);
   d.nq0 = carve<float4>(p, nodes);
   d.nq1 = carve<float4>(p, nodes);
+  // half leaves exist for leaves of >= 16 points, so 2 · (n / 16) entries, which the n / 8 of L covers
+  d.hcom = carve<float4>(p, L);
+  d.hq0 = carve<float4>(p, L);
+  d.hq1 = carve<float2>(p, L);
+  d.hrc = carve<float2>(p, L);
   d.P = carve<DevParams>(p, 1);
   return d;
 }

@@ -135,6 +135,10 @@ sph_status alloc_dev(sph_ctx* ctx, Dev& d, uint32_t cap, uint32_t K, uint32_t nb
   ALLOC(d.nbmax, nodes);
   ALLOC(d.nq0, nodes);
   ALLOC(d.nq1, nodes);
+  ALLOC(d.hcom, 2 * Lmax);
+  ALLOC(d.hq0, 2 * Lmax);
+  ALLOC(d.hq1, 2 * Lmax);
+  ALLOC(d.hrc, Lmax);
   ALLOC(d.grav, capw);
   ALLOC(d.groups, Lmax);
   ALLOC(d.ngroups, 1);

@@ -156,6 +156,12 @@ struct Dev {
   float4* nbmax = nullptr;      // [2L-1] bmax.xyz, opening radius
   float4* nq0 = nullptr;        // [2L-1] Qxx, Qyy, Qzz, Qxy
   float4* nq1 = nullptr;        // [2L-1] Qxz, Qyz, 0, 0
+  // Half-leaf moments (group walk, leaves of >= 16 particles): leaf c's particles [s, s + K/2) and [s + K/2, e)
+  // as two multipoles, entries 2c and 2c + 1, for far leaves the walk splits
+  float4* hcom = nullptr;       // [2L] com.xyz, mass
+  float4* hq0 = nullptr;        // [2L] Qxx, Qyy, Qzz, Qxy
+  float2* hq1 = nullptr;        // [2L] Qxz, Qyz
+  float2* hrc = nullptr;        // [L] opening radii of the two halves (size/θ + |centre − COM|)
   uint2* groups = nullptr;      // [L] walk groups: (first leaf, last leaf) of runs of 32/K leaves of one impact
   unsigned* ngroups = nullptr;  // [1] number of groups
   unsigned* nbr = nullptr;      // interleaved neighbour lists [n/32][nbr_cap][32]
@@ -224,6 +230,8 @@ int launch_segments_single(const Dev& d, float soft2, double dt, cudaStream_t s)
 int launch_bbox(const Dev& d, cudaStream_t s);
 int launch_sort_permute(Dev& d, cudaStream_t s);      // keys → radix sort → permute (swaps d.cur)
 int launch_tree(const Dev& d, const Cfg& c, float theta, cudaStream_t s);  // Karras + moments
+// particles per half leaf the group walk splits far leaves into (0: leaves are not split)
+int half_leaf(const Dev& d, const Cfg& c);
 size_t radix_tiles(int n);
 // stable LSD radix sort of (keys, vals) on the low `bits` key bits; the result lands in buffer `src`
 int launch_radix_sort(unsigned long long* keys[2], unsigned* vals[2], int n, int bits, unsigned* hist,
