@@ -109,8 +109,11 @@ def _compare_sph(s, p_state, I, tol_rho=2e-6, tol_acc=1e-4, tol_du=1e-3):
     rho_o = oracle.density32(pos4, mass, kernel=KERNEL)
     assert np.max(np.abs(rho - rho_o) / rho_o) < tol_rho
     P_o, c_o = oracle.eos32(I.eos, p_state["mat"], rho_o, p_state["u"], du_floor=u.du_floor, rho_floor=u.rho_floor)
-    # (c vanishes where the expanded branch of the EOS has no pressure: relative to the largest c there)
-    assert np.max(np.abs(s.inspect("SOUND") - c_o) / np.maximum(c_o, 1e-3 * c_o.max())) < 2e-3
+    # c² = ∂P/∂ρ + P/ρ² ∂P/∂u from central differences is clamped at 0 in expanded material, where the f32 noise of
+    # the differences decides the clamp: the largest difference is held against the largest c, the bulk by RMS
+    dc = s.inspect("SOUND").astype(np.float64) - c_o
+    assert np.abs(dc).max() < 2e-3 * c_o.max()
+    assert math.sqrt((dc ** 2).sum() / (c_o.astype(np.float64) ** 2).sum()) < 1e-4
     vel4 = np.ascontiguousarray(np.concatenate([p_state["vel"], p_state["u"][:, None]], axis=1), dtype=np.float32)
     f_o = oracle.sph_forces32(pos4, vel4, mass, rho_o, P_o, c_o, r_min=u.r_min, kernel=KERNEL)
     acc = s.inspect("ACC_SPH")
