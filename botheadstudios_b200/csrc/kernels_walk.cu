@@ -486,7 +486,12 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
 
   const unsigned nvalid = __popc(__ballot_sync(SPH_FULL_MASK, valid));
   unsigned long long part_m2p = 0, part_p2p = 0, part_m2l = 0, part_src = 0;
-  while (sp > 0) {
+  // One pass per pop; the pass after the stack empties flushes what the lists still hold, so that every flush
+  // loop has one call site (the walk's hot code is instruction-cache bound: a second inlined copy of each flush
+  // loop measurably stalled instruction fetch).
+  for (;;) {
+  const bool done = sp == 0;
+  if (!done) {
     const int take = min(sp, 32);
     sp -= take;
     st_visits += take;
@@ -569,24 +574,31 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
       const unsigned cl = node - leaf0, mid = ls0 + (unsigned)half;
       const float2 rch = hrc[cl];
       fk = (unsigned)half;
-      auto classify = [&](unsigned hidx, float rc_h, bool& m, bool& l, bool& f) {
-        const float4 hc = hcom[hidx];
+      const unsigned nh = ls1 > mid ? 2u : 1u;
+      const float4 hA = hcom[2u * cl], hB = hcom[2u * cl + 1u];
+      unsigned hf = 0u;  // bit b: half b passes the MAC; bit 2 + b: ... and lies far enough for the expansion
+#pragma unroll 1
+      for (unsigned b = 0; b < nh; ++b) {
+        const float4 hc = b ? hB : hA;
         const float ddx = fmaxf(fmaxf(gx0 - hc.x, hc.x - gx1), 0.0f);
         const float ddy = fmaxf(fmaxf(gy0 - hc.y, hc.y - gy1), 0.0f);
         const float ddz = fmaxf(fmaxf(gz0 - hc.z, hc.z - gz1), 0.0f);
-        const bool mac_h = sqrtf(ddx * ddx + ddy * ddy + ddz * ddz + soft2) >= rc_h * 1.00001f;
+        const bool mac_h = sqrtf(ddx * ddx + ddy * ddy + ddz * ddz + soft2) >= (b ? rch.y : rch.x) * 1.00001f;
         const float ux = hc.x - zx, uy = hc.y - zy, uz = hc.z - zz;
         const bool far_h = ux * ux + uy * uy + uz * uz >= far2;
-        m = mac_h && !far_h;
-        l = mac_h && far_h;
-        f = !mac_h;
-      };
-      classify(2u * cl, rch.x, m0, l0, f0);
+        hf |= (mac_h ? 1u : 0u) << b;
+        hf |= (mac_h && far_h ? 1u : 0u) << (2u + b);
+      }
+      m0 = (hf & 5u) == 1u;
+      l0 = (hf & 4u) != 0u;
+      f0 = (hf & 1u) == 0u;
       v0 = 0x80000000u | (2u * cl);
       fe0 = (ls0 << 5) | (min(ls1, mid) - ls0 - 1u);
       fs0 = min(ls1, mid) - ls0;
-      if (ls1 > mid) {
-        classify(2u * cl + 1u, rch.y, m1, l1, f1);
+      if (nh == 2u) {
+        m1 = (hf & 10u) == 2u;
+        l1 = (hf & 8u) != 0u;
+        f1 = (hf & 2u) == 0u;
         v1 = 0x80000000u | (2u * cl + 1u);
         fe1 = (mid << 5) | (ls1 - mid - 1u);
         fs1 = ls1 - mid;
@@ -642,28 +654,26 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
       part_src += pk & 0xffffu;
       part_p2p += pk >> 16;
     }
+  }  // !done
     __syncwarp();
-    if (nm > TW_LIST - 64) {
+    if (nm > TW_LIST - 64 || (done && nm)) {
       flush_m2p(nm);
       nm = 0;
     }
-    if (nl > TW_LIST - 64) {
+    if (nl > TW_LIST - 64 || (done && nl)) {
       flush_m2l(nl);
       nl = 0;
     }
-    if (np > TW_LIST - 64) {
+    if (np > TW_LIST - 64 || (done && np)) {
       flush_p2p(np);
       np = 0;
     }
-    if (nf > TW_LIST - 64) {
+    if (nf > TW_LIST - 64 || (done && nf)) {
       flush_far(nf);
       nf = 0;
     }
+    if (done) break;
   }
-  if (nm) flush_m2p(nm);
-  if (nl) flush_m2l(nl);
-  if (np) flush_p2p(np);
-  if (nf) flush_far(nf);
   if (GRAV && part_m2l) {
     // the part's expansion (lane k holds coefficient k) evaluated by every particle of the part
     float cf[kLocal];
