@@ -1,8 +1,9 @@
 """Batched impacts by size bucket, with a launch-configuration autotuner.
 
-A batch of impacts of uneven size is split into size buckets; each bucket is one context (its own CUDA stream
-and tuned launch configuration) that advances all of its impacts with one launch per phase, and the buckets run
-concurrently on their streams. The autotuner picks, per bucket, the LBVH leaf size, the block size of the
+A batch of impacts of uneven size is split into size buckets, each tuned on its own; buckets whose tuned launch
+configurations agree share one context, which advances all of their impacts with one launch per phase (with one
+configuration for every bucket, the whole batch is one context), and contexts of different configurations run
+concurrently on their own streams. The autotuner picks, per bucket, the LBVH leaf size, the block size of the
 per-particle gather kernels (density, h-solve, forces) and the traversal tile of the fused walk (warps per
 block) by timing candidates on a probe batch drawn from that bucket. Choices are cached in a JSON file keyed
 by the GPU name and the bucket.
@@ -115,23 +116,41 @@ class Autotuner:
         return dict(best)
 
 
+def context_groups(bucket_ids, choices: dict) -> list:
+    """Buckets that share a context: those whose tuned choices are equal (in bucket order)."""
+    groups = []
+    for b in sorted(bucket_ids):
+        ch = choices.get(b, DEFAULT_CHOICE)
+        for g in groups:
+            if choices.get(g[0], DEFAULT_CHOICE) == ch:
+                g.append(b)
+                break
+        else:
+            groups.append([b])
+    return groups
+
+
 class BucketedBatch:
-    """A batch of impacts advanced as one context per size bucket (impacts reordered so that each bucket is a
-    contiguous range of the particle array; `order` maps back to the caller's impact order)."""
+    """A batch of impacts advanced as one context per group of buckets with equal tuned choices (impacts
+    reordered so that each context holds a contiguous range of the particle array; `order` maps back to the
+    caller's impact order)."""
 
     def __init__(self, B: ic.Batch, base: dict, choices: dict | None = None, device: int = -1):
         sizes = np.diff(B.offsets).astype(np.int64)
         buckets = np.array([bucket_of(int(n)) for n in sizes])
-        self.order = np.argsort(buckets, kind="stable")
-        self.batch = subset(B, self.order)
-        self.bucket_ids = sorted(set(buckets.tolist()))
-        self.ranges, self.ctxs, self.sub = [], [], []
         choices = choices or {}
+        self.bucket_ids = sorted(set(buckets.tolist()))
+        self.groups = context_groups(self.bucket_ids, choices)
+        group_of = {b: gi for gi, g in enumerate(self.groups) for b in g}
+        gidx = np.array([group_of[int(b)] for b in buckets])
+        self.order = np.argsort(gidx, kind="stable")
+        self.batch = subset(B, self.order)
+        self.ranges, self.ctxs, self.sub = [], [], []
         k0 = 0
-        for b in self.bucket_ids:
-            k1 = k0 + int((buckets == b).sum())
+        for gi, g in enumerate(self.groups):
+            k1 = k0 + int((gidx == gi).sum())
             sub = subset(self.batch, range(k0, k1))
-            cfg = dict(base, **choices.get(b, DEFAULT_CHOICE))
+            cfg = dict(base, **choices.get(g[0], DEFAULT_CHOICE))
             s = GpuSph(len(sub.particles), device=device, **cfg)
             _load_network(s, cfg)
             self.ctxs.append(s)

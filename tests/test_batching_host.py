@@ -105,3 +105,14 @@ def test_tune_buckets_probes_each_populated_bucket_with_its_first_impacts(monkey
         for j, k in enumerate(want):
             assert np.array_equal(p.particles[int(p.offsets[j]):int(p.offsets[j + 1])], B.impact(k))
     assert len(log) == 7 * 2
+
+
+def test_buckets_with_equal_choices_share_one_context():
+    """One launch per phase for the whole batch when every bucket is tuned to the same configuration; buckets
+    tuned differently keep contexts of their own."""
+    same = dict(leaf_size=8, walk_warps=2, block_threads=256)
+    assert batching.context_groups([0, 1, 2], {0: same, 1: dict(same), 2: dict(same)}) == [[0, 1, 2]]
+    other = dict(same, leaf_size=16)
+    assert batching.context_groups([0, 1, 2], {0: same, 1: other, 2: dict(same)}) == [[0, 2], [1]]
+    assert batching.context_groups([1], {}) == [[1]]
+    assert batching.context_groups([0, 2], {}) == [[0, 2]]  # both untuned: the default choice
