@@ -262,17 +262,46 @@ def timed(ctxs, encode, steps: int, local: int) -> float:
     return e0.elapsed_time(e1)
 
 
-def plain_same(wl: dict, I, device: int, steps: int, warmup: int) -> dict:
-    """The plain GPU form (iterated h: SPH_H_SOLVE) on the same initial conditions, timed the same way: the
-    comparison of the learned form."""
+def density_error(wl: dict, I, state, device: int) -> dict:
+    """Densities of a state (48-byte particles) against a converged smoothing-length solve (8 Newton iterations)
+    on the same positions: the accuracy the learned and the plain forms are compared at."""
     from botheadstudios_b200 import workloads
-    with workloads.solver(wl, I, device, h_mode=1) as s:
+    with workloads.solver(wl, I, device, h_mode=1, h_iters=8) as s:
+        s.upload(state, I.eos, I.softening)
+        s.eval_forces()
+        rho = s.inspect("RHO")
+    e = np.abs(state["rho"].astype(np.float64) / rho - 1.0)
+    return dict(rms=float(np.sqrt(np.mean(e * e))), max=float(e.max()))
+
+
+def plain_same(wl: dict, I, device: int, steps: int, warmup: int, h_iters: int = 2) -> dict:
+    """The plain GPU form (iterated h: SPH_H_SOLVE with h_iters Newton iterations) on the same initial
+    conditions, timed the same way, with the density error of its final state: the comparison of the learned
+    form."""
+    from botheadstudios_b200 import workloads
+    with workloads.solver(wl, I, device, h_mode=1, h_iters=h_iters) as s:
         workloads.upload(s, I)
         s.encode_kdk(warmup)
         s.sync()
         ms = timed([s], s.encode_kdk, steps, max(device, 0))
         d = s.diag()
-    return dict(value=len(I.particles) * steps / (ms / 1000.0), ms_per_step=ms / steps, h_residual=d["h_residual"])
+        state = s.readback()
+    return dict(value=len(I.particles) * steps / (ms / 1000.0), ms_per_step=ms / steps, h_iters=h_iters,
+                h_residual=d["h_residual"], density_error=density_error(wl, I, state, device))
+
+
+def plain_batched(wl: dict, B, choices: dict, device: int, steps: int, warmup: int) -> dict:
+    """The plain form (iterated h) of a batch with the learned run's tuned choices, contexts and graphs, timed the
+    same way: what the learned smoothing length changes with everything else equal."""
+    from botheadstudios_b200 import batching, workloads
+    base = workloads.config(wl, B, h_mode=1)
+    with batching.BucketedBatch(B, base, choices, device=device) as r:
+        r.upload()
+        r.encode_kdk(warmup)
+        r.sync()
+        ms = timed(r.ctxs, r.encode_kdk, steps, max(device, 0))
+        res = max(d["h_residual"] for d in r.diag())
+    return dict(value=r.n * steps / (ms / 1000.0), ms_per_step=ms / steps, h_residual=res, contexts=len(r.ctxs))
 
 
 def plain_sequential(wl: dict, B, device: int, impacts: int = 16, steps: int = 2) -> dict:
@@ -473,6 +502,10 @@ def run_ours(args, wl, world, rank, local, pg):
     def dsum(ds, key):
         return sum(d[key] for d in ds)
 
+    learned_state = None
+    if wl.get("h_solve") == 2 and wl.get("kind") != "batch" and rank == 0 and not args.no_plain:
+        learned_state = runner.s.readback()  # the learned form's state after its timed and profiled steps
+
     # mean neighbour-list length (the lists the gather phases stream)
     lsum, lcnt = 0.0, 0
     for s in runner.ctxs:
@@ -499,8 +532,14 @@ def run_ours(args, wl, world, rank, local, pg):
     plain = None
     if wl.get("kind") == "batch" and rank == 0 and not args.no_plain:
         plain = plain_sequential(wl, I, local)
+        if wl.get("h_solve") == 2:
+            plain = dict(sequential=plain, batched_same_tuning=plain_batched(
+                wl, I, {int(b): c for b, c in (tuned or {}).get("choices", {}).items()}, local, args.steps,
+                args.warmup))
     elif wl.get("h_solve") == 2 and rank == 0 and not args.no_plain:
-        plain = plain_same(wl, I, local, args.steps, args.warmup)
+        plain = dict(newton_2=plain_same(wl, I, local, args.steps, args.warmup, h_iters=2),
+                     newton_1=plain_same(wl, I, local, args.steps, args.warmup, h_iters=1),
+                     learned_density_error=density_error(wl, I, learned_state, local))
 
     if rank != 0:
         return
@@ -576,8 +615,8 @@ def run_ours(args, wl, world, rank, local, pg):
                          steps=e2e_steps),
                 gpu_launches=launches, roofline=roof, roofline_hbm=roof_hbm, phases=phases, cpu_baseline=cpu,
                 clocks=clk.summary(),
-                autotune=tuned, **({"plain_sequential": plain} if wl.get("kind") == "batch" else
-                                   {"plain_form": plain} if plain else {}),
+                autotune=tuned, **({} if not plain else
+                                   {"plain_sequential": plain} if wl.get("h_solve") != 2 else {"plain_form": plain}),
                 physics=dict(**conservation_drifts(dstart, d1),
                              sim_time=dd["time"], dt=dd["dt"],
                              max_neighbours=max(d["max_neighbours_seen"] for d in d1),
