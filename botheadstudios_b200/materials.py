@@ -24,9 +24,16 @@ G_SI = 6.674e-11  # sph_step.wgsl:21, bh_gravity.wgsl:11, orbit::G
 TILLOTSON_SI = {
     "basalt": (2700.0, 0.5, 1.5, 2.67e10, 2.67e10, 4.87e8, 4.72e6, 1.82e7, 5.0, 5.0),
     "iron": (7850.0, 0.5, 1.28, 1.28e11, 1.815e11, 1.425e7, 2.4e6, 8.67e6, 5.0, 5.0),
+    # the catalogue's other layer materials, for the reference's layered bodies (HydroBody::particalize)
+    "peridotite": (3500.0, 0.5, 1.4, 1.31e11, 4.9e10, 5.5e8, 4.5e6, 1.45e7, 5.0, 5.0),
+    "ice": (917.0, 0.3, 0.1, 9.47e9, 9.47e9, 1.0e7, 7.73e5, 3.04e6, 10.0, 5.0),
 }
+# the catalogue's specific heats (J/kg/K), u = c·T for the layered bodies' geotherms
+SPECIFIC_HEAT = {"basalt": 840.0, "iron": 449.0, "peridotite": 1000.0, "ice": 2090.0}
 MAT_BASALT = 0  # gpu_sph.rs:107
 MAT_IRON = 1  # gpu_sph.rs:108
+MAT_PERIDOTITE = 2  # further rows of this library's material table (the engine's table holds up to 16)
+MAT_ICE = 3
 MAX_MATERIALS = 16  # gpu_sph.rs:113
 
 EARTH_MASS = 5.972e24
