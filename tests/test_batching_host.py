@@ -107,12 +107,17 @@ def test_tune_buckets_probes_each_populated_bucket_with_its_first_impacts(monkey
     assert len(log) == 7 * 2
 
 
-def test_buckets_with_equal_choices_share_one_context():
-    """One launch per phase for the whole batch when every bucket is tuned to the same configuration; buckets
-    tuned differently keep contexts of their own."""
+def test_buckets_with_equal_walk_choices_share_one_context():
+    """One launch per phase for the whole batch when every bucket is tuned to the same leaf size and walk tile;
+    buckets tuned to another tree or walk keep contexts of their own; the merged context takes the gather block
+    size of its bucket with the most particles."""
     same = dict(leaf_size=8, walk_warps=2, block_threads=256)
     assert batching.context_groups([0, 1, 2], {0: same, 1: dict(same), 2: dict(same)}) == [[0, 1, 2]]
+    blk = {0: dict(same, block_threads=128), 1: same, 2: dict(same, block_threads=512)}
+    assert batching.context_groups([0, 1, 2], blk) == [[0, 1, 2]]
+    assert batching.group_choice([0, 1, 2], blk, {0: 10, 1: 50, 2: 30})["block_threads"] == 256
     other = dict(same, leaf_size=16)
     assert batching.context_groups([0, 1, 2], {0: same, 1: other, 2: dict(same)}) == [[0, 2], [1]]
+    assert batching.context_groups([0, 1, 2], {0: same, 1: dict(same, walk_warps=4), 2: same}) == [[0, 2], [1]]
     assert batching.context_groups([1], {}) == [[1]]
     assert batching.context_groups([0, 2], {}) == [[0, 2]]  # both untuned: the default choice
