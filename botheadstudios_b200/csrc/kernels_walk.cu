@@ -234,6 +234,12 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
   const float G = P->G, soft2 = sgr.soft2;
   const unsigned leaf0 = (unsigned)(L - 1);
   const unsigned lt = (1u << lane) - 1u;
+  // staging of the pairwise lists: entries of K (near) or K/2 (far, when far leaves are split into halves)
+  // sources, 32/K entries per 32-source chunk; K is a power of two in the group walk, so shifts, not divisions
+  const int ksh = 31 - __clz(K);
+  const int kfsh = half > 0 ? ksh - 1 : ksh;
+  const int near_per = 32 >> ksh, near_li = (int)lane >> ksh, near_off = (int)lane & (K - 1);
+  const int far_per = 32 >> kfsh, far_li = (int)lane >> kfsh, far_off = (int)lane & ((1 << kfsh) - 1);
 
   Acc3 acc;
   float phi = 0.f;
@@ -262,11 +268,8 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
   // ---- far leaves: branch-free pairwise gravity, 32 staged sources per pass ---------------------------
   // The next chunk's sources are loaded into registers before this chunk is evaluated, so the gather
   // overlaps the arithmetic.
-  // far entries hold at most KF sources: half leaves when far leaves are split, whole leaves otherwise
-  const int KF = half > 0 ? half : K;
   auto far_source = [&](int base, int count) {
-    const int per = 32 / KF;
-    const int li = lane / KF, off = lane % KF;
+    const int per = far_per, li = far_li, off = far_off;
     float4 src = make_float4(3.0e18f, 3.0e18f, 3.0e18f, 0.0f);  // padding: massless and far away
     if (li < min(per, count - base)) {
       const unsigned e = S.p2f[w][base + li];  // first source << 5 | (sources − 1)
@@ -275,7 +278,7 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
     return src;
   };
   auto flush_far = [&](int count) {
-    const int per = 32 / KF;
+    const int per = far_per;
     float4 nxt = far_source(0, count);
     for (int base = 0; base < count; base += per) {
       float4 src = nxt;
@@ -397,8 +400,7 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
 
   // ---- direct list: leaves of <= K sources (K divides 32), 32 sources per chunk ------------------------
   auto near_source = [&](int base, int count, float4& src, float& hsrc) {
-    const int per = 32 / K;  // leaves per chunk
-    const int li = lane / K, off = lane % K;
+    const int per = near_per, li = near_li, off = near_off;  // leaves per chunk, this lane's leaf and source
     int sidx = -1;
     if (li < min(per, count - base)) {
       const unsigned e = S.p2p[w][base + li];  // first source << 5 | (sources − 1)
@@ -421,7 +423,9 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
       const bool other = s != t;
       const float4 bj = S.src[w][k];
       const float dx = fsub(bj.x, pi.x), dy = fsub(bj.y, pi.y), dz = fsub(bj.z, pi.z);
-      const float dd = dot3_exact(dx, dy, dz);
+      // the exact predicate needs the single-rounded distance; the conservative one's 2^-19 margin is far above
+      // the few ulp a fused form differs by
+      const float dd = decltype(loose)::value ? fmaf(dz, dz, fmaf(dy, dy, dx * dx)) : dot3_exact(dx, dy, dz);
       if (NBR && other) {
         bool inside;
         if constexpr (decltype(loose)::value) {
@@ -448,17 +452,19 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
           ez -= zlo;
           d2 = ex * ex + ey * ey + ez * ez;
         }
+        // the particle itself (d = 0) gets r² = 1: a finite g times a zero offset adds nothing (with hi/lo
+        // coordinates its offset is −lo, so there the mass is masked)
         const float r2 = other ? d2 + soft2 : 1.0f;
         const float rinv = rsqrt_ftz(r2);
-        const float gm = other ? bj.w * rinv : 0.0f;
+        const float gm = (HILO && !other) ? 0.0f : bj.w * rinv;
         const float g = gm * rinv * rinv;
         acc.add<HILO>(g * ex, g * ey, g * ez);
-        if (OUT != kWalkAcc) phi -= gm;
+        if (OUT != kWalkAcc && other) phi -= gm;
       }
     }
   };
   auto flush_p2p = [&](int count) {
-    const int per = 32 / K;  // leaves per chunk
+    const int per = near_per;  // leaves per chunk
     float4 nsrc;
     float nh;
     int nidx = near_source(0, count, nsrc, nh);
@@ -646,7 +652,7 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
     part_m2l += __popc(bl0) + __popc(bl1);
     {
       // source particles of this pop's pairwise entries (low half) and the slots the lanes run for them
-      // (high half: K per near leaf, KF per far entry, the padding of partial leaves included); <= 1,024 each
+      // (high half: K per near leaf, K or K/2 per far entry, the padding of partial leaves included); <= 1,024 each
       unsigned pk = (near_leaf ? ls1 - ls0 + ((unsigned)K << 16) : 0u) + (f0 ? fs0 + (fk << 16) : 0u) +
                     (f1 ? fs1 + (fk << 16) : 0u);
 #pragma unroll
