@@ -537,8 +537,9 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
         const float ddx = fmaxf(fmaxf(gx0 - c.x, c.x - gx1), 0.0f);
         const float ddy = fmaxf(fmaxf(gy0 - c.y, c.y - gy1), 0.0f);
         const float ddz = fmaxf(fmaxf(gz0 - c.z, c.z - gz1), 0.0f);
-        const float dmin = sqrtf(ddx * ddx + ddy * ddy + ddz * ddz + soft2);
-        mac = dmin >= bh.w * 1.00001f;
+        // sqrt(d² + ε²) >= r_open, compared squared (both sides are non-negative; no square root per node)
+        const float ro = bh.w * 1.00001f;
+        mac = ddx * ddx + ddy * ddy + ddz * ddz + soft2 >= ro * ro;
         const float ux = c.x - zx, uy = c.y - zy, uz = c.z - zz;
         far_l = ux * ux + uy * uy + uz * uz >= far2;
       }
@@ -589,7 +590,8 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
         const float ddx = fmaxf(fmaxf(gx0 - hc.x, hc.x - gx1), 0.0f);
         const float ddy = fmaxf(fmaxf(gy0 - hc.y, hc.y - gy1), 0.0f);
         const float ddz = fmaxf(fmaxf(gz0 - hc.z, hc.z - gz1), 0.0f);
-        const bool mac_h = sqrtf(ddx * ddx + ddy * ddy + ddz * ddz + soft2) >= (b ? rch.y : rch.x) * 1.00001f;
+        const float ro = (b ? rch.y : rch.x) * 1.00001f;
+        const bool mac_h = ddx * ddx + ddy * ddy + ddz * ddz + soft2 >= ro * ro;
         const float ux = hc.x - zx, uy = hc.y - zy, uz = hc.z - zz;
         const bool far_h = ux * ux + uy * uy + uz * uz >= far2;
         hf |= (mac_h ? 1u : 0u) << b;
