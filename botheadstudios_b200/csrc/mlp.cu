@@ -413,6 +413,224 @@ __global__ void __launch_bounds__(ROWS) k_mlp_forward(const MlpPacked* __restric
   if (!tc_teardown(S, phase) && threadIdx.x == 0) atomicOr(err, 1u);
 }
 
+// ---- training on tcgen05: forward + backward of one 128-sample tile ----------------------------------------
+// The same tiles as inference (M = 128 × N = 64, BF16 × BF16 → FP32 in tensor memory, one issuing thread,
+// bounded mbarrier waits), five MMA groups per tile: the two forward layers (D1 = x'·W1ᵀ, D2 = a1·W2ᵀ), then
+// da1 = dz2·W2 (D3) together with dW2 = a1ᵀ·dz2 (D4), then dW1 = x'ᵀ·dz1 (D5, in D1's columns). The weight
+// gradients contract over the tile's 128 samples (K = 128); their M (64 inputs of layer 2, 16 padded inputs of
+// layer 1) is padded to the instruction's 128 rows, whose extra rows are read from the operand buffer's unused
+// rows and never used. Thread r owns sample r: it writes its rows of every A/B operand (the transposed ones
+// column r), reads its row of each accumulator, and the bias and W3 gradients are column sums in shared memory.
+constexpr int TT_COLS = 256;  // TMEM columns: D1 [0, 64) (then D5), D2 [64, 128), D3 [128, 192), D4 [192, 256)
+
+struct TrainTcSmem {
+  __nv_bfloat16 xa[ROWS * 16];       // x' [row][k], K = 16 (A of layer 1)
+  __nv_bfloat16 ha[ROWS * MLP_H];    // a1 [row][i], K = 64 (A of layer 2)
+  __nv_bfloat16 w1[MLP_H * 16];      // W1ᵀ [out][k] (B of layer 1)
+  __nv_bfloat16 w2t[MLP_H * MLP_H];  // W2ᵀ [out][i] (B of layer 2)
+  __nv_bfloat16 w2b[MLP_H * MLP_H];  // W2 [i][out] (B of da1 = dz2 W2: N = i, K = out)
+  __nv_bfloat16 dza[ROWS * MLP_H];   // dz2 [row][out], K = 64 (A of da1)
+  __nv_bfloat16 gta[ROWS * ROWS];    // a1ᵀ [i][row] then x'ᵀ [k][row], K = 128 (A of the weight gradients)
+  __nv_bfloat16 gtb[MLP_H * ROWS];   // dz2ᵀ [out][row] then dz1ᵀ [i][row], K = 128 (B of the weight gradients)
+  float z1[ROWS * MLP_H];            // z1, then dz1 (FP32)
+  float z2[ROWS * MLP_H];            // z2 (FP32)
+  float dy[ROWS];
+  unsigned long long mbar;
+  unsigned tmem;
+  int ok;
+};
+
+// Issue (thread 0) the MMAs of `fn`, commit to the barrier, wait (bounded) for them; false on a timeout.
+template <typename F>
+__device__ bool tt_run(TrainTcSmem& S, uint32_t& phase, F fn) {
+  fence_async_smem();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (!S.ok) return false;
+  const uint32_t mbar = smem_u32(&S.mbar);
+  if (threadIdx.x == 0) {
+    fn();
+    tc_commit(mbar);
+  }
+  const bool got = mbar_wait(mbar, phase);
+  if (!__syncthreads_and(got)) {
+    if (threadIdx.x == 0) S.ok = 0;
+    return false;
+  }
+  phase ^= 1u;
+  tc_fence_after();
+  return true;
+}
+
+// 64 FP32 accumulator columns of this thread's row (TMEM lane = row).
+__device__ __forceinline__ void tt_row(const TrainTcSmem& S, uint32_t col, float v[64]) {
+  const uint32_t t = S.tmem + ((uint32_t)((threadIdx.x >> 5) * 32) << 16) + col;
+#pragma unroll
+  for (int c = 0; c < 4; ++c) tc_ld16(t + 16 * c, v + 16 * c);
+  tc_wait_ld();
+}
+
+__global__ void __launch_bounds__(ROWS) k_mlp_train_tc(const MlpPacked* __restrict__ W, const float* __restrict__ x,
+                                                      const float* __restrict__ tgt, const unsigned* __restrict__ idx,
+                                                      int m, float denom, float* __restrict__ grad,
+                                                      float* __restrict__ loss, unsigned* __restrict__ err) {
+  extern __shared__ __align__(1024) unsigned char tt_raw[];
+  TrainTcSmem& S = *reinterpret_cast<TrainTcSmem*>(tt_raw);
+  const int r = threadIdx.x, lane = r & 31;
+  // weights in the K-major operand layout
+  for (int i = r; i < MLP_H * 16; i += ROWS) S.w1[cm(i >> 4, i & 15, 16)] = W->w1t[i];
+  for (int i = r; i < MLP_H * MLP_H; i += ROWS) {
+    S.w2t[cm(i >> 6, i & 63, 64)] = W->w2t[i];  // [out][in]: row out, K = in
+    S.w2b[cm(i >> 6, i & 63, 64)] = W->w2[i];   // [in][out]: row in, K = out
+  }
+  if (r == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&S.mbar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    S.ok = 1;
+  }
+  if (r < 32) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                 :: "r"(smem_u32(&S.tmem)), "r"(TT_COLS) : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  // this thread's sample: normalised inputs (rows past m carry dy = 0 and add nothing)
+  const int s = blockIdx.x * ROWS + r;
+  const bool valid = s < m;
+  float f[MLP_IN] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, xq[MLP_IN];
+  float tn = 0.0f;
+  if (valid) {
+    const unsigned j = idx[s];
+#pragma unroll
+    for (int k = 0; k < MLP_IN; ++k) f[k] = x[(size_t)j * MLP_IN + k];
+    tn = (tgt[j] - W->ym) / W->ys;
+  }
+  normalise(f, W, xq);
+  const float zero8[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  *reinterpret_cast<uint4*>(S.xa + cm(r, 0, 16)) = pack8(xq);
+  *reinterpret_cast<uint4*>(S.xa + cm(r, 8, 16)) = pack8(zero8);
+  uint32_t phase = 0;
+  const uint32_t xa = smem_u32(S.xa), ha = smem_u32(S.ha), w1 = smem_u32(S.w1), w2t = smem_u32(S.w2t);
+  const uint32_t w2b = smem_u32(S.w2b), dza = smem_u32(S.dza), gta = smem_u32(S.gta), gtb = smem_u32(S.gtb);
+  float v[64];
+  // ---- layer 1: z1 = x'·W1ᵀ + b1, a1 = GELU(z1) (bf16 rows for layer 2, bf16 columns for dW2) -------------
+  if (tt_run(S, phase, [&] { tc_mma(S.tmem, umma_desc(xa, 128, 256), umma_desc(w1, 128, 256), 0u); })) {
+    tt_row(S, 0, v);
+#pragma unroll
+    for (int kb = 0; kb < 8; ++kb) {
+      float h[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const float z = v[8 * kb + i] + W->b1[8 * kb + i];
+        S.z1[r * MLP_H + 8 * kb + i] = z;
+        h[i] = gelu(z);
+      }
+      const uint4 hp = pack8(h);
+      *reinterpret_cast<uint4*>(S.ha + cm(r, 8 * kb, 64)) = hp;
+      const __nv_bfloat16* hb = reinterpret_cast<const __nv_bfloat16*>(&hp);
+#pragma unroll
+      for (int i = 0; i < 8; ++i) S.gta[cm(8 * kb + i, r, ROWS)] = hb[i];
+    }
+  }
+  // ---- layer 2 and the output: y = Σ GELU(z2)·w3 + b3, dy, dz2 = dy·w3·GELU'(z2) --------------------------
+  if (tt_run(S, phase, [&] {
+        for (int kt = 0; kt < 4; ++kt)
+          tc_mma(S.tmem + 64, umma_desc(ha + 256 * kt, 128, 1024), umma_desc(w2t + 256 * kt, 128, 1024), kt > 0 ? 1u : 0u);
+      })) {
+    tt_row(S, 64, v);
+    float y = 0.0f;
+#pragma unroll
+    for (int o = 0; o < MLP_H; ++o) {
+      v[o] += W->b2[o];
+      S.z2[r * MLP_H + o] = v[o];
+      y += gelu(v[o]) * W->w3[o];
+    }
+    const float e = valid ? (y + W->b3 - tn) : 0.0f;
+    const float dy = 2.0f * e / denom;
+    S.dy[r] = dy;
+    float e2 = e * e;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) e2 += __shfl_xor_sync(SPH_FULL_MASK, e2, o);
+    if (lane == 0) atomicAdd(loss, e2);
+#pragma unroll
+    for (int ob = 0; ob < 8; ++ob) {
+      float dz[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) dz[i] = dy * W->w3[8 * ob + i] * gelu_d(v[8 * ob + i]);
+      const uint4 dp = pack8(dz);
+      *reinterpret_cast<uint4*>(S.dza + cm(r, 8 * ob, 64)) = dp;
+      const __nv_bfloat16* db = reinterpret_cast<const __nv_bfloat16*>(&dp);
+#pragma unroll
+      for (int i = 0; i < 8; ++i) S.gtb[cm(8 * ob + i, r, ROWS)] = db[i];
+    }
+  }
+  // ---- da1 = dz2·W2 (D3) and dW2 = a1ᵀ·dz2 (D4, rows 0..63) -------------------------------------------------
+  if (tt_run(S, phase, [&] {
+        for (int kt = 0; kt < 4; ++kt)
+          tc_mma(S.tmem + 128, umma_desc(dza + 256 * kt, 128, 1024), umma_desc(w2b + 256 * kt, 128, 1024),
+                 kt > 0 ? 1u : 0u);
+        for (int kt = 0; kt < 8; ++kt)
+          tc_mma(S.tmem + 192, umma_desc(gta + 256 * kt, 128, 2048), umma_desc(gtb + 256 * kt, 128, 2048),
+                 kt > 0 ? 1u : 0u);
+      })) {
+    if (r < MLP_H) {  // warps 0 and 1: the rows of dW2 (input i = r)
+      tt_row(S, 192, v);
+#pragma unroll 8
+      for (int o = 0; o < MLP_H; ++o) atomicAdd(&grad[MLP_W2 + r * MLP_H + o], v[o]);
+    }
+    tt_row(S, 128, v);
+#pragma unroll
+    for (int i = 0; i < MLP_H; ++i) {
+      const float dz = v[i] * gelu_d(S.z1[r * MLP_H + i]);
+      S.z1[r * MLP_H + i] = dz;
+      S.gtb[cm(i, r, ROWS)] = __float2bfloat16_rn(dz);
+    }
+#pragma unroll
+    for (int k = 0; k < 16; ++k) S.gta[cm(k, r, ROWS)] = S.xa[cm(r, k, 16)];
+  }
+  // ---- dW1 = x'ᵀ·dz1 (D5 in D1's columns, rows k < 8) --------------------------------------------------------
+  if (tt_run(S, phase, [&] {
+        for (int kt = 0; kt < 8; ++kt)
+          tc_mma(S.tmem, umma_desc(gta + 256 * kt, 128, 2048), umma_desc(gtb + 256 * kt, 128, 2048), kt > 0 ? 1u : 0u);
+      })) {
+    if (r < 32) {
+      tt_row(S, 0, v);
+      if (r < MLP_IN)
+#pragma unroll 8
+        for (int i = 0; i < MLP_H; ++i) atomicAdd(&grad[MLP_W1 + r * MLP_H + i], v[i]);
+    }
+  }
+  // ---- the bias and W3 gradients: column sums over the tile ---------------------------------------------------
+  __syncthreads();
+  if (S.ok) {
+    const int col = r & 63, half = r >> 6;
+    float gw3 = 0.f, gb2 = 0.f, gb1 = 0.f;
+    for (int rr = half * 64; rr < half * 64 + 64; ++rr) {
+      const float z = S.z2[rr * MLP_H + col], d = S.dy[rr];
+      gw3 += d * gelu(z);
+      gb2 += d * W->w3[col] * gelu_d(z);
+      gb1 += S.z1[rr * MLP_H + col];
+    }
+    atomicAdd(&grad[MLP_W3 + col], gw3);
+    atomicAdd(&grad[MLP_B2 + col], gb2);
+    atomicAdd(&grad[MLP_B1 + col], gb1);
+    if (r == 0) {
+      float gb3 = 0.f;
+      for (int rr = 0; rr < ROWS; ++rr) gb3 += S.dy[rr];
+      atomicAdd(&grad[MLP_B3], gb3);
+    }
+  }
+  // ---- tear-down: after a timeout wait (bounded) for what was issued, then free the tensor memory -------------
+  const bool failed = !S.ok;
+  if (failed) mbar_wait(smem_u32(&S.mbar), phase);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (r < 32)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(S.tmem), "r"(TT_COLS) : "memory");
+  if (failed && r == 0) atomicOr(err, 1u);
+}
+
 // ---- training: forward + backward of one 128-sample tile ----------------------------------------------
 struct TrainSmem {
   FwdW w;
@@ -642,10 +860,10 @@ int launch_mlp_forward(const MlpPacked* w, const float* x, int n, float* out, un
 }
 
 int launch_mlp_train_batch(const MlpPacked* w, const float* x, const float* t, const unsigned* idx, int m,
-                           float denom, float* grad, float* loss, cudaStream_t s) {
+                           float denom, float* grad, float* loss, unsigned* err, cudaStream_t s) {
   static std::atomic<unsigned long long> attr{0};
-  smem_limit_per_device(k_mlp_train, (int)sizeof(TrainSmem), attr);
-  k_mlp_train<<<(m + ROWS - 1) / ROWS, ROWS, sizeof(TrainSmem), s>>>(w, x, t, idx, m, denom, grad, loss);
+  smem_limit_per_device(k_mlp_train_tc, (int)sizeof(TrainTcSmem), attr);
+  k_mlp_train_tc<<<(m + ROWS - 1) / ROWS, ROWS, sizeof(TrainTcSmem), s>>>(w, x, t, idx, m, denom, grad, loss, err);
   return 1;
 }
 
@@ -727,6 +945,7 @@ sph_status sph_mlp_grad(const float* params, const float* x, const float* t, uin
   float* dt = b.get<float>(n);
   unsigned* idx = b.get<unsigned>(n);
   float* dg = b.get<float>(MLP_TRAIN + 1);  // gradient, then the summed squared error
+  unsigned* flag = b.get<unsigned>(1);
   if (b.err != cudaSuccess) return status_of(b.err);
   std::vector<unsigned> id(n);
   for (uint32_t i = 0; i < n; ++i) id[i] = i;
@@ -735,13 +954,17 @@ sph_status sph_mlp_grad(const float* params, const float* x, const float* t, uin
   if (e == cudaSuccess) e = cudaMemcpy(dt, t, (size_t)n * sizeof(float), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(idx, id.data(), (size_t)n * sizeof(unsigned), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemset(dg, 0, (MLP_TRAIN + 1) * sizeof(float));
+  if (e == cudaSuccess) e = cudaMemset(flag, 0, sizeof(unsigned));
   if (e != cudaSuccess) return status_of(e);
   launch_mlp_pack(dp, w, 0);
-  launch_mlp_train_batch(w, dx, dt, idx, (int)n, (float)n, dg, dg + MLP_TRAIN, 0);
+  launch_mlp_train_batch(w, dx, dt, idx, (int)n, (float)n, dg, dg + MLP_TRAIN, flag, 0);
   e = cudaGetLastError();
   std::vector<float> h(MLP_TRAIN + 1);
   if (e == cudaSuccess) e = cudaMemcpy(h.data(), dg, h.size() * sizeof(float), cudaMemcpyDeviceToHost);
+  unsigned timeout = 0;
+  if (e == cudaSuccess) e = cudaMemcpy(&timeout, flag, sizeof(unsigned), cudaMemcpyDeviceToHost);
   if (e != cudaSuccess) return status_of(e);
+  if (timeout) return SPH_ERR_TIMEOUT;
   std::memcpy(grad, h.data(), MLP_TRAIN * sizeof(float));
   *loss = h[MLP_TRAIN] / (float)n;
   return SPH_OK;
@@ -760,12 +983,14 @@ sph_status sph_mlp_train(float* params, const float* x, const float* t, uint32_t
   float* dm = b.get<float>(MLP_TRAIN);
   float* dv = b.get<float>(MLP_TRAIN);
   float* dl = b.get<float>(1);
+  unsigned* flag = b.get<unsigned>(1);
   if (b.err != cudaSuccess) return status_of(b.err);
   cudaError_t e = cudaMemcpy(dp, params, MLP_TOTAL * sizeof(float), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(dx, x, (size_t)n * MLP_IN * sizeof(float), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(dt, t, (size_t)n * sizeof(float), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemset(dm, 0, MLP_TRAIN * sizeof(float));
   if (e == cudaSuccess) e = cudaMemset(dv, 0, MLP_TRAIN * sizeof(float));
+  if (e == cudaSuccess) e = cudaMemset(flag, 0, sizeof(unsigned));
   if (e != cudaSuccess) return status_of(e);
   std::vector<unsigned> perm(n);
   for (uint32_t i = 0; i < n; ++i) perm[i] = i;
@@ -782,13 +1007,16 @@ sph_status sph_mlp_train(float* params, const float* x, const float* t, uint32_t
     for (uint32_t off = 0; off < n; off += cfg->batch) {
       const uint32_t m = n - off < cfg->batch ? n - off : cfg->batch;
       cudaMemsetAsync(dg, 0, MLP_TRAIN * sizeof(float), 0);
-      launch_mlp_train_batch(w, dx, dt, idx + off, (int)m, (float)m, dg, dl, 0);
+      launch_mlp_train_batch(w, dx, dt, idx + off, (int)m, (float)m, dg, dl, flag, 0);
       launch_mlp_adam(dp, dg, dm, dv, ++step, cfg->lr, b1, b2, eps, cfg->weight_decay, 0);
       launch_mlp_pack(dp, w, 0);
     }
     float l = 0.0f;
+    unsigned timeout = 0;
     e = cudaMemcpy(&l, dl, sizeof(float), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(&timeout, flag, sizeof(unsigned), cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return status_of(e);
+    if (timeout) return SPH_ERR_TIMEOUT;
     if (loss_per_epoch) loss_per_epoch[ep] = l / (float)n;
   }
   e = cudaMemcpy(params, dp, MLP_TRAIN * sizeof(float), cudaMemcpyDeviceToHost);

@@ -49,11 +49,11 @@ int launch_mlp_propose(const Dev& d, const MlpPacked* w, const MlpFeatureArgs& f
 // wait gave up (the outputs are then NaN).
 int launch_mlp_forward(const MlpPacked* w, const float* x, int n, float* out, unsigned* err, cudaStream_t s);
 
-// One training minibatch: forward + backward over rows idx[0..m) of (x, t), gradients of the mean squared
-// error on the normalised target (divided by `denom`) accumulated into grad[4801], the summed squared error
-// into *loss.
+// One training minibatch on tcgen05: forward + backward over rows idx[0..m) of (x, t), gradients of the mean
+// squared error on the normalised target (divided by `denom`) accumulated into grad[4801], the summed squared
+// error into *loss; *err |= 1 if a tensor-core barrier wait gave up (the tile's gradients are then incomplete).
 int launch_mlp_train_batch(const MlpPacked* w, const float* x, const float* t, const unsigned* idx, int m,
-                           float denom, float* grad, float* loss, cudaStream_t s);
+                           float denom, float* grad, float* loss, unsigned* err, cudaStream_t s);
 
 // Adam on the trainable parameters (FP32 master copy), step count `step` (1-based).
 int launch_mlp_adam(float* params, const float* grad, float* m, float* v, int step, float lr, float b1, float b2,
