@@ -1,15 +1,8 @@
 // Learned smoothing-length MLP on the tensor cores: 8 → 64 → 64 → 1 with GELU, BF16 operands and FP32
-// accumulation. Inference (the in-step proposal and the standalone forward) runs on tcgen05: the two hidden
-// layers are M = 128 × N = 64 tcgen05.mma tiles with the accumulators in tensor memory (see the inference
-// section). Training uses mma.sync.m16n8k16 tiles: a CTA of 4 warps holds 128 samples, each warp owns 32 rows
-// (two 16-row MMA tiles) through both hidden layers, and the backward pass computes the weight gradients as
-// GEMMs over the CTA's samples; Adam updates an FP32 master copy.
-//
-// Fragment layouts of m16n8k16 (row.col): lane = 4·g + q. A (16×16, row-major): a0 = (g, 2q..2q+1),
-// a1 = (g+8, 2q..), a2 = (g, 8+2q..), a3 = (g+8, 8+2q..). B (16×8, K×N): b0 = (k 2q..2q+1, n g),
-// b1 = (k 8+2q.., n g). C (16×8): c0,c1 = (g, 2q..2q+1), c2,c3 = (g+8, 2q..2q+1). Every operand is kept in
-// shared memory with its K index contiguous, so each fragment register is one aligned 32-bit load; row
-// strides of 24/72/136 elements put the 8 rows a fragment touches in distinct banks.
+// accumulation. Inference (the in-step proposal and the standalone forward) and training both run on tcgen05:
+// M = 128 × N = 64 tcgen05.mma tiles issued by one thread, operands in shared memory in the canonical
+// no-swizzle K-major layout, accumulators in tensor memory (see the inference and training sections). Training
+// computes the weight gradients as tcgen05 GEMMs over a tile's 128 samples; Adam updates an FP32 master copy.
 #include <cstdint>
 #include <cstring>
 #include <vector>
@@ -21,130 +14,14 @@ namespace sphb {
 
 namespace {
 
-constexpr int XS = 24;    // row stride of K=16 operands
-constexpr int HS = 72;    // row stride of K=64 operands
-constexpr int TS = 136;   // row stride of K=128 (sample-major) operands
 constexpr int ROWS = 128;
 // Largest proposed change of log h: an outlier proposal stays within reach of the fallback's Newton steps
 // (±20 % each, inside the list skin around the proposal).
 constexpr float kMaxStep = 0.03f;
 
-__device__ __forceinline__ unsigned ld32(const __nv_bfloat16* p) { return *reinterpret_cast<const unsigned*>(p); }
-__device__ __forceinline__ void st32(__nv_bfloat16* p, float a, float b) {
-  *reinterpret_cast<__nv_bfloat162*>(p) = __floats2bfloat162_rn(a, b);
-}
-__device__ __forceinline__ void mma16816(float c[4], const unsigned a[4], unsigned b0, unsigned b1) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-      "{%0,%1,%2,%3};\n"
-      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
-      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
-}
 __device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
 __device__ __forceinline__ float gelu_d(float z) {
   return 0.5f * (1.0f + erff(z * 0.70710678118654752f)) + z * expf(-0.5f * z * z) * 0.39894228040143268f;
-}
-
-// Shared-memory weights of the forward pass.
-struct FwdW {
-  __nv_bfloat16 w1t[MLP_H * XS];
-  __nv_bfloat16 w2t[MLP_H * HS];
-  float b1[MLP_H], b2[MLP_H], w3[MLP_H];
-};
-
-__device__ void load_fwd(const MlpPacked* __restrict__ W, FwdW& s) {
-  for (int i = threadIdx.x; i < MLP_H * 16; i += blockDim.x) s.w1t[(i >> 4) * XS + (i & 15)] = W->w1t[i];
-  for (int i = threadIdx.x; i < MLP_H * MLP_H; i += blockDim.x) s.w2t[(i >> 6) * HS + (i & 63)] = W->w2t[i];
-  for (int i = threadIdx.x; i < MLP_H; i += blockDim.x) {
-    s.b1[i] = W->b1[i];
-    s.b2[i] = W->b2[i];
-    s.w3[i] = W->w3[i];
-  }
-}
-
-// Forward pass of one warp's 32 rows [r0, r0+32): x (bf16, [row][XS]) → h1 (bf16, [row][HS]) → y[row]
-// (FP32, without b3). Optionally keeps z1, z2 (FP32, [row][64]) and h1 transposed ([col][TS]).
-__device__ void mlp_rows(int r0, const __nv_bfloat16* sx, __nv_bfloat16* sh1, const FwdW& w, float* sy,
-                         float* z1o, float* z2o, __nv_bfloat16* h1t) {
-  const int lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
-#pragma unroll
-  for (int mt = 0; mt < 2; ++mt) {
-    const int ra = r0 + mt * 16;
-    unsigned a[4];
-    a[0] = ld32(sx + (ra + g) * XS + 2 * q);
-    a[1] = ld32(sx + (ra + g + 8) * XS + 2 * q);
-    a[2] = ld32(sx + (ra + g) * XS + 8 + 2 * q);
-    a[3] = ld32(sx + (ra + g + 8) * XS + 8 + 2 * q);
-#pragma unroll
-    for (int nt = 0; nt < 8; ++nt) {
-      const int c0 = nt * 8 + 2 * q;
-      float c[4] = {w.b1[c0], w.b1[c0 + 1], w.b1[c0], w.b1[c0 + 1]};
-      mma16816(c, a, ld32(w.w1t + (nt * 8 + g) * XS + 2 * q), ld32(w.w1t + (nt * 8 + g) * XS + 8 + 2 * q));
-      if (z1o) {
-        z1o[(ra + g) * MLP_H + c0] = c[0];
-        z1o[(ra + g) * MLP_H + c0 + 1] = c[1];
-        z1o[(ra + g + 8) * MLP_H + c0] = c[2];
-        z1o[(ra + g + 8) * MLP_H + c0 + 1] = c[3];
-      }
-      const float h0 = gelu(c[0]), h1 = gelu(c[1]), h2 = gelu(c[2]), h3 = gelu(c[3]);
-      st32(sh1 + (ra + g) * HS + c0, h0, h1);
-      st32(sh1 + (ra + g + 8) * HS + c0, h2, h3);
-      if (h1t) {
-        h1t[c0 * TS + ra + g] = __float2bfloat16_rn(h0);
-        h1t[(c0 + 1) * TS + ra + g] = __float2bfloat16_rn(h1);
-        h1t[c0 * TS + ra + g + 8] = __float2bfloat16_rn(h2);
-        h1t[(c0 + 1) * TS + ra + g + 8] = __float2bfloat16_rn(h3);
-      }
-    }
-  }
-  __syncwarp();
-#pragma unroll
-  for (int mt = 0; mt < 2; ++mt) {
-    const int ra = r0 + mt * 16;
-    unsigned a[4][4];
-#pragma unroll
-    for (int kt = 0; kt < 4; ++kt) {
-      a[kt][0] = ld32(sh1 + (ra + g) * HS + kt * 16 + 2 * q);
-      a[kt][1] = ld32(sh1 + (ra + g + 8) * HS + kt * 16 + 2 * q);
-      a[kt][2] = ld32(sh1 + (ra + g) * HS + kt * 16 + 8 + 2 * q);
-      a[kt][3] = ld32(sh1 + (ra + g + 8) * HS + kt * 16 + 8 + 2 * q);
-    }
-    float y0 = 0.0f, y1 = 0.0f;
-#pragma unroll
-    for (int nt = 0; nt < 8; ++nt) {
-      const int c0 = nt * 8 + 2 * q;
-      float c[4] = {w.b2[c0], w.b2[c0 + 1], w.b2[c0], w.b2[c0 + 1]};
-      const __nv_bfloat16* bp = w.w2t + (nt * 8 + g) * HS + 2 * q;
-#pragma unroll
-      for (int kt = 0; kt < 4; ++kt) mma16816(c, a[kt], ld32(bp + kt * 16), ld32(bp + kt * 16 + 8));
-      if (z2o) {
-        z2o[(ra + g) * MLP_H + c0] = c[0];
-        z2o[(ra + g) * MLP_H + c0 + 1] = c[1];
-        z2o[(ra + g + 8) * MLP_H + c0] = c[2];
-        z2o[(ra + g + 8) * MLP_H + c0 + 1] = c[3];
-      }
-      y0 += gelu(c[0]) * w.w3[c0] + gelu(c[1]) * w.w3[c0 + 1];
-      y1 += gelu(c[2]) * w.w3[c0] + gelu(c[3]) * w.w3[c0 + 1];
-    }
-    y0 += __shfl_xor_sync(SPH_FULL_MASK, y0, 1);
-    y0 += __shfl_xor_sync(SPH_FULL_MASK, y0, 2);
-    y1 += __shfl_xor_sync(SPH_FULL_MASK, y1, 1);
-    y1 += __shfl_xor_sync(SPH_FULL_MASK, y1, 2);
-    if (q == 0) {
-      sy[ra + g] = y0;
-      sy[ra + g + 8] = y1;
-    }
-  }
-  __syncwarp();
-}
-
-// One row of normalised features, rounded to bf16, into the A operand (K padded to 16 with zeros).
-__device__ __forceinline__ void put_row(__nv_bfloat16* sx, int r, const float f[MLP_IN], const MlpPacked* W) {
-#pragma unroll
-  for (int k = 0; k < MLP_IN; k += 2)
-    st32(sx + r * XS + k, (f[k] - W->xm[k]) * W->xs[k], (f[k + 1] - W->xm[k + 1]) * W->xs[k + 1]);
-#pragma unroll
-  for (int k = MLP_IN; k < 16; k += 2) st32(sx + r * XS + k, 0.0f, 0.0f);
 }
 
 // ---- feature definition (the solver's state at the start of the step's drift) ---------------------------
@@ -629,159 +506,6 @@ __global__ void __launch_bounds__(ROWS) k_mlp_train_tc(const MlpPacked* __restri
   if (r < 32)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(S.tmem), "r"(TT_COLS) : "memory");
   if (failed && r == 0) atomicOr(err, 1u);
-}
-
-// ---- training: forward + backward of one 128-sample tile ----------------------------------------------
-struct TrainSmem {
-  FwdW w;
-  __nv_bfloat16 w2[MLP_H * HS];      // W2 [in][out] (B operand of dh1 = dz2 W2ᵀ)
-  __nv_bfloat16 sx[ROWS * XS];       // x' [row][k]
-  __nv_bfloat16 sxt[16 * TS];        // x' [k][row]
-  __nv_bfloat16 sh1[ROWS * HS];      // a1 [row][i]
-  __nv_bfloat16 sh1t[MLP_H * TS];    // a1 [i][row]
-  __nv_bfloat16 dz2[ROWS * HS];      // dz2 [row][j]
-  __nv_bfloat16 dz2t[MLP_H * TS];    // dz2 [j][row]
-  __nv_bfloat16 dz1t[MLP_H * TS];    // dz1 [i][row]
-  float z1[ROWS * MLP_H];            // z1, then dz1 (FP32)
-  float z2[ROWS * MLP_H];
-  float y[ROWS], dy[ROWS];
-};
-
-__global__ void __launch_bounds__(ROWS) k_mlp_train(const MlpPacked* __restrict__ W, const float* __restrict__ x,
-                                                   const float* __restrict__ tgt, const unsigned* __restrict__ idx,
-                                                   int m, float denom, float* __restrict__ grad,
-                                                   float* __restrict__ loss) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  TrainSmem& S = *reinterpret_cast<TrainSmem*>(smem_raw);
-  load_fwd(W, S.w);
-  for (int i = threadIdx.x; i < MLP_H * MLP_H; i += ROWS) S.w2[(i >> 6) * HS + (i & 63)] = W->w2[i];
-  const int r = threadIdx.x, wp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
-  const int s = blockIdx.x * ROWS + r;
-  const bool valid = s < m;
-  const unsigned j = valid ? idx[s] : 0u;
-  float f[MLP_IN] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-  float tn = 0.0f;
-  if (valid) {
-#pragma unroll
-    for (int k = 0; k < MLP_IN; ++k) f[k] = x[(size_t)j * MLP_IN + k];
-    tn = (tgt[j] - W->ym) / W->ys;
-  }
-  put_row(S.sx, r, f, W);
-#pragma unroll
-  for (int k = 0; k < 16; ++k) S.sxt[k * TS + r] = S.sx[r * XS + k];
-  __syncthreads();
-  mlp_rows(wp * 32, S.sx, S.sh1, S.w, S.y, S.z1, S.z2, S.sh1t);
-  __syncthreads();
-  // output error: d(loss)/dy with loss = Σ (y − t)² / denom
-  {
-    const float e = valid ? (S.y[r] + W->b3 - tn) : 0.0f;
-    S.dy[r] = 2.0f * e / denom;
-    float e2 = e * e;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) e2 += __shfl_xor_sync(SPH_FULL_MASK, e2, o);
-    if (lane == 0) atomicAdd(loss, e2);
-  }
-  __syncthreads();
-  // dW3, db2 and dz2 (= dy w3 gelu'(z2)), one column per thread over half the rows
-  {
-    const int col = r & 63, h = r >> 6;
-    float gw3 = 0.f, gb2 = 0.f;
-    for (int rr = h * 64; rr < h * 64 + 64; ++rr) {
-      const float z = S.z2[rr * MLP_H + col];
-      gw3 += S.dy[rr] * gelu(z);
-      const float dz = S.dy[rr] * S.w.w3[col] * gelu_d(z);
-      gb2 += dz;
-      const __nv_bfloat16 b = __float2bfloat16_rn(dz);
-      S.dz2[rr * HS + col] = b;
-      S.dz2t[col * TS + rr] = b;
-    }
-    atomicAdd(&grad[MLP_W3 + col], gw3);
-    atomicAdd(&grad[MLP_B2 + col], gb2);
-    if (r == 0) {
-      float gb3 = 0.f;
-      for (int rr = 0; rr < ROWS; ++rr) gb3 += S.dy[rr];
-      atomicAdd(&grad[MLP_B3], gb3);
-    }
-  }
-  __syncthreads();
-  // dW2[i][j] = Σ_r a1[r][i] dz2[r][j]: warp wp takes rows i in [16wp, 16wp+16), all 8 column tiles
-#pragma unroll 1
-  for (int nt = 0; nt < 8; ++nt) {
-    float c[4] = {0.f, 0.f, 0.f, 0.f};
-#pragma unroll
-    for (int kt = 0; kt < 8; ++kt) {
-      unsigned a[4];
-      a[0] = ld32(S.sh1t + (16 * wp + g) * TS + kt * 16 + 2 * q);
-      a[1] = ld32(S.sh1t + (16 * wp + g + 8) * TS + kt * 16 + 2 * q);
-      a[2] = ld32(S.sh1t + (16 * wp + g) * TS + kt * 16 + 8 + 2 * q);
-      a[3] = ld32(S.sh1t + (16 * wp + g + 8) * TS + kt * 16 + 8 + 2 * q);
-      const __nv_bfloat16* bp = S.dz2t + (nt * 8 + g) * TS + kt * 16 + 2 * q;
-      mma16816(c, a, ld32(bp), ld32(bp + 8));
-    }
-    const int i0 = 16 * wp + g, c0 = nt * 8 + 2 * q;
-    atomicAdd(&grad[MLP_W2 + i0 * MLP_H + c0], c[0]);
-    atomicAdd(&grad[MLP_W2 + i0 * MLP_H + c0 + 1], c[1]);
-    atomicAdd(&grad[MLP_W2 + (i0 + 8) * MLP_H + c0], c[2]);
-    atomicAdd(&grad[MLP_W2 + (i0 + 8) * MLP_H + c0 + 1], c[3]);
-  }
-  // da1 = dz2 W2ᵀ for this warp's rows, then dz1 = da1 gelu'(z1) (FP32 into z1, bf16 transposed into dz1t)
-#pragma unroll 1
-  for (int mt = 0; mt < 2; ++mt) {
-    const int ra = wp * 32 + mt * 16;
-    unsigned a[4][4];
-#pragma unroll
-    for (int kt = 0; kt < 4; ++kt) {
-      a[kt][0] = ld32(S.dz2 + (ra + g) * HS + kt * 16 + 2 * q);
-      a[kt][1] = ld32(S.dz2 + (ra + g + 8) * HS + kt * 16 + 2 * q);
-      a[kt][2] = ld32(S.dz2 + (ra + g) * HS + kt * 16 + 8 + 2 * q);
-      a[kt][3] = ld32(S.dz2 + (ra + g + 8) * HS + kt * 16 + 8 + 2 * q);
-    }
-#pragma unroll
-    for (int nt = 0; nt < 8; ++nt) {
-      float c[4] = {0.f, 0.f, 0.f, 0.f};
-      const __nv_bfloat16* bp = S.w2 + (nt * 8 + g) * HS + 2 * q;
-#pragma unroll
-      for (int kt = 0; kt < 4; ++kt) mma16816(c, a[kt], ld32(bp + kt * 16), ld32(bp + kt * 16 + 8));
-      const int c0 = nt * 8 + 2 * q;
-      const int rows[2] = {ra + g, ra + g + 8};
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-#pragma unroll
-        for (int e = 0; e < 2; ++e) {
-          float* zp = &S.z1[rows[h] * MLP_H + c0 + e];
-          const float dz = c[2 * h + e] * gelu_d(*zp);
-          *zp = dz;
-          S.dz1t[(c0 + e) * TS + rows[h]] = __float2bfloat16_rn(dz);
-        }
-      }
-    }
-  }
-  __syncthreads();
-  // db1: column sums of dz1
-  if (r < MLP_H) {
-    float gb1 = 0.f;
-    for (int rr = 0; rr < ROWS; ++rr) gb1 += S.z1[rr * MLP_H + r];
-    atomicAdd(&grad[MLP_B1 + r], gb1);
-  }
-  // dW1[k][i] = Σ_r x'[r][k] dz1[r][i]: one 16-row tile (k, padded), warp wp takes column tiles 2wp, 2wp+1
-#pragma unroll 1
-  for (int u = 0; u < 2; ++u) {
-    const int nt = 2 * wp + u;
-    float c[4] = {0.f, 0.f, 0.f, 0.f};
-#pragma unroll
-    for (int kt = 0; kt < 8; ++kt) {
-      unsigned a[4];
-      a[0] = ld32(S.sxt + g * TS + kt * 16 + 2 * q);
-      a[1] = ld32(S.sxt + (g + 8) * TS + kt * 16 + 2 * q);
-      a[2] = ld32(S.sxt + g * TS + kt * 16 + 8 + 2 * q);
-      a[3] = ld32(S.sxt + (g + 8) * TS + kt * 16 + 8 + 2 * q);
-      const __nv_bfloat16* bp = S.dz1t + (nt * 8 + g) * TS + kt * 16 + 2 * q;
-      mma16816(c, a, ld32(bp), ld32(bp + 8));
-    }
-    const int c0 = nt * 8 + 2 * q;  // rows g < 8 are the real inputs; rows g + 8 are the K padding
-    atomicAdd(&grad[MLP_W1 + g * MLP_H + c0], c[0]);
-    atomicAdd(&grad[MLP_W1 + g * MLP_H + c0 + 1], c[1]);
-  }
 }
 
 __global__ void k_mlp_pack(const float* __restrict__ P, MlpPacked* __restrict__ o) {

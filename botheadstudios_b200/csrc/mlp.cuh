@@ -15,7 +15,7 @@ constexpr int MLP_W1 = 0, MLP_B1 = MLP_W1 + MLP_IN * MLP_H, MLP_W2 = MLP_B1 + ML
               MLP_XS = MLP_XM + MLP_IN, MLP_YM = MLP_XS + MLP_IN, MLP_YS = MLP_YM + 1, MLP_TOTAL = MLP_YS + 1;
 static_assert(MLP_TRAIN == 4801 && MLP_TOTAL == 4819, "parameter block");
 
-// Weights as the kernels read them: BF16 matrices in the layouts the mma fragments load from (K padded to
+// Weights as the kernels read them: BF16 matrices row by row (the kernels copy them into the tcgen05 operand layout; K padded to
 // 16 for the first layer), FP32 biases and normalisation, W3 rounded to BF16 and held as FP32.
 struct MlpPacked {
   __nv_bfloat16 w1t[MLP_H * 16];     // [out][in], in 8..15 zero
