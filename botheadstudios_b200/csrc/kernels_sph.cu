@@ -27,24 +27,25 @@ __device__ __forceinline__ float pair_h(float hi, float hj) { return fmul(0.5f, 
 // then all of its neighbour records, before any is used, so each thread keeps kGather gathers in flight
 // instead of one dependent chain; the next chunk's indices are requested before this chunk's records, so the
 // list stream (HBM) overlaps the record gathers (mostly L1/L2) and the arithmetic. `lst` is the particle's
-// first list slot (entries 32 apart, interleaved); slots past the count read the particle itself (harmless
-// filler, never summed). The lists are read once per pass and streamed past the cache (evict-first), so they
-// do not push the neighbours' records out of L2.
+// first list slot (entries 32 apart, interleaved); slots past the count read the sentinel record `sent` (a
+// massless particle outside every support), so a pair is evaluated without testing the count or the support
+// (kern_pair_bf vanishes outside it). The lists are read once per pass and streamed past the cache
+// (evict-first), so they do not push the neighbours' records out of L2.
 constexpr int kGather = 4;
 template <int G>
-__device__ __forceinline__ void list_chunk(const unsigned* __restrict__ lst, unsigned k0, unsigned c, unsigned self,
+__device__ __forceinline__ void list_chunk(const unsigned* __restrict__ lst, unsigned k0, unsigned c, unsigned sent,
                                            unsigned j[G]) {
 #pragma unroll
-  for (int u = 0; u < G; ++u) j[u] = k0 + u < c ? __ldcs(&lst[(size_t)(k0 + u) * 32u]) : self;
+  for (int u = 0; u < G; ++u) j[u] = k0 + u < c ? __ldcs(&lst[(size_t)(k0 + u) * 32u]) : sent;
 }
 // Records of the chunk whose indices are in `jn` (k0 = its first slot); on return jn holds the next chunk's.
 __device__ __forceinline__ void gather_pos_mass(const State& st, const unsigned* __restrict__ lst, unsigned k0,
-                                                unsigned c, unsigned self, unsigned jn[kGather],
+                                                unsigned c, unsigned sent, unsigned jn[kGather],
                                                 float4 pj[kGather], float mj[kGather]) {
   unsigned j[kGather];
 #pragma unroll
   for (int u = 0; u < kGather; ++u) j[u] = jn[u];
-  list_chunk<kGather>(lst, k0 + kGather, c, self, jn);
+  list_chunk<kGather>(lst, k0 + kGather, c, sent, jn);
 #pragma unroll
   for (int u = 0; u < kGather; ++u) {
     pj[u] = st.pos_h[j[u]];
@@ -68,8 +69,9 @@ __device__ __forceinline__ float4 eos_record(const Eos* __restrict__ eos, unsign
 
 template <int KERNEL>
 __global__ void k_density_eos(int n, State st, const unsigned* __restrict__ nbr,
-                              const unsigned* __restrict__ nbr_cnt, unsigned cap, const Eos* __restrict__ eos,
-                              const DevParams* __restrict__ P, float* __restrict__ rho, float4* __restrict__ fdata) {
+                              const unsigned* __restrict__ nbr_cnt, unsigned cap, unsigned sent,
+                              const Eos* __restrict__ eos, const DevParams* __restrict__ P,
+                              float* __restrict__ rho, float4* __restrict__ fdata) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
   const float4 pi = st.pos_h[t];
@@ -80,21 +82,17 @@ __global__ void k_density_eos(int n, State st, const unsigned* __restrict__ nbr,
   const unsigned c = min(nbr_cnt[t], cap);
   const unsigned* lst = nbr + nbr_slot((unsigned)t, 0u, cap);
   unsigned jn[kGather];
-  list_chunk<kGather>(lst, 0u, c, (unsigned)t, jn);
+  list_chunk<kGather>(lst, 0u, c, sent, jn);
   for (unsigned k0 = 0; k0 < c; k0 += kGather) {
     float4 pj[kGather];
     float mj[kGather];
-    gather_pos_mass(st, lst, k0, c, (unsigned)t, jn, pj, mj);
+    gather_pos_mass(st, lst, k0, c, sent, jn, pj, mj);
 #pragma unroll
     for (int u = 0; u < kGather; ++u) {
-      if (k0 + u >= c) break;
       float ri;
       const float r = pair_r(pi, pj[u], ri);
-      const float hij = pair_h(pi.w, pj[u].w);
-      if (r < hij) {
-        kern_pair<KERNEL>(r, hij, w, dwdr, dwdh);
-        r_i += mj[u] * w;
-      }
+      kern_pair_bf<KERNEL>(r, pair_h(pi.w, pj[u].w), w, dwdr, dwdh);
+      r_i += mj[u] * w;
     }
   }
   rho[t] = r_i;
@@ -104,9 +102,11 @@ __global__ void k_density_eos(int n, State st, const unsigned* __restrict__ nbr,
 int launch_density_eos(const Dev& d, const Cfg& c, cudaStream_t s) {
   const int blocks = (d.n + c.blk - 1) / c.blk;
   if (c.kernel == 1)
-    k_density_eos<1><<<blocks, c.blk, 0, s>>>(d.n, d.s(), d.nbr, d.nbr_cnt, d.nbr_cap, d.eos, d.P, d.rho, d.fdata);
+    k_density_eos<1><<<blocks, c.blk, 0, s>>>(d.n, d.s(), d.nbr, d.nbr_cnt, d.nbr_cap, d.sent, d.eos, d.P, d.rho,
+                                              d.fdata);
   else
-    k_density_eos<0><<<blocks, c.blk, 0, s>>>(d.n, d.s(), d.nbr, d.nbr_cnt, d.nbr_cap, d.eos, d.P, d.rho, d.fdata);
+    k_density_eos<0><<<blocks, c.blk, 0, s>>>(d.n, d.s(), d.nbr, d.nbr_cnt, d.nbr_cap, d.sent, d.eos, d.P, d.rho,
+                                              d.fdata);
   return 1;
 }
 
@@ -131,36 +131,34 @@ int launch_eos_only(const Dev& d, cudaStream_t s) {
 // same terms in the same order).
 template <int KERNEL>
 __device__ __forceinline__ void h_sums(int t, const State& st, const unsigned* __restrict__ nbr,
-                                       const unsigned* __restrict__ nbr_cnt, unsigned cap, float& rho,
-                                       float& drho) {
+                                       const unsigned* __restrict__ nbr_cnt, unsigned cap, unsigned sent,
+                                       float& rho, float& drho) {
   const float4 pi = st.pos_h[t];
   const float m = st.mass[t];
   const float h = pi.w;
   float w, dwdr, dwdh;
   kern_pair<KERNEL>(0.0f, h, w, dwdr, dwdh);
   rho = m * w;
-  drho = m * dwdh;
+  const float dself = m * dwdh;
+  float dsum = 0.0f;  // Σ m_j ∂W/∂h_ij; ∂h_ij/∂h_i = ½ is applied once
   const unsigned c = min(nbr_cnt[t], cap);
   const unsigned* lst = nbr + nbr_slot((unsigned)t, 0u, cap);
   unsigned jn[kGather];
-  list_chunk<kGather>(lst, 0u, c, (unsigned)t, jn);
+  list_chunk<kGather>(lst, 0u, c, sent, jn);
   for (unsigned k0 = 0; k0 < c; k0 += kGather) {
     float4 pj[kGather];
     float mj[kGather];
-    gather_pos_mass(st, lst, k0, c, (unsigned)t, jn, pj, mj);
+    gather_pos_mass(st, lst, k0, c, sent, jn, pj, mj);
 #pragma unroll
     for (int u = 0; u < kGather; ++u) {
-      if (k0 + u >= c) break;
       float ri;
       const float r = pair_r(pi, pj[u], ri);
-      const float hij = pair_h(h, pj[u].w);
-      if (r < hij) {
-        kern_pair<KERNEL>(r, hij, w, dwdr, dwdh);
-        rho += mj[u] * w;
-        drho += mj[u] * 0.5f * dwdh;
-      }
+      kern_pair_bf<KERNEL>(r, pair_h(h, pj[u].w), w, dwdr, dwdh);
+      rho += mj[u] * w;
+      dsum += mj[u] * dwdh;
     }
   }
+  drho = dself + 0.5f * dsum;
 }
 
 // The Newton update of h from the residual f = ρ − m(η/h)³, limited to ±20 % and to the list's skin. `res`
@@ -185,7 +183,7 @@ __device__ __forceinline__ float h_newton(float h, float m, float rho, float drh
 
 template <int KERNEL>
 __global__ void k_h_iter(int n, State st, const unsigned* __restrict__ nbr, const unsigned* __restrict__ nbr_cnt,
-                         unsigned cap, const float* __restrict__ h0, float eta, DevParams* P, Seg* __restrict__ segs,
+                         unsigned cap, unsigned sent, const float* __restrict__ h0, float eta, DevParams* P, Seg* __restrict__ segs,
                          float* __restrict__ hnew, int last, const Eos* __restrict__ eos, float* __restrict__ rho_out,
                          float4* __restrict__ fdata) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -193,7 +191,7 @@ __global__ void k_h_iter(int n, State st, const unsigned* __restrict__ nbr, cons
   const unsigned sg = t < n ? st.seg[t] : kNoSeg;
   if (t < n) {
     float rho, drho;
-    h_sums<KERNEL>(t, st, nbr, nbr_cnt, cap, rho, drho);
+    h_sums<KERNEL>(t, st, nbr, nbr_cnt, cap, sent, rho, drho);
     const float m = st.mass[t], h = st.pos_h[t].w;
     float drel;
     float hn = h_newton(h, m, rho, drho, eta, h0[t], segs[sg].skin, res, drel);
@@ -216,7 +214,7 @@ constexpr float kDensityTolFraction = 0.25f;
 template <int KERNEL>
 __global__ void k_h_check(int n, const unsigned* __restrict__ list, const unsigned* __restrict__ list_n, State st,
                           const unsigned* __restrict__ nbr, const unsigned* __restrict__ nbr_cnt, unsigned cap,
-                          const float* __restrict__ h0, float eta, float tol, DevParams* P, Seg* __restrict__ segs,
+                          unsigned sent, const float* __restrict__ h0, float eta, float tol, DevParams* P, Seg* __restrict__ segs,
                           float* __restrict__ hnew, unsigned* __restrict__ next, unsigned* __restrict__ next_n,
                           int last, const Eos* __restrict__ eos, float* __restrict__ rho_out,
                           float4* __restrict__ fdata) {
@@ -233,7 +231,7 @@ __global__ void k_h_check(int n, const unsigned* __restrict__ list, const unsign
     if (i < count) {
       t = list ? (int)list[i] : i;
       float rho, drho, res, drel;
-      h_sums<KERNEL>(t, st, nbr, nbr_cnt, cap, rho, drho);
+      h_sums<KERNEL>(t, st, nbr, nbr_cnt, cap, sent, rho, drho);
       const float m = st.mass[t], h = st.pos_h[t].w;
       const unsigned s = st.seg[t];
       const float hn = h_newton(h, m, rho, drho, eta, h0[t], segs[s].skin, res, drel);
@@ -310,10 +308,10 @@ int launch_h_solve(const Dev& d, const Cfg& c, cudaStream_t s) {
     const int last = it == c.h_iters;
     k_h_reset<<<1, kMaxSegments, 0, s>>>(d.P, d.segs, d.nseg, c.h_iters);
     if (c.kernel == 1)
-      k_h_iter<1><<<blocks, c.blk, 0, s>>>(d.n, d.s(), d.nbr, d.nbr_cnt, d.nbr_cap, d.h0, c.h_eta, d.P, d.segs, d.hnew,
+      k_h_iter<1><<<blocks, c.blk, 0, s>>>(d.n, d.s(), d.nbr, d.nbr_cnt, d.nbr_cap, d.sent, d.h0, c.h_eta, d.P, d.segs, d.hnew,
                                           last, d.eos, d.rho, d.fdata);
     else
-      k_h_iter<0><<<blocks, c.blk, 0, s>>>(d.n, d.s(), d.nbr, d.nbr_cnt, d.nbr_cap, d.h0, c.h_eta, d.P, d.segs, d.hnew,
+      k_h_iter<0><<<blocks, c.blk, 0, s>>>(d.n, d.s(), d.nbr, d.nbr_cnt, d.nbr_cap, d.sent, d.h0, c.h_eta, d.P, d.segs, d.hnew,
                                           last, d.eos, d.rho, d.fdata);
     if (!last) k_h_commit<<<blocks, c.blk, 0, s>>>(d.n, d.s(), d.hnew);
   }
@@ -331,7 +329,7 @@ int launch_h_learned(const Dev& d, const Cfg& c, cudaStream_t s) {
   cudaMemsetAsync(d.pend_n, 0, 2 * sizeof(unsigned), s);
   int launches = 2;
 #define HC_ARGS(list, ln, nx, nxn, last)                                                                   \
-  d.n, list, ln, d.s(), d.nbr, d.nbr_cnt, d.nbr_cap, d.h0, c.h_eta, c.h_tol, d.P, d.segs, d.hnew, nx, nxn, last, \
+  d.n, list, ln, d.s(), d.nbr, d.nbr_cnt, d.nbr_cap, d.sent, d.h0, c.h_eta, c.h_tol, d.P, d.segs, d.hnew, nx, nxn, last, \
       d.eos, d.rho, d.fdata
   if (c.kernel == 1)
     k_h_check<1><<<full, c.blk, 0, s>>>(HC_ARGS(nullptr, nullptr, d.pend[0], d.pend_n, c.h_iters == 0 ? 1 : 0));
@@ -363,9 +361,9 @@ constexpr int kForceGather = 2;  // neighbours of a force chunk (three records e
 
 template <int KERNEL, bool GRAV, bool DIVV>
 __global__ void k_forces(int n, State st, const float4* __restrict__ fdata, const unsigned* __restrict__ nbr,
-                         const unsigned* __restrict__ nbr_cnt, unsigned cap, const float4* __restrict__ grav,
-                         const DevParams* __restrict__ P, Seg* __restrict__ segs, float4* __restrict__ acc,
-                         float* __restrict__ divv) {
+                         const unsigned* __restrict__ nbr_cnt, unsigned cap, unsigned sent,
+                         const float4* __restrict__ grav, const DevParams* __restrict__ P, Seg* __restrict__ segs,
+                         float4* __restrict__ acc, float* __restrict__ divv) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   float sig = __int_as_float(0x7f800000);
   const unsigned sg = t < n ? st.seg[t] : kNoSeg;
@@ -378,7 +376,7 @@ __global__ void k_forces(int n, State st, const float4* __restrict__ fdata, cons
     const unsigned c = min(nbr_cnt[t], cap);
     const unsigned* lst = nbr + nbr_slot((unsigned)t, 0u, cap);
     unsigned jn[kForceGather];
-    list_chunk<kForceGather>(lst, 0u, c, (unsigned)t, jn);
+    list_chunk<kForceGather>(lst, 0u, c, sent, jn);
     for (unsigned k0 = 0; k0 < c; k0 += kForceGather) {
       // a chunk's positions, velocities and force records in flight together, the next chunk's indices
       // requested ahead of them
@@ -386,47 +384,44 @@ __global__ void k_forces(int n, State st, const float4* __restrict__ fdata, cons
       float4 pjs[kForceGather], vjs[kForceGather], fjs[kForceGather];
 #pragma unroll
       for (int u = 0; u < kForceGather; ++u) jj[u] = jn[u];
-      list_chunk<kForceGather>(lst, k0 + kForceGather, c, (unsigned)t, jn);
+      list_chunk<kForceGather>(lst, k0 + kForceGather, c, sent, jn);
 #pragma unroll
       for (int u = 0; u < kForceGather; ++u) {
         pjs[u] = st.pos_h[jj[u]];
         vjs[u] = st.vel_u[jj[u]];
         fjs[u] = fdata[jj[u]];
       }
+      // Branch-free pair: outside the support (and for the sentinel) ∇W = 0; pairs closer than r_min are
+      // left out as the reference leaves them out (∇W zeroed); a receding pair (v_ij·r_ij ≥ 0) has μ = 0 and
+      // so no viscosity.
 #pragma unroll
       for (int u = 0; u < kForceGather; ++u) {
-      if (k0 + u >= c) break;
-      const float4 pj = pjs[u];
-      const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-      const float dd = dx * dx + dy * dy + dz * dz;
-      const float rinv = rsqrt_ftz(dd);
-      const float r = dd > 0.0f ? dd * rinv : 0.0f;
-      const float hij = pair_h(pi.w, pj.w);
-      if (!(r < hij && r > r_min)) continue;
-      const float4 vj = vjs[u];
-      const float4 fj = fjs[u];
-      const float vx = vi.x - vj.x, vy = vi.y - vj.y, vz = vi.z - vj.z;
-      const float vr = vx * dx + vy * dy + vz * dz;
-      float pij = 0.0f;
-      if (vr < 0.0f) {
-        // approximate divisions (within 2 ulp): both denominators are positive and far from the limits
-        const float mu = div_ftz(hij * vr, dd + 0.01f * hij * hij);
+        const float4 pj = pjs[u];
+        const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+        const float dd = dx * dx + dy * dy + dz * dz;
+        const float rinv = rsqrt_ftz(dd);
+        const float r = dd > 0.0f ? dd * rinv : 0.0f;
+        const float hij = pair_h(pi.w, pj.w);
+        const float4 vj = vjs[u];
+        const float4 fj = fjs[u];
+        const float vx = vi.x - vj.x, vy = vi.y - vj.y, vz = vi.z - vj.z;
+        const float vr = vx * dx + vy * dy + vz * dz;
+        // approximate reciprocals (within 2 ulp): both denominators are positive and far from the limits
+        const float mu = hij * fminf(vr, 0.0f) * rcp_ftz(dd + 0.01f * hij * hij);
         const float c_bar = 0.5f * (fi.w + fj.w);
-        const float rho_bar = 0.5f * (fi.y + fj.y);
-        pij = div_ftz(-alpha * c_bar * mu + beta * mu * mu, rho_bar);
-      }
-      const float coeff = fi.z + fj.z + pij;
-      float w, dw, dwdh;
-      kern_pair<KERNEL>(r, hij, w, dw, dwdh);
-      const float dwr = dw * rinv;  // ∇_i W = (dx/r) ∂W/∂r
-      const float gx = dx * dwr, gy = dy * dwr, gz = dz * dwr;
-      const float s = -coeff * fj.x;
-      ax += gx * s;
-      ay += gy * s;
-      az += gz * s;
-      const float vg = vx * gx + vy * gy + vz * gz;
-      de += 0.5f * fj.x * coeff * vg;
-      if (DIVV) dv += fj.x * vg;
+        const float pij = (beta * mu - alpha * c_bar) * mu * rcp_ftz(0.5f * (fi.y + fj.y));
+        const float coeff = fi.z + fj.z + pij;
+        float w, dw, dwdh;
+        kern_pair_bf<KERNEL>(r, hij, w, dw, dwdh);
+        const float dwr = r > r_min ? dw * rinv : 0.0f;  // ∇_i W = (dx/r) ∂W/∂r
+        const float gx = dx * dwr, gy = dy * dwr, gz = dz * dwr;
+        const float s = -coeff * fj.x;
+        ax += gx * s;
+        ay += gy * s;
+        az += gz * s;
+        const float vg = vx * gx + vy * gy + vz * gz;
+        de += 0.5f * fj.x * coeff * vg;
+        if (DIVV) dv += fj.x * vg;
       }
     }
     if (GRAV) {
@@ -454,7 +449,7 @@ __global__ void k_forces(int n, State st, const float4* __restrict__ fdata, cons
 int launch_forces(const Dev& d, const Cfg& c, cudaStream_t s) {
   const int blocks = (d.n + c.blk - 1) / c.blk;
   const bool g = c.gravity != 2;
-#define FARGS d.n, d.s(), d.fdata, d.nbr, d.nbr_cnt, d.nbr_cap, d.grav, d.P, d.segs, d.acc, d.divv
+#define FARGS d.n, d.s(), d.fdata, d.nbr, d.nbr_cnt, d.nbr_cap, d.sent, d.grav, d.P, d.segs, d.acc, d.divv
   if (c.divv) {
     if (c.kernel == 1) {
       if (g) k_forces<1, true, true><<<blocks, c.blk, 0, s>>>(FARGS);

@@ -106,12 +106,12 @@ sph_status alloc_dev(sph_ctx* ctx, Dev& d, uint32_t cap, uint32_t K, uint32_t nb
   const size_t nodes = 2 * Lmax;
   for (int b = 0; b < 2; ++b) {
     State& s = d.st[b];
-    ALLOC(s.pos_h, capw);
-    ALLOC(s.vel_u, capw);
+    ALLOC(s.pos_h, capw + 32);  // + the sentinel record at index capw (the gather kernels' list filler)
+    ALLOC(s.vel_u, capw + 32);
     ALLOC(s.x, capw);
     ALLOC(s.y, capw);
     ALLOC(s.z, capw);
-    ALLOC(s.mass, capw);
+    ALLOC(s.mass, capw + 32);
     ALLOC(s.mat, capw);
     ALLOC(s.prov, capw);
     ALLOC(s.id, capw);
@@ -148,7 +148,7 @@ sph_status alloc_dev(sph_ctx* ctx, Dev& d, uint32_t cap, uint32_t K, uint32_t nb
     ALLOC(d.nbr, capw * nbr_cap);
     ALLOC(d.nbr_cnt, capw);
     ALLOC(d.rho, capw);
-    ALLOC(d.fdata, capw);
+    ALLOC(d.fdata, capw + 32);
     ALLOC(d.acc, capw);
     ALLOC(d.hnew, capw);
     ALLOC(d.h0, capw);
@@ -162,6 +162,19 @@ sph_status alloc_dev(sph_ctx* ctx, Dev& d, uint32_t cap, uint32_t K, uint32_t nb
     uint8_t* aos = nullptr;
     ALLOC(aos, capw * 48);
     d.aos = aos;
+    // The sentinel particle: massless, at rest, h = 0 and 1e18 m out on every axis, so it lies outside every
+    // support (W, ∇W = 0) and its terms vanish; its force record (m 0, ρ 1, P/ρ² 0, c 0) keeps the AV finite.
+    // The permutation and the passes write indices below n only, so it stays as written here.
+    d.sent = (unsigned)capw;
+    const float4 far = make_float4(1.0e18f, 1.0e18f, 1.0e18f, 0.0f), zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 rec = make_float4(0.0f, 1.0f, 0.0f, 0.0f);
+    const float zm = 0.0f;
+    for (int b = 0; b < 2; ++b) {
+      CK(cudaMemcpy(d.st[b].pos_h + capw, &far, sizeof(far), cudaMemcpyHostToDevice));
+      CK(cudaMemcpy(d.st[b].vel_u + capw, &zero4, sizeof(zero4), cudaMemcpyHostToDevice));
+      CK(cudaMemcpy(d.st[b].mass + capw, &zm, sizeof(zm), cudaMemcpyHostToDevice));
+    }
+    CK(cudaMemcpy(d.fdata + capw, &rec, sizeof(rec), cudaMemcpyHostToDevice));
   }
   return SPH_OK;
 }

@@ -155,6 +155,34 @@ __device__ __forceinline__ void kern_pair(float r, float h, float& w, float& dwd
   dwdh = -sih * (3.0f * f + q * fp);
 }
 
+// The same kernel with the support test folded into the polynomial: t = max(1 − q, 0) (and, for the cubic
+// spline, s = max(½ − q, 0), f = 2t³ − 8s³, which is 1 − 6q² + 6q³ below q = ½), so every term vanishes for
+// q ≥ 1 and the gather loops evaluate a pair without a branch. Equal to kern_pair to a few ulp inside the
+// support.
+template <int KERNEL>
+__device__ __forceinline__ void kern_pair_bf(float r, float h, float& w, float& dwdr, float& dwdh) {
+  const float ih = rcp_ftz(h);
+  const float q = r * ih;
+  const float t = fmaxf(1.0f - q, 0.0f);
+  float f, fp;
+  if (KERNEL == 1) {
+    const float t3 = t * t * t;
+    f = t3 * t * (1.0f + 4.0f * q);
+    fp = -20.0f * q * t3;
+  } else {
+    const float u = fmaxf(0.5f - q, 0.0f);
+    const float t2 = t * t, u2 = u * u;
+    f = 2.0f * t2 * t - 8.0f * u2 * u;
+    fp = 24.0f * u2 - 6.0f * t2;
+  }
+  const float c = KERNEL == 1 ? 3.34225380f : 2.54647909f;
+  const float sig = c * ih * ih * ih;
+  const float sih = sig * ih;
+  w = sig * f;
+  dwdr = sih * fp;
+  dwdh = -sih * (3.0f * f + q * fp);
+}
+
 // ---- Tillotson EOS in f32 (sph_step.wgsl:78-100), SI guards carried as parameters --------------------
 __device__ __forceinline__ float tillotson_p(const Eos& e, float rho, float u, float rho_floor) {
   const float r = fmaxf(rho, rho_floor);

@@ -132,6 +132,7 @@ __device__ __forceinline__ void seg_res_max(Seg* segs, unsigned sg, float v) {
 
 struct Dev {
   int n = 0, cap = 0;
+  unsigned sent = 0;  // index of the sentinel record (the gather kernels' list filler), past the capacity
   int K = 1;        // leaf size
   int L = 0;        // number of leaves
   State st[2];
