@@ -243,6 +243,8 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
 
   Acc3 acc;
   float phi = 0.f;
+  // the far loop's packed sums (two sources per FP32x2 instruction), folded into acc at the end
+  float2 fx2 = make_float2(0.f, 0.f), fy2 = fx2, fz2 = fx2, fphi2 = fx2;
   unsigned cnt = 0;
   unsigned overflow = 0;
   unsigned* stack = S.stack[w];
@@ -277,6 +279,10 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
     }
     return src;
   };
+  // Without hi/lo coordinates the chunk is staged as 16 source pairs, (x₀ x₁ y₀ y₁) and (z₀ z₁ m₀ m₁) in two
+  // consecutive float4, and each pair is evaluated with the packed FP32x2 operations of sm_100 (add, multiply
+  // and fused multiply-add on two lanes of a register pair, each rounded as its scalar form): one instruction
+  // does both sources' arithmetic, the reciprocal square roots stay scalar.
   auto flush_far = [&](int count) {
     const int per = far_per;
     float4 nxt = far_source(0, count);
@@ -284,9 +290,36 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
       float4 src = nxt;
       if (base + per < count) nxt = far_source(base + per, count);
       src.w *= G;
-      S.src[w][lane] = src;
+      if (HILO) {
+        S.src[w][lane] = src;
+      } else {
+        float* f = reinterpret_cast<float*>(&S.src[w][0]) + 8 * (lane >> 1) + (lane & 1u);
+        f[0] = src.x;
+        f[2] = src.y;
+        f[4] = src.z;
+        f[6] = src.w;
+      }
       __syncwarp();
-      if (valid) {
+      if (valid && !HILO) {
+        const float2 npx = make_float2(-pi.x, -pi.x), npy = make_float2(-pi.y, -pi.y),
+                     npz = make_float2(-pi.z, -pi.z), s2 = make_float2(soft2, soft2);
+#pragma unroll 4
+        for (int k = 0; k < 16; ++k) {
+          const float4 xy = S.src[w][2 * k], zm = S.src[w][2 * k + 1];
+          const float2 dx = __fadd2_rn(make_float2(xy.x, xy.y), npx);
+          const float2 dy = __fadd2_rn(make_float2(xy.z, xy.w), npy);
+          const float2 dz = __fadd2_rn(make_float2(zm.x, zm.y), npz);
+          const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, s2)));
+          const float2 rinv = make_float2(rsqrt_ftz(r2.x), rsqrt_ftz(r2.y));
+          const float2 gm = __fmul2_rn(make_float2(zm.z, zm.w), rinv);
+          const float2 g = __fmul2_rn(__fmul2_rn(gm, rinv), rinv);
+          fx2 = __ffma2_rn(g, dx, fx2);
+          fy2 = __ffma2_rn(g, dy, fy2);
+          fz2 = __ffma2_rn(g, dz, fz2);
+          if (OUT != kWalkAcc) fphi2 = __fadd2_rn(fphi2, make_float2(-gm.x, -gm.y));
+        }
+      }
+      if (valid && HILO) {
 #pragma unroll 4
         for (int k = 0; k < 32; ++k) {
           const float4 bj = S.src[w][k];
@@ -702,6 +735,10 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
   }  // parts
 
   if (in_group && GRAV) {
+    if (!HILO) {
+      acc.add<false>(fx2.x + fx2.y, fy2.x + fy2.y, fz2.x + fz2.y);
+      phi += fphi2.x + fphi2.y;
+    }
     if (OUT == kWalkPhi) reinterpret_cast<float*>(gout)[4 * (size_t)t + 3] = phi;
     else gout[t] = make_float4(acc.x, acc.y, acc.z, OUT == kWalkAccPhi ? phi : 0.0f);
   }
