@@ -447,6 +447,65 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
     }
     return sidx;
   };
+  // The neighbour test and the append of one source that passed it (the list keeps the chunk's order).
+  auto near_append = [&](bool inside, int s) {
+    if (inside) {
+      if (cnt < cap) nbr[nbr_slot((unsigned)t, cnt, cap)] = (unsigned)s;
+      ++cnt;
+    }
+  };
+  // Without hi/lo coordinates: sources in pairs, as in the far loop (the pair (x₀ x₁ y₀ y₁)(z₀ z₁ m₀ m₁) and
+  // (index₀ index₁ h₀ h₁)); every packed operation rounds as its scalar form, so the distances and the
+  // predicate are those of the scalar loop below, source by source.
+  auto near_pairs = [&](auto loose) {
+    const float2 npx = make_float2(-pi.x, -pi.x), npy = make_float2(-pi.y, -pi.y), npz = make_float2(-pi.z, -pi.z);
+    const float2 s2 = make_float2(soft2, soft2);
+    const float4* shp = reinterpret_cast<const float4*>(&S.sh[w][0]);
+#pragma unroll 2
+    for (int k = 0; k < 16; ++k) {
+      const float4 xy = S.src[w][2 * k], zm = S.src[w][2 * k + 1], sh = shp[k];
+      const int sa = __float_as_int(sh.x), sb = __float_as_int(sh.y);
+      const bool oa = sa != t, ob = sb != t;
+      const float2 dx = __fadd2_rn(make_float2(xy.x, xy.y), npx);
+      const float2 dy = __fadd2_rn(make_float2(xy.z, xy.w), npy);
+      const float2 dz = __fadd2_rn(make_float2(zm.x, zm.y), npz);
+      float2 dd;
+      if constexpr (decltype(loose)::value) dd = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+      else dd = __fadd2_rn(__fadd2_rn(__fmul2_rn(dx, dx), __fmul2_rn(dy, dy)), __fmul2_rn(dz, dz));
+      if (NBR) {
+        bool ia, ib;
+        if constexpr (decltype(loose)::value) {
+          const float2 lim = __ffma2_rn(make_float2(sh.z, sh.w), make_float2(lim_j, lim_j), make_float2(lim_i, lim_i));
+          const float2 l2 = __fmul2_rn(lim, lim);
+          ia = dd.x < l2.x;
+          ib = dd.y < l2.y;
+        } else {
+          const float2 lim = __fmul2_rn(make_float2(0.5f, 0.5f), __fadd2_rn(make_float2(pi.w, pi.w), make_float2(sh.z, sh.w)));
+          const float2 q = __fmul2_rn(lim, lim);
+          const float2 qlo = __fmul2_rn(q, make_float2(1.0f - 1.9073486e-6f, 1.0f - 1.9073486e-6f));
+          const float2 qhi = __fmul2_rn(q, make_float2(1.0f + 1.9073486e-6f, 1.0f + 1.9073486e-6f));
+          ia = dd.x < qlo.x;
+          if (!ia && !(dd.x > qhi.x)) ia = fsqrt(dd.x) < lim.x;
+          ib = dd.y < qlo.y;
+          if (!ib && !(dd.y > qhi.y)) ib = fsqrt(dd.y) < lim.y;
+        }
+        near_append(oa && ia, sa);
+        near_append(ob && ib, sb);
+      }
+      if (GRAV) {
+        // the particle itself (d = 0) gets r² = 1: a finite g times a zero offset adds nothing
+        const float2 r2s = __fadd2_rn(dd, s2);
+        const float2 r2 = make_float2(oa ? r2s.x : 1.0f, ob ? r2s.y : 1.0f);
+        const float2 rinv = make_float2(rsqrt_ftz(r2.x), rsqrt_ftz(r2.y));
+        const float2 gm = __fmul2_rn(make_float2(zm.z, zm.w), rinv);
+        const float2 g = __fmul2_rn(__fmul2_rn(gm, rinv), rinv);
+        fx2 = __ffma2_rn(g, dx, fx2);
+        fy2 = __ffma2_rn(g, dy, fy2);
+        fz2 = __ffma2_rn(g, dz, fz2);
+        if (OUT != kWalkAcc) fphi2 = __fadd2_rn(fphi2, make_float2(oa ? -gm.x : 0.0f, ob ? -gm.y : 0.0f));
+      }
+    }
+  };
   auto near_sources = [&](auto loose) {
 #pragma unroll 4
     for (int k = 0; k < 32; ++k) {
@@ -472,10 +531,7 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
           inside = dd < fmul(q, 1.0f - 1.9073486e-6f);
           if (!inside && !(dd > fmul(q, 1.0f + 1.9073486e-6f))) inside = fsqrt(dd) < lim;
         }
-        if (inside) {
-          if (cnt < cap) nbr[nbr_slot((unsigned)t, cnt, cap)] = (unsigned)s;
-          ++cnt;
-        }
+        near_append(inside, s);
       }
       if (GRAV) {
         float ex = dx, ey = dy, ez = dz, d2 = dd;
@@ -507,10 +563,25 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
       const int sidx = nidx;
       if (base + per < count) nidx = near_source(base + per, count, nsrc, nh);
       src.w *= G;
-      S.src[w][lane] = src;
-      S.sh[w][lane] = make_float2(__int_as_float(sidx), hsrc);
+      if (HILO) {
+        S.src[w][lane] = src;
+        S.sh[w][lane] = make_float2(__int_as_float(sidx), hsrc);
+      } else {
+        float* f = reinterpret_cast<float*>(&S.src[w][0]) + 8 * (lane >> 1) + (lane & 1u);
+        f[0] = src.x;
+        f[2] = src.y;
+        f[4] = src.z;
+        f[6] = src.w;
+        float* e = reinterpret_cast<float*>(&S.sh[w][0]) + 4 * (lane >> 1) + (lane & 1u);
+        e[0] = __int_as_float(sidx);
+        e[2] = hsrc;
+      }
       __syncwarp();
-      if (valid) {
+      if (valid && !HILO) {
+        if (NBR && skin > 0.0f) near_pairs(std::true_type{});
+        else near_pairs(std::false_type{});
+      }
+      if (valid && HILO) {
         // A list built with a skin is a candidate set: the gather kernels keep r < h_ij at the current h,
         // and the smoothing-length solve holds h below h0·(1 + skin)·0.999, so every superset of the exact
         // predicate gives the same sums in the same order. With a skin the test is therefore a conservative
