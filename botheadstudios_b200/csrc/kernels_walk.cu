@@ -375,23 +375,92 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
   };
 
   // ---- multipole list: stage 32 nodes in shared memory, then every lane applies them -------------------
+  // Without hi/lo coordinates the nodes are staged in pairs, (x₀ x₁ y₀ y₁)(z₀ z₁ m₀ m₁) in src,
+  // (Qxx Qyy)(Qzz Qxy) pairs in q0 and (Qxz Qyz) pairs in q1, and evaluated two at a time with the packed
+  // FP32x2 operations; an odd chunk is padded with a massless node far away.
   auto flush_m2p = [&](int count) {
     for (int base = 0; base < count; base += 32) {
       const int m = min(32, count - base);
-      if ((int)lane < m) {
-        // staged with G folded in: (com, G·M) and G·Q
-        float4 c, q;
-        float2 b;
-        load_multipole(S.m2p[w][base + lane], c, q, b);
-        c.w *= G;
-        S.src[w][lane] = c;
+      if (HILO) {
+        if ((int)lane < m) {
+          // staged with G folded in: (com, G·M) and G·Q
+          float4 c, q;
+          float2 b;
+          load_multipole(S.m2p[w][base + lane], c, q, b);
+          c.w *= G;
+          S.src[w][lane] = c;
+          if (QUAD) {
+            S.q0[w][lane] = make_float4(G * q.x, G * q.y, G * q.z, G * q.w);
+            S.q1[w][lane] = make_float2(G * b.x, G * b.y);
+          }
+        }
+      } else if ((int)lane < ((m + 1) & ~1)) {
+        float4 c = make_float4(3.0e18f, 3.0e18f, 3.0e18f, 0.0f), q = make_float4(0.f, 0.f, 0.f, 0.f);
+        float2 b = make_float2(0.f, 0.f);
+        if ((int)lane < m) load_multipole(S.m2p[w][base + lane], c, q, b);
+        float* f = reinterpret_cast<float*>(&S.src[w][0]) + 8 * (lane >> 1) + (lane & 1u);
+        f[0] = c.x;
+        f[2] = c.y;
+        f[4] = c.z;
+        f[6] = G * c.w;
         if (QUAD) {
-          S.q0[w][lane] = make_float4(G * q.x, G * q.y, G * q.z, G * q.w);
-          S.q1[w][lane] = make_float2(G * b.x, G * b.y);
+          float* g0 = reinterpret_cast<float*>(&S.q0[w][0]) + 8 * (lane >> 1) + (lane & 1u);
+          g0[0] = G * q.x;
+          g0[2] = G * q.y;
+          g0[4] = G * q.z;
+          g0[6] = G * q.w;
+          float* g1 = reinterpret_cast<float*>(&S.q1[w][0]) + 4 * (lane >> 1) + (lane & 1u);
+          g1[0] = G * b.x;
+          g1[2] = G * b.y;
         }
       }
       __syncwarp();
-      if (valid) {
+      if (valid && !HILO) {
+        const float2 npx = make_float2(-pi.x, -pi.x), npy = make_float2(-pi.y, -pi.y),
+                     npz = make_float2(-pi.z, -pi.z), s2 = make_float2(soft2, soft2);
+        const float4* q1p = reinterpret_cast<const float4*>(&S.q1[w][0]);
+        const int mp = (m + 1) >> 1;
+        for (int k = 0; k < mp; ++k) {
+          const float4 xy = S.src[w][2 * k], zm = S.src[w][2 * k + 1];
+          const float2 dx = __fadd2_rn(make_float2(xy.x, xy.y), npx);
+          const float2 dy = __fadd2_rn(make_float2(xy.z, xy.w), npy);
+          const float2 dz = __fadd2_rn(make_float2(zm.x, zm.y), npz);
+          const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, s2)));
+          const float2 rinv = make_float2(rsqrt_ftz(r2.x), rsqrt_ftz(r2.y));
+          const float2 rinv2 = __fmul2_rn(rinv, rinv);
+          const float2 mm = make_float2(zm.z, zm.w);
+          const float2 gm = __fmul2_rn(mm, rinv);  // G M / R
+          const float2 g = __fmul2_rn(gm, rinv2);  // G M / R³
+          if (QUAD) {
+            // as the scalar form below: a = d (G M/R³ + 5/2 eᵀQe/R⁵) − Q e/R⁴, φ = −G M/R − ½ eᵀQe/R³
+            const float4 qa = S.q0[w][2 * k], qb = S.q0[w][2 * k + 1], qc = q1p[k];
+            const float2 qxx = make_float2(qa.x, qa.y), qyy = make_float2(qa.z, qa.w);
+            const float2 qzz = make_float2(qb.x, qb.y), qxy = make_float2(qb.z, qb.w);
+            const float2 qxz = make_float2(qc.x, qc.y), qyz = make_float2(qc.z, qc.w);
+            const float2 ex = __fmul2_rn(dx, rinv), ey = __fmul2_rn(dy, rinv), ez = __fmul2_rn(dz, rinv);
+            const float2 Qex = __ffma2_rn(qxz, ez, __ffma2_rn(qxy, ey, __fmul2_rn(qxx, ex)));
+            const float2 Qey = __ffma2_rn(qyz, ez, __ffma2_rn(qyy, ey, __fmul2_rn(qxy, ex)));
+            const float2 Qez = __ffma2_rn(qzz, ez, __ffma2_rn(qyz, ey, __fmul2_rn(qxz, ex)));
+            const float2 eQe = __ffma2_rn(ez, Qez, __ffma2_rn(ey, Qey, __fmul2_rn(ex, Qex)));
+            const float2 rinv4 = __fmul2_rn(rinv2, rinv2);
+            const float2 nr4 = make_float2(-rinv4.x, -rinv4.y);
+            const float2 c1 = __ffma2_rn(__fmul2_rn(make_float2(2.5f, 2.5f), eQe), __fmul2_rn(rinv4, rinv), g);
+            fx2 = __ffma2_rn(nr4, Qex, __ffma2_rn(c1, dx, fx2));
+            fy2 = __ffma2_rn(nr4, Qey, __ffma2_rn(c1, dy, fy2));
+            fz2 = __ffma2_rn(nr4, Qez, __ffma2_rn(c1, dz, fz2));
+            if (OUT != kWalkAcc) {
+              const float2 t = __ffma2_rn(__fmul2_rn(make_float2(0.5f, 0.5f), eQe), rinv2, mm);
+              fphi2 = __ffma2_rn(make_float2(-t.x, -t.y), rinv, fphi2);
+            }
+          } else {
+            fx2 = __ffma2_rn(g, dx, fx2);
+            fy2 = __ffma2_rn(g, dy, fy2);
+            fz2 = __ffma2_rn(g, dz, fz2);
+            if (OUT != kWalkAcc) fphi2 = __fadd2_rn(fphi2, make_float2(-gm.x, -gm.y));
+          }
+        }
+      }
+      if (valid && HILO) {
         for (int k = 0; k < m; ++k) {
           const float4 c = S.src[w][k];
           float dx = c.x - pi.x, dy = c.y - pi.y, dz = c.z - pi.z;
