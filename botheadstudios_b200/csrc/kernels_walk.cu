@@ -25,7 +25,7 @@
 
 namespace sphb {
 
-constexpr int TW_STACK = 1536;  // per-warp node stack
+constexpr int TW_STACK = 1280;  // per-warp node stack
 constexpr int TW_LIST = 96;     // per-warp list capacity (a pop adds <= 64 entries; flushed above 32)
 constexpr int TW_WARPS_PER_SM = 24;  // resident walk warps per SM (80 registers, ~8.4 KB shared each)
 
@@ -37,6 +37,7 @@ struct WalkSmem {
   unsigned m2l[W][TW_LIST];   // accepted nodes far from the group: into the group's local expansion
   unsigned p2p[W][TW_LIST];   // near leaves: pairwise gravity + neighbour predicate
   unsigned p2f[W][TW_LIST];   // far leaves: pairwise gravity only
+  unsigned hl[W][TW_LIST];    // far leaves queued for the classification of their halves
   float4 src[W][32];   // staged sources: x, y, z, m
   float4 q0[W][32];    // staged quadrupoles
   float2 q1[W][32];
@@ -667,129 +668,158 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
   unsigned long long part_m2p = 0, part_p2p = 0, part_m2l = 0, part_src = 0;
   // One pass per pop; the pass after the stack empties flushes what the lists still hold, so that every flush
   // loop has one call site (the walk's hot code is instruction-cache bound: a second inlined copy of each flush
-  // loop measurably stalled instruction fetch).
+  // loop measurably stalled instruction fetch). With half leaves a pass is of one of two kinds: a pop of up to
+  // 32 nodes, whose far leaves are queued (S.hl), or a batch of up to 32 queued far leaves whose halves are
+  // classified, one leaf per lane. Classifying halves in the pop that found the leaf ran that code once per pop
+  // with a few lanes active; batched, it runs once per 32 leaves.
+  int nq = 0;  // far leaves queued for the half classification
   for (;;) {
-  const bool done = sp == 0;
+  const bool halves = GRAV && half > 0 && (nq >= 32 || (sp == 0 && nq > 0));
+  const bool done = sp == 0 && nq == 0;
   if (!done) {
-    const int take = min(sp, 32);
-    sp -= take;
-    st_visits += take;
-    ++st_pops;
-    const bool have = (int)lane < take;
-    const unsigned node = have ? stack[sp + lane] : 0u;
-    __syncwarp();
-    bool acc_node = false, leaf = false, open = false, near_leaf = false, far_l = false;
-    unsigned ls0 = 0u, ls1 = 1u;  // a leaf's source range, loaded alongside its box
-    unsigned lc = 0u, rc = 0u;    // an internal node's children, loaded alongside its box (no second round trip)
-    float4 lbl = make_float4(0.f, 0.f, 0.f, 0.f), lbh = lbl;  // the node's box (and max h), for the lane test
-    if (have) {
-      const float4 bl = nbmin[node], bh = nbmax[node];
-      lbl = bl;
-      lbh = bh;
-      const bool is_leaf = node >= leaf0;
-      if (is_leaf) {
-        ls0 = leaf_start[node - leaf0];
-        ls1 = leaf_start[node - leaf0 + 1];
-      } else {
-        lc = left[node];
-        rc = right[node];
-      }
-      bool near = false;
-      {
-        // SPH reach (or, for gravity alone, plain overlap with the group box so that a group's own leaves
-        // take the careful path that skips self-pairs)
-        const float reach = NBR ? 0.5f * (ghmax + bl.w) * grow : 0.0f;
-        near = (bl.x - reach <= gx1) && (bh.x + reach >= gx0) && (bl.y - reach <= gy1) && (bh.y + reach >= gy0) &&
-               (bl.z - reach <= gz1) && (bh.z + reach >= gz0);
-      }
-      bool mac = false;
-      if (GRAV) {
-        // leaves carry their own moments and may be accepted as well
-        const float4 c = ncom[node];
-        // distance from the COM to the nearest point of the group box
-        const float ddx = fmaxf(fmaxf(gx0 - c.x, c.x - gx1), 0.0f);
-        const float ddy = fmaxf(fmaxf(gy0 - c.y, c.y - gy1), 0.0f);
-        const float ddz = fmaxf(fmaxf(gz0 - c.z, c.z - gz1), 0.0f);
-        // sqrt(d² + ε²) >= r_open, compared squared (both sides are non-negative; no square root per node)
-        const float ro = bh.w * 1.00001f;
-        mac = ddx * ddx + ddy * ddy + ddz * ddz + soft2 >= ro * ro;
-        const float ux = c.x - zx, uy = c.y - zy, uz = c.z - zz;
-        far_l = ux * ux + uy * uy + uz * uz >= far2;
-      }
-      if (mac && !near) acc_node = true;
-      else if (is_leaf) leaf = GRAV || near;
-      else open = GRAV || (NBR && near);
-      if (is_leaf && ls1 <= ls0) acc_node = leaf = false;  // an empty leaf (none are built) adds nothing
-      near_leaf = leaf && near;
-    }
-    if (NBR && GRAV) {
-      // A leaf near the group box may still be out of every particle's own reach: then it can hold no
-      // neighbour and takes the cheaper far path. The test is conservative (reach with the list's skin and a
-      // margin), and a leaf holding a particle of the part is at distance 0, so self-pairs stay on the near path.
-      const unsigned cand = __ballot_sync(SPH_FULL_MASK, near_leaf);
-      unsigned keep = 0;
-      for (unsigned b = cand; b; b &= b - 1) {
-        const int k = __ffs(b) - 1;
-        const float x0 = __shfl_sync(SPH_FULL_MASK, lbl.x, k), y0 = __shfl_sync(SPH_FULL_MASK, lbl.y, k),
-                    z0 = __shfl_sync(SPH_FULL_MASK, lbl.z, k), hm = __shfl_sync(SPH_FULL_MASK, lbl.w, k);
-        const float x1 = __shfl_sync(SPH_FULL_MASK, lbh.x, k), y1 = __shfl_sync(SPH_FULL_MASK, lbh.y, k),
-                    z1 = __shfl_sync(SPH_FULL_MASK, lbh.z, k);
-        const float ex = fmaxf(fmaxf(x0 - pi.x, pi.x - x1), 0.0f), ey = fmaxf(fmaxf(y0 - pi.y, pi.y - y1), 0.0f),
-                    ez = fmaxf(fmaxf(z0 - pi.z, pi.z - z1), 0.0f);
-        const float r = 0.5f * (pi.w + hm) * grow * 1.0001f;
-        if (__any_sync(SPH_FULL_MASK, valid && ex * ex + ey * ey + ez * ez <= r * r)) keep |= 1u << k;
-      }
-      if (near_leaf && !((keep >> lane) & 1u)) near_leaf = false;
-    }
-    const bool acc_l = acc_node && far_l;
-    acc_node = acc_node && !far_l;
     // Entries of this lane: a node for the multipole lists (m0 per particle, l0 into the group's expansion), a
-    // near leaf, or a far leaf; with half leaves a far leaf becomes two entries, each half accepted as a
-    // multipole when the MAC holds for its own moments, else its <= half sources go to the far list.
-    bool m0 = acc_node, m1 = false, l0 = acc_l, l1 = false, f0 = leaf && !near_leaf, f1 = false;
-    unsigned v0 = node, v1 = 0u;                                 // multipole entries
-    unsigned fe0 = (ls0 << 5) | min(ls1 - ls0 - 1u, 31u), fe1 = 0u;  // far entries: first << 5 | (count − 1)
-    unsigned fs0 = ls1 - ls0, fs1 = 0u, fk = (unsigned)K;           // their sources, slots per far entry
-    if (GRAV && half > 0 && f0) {
-      const unsigned cl = node - leaf0, mid = ls0 + (unsigned)half;
-      const float2 rch = hrc[cl];
-      fk = (unsigned)half;
-      const unsigned nh = ls1 > mid ? 2u : 1u;
-      const float4 hA = hcom[2u * cl], hB = hcom[2u * cl + 1u];
-      unsigned hf = 0u;  // bit b: half b passes the MAC; bit 2 + b: ... and lies far enough for the expansion
+    // near leaf, a far leaf (or, with half leaves, a far leaf queued), and in a batch of queued leaves up to
+    // two of each kind, one per half: a half accepted as a multipole when the MAC holds for its own moments,
+    // else its <= half sources go to the far list.
+    bool m0 = false, m1 = false, l0 = false, l1 = false, f0 = false, f1 = false, near_leaf = false, open = false,
+         queue = false;
+    unsigned v0 = 0u, v1 = 0u;                      // multipole entries
+    unsigned fe0 = 0u, fe1 = 0u, fs0 = 0u, fs1 = 0u;  // far entries (first << 5 | (count − 1)) and their sources
+    unsigned fk = (unsigned)K;                      // slots per far entry
+    unsigned ls0 = 0u, ls1 = 1u;                    // a leaf's source range
+    unsigned lc = 0u, rc = 0u;                      // an internal node's children, loaded alongside its box
+    unsigned node = 0u;
+    if (halves) {
+      const int take = min(nq, 32);
+      nq -= take;
+      const bool have = (int)lane < take;
+      const unsigned cl = have ? S.hl[w][nq + (int)lane] : 0u;
+      __syncwarp();
+      if (have) {
+        ls0 = leaf_start[cl];
+        ls1 = leaf_start[cl + 1];
+        const unsigned mid = ls0 + (unsigned)half;
+        const float2 rch = hrc[cl];
+        fk = (unsigned)half;
+        const unsigned nh = ls1 > mid ? 2u : 1u;
+        const float4 hA = hcom[2u * cl], hB = hcom[2u * cl + 1u];
+        unsigned hf = 0u;  // bit b: half b passes the MAC; bit 2 + b: ... and lies far enough for the expansion
 #pragma unroll 1
-      for (unsigned b = 0; b < nh; ++b) {
-        const float4 hc = b ? hB : hA;
-        const float ddx = fmaxf(fmaxf(gx0 - hc.x, hc.x - gx1), 0.0f);
-        const float ddy = fmaxf(fmaxf(gy0 - hc.y, hc.y - gy1), 0.0f);
-        const float ddz = fmaxf(fmaxf(gz0 - hc.z, hc.z - gz1), 0.0f);
-        const float ro = (b ? rch.y : rch.x) * 1.00001f;
-        const bool mac_h = ddx * ddx + ddy * ddy + ddz * ddz + soft2 >= ro * ro;
-        const float ux = hc.x - zx, uy = hc.y - zy, uz = hc.z - zz;
-        const bool far_h = ux * ux + uy * uy + uz * uz >= far2;
-        hf |= (mac_h ? 1u : 0u) << b;
-        hf |= (mac_h && far_h ? 1u : 0u) << (2u + b);
+        for (unsigned b = 0; b < nh; ++b) {
+          const float4 hc = b ? hB : hA;
+          const float ddx = fmaxf(fmaxf(gx0 - hc.x, hc.x - gx1), 0.0f);
+          const float ddy = fmaxf(fmaxf(gy0 - hc.y, hc.y - gy1), 0.0f);
+          const float ddz = fmaxf(fmaxf(gz0 - hc.z, hc.z - gz1), 0.0f);
+          const float ro = (b ? rch.y : rch.x) * 1.00001f;
+          const bool mac_h = ddx * ddx + ddy * ddy + ddz * ddz + soft2 >= ro * ro;
+          const float ux = hc.x - zx, uy = hc.y - zy, uz = hc.z - zz;
+          const bool far_h = ux * ux + uy * uy + uz * uz >= far2;
+          hf |= (mac_h ? 1u : 0u) << b;
+          hf |= (mac_h && far_h ? 1u : 0u) << (2u + b);
+        }
+        m0 = (hf & 5u) == 1u;
+        l0 = (hf & 4u) != 0u;
+        f0 = (hf & 1u) == 0u;
+        v0 = 0x80000000u | (2u * cl);
+        fe0 = (ls0 << 5) | (min(ls1, mid) - ls0 - 1u);
+        fs0 = min(ls1, mid) - ls0;
+        if (nh == 2u) {
+          m1 = (hf & 10u) == 2u;
+          l1 = (hf & 8u) != 0u;
+          f1 = (hf & 2u) == 0u;
+          v1 = 0x80000000u | (2u * cl + 1u);
+          fe1 = (mid << 5) | (ls1 - mid - 1u);
+          fs1 = ls1 - mid;
+        }
       }
-      m0 = (hf & 5u) == 1u;
-      l0 = (hf & 4u) != 0u;
-      f0 = (hf & 1u) == 0u;
-      v0 = 0x80000000u | (2u * cl);
-      fe0 = (ls0 << 5) | (min(ls1, mid) - ls0 - 1u);
-      fs0 = min(ls1, mid) - ls0;
-      if (nh == 2u) {
-        m1 = (hf & 10u) == 2u;
-        l1 = (hf & 8u) != 0u;
-        f1 = (hf & 2u) == 0u;
-        v1 = 0x80000000u | (2u * cl + 1u);
-        fe1 = (mid << 5) | (ls1 - mid - 1u);
-        fs1 = ls1 - mid;
+    } else {
+      const int take = min(sp, 32);
+      sp -= take;
+      st_visits += take;
+      ++st_pops;
+      const bool have = (int)lane < take;
+      node = have ? stack[sp + lane] : 0u;
+      __syncwarp();
+      bool acc_node = false, leaf = false, far_l = false;
+      float4 lbl = make_float4(0.f, 0.f, 0.f, 0.f), lbh = lbl;  // the node's box (and max h), for the lane test
+      if (have) {
+        const float4 bl = nbmin[node], bh = nbmax[node];
+        lbl = bl;
+        lbh = bh;
+        const bool is_leaf = node >= leaf0;
+        if (is_leaf) {
+          ls0 = leaf_start[node - leaf0];
+          ls1 = leaf_start[node - leaf0 + 1];
+        } else {
+          lc = left[node];
+          rc = right[node];
+        }
+        bool near = false;
+        {
+          // SPH reach (or, for gravity alone, plain overlap with the group box so that a group's own leaves
+          // take the careful path that skips self-pairs)
+          const float reach = NBR ? 0.5f * (ghmax + bl.w) * grow : 0.0f;
+          near = (bl.x - reach <= gx1) && (bh.x + reach >= gx0) && (bl.y - reach <= gy1) &&
+                 (bh.y + reach >= gy0) && (bl.z - reach <= gz1) && (bh.z + reach >= gz0);
+        }
+        bool mac = false;
+        if (GRAV) {
+          // leaves carry their own moments and may be accepted as well
+          const float4 c = ncom[node];
+          // distance from the COM to the nearest point of the group box
+          const float ddx = fmaxf(fmaxf(gx0 - c.x, c.x - gx1), 0.0f);
+          const float ddy = fmaxf(fmaxf(gy0 - c.y, c.y - gy1), 0.0f);
+          const float ddz = fmaxf(fmaxf(gz0 - c.z, c.z - gz1), 0.0f);
+          // sqrt(d² + ε²) >= r_open, compared squared (both sides are non-negative; no square root per node)
+          const float ro = bh.w * 1.00001f;
+          mac = ddx * ddx + ddy * ddy + ddz * ddz + soft2 >= ro * ro;
+          const float ux = c.x - zx, uy = c.y - zy, uz = c.z - zz;
+          far_l = ux * ux + uy * uy + uz * uz >= far2;
+        }
+        if (mac && !near) acc_node = true;
+        else if (is_leaf) leaf = GRAV || near;
+        else open = GRAV || (NBR && near);
+        if (is_leaf && ls1 <= ls0) acc_node = leaf = false;  // an empty leaf (none are built) adds nothing
+        near_leaf = leaf && near;
       }
+      if (NBR && GRAV) {
+        // A leaf near the group box may still be out of every particle's own reach: then it can hold no
+        // neighbour and takes the cheaper far path. The test is conservative (reach with the list's skin and a
+        // margin), and a leaf holding a particle of the part is at distance 0, so self-pairs stay on the near
+        // path.
+        const unsigned cand = __ballot_sync(SPH_FULL_MASK, near_leaf);
+        unsigned keep = 0;
+        for (unsigned b = cand; b; b &= b - 1) {
+          const int k = __ffs(b) - 1;
+          const float x0 = __shfl_sync(SPH_FULL_MASK, lbl.x, k), y0 = __shfl_sync(SPH_FULL_MASK, lbl.y, k),
+                      z0 = __shfl_sync(SPH_FULL_MASK, lbl.z, k), hm = __shfl_sync(SPH_FULL_MASK, lbl.w, k);
+          const float x1 = __shfl_sync(SPH_FULL_MASK, lbh.x, k), y1 = __shfl_sync(SPH_FULL_MASK, lbh.y, k),
+                      z1 = __shfl_sync(SPH_FULL_MASK, lbh.z, k);
+          const float ex = fmaxf(fmaxf(x0 - pi.x, pi.x - x1), 0.0f),
+                      ey = fmaxf(fmaxf(y0 - pi.y, pi.y - y1), 0.0f),
+                      ez = fmaxf(fmaxf(z0 - pi.z, pi.z - z1), 0.0f);
+          const float r = 0.5f * (pi.w + hm) * grow * 1.0001f;
+          if (__any_sync(SPH_FULL_MASK, valid && ex * ex + ey * ey + ez * ez <= r * r)) keep |= 1u << k;
+        }
+        if (near_leaf && !((keep >> lane) & 1u)) near_leaf = false;
+      }
+      m0 = acc_node && !far_l;
+      l0 = acc_node && far_l;
+      v0 = node;
+      const bool far_leaf = leaf && !near_leaf;
+      queue = GRAV && half > 0 && far_leaf;  // its halves are classified in a later batch
+      f0 = far_leaf && !queue;
+      fe0 = (ls0 << 5) | min(ls1 - ls0 - 1u, 31u);
+      fs0 = ls1 - ls0;
     }
     const unsigned bm0 = __ballot_sync(SPH_FULL_MASK, m0), bm1 = __ballot_sync(SPH_FULL_MASK, m1);
     const unsigned bl0 = __ballot_sync(SPH_FULL_MASK, l0), bl1 = __ballot_sync(SPH_FULL_MASK, l1);
     const unsigned bf0 = __ballot_sync(SPH_FULL_MASK, f0), bf1 = __ballot_sync(SPH_FULL_MASK, f1);
     const unsigned bo = __ballot_sync(SPH_FULL_MASK, open);
     const unsigned bn = __ballot_sync(SPH_FULL_MASK, near_leaf);
+    const unsigned bq = __ballot_sync(SPH_FULL_MASK, queue);
+    if (queue) S.hl[w][nq + __popc(bq & lt)] = node - leaf0;
+    nq += __popc(bq);
     // two entries per lane: lanes below this one come first, then this lane's first and second entry
     if (m0 || m1) {
       const int k = nm + __popc(bm0 & lt) + __popc(bm1 & lt);
