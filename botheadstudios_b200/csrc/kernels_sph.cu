@@ -375,16 +375,20 @@ __global__ void k_forces(int n, State st, const float4* __restrict__ fdata, cons
     float ax = 0.f, ay = 0.f, az = 0.f, de = 0.f, dv = 0.f;
     const unsigned c = min(nbr_cnt[t], cap);
     const unsigned* lst = nbr + nbr_slot((unsigned)t, 0u, cap);
-    unsigned jn[kForceGather];
+    unsigned jn[kForceGather], jn2[kForceGather];
     list_chunk<kForceGather>(lst, 0u, c, sent, jn);
+    list_chunk<kForceGather>(lst, kForceGather, c, sent, jn2);
     for (unsigned k0 = 0; k0 < c; k0 += kForceGather) {
-      // a chunk's positions, velocities and force records in flight together, the next chunk's indices
-      // requested ahead of them
+      // a chunk's positions, velocities and force records in flight together, the indices of the two chunks
+      // after it requested ahead of them (one chunk ahead left the loads waiting on the list stream)
       unsigned jj[kForceGather];
       float4 pjs[kForceGather], vjs[kForceGather], fjs[kForceGather];
 #pragma unroll
-      for (int u = 0; u < kForceGather; ++u) jj[u] = jn[u];
-      list_chunk<kForceGather>(lst, k0 + kForceGather, c, sent, jn);
+      for (int u = 0; u < kForceGather; ++u) {
+        jj[u] = jn[u];
+        jn[u] = jn2[u];
+      }
+      list_chunk<kForceGather>(lst, k0 + 2 * kForceGather, c, sent, jn2);
 #pragma unroll
       for (int u = 0; u < kForceGather; ++u) {
         pjs[u] = st.pos_h[jj[u]];
