@@ -249,7 +249,8 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
   unsigned cnt = 0;
   unsigned overflow = 0;
   unsigned* stack = S.stack[w];
-  unsigned long long st_visits = 0, st_pops = 0, st_m2p = 0, st_p2p = 0, st_m2l = 0, st_slots = 0;
+  // per-warp counters, 32-bit (a warp's totals stay far below 2^32); the device totals are 64-bit
+  unsigned st_visits = 0, st_pops = 0, st_m2p = 0, st_p2p = 0, st_m2l = 0, st_slots = 0;
 
   for (int part = 0; part < nparts; ++part) {
   const bool valid = in_group && mypart == part;
@@ -271,12 +272,19 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
   // ---- far leaves: branch-free pairwise gravity, 32 staged sources per pass ---------------------------
   // The next chunk's sources are loaded into registers before this chunk is evaluated, so the gather
   // overlaps the arithmetic.
-  auto far_source = [&](int base, int count) {
+  // the part's interactions (counters of the walk statistics): multipole nodes, expanded nodes, pairwise
+  // slots the lanes run (partial leaves padded) and the real sources among them
+  unsigned part_m2p = 0, part_p2p = 0, part_m2l = 0, part_src = 0;
+  auto far_source = [&](int base, int count, bool& real) {
     const int per = far_per, li = far_li, off = far_off;
     float4 src = make_float4(3.0e18f, 3.0e18f, 3.0e18f, 0.0f);  // padding: massless and far away
+    real = false;
     if (li < min(per, count - base)) {
       const unsigned e = S.p2f[w][base + li];  // first source << 5 | (sources − 1)
-      if (off <= (int)(e & 31u)) src = body[(e >> 5) + off];
+      if (off <= (int)(e & 31u)) {
+        src = body[(e >> 5) + off];
+        real = true;
+      }
     }
     return src;
   };
@@ -286,10 +294,13 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
   // does both sources' arithmetic, the reciprocal square roots stay scalar.
   auto flush_far = [&](int count) {
     const int per = far_per;
-    float4 nxt = far_source(0, count);
+    part_p2p += (unsigned)count << kfsh;
+    bool nreal;
+    float4 nxt = far_source(0, count, nreal);
     for (int base = 0; base < count; base += per) {
       float4 src = nxt;
-      if (base + per < count) nxt = far_source(base + per, count);
+      part_src += __popc(__ballot_sync(SPH_FULL_MASK, nreal));
+      if (base + per < count) nxt = far_source(base + per, count, nreal);
       src.w *= G;
       if (HILO) {
         S.src[w][lane] = src;
@@ -518,9 +529,11 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
     return sidx;
   };
   // The neighbour test and the append of one source that passed it (the list keeps the chunk's order).
+  // (the particle's first list slot once, entries 32 apart: the interleaved layout of nbr_slot)
+  unsigned* const nlst = NBR ? nbr + nbr_slot((unsigned)t, 0u, cap) : nullptr;
   auto near_append = [&](bool inside, int s) {
     if (inside) {
-      if (cnt < cap) nbr[nbr_slot((unsigned)t, cnt, cap)] = (unsigned)s;
+      if (cnt < cap) nlst[(size_t)cnt * 32u] = (unsigned)s;
       ++cnt;
     }
   };
@@ -626,11 +639,13 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
     const int per = near_per;  // leaves per chunk
     float4 nsrc;
     float nh;
+    part_p2p += (unsigned)count << ksh;
     int nidx = near_source(0, count, nsrc, nh);
     for (int base = 0; base < count; base += per) {
       float4 src = nsrc;
       const float hsrc = nh;
       const int sidx = nidx;
+      part_src += __popc(__ballot_sync(SPH_FULL_MASK, sidx >= 0));
       if (base + per < count) nidx = near_source(base + per, count, nsrc, nh);
       src.w *= G;
       if (HILO) {
@@ -665,7 +680,6 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
   };
 
   const unsigned nvalid = __popc(__ballot_sync(SPH_FULL_MASK, valid));
-  unsigned long long part_m2p = 0, part_p2p = 0, part_m2l = 0, part_src = 0;
   // One pass per pop; the pass after the stack empties flushes what the lists still hold, so that every flush
   // loop has one call site (the walk's hot code is instruction-cache bound: a second inlined copy of each flush
   // loop measurably stalled instruction fetch). With half leaves a pass is of one of two kinds: a pop of up to
@@ -684,8 +698,7 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
     bool m0 = false, m1 = false, l0 = false, l1 = false, f0 = false, f1 = false, near_leaf = false, open = false,
          queue = false;
     unsigned v0 = 0u, v1 = 0u;                      // multipole entries
-    unsigned fe0 = 0u, fe1 = 0u, fs0 = 0u, fs1 = 0u;  // far entries (first << 5 | (count − 1)) and their sources
-    unsigned fk = (unsigned)K;                      // slots per far entry
+    unsigned fe0 = 0u, fe1 = 0u;                    // far entries: first << 5 | (count − 1)
     unsigned ls0 = 0u, ls1 = 1u;                    // a leaf's source range
     unsigned lc = 0u, rc = 0u;                      // an internal node's children, loaded alongside its box
     unsigned node = 0u;
@@ -700,7 +713,6 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
         ls1 = leaf_start[cl + 1];
         const unsigned mid = ls0 + (unsigned)half;
         const float2 rch = hrc[cl];
-        fk = (unsigned)half;
         const unsigned nh = ls1 > mid ? 2u : 1u;
         const float4 hA = hcom[2u * cl], hB = hcom[2u * cl + 1u];
         unsigned hf = 0u;  // bit b: half b passes the MAC; bit 2 + b: ... and lies far enough for the expansion
@@ -722,14 +734,12 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
         f0 = (hf & 1u) == 0u;
         v0 = 0x80000000u | (2u * cl);
         fe0 = (ls0 << 5) | (min(ls1, mid) - ls0 - 1u);
-        fs0 = min(ls1, mid) - ls0;
         if (nh == 2u) {
           m1 = (hf & 10u) == 2u;
           l1 = (hf & 8u) != 0u;
           f1 = (hf & 2u) == 0u;
           v1 = 0x80000000u | (2u * cl + 1u);
           fe1 = (mid << 5) | (ls1 - mid - 1u);
-          fs1 = ls1 - mid;
         }
       }
     } else {
@@ -810,7 +820,6 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
       queue = GRAV && half > 0 && far_leaf;  // its halves are classified in a later batch
       f0 = far_leaf && !queue;
       fe0 = (ls0 << 5) | min(ls1 - ls0 - 1u, 31u);
-      fs0 = ls1 - ls0;
     }
     const unsigned bm0 = __ballot_sync(SPH_FULL_MASK, m0), bm1 = __ballot_sync(SPH_FULL_MASK, m1);
     const unsigned bl0 = __ballot_sync(SPH_FULL_MASK, l0), bl1 = __ballot_sync(SPH_FULL_MASK, l1);
@@ -855,16 +864,6 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
     nf += __popc(bf0) + __popc(bf1);
     part_m2p += __popc(bm0) + __popc(bm1);
     part_m2l += __popc(bl0) + __popc(bl1);
-    {
-      // source particles of this pop's pairwise entries (low half) and the slots the lanes run for them
-      // (high half: K per near leaf, K or K/2 per far entry, the padding of partial leaves included); <= 1,024 each
-      unsigned pk = (near_leaf ? ls1 - ls0 + ((unsigned)K << 16) : 0u) + (f0 ? fs0 + (fk << 16) : 0u) +
-                    (f1 ? fs1 + (fk << 16) : 0u);
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) pk += __shfl_xor_sync(SPH_FULL_MASK, pk, o);
-      part_src += pk & 0xffffu;
-      part_p2p += pk >> 16;
-    }
   }  // !done
     __syncwarp();
     if (nm > TW_LIST - 64 || (done && nm)) {
@@ -922,12 +921,12 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
   }
   if (overflow && lane == 0) atomicOr(&P->flags, kFlagStackOverflow);
   if (lane == 0 && OUT != kWalkPhi) {  // a diagnostic's potential walk is not a step's walk
-    atomicAdd(&P->stat_visits, st_visits);
-    atomicAdd(&P->stat_pops, st_pops);
-    atomicAdd(&P->stat_m2p, st_m2p);
-    atomicAdd(&P->stat_p2p, st_p2p);
-    atomicAdd(&P->stat_m2l, st_m2l);
-    atomicAdd(&P->stat_p2p_slots, st_slots);
+    atomicAdd(&P->stat_visits, (unsigned long long)st_visits);
+    atomicAdd(&P->stat_pops, (unsigned long long)st_pops);
+    atomicAdd(&P->stat_m2p, (unsigned long long)st_m2p);
+    atomicAdd(&P->stat_p2p, (unsigned long long)st_p2p);
+    atomicAdd(&P->stat_m2l, (unsigned long long)st_m2l);
+    atomicAdd(&P->stat_p2p_slots, (unsigned long long)st_slots);
   }
 }
 
