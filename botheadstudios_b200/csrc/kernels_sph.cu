@@ -38,14 +38,18 @@ __device__ __forceinline__ void list_chunk(const unsigned* __restrict__ lst, uns
 #pragma unroll
   for (int u = 0; u < G; ++u) j[u] = k0 + u < c ? __ldcs(&lst[(size_t)(k0 + u) * 32u]) : sent;
 }
-// Records of the chunk whose indices are in `jn` (k0 = its first slot); on return jn holds the next chunk's.
+// Records of the chunk whose indices are in `jn` (k0 = its first slot); jn2 holds the next chunk's indices.
+// On return jn holds the next chunk's and jn2 the one after it: the list stays two chunks ahead of the records.
 __device__ __forceinline__ void gather_pos_mass(const State& st, const unsigned* __restrict__ lst, unsigned k0,
                                                 unsigned c, unsigned sent, unsigned jn[kGather],
-                                                float4 pj[kGather], float mj[kGather]) {
+                                                unsigned jn2[kGather], float4 pj[kGather], float mj[kGather]) {
   unsigned j[kGather];
 #pragma unroll
-  for (int u = 0; u < kGather; ++u) j[u] = jn[u];
-  list_chunk<kGather>(lst, k0 + kGather, c, sent, jn);
+  for (int u = 0; u < kGather; ++u) {
+    j[u] = jn[u];
+    jn[u] = jn2[u];
+  }
+  list_chunk<kGather>(lst, k0 + 2 * kGather, c, sent, jn2);
 #pragma unroll
   for (int u = 0; u < kGather; ++u) {
     pj[u] = st.pos_h[j[u]];
@@ -81,12 +85,13 @@ __global__ void k_density_eos(int n, State st, const unsigned* __restrict__ nbr,
   float r_i = m * w;
   const unsigned c = min(nbr_cnt[t], cap);
   const unsigned* lst = nbr + nbr_slot((unsigned)t, 0u, cap);
-  unsigned jn[kGather];
+  unsigned jn[kGather], jn2[kGather];
   list_chunk<kGather>(lst, 0u, c, sent, jn);
+  list_chunk<kGather>(lst, kGather, c, sent, jn2);
   for (unsigned k0 = 0; k0 < c; k0 += kGather) {
     float4 pj[kGather];
     float mj[kGather];
-    gather_pos_mass(st, lst, k0, c, sent, jn, pj, mj);
+    gather_pos_mass(st, lst, k0, c, sent, jn, jn2, pj, mj);
 #pragma unroll
     for (int u = 0; u < kGather; ++u) {
       float ri;
@@ -143,12 +148,13 @@ __device__ __forceinline__ void h_sums(int t, const State& st, const unsigned* _
   float dsum = 0.0f;  // Σ m_j ∂W/∂h_ij; ∂h_ij/∂h_i = ½ is applied once
   const unsigned c = min(nbr_cnt[t], cap);
   const unsigned* lst = nbr + nbr_slot((unsigned)t, 0u, cap);
-  unsigned jn[kGather];
+  unsigned jn[kGather], jn2[kGather];
   list_chunk<kGather>(lst, 0u, c, sent, jn);
+  list_chunk<kGather>(lst, kGather, c, sent, jn2);
   for (unsigned k0 = 0; k0 < c; k0 += kGather) {
     float4 pj[kGather];
     float mj[kGather];
-    gather_pos_mass(st, lst, k0, c, sent, jn, pj, mj);
+    gather_pos_mass(st, lst, k0, c, sent, jn, jn2, pj, mj);
 #pragma unroll
     for (int u = 0; u < kGather; ++u) {
       float ri;

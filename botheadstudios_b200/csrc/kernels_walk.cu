@@ -10,15 +10,21 @@
 //                 node's box is outside the SPH reach: appended to the multipole list;
 //   * leaf      — appended to the near list (pairwise gravity + the neighbour test) when some particle of the
 //                 group can reach it with its own smoothing length (a per-lane test after the group test),
-//                 otherwise to the far list (pairwise gravity only);
+//                 otherwise to the far list (pairwise gravity only); with half leaves a far leaf is queued, and
+//                 a later pass classifies the halves of up to 32 queued leaves at once (each half a multipole,
+//                 a term of the group's local expansion, or 8 pairwise sources);
 //   * opened    — children pushed (ballot + popc compaction).
+// Accepted nodes far from the group (beyond r_group/θ_L) go into the group's local expansion instead of the
+// per-particle multipole list.
 // Nodes whose box lies within ½(h_group,max + h_node,max) of the group are always opened, so every leaf
 // that can hold an SPH neighbour reaches the direct list: the neighbour set {j != i : r_ij < h_ij} is
 // complete. Without a skin (fixed h) the test is the reference predicate, single-rounded, so the set is
 // identical to it (sph_step.wgsl:141-143); with a skin the list is a candidate set that contains it.
 // Lists are flushed through shared memory in chunks of 32 sources (the next chunk's loads issued before the
-// current chunk is evaluated); every lane then runs the chunk against its own particle with no dependent loads
-// (the interaction loop is pure FP32 work, its reciprocal square root the bare special-function operation).
+// current chunk is evaluated); every lane then runs the chunk against its own particle with no dependent loads.
+// The interaction loops take the staged sources two at a time with the packed FP32x2 add/multiply/fma of sm_100
+// (each half rounded as the scalar operation); their reciprocal square roots are the bare special-function
+// operation.
 #include <type_traits>
 
 #include "sph_kernels.cuh"
