@@ -75,6 +75,7 @@ class Autotuner:
         if cache_path and os.path.exists(cache_path):
             self.cache = json.load(open(cache_path))
         self.log = []
+        self.bucket_logs = {}  # bucket → the measurements its own tuning made (none for a cached choice)
 
     def _key(self, bucket: int) -> str:
         import torch
@@ -98,6 +99,7 @@ class Autotuner:
         key = self._key(bucket)
         if key in self.cache:
             return dict(self.cache[key])
+        start = len(self.log)
         best = dict(DEFAULT_CHOICE)
         best_rate = self.measure(probe, best)
         timed = [dict(best)]  # each configuration is timed once (a coordinate's first value may already be)
@@ -110,6 +112,7 @@ class Autotuner:
                 r = self.measure(probe, trial)
                 if r > best_rate:
                     best, best_rate = trial, r
+        self.bucket_logs[bucket] = self.log[start:]
         self.cache[key] = best
         if self.cache_path:
             json.dump(self.cache, open(self.cache_path, "w"), indent=1)
@@ -134,6 +137,34 @@ def context_groups(bucket_ids, choices: dict) -> list:
         else:
             groups.append([b])
     return groups
+
+
+UNIFY_TOL = 0.03
+
+
+def unify_tree_choices(choices: dict, bucket_logs: dict, particles: dict, tol: float = UNIFY_TOL) -> dict:
+    """One context (one launch per phase) for the whole batch where the measurements allow it. The tree choice
+    (leaf size, walk tile) of the bucket with the most particles is taken by every other bucket whose own
+    measurements put that tree choice within `tol` of its best rate (with the block size it measured best
+    under it). A bucket with no such measurement (a cached choice, or the tree choice never timed on it) keeps
+    its own choice."""
+    if not choices:
+        return {}
+    lead = max(choices, key=lambda b: particles.get(b, 0))
+    tree = {k: choices[lead][k] for k in TREE_KEYS}
+    out = {}
+    for b, ch in choices.items():
+        out[b] = dict(ch)
+        log = bucket_logs.get(b) or []
+        if all(ch[k] == tree[k] for k in TREE_KEYS) or not log:
+            continue
+        best = max(e["rate"] for e in log)
+        same = [e for e in log if all(e["choice"][k] == tree[k] for k in TREE_KEYS)]
+        if same:
+            e = max(same, key=lambda e: e["rate"])
+            if e["rate"] >= (1.0 - tol) * best:
+                out[b] = dict(e["choice"])
+    return out
 
 
 def group_choice(group, choices: dict, particles: dict) -> dict:
@@ -215,10 +246,14 @@ class BucketedBatch:
 def tune_buckets(B: ic.Batch, base: dict, cache_path: str | None = None, probe_particles: int = 600_000,
                  device: int = -1) -> tuple[dict, list]:
     """Autotune every bucket that `B` populates, on a probe of that bucket's impacts (about probe_particles
-    particles, the bucket's first impacts). Returns ({bucket: choice}, measurement log)."""
+    particles, the bucket's first impacts), then unify the tree choices where the measurements allow one
+    context (unify_tree_choices). Returns ({bucket: choice}, measurement log)."""
     tuner = Autotuner(base, cache_path=cache_path, device=device)
     sizes = np.diff(B.offsets).astype(np.int64)
     choices = {}
+    particles = {}
+    for n in sizes:
+        particles[bucket_of(int(n))] = particles.get(bucket_of(int(n)), 0) + int(n)
     for b in sorted({bucket_of(int(n)) for n in sizes}):
         idx, tot = [], 0
         for k, n in enumerate(sizes):
@@ -226,4 +261,4 @@ def tune_buckets(B: ic.Batch, base: dict, cache_path: str | None = None, probe_p
                 idx.append(k)
                 tot += int(n)
         choices[b] = tuner.tune(b, subset(B, idx))
-    return choices, tuner.log
+    return unify_tree_choices(choices, getattr(tuner, "bucket_logs", {}), particles), tuner.log

@@ -121,3 +121,49 @@ def test_buckets_with_equal_walk_choices_share_one_context():
     assert batching.context_groups([0, 1, 2], {0: same, 1: dict(same, walk_warps=4), 2: same}) == [[0, 2], [1]]
     assert batching.context_groups([1], {}) == [[1]]
     assert batching.context_groups([0, 2], {}) == [[0, 2]]  # both untuned: the default choice
+
+
+def test_unify_takes_the_largest_buckets_tree_where_the_measurements_allow():
+    """A bucket takes the tree choice (leaf size, walk tile) of the bucket with the most particles when its own
+    measurements put that choice within 3 % of its best, so the batch runs as one context; otherwise, and for
+    a bucket without measurements, it keeps its own."""
+    a = dict(leaf_size=8, walk_warps=2, block_threads=256)
+    b = dict(leaf_size=16, walk_warps=2, block_threads=256)
+
+    def log(*entries):
+        return [dict(choice=c, rate=r) for c, r in entries]
+
+    choices = {0: dict(a), 1: dict(b), 2: dict(b)}
+    particles = {0: 100, 1: 500, 2: 50}
+    logs = {0: log((a, 100.0), (b, 98.0), (dict(b, block_threads=512), 99.5)),
+            1: log((b, 200.0), (a, 190.0)),
+            2: log((b, 100.0), (a, 90.0))}
+    out = batching.unify_tree_choices(choices, logs, particles)
+    # bucket 1 leads; bucket 0 measured its tree within 3 % (99.5 with 512 threads), bucket 2 already has it
+    assert out == {0: dict(b, block_threads=512), 1: b, 2: b}
+    assert batching.context_groups([0, 1, 2], out) == [[0, 1, 2]]
+    # 5 % slower than its best: bucket 0 keeps its own choice
+    logs[0] = log((a, 100.0), (b, 95.0))
+    assert batching.unify_tree_choices(choices, logs, particles)[0] == a
+    # no measurements (a cached choice) or the lead's tree never timed on it: kept
+    assert batching.unify_tree_choices(choices, {}, particles) == choices
+    logs[0] = log((a, 100.0), (dict(a, walk_warps=4), 99.0))
+    assert batching.unify_tree_choices(choices, logs, particles)[0] == a
+    assert batching.unify_tree_choices({}, {}, {}) == {}
+
+
+def test_tune_buckets_unifies_when_rates_tie(monkeypatch):
+    """Through tune_buckets: with a rate table that does not depend on the bucket, every bucket tunes to the same
+    tree, and the result is one context."""
+    B = ic.batch(6, 600, 2_000, seed=5)
+    sizes = np.diff(B.offsets).astype(np.int64)
+    m = int(np.median(sizes)) + 1
+    monkeypatch.setattr(batching, "BUCKETS", ((0, m), (m, 1 << 31)))
+
+    class Fake(_FakeTuner):
+        def __init__(self, base, cache_path=None, device=-1):
+            super().__init__(_rate)
+
+    monkeypatch.setattr(batching, "Autotuner", Fake)
+    choices, _ = batching.tune_buckets(B, dict(kernel="wendland"))
+    assert batching.context_groups(sorted(choices), choices) == [sorted(choices)]
