@@ -89,7 +89,7 @@ typedef struct sph_config {
   float h_skin;           /* SOLVE/LEARNED: neighbour lists are built at h·(1 + h_skin) and h moves at most that far
                              per rebuild, once the previous solve converged (residual <= 10·h_tol); after an
                              upload or an unconverged solve the skin is 0.15. 0 = 0.05 (at most 0.5) */
-  uint32_t walk_stack;    /* traversal-stack entries a walk may use (per warp in GROUP mode, 1,536 there; per
+  uint32_t walk_stack;    /* traversal-stack entries a walk may use (per warp in GROUP mode, 1,280 there; per
                              particle in PARTICLE mode, 64 there as in bh_gravity.wgsl:336); 0 = all of them. A
                              smaller limit is for testing the overflow path: children that do not fit are
                              skipped and SPH_ERR_OVERFLOW is raised through sph_diag (the reference drops them
@@ -406,7 +406,7 @@ uint32_t sph_dem_count(const sph_dem* dem);
  * first call before any stream capture (a first call inside a capture returns SPH_ERR_STATE). Every call
  * uses the same array, so calls whose work overlaps on the GPU (different streams, or different host threads
  * on one device) race and corrupt each other's results: order them on one stream. If the traversal stack
- * (1,536 nodes per warp) overflows, every output is NaN. A CUDA error already pending on the calling thread
+ * (1,280 nodes per warp) overflows, every output is NaN. A CUDA error already pending on the calling thread
  * is left in place and returns SPH_ERR_CUDA before any work is enqueued. */
 sph_status sph_gravity_tree_noalloc(const void* d_bodies4, uint32_t n, double G, float softening, float theta,
                                     uint32_t leaf_size, uint32_t multipole, void* d_acc4, void* stream);
