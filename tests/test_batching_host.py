@@ -124,9 +124,10 @@ def test_buckets_with_equal_walk_choices_share_one_context():
 
 
 def test_unify_takes_the_largest_buckets_tree_where_the_measurements_allow():
-    """A bucket takes the tree choice (leaf size, walk tile) of the bucket with the most particles when its own
-    measurements put that choice within 3 % of its best, so the batch runs as one context; otherwise, and for
-    a bucket without measurements, it keeps its own."""
+    """With a tolerance, a bucket takes the tree choice (leaf size, walk tile) of the bucket with the most
+    particles when its own measurements put that choice within 3 % of its best, so the batch runs as one
+    context; otherwise, and for a bucket without measurements, it keeps its own. Without one (the default)
+    every bucket takes it."""
     a = dict(leaf_size=8, walk_warps=2, block_threads=256)
     b = dict(leaf_size=16, walk_warps=2, block_threads=256)
 
@@ -138,18 +139,22 @@ def test_unify_takes_the_largest_buckets_tree_where_the_measurements_allow():
     logs = {0: log((a, 100.0), (b, 98.0), (dict(b, block_threads=512), 99.5)),
             1: log((b, 200.0), (a, 190.0)),
             2: log((b, 100.0), (a, 90.0))}
-    out = batching.unify_tree_choices(choices, logs, particles)
+    out = batching.unify_tree_choices(choices, logs, particles, tol=0.03)
     # bucket 1 leads; bucket 0 measured its tree within 3 % (99.5 with 512 threads), bucket 2 already has it
     assert out == {0: dict(b, block_threads=512), 1: b, 2: b}
     assert batching.context_groups([0, 1, 2], out) == [[0, 1, 2]]
     # 5 % slower than its best: bucket 0 keeps its own choice
     logs[0] = log((a, 100.0), (b, 95.0))
-    assert batching.unify_tree_choices(choices, logs, particles)[0] == a
+    assert batching.unify_tree_choices(choices, logs, particles, tol=0.03)[0] == a
     # no measurements (a cached choice) or the lead's tree never timed on it: kept
-    assert batching.unify_tree_choices(choices, {}, particles) == choices
+    assert batching.unify_tree_choices(choices, {}, particles, tol=0.03) == choices
     logs[0] = log((a, 100.0), (dict(a, walk_warps=4), 99.0))
-    assert batching.unify_tree_choices(choices, logs, particles)[0] == a
+    assert batching.unify_tree_choices(choices, logs, particles, tol=0.03)[0] == a
     assert batching.unify_tree_choices({}, {}, {}) == {}
+    # the default: unconditional, every bucket on the lead's tree (its own block size kept)
+    out = batching.unify_tree_choices(choices, {}, particles)
+    assert out == {0: dict(a, leaf_size=16), 1: b, 2: b}
+    assert batching.context_groups([0, 1, 2], out) == [[0, 1, 2]]
 
 
 def test_tune_buckets_unifies_when_rates_tie(monkeypatch):
