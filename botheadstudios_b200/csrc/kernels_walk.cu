@@ -250,7 +250,8 @@ __global__ void __launch_bounds__(W * 32, TW_WARPS_PER_SM / W) k_tree_walk(
 
   Acc3 acc;
   float phi = 0.f;
-  // the far loop's packed sums (two sources per FP32x2 instruction), folded into acc at the end
+  // the packed sums of the far, near and multipole loops (two sources per FP32x2 instruction: half x for the
+  // first source of each pair, half y for the second), folded into acc at the end
   float2 fx2 = make_float2(0.f, 0.f), fy2 = fx2, fz2 = fx2, fphi2 = fx2;
   unsigned cnt = 0;
   unsigned overflow = 0;
